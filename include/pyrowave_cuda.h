@@ -1,0 +1,133 @@
+/*
+ * PyroWave CUDA extension API (B200 implementation only).
+ *
+ * The reference exposes its GPU path through Vulkan images and semaphores
+ * (pyrowave.h:457-462, :528-532 of the reference). On B200 the same role is
+ * played by CUDA device pointers and a CUDA stream: these entry points encode
+ * from and decode to device memory, ordered on the caller's stream, with no
+ * host round trip. All types are plain C; the stream is a cudaStream_t.
+ *
+ * Also declared here are the introspection entry points the parity tests use:
+ * encoding a caller-provided wavelet pyramid (the reference's
+ * Encoder::encode_pre_transformed, pyrowave_encoder.hpp:44-47) and reading the
+ * pyramid and the rate-control decisions back.
+ */
+#ifndef PYROWAVE_CUDA_H_
+#define PYROWAVE_CUDA_H_
+
+#include "pyrowave.h"
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct CUstream_st *pyrowave_cuda_stream; /* cudaStream_t */
+
+/* Three 8-bit planes in device memory. For 4:2:0 the chroma planes are
+ * (width/2) x (height/2). */
+typedef struct pyrowave_cuda_planes
+{
+	void *data[3];
+	size_t row_stride_in_bytes[3];
+} pyrowave_cuda_planes;
+
+typedef struct pyrowave_cuda_layout
+{
+	int width, height, chroma444;
+	int aligned_width, aligned_height;
+	int block_count_8x8, block_count_32x32;
+	size_t pyramid_size;       /* coefficients of all transmitted bands (canonical layout) */
+	uint32_t fp16_level_mask;  /* bit L set: level L coefficients stored as FP16 */
+} pyrowave_cuda_layout;
+
+/* Coefficient storage precision per decomposition level. Default 0 (FP32 at
+ * every level); 0x3 matches the reference's default precision layout (FP16 for
+ * levels 0-1). Must be called before the first encode / decode. */
+PYROWAVE_PUBLIC_API pyrowave_result pyrowave_cuda_encoder_set_precision(pyrowave_encoder encoder, uint32_t fp16_level_mask);
+PYROWAVE_PUBLIC_API pyrowave_result pyrowave_cuda_decoder_set_precision(pyrowave_decoder decoder, uint32_t fp16_level_mask);
+
+PYROWAVE_PUBLIC_API pyrowave_result pyrowave_cuda_encoder_get_layout(pyrowave_encoder encoder, pyrowave_cuda_layout *layout);
+PYROWAVE_PUBLIC_API pyrowave_result pyrowave_cuda_decoder_get_layout(pyrowave_decoder decoder, pyrowave_cuda_layout *layout);
+
+/* Encode device planes on `stream`; returns without waiting. The packetized
+ * frame (8-byte start-of-frame header followed by the coded 32x32 blocks in
+ * block index order, exactly what pyrowave_encoder_packetize emits with an
+ * unbounded packet size) stays in device memory until the next encode. */
+PYROWAVE_PUBLIC_API pyrowave_result pyrowave_cuda_encoder_encode(pyrowave_encoder encoder,
+                                                                 const pyrowave_cuda_planes *planes,
+                                                                 const pyrowave_rate_control *rate_control,
+                                                                 pyrowave_cuda_stream stream);
+
+/* Device view of the last encode: stream = packetized frame (words), block_meta
+ * = {offset_u32, num_words} per 32x32 block (the reference's BitstreamPacket
+ * table, offsets relative to stream + 2). Valid once `stream` work completes. */
+PYROWAVE_PUBLIC_API pyrowave_result pyrowave_cuda_encoder_get_device_bitstream(pyrowave_encoder encoder,
+                                                                               const uint32_t **stream,
+                                                                               const uint32_t **block_meta,
+                                                                               size_t *capacity_words);
+
+/* Bytes of the last packetized frame (waits for the encode). */
+PYROWAVE_PUBLIC_API pyrowave_result pyrowave_cuda_encoder_get_size(pyrowave_encoder encoder, size_t *bytes);
+
+/* Encode a wavelet pyramid given in device memory in the canonical layout
+ * (transmitted bands in block-index order, each band row-major and unpadded).
+ * quant_scale < 0 uses the per-band resolutions; >= 0 overrides them
+ * (reference pyrowave_encoder.cpp:449,251). */
+PYROWAVE_PUBLIC_API pyrowave_result pyrowave_cuda_encoder_encode_pre_transformed(pyrowave_encoder encoder,
+                                                                                 const float *pyramid,
+                                                                                 const pyrowave_rate_control *rate_control,
+                                                                                 float quant_scale,
+                                                                                 pyrowave_cuda_stream stream);
+
+/* Copy the last encode's wavelet pyramid (canonical layout, device memory). */
+PYROWAVE_PUBLIC_API pyrowave_result pyrowave_cuda_encoder_read_wavelet(pyrowave_encoder encoder, float *pyramid,
+                                                                       pyrowave_cuda_stream stream);
+
+/* Host copies of the last encode's decisions (waits). Any pointer may be NULL.
+ * code_words: per 8x8; rd_cost/rd_bucket/rd_dist: 16 per 32x32; histogram: 2048
+ * savings counters (not scanned); quant: per 32x32; block_meta: 2 per 32x32. */
+typedef struct pyrowave_cuda_encoder_debug
+{
+	uint32_t *code_words;
+	uint16_t *rd_cost;
+	uint8_t *rd_bucket;
+	float *rd_dist;
+	uint32_t *histogram;
+	uint32_t *consumed;
+	int32_t *quant;
+	uint32_t *block_meta;
+	uint32_t *error_flags;
+} pyrowave_cuda_encoder_debug;
+
+PYROWAVE_PUBLIC_API pyrowave_result pyrowave_cuda_encoder_read_debug(pyrowave_encoder encoder,
+                                                                     const pyrowave_cuda_encoder_debug *debug);
+
+/* Decode the packets pushed so far into device planes on `stream` (uploads the
+ * parsed payload, then dequantises and inverse transforms). */
+PYROWAVE_PUBLIC_API pyrowave_result pyrowave_cuda_decoder_decode(pyrowave_decoder decoder,
+                                                                 const pyrowave_cuda_planes *planes,
+                                                                 pyrowave_cuda_stream stream);
+
+/* Decode coded blocks already in device memory: block_meta = {offset_u32,
+ * num_words} per 32x32 block (num_words == 0: block missing), words = the
+ * concatenated block words the offsets index. Nothing touches the host. */
+PYROWAVE_PUBLIC_API pyrowave_result pyrowave_cuda_decoder_decode_blocks(pyrowave_decoder decoder,
+                                                                        const uint32_t *block_meta,
+                                                                        const uint32_t *words, size_t num_words,
+                                                                        const pyrowave_cuda_planes *planes,
+                                                                        pyrowave_cuda_stream stream);
+
+/* Copy the last decode's dequantised pyramid (canonical layout, device memory). */
+PYROWAVE_PUBLIC_API pyrowave_result pyrowave_cuda_decoder_read_wavelet(pyrowave_decoder decoder, float *pyramid,
+                                                                       pyrowave_cuda_stream stream);
+
+/* Inverse transform of a canonical pyramid in device memory into device planes. */
+PYROWAVE_PUBLIC_API pyrowave_result pyrowave_cuda_decoder_decode_pyramid(pyrowave_decoder decoder, const float *pyramid,
+                                                                         const pyrowave_cuda_planes *planes,
+                                                                         pyrowave_cuda_stream stream);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif

@@ -74,6 +74,7 @@ def lib():
         L.oracle_get_histogram.argtypes = [c_void_p, c_void_p, c_void_p]
         L.oracle_get_bitstream_words.restype = c_size_t
         L.oracle_get_bitstream_words.argtypes = [c_void_p]
+        L.oracle_set_encoded.argtypes = [c_void_p, c_void_p, c_void_p, c_size_t, c_uint32]
         L.oracle_compute_num_packets.restype = c_size_t
         L.oracle_compute_num_packets.argtypes = [c_void_p, c_size_t]
         L.oracle_packetize.restype = c_size_t
@@ -213,7 +214,7 @@ class Oracle:
         return out
 
     def block_stats(self):
-        out = np.zeros((self.blocks8, 16), np.uint32)
+        out = np.zeros((self.blocks8, 17), np.uint32)
         self.L.oracle_get_block_stats(self.h, _ptr(out))
         return out
 
@@ -246,6 +247,16 @@ class Oracle:
         if n:
             self.L.oracle_get_bitstream(self.h, _ptr(out))
         return out
+
+    def set_encoded(self, meta: np.ndarray, words: np.ndarray, sequence: int):
+        m = np.ascontiguousarray(meta, np.uint32)
+        w = np.ascontiguousarray(words, np.uint32)
+        if w.size == 0:
+            w = np.zeros(1, np.uint32)
+            n = 0
+        else:
+            n = w.size
+        self.L.oracle_set_encoded(self.h, _ptr(m), _ptr(w), n, sequence)
 
     def compute_num_packets(self, boundary: int) -> int:
         return int(self.L.oracle_compute_num_packets(self.h, boundary))

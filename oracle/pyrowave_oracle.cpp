@@ -394,12 +394,17 @@ struct QuantStats
 	uint16_t square_error_fp16;
 	uint16_t encode_cost_bits;
 };
+// The reference's BlockStats (pyrowave_common.hpp:99-103) holds 15 entries and
+// relies on num_planes <= 14. Scaled magnitudes are clamped below 2^15 here (a
+// no-op for 8-bit content) and the table has 16 entries, so that every index
+// min(q, num_planes) with q <= 15 stays inside it.
+constexpr float MaxScaledMagnitude = 32767.0f;
 struct BlockStats
 {
 	uint32_t num_planes;
-	QuantStats errors[15];
+	QuantStats errors[16];
 };
-static_assert(sizeof(BlockStats) == 64, "BlockStats layout");
+static_assert(sizeof(BlockStats) == 68, "BlockStats layout");
 
 struct BandInfo
 {
@@ -671,10 +676,13 @@ void encode_payload_8x8(oracle_codec &c, uint32_t block_index, float texels[8][8
 	for (int s = 0; s < 8; s++)
 	{
 		for (int i = 0; i < 8; i++)
-			texels[s][i] = texels[s][i] * quant_scale;
-		max_sub[s] = max_sub[s] * quant_scale;
+		{
+			float t = texels[s][i] * quant_scale;
+			texels[s][i] = std::min(std::max(t, -MaxScaledMagnitude), MaxScaledMagnitude);
+		}
+		max_sub[s] = std::min(max_sub[s] * quant_scale, MaxScaledMagnitude);
 	}
-	max_wave = max_wave * quant_scale;
+	max_wave = std::min(max_wave * quant_scale, MaxScaledMagnitude);
 
 	float overall_quant_scale = quant_resolution_value * quant_scale;
 	float inv_quant = 1.0f / overall_quant_scale;
@@ -746,8 +754,7 @@ void encode_payload_8x8(oracle_codec &c, uint32_t block_index, float texels[8][8
 			cost_sum += std::max(r.encode_cost_early - 1, 0);
 		}
 		float square_error = butterfly8(se);
-		if (q < 15)
-			st.errors[q] = {float_to_half(std::min(square_error, 60000.0f)), uint16_t(8 * cost_sum + nsig)};
+		st.errors[q] = {float_to_half(std::min(square_error, 60000.0f)), uint16_t(8 * cost_sum + nsig)};
 	}
 
 	float total[8];
@@ -757,8 +764,7 @@ void encode_payload_8x8(oracle_codec &c, uint32_t block_index, float texels[8][8
 		total[s] = d * inv_quant_squared;
 	}
 	float square_error = butterfly8(total);
-	if (msb + 1 < 15)
-		st.errors[msb + 1] = {float_to_half(std::min(60000.0f, square_error)), 0};
+	st.errors[msb + 1] = {float_to_half(std::min(60000.0f, square_error)), 0};
 
 	// Sign byte + magnitude planes per sub-block (wavelet_quant.comp:258-289).
 	for (int s = 0; s < 8; s++)
@@ -1668,6 +1674,15 @@ size_t oracle_get_bitstream_words(const oracle_codec *c) { return c->bitstream.s
 void oracle_get_bitstream(const oracle_codec *c, uint32_t *out)
 {
 	memcpy(out, c->bitstream.data(), c->bitstream.size() * 4);
+}
+
+// Replace the encoder output (per-block meta + block words) with given data,
+// so that packetize can be checked on arbitrary block tables.
+void oracle_set_encoded(oracle_codec *c, const uint32_t *meta, const uint32_t *words, size_t nwords, uint32_t sequence)
+{
+	c->meta.assign(meta, meta + size_t(c->block_count_32x32) * 2);
+	c->bitstream.assign(words, words + nwords);
+	c->sequence = sequence & 7u;
 }
 
 // pyrowave_encoder.cpp:596-623

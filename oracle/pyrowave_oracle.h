@@ -79,7 +79,7 @@ int oracle_encode_pyramid(oracle_codec *codec, const float *pyramid, uint64_t ma
                           uint32_t sequence, float quant_scale);
 
 void oracle_get_code_words(const oracle_codec *codec, uint32_t *out);   /* block_count_8x8 */
-void oracle_get_block_stats(const oracle_codec *codec, uint32_t *out);  /* block_count_8x8 * 16 words (BlockStats) */
+void oracle_get_block_stats(const oracle_codec *codec, uint32_t *out);  /* block_count_8x8 * 17 words: num_planes + 16 x {fp16 error, cost bits} */
 void oracle_get_rd(const oracle_codec *codec, uint32_t *rate_cost, float *distortion, uint32_t *bucket); /* blocks32 * 16 each */
 void oracle_get_histogram(const oracle_codec *codec, uint32_t *scan2048, uint32_t *consumed);
 void oracle_get_quant(const oracle_codec *codec, int32_t *out);          /* block_count_32x32 */
@@ -89,6 +89,8 @@ void oracle_get_bitstream(const oracle_codec *codec, uint32_t *out);
 
 /* Packetization of the last encode (pyrowave_encoder.cpp:596-623,1048-1115).
  * packets: pairs of {offset, size}. */
+void oracle_set_encoded(oracle_codec *codec, const uint32_t *meta, const uint32_t *words, size_t nwords,
+                        uint32_t sequence);
 size_t oracle_compute_num_packets(const oracle_codec *codec, size_t packet_boundary);
 size_t oracle_packetize(const oracle_codec *codec, uint64_t *packets, size_t packet_boundary, uint8_t *out, size_t size);
 

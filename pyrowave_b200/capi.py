@@ -1,0 +1,408 @@
+"""ctypes binding of libpyrowave-shared.so.0 (include/pyrowave.h + include/pyrowave_cuda.h).
+
+This is the Python-side mirror of the reference's C API: the same entry points,
+argument meaning and result codes. Every call goes through the C ABI; there is
+no other compute path. Loading fails loudly when the library is missing.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+from ctypes import (POINTER, Structure, c_bool, c_float, c_int, c_int32, c_size_t, c_uint8, c_uint16, c_uint32,
+                    c_void_p)
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libpyrowave-shared.so.0")
+
+PYROWAVE_SUCCESS = 0
+PYROWAVE_TIMEOUT = 1
+PYROWAVE_ERROR_GENERIC = -1
+PYROWAVE_ERROR_INVALID_ARGUMENT = -2
+PYROWAVE_ERROR_OUT_OF_HOST_MEMORY = -3
+PYROWAVE_ERROR_OUT_OF_DEVICE_MEMORY = -4
+PYROWAVE_ERROR_NO_VULKAN = -5
+PYROWAVE_ERROR_NOT_IMPLEMENTED = -6
+
+CHROMA_420 = 0
+CHROMA_444 = 1
+
+FORMAT_NV12 = 0
+FORMAT_YUV420P = 1
+FORMAT_YUV444P = 2
+
+# Every exported symbol of include/pyrowave.h and include/pyrowave_cuda.h.
+API_SYMBOLS = [
+    "pyrowave_get_api_version", "pyrowave_create_default_device", "pyrowave_create_device_by_compat",
+    "pyrowave_create_device", "pyrowave_device_set_command_buffer", "pyrowave_device_report_performance_stats",
+    "pyrowave_device_get_vk_device_handles", "pyrowave_device_confirm_interop_support",
+    "pyrowave_device_set_queue_type", "pyrowave_device_destroy", "pyrowave_sync_object_create",
+    "pyrowave_sync_object_get_semaphore", "pyrowave_sync_object_export_handle", "pyrowave_sync_object_cpu_wait",
+    "pyrowave_sync_object_cpu_signal", "pyrowave_sync_object_destroy", "pyrowave_image_create",
+    "pyrowave_image_get_handle", "pyrowave_image_get_image_view", "pyrowave_image_destroy",
+    "pyrowave_encoder_create", "pyrowave_encoder_encode_gpu_synchronous", "pyrowave_encoder_encode_cpu_synchronous",
+    "pyrowave_encoder_compute_num_packets", "pyrowave_encoder_packetize", "pyrowave_encoder_destroy",
+    "pyrowave_decoder_device_prefers_fragment_path", "pyrowave_decoder_create", "pyrowave_decoder_clear",
+    "pyrowave_decoder_push_packet", "pyrowave_decoder_decode_is_ready", "pyrowave_decoder_decode_gpu_buffer",
+    "pyrowave_decoder_decode_cpu_buffer_synchronous", "pyrowave_decoder_destroy",
+    # CUDA extension
+    "pyrowave_cuda_encoder_set_precision", "pyrowave_cuda_decoder_set_precision", "pyrowave_cuda_encoder_get_layout",
+    "pyrowave_cuda_decoder_get_layout", "pyrowave_cuda_encoder_encode", "pyrowave_cuda_encoder_get_device_bitstream",
+    "pyrowave_cuda_encoder_get_size", "pyrowave_cuda_encoder_encode_pre_transformed",
+    "pyrowave_cuda_encoder_read_wavelet", "pyrowave_cuda_encoder_read_debug", "pyrowave_cuda_decoder_decode",
+    "pyrowave_cuda_decoder_decode_blocks", "pyrowave_cuda_decoder_read_wavelet", "pyrowave_cuda_decoder_decode_pyramid",
+]
+
+
+class PyrowaveError(RuntimeError):
+    def __init__(self, what: str, code: int):
+        super().__init__(f"{what} failed with pyrowave_result {code}")
+        self.code = code
+
+
+class EncoderCreateInfo(Structure):
+    _fields_ = [("device", c_void_p), ("width", c_int), ("height", c_int), ("chroma", c_int)]
+
+
+class DecoderCreateInfo(Structure):
+    _fields_ = [("device", c_void_p), ("width", c_int), ("height", c_int), ("chroma", c_int), ("fragment_path", c_bool)]
+
+
+class CpuBuffer(Structure):
+    _fields_ = [("data", c_void_p * 3), ("row_stride_in_bytes", c_size_t * 3), ("plane_size_in_bytes", c_size_t * 3),
+                ("width", c_int), ("height", c_int), ("format", c_int)]
+
+
+class RateControl(Structure):
+    _fields_ = [("maximum_bitstream_size", c_size_t)]
+
+
+class Packet(Structure):
+    _fields_ = [("offset", c_size_t), ("size", c_size_t)]
+
+
+class CudaPlanes(Structure):
+    _fields_ = [("data", c_void_p * 3), ("row_stride_in_bytes", c_size_t * 3)]
+
+
+class CudaLayout(Structure):
+    _fields_ = [("width", c_int), ("height", c_int), ("chroma444", c_int), ("aligned_width", c_int),
+                ("aligned_height", c_int), ("block_count_8x8", c_int), ("block_count_32x32", c_int),
+                ("pyramid_size", c_size_t), ("fp16_level_mask", c_uint32)]
+
+
+class CudaEncoderDebug(Structure):
+    _fields_ = [("code_words", c_void_p), ("rd_cost", c_void_p), ("rd_bucket", c_void_p), ("rd_dist", c_void_p),
+                ("histogram", c_void_p), ("consumed", c_void_p), ("quant", c_void_p), ("block_meta", c_void_p),
+                ("error_flags", c_void_p)]
+
+
+MESSAGE_CB = ctypes.CFUNCTYPE(None, c_void_p, ctypes.c_char_p)
+
+_lib = None
+
+
+def library_path() -> str:
+    return LIB_PATH
+
+
+def lib():
+    """Load the C-ABI library. Raises if it has not been built."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIB_PATH):
+        raise RuntimeError(
+            f"{LIB_PATH} is missing: build it with `python -m pyrowave_b200.build` (there is no fallback path)")
+    L = ctypes.CDLL(LIB_PATH)
+    L.pyrowave_get_api_version.argtypes = [POINTER(c_uint32)] * 3
+    L.pyrowave_get_api_version.restype = None
+    L.pyrowave_create_default_device.argtypes = [POINTER(c_void_p)]
+    L.pyrowave_device_destroy.argtypes = [c_void_p]
+    L.pyrowave_device_destroy.restype = None
+    L.pyrowave_device_report_performance_stats.argtypes = [c_void_p, MESSAGE_CB, c_void_p, c_bool]
+    L.pyrowave_device_report_performance_stats.restype = None
+    L.pyrowave_device_set_queue_type.argtypes = [c_void_p, c_int]
+    L.pyrowave_device_confirm_interop_support.argtypes = [c_void_p]
+    L.pyrowave_device_confirm_interop_support.restype = c_bool
+    L.pyrowave_decoder_device_prefers_fragment_path.argtypes = [c_void_p]
+    L.pyrowave_decoder_device_prefers_fragment_path.restype = c_bool
+    L.pyrowave_encoder_create.argtypes = [POINTER(EncoderCreateInfo), POINTER(c_void_p)]
+    L.pyrowave_encoder_destroy.argtypes = [c_void_p]
+    L.pyrowave_encoder_destroy.restype = None
+    L.pyrowave_encoder_encode_cpu_synchronous.argtypes = [c_void_p, POINTER(CpuBuffer), POINTER(RateControl)]
+    L.pyrowave_encoder_encode_gpu_synchronous.argtypes = [c_void_p, c_void_p, c_void_p, c_void_p, POINTER(RateControl)]
+    L.pyrowave_encoder_compute_num_packets.argtypes = [c_void_p, c_size_t, POINTER(c_size_t)]
+    L.pyrowave_encoder_packetize.argtypes = [c_void_p, POINTER(Packet), c_size_t, POINTER(c_size_t), c_void_p, c_size_t]
+    L.pyrowave_decoder_create.argtypes = [POINTER(DecoderCreateInfo), POINTER(c_void_p)]
+    L.pyrowave_decoder_destroy.argtypes = [c_void_p]
+    L.pyrowave_decoder_destroy.restype = None
+    L.pyrowave_decoder_clear.argtypes = [c_void_p]
+    L.pyrowave_decoder_clear.restype = None
+    L.pyrowave_decoder_push_packet.argtypes = [c_void_p, c_void_p, c_size_t]
+    L.pyrowave_decoder_decode_is_ready.argtypes = [c_void_p, c_bool]
+    L.pyrowave_decoder_decode_is_ready.restype = c_bool
+    L.pyrowave_decoder_decode_cpu_buffer_synchronous.argtypes = [c_void_p, POINTER(CpuBuffer)]
+    L.pyrowave_decoder_decode_gpu_buffer.argtypes = [c_void_p, c_void_p, c_void_p, c_void_p]
+    L.pyrowave_cuda_encoder_set_precision.argtypes = [c_void_p, c_uint32]
+    L.pyrowave_cuda_decoder_set_precision.argtypes = [c_void_p, c_uint32]
+    L.pyrowave_cuda_encoder_get_layout.argtypes = [c_void_p, POINTER(CudaLayout)]
+    L.pyrowave_cuda_decoder_get_layout.argtypes = [c_void_p, POINTER(CudaLayout)]
+    L.pyrowave_cuda_encoder_encode.argtypes = [c_void_p, POINTER(CudaPlanes), POINTER(RateControl), c_void_p]
+    L.pyrowave_cuda_encoder_get_device_bitstream.argtypes = [c_void_p, POINTER(c_void_p), POINTER(c_void_p),
+                                                             POINTER(c_size_t)]
+    L.pyrowave_cuda_encoder_get_size.argtypes = [c_void_p, POINTER(c_size_t)]
+    L.pyrowave_cuda_encoder_encode_pre_transformed.argtypes = [c_void_p, c_void_p, POINTER(RateControl), c_float,
+                                                               c_void_p]
+    L.pyrowave_cuda_encoder_read_wavelet.argtypes = [c_void_p, c_void_p, c_void_p]
+    L.pyrowave_cuda_encoder_read_debug.argtypes = [c_void_p, POINTER(CudaEncoderDebug)]
+    L.pyrowave_cuda_decoder_decode.argtypes = [c_void_p, POINTER(CudaPlanes), c_void_p]
+    L.pyrowave_cuda_decoder_decode_blocks.argtypes = [c_void_p, c_void_p, c_void_p, c_size_t, POINTER(CudaPlanes),
+                                                      c_void_p]
+    L.pyrowave_cuda_decoder_read_wavelet.argtypes = [c_void_p, c_void_p, c_void_p]
+    L.pyrowave_cuda_decoder_decode_pyramid.argtypes = [c_void_p, c_void_p, POINTER(CudaPlanes), c_void_p]
+    for name in API_SYMBOLS:
+        fn = getattr(L, name)
+        if fn.restype is ctypes.c_int and name not in ("pyrowave_get_api_version",):
+            fn.restype = c_int
+    _lib = L
+    return L
+
+
+def check(code: int, what: str):
+    if code != PYROWAVE_SUCCESS:
+        raise PyrowaveError(what, code)
+
+
+def api_version():
+    L = lib()
+    a, b, c = c_uint32(), c_uint32(), c_uint32()
+    L.pyrowave_get_api_version(ctypes.byref(a), ctypes.byref(b), ctypes.byref(c))
+    return a.value, b.value, c.value
+
+
+def _ptr(a):
+    return ctypes.c_void_p(a.ctypes.data)
+
+
+class Device:
+    """pyrowave_device: binds the current CUDA device."""
+
+    def __init__(self):
+        self.L = lib()
+        h = c_void_p()
+        check(self.L.pyrowave_create_default_device(ctypes.byref(h)), "pyrowave_create_default_device")
+        self.h = h
+
+    def close(self):
+        if self.h:
+            self.L.pyrowave_device_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        self.close()
+
+    def report_performance_stats(self, reset: bool = True):
+        out = []
+        cb = MESSAGE_CB(lambda ud, msg: out.append(msg.decode()))
+        self.L.pyrowave_device_report_performance_stats(self.h, cb, None, reset)
+        return out
+
+
+def _plane_shapes(width, height, chroma):
+    if chroma == CHROMA_444:
+        return [(height, width)] * 3
+    return [(height, width), (height // 2, width // 2), (height // 2, width // 2)]
+
+
+def cpu_buffer(planes, width, height, fmt):
+    buf = CpuBuffer()
+    keep = []
+    for i, p in enumerate(planes):
+        if p is None:
+            continue
+        a = np.ascontiguousarray(p) if not p.flags.c_contiguous else p
+        keep.append(a)
+        buf.data[i] = a.ctypes.data
+        buf.row_stride_in_bytes[i] = a.strides[0]
+        buf.plane_size_in_bytes[i] = a.strides[0] * a.shape[0]
+    buf.width = width
+    buf.height = height
+    buf.format = fmt
+    return buf, keep
+
+
+class Encoder:
+    """pyrowave_encoder (reference pyrowave.h:442-481)."""
+
+    def __init__(self, device: Device, width: int, height: int, chroma: int = CHROMA_420, fp16_level_mask: int = 0):
+        self.L = lib()
+        self.device = device
+        info = EncoderCreateInfo(device.h, width, height, chroma)
+        h = c_void_p()
+        check(self.L.pyrowave_encoder_create(ctypes.byref(info), ctypes.byref(h)), "pyrowave_encoder_create")
+        self.h = h
+        self.width, self.height, self.chroma = width, height, chroma
+        if fp16_level_mask:
+            check(self.L.pyrowave_cuda_encoder_set_precision(self.h, fp16_level_mask), "set_precision")
+
+    def close(self):
+        if self.h:
+            self.L.pyrowave_encoder_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        self.close()
+
+    def layout(self) -> CudaLayout:
+        lay = CudaLayout()
+        check(self.L.pyrowave_cuda_encoder_get_layout(self.h, ctypes.byref(lay)), "get_layout")
+        return lay
+
+    def encode_cpu(self, planes, budget: int, fmt: int | None = None) -> int:
+        if fmt is None:
+            fmt = FORMAT_YUV444P if self.chroma == CHROMA_444 else FORMAT_YUV420P
+        buf, keep = cpu_buffer(planes, self.width, self.height, fmt)
+        rc = RateControl(budget)
+        return self.L.pyrowave_encoder_encode_cpu_synchronous(self.h, ctypes.byref(buf), ctypes.byref(rc))
+
+    def compute_num_packets(self, boundary: int) -> int:
+        n = c_size_t()
+        check(self.L.pyrowave_encoder_compute_num_packets(self.h, boundary, ctypes.byref(n)), "compute_num_packets")
+        return n.value
+
+    def packetize(self, boundary: int, size: int):
+        n = self.compute_num_packets(boundary)
+        packets = (Packet * max(n, 1))()
+        out = np.zeros(size, np.uint8)
+        got = c_size_t()
+        check(self.L.pyrowave_encoder_packetize(self.h, packets, boundary, ctypes.byref(got), _ptr(out), size),
+              "packetize")
+        return out, [(packets[i].offset, packets[i].size) for i in range(got.value)]
+
+    # --- CUDA extension --------------------------------------------------------
+    def encode_device(self, plane_ptrs, strides, budget: int, stream: int = 0):
+        cp = CudaPlanes()
+        for i in range(3):
+            cp.data[i] = plane_ptrs[i]
+            cp.row_stride_in_bytes[i] = strides[i]
+        rc = RateControl(budget)
+        check(self.L.pyrowave_cuda_encoder_encode(self.h, ctypes.byref(cp), ctypes.byref(rc), c_void_p(stream)),
+              "pyrowave_cuda_encoder_encode")
+
+    def encode_pre_transformed(self, pyramid_dev_ptr: int, budget: int, quant_scale: float = -1.0, stream: int = 0):
+        rc = RateControl(budget)
+        check(self.L.pyrowave_cuda_encoder_encode_pre_transformed(self.h, c_void_p(pyramid_dev_ptr), ctypes.byref(rc),
+                                                                  quant_scale, c_void_p(stream)),
+              "encode_pre_transformed")
+
+    def read_wavelet(self, pyramid_dev_ptr: int, stream: int = 0):
+        check(self.L.pyrowave_cuda_encoder_read_wavelet(self.h, c_void_p(pyramid_dev_ptr), c_void_p(stream)),
+              "read_wavelet")
+
+    def device_bitstream(self):
+        s, m, cap = c_void_p(), c_void_p(), c_size_t()
+        check(self.L.pyrowave_cuda_encoder_get_device_bitstream(self.h, ctypes.byref(s), ctypes.byref(m),
+                                                                ctypes.byref(cap)), "get_device_bitstream")
+        return s.value, m.value, cap.value
+
+    def size(self) -> int:
+        n = c_size_t()
+        check(self.L.pyrowave_cuda_encoder_get_size(self.h, ctypes.byref(n)), "get_size")
+        return n.value
+
+    def debug(self):
+        lay = self.layout()
+        n8, n32 = lay.block_count_8x8, lay.block_count_32x32
+        d = {
+            "code_words": np.zeros(n8, np.uint32),
+            "rd_cost": np.zeros((n32, 16), np.uint16),
+            "rd_bucket": np.zeros((n32, 16), np.uint8),
+            "rd_dist": np.zeros((n32, 16), np.float32),
+            "histogram": np.zeros(2048, np.uint32),
+            "consumed": np.zeros(1, np.uint32),
+            "quant": np.zeros(n32, np.int32),
+            "block_meta": np.zeros((n32, 2), np.uint32),
+            "error_flags": np.zeros(1, np.uint32),
+        }
+        dbg = CudaEncoderDebug(*[d[k].ctypes.data for k in ("code_words", "rd_cost", "rd_bucket", "rd_dist", "histogram",
+                                                            "consumed", "quant", "block_meta", "error_flags")])
+        check(self.L.pyrowave_cuda_encoder_read_debug(self.h, ctypes.byref(dbg)), "read_debug")
+        return d
+
+
+class Decoder:
+    """pyrowave_decoder (reference pyrowave.h:485-539)."""
+
+    def __init__(self, device: Device, width: int, height: int, chroma: int = CHROMA_420, fp16_level_mask: int = 0):
+        self.L = lib()
+        self.device = device
+        info = DecoderCreateInfo(device.h, width, height, chroma, False)
+        h = c_void_p()
+        check(self.L.pyrowave_decoder_create(ctypes.byref(info), ctypes.byref(h)), "pyrowave_decoder_create")
+        self.h = h
+        self.width, self.height, self.chroma = width, height, chroma
+        if fp16_level_mask:
+            check(self.L.pyrowave_cuda_decoder_set_precision(self.h, fp16_level_mask), "set_precision")
+
+    def close(self):
+        if self.h:
+            self.L.pyrowave_decoder_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        self.close()
+
+    def layout(self) -> CudaLayout:
+        lay = CudaLayout()
+        check(self.L.pyrowave_cuda_decoder_get_layout(self.h, ctypes.byref(lay)), "get_layout")
+        return lay
+
+    def clear(self):
+        self.L.pyrowave_decoder_clear(self.h)
+
+    def push_packet(self, data) -> int:
+        buf = np.frombuffer(bytes(data), np.uint8) if not isinstance(data, np.ndarray) else np.ascontiguousarray(data)
+        if buf.size == 0:
+            return self.L.pyrowave_decoder_push_packet(self.h, None, 0)
+        return self.L.pyrowave_decoder_push_packet(self.h, _ptr(buf), buf.size)
+
+    def is_ready(self, allow_partial: bool = False) -> bool:
+        return bool(self.L.pyrowave_decoder_decode_is_ready(self.h, allow_partial))
+
+    def decode_cpu(self, planes=None, fmt: int | None = None):
+        if fmt is None:
+            fmt = FORMAT_YUV444P if self.chroma == CHROMA_444 else FORMAT_YUV420P
+        if planes is None:
+            planes = [np.zeros(s, np.uint8) for s in _plane_shapes(self.width, self.height, self.chroma)]
+        buf, keep = cpu_buffer(planes, self.width, self.height, fmt)
+        code = self.L.pyrowave_decoder_decode_cpu_buffer_synchronous(self.h, ctypes.byref(buf))
+        return code, planes
+
+    def decode_device(self, plane_ptrs, strides, stream: int = 0):
+        cp = CudaPlanes()
+        for i in range(3):
+            cp.data[i] = plane_ptrs[i]
+            cp.row_stride_in_bytes[i] = strides[i]
+        check(self.L.pyrowave_cuda_decoder_decode(self.h, ctypes.byref(cp), c_void_p(stream)), "cuda_decoder_decode")
+
+    def decode_blocks(self, meta_ptr: int, words_ptr: int, num_words: int, plane_ptrs, strides, stream: int = 0):
+        cp = CudaPlanes()
+        for i in range(3):
+            cp.data[i] = plane_ptrs[i]
+            cp.row_stride_in_bytes[i] = strides[i]
+        check(self.L.pyrowave_cuda_decoder_decode_blocks(self.h, c_void_p(meta_ptr), c_void_p(words_ptr), num_words,
+                                                         ctypes.byref(cp), c_void_p(stream)), "decode_blocks")
+
+    def decode_pyramid(self, pyramid_ptr: int, plane_ptrs, strides, stream: int = 0):
+        cp = CudaPlanes()
+        for i in range(3):
+            cp.data[i] = plane_ptrs[i]
+            cp.row_stride_in_bytes[i] = strides[i]
+        check(self.L.pyrowave_cuda_decoder_decode_pyramid(self.h, c_void_p(pyramid_ptr), ctypes.byref(cp),
+                                                          c_void_p(stream)), "decode_pyramid")
+
+    def read_wavelet(self, pyramid_dev_ptr: int, stream: int = 0):
+        check(self.L.pyrowave_cuda_decoder_read_wavelet(self.h, c_void_p(pyramid_dev_ptr), c_void_p(stream)),
+              "decoder_read_wavelet")

@@ -1,0 +1,365 @@
+// Decoder kernels for sm_100a: dequantiser and inverse CDF 9/7 level.
+//
+// Reference behaviour followed (file:line in the reference tree):
+//   dequantiser   shaders/wavelet_dequant.comp:100-391 (STORAGE_MODE 0), pyrowave_decoder.cpp:280-381
+//   inverse level shaders/idwt.comp:25-214, pyrowave_decoder.cpp:699-778
+//
+// Every payload read is bounds-checked against the payload size: the payload
+// comes from the network and a malformed packet must decode to garbage, never
+// to an out-of-bounds access. Reads past the end return zero.
+#include "pw_device.cuh"
+
+namespace pw
+{
+namespace
+{
+struct PayloadReader
+{
+	const uint32_t *words;
+	uint32_t nwords;
+	__device__ __forceinline__ uint32_t w32(uint32_t i) const { return i < nwords ? __ldg(words + i) : 0u; }
+	__device__ __forceinline__ uint32_t u8(uint32_t i) const { return (w32(i >> 2) >> (8u * (i & 3u))) & 0xffu; }
+	__device__ __forceinline__ uint32_t u16(uint32_t i) const { return (w32(i >> 1) >> (16u * (i & 1u))) & 0xffffu; }
+};
+
+__device__ __forceinline__ void store_coef(float *c32, __half *c16, bool fp16, int64_t idx, float v)
+{
+	if (fp16)
+		c16[idx] = __float2half_rn(v);
+	else
+		c32[idx] = v;
+}
+
+// One 32x32 block per 128-thread CTA; thread = one 4x2 sub-block (the
+// reference's mapping, wavelet_dequant.comp:222-238).
+__global__ void __launch_bounds__(128) dequant_kernel(Geometry g, DecodeInput in)
+{
+	__shared__ uint32_t s_plane_off[16];
+	__shared__ uint32_t s_sign_base;
+	__shared__ uint32_t s_sig[4];
+	const int blk = blockIdx.x;
+	int level, comp, band, bx32, by32;
+	unpack_job(in.jobs[blk], level, comp, band, bx32, by32);
+	const LevelDesc &L = g.level[level];
+	const BandDesc &B = g.band[comp][level][band];
+	const bool f16 = L.fp16 != 0;
+	const int t = threadIdx.x, lane = t & 31;
+	const int sub = t & 7, lx = (t >> 3) & 3, ly = t >> 5;
+	const int grp = ly * 4 + lx;
+	const int ox = bx32 * 32 + lx * 8 + sub_x(sub), oy = by32 * 32 + ly * 8 + sub_y(sub);
+
+	uint32_t off;
+	if (in.offsets)
+		off = in.offsets[blk];
+	else
+		off = in.block_meta[2 * blk + 1] ? in.block_meta[2 * blk] : 0xffffffffu;
+
+	if (off == 0xffffffffu)
+	{
+		// Missing block: all coefficients are zero (wavelet_dequant.comp:242-248).
+#pragma unroll
+		for (int i = 0; i < 8; i++)
+			store_coef(in.coef32, in.coef16, f16, B.offset + int64_t(oy + (i & 1)) * L.pitch + ox + (i >> 1), 0.0f);
+		return;
+	}
+
+	const PayloadReader rd{in.payload, in.payload_words};
+	const uint32_t ballot = rd.w32(off) & 0xffffu;
+	const uint32_t q_code = rd.w32(off + 1) & 0xffu;
+	const uint32_t n = uint32_t(__popc(ballot));
+
+	if (t < 16)
+	{
+		uint32_t cw = 0, qb = 0;
+		if ((ballot >> t) & 1u)
+		{
+			uint32_t local = uint32_t(__popc(ballot & ((1u << t) - 1u)));
+			cw = rd.u16(off * 2 + 4 + local);
+			qb = rd.u8(off * 4 + 8 + n * 2 + local) & 0xfu;
+		}
+		uint32_t lsbs = cw & 0x5555u, msbs = cw & 0xaaaau;
+		msbs |= msbs >> 1;
+		uint32_t cost = uint32_t(__popc(lsbs) + __popc(msbs)) + qb * 8u;
+		uint32_t inc = cost;
+#pragma unroll
+		for (int o = 1; o < 16; o *= 2)
+		{
+			uint32_t y = __shfl_up_sync(0x0000ffffu, inc, o);
+			if (t >= o)
+				inc += y;
+		}
+		const uint32_t base = off * 4 + 8 + 3 * n;
+		s_plane_off[t] = base + inc - cost;
+		if (t == 15)
+			s_sign_base = 8u * (base + inc);
+	}
+	__syncthreads();
+
+	float v[8];
+#pragma unroll
+	for (int i = 0; i < 8; i++)
+		v[i] = 0.0f;
+	if ((ballot >> grp) & 1u)
+	{
+		const uint32_t local = uint32_t(__popc(ballot & ((1u << grp) - 1u)));
+		const uint32_t cw = rd.u16(off * 2 + 4 + local);
+		const uint32_t cw2 = rd.u8(off * 4 + 8 + n * 2 + local);
+		const uint32_t qb = cw2 & 0xfu;
+		if (cw != 0)
+		{
+			const uint32_t mask = (1u << (2 * sub)) - 1u;
+			const uint32_t lsbs = cw & 0x5555u;
+			uint32_t msbs = cw & 0xaaaau;
+			msbs |= msbs >> 1;
+			uint32_t byte_offset = uint32_t(__popc(lsbs & mask) + __popc(msbs & mask)) + qb * uint32_t(sub) + s_plane_off[grp];
+			const int planes = int(qb + ((cw >> (2 * sub)) & 3u));
+			uint32_t dec[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+			for (int p = planes - 1; p >= 0; p--)
+			{
+				uint32_t pl = rd.u8(byte_offset++);
+#pragma unroll
+				for (int i = 0; i < 8; i++)
+					dec[i] |= ((pl >> i) & 1u) << p;
+			}
+#pragma unroll
+			for (int i = 0; i < 8; i++)
+			{
+				float f = float(dec[i]);
+				if (f != 0.0f)
+					f = __fadd_rn(f, 0.5f);
+				v[i] = f;
+			}
+		}
+		const float inv_scale = __fmul_rn(decode_quant(q_code), decode_quant_scale((cw2 >> 4) & 0xfu));
+#pragma unroll
+		for (int i = 0; i < 8; i++)
+			v[i] = __fmul_rn(v[i], inv_scale);
+	}
+
+	// Sign bits: position = number of significant coefficients before this one.
+	uint32_t nsig = 0;
+#pragma unroll
+	for (int i = 0; i < 8; i++)
+		nsig += v[i] != 0.0f ? 1u : 0u;
+	uint32_t inc = nsig;
+#pragma unroll
+	for (int o = 1; o < 32; o *= 2)
+	{
+		uint32_t y = __shfl_up_sync(0xffffffffu, inc, o);
+		if (lane >= o)
+			inc += y;
+	}
+	if (lane == 31)
+		s_sig[ly] = inc;
+	__syncthreads();
+	uint32_t bitpos = s_sign_base + inc - nsig;
+	for (int w = 0; w < ly; w++)
+		bitpos += s_sig[w];
+#pragma unroll
+	for (int i = 0; i < 8; i++)
+	{
+		if (v[i] != 0.0f)
+		{
+			uint32_t bit = (rd.w32(bitpos >> 5) >> (bitpos & 31u)) & 1u;
+			if (bit)
+				v[i] = -v[i];
+			bitpos++;
+		}
+	}
+#pragma unroll
+	for (int i = 0; i < 8; i++)
+		store_coef(in.coef32, in.coef16, f16, B.offset + int64_t(oy + (i & 1)) * L.pitch + ox + (i >> 1), v[i]);
+}
+
+constexpr int kIdwtThreads = 256;
+constexpr int kBandTile = 36; // 32 band samples + 2 on each side
+constexpr int kBandTilePitch = 37;
+
+struct IdwtShared
+{
+	int yl[kBandTile], yh[kBandTile], xl[kBandTile], xh[kBandTile];
+	float band[4][kBandTile][kBandTilePitch];
+	float v[2][64][kBandTilePitch]; // after vertical lifting: [horizontal low/high][output row][band column]
+};
+
+// One inverse level for a 64x64 output tile (32x32 band tile) of one component.
+__global__ void __launch_bounds__(kIdwtThreads) idwt_kernel(Geometry g, int level, DecodeInput in, PlaneOutput out)
+{
+	__shared__ IdwtShared sh;
+	const int comp = (level == 0 && !g.chroma444) ? 0 : int(blockIdx.y);
+	const LevelDesc &L = g.level[level];
+	const int tile = blockIdx.x;
+	const int tx = tile % L.tiles_x, ty = tile / L.tiles_x;
+	const int nx = L.width, ny = L.height;
+	const bool final_level = level == 0 || (level == 1 && comp != 0 && !g.chroma444);
+
+	for (int k = threadIdx.x; k < 4 * kBandTile; k += kIdwtThreads)
+	{
+		const int j = k % kBandTile, which = k / kBandTile;
+		const int px = tx * 32 - 2 + j, py = ty * 32 - 2 + j;
+		if (which == 0)
+			sh.xl[j] = inv_index_low(px, nx);
+		else if (which == 1)
+			sh.xh[j] = inv_index_high(px, nx);
+		else if (which == 2)
+			sh.yl[j] = inv_index_low(py, ny);
+		else
+			sh.yh[j] = inv_index_high(py, ny);
+	}
+	__syncthreads();
+
+	const bool f16 = L.fp16 != 0;
+	for (int k = threadIdx.x; k < 4 * kBandTile * kBandTile; k += kIdwtThreads)
+	{
+		const int b = k / (kBandTile * kBandTile);
+		const int r = k - b * kBandTile * kBandTile;
+		const int i = r / kBandTile, j = r - i * kBandTile;
+		const int yy = (b >> 1) ? sh.yh[i] : sh.yl[i];
+		const int xx = (b & 1) ? sh.xh[j] : sh.xl[j];
+		const BandDesc &B = g.band[comp][level][b];
+		sh.band[b][i][j] = load_coef(in.coef32, in.coef16, f16, B.offset + int64_t(yy) * L.pitch + xx);
+	}
+	__syncthreads();
+
+	// Vertical lifting: 36 band columns x {horizontal low: LL/LH, horizontal high: HL/HH} x 4 segments.
+	for (int item = threadIdx.x; item < kBandTile * 2 * 4; item += kIdwtThreads)
+	{
+		const int col = item % kBandTile;
+		const int which = (item / kBandTile) & 1;
+		const int seg = item / (2 * kBandTile);
+		const int b_low = which ? 1 : 0, b_high = which ? 3 : 2;
+		float e[24];
+#pragma unroll
+		for (int jj = 0; jj < 24; jj++)
+		{
+			const int q = seg * 16 + jj;
+			const int i = q >> 1;
+			e[jj] = (q & 1) ? __fmul_rn(sh.band[b_high][i][col], kInvK) : __fmul_rn(sh.band[b_low][i][col], kK);
+		}
+		lift_inverse(e);
+#pragma unroll
+		for (int jj = 4; jj < 20; jj++)
+			sh.v[which][seg * 16 + jj - 4][col] = e[jj];
+	}
+	__syncthreads();
+
+	// Horizontal lifting: 64 output rows x 4 segments of 16 outputs.
+	{
+		const int row = threadIdx.x & 63, seg = threadIdx.x >> 6;
+		float e[24];
+#pragma unroll
+		for (int jj = 0; jj < 24; jj++)
+		{
+			const int q = seg * 16 + jj;
+			const int i = q >> 1;
+			e[jj] = (q & 1) ? __fmul_rn(sh.v[1][row][i], kInvK) : __fmul_rn(sh.v[0][row][i], kK);
+		}
+		lift_inverse(e);
+		const int gy = ty * 64 + row;
+		const int gx0 = tx * 64 + seg * 16;
+		if (final_level)
+		{
+			const int pw = g.plane_width[comp], ph = g.plane_height[comp];
+			if (gy < ph)
+			{
+				uint8_t *dst = out.data[comp] + size_t(gy) * out.pitch[comp];
+#pragma unroll
+				for (int jj = 4; jj < 20; jj++)
+				{
+					const int gx = gx0 + jj - 4;
+					if (gx < pw)
+					{
+						float f = __fadd_rn(e[jj], 0.5f);
+						f = fminf(fmaxf(f, 0.0f), 1.0f);
+						dst[gx] = uint8_t(int(__fadd_rn(__fmul_rn(f, 255.0f), 0.5f)));
+					}
+				}
+			}
+		}
+		else
+		{
+			const LevelDesc &P = g.level[level - 1];
+			const BandDesc &B = g.band[comp][level - 1][0];
+			const bool pf16 = P.fp16 != 0;
+			if (gy < P.height)
+			{
+#pragma unroll
+				for (int jj = 4; jj < 20; jj++)
+				{
+					const int gx = gx0 + jj - 4;
+					if (gx < P.width)
+						store_coef(in.coef32, in.coef16, pf16, B.offset + int64_t(gy) * P.pitch + gx, e[jj]);
+				}
+			}
+		}
+	}
+}
+
+struct BandList
+{
+	int32_t count;
+	int32_t comp[48], level[48], band[48];
+	int64_t canon[48];
+};
+
+// Canonical pyramid (all transmitted bands, band-major, unpadded) <-> padded storage.
+__global__ void pyramid_io_kernel(Geometry g, BandList list, float *canonical, float *coef32, __half *coef16,
+                                  int to_canonical)
+{
+	const int k = blockIdx.y;
+	const int comp = list.comp[k], level = list.level[k], band = list.band[k];
+	const LevelDesc &L = g.level[level];
+	const BandDesc &B = g.band[comp][level][band];
+	const int64_t n = int64_t(L.width) * L.height;
+	for (int64_t i = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; i < n; i += int64_t(gridDim.x) * blockDim.x)
+	{
+		const int y = int(i / L.width), x = int(i - int64_t(y) * L.width);
+		const int64_t s = B.offset + int64_t(y) * L.pitch + x;
+		if (to_canonical)
+			canonical[list.canon[k] + i] = L.fp16 ? __half2float(coef16[s]) : coef32[s];
+		else
+		{
+			float v = canonical[list.canon[k] + i];
+			if (L.fp16)
+				coef16[s] = __float2half_rn(v);
+			else
+				coef32[s] = v;
+		}
+	}
+}
+} // namespace
+
+void launch_dequant(const Geometry &g, const DecodeInput &in, cudaStream_t stream)
+{
+	dequant_kernel<<<g.block_count_32x32, 128, 0, stream>>>(g, in);
+}
+
+void launch_idwt_level(const Geometry &g, int level, const DecodeInput &in, const PlaneOutput &out, cudaStream_t stream)
+{
+	const LevelDesc &L = g.level[level];
+	dim3 grid(L.tiles_x * L.tiles_y, (level == 0 && !g.chroma444) ? 1 : 3);
+	idwt_kernel<<<grid, kIdwtThreads, 0, stream>>>(g, level, in, out);
+}
+
+void launch_pyramid_io(const Geometry &g, float *canonical, float *coef32, __half *coef16, bool to_canonical,
+                       cudaStream_t stream)
+{
+	BandList list = {};
+	int64_t canon = 0;
+	for (int level = kLevels - 1; level >= 0; level--)
+		for (int comp = 0; comp < kComponents; comp++)
+			for (int band = 0; band < 4; band++)
+			{
+				if (!g.band[comp][level][band].present)
+					continue;
+				list.comp[list.count] = comp;
+				list.level[list.count] = level;
+				list.band[list.count] = band;
+				list.canon[list.count] = canon;
+				list.count++;
+				canon += int64_t(g.level[level].width) * g.level[level].height;
+			}
+	dim3 grid(64, list.count);
+	pyramid_io_kernel<<<grid, 256, 0, stream>>>(g, list, canonical, coef32, coef16, to_canonical ? 1 : 0);
+}
+} // namespace pw

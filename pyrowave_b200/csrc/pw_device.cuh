@@ -1,0 +1,228 @@
+// Device helpers shared by the sm_100a kernels.
+//
+// Floating point conventions (mirrored by the CPU oracle, which is how the two
+// are compared bit for bit): every FP32 operation is a separate IEEE
+// round-to-nearest operation (the library is built with --fmad=false and the
+// lifting steps are written with explicit _rn intrinsics), reductions use the
+// xor-butterfly order, FP16 rounding is round-to-nearest-even.
+#pragma once
+
+#include "pw_internal.h"
+
+namespace pw
+{
+// CDF 9/7 lifting constants (T.800 F.4.8.2, the values used in the reference's
+// dwt_common.h:37-42), as single-precision literals; 1/K is a float division.
+constexpr float kAlpha = -1.586134342059924f;
+constexpr float kBeta = -0.052980118572961f;
+constexpr float kGamma = 0.882911075530934f;
+constexpr float kDelta = 0.443506852043971f;
+constexpr float kK = 1.230174104914001f;
+constexpr float kInvK = 1.0f / 1.230174104914001f;
+
+// Vulkan MIRRORED_REPEAT addressing over [0, n).
+__device__ __forceinline__ int mirrored_repeat(int i, int n)
+{
+	int p = 2 * n;
+	int t = i % p;
+	if (t < 0)
+		t += p;
+	return t < n ? t : p - 1 - t;
+}
+
+// Forward transform input addressing (reference: dwt.comp:27-36 gather on a
+// mirrored-repeat sampler, with the clamp-to-edge fold for the region between
+// the real size and the aligned size). Resolved per sample; the coordinate
+// adjustment is decided on the even sample of each pair.
+__device__ __forceinline__ int fwd_index(int p, int resolution, int aligned)
+{
+	int x = p & ~1;
+	int idx;
+	if (x < 0)
+		idx = p - 1;
+	else if (x + 1 >= 2 * aligned - resolution)
+		idx = p + 1 + 2 * (resolution - aligned);
+	else
+		idx = min(p, resolution);
+	return mirrored_repeat(idx, resolution);
+}
+
+// Inverse transform band addressing (reference: idwt.comp:25-32): low-pass
+// (even) and high-pass (odd) samples of a band of n samples.
+__device__ __forceinline__ int inv_index_low(int p, int n) { return mirrored_repeat(p < 0 ? p - 1 : p, n); }
+__device__ __forceinline__ int inv_index_high(int p, int n)
+{
+	int q = p & ~1;
+	return mirrored_repeat(q + 1 >= n ? p + 1 : p, n);
+}
+
+__device__ __forceinline__ float lift_add(float v, float c, float a, float b)
+{
+	float t = __fadd_rn(a, b);
+	t = __fmul_rn(c, t);
+	return __fadd_rn(v, t);
+}
+__device__ __forceinline__ float lift_sub(float v, float c, float a, float b)
+{
+	float t = __fadd_rn(a, b);
+	t = __fmul_rn(c, t);
+	return __fsub_rn(v, t);
+}
+
+// Forward lifting over a register window e[0..N); window position j has the
+// same parity as the signal position it holds. Outputs e[4 .. N-4) are exact.
+template <int N> __device__ __forceinline__ void lift_forward(float (&e)[N])
+{
+#pragma unroll
+	for (int j = 1; j + 1 < N; j += 2)
+		e[j] = lift_add(e[j], kAlpha, e[j - 1], e[j + 1]);
+#pragma unroll
+	for (int j = 2; j + 1 < N; j += 2)
+		e[j] = lift_add(e[j], kBeta, e[j - 1], e[j + 1]);
+#pragma unroll
+	for (int j = 3; j + 1 < N; j += 2)
+		e[j] = lift_add(e[j], kGamma, e[j - 1], e[j + 1]);
+#pragma unroll
+	for (int j = 4; j + 1 < N; j += 2)
+		e[j] = lift_add(e[j], kDelta, e[j - 1], e[j + 1]);
+}
+
+template <int N> __device__ __forceinline__ void lift_inverse(float (&e)[N])
+{
+#pragma unroll
+	for (int j = 2; j + 1 < N; j += 2)
+		e[j] = lift_sub(e[j], kDelta, e[j - 1], e[j + 1]);
+#pragma unroll
+	for (int j = 3; j + 1 < N; j += 2)
+		e[j] = lift_sub(e[j], kGamma, e[j - 1], e[j + 1]);
+#pragma unroll
+	for (int j = 4; j + 1 < N; j += 2)
+		e[j] = lift_sub(e[j], kBeta, e[j - 1], e[j + 1]);
+#pragma unroll
+	for (int j = 5; j + 1 < N; j += 2)
+		e[j] = lift_sub(e[j], kAlpha, e[j - 1], e[j + 1]);
+}
+
+__device__ __forceinline__ float round_to_half(float v) { return __half2float(__float2half_rn(v)); }
+
+__device__ __forceinline__ float load_coef(const float *c32, const __half *c16, bool fp16, int64_t idx)
+{
+	return fp16 ? __half2float(c16[idx]) : c32[idx];
+}
+
+// ---------------------------------------------------------------------------
+// Quantiser helpers (reference: dwt_quant_scale.h, wavelet_quant.comp,
+// block_packing.comp, pyrowave_common.hpp:124-145).
+__device__ __forceinline__ float decode_quant_scale(uint32_t code)
+{
+	return __fadd_rn(__fdiv_rn(float(code), 8.0f), 0.25f);
+}
+
+// Custom FP quant code of the 32x32 header: (8+m) * 2^(20+e) / 2^23 with
+// e = 4 - (code >> 3), written as an exact ldexp.
+__device__ __forceinline__ float decode_quant(uint32_t code)
+{
+	int e = kMaxScaleExp - int(code >> 3);
+	int m = int(code & 7u);
+	return ldexpf(float(8 + m), e - 3);
+}
+
+__device__ __forceinline__ int find_msb(uint32_t v) { return v ? 31 - __clz(v) : -1; }
+
+// 8-bit quant scale per 8x8 block (wavelet_quant.comp:95-111).
+__device__ __forceinline__ void compute_quant_scale(float max_wave, uint32_t &code, float &scale)
+{
+	if (max_wave < 1.0f)
+	{
+		code = 6u;
+		scale = 1.0f;
+	}
+	else
+	{
+		int e;
+		frexpf(__fsub_rn(max_wave, 0.25f), &e);
+		float target_max = __fsub_rn(float(1 << e), 0.25f);
+		float inv_scale = __fdiv_rn(max_wave, target_max);
+		code = uint32_t(ceilf(__fmul_rn(__fsub_rn(inv_scale, 0.25f), 8.0f)));
+		scale = __fdiv_rn(1.0f, decode_quant_scale(code));
+	}
+}
+
+// Required plane bytes of an 8x8 block (block_packing.comp:97-105).
+__device__ __forceinline__ uint32_t required_8x8_bytes(uint32_t cw)
+{
+	uint32_t q_bits = (cw >> kQPlanesOffset) & 0xfu;
+	uint32_t lsbs = cw & 0x5555u;
+	uint32_t msbs = cw & 0xaaaau;
+	msbs |= msbs >> 1;
+	return uint32_t(__popc(lsbs) + __popc(msbs)) + q_bits * 8u;
+}
+
+// Drop `quant` planes from a code word (block_packing.comp:107-142): first the
+// Q planes, then max(code - rest, 0) per 4x2 sub-block.
+__device__ __forceinline__ uint32_t quantize_code_word(uint32_t cw, int quant)
+{
+	if (quant != 0 && cw != 0)
+	{
+		int q_bits = int((cw >> kQPlanesOffset) & 0xfu);
+		int sub = min(q_bits, quant);
+		q_bits -= sub;
+		quant -= sub;
+		if (quant != 0)
+		{
+			quant = min(quant, 3);
+			uint32_t p0 = cw & 0x5555u;
+			uint32_t p1 = (cw & 0xaaaau) >> 1;
+			uint32_t p2 = p0 & p1;
+			for (int i = 0; i < quant; i++)
+			{
+				p0 = p1;
+				p1 = p2;
+				p2 = 0;
+			}
+			p0 &= ~p1;
+			cw = (cw & ~0xffffu) | ((p0 | (p1 << 1)) & 0xffffu);
+		}
+		cw = (cw & ~(0xfu << kQPlanesOffset)) | (uint32_t(q_bits) << kQPlanesOffset);
+	}
+	return cw;
+}
+
+// block_packing.comp:161-167
+__device__ __forceinline__ uint32_t modify_quant_code(uint32_t code, int quant)
+{
+	int e = int((code >> 3) & 31u);
+	e = max(e - quant, 0);
+	return (code & ~(31u << 3)) | (uint32_t(e) << 3);
+}
+
+// Rate-control bucket of a quant step (analyze_rate_control.comp:73-83):
+// uint(max(60 + 2*log2(r) + 0.5, 0)), evaluated with the exact value of log2:
+// for r = m * 2^e, m in [1,2), the result is 60 + 2e + [m >= 2^0.25] + [m >= 2^0.75].
+// 0x1837f1 / 0x5744fd are the mantissas of the smallest floats >= 2^0.25 / 2^0.75.
+__device__ __forceinline__ uint32_t bucket_index(float d, float cost, float d_base, float cost_base)
+{
+	if (cost == cost_base)
+		return 0;
+	float num = fmaxf(__fsub_rn(d, d_base), 0.0f);
+	float den = __fsub_rn(cost_base, cost);
+	float r = __fdiv_rn(num, den);
+	if (!(r > 0.0f))
+		return 0;
+	uint32_t bits = __float_as_uint(r);
+	uint32_t ef = bits >> 23;
+	if (ef == 0)
+		return 0;
+	if (ef >= 255)
+		return 255;
+	int e = int(ef) - 127;
+	uint32_t mant = bits & 0x7fffffu;
+	int idx = 60 + 2 * e + (mant >= 0x1837f1u ? 1 : 0) + (mant >= 0x5744fdu ? 1 : 0);
+	return idx < 0 ? 0u : uint32_t(idx);
+}
+
+// Origin of 4x2 sub-block s inside an 8x8 block (the reference's
+// unswizzle8x8(s << 3)) and the pixel order inside it (bitstream.md:350-368).
+__device__ __forceinline__ int sub_x(int s) { return (s >> 2) * 4; }
+__device__ __forceinline__ int sub_y(int s) { return (s & 3) * 2; }
+} // namespace pw

@@ -1,0 +1,801 @@
+// Encoder kernels for sm_100a: fused forward CDF 9/7 level + quantiser + RD
+// analysis, the single-CTA rate-control resolve, and block packing.
+//
+// Reference behaviour followed (file:line in the reference tree):
+//   forward level      shaders/dwt.comp:38-234 (tile + apron, H then V lifting)
+//   quantiser / stats  shaders/wavelet_quant.comp:72-316
+//   RD analysis        shaders/analyze_rate_control.comp:73-220
+//   finalize/resolve   shaders/analyze_rate_control_finalize.comp:14-38,
+//                      shaders/resolve_rate_control.comp:38-81, pyrowave_encoder.cpp:283-338
+//   block packing      shaders/block_packing.comp:97-379
+//   packetize layout   pyrowave_encoder.cpp:1048-1115
+#include "pw_device.cuh"
+
+namespace pw
+{
+namespace
+{
+constexpr int kDwtThreads = 256;
+constexpr int kTileIn = 72;  // 64 input samples + 4-sample apron on each side
+constexpr int kInPitch = 73; // odd pitch: conflict-free column walks
+constexpr int kHPitch = 65;
+constexpr int kBandPitch = 33;
+
+// Reduction scratch of one 128-thread quantiser group (one 32x32 block).
+struct QuantGroupShared
+{
+	float dist[4][16];
+	uint32_t cost[4][16];
+};
+
+// ---------------------------------------------------------------------------
+// Quantiser + RD analysis of one 32x32 block held in shared memory.
+//
+// Thread t of the 128-thread group owns one 4x2 sub-block: sub = t & 7,
+// 8x8 column lx = (t >> 3) & 3, 8x8 row ly = t >> 5 (one warp per 8x8 row),
+// exactly the reference's mapping (wavelet_quant.comp:294-306).
+//
+// Every thread of the CTA must call this the same number of times (it contains
+// __syncthreads); `active` is false for groups without a block this round.
+__device__ void quant_analyze_block(const float *tile, int tile_pitch, bool active, int t, QuantGroupShared &sh,
+                                    const Geometry &g, int level, int comp, int band, int bx32, int by32,
+                                    const EncodeBuffers &buf)
+{
+	const LevelDesc &L = g.level[level];
+	const BandDesc &B = g.band[comp][level][band];
+	const int sub = t & 7, lx = (t >> 3) & 3, ly = t >> 5;
+	const int lane = threadIdx.x & 31;
+	const int x8 = bx32 * 4 + lx, y8 = by32 * 4 + ly;
+	const bool in_range = active && x8 < L.blocks8_x && y8 < L.blocks8_y;
+	const float qres = active ? B.quant_resolution : 1.0f;
+
+	float v[8];
+	const int ox = lx * 8 + sub_x(sub), oy = ly * 8 + sub_y(sub);
+#pragma unroll
+	for (int i = 0; i < 8; i++)
+	{
+		float c = in_range ? tile[(oy + (i & 1)) * tile_pitch + ox + (i >> 1)] : 0.0f;
+		v[i] = __fmul_rn(c, qres);
+	}
+
+	// 8x8 maximum and quant scale (wavelet_quant.comp:174-181).
+	float max_sub = 0.0f;
+#pragma unroll
+	for (int i = 0; i < 8; i++)
+		max_sub = fmaxf(max_sub, fabsf(v[i]));
+	float max_wave = max_sub;
+	max_wave = fmaxf(max_wave, __shfl_xor_sync(0xffffffffu, max_wave, 1));
+	max_wave = fmaxf(max_wave, __shfl_xor_sync(0xffffffffu, max_wave, 2));
+	max_wave = fmaxf(max_wave, __shfl_xor_sync(0xffffffffu, max_wave, 4));
+
+	uint32_t qcode;
+	float qs;
+	compute_quant_scale(max_wave, qcode, qs);
+#pragma unroll
+	for (int i = 0; i < 8; i++)
+		v[i] = fminf(fmaxf(__fmul_rn(v[i], qs), -kMaxScaledMagnitude), kMaxScaledMagnitude);
+	max_sub = fminf(__fmul_rn(max_sub, qs), kMaxScaledMagnitude);
+	max_wave = fminf(__fmul_rn(max_wave, qs), kMaxScaledMagnitude);
+
+	const float overall = __fmul_rn(qres, qs);
+	const float inv_quant = __fdiv_rn(1.0f, overall);
+	const float iqs = __fmul_rn(inv_quant, inv_quant);
+	const float rdo = active ? B.rdo_scale : 0.0f;
+	const int block4x2_max = int(max_sub);
+	const int max_abs = int(max_wave);
+	const int msb = find_msb(uint32_t(max_abs));
+
+	// Stats at q = 0 (wavelet_quant.comp:139-165,205-238).
+	int qp0 = 0, shifted0 = block4x2_max, cost_early0 = block4x2_max > 0 ? 1 : 0;
+	if (msb >= 3)
+	{
+		qp0 = msb - 2;
+		cost_early0 = qp0 + 1;
+		shifted0 >>= qp0;
+	}
+	cost_early0 += find_msb(uint32_t(shifted0)) + 1;
+	int nsig0 = 0;
+#pragma unroll
+	for (int i = 0; i < 8; i++)
+		nsig0 += (fabsf(v[i]) >= 1.0f) ? 1 : 0;
+	int csum0 = max(cost_early0 - 1, 0) * 8 + nsig0;
+	csum0 += __shfl_xor_sync(0xffffffffu, csum0, 1);
+	csum0 += __shfl_xor_sync(0xffffffffu, csum0, 2);
+	csum0 += __shfl_xor_sync(0xffffffffu, csum0, 4);
+
+	uint32_t plane_code = uint32_t(find_msb(uint32_t(shifted0)) + 1);
+	uint32_t cw = plane_code << (2 * sub);
+	cw |= __shfl_xor_sync(0xffffffffu, cw, 1);
+	cw |= __shfl_xor_sync(0xffffffffu, cw, 2);
+	cw |= __shfl_xor_sync(0xffffffffu, cw, 4);
+	cw |= (uint32_t(qp0) << kQPlanesOffset) | ((qcode & 0xfu) << kQuantScaleOffset);
+	if (max_abs == 0)
+		cw = 0;
+
+	// Distortion of dropping every plane (wavelet_quant.comp:253-256).
+	float drop;
+	{
+		float s0 = __fmul_rn(v[0], v[0]);
+		s0 = __fadd_rn(s0, __fmul_rn(v[1], v[1]));
+		s0 = __fadd_rn(s0, __fmul_rn(v[2], v[2]));
+		s0 = __fadd_rn(s0, __fmul_rn(v[3], v[3]));
+		float s1 = __fmul_rn(v[4], v[4]);
+		s1 = __fadd_rn(s1, __fmul_rn(v[5], v[5]));
+		s1 = __fadd_rn(s1, __fmul_rn(v[6], v[6]));
+		s1 = __fadd_rn(s1, __fmul_rn(v[7], v[7]));
+		drop = __fmul_rn(__fadd_rn(s0, s1), iqs);
+		drop = __fadd_rn(drop, __shfl_xor_sync(0xffffffffu, drop, 1));
+		drop = __fadd_rn(drop, __shfl_xor_sync(0xffffffffu, drop, 2));
+		drop = __fadd_rn(drop, __shfl_xor_sync(0xffffffffu, drop, 4));
+		drop = __half2float(__float2half_rn(fminf(60000.0f, drop)));
+	}
+
+	// Lane `sub` keeps the 8x8's entries for quant levels i = sub and sub + 8:
+	// errors[min(i, num_planes)] of the reference's BlockStats.
+	float d_lo = 0.0f, d_hi = drop;
+	uint32_t c_lo = (sub == 0) ? uint32_t(csum0) : 0u, c_hi = 0u;
+	if (sub != 0 && sub > msb)
+		d_lo = drop;
+
+	const int warp_msb = __reduce_max_sync(0xffffffffu, max(msb, 0));
+	for (int q = 1; q <= warp_msb; q++)
+	{
+		// compute_square_error + compute_quant_stats at q (wavelet_quant.comp:113-165).
+		int nsig = 0;
+		float e0 = 0.0f, e1 = 0.0f;
+#pragma unroll
+		for (int i = 0; i < 8; i++)
+		{
+			float a = fabsf(v[i]);
+			float iv = floorf(ldexpf(a, -q));
+			nsig += iv != 0.0f ? 1 : 0;
+			if (iv != 0.0f)
+				iv = __fadd_rn(iv, 0.5f);
+			iv = truncf(ldexpf(iv, q));
+			float err = __fsub_rn(a, iv);
+			float sq = __fmul_rn(err, err);
+			if (i < 4)
+				e0 = (i == 0) ? sq : __fadd_rn(e0, sq);
+			else
+				e1 = (i == 4) ? sq : __fadd_rn(e1, sq);
+		}
+		float se = __fmul_rn(__fmul_rn(__fadd_rn(e0, e1), rdo), iqs);
+		se = __fadd_rn(se, __shfl_xor_sync(0xffffffffu, se, 1));
+		se = __fadd_rn(se, __shfl_xor_sync(0xffffffffu, se, 2));
+		se = __fadd_rn(se, __shfl_xor_sync(0xffffffffu, se, 4));
+
+		int m = msb - q;
+		int shifted = block4x2_max >> q;
+		int ce = shifted > 0 ? 1 : 0;
+		if (m >= 3)
+		{
+			int qp = m - 2;
+			ce = qp + 1;
+			shifted >>= qp;
+		}
+		ce += find_msb(uint32_t(shifted)) + 1;
+		int csum = max(ce - 1, 0) * 8 + nsig;
+		csum += __shfl_xor_sync(0xffffffffu, csum, 1);
+		csum += __shfl_xor_sync(0xffffffffu, csum, 2);
+		csum += __shfl_xor_sync(0xffffffffu, csum, 4);
+
+		if (q <= msb)
+		{
+			float d = __half2float(__float2half_rn(fminf(se, 60000.0f)));
+			if (q == sub)
+			{
+				d_lo = d;
+				c_lo = uint32_t(csum);
+			}
+			if (q == sub + 8)
+			{
+				d_hi = d;
+				c_hi = uint32_t(csum);
+			}
+		}
+	}
+	if (max_abs == 0)
+	{
+		d_lo = d_hi = 0.0f;
+		c_lo = c_hi = 0u;
+	}
+
+	// Per-32x32 sums (analyze_rate_control.comp:169-215): +24 bits per coded
+	// 8x8, butterfly over the 16 8x8 blocks in index order lx + 4 * ly.
+	if (c_lo != 0)
+		c_lo += 24;
+	if (c_hi != 0)
+		c_hi += 24;
+	d_lo = __fadd_rn(d_lo, __shfl_xor_sync(0xffffffffu, d_lo, 8));
+	d_lo = __fadd_rn(d_lo, __shfl_xor_sync(0xffffffffu, d_lo, 16));
+	d_hi = __fadd_rn(d_hi, __shfl_xor_sync(0xffffffffu, d_hi, 8));
+	d_hi = __fadd_rn(d_hi, __shfl_xor_sync(0xffffffffu, d_hi, 16));
+	c_lo += __shfl_xor_sync(0xffffffffu, c_lo, 8);
+	c_lo += __shfl_xor_sync(0xffffffffu, c_lo, 16);
+	c_hi += __shfl_xor_sync(0xffffffffu, c_hi, 8);
+	c_hi += __shfl_xor_sync(0xffffffffu, c_hi, 16);
+	if (lane < 8)
+	{
+		sh.dist[ly][sub] = d_lo;
+		sh.dist[ly][sub + 8] = d_hi;
+		sh.cost[ly][sub] = c_lo;
+		sh.cost[ly][sub + 8] = c_hi;
+	}
+	if (in_range && sub == 0)
+		buf.code_words[B.block8_offset + y8 * B.block8_stride + x8] = cw;
+	__syncthreads();
+
+	if (active && t < 16)
+	{
+		const int i = t;
+		float d = __fadd_rn(__fadd_rn(sh.dist[0][i], sh.dist[1][i]), __fadd_rn(sh.dist[2][i], sh.dist[3][i]));
+		uint32_t c = sh.cost[0][i] + sh.cost[1][i] + sh.cost[2][i] + sh.cost[3][i];
+		if (c != 0)
+			c += 64;
+		uint32_t rate = (c + 31) >> 5;
+		const unsigned m16 = 0x0000ffffu;
+		float d0 = __shfl_sync(m16, d, 0);
+		uint32_t r0 = __shfl_sync(m16, rate, 0);
+		uint32_t bk = bucket_index(d, float(rate), d0, float(r0));
+		if (i == 0)
+			bk = 0;
+		// inclusive_max_clustered16 (analyze_rate_control.comp:85-99)
+		bk = min(bk, uint32_t(128 - 16 + i));
+#pragma unroll
+		for (int off = 1; off < 16; off *= 2)
+		{
+			uint32_t up = __shfl_up_sync(m16, bk, off) + uint32_t(off);
+			if (i >= off)
+				bk = max(bk, up);
+		}
+		uint32_t rate_prev = __shfl_up_sync(m16, rate, 1);
+		const uint32_t block_index = uint32_t(B.block32_offset + by32 * B.block32_stride + bx32);
+		buf.rd_cost[block_index * 16 + i] = uint16_t(rate);
+		buf.rd_bucket[block_index * 16 + i] = uint8_t(bk);
+		buf.rd_dist[block_index * 16 + i] = d;
+		if (i == 0)
+			atomicAdd(&buf.rc->consumed, rate);
+		else
+		{
+			uint32_t saving = rate_prev - rate;
+			if (saving != 0)
+			{
+				uint32_t subdivision = block_index >> g.subdivision_shift;
+				atomicAdd(&buf.rc->histogram[bk * kSubdivisions + subdivision], saving);
+			}
+		}
+	}
+	__syncthreads();
+}
+
+struct DwtShared
+{
+	int xidx[kTileIn];
+	int yidx[kTileIn];
+	float in[kTileIn][kInPitch]; // input tile, later the four 32x32 band tiles
+	float h[kTileIn][kHPitch];   // after horizontal lifting: low in 0..31, high in 32..63
+	QuantGroupShared q[2];
+};
+
+// One forward level for one 32x32 band tile of one component (64x64 input
+// samples). grid.x = tile, grid.y = component index among those at this level.
+__global__ void __launch_bounds__(kDwtThreads) dwt_forward_kernel(Geometry g, int level, PlaneInput in,
+                                                                   EncodeBuffers buf, int fused)
+{
+	__shared__ DwtShared sh;
+	const int comp = (level == 0 && !g.chroma444) ? 0 : int(blockIdx.y);
+	const LevelDesc &L = g.level[level];
+	const int tile = blockIdx.x;
+	const int tx = tile % L.tiles_x, ty = tile / L.tiles_x;
+	const bool from_plane = level == 0 || (level == 1 && comp != 0 && !g.chroma444);
+
+	int res_w, res_h, al_w, al_h;
+	if (from_plane)
+	{
+		res_w = g.plane_width[comp];
+		res_h = g.plane_height[comp];
+		al_w = level == 0 ? g.aligned_width : g.aligned_width >> 1;
+		al_h = level == 0 ? g.aligned_height : g.aligned_height >> 1;
+	}
+	else
+	{
+		res_w = al_w = g.level[level - 1].width;
+		res_h = al_h = g.level[level - 1].height;
+	}
+
+	for (int k = threadIdx.x; k < 2 * kTileIn; k += kDwtThreads)
+	{
+		if (k < kTileIn)
+			sh.xidx[k] = fwd_index(tx * 64 - 4 + k, res_w, al_w);
+		else
+			sh.yidx[k - kTileIn] = fwd_index(ty * 64 - 4 + (k - kTileIn), res_h, al_h);
+	}
+	__syncthreads();
+
+	if (from_plane)
+	{
+		const uint8_t *p = in.data[comp];
+		const int pitch = in.pitch[comp], xs = in.xstride[comp];
+		for (int k = threadIdx.x; k < kTileIn * kTileIn; k += kDwtThreads)
+		{
+			int i = k / kTileIn, j = k - i * kTileIn;
+			float f = __fdiv_rn(float(p[size_t(sh.yidx[i]) * pitch + size_t(sh.xidx[j]) * xs]), 255.0f);
+			sh.in[i][j] = __fsub_rn(f, 0.5f);
+		}
+	}
+	else
+	{
+		const LevelDesc &P = g.level[level - 1];
+		const BandDesc &B = g.band[comp][level - 1][0];
+		const bool f16 = P.fp16 != 0;
+		for (int k = threadIdx.x; k < kTileIn * kTileIn; k += kDwtThreads)
+		{
+			int i = k / kTileIn, j = k - i * kTileIn;
+			int64_t idx = B.offset + int64_t(sh.yidx[i]) * P.pitch + sh.xidx[j];
+			sh.in[i][j] = load_coef(buf.coef32, buf.coef16, f16, idx);
+		}
+	}
+	__syncthreads();
+
+	// Horizontal lifting: 72 rows x 4 segments of 8 output pairs.
+	for (int item = threadIdx.x; item < kTileIn * 4; item += kDwtThreads)
+	{
+		const int row = item % kTileIn, seg = item / kTileIn;
+		float e[24];
+#pragma unroll
+		for (int j = 0; j < 24; j++)
+			e[j] = sh.in[row][seg * 16 + j];
+		lift_forward(e);
+#pragma unroll
+		for (int k = 0; k < 8; k++)
+		{
+			sh.h[row][seg * 8 + k] = __fmul_rn(e[4 + 2 * k], kInvK);
+			sh.h[row][32 + seg * 8 + k] = __fmul_rn(e[5 + 2 * k], kK);
+		}
+	}
+	__syncthreads();
+
+	// Vertical lifting: 64 columns x 4 segments. Columns 0..31 hold the
+	// horizontal low band (-> LL, LH), 32..63 the high band (-> HL, HH).
+	float(*bands)[32][kBandPitch] = reinterpret_cast<float(*)[32][kBandPitch]>(&sh.in[0][0]);
+	{
+		const int col = threadIdx.x & 63, seg = threadIdx.x >> 6;
+		float e[24];
+#pragma unroll
+		for (int j = 0; j < 24; j++)
+			e[j] = sh.h[seg * 16 + j][col];
+		lift_forward(e);
+		const int c = col & 31;
+		const int b_low = col < 32 ? 0 : 1, b_high = col < 32 ? 2 : 3;
+		const int gx = tx * 32 + c;
+#pragma unroll
+		for (int k = 0; k < 8; k++)
+		{
+			const int r = seg * 8 + k;
+			const int gy = ty * 32 + r;
+			float lo = __fmul_rn(e[4 + 2 * k], kInvK);
+			float hi = __fmul_rn(e[5 + 2 * k], kK);
+			if (gx >= L.width || gy >= L.height)
+				lo = hi = 0.0f;
+			else if (L.fp16)
+			{
+				lo = round_to_half(lo);
+				hi = round_to_half(hi);
+			}
+			bands[b_low][r][c] = lo;
+			bands[b_high][r][c] = hi;
+		}
+	}
+	__syncthreads();
+
+	// Store all four bands (LL feeds the next level).
+	{
+		const int r = threadIdx.x >> 3, c4 = (threadIdx.x & 7) * 4;
+		for (int b = 0; b < 4; b++)
+		{
+			const BandDesc &B = g.band[comp][level][b];
+			const int64_t idx = B.offset + int64_t(ty * 32 + r) * L.pitch + tx * 32 + c4;
+			if (L.fp16)
+			{
+				__half2 h0 = __floats2half2_rn(bands[b][r][c4 + 0], bands[b][r][c4 + 1]);
+				__half2 h1 = __floats2half2_rn(bands[b][r][c4 + 2], bands[b][r][c4 + 3]);
+				uint2 u;
+				u.x = *reinterpret_cast<uint32_t *>(&h0);
+				u.y = *reinterpret_cast<uint32_t *>(&h1);
+				*reinterpret_cast<uint2 *>(buf.coef16 + idx) = u;
+			}
+			else
+			{
+				float4 f = make_float4(bands[b][r][c4 + 0], bands[b][r][c4 + 1], bands[b][r][c4 + 2], bands[b][r][c4 + 3]);
+				*reinterpret_cast<float4 *>(buf.coef32 + idx) = f;
+			}
+		}
+	}
+
+	if (!fused)
+		return;
+
+	// Quantise the transmitted bands of this tile: HL, LH, HH (+ LL at the last level).
+	const int first_band = level == kLevels - 1 ? 0 : 1;
+	const int nb = 4 - first_band;
+	const int grp = threadIdx.x >> 7, t = threadIdx.x & 127;
+	for (int round = 0; round < 2; round++)
+	{
+		const int bi = round * 2 + grp;
+		const bool active = bi < nb;
+		const int band = active ? first_band + bi : first_band;
+		quant_analyze_block(&bands[band][0][0], kBandPitch, active, t, sh.q[grp], g, level, comp, band, tx, ty, buf);
+	}
+}
+
+// Quantiser over a pyramid already in storage (the reference's
+// Encoder::encode_pre_transformed, pyrowave_encoder.cpp:1138-1151).
+// Two 32x32 blocks per CTA.
+__global__ void __launch_bounds__(256) quant_pretransformed_kernel(Geometry g, EncodeBuffers buf)
+{
+	__shared__ float tile[2][32][kBandPitch];
+	__shared__ QuantGroupShared q[2];
+	const int grp = threadIdx.x >> 7, t = threadIdx.x & 127;
+	const int b = blockIdx.x * 2 + grp;
+	const bool active = b < g.block_count_32x32;
+	int level = 0, comp = 0, band = 1, bx = 0, by = 0;
+	if (active)
+		unpack_job(buf.jobs[b], level, comp, band, bx, by);
+	if (active)
+	{
+		const LevelDesc &L = g.level[level];
+		const BandDesc &B = g.band[comp][level][band];
+		for (int k = t; k < 1024; k += 128)
+		{
+			int r = k >> 5, c = k & 31;
+			int64_t idx = B.offset + int64_t(by * 32 + r) * L.pitch + bx * 32 + c;
+			tile[grp][r][c] = load_coef(buf.coef32, buf.coef16, L.fp16 != 0, idx);
+		}
+	}
+	__syncthreads();
+	quant_analyze_block(&tile[grp][0][0], kBandPitch, active, t, q[grp], g, level, comp, band, bx, by, buf);
+}
+
+// ---------------------------------------------------------------------------
+// Block-wide (1024 threads) exclusive scan; returns the exclusive prefix and
+// the block total.
+__device__ __forceinline__ uint32_t block_exclusive_scan_1024(uint32_t v, uint32_t *warp_sums, uint32_t &total)
+{
+	const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+	uint32_t x = v;
+#pragma unroll
+	for (int off = 1; off < 32; off *= 2)
+	{
+		uint32_t y = __shfl_up_sync(0xffffffffu, x, off);
+		if (lane >= off)
+			x += y;
+	}
+	if (lane == 31)
+		warp_sums[warp] = x;
+	__syncthreads();
+	if (warp == 0)
+	{
+		uint32_t s = warp_sums[lane];
+#pragma unroll
+		for (int off = 1; off < 32; off *= 2)
+		{
+			uint32_t y = __shfl_up_sync(0xffffffffu, s, off);
+			if (lane >= off)
+				s += y;
+		}
+		warp_sums[lane] = s;
+	}
+	__syncthreads();
+	uint32_t base = warp == 0 ? 0u : warp_sums[warp - 1];
+	total = warp_sums[31];
+	__syncthreads();
+	return base + x - v;
+}
+
+// Exact-rate resolve (analyze_rate_control_finalize.comp + resolve_rate_control.comp).
+//
+// The reference walks all 2048 (bucket, subdivision) slots; for each slot with
+// savings it applies RD operations in block order while the running saving
+// stays below need - savings_of_earlier_slots. Every slot before the first slot
+// x* whose inclusive prefix reaches `need` is applied in full, slots after x*
+// not at all, and x* up to the first operation whose exclusive prefix reaches
+// its requirement. This kernel computes x* and that cut, then gives every
+// block its quant (the largest applied step), its word count and its offset.
+__global__ void __launch_bounds__(1024) resolve_kernel(Geometry g, EncodeBuffers buf, uint32_t target_words,
+                                                      uint32_t sequence)
+{
+	__shared__ uint32_t scan[kHistSize];
+	__shared__ uint32_t warp_sums[32];
+	__shared__ int s_xstar;
+	__shared__ uint32_t s_cut;
+	RateControlState *rc = buf.rc;
+	const int t = threadIdx.x;
+	const int nblocks = g.block_count_32x32;
+	const int nbps = g.blocks_per_subdivision;
+
+	uint32_t a = rc->histogram[2 * t], b = rc->histogram[2 * t + 1];
+	uint32_t total;
+	uint32_t excl = block_exclusive_scan_1024(a + b, warp_sums, total);
+	scan[2 * t] = excl + a;
+	scan[2 * t + 1] = excl + a + b;
+	if (t == 0)
+	{
+		s_xstar = -1;
+		s_cut = 0xffffffffu;
+	}
+	__syncthreads();
+
+	const int64_t need = int64_t(rc->consumed) - int64_t(target_words);
+	if (need > 0)
+	{
+		for (int x = 2 * t; x < 2 * t + 2; x++)
+			if (int64_t(scan[x]) >= need && (x == 0 || int64_t(scan[x - 1]) < need))
+				s_xstar = x;
+	}
+	__syncthreads();
+	const int xstar = s_xstar;
+
+	if (xstar >= 0)
+	{
+		const int64_t required = need - (xstar > 0 ? int64_t(scan[xstar - 1]) : 0);
+		const int sdiv = xstar & (kSubdivisions - 1);
+		const uint32_t bk = uint32_t(xstar >> 4);
+		const int start = sdiv * nbps;
+		const int end = min(start + nbps, nblocks);
+		uint32_t carry = 0;
+		for (int base = start; base < end; base += 1024)
+		{
+			const int blk = base + t;
+			uint32_t sv = 0;
+			if (blk < end)
+			{
+				const uint16_t *cost = buf.rd_cost + size_t(blk) * 16;
+				const uint8_t *bucket = buf.rd_bucket + size_t(blk) * 16;
+				for (int l = 1; l < 16; l++)
+					if (bucket[l] == bk)
+					{
+						sv = uint32_t(cost[l - 1]) - uint32_t(cost[l]);
+						break;
+					}
+			}
+			uint32_t tot;
+			uint32_t ex = block_exclusive_scan_1024(sv, warp_sums, tot);
+			if (sv != 0 && int64_t(carry) + int64_t(ex) >= required)
+				atomicMin(&s_cut, uint32_t(blk));
+			carry += tot;
+		}
+	}
+	__syncthreads();
+	const uint32_t cut = s_cut;
+
+	uint32_t carry = 0, non_zero = 0;
+	for (int base = 0; base < nblocks; base += 1024)
+	{
+		const int blk = base + t;
+		uint32_t words = 0;
+		int q = 0;
+		if (blk < nblocks)
+		{
+			const uint16_t *cost = buf.rd_cost + size_t(blk) * 16;
+			const uint8_t *bucket = buf.rd_bucket + size_t(blk) * 16;
+			const int sdiv = blk >> g.subdivision_shift;
+			for (int l = 1; l < 16; l++)
+			{
+				uint32_t saving = uint32_t(cost[l - 1]) - uint32_t(cost[l]);
+				if (saving == 0)
+					continue;
+				int x = int(bucket[l]) * kSubdivisions + sdiv;
+				if (x < xstar || (x == xstar && uint32_t(blk) < cut))
+					q = l;
+			}
+			words = cost[q];
+		}
+		uint32_t tot;
+		uint32_t ex = block_exclusive_scan_1024(words, warp_sums, tot);
+		if (blk < nblocks)
+		{
+			buf.quant[blk] = q;
+			buf.block_meta[2 * blk + 0] = carry + ex;
+			buf.block_meta[2 * blk + 1] = words;
+		}
+		uint32_t nz = __syncthreads_count(words != 0);
+		non_zero += nz;
+		carry += tot;
+	}
+
+	if (t == 0)
+	{
+		rc->total_words = carry;
+		rc->non_zero_blocks = non_zero;
+		rc->xstar = xstar;
+		rc->block_cut = cut;
+		rc->sequence = sequence & 7u;
+		if (2 + carry > buf.stream_capacity_words)
+			rc->error |= 1u;
+		// Start-of-frame sequence header (bitstream.md:250-265).
+		buf.stream[0] = uint32_t(g.width - 1) | (uint32_t(g.height - 1) << 14) | ((sequence & 7u) << 28) | (1u << 31);
+		buf.stream[1] = (non_zero & 0xffffffu) | (uint32_t(g.chroma444 ? 1 : 0) << 26);
+	}
+}
+
+// ---------------------------------------------------------------------------
+// Block packing: one 32x32 block per 128-thread CTA, assembled in shared
+// memory and written as whole words at its prefix-scanned offset.
+__global__ void __launch_bounds__(128) pack_kernel(Geometry g, EncodeBuffers buf)
+{
+	__shared__ uint32_t pkt[kMaxBlockWords];
+	__shared__ uint32_t s_ballot[4];
+	__shared__ uint32_t s_bytes[16];
+	__shared__ uint32_t s_sig[4];
+	const int blk = blockIdx.x;
+	const uint32_t words = buf.block_meta[2 * blk + 1];
+	if (words == 0)
+		return;
+	const uint32_t offset = buf.block_meta[2 * blk + 0];
+	const int quant = buf.quant[blk];
+	int level, comp, band, bx32, by32;
+	unpack_job(buf.jobs[blk], level, comp, band, bx32, by32);
+	const LevelDesc &L = g.level[level];
+	const BandDesc &B = g.band[comp][level][band];
+
+	const int t = threadIdx.x, lane = t & 31;
+	const int sub = t & 7, lx = (t >> 3) & 3, ly = t >> 5;
+	const int grp = ly * 4 + lx;
+	const int x8 = bx32 * 4 + lx, y8 = by32 * 4 + ly;
+	const bool in_range = x8 < L.blocks8_x && y8 < L.blocks8_y;
+	const uint32_t cw0 = in_range ? buf.code_words[B.block8_offset + y8 * B.block8_stride + x8] : 0u;
+	const uint32_t cw = quantize_code_word(cw0, quant);
+	const bool active = (cw & 0xffffu) != 0;
+
+	// Re-quantise this sub-block exactly as the quantiser did.
+	const float qs = __fdiv_rn(1.0f, decode_quant_scale((cw0 >> kQuantScaleOffset) & 0xfu));
+	const int ox = bx32 * 32 + lx * 8 + sub_x(sub), oy = by32 * 32 + ly * 8 + sub_y(sub);
+	uint32_t mag[8];
+	uint32_t neg = 0;
+#pragma unroll
+	for (int i = 0; i < 8; i++)
+	{
+		float c = load_coef(buf.coef32, buf.coef16, L.fp16 != 0,
+		                    B.offset + int64_t(oy + (i & 1)) * L.pitch + ox + (i >> 1));
+		float v = __fmul_rn(__fmul_rn(c, B.quant_resolution), qs);
+		v = fminf(fmaxf(v, -kMaxScaledMagnitude), kMaxScaledMagnitude);
+		mag[i] = uint32_t(abs(int(v)));
+		if (v < 0.0f)
+			neg |= 1u << i;
+	}
+	const uint32_t out_q = (cw >> kQPlanesOffset) & 0xfu;
+	const uint32_t planes = active ? ((cw >> (2 * sub)) & 3u) + out_q : 0u;
+	uint32_t sig = 0;
+	if (planes != 0)
+	{
+#pragma unroll
+		for (int i = 0; i < 8; i++)
+			if ((mag[i] >> quant) != 0)
+				sig |= 1u << i;
+	}
+
+	const uint32_t wb = __ballot_sync(0xffffffffu, active && sub == 0);
+	if (lane == 0)
+		s_ballot[ly] = ((wb >> 0) & 1u) | ((wb >> 7) & 2u) | ((wb >> 14) & 4u) | ((wb >> 21) & 8u);
+	if (sub == 0)
+		s_bytes[grp] = required_8x8_bytes(cw);
+
+	// Exclusive prefix of significant coefficients over threads 0..127.
+	const uint32_t nsig = uint32_t(__popc(sig));
+	uint32_t inc = nsig;
+#pragma unroll
+	for (int off = 1; off < 32; off *= 2)
+	{
+		uint32_t y = __shfl_up_sync(0xffffffffu, inc, off);
+		if (lane >= off)
+			inc += y;
+	}
+	if (lane == 31)
+		s_sig[ly] = inc;
+	// Exclusive prefix of plane bytes over the 8 sub-blocks of this 8x8.
+	uint32_t pinc = planes;
+#pragma unroll
+	for (int off = 1; off < 8; off *= 2)
+	{
+		uint32_t y = __shfl_up_sync(0xffffffffu, pinc, off);
+		if (sub >= off)
+			pinc += y;
+	}
+	const uint32_t sub_plane_offset = pinc - planes;
+	for (int w = t; w < int(words); w += 128)
+		pkt[w] = 0u;
+	__syncthreads();
+
+	const uint32_t ballot = s_ballot[0] | (s_ballot[1] << 4) | (s_ballot[2] << 8) | (s_ballot[3] << 12);
+	const uint32_t n = uint32_t(__popc(ballot));
+	uint32_t excl_bytes = 0, total_bytes = 0;
+	for (int k = 0; k < 16; k++)
+	{
+		if (k < grp)
+			excl_bytes += s_bytes[k];
+		total_bytes += s_bytes[k];
+	}
+	uint32_t sig_base = 0;
+	for (int w = 0; w < ly; w++)
+		sig_base += s_sig[w];
+	const uint32_t total_sig = s_sig[0] + s_sig[1] + s_sig[2] + s_sig[3];
+	const uint32_t sig_excl = sig_base + inc - nsig;
+
+	uint8_t *bytes = reinterpret_cast<uint8_t *>(pkt);
+	if (t == 0)
+	{
+		pkt[0] = (ballot & 0xffffu) | (words << 16) | ((buf.rc->sequence & 7u) << 28);
+		pkt[1] = modify_quant_code(B.quant_code, quant) | (uint32_t(blk) << 8);
+	}
+	if (active && sub == 0)
+	{
+		uint32_t compact = uint32_t(__popc(ballot & ((1u << grp) - 1u)));
+		bytes[8 + 2 * compact + 0] = uint8_t(cw);
+		bytes[8 + 2 * compact + 1] = uint8_t(cw >> 8);
+		bytes[8 + 2 * n + compact] = uint8_t(cw >> 16);
+	}
+	const uint32_t plane_base = 8 + 3 * n + excl_bytes + sub_plane_offset;
+	for (uint32_t p = 0; p < planes; p++)
+	{
+		const uint32_t bit = uint32_t(quant) + planes - 1u - p; // most significant plane first
+		uint32_t by = 0;
+#pragma unroll
+		for (int i = 0; i < 8; i++)
+			by |= ((mag[i] >> bit) & 1u) << i;
+		if (plane_base + p < uint32_t(kMaxBlockWords) * 4)
+			bytes[plane_base + p] = uint8_t(by);
+	}
+	__syncthreads();
+
+	// Sign bits of significant coefficients, in coefficient order, after the planes.
+	uint32_t bitpos = (8 + 3 * n + total_bytes) * 8 + sig_excl;
+#pragma unroll
+	for (int i = 0; i < 8; i++)
+	{
+		if ((sig >> i) & 1u)
+		{
+			if (((neg >> i) & 1u) && (bitpos >> 5) < uint32_t(kMaxBlockWords))
+				atomicOr(&pkt[bitpos >> 5], 1u << (bitpos & 31u));
+			bitpos++;
+		}
+	}
+	__syncthreads();
+
+	// The word count must match the rate-control estimate the offsets were built from.
+	const uint32_t bits = 8 * (3 * n + total_bytes) + total_sig;
+	const uint32_t expect = (bits + 31) / 32 + 2;
+	if (t == 0 && (expect != words || words > uint32_t(kMaxBlockWords) ||
+	               2 + offset + words > buf.stream_capacity_words))
+		atomicOr(&buf.rc->error, 2u);
+	if (words > uint32_t(kMaxBlockWords) || 2 + offset + words > buf.stream_capacity_words)
+		return;
+	uint32_t *dst = buf.stream + 2 + offset;
+	for (int w = t; w < int(words); w += 128)
+		dst[w] = pkt[w];
+}
+} // namespace
+
+void launch_dwt_forward_level(const Geometry &g, int level, const PlaneInput &in, const EncodeBuffers &buf,
+                              bool fused_quant, cudaStream_t stream)
+{
+	const LevelDesc &L = g.level[level];
+	dim3 grid(L.tiles_x * L.tiles_y, (level == 0 && !g.chroma444) ? 1 : 3);
+	dwt_forward_kernel<<<grid, kDwtThreads, 0, stream>>>(g, level, in, buf, fused_quant ? 1 : 0);
+}
+
+void launch_quant_pretransformed(const Geometry &g, const EncodeBuffers &buf, cudaStream_t stream)
+{
+	quant_pretransformed_kernel<<<(g.block_count_32x32 + 1) / 2, 256, 0, stream>>>(g, buf);
+}
+
+void launch_resolve(const Geometry &g, const EncodeBuffers &buf, uint32_t target_words, uint32_t sequence,
+                    cudaStream_t stream)
+{
+	resolve_kernel<<<1, 1024, 0, stream>>>(g, buf, target_words, sequence);
+}
+
+void launch_pack(const Geometry &g, const EncodeBuffers &buf, cudaStream_t stream)
+{
+	pack_kernel<<<g.block_count_32x32, 128, 0, stream>>>(g, buf);
+}
+} // namespace pw

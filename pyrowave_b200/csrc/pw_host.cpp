@@ -1,0 +1,1538 @@
+// Host side of the B200 PyroWave library: frame geometry, encoder and decoder
+// objects, the packet parser and the C API of include/pyrowave.h and
+// include/pyrowave_cuda.h.
+//
+// Reference interfaces replaced (file:line in the reference tree):
+//   C API                   pyrowave.h:73-539, pyrowave_c.cpp:32-1498
+//   geometry / block tables pyrowave_common.cpp:191-241 (and bitstream.md:472-511)
+//   quant tables            pyrowave_encoder.cpp:107-172
+//   encode sequence         pyrowave_encoder.cpp:1153-1183
+//   packetize               pyrowave_encoder.cpp:596-623,1048-1115
+//   packet parser           pyrowave_decoder.cpp:126-262,780-794,832-840
+//   decode sequence         pyrowave_decoder.cpp:796-830
+#include "pw_internal.h"
+
+#include "pyrowave.h"
+#include "pyrowave_cuda.h"
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <mutex>
+#include <new>
+#include <string>
+#include <vector>
+
+using namespace pw;
+
+namespace
+{
+int align_up(int v, int a) { return (v + a - 1) & ~(a - 1); }
+
+uint32_t float_bits(float f)
+{
+	uint32_t u;
+	memcpy(&u, &f, 4);
+	return u;
+}
+
+// 32x32 header quant code (pyrowave_common.hpp:135-145 / bitstream.md:441-449).
+uint32_t encode_quant(float decoder_q_scale)
+{
+	uint32_t v = float_bits(decoder_q_scale);
+	int e = int((v >> 23) & 0xffu) - 127 - kMaxScaleExp;
+	int m = int((v >> 20) & 7u);
+	e = std::min(std::max(-e, 0), 31);
+	return uint32_t((e << 3) | m) & 0xffu;
+}
+
+float decode_quant(uint32_t code)
+{
+	int e = kMaxScaleExp - int(code >> 3);
+	int m = int(code & 7u);
+	return std::ldexp(float(8 + m), e - 3);
+}
+
+// Initial quantiser resolution: a flat spectrum with noise-power normalisation,
+// 8 bits plus 2 for LL, 1 for HL/LH, plus the level, one less for chroma,
+// capped at 4096 (pyrowave_encoder.cpp:144-172).
+float noise_normalized_resolution(int level, int comp, int band)
+{
+	int bits = 8 + (band == 0 ? 2 : (band < 3 ? 1 : 0)) + level - (comp != 0 ? 1 : 0);
+	return float(1 << bits);
+}
+
+float quant_resolution(int level, int comp, int band)
+{
+	return std::min(4096.0f, noise_normalized_resolution(level, comp, band));
+}
+
+// Contrast-sensitivity weighting of the RD distortion (pyrowave_encoder.cpp:107-142):
+// band centre frequency in cycles per degree at 96 dpi and 1 m viewing distance,
+// CSF 2.6 (0.0192 + 0.114 f) exp(-(0.114 f)^1.1), chroma discounted 0.6 at 4:2:0,
+// squared because distortion is measured in power.
+float rdo_distortion_scale(int level, int comp, int band, bool chroma444)
+{
+	const float hx = (band & 1) ? 0.75f : 0.25f;
+	const float vy = (band & 2) ? 0.75f : 0.25f;
+	const float cpd_nyquist = 0.34f * 1.0f * 96.0f;
+	float cpd = std::sqrt(hx * hx + vy * vy) * cpd_nyquist * std::exp2(-float(level));
+	cpd = std::max(cpd, 8.0f);
+	float csf = 2.6f * (0.0192f + 0.114f * cpd) * std::exp(-std::pow(0.114f * cpd, 1.1f));
+	if (comp != 0 && level != kLevels - 1 && !chroma444)
+		csf *= 0.6f;
+	float weighted = csf * noise_normalized_resolution(level, comp, band);
+	return weighted * weighted;
+}
+
+bool has_level(int comp, int level, bool chroma444) { return !(level == 0 && comp != 0 && !chroma444); }
+
+// Frame geometry, padded band storage and the block tables.
+bool build_geometry(Geometry &g, std::vector<uint32_t> &jobs, int width, int height, bool chroma444, uint32_t fp16_mask)
+{
+	if (width <= 0 || height <= 0 || width > 16384 || height > 16384)
+		return false;
+	memset(&g, 0, sizeof(g));
+	g.width = width;
+	g.height = height;
+	g.chroma444 = chroma444 ? 1 : 0;
+	g.aligned_width = std::max(align_up(width, kAlignment), kMinImageSize);
+	g.aligned_height = std::max(align_up(height, kAlignment), kMinImageSize);
+	for (int c = 0; c < 3; c++)
+	{
+		g.plane_width[c] = (c == 0 || chroma444) ? width : width / 2;
+		g.plane_height[c] = (c == 0 || chroma444) ? height : height / 2;
+	}
+	for (int level = 0; level < kLevels; level++)
+	{
+		LevelDesc &L = g.level[level];
+		L.width = std::max(1, (g.aligned_width / 2) >> level);
+		L.height = std::max(1, (g.aligned_height / 2) >> level);
+		L.pitch = align_up(L.width, 32);
+		L.rows = align_up(L.height, 32);
+		L.tiles_x = L.pitch / 32;
+		L.tiles_y = L.rows / 32;
+		L.blocks8_x = (L.width + 7) / 8;
+		L.blocks8_y = (L.height + 7) / 8;
+		L.fp16 = (fp16_mask >> level) & 1u;
+	}
+
+	// Storage: every band of every (component, level) that exists, LL included.
+	int64_t off32 = 0, off16 = 0;
+	for (int level = 0; level < kLevels; level++)
+		for (int comp = 0; comp < kComponents; comp++)
+		{
+			if (!has_level(comp, level, chroma444))
+				continue;
+			const LevelDesc &L = g.level[level];
+			for (int band = 0; band < 4; band++)
+			{
+				int64_t &off = L.fp16 ? off16 : off32;
+				g.band[comp][level][band].offset = off;
+				off += int64_t(L.pitch) * L.rows;
+			}
+		}
+	g.storage_elems32 = off32;
+	g.storage_elems16 = off16;
+
+	// Block index order (bitstream.md:472-511): level 4 -> 0, component, band.
+	jobs.clear();
+	int count8 = 0, count32 = 0;
+	for (int level = kLevels - 1; level >= 0; level--)
+		for (int comp = 0; comp < kComponents; comp++)
+		{
+			if (!has_level(comp, level, chroma444))
+				continue;
+			for (int band = (level == kLevels - 1 ? 0 : 1); band < 4; band++)
+			{
+				const LevelDesc &L = g.level[level];
+				BandDesc &B = g.band[comp][level][band];
+				B.present = 1;
+				B.block8_offset = count8;
+				B.block8_stride = L.blocks8_x;
+				B.block32_offset = count32;
+				B.block32_stride = (L.width + 31) / 32;
+				float qr = quant_resolution(level, comp, band);
+				B.quant_code = encode_quant(1.0f / qr);
+				B.quant_resolution = 1.0f / decode_quant(B.quant_code);
+				B.rdo_scale = rdo_distortion_scale(level, comp, band, chroma444) * (1.0f / 256.0f);
+				int by32n = (L.height + 31) / 32;
+				for (int by = 0; by < by32n; by++)
+					for (int bx = 0; bx < B.block32_stride; bx++)
+						jobs.push_back(pack_job(level, comp, band, bx, by));
+				count32 += B.block32_stride * by32n;
+				count8 += L.blocks8_x * L.blocks8_y;
+			}
+		}
+	g.block_count_8x8 = count8;
+	g.block_count_32x32 = count32;
+	// Blocks per subdivision: next power of two of ceil(count / 16) (pyrowave_encoder.cpp:21-26).
+	int per = (count32 + kSubdivisions - 1) / kSubdivisions;
+	int pot = 1, shift = 0;
+	while (pot < per)
+	{
+		pot *= 2;
+		shift++;
+	}
+	g.blocks_per_subdivision = pot;
+	g.subdivision_shift = shift;
+	return true;
+}
+
+// Per-band resolution override of encode_pre_transformed (pyrowave_encoder.cpp:449,251).
+void apply_quant_scale_override(Geometry &g, float quant_scale)
+{
+	for (int comp = 0; comp < kComponents; comp++)
+		for (int level = 0; level < kLevels; level++)
+			for (int band = 0; band < 4; band++)
+			{
+				BandDesc &B = g.band[comp][level][band];
+				if (!B.present)
+					continue;
+				float qr = quant_scale < 0.0f ? quant_resolution(level, comp, band) : quant_scale;
+				B.quant_code = encode_quant(1.0f / qr);
+				B.quant_resolution = 1.0f / decode_quant(B.quant_code);
+			}
+}
+
+template <typename T> T *dev_alloc(size_t count, bool &ok)
+{
+	if (count == 0)
+		count = 1;
+	void *p = nullptr;
+	if (cudaMalloc(&p, count * sizeof(T)) != cudaSuccess)
+	{
+		ok = false;
+		(void)cudaGetLastError();
+		return nullptr;
+	}
+	return static_cast<T *>(p);
+}
+
+template <typename T> T *host_alloc(size_t count, bool &ok)
+{
+	if (count == 0)
+		count = 1;
+	void *p = nullptr;
+	if (cudaMallocHost(&p, count * sizeof(T)) != cudaSuccess)
+	{
+		ok = false;
+		(void)cudaGetLastError();
+		return nullptr;
+	}
+	return static_cast<T *>(p);
+}
+
+void dev_free(void *p)
+{
+	if (p)
+		cudaFree(p);
+}
+void host_free(void *p)
+{
+	if (p)
+		cudaFreeHost(p);
+}
+
+struct StageTimer
+{
+	const char *tag;
+	double total_ms = 0.0;
+	uint64_t frames = 0;
+};
+
+} // namespace
+
+// ---------------------------------------------------------------------------
+struct pyrowave_device_opaque
+{
+	int cuda_device = 0;
+	cudaStream_t stream = nullptr;
+	bool stage_timing = false;
+	std::mutex lock;
+	std::vector<StageTimer> timers;
+
+	void add_time(const char *tag, double ms)
+	{
+		std::lock_guard<std::mutex> g(lock);
+		for (auto &t : timers)
+			if (strcmp(t.tag, tag) == 0)
+			{
+				t.total_ms += ms;
+				t.frames++;
+				return;
+			}
+		timers.push_back({tag, ms, 1});
+	}
+};
+
+namespace
+{
+// Per-stage GPU timing with CUDA events (the reference's register_time_interval,
+// pyrowave_encoder.cpp:277,335,411,486,591; surfaced by report_performance_stats).
+struct StageEvents
+{
+	static constexpr int kMax = 8;
+	cudaEvent_t ev[kMax + 1] = {};
+	const char *tags[kMax] = {};
+	int count = 0;
+	bool pending = false;
+	bool created = false;
+
+	void begin(pyrowave_device_opaque *dev, cudaStream_t s)
+	{
+		if (!dev->stage_timing)
+			return;
+		if (!created)
+		{
+			for (auto &e : ev)
+				cudaEventCreate(&e);
+			created = true;
+		}
+		count = 0;
+		cudaEventRecord(ev[0], s);
+	}
+	void mark(pyrowave_device_opaque *dev, cudaStream_t s, const char *tag)
+	{
+		if (!dev->stage_timing || count >= kMax)
+			return;
+		tags[count++] = tag;
+		cudaEventRecord(ev[count], s);
+		pending = true;
+	}
+	void collect(pyrowave_device_opaque *dev)
+	{
+		if (!pending)
+			return;
+		pending = false;
+		cudaEventSynchronize(ev[count]);
+		for (int i = 0; i < count; i++)
+		{
+			float ms = 0.0f;
+			cudaEventElapsedTime(&ms, ev[i], ev[i + 1]);
+			dev->add_time(tags[i], ms);
+		}
+	}
+	void destroy()
+	{
+		if (created)
+			for (auto &e : ev)
+				cudaEventDestroy(e);
+		created = false;
+	}
+};
+} // namespace
+
+struct pyrowave_encoder_opaque
+{
+	pyrowave_device device = nullptr;
+	Geometry g = {};
+	std::vector<uint32_t> jobs;
+	uint32_t fp16_mask = 0;
+	bool allocated = false;
+
+	float *coef32 = nullptr;
+	__half *coef16 = nullptr;
+	uint32_t *code_words = nullptr;
+	uint16_t *rd_cost = nullptr;
+	uint8_t *rd_bucket = nullptr;
+	float *rd_dist = nullptr;
+	RateControlState *rc = nullptr;
+	int32_t *quant = nullptr;
+	uint32_t *block_meta = nullptr;
+	uint32_t *stream_buf = nullptr;
+	uint32_t stream_capacity = 0;
+	uint32_t *jobs_d = nullptr;
+	uint8_t *in_planes[3] = {};
+	int in_pitch[3] = {};
+
+	uint32_t *h_meta = nullptr;
+	uint32_t *h_stream = nullptr;
+	uint32_t h_stream_capacity = 0;
+	uint32_t *h_total = nullptr;
+	cudaEvent_t done = nullptr;
+	bool has_frame = false;     // a completed CPU-visible encode exists
+	bool has_device_frame = false;
+	uint32_t sequence_count = 0;
+	StageEvents timing;
+
+	EncodeBuffers buffers() const
+	{
+		EncodeBuffers b;
+		b.coef32 = coef32;
+		b.coef16 = coef16;
+		b.code_words = code_words;
+		b.rd_cost = rd_cost;
+		b.rd_bucket = rd_bucket;
+		b.rd_dist = rd_dist;
+		b.rc = rc;
+		b.quant = quant;
+		b.block_meta = block_meta;
+		b.stream = stream_buf;
+		b.stream_capacity_words = stream_capacity;
+		b.jobs = jobs_d;
+		return b;
+	}
+
+	void release()
+	{
+		if (device)
+			cudaStreamSynchronize(device->stream);
+		dev_free(coef32);
+		dev_free(coef16);
+		dev_free(code_words);
+		dev_free(rd_cost);
+		dev_free(rd_bucket);
+		dev_free(rd_dist);
+		dev_free(rc);
+		dev_free(quant);
+		dev_free(block_meta);
+		dev_free(stream_buf);
+		dev_free(jobs_d);
+		for (auto &p : in_planes)
+			dev_free(p);
+		host_free(h_meta);
+		host_free(h_stream);
+		host_free(h_total);
+		if (done)
+			cudaEventDestroy(done);
+		timing.destroy();
+		coef32 = nullptr;
+		coef16 = nullptr;
+		allocated = false;
+	}
+
+	pyrowave_result allocate()
+	{
+		if (allocated)
+			return PYROWAVE_SUCCESS;
+		if (!build_geometry(g, jobs, g.width, g.height, g.chroma444 != 0, fp16_mask))
+			return PYROWAVE_ERROR_INVALID_ARGUMENT;
+		bool ok = true;
+		coef32 = dev_alloc<float>(size_t(g.storage_elems32), ok);
+		coef16 = dev_alloc<__half>(size_t(g.storage_elems16), ok);
+		code_words = dev_alloc<uint32_t>(size_t(g.block_count_8x8), ok);
+		rd_cost = dev_alloc<uint16_t>(size_t(g.block_count_32x32) * 16, ok);
+		rd_bucket = dev_alloc<uint8_t>(size_t(g.block_count_32x32) * 16, ok);
+		rd_dist = dev_alloc<float>(size_t(g.block_count_32x32) * 16, ok);
+		rc = dev_alloc<RateControlState>(1, ok);
+		quant = dev_alloc<int32_t>(size_t(g.block_count_32x32), ok);
+		block_meta = dev_alloc<uint32_t>(size_t(g.block_count_32x32) * 2, ok);
+		jobs_d = dev_alloc<uint32_t>(jobs.size(), ok);
+		h_meta = host_alloc<uint32_t>(size_t(g.block_count_32x32) * 2, ok);
+		h_total = host_alloc<uint32_t>(4, ok);
+		if (ok && cudaEventCreateWithFlags(&done, cudaEventDisableTiming) != cudaSuccess)
+			ok = false;
+		if (!ok)
+		{
+			release();
+			return PYROWAVE_ERROR_OUT_OF_DEVICE_MEMORY;
+		}
+		cudaMemcpy(jobs_d, jobs.data(), jobs.size() * 4, cudaMemcpyHostToDevice);
+		allocated = true;
+		return PYROWAVE_SUCCESS;
+	}
+
+	pyrowave_result ensure_stream_capacity(uint32_t words)
+	{
+		if (words <= stream_capacity)
+			return PYROWAVE_SUCCESS;
+		cudaStreamSynchronize(device->stream);
+		dev_free(stream_buf);
+		bool ok = true;
+		stream_buf = dev_alloc<uint32_t>(words, ok);
+		stream_capacity = ok ? words : 0;
+		return ok ? PYROWAVE_SUCCESS : PYROWAVE_ERROR_OUT_OF_DEVICE_MEMORY;
+	}
+
+	pyrowave_result ensure_host_capacity(uint32_t words)
+	{
+		if (words <= h_stream_capacity)
+			return PYROWAVE_SUCCESS;
+		host_free(h_stream);
+		bool ok = true;
+		h_stream = host_alloc<uint32_t>(words, ok);
+		h_stream_capacity = ok ? words : 0;
+		return ok ? PYROWAVE_SUCCESS : PYROWAVE_ERROR_OUT_OF_HOST_MEMORY;
+	}
+
+	pyrowave_result ensure_input_planes()
+	{
+		if (in_planes[0])
+			return PYROWAVE_SUCCESS;
+		bool ok = true;
+		for (int c = 0; c < 3; c++)
+		{
+			// Chroma rows are sized for the interleaved CbCr plane of NV12 as well.
+			in_pitch[c] = align_up(c == 0 ? g.plane_width[c] : 2 * g.plane_width[c], 128);
+			in_planes[c] = dev_alloc<uint8_t>(size_t(in_pitch[c]) * g.plane_height[c], ok);
+		}
+		return ok ? PYROWAVE_SUCCESS : PYROWAVE_ERROR_OUT_OF_DEVICE_MEMORY;
+	}
+
+	// Validates the budget (pyrowave_c.cpp:957-961) and returns the target in
+	// words after the 8-byte sequence header (pyrowave_encoder.cpp:289-324).
+	static bool budget_words(const pyrowave_rate_control *rc, uint32_t &target_words, uint32_t &capacity_words)
+	{
+		if (!rc)
+			return false;
+		uint64_t target = uint64_t(rc->maximum_bitstream_size) & ~uint64_t(3);
+		if (target == 0 || target > 0xffffffffull)
+			return false;
+		uint64_t payload = target >= 8 ? target - 8 : target;
+		target_words = uint32_t(payload / 4);
+		capacity_words = target_words + 2;
+		return true;
+	}
+
+	// Queue the encode of resident input planes (pyrowave_encoder.cpp:1153-1183).
+	pyrowave_result enqueue(const PlaneInput &in, const pyrowave_rate_control *rc_in, cudaStream_t s)
+	{
+		uint32_t target_words, capacity;
+		if (!budget_words(rc_in, target_words, capacity))
+			return PYROWAVE_ERROR_INVALID_ARGUMENT;
+		pyrowave_result r = ensure_stream_capacity(capacity);
+		if (r != PYROWAVE_SUCCESS)
+			return r;
+		sequence_count = (sequence_count + 1) & 7u;
+		EncodeBuffers b = buffers();
+		timing.collect(device);
+		timing.begin(device, s);
+		cudaMemsetAsync(rc, 0, sizeof(RateControlState), s);
+		for (int level = 0; level < kLevels; level++)
+			launch_dwt_forward_level(g, level, in, b, true, s);
+		timing.mark(device, s, "DWT+Quant+Analyze");
+		launch_resolve(g, b, target_words, sequence_count, s);
+		timing.mark(device, s, "Resolve");
+		launch_pack(g, b, s);
+		timing.mark(device, s, "Packing");
+		if (cudaPeekAtLastError() != cudaSuccess)
+			return PYROWAVE_ERROR_GENERIC;
+		has_device_frame = true;
+		return PYROWAVE_SUCCESS;
+	}
+
+	// Copy the result to pinned host memory for compute_num_packets / packetize.
+	pyrowave_result queue_readback(cudaStream_t s)
+	{
+		pyrowave_result r = ensure_host_capacity(stream_capacity);
+		if (r != PYROWAVE_SUCCESS)
+			return r;
+		cudaMemcpyAsync(h_meta, block_meta, size_t(g.block_count_32x32) * 8, cudaMemcpyDeviceToHost, s);
+		cudaMemcpyAsync(h_total, &rc->error, 8, cudaMemcpyDeviceToHost, s); // error, total_words
+		cudaMemcpyAsync(h_stream, stream_buf, size_t(stream_capacity) * 4, cudaMemcpyDeviceToHost, s);
+		cudaEventRecord(done, s);
+		has_frame = true;
+		return PYROWAVE_SUCCESS;
+	}
+
+	bool wait()
+	{
+		if (!has_frame)
+			return false;
+		cudaEventSynchronize(done);
+		return true;
+	}
+};
+
+struct pyrowave_decoder_opaque
+{
+	pyrowave_device device = nullptr;
+	Geometry g = {};
+	std::vector<uint32_t> jobs;
+	uint32_t fp16_mask = 0;
+	bool allocated = false;
+
+	float *coef32 = nullptr;
+	__half *coef16 = nullptr;
+	uint32_t *jobs_d = nullptr;
+	uint32_t *offsets_d = nullptr;
+	uint32_t *payload_d = nullptr;
+	size_t payload_capacity = 0;
+	uint8_t *out_planes[3] = {};
+	int out_pitch[3] = {};
+	uint32_t *h_upload = nullptr;
+	size_t h_upload_capacity = 0;
+	StageEvents timing;
+
+	// Parser state (pyrowave_decoder.cpp:24-39).
+	std::vector<uint32_t> offsets;
+	std::vector<uint32_t> payload;
+	int decoded_blocks = 0;
+	int total_blocks_in_sequence = 0;
+	uint32_t last_seq = UINT32_MAX;
+	bool decoded_frame_for_current_sequence = false;
+
+	void clear()
+	{
+		std::fill(offsets.begin(), offsets.end(), UINT32_MAX);
+		decoded_blocks = 0;
+		last_seq = UINT32_MAX;
+		decoded_frame_for_current_sequence = false;
+		total_blocks_in_sequence = g.block_count_32x32;
+		payload.clear();
+	}
+
+	// Append one coded block; the first copy of a block index wins.
+	bool add_block(const uint8_t *data, uint32_t block_index, uint32_t payload_words)
+	{
+		uint32_t &off = offsets[block_index];
+		if (off != UINT32_MAX)
+			return true;
+		decoded_blocks++;
+		off = uint32_t(payload.size());
+		if (payload_words < 2)
+			return false;
+		size_t base = payload.size();
+		payload.resize(base + payload_words);
+		memcpy(&payload[base], data, size_t(payload_words) * 4);
+		return true;
+	}
+
+	// Packet parser with the reference's sequence handling (pyrowave_decoder.cpp:154-262):
+	// a start-of-frame or block header from an older sequence (3-bit wrapping
+	// difference > 3) is dropped, a newer one restarts the frame.
+	bool push_packet(const uint8_t *data, size_t size)
+	{
+		while (size >= 8)
+		{
+			uint32_t w0, w1;
+			memcpy(&w0, data, 4);
+			memcpy(&w1, data + 4, 4);
+			const uint32_t seq = (w0 >> 28) & 7u;
+			if ((w0 >> 31) & 1u)
+			{
+				// BitstreamSequenceHeader (bitstream.md:250-265).
+				const uint32_t chroma_resolution = (w1 >> 26) & 1u;
+				if (chroma_resolution != uint32_t(g.chroma444))
+					return false;
+				const uint32_t diff = (seq - last_seq) & 7u;
+				if (last_seq != UINT32_MAX && diff > 3)
+					return true;
+				if (last_seq == UINT32_MAX || diff != 0)
+				{
+					clear();
+					last_seq = seq;
+				}
+				const uint32_t code = (w1 >> 24) & 3u;
+				if (code != 0)
+					return false;
+				if (int(w0 & 0x3fffu) + 1 != g.width || int((w0 >> 14) & 0x3fffu) + 1 != g.height)
+					return false;
+				total_blocks_in_sequence = int(w1 & 0xffffffu);
+				data += 8;
+				size -= 8;
+				continue;
+			}
+			const uint32_t words = (w0 >> 16) & 0xfffu;
+			const size_t packet_size = size_t(words) * 4;
+			if (packet_size > size)
+				return false;
+			bool restart;
+			if (last_seq == UINT32_MAX)
+				restart = true;
+			else
+			{
+				const uint32_t diff = (seq - last_seq) & 7u;
+				if (diff > 3)
+					return true;
+				restart = diff != 0;
+			}
+			if (restart)
+			{
+				clear();
+				last_seq = seq;
+			}
+			const uint32_t block_index = (w1 >> 8) & 0xffffffu;
+			if (block_index >= uint32_t(g.block_count_32x32))
+				return false;
+			if (!add_block(data, block_index, words))
+				return false;
+			data += packet_size;
+			size -= packet_size;
+		}
+		return size == 0;
+	}
+
+	bool decode_is_ready(bool allow_partial) const
+	{
+		if (decoded_frame_for_current_sequence || last_seq == UINT32_MAX)
+			return false;
+		if (decoded_blocks < total_blocks_in_sequence)
+			if (!allow_partial || decoded_blocks <= total_blocks_in_sequence / 2)
+				return false;
+		return true;
+	}
+
+	void release()
+	{
+		if (device)
+			cudaStreamSynchronize(device->stream);
+		dev_free(coef32);
+		dev_free(coef16);
+		dev_free(jobs_d);
+		dev_free(offsets_d);
+		dev_free(payload_d);
+		for (auto &p : out_planes)
+			dev_free(p);
+		host_free(h_upload);
+		timing.destroy();
+		allocated = false;
+	}
+
+	pyrowave_result allocate()
+	{
+		if (allocated)
+			return PYROWAVE_SUCCESS;
+		if (!build_geometry(g, jobs, g.width, g.height, g.chroma444 != 0, fp16_mask))
+			return PYROWAVE_ERROR_INVALID_ARGUMENT;
+		bool ok = true;
+		coef32 = dev_alloc<float>(size_t(g.storage_elems32), ok);
+		coef16 = dev_alloc<__half>(size_t(g.storage_elems16), ok);
+		jobs_d = dev_alloc<uint32_t>(jobs.size(), ok);
+		offsets_d = dev_alloc<uint32_t>(size_t(g.block_count_32x32), ok);
+		if (!ok)
+		{
+			release();
+			return PYROWAVE_ERROR_OUT_OF_DEVICE_MEMORY;
+		}
+		cudaMemcpy(jobs_d, jobs.data(), jobs.size() * 4, cudaMemcpyHostToDevice);
+		if (offsets.size() != size_t(g.block_count_32x32))
+		{
+			offsets.assign(size_t(g.block_count_32x32), UINT32_MAX);
+			payload.reserve(1 << 18);
+			clear();
+		}
+		allocated = true;
+		return PYROWAVE_SUCCESS;
+	}
+
+	pyrowave_result ensure_payload(size_t words)
+	{
+		words += 4; // keep one extra word for sign reads at the very end
+		if (words > payload_capacity)
+		{
+			dev_free(payload_d);
+			bool ok = true;
+			size_t cap = std::max<size_t>(words * 2, 1 << 16);
+			payload_d = dev_alloc<uint32_t>(cap, ok);
+			payload_capacity = ok ? cap : 0;
+			if (!ok)
+				return PYROWAVE_ERROR_OUT_OF_DEVICE_MEMORY;
+		}
+		size_t need = words + size_t(g.block_count_32x32);
+		if (need > h_upload_capacity)
+		{
+			host_free(h_upload);
+			bool ok = true;
+			size_t cap = std::max<size_t>(need * 2, 1 << 16);
+			h_upload = host_alloc<uint32_t>(cap, ok);
+			h_upload_capacity = ok ? cap : 0;
+			if (!ok)
+				return PYROWAVE_ERROR_OUT_OF_HOST_MEMORY;
+		}
+		return PYROWAVE_SUCCESS;
+	}
+
+	pyrowave_result ensure_output_planes()
+	{
+		if (out_planes[0])
+			return PYROWAVE_SUCCESS;
+		bool ok = true;
+		for (int c = 0; c < 3; c++)
+		{
+			out_pitch[c] = align_up(g.plane_width[c], 128);
+			out_planes[c] = dev_alloc<uint8_t>(size_t(out_pitch[c]) * g.plane_height[c], ok);
+		}
+		return ok ? PYROWAVE_SUCCESS : PYROWAVE_ERROR_OUT_OF_DEVICE_MEMORY;
+	}
+
+	// Dequantise + inverse transform (pyrowave_decoder.cpp:796-830).
+	void run(const DecodeInput &in, const PlaneOutput &out, cudaStream_t s, bool dequant)
+	{
+		timing.collect(device);
+		timing.begin(device, s);
+		if (dequant)
+		{
+			launch_dequant(g, in, s);
+			timing.mark(device, s, "Dequant");
+		}
+		for (int level = kLevels - 1; level >= 0; level--)
+			launch_idwt_level(g, level, in, out, s);
+		timing.mark(device, s, "iDWT");
+		decoded_frame_for_current_sequence = true;
+	}
+
+	// Upload the parsed frame and decode it.
+	pyrowave_result decode_parsed(const PlaneOutput &out, cudaStream_t s)
+	{
+		pyrowave_result r = ensure_payload(payload.size());
+		if (r != PYROWAVE_SUCCESS)
+			return r;
+		const size_t nb = size_t(g.block_count_32x32);
+		memcpy(h_upload, offsets.data(), nb * 4);
+		if (!payload.empty())
+			memcpy(h_upload + nb, payload.data(), payload.size() * 4);
+		cudaMemcpyAsync(offsets_d, h_upload, nb * 4, cudaMemcpyHostToDevice, s);
+		if (!payload.empty())
+			cudaMemcpyAsync(payload_d, h_upload + nb, payload.size() * 4, cudaMemcpyHostToDevice, s);
+		DecodeInput in = {};
+		in.offsets = offsets_d;
+		in.payload = payload_d;
+		in.payload_words = uint32_t(payload.size());
+		in.jobs = jobs_d;
+		in.coef32 = coef32;
+		in.coef16 = coef16;
+		run(in, out, s, true);
+		return cudaPeekAtLastError() == cudaSuccess ? PYROWAVE_SUCCESS : PYROWAVE_ERROR_GENERIC;
+	}
+};
+
+// ---------------------------------------------------------------------------
+namespace
+{
+cudaStream_t pick_stream(pyrowave_device dev, pyrowave_cuda_stream s)
+{
+	return s ? reinterpret_cast<cudaStream_t>(s) : dev->stream;
+}
+
+bool plane_dims(pyrowave_chroma_subsampling chroma, int width, int height, int plane, int &w, int &h)
+{
+	w = width;
+	h = height;
+	if (plane != 0 && chroma == PYROWAVE_CHROMA_SUBSAMPLING_420)
+	{
+		w /= 2;
+		h /= 2;
+	}
+	return true;
+}
+
+pyrowave_result fill_layout(const Geometry &g, uint32_t mask, pyrowave_cuda_layout *layout)
+{
+	if (!layout)
+		return PYROWAVE_ERROR_INVALID_ARGUMENT;
+	layout->width = g.width;
+	layout->height = g.height;
+	layout->chroma444 = g.chroma444;
+	layout->aligned_width = g.aligned_width;
+	layout->aligned_height = g.aligned_height;
+	layout->block_count_8x8 = g.block_count_8x8;
+	layout->block_count_32x32 = g.block_count_32x32;
+	size_t n = 0;
+	for (int level = 0; level < kLevels; level++)
+		for (int comp = 0; comp < kComponents; comp++)
+			for (int band = 0; band < 4; band++)
+				if (g.band[comp][level][band].present)
+					n += size_t(g.level[level].width) * g.level[level].height;
+	layout->pyramid_size = n;
+	layout->fp16_level_mask = mask;
+	return PYROWAVE_SUCCESS;
+}
+} // namespace
+
+extern "C" {
+
+void pyrowave_get_api_version(uint32_t *major, uint32_t *minor, uint32_t *patch)
+{
+	*major = PYROWAVE_API_VERSION_MAJOR;
+	*minor = PYROWAVE_API_VERSION_MINOR;
+	*patch = PYROWAVE_API_VERSION_PATCH;
+}
+
+pyrowave_result pyrowave_create_default_device(pyrowave_device *device)
+{
+	if (!device)
+		return PYROWAVE_ERROR_INVALID_ARGUMENT;
+	int count = 0;
+	if (cudaGetDeviceCount(&count) != cudaSuccess || count == 0)
+	{
+		(void)cudaGetLastError();
+		return PYROWAVE_ERROR_NO_VULKAN;
+	}
+	auto *dev = new (std::nothrow) pyrowave_device_opaque;
+	if (!dev)
+		return PYROWAVE_ERROR_OUT_OF_HOST_MEMORY;
+	cudaGetDevice(&dev->cuda_device);
+	if (cudaStreamCreateWithFlags(&dev->stream, cudaStreamNonBlocking) != cudaSuccess)
+	{
+		delete dev;
+		return PYROWAVE_ERROR_GENERIC;
+	}
+	const char *env = getenv("PYROWAVE_STAGE_TIMING");
+	dev->stage_timing = env && atoi(env) != 0;
+	*device = dev;
+	return PYROWAVE_SUCCESS;
+}
+
+pyrowave_result pyrowave_create_device(const pyrowave_device_create_info *, pyrowave_device *)
+{
+	return PYROWAVE_ERROR_NO_VULKAN;
+}
+
+pyrowave_result pyrowave_create_device_by_compat(uint32_t vid, uint32_t pid, const pyrowave_uuid *device_uuid,
+                                                 const pyrowave_uuid *, const pyrowave_luid *,
+                                                 pyrowave_device *device)
+{
+	if (!device)
+		return PYROWAVE_ERROR_INVALID_ARGUMENT;
+	if (vid != 0 && vid != 0x10de)
+		return PYROWAVE_ERROR_NO_VULKAN;
+	(void)pid;
+	if (device_uuid)
+	{
+		int count = 0;
+		cudaGetDeviceCount(&count);
+		bool found = false;
+		for (int i = 0; i < count && !found; i++)
+		{
+			cudaDeviceProp prop;
+			if (cudaGetDeviceProperties(&prop, i) == cudaSuccess &&
+			    memcmp(prop.uuid.bytes, device_uuid->uuid, 16) == 0)
+			{
+				cudaSetDevice(i);
+				found = true;
+			}
+		}
+		if (!found)
+			return PYROWAVE_ERROR_NO_VULKAN;
+	}
+	return pyrowave_create_default_device(device);
+}
+
+void pyrowave_device_report_performance_stats(pyrowave_device device, pyrowave_message_cb cb, void *userdata, bool reset)
+{
+	if (!device || !cb)
+		return;
+	std::lock_guard<std::mutex> g(device->lock);
+	for (auto &t : device->timers)
+	{
+		char msg[256];
+		snprintf(msg, sizeof(msg), "%s: %.3f ms per frame\n", t.tag, t.frames ? t.total_ms / double(t.frames) : 0.0);
+		cb(userdata, msg);
+	}
+	if (reset)
+		device->timers.clear();
+}
+
+void pyrowave_device_get_vk_device_handles(pyrowave_device, VkInstance *vk_instance,
+                                           VkPhysicalDevice *vk_physical_device, VkDevice *vk_device)
+{
+	if (vk_instance)
+		*vk_instance = nullptr;
+	if (vk_physical_device)
+		*vk_physical_device = nullptr;
+	if (vk_device)
+		*vk_device = nullptr;
+}
+
+void pyrowave_device_set_command_buffer(pyrowave_device, VkCommandBuffer) {}
+
+pyrowave_result pyrowave_device_set_queue_type(pyrowave_device device, VkQueueFlagBits)
+{
+	return device ? PYROWAVE_SUCCESS : PYROWAVE_ERROR_INVALID_ARGUMENT;
+}
+
+bool pyrowave_device_confirm_interop_support(pyrowave_device) { return false; }
+
+void pyrowave_device_destroy(pyrowave_device device)
+{
+	if (!device)
+		return;
+	cudaStreamSynchronize(device->stream);
+	cudaStreamDestroy(device->stream);
+	delete device;
+}
+
+pyrowave_result pyrowave_sync_object_create(const pyrowave_sync_object_create_info *, pyrowave_sync_object *sync)
+{
+	if (sync)
+		*sync = nullptr;
+	return PYROWAVE_ERROR_NOT_IMPLEMENTED;
+}
+VkSemaphore pyrowave_sync_object_get_semaphore(pyrowave_sync_object) { return nullptr; }
+pyrowave_result pyrowave_sync_object_export_handle(pyrowave_sync_object, pyrowave_os_handle *)
+{
+	return PYROWAVE_ERROR_NOT_IMPLEMENTED;
+}
+pyrowave_result pyrowave_sync_object_cpu_wait(pyrowave_sync_object, uint64_t, uint64_t)
+{
+	return PYROWAVE_ERROR_NOT_IMPLEMENTED;
+}
+pyrowave_result pyrowave_sync_object_cpu_signal(pyrowave_sync_object, uint64_t) { return PYROWAVE_ERROR_NOT_IMPLEMENTED; }
+void pyrowave_sync_object_destroy(pyrowave_sync_object) {}
+
+pyrowave_result pyrowave_image_create(const pyrowave_image_create_info *, pyrowave_image *image)
+{
+	if (image)
+		*image = nullptr;
+	return PYROWAVE_ERROR_NOT_IMPLEMENTED;
+}
+VkImage pyrowave_image_get_handle(pyrowave_image) { return nullptr; }
+pyrowave_result pyrowave_image_get_image_view(pyrowave_image, VkImageAspectFlagBits, VkImageUsageFlagBits,
+                                              pyrowave_image_view *)
+{
+	return PYROWAVE_ERROR_NOT_IMPLEMENTED;
+}
+void pyrowave_image_destroy(pyrowave_image) {}
+
+// --- encoder ---------------------------------------------------------------
+pyrowave_result pyrowave_encoder_create(const pyrowave_encoder_create_info *info, pyrowave_encoder *encoder)
+{
+	if (!info || !encoder || !info->device)
+		return PYROWAVE_ERROR_INVALID_ARGUMENT;
+	if (info->width <= 0 || info->height <= 0)
+		return PYROWAVE_ERROR_INVALID_ARGUMENT;
+	if (info->chroma == PYROWAVE_CHROMA_SUBSAMPLING_420 && ((info->width & 1) || (info->height & 1)))
+		return PYROWAVE_ERROR_INVALID_ARGUMENT;
+	if (info->chroma != PYROWAVE_CHROMA_SUBSAMPLING_420 && info->chroma != PYROWAVE_CHROMA_SUBSAMPLING_444)
+		return PYROWAVE_ERROR_INVALID_ARGUMENT;
+	auto *enc = new (std::nothrow) pyrowave_encoder_opaque;
+	if (!enc)
+		return PYROWAVE_ERROR_OUT_OF_HOST_MEMORY;
+	enc->device = info->device;
+	std::vector<uint32_t> jobs;
+	if (!build_geometry(enc->g, jobs, info->width, info->height, info->chroma == PYROWAVE_CHROMA_SUBSAMPLING_444, 0))
+	{
+		delete enc;
+		return PYROWAVE_ERROR_GENERIC;
+	}
+	*encoder = enc;
+	return PYROWAVE_SUCCESS;
+}
+
+pyrowave_result pyrowave_encoder_encode_gpu_synchronous(pyrowave_encoder, const pyrowave_gpu_sync_operation *,
+                                                        const pyrowave_gpu_sync_operation *, const pyrowave_gpu_buffers *,
+                                                        const pyrowave_rate_control *)
+{
+	return PYROWAVE_ERROR_NOT_IMPLEMENTED;
+}
+
+pyrowave_result pyrowave_encoder_encode_cpu_synchronous(pyrowave_encoder encoder, const pyrowave_cpu_buffer *buffers,
+                                                        const pyrowave_rate_control *rate_control)
+{
+	if (!encoder || !buffers || !rate_control)
+		return PYROWAVE_ERROR_INVALID_ARGUMENT;
+	const Geometry &g = encoder->g;
+	const pyrowave_chroma_subsampling chroma =
+	    g.chroma444 ? PYROWAVE_CHROMA_SUBSAMPLING_444 : PYROWAVE_CHROMA_SUBSAMPLING_420;
+	// Validation order and rules of pyrowave_c.cpp:1058-1088.
+	const int num_planes = buffers->format == PYROWAVE_CPU_BUFFER_FORMAT_NV12 ? 2 : 3;
+	if (buffers->width != g.width || buffers->height != g.height)
+		return PYROWAVE_ERROR_INVALID_ARGUMENT;
+	if (chroma == PYROWAVE_CHROMA_SUBSAMPLING_420 && buffers->format == PYROWAVE_CPU_BUFFER_FORMAT_YUV444P)
+		return PYROWAVE_ERROR_INVALID_ARGUMENT;
+	if (chroma == PYROWAVE_CHROMA_SUBSAMPLING_444 && buffers->format != PYROWAVE_CPU_BUFFER_FORMAT_YUV444P)
+		return PYROWAVE_ERROR_INVALID_ARGUMENT;
+	if (buffers->format != PYROWAVE_CPU_BUFFER_FORMAT_NV12 && buffers->format != PYROWAVE_CPU_BUFFER_FORMAT_YUV420P &&
+	    buffers->format != PYROWAVE_CPU_BUFFER_FORMAT_YUV444P)
+		return PYROWAVE_ERROR_INVALID_ARGUMENT;
+	for (int p = 0; p < num_planes; p++)
+	{
+		int w, h;
+		plane_dims(chroma, g.width, g.height, p, w, h);
+		const size_t bpp = (num_planes == 2 && p == 1) ? 2 : 1;
+		if (buffers->row_stride_in_bytes[p] < size_t(w) * bpp)
+			return PYROWAVE_ERROR_INVALID_ARGUMENT;
+		if (buffers->row_stride_in_bytes[p] * size_t(h) > buffers->plane_size_in_bytes[p])
+			return PYROWAVE_ERROR_INVALID_ARGUMENT;
+		if (!buffers->data[p])
+			return PYROWAVE_ERROR_INVALID_ARGUMENT;
+	}
+	uint32_t tw, cap;
+	if (!pyrowave_encoder_opaque::budget_words(rate_control, tw, cap))
+		return PYROWAVE_ERROR_INVALID_ARGUMENT;
+
+	pyrowave_result r = encoder->allocate();
+	if (r != PYROWAVE_SUCCESS)
+		return r;
+	r = encoder->ensure_input_planes();
+	if (r != PYROWAVE_SUCCESS)
+		return r;
+	cudaStream_t s = encoder->device->stream;
+	PlaneInput in = {};
+	if (num_planes == 2)
+	{
+		// NV12: the interleaved CbCr plane is uploaded once and read with a
+		// 2-byte sample stride (Cb = byte 0, Cr = byte 1).
+		int w, h;
+		plane_dims(chroma, g.width, g.height, 0, w, h);
+		cudaMemcpy2DAsync(encoder->in_planes[0], encoder->in_pitch[0], buffers->data[0], buffers->row_stride_in_bytes[0],
+		                  size_t(w), size_t(h), cudaMemcpyHostToDevice, s);
+		plane_dims(chroma, g.width, g.height, 1, w, h);
+		cudaMemcpy2DAsync(encoder->in_planes[1], size_t(encoder->in_pitch[1]), buffers->data[1],
+		                  buffers->row_stride_in_bytes[1], size_t(w) * 2, size_t(h), cudaMemcpyHostToDevice, s);
+		in.data[0] = encoder->in_planes[0];
+		in.pitch[0] = encoder->in_pitch[0];
+		in.xstride[0] = 1;
+		in.data[1] = encoder->in_planes[1];
+		in.data[2] = encoder->in_planes[1] + 1;
+		in.pitch[1] = in.pitch[2] = encoder->in_pitch[1];
+		in.xstride[1] = in.xstride[2] = 2;
+	}
+	else
+	{
+		for (int p = 0; p < 3; p++)
+		{
+			int w, h;
+			plane_dims(chroma, g.width, g.height, p, w, h);
+			cudaMemcpy2DAsync(encoder->in_planes[p], encoder->in_pitch[p], buffers->data[p],
+			                  buffers->row_stride_in_bytes[p], size_t(w), size_t(h), cudaMemcpyHostToDevice, s);
+			in.data[p] = encoder->in_planes[p];
+			in.pitch[p] = encoder->in_pitch[p];
+			in.xstride[p] = 1;
+		}
+	}
+	r = encoder->enqueue(in, rate_control, s);
+	if (r != PYROWAVE_SUCCESS)
+		return r;
+	return encoder->queue_readback(s);
+}
+
+pyrowave_result pyrowave_encoder_compute_num_packets(pyrowave_encoder encoder, size_t packet_boundary, size_t *num_packets)
+{
+	if (!encoder || !num_packets)
+		return PYROWAVE_ERROR_INVALID_ARGUMENT;
+	if (!encoder->wait())
+		return PYROWAVE_ERROR_GENERIC;
+	const uint32_t *meta = encoder->h_meta;
+	size_t n = 0, in_packet = 8;
+	for (int i = 0; i < encoder->g.block_count_32x32; i++)
+	{
+		const size_t bytes = size_t(meta[2 * i + 1]) * 4;
+		if (!bytes)
+			continue;
+		if (in_packet + bytes > packet_boundary)
+		{
+			in_packet = 0;
+			n++;
+		}
+		in_packet += bytes;
+	}
+	if (in_packet)
+		n++;
+	*num_packets = n;
+	return PYROWAVE_SUCCESS;
+}
+
+pyrowave_result pyrowave_encoder_packetize(pyrowave_encoder encoder, pyrowave_packet *packets, size_t packet_boundary,
+                                           size_t *out_packets, void *bitstream, size_t size)
+{
+	if (!encoder || !out_packets || !bitstream || !packets)
+		return PYROWAVE_ERROR_INVALID_ARGUMENT;
+	if (!encoder->wait())
+		return PYROWAVE_ERROR_GENERIC;
+	if (encoder->h_total[0] != 0)
+		return PYROWAVE_ERROR_GENERIC; // device-side consistency check failed
+	// The device stream already holds header + blocks contiguously in block
+	// order, which is what the packet loop of pyrowave_encoder.cpp:1085-1109
+	// produces; only the packet boundaries are computed here.
+	const uint32_t *meta = encoder->h_meta;
+	size_t n = 0, in_packet = 0, packet_offset = 0, output_offset = 0;
+	if (size < 8)
+	{
+		*out_packets = 0;
+		return PYROWAVE_SUCCESS;
+	}
+	output_offset = 8;
+	in_packet = 8;
+	bool truncated = false;
+	for (int i = 0; i < encoder->g.block_count_32x32; i++)
+	{
+		const size_t bytes = size_t(meta[2 * i + 1]) * 4;
+		if (!bytes)
+			continue;
+		if (in_packet + bytes > packet_boundary)
+		{
+			packets[n].offset = packet_offset;
+			packets[n].size = in_packet;
+			n++;
+			in_packet = 0;
+			packet_offset = output_offset;
+		}
+		// An output buffer that is too small ends packetization early
+		// (metal/pyrowave_bitstream.cpp:367-368 of the reference).
+		if (output_offset + bytes > size)
+		{
+			truncated = true;
+			break;
+		}
+		output_offset += bytes;
+		in_packet += bytes;
+	}
+	if (!truncated && in_packet)
+	{
+		packets[n].offset = packet_offset;
+		packets[n].size = in_packet;
+		n++;
+	}
+	memcpy(bitstream, encoder->h_stream, output_offset);
+	*out_packets = n;
+	return PYROWAVE_SUCCESS;
+}
+
+void pyrowave_encoder_destroy(pyrowave_encoder encoder)
+{
+	if (!encoder)
+		return;
+	encoder->release();
+	delete encoder;
+}
+
+// --- decoder ---------------------------------------------------------------
+bool pyrowave_decoder_device_prefers_fragment_path(pyrowave_device) { return false; }
+
+pyrowave_result pyrowave_decoder_create(const pyrowave_decoder_create_info *info, pyrowave_decoder *decoder)
+{
+	if (!info || !decoder || !info->device)
+		return PYROWAVE_ERROR_INVALID_ARGUMENT;
+	if (info->width <= 0 || info->height <= 0)
+		return PYROWAVE_ERROR_INVALID_ARGUMENT;
+	if (info->chroma == PYROWAVE_CHROMA_SUBSAMPLING_420 && ((info->width & 1) || (info->height & 1)))
+		return PYROWAVE_ERROR_INVALID_ARGUMENT;
+	if (info->chroma != PYROWAVE_CHROMA_SUBSAMPLING_420 && info->chroma != PYROWAVE_CHROMA_SUBSAMPLING_444)
+		return PYROWAVE_ERROR_INVALID_ARGUMENT;
+	auto *dec = new (std::nothrow) pyrowave_decoder_opaque;
+	if (!dec)
+		return PYROWAVE_ERROR_OUT_OF_HOST_MEMORY;
+	dec->device = info->device;
+	if (!build_geometry(dec->g, dec->jobs, info->width, info->height,
+	                    info->chroma == PYROWAVE_CHROMA_SUBSAMPLING_444, 0))
+	{
+		delete dec;
+		return PYROWAVE_ERROR_INVALID_ARGUMENT;
+	}
+	dec->offsets.assign(size_t(dec->g.block_count_32x32), UINT32_MAX);
+	dec->clear();
+	*decoder = dec;
+	return PYROWAVE_SUCCESS;
+}
+
+void pyrowave_decoder_clear(pyrowave_decoder decoder)
+{
+	if (decoder)
+		decoder->clear();
+}
+
+pyrowave_result pyrowave_decoder_push_packet(pyrowave_decoder decoder, const void *data, size_t size)
+{
+	if (!decoder || (!data && size))
+		return PYROWAVE_ERROR_INVALID_ARGUMENT;
+	return decoder->push_packet(static_cast<const uint8_t *>(data), size) ? PYROWAVE_SUCCESS
+	                                                                      : PYROWAVE_ERROR_INVALID_ARGUMENT;
+}
+
+bool pyrowave_decoder_decode_is_ready(pyrowave_decoder decoder, bool allow_partial_frame)
+{
+	return decoder && decoder->decode_is_ready(allow_partial_frame);
+}
+
+pyrowave_result pyrowave_decoder_decode_gpu_buffer(pyrowave_decoder, const pyrowave_gpu_sync_operation *,
+                                                   const pyrowave_gpu_sync_operation *, const pyrowave_gpu_buffers *)
+{
+	return PYROWAVE_ERROR_NOT_IMPLEMENTED;
+}
+
+pyrowave_result pyrowave_decoder_decode_cpu_buffer_synchronous(pyrowave_decoder decoder, const pyrowave_cpu_buffer *buffers)
+{
+	if (!decoder || !buffers)
+		return PYROWAVE_ERROR_INVALID_ARGUMENT;
+	const Geometry &g = decoder->g;
+	const pyrowave_chroma_subsampling chroma =
+	    g.chroma444 ? PYROWAVE_CHROMA_SUBSAMPLING_444 : PYROWAVE_CHROMA_SUBSAMPLING_420;
+	// Validation of pyrowave_c.cpp:1345-1373.
+	if (buffers->width != g.width || buffers->height != g.height)
+		return PYROWAVE_ERROR_INVALID_ARGUMENT;
+	if (buffers->format == PYROWAVE_CPU_BUFFER_FORMAT_NV12)
+		return PYROWAVE_ERROR_INVALID_ARGUMENT;
+	if (chroma == PYROWAVE_CHROMA_SUBSAMPLING_420 && buffers->format == PYROWAVE_CPU_BUFFER_FORMAT_YUV444P)
+		return PYROWAVE_ERROR_INVALID_ARGUMENT;
+	if (chroma == PYROWAVE_CHROMA_SUBSAMPLING_444 && buffers->format != PYROWAVE_CPU_BUFFER_FORMAT_YUV444P)
+		return PYROWAVE_ERROR_INVALID_ARGUMENT;
+	if (buffers->format != PYROWAVE_CPU_BUFFER_FORMAT_YUV420P && buffers->format != PYROWAVE_CPU_BUFFER_FORMAT_YUV444P)
+		return PYROWAVE_ERROR_INVALID_ARGUMENT;
+	for (int p = 0; p < 3; p++)
+	{
+		int w, h;
+		plane_dims(chroma, g.width, g.height, p, w, h);
+		if (buffers->row_stride_in_bytes[p] < size_t(w))
+			return PYROWAVE_ERROR_INVALID_ARGUMENT;
+		if (buffers->row_stride_in_bytes[p] * size_t(h) > buffers->plane_size_in_bytes[p])
+			return PYROWAVE_ERROR_INVALID_ARGUMENT;
+		if (!buffers->data[p])
+			return PYROWAVE_ERROR_INVALID_ARGUMENT;
+	}
+	pyrowave_result r = decoder->allocate();
+	if (r != PYROWAVE_SUCCESS)
+		return r;
+	r = decoder->ensure_output_planes();
+	if (r != PYROWAVE_SUCCESS)
+		return r;
+	cudaStream_t s = decoder->device->stream;
+	PlaneOutput out = {};
+	for (int p = 0; p < 3; p++)
+	{
+		out.data[p] = decoder->out_planes[p];
+		out.pitch[p] = decoder->out_pitch[p];
+	}
+	r = decoder->decode_parsed(out, s);
+	if (r != PYROWAVE_SUCCESS)
+		return r;
+	for (int p = 0; p < 3; p++)
+	{
+		int w, h;
+		plane_dims(chroma, g.width, g.height, p, w, h);
+		cudaMemcpy2DAsync(buffers->data[p], buffers->row_stride_in_bytes[p], decoder->out_planes[p],
+		                  decoder->out_pitch[p], size_t(w), size_t(h), cudaMemcpyDeviceToHost, s);
+	}
+	if (cudaStreamSynchronize(s) != cudaSuccess)
+		return PYROWAVE_ERROR_GENERIC;
+	return PYROWAVE_SUCCESS;
+}
+
+void pyrowave_decoder_destroy(pyrowave_decoder decoder)
+{
+	if (!decoder)
+		return;
+	decoder->release();
+	delete decoder;
+}
+
+// --- CUDA extension ----------------------------------------------------------
+pyrowave_result pyrowave_cuda_encoder_set_precision(pyrowave_encoder encoder, uint32_t fp16_level_mask)
+{
+	if (!encoder || (fp16_level_mask & ~0x1fu))
+		return PYROWAVE_ERROR_INVALID_ARGUMENT;
+	if (encoder->allocated && fp16_level_mask != encoder->fp16_mask)
+		encoder->release();
+	encoder->fp16_mask = fp16_level_mask;
+	return PYROWAVE_SUCCESS;
+}
+
+pyrowave_result pyrowave_cuda_decoder_set_precision(pyrowave_decoder decoder, uint32_t fp16_level_mask)
+{
+	if (!decoder || (fp16_level_mask & ~0x1fu))
+		return PYROWAVE_ERROR_INVALID_ARGUMENT;
+	if (decoder->allocated && fp16_level_mask != decoder->fp16_mask)
+		decoder->release();
+	decoder->fp16_mask = fp16_level_mask;
+	return PYROWAVE_SUCCESS;
+}
+
+pyrowave_result pyrowave_cuda_encoder_get_layout(pyrowave_encoder encoder, pyrowave_cuda_layout *layout)
+{
+	if (!encoder)
+		return PYROWAVE_ERROR_INVALID_ARGUMENT;
+	return fill_layout(encoder->g, encoder->fp16_mask, layout);
+}
+
+pyrowave_result pyrowave_cuda_decoder_get_layout(pyrowave_decoder decoder, pyrowave_cuda_layout *layout)
+{
+	if (!decoder)
+		return PYROWAVE_ERROR_INVALID_ARGUMENT;
+	return fill_layout(decoder->g, decoder->fp16_mask, layout);
+}
+
+pyrowave_result pyrowave_cuda_encoder_encode(pyrowave_encoder encoder, const pyrowave_cuda_planes *planes,
+                                             const pyrowave_rate_control *rate_control, pyrowave_cuda_stream stream)
+{
+	if (!encoder || !planes || !rate_control)
+		return PYROWAVE_ERROR_INVALID_ARGUMENT;
+	pyrowave_result r = encoder->allocate();
+	if (r != PYROWAVE_SUCCESS)
+		return r;
+	const Geometry &g = encoder->g;
+	PlaneInput in = {};
+	for (int p = 0; p < 3; p++)
+	{
+		if (!planes->data[p] || planes->row_stride_in_bytes[p] < size_t(g.plane_width[p]) ||
+		    planes->row_stride_in_bytes[p] > 0x7fffffffu)
+			return PYROWAVE_ERROR_INVALID_ARGUMENT;
+		in.data[p] = static_cast<const uint8_t *>(planes->data[p]);
+		in.pitch[p] = int32_t(planes->row_stride_in_bytes[p]);
+		in.xstride[p] = 1;
+	}
+	return encoder->enqueue(in, rate_control, pick_stream(encoder->device, stream));
+}
+
+pyrowave_result pyrowave_cuda_encoder_get_device_bitstream(pyrowave_encoder encoder, const uint32_t **stream,
+                                                           const uint32_t **block_meta, size_t *capacity_words)
+{
+	if (!encoder || !encoder->has_device_frame)
+		return PYROWAVE_ERROR_GENERIC;
+	if (stream)
+		*stream = encoder->stream_buf;
+	if (block_meta)
+		*block_meta = encoder->block_meta;
+	if (capacity_words)
+		*capacity_words = encoder->stream_capacity;
+	return PYROWAVE_SUCCESS;
+}
+
+pyrowave_result pyrowave_cuda_encoder_get_size(pyrowave_encoder encoder, size_t *bytes)
+{
+	if (!encoder || !bytes || !encoder->has_device_frame)
+		return PYROWAVE_ERROR_INVALID_ARGUMENT;
+	uint32_t v[2] = {0, 0};
+	if (cudaMemcpy(v, &encoder->rc->error, 8, cudaMemcpyDeviceToHost) != cudaSuccess)
+		return PYROWAVE_ERROR_GENERIC;
+	if (v[0] != 0)
+		return PYROWAVE_ERROR_GENERIC;
+	*bytes = 8 + size_t(v[1]) * 4;
+	return PYROWAVE_SUCCESS;
+}
+
+pyrowave_result pyrowave_cuda_encoder_encode_pre_transformed(pyrowave_encoder encoder, const float *pyramid,
+                                                             const pyrowave_rate_control *rate_control,
+                                                             float quant_scale, pyrowave_cuda_stream stream)
+{
+	if (!encoder || !pyramid || !rate_control)
+		return PYROWAVE_ERROR_INVALID_ARGUMENT;
+	pyrowave_result r = encoder->allocate();
+	if (r != PYROWAVE_SUCCESS)
+		return r;
+	uint32_t target_words, capacity;
+	if (!pyrowave_encoder_opaque::budget_words(rate_control, target_words, capacity))
+		return PYROWAVE_ERROR_INVALID_ARGUMENT;
+	r = encoder->ensure_stream_capacity(capacity);
+	if (r != PYROWAVE_SUCCESS)
+		return r;
+	cudaStream_t s = pick_stream(encoder->device, stream);
+	Geometry g = encoder->g;
+	apply_quant_scale_override(g, quant_scale);
+	encoder->sequence_count = (encoder->sequence_count + 1) & 7u;
+	EncodeBuffers b = encoder->buffers();
+	cudaMemsetAsync(encoder->rc, 0, sizeof(RateControlState), s);
+	launch_pyramid_io(g, const_cast<float *>(pyramid), encoder->coef32, encoder->coef16, false, s);
+	launch_quant_pretransformed(g, b, s);
+	launch_resolve(g, b, target_words, encoder->sequence_count, s);
+	launch_pack(g, b, s);
+	if (cudaPeekAtLastError() != cudaSuccess)
+		return PYROWAVE_ERROR_GENERIC;
+	encoder->has_device_frame = true;
+	return encoder->queue_readback(s);
+}
+
+pyrowave_result pyrowave_cuda_encoder_read_wavelet(pyrowave_encoder encoder, float *pyramid, pyrowave_cuda_stream stream)
+{
+	if (!encoder || !pyramid || !encoder->allocated)
+		return PYROWAVE_ERROR_INVALID_ARGUMENT;
+	launch_pyramid_io(encoder->g, pyramid, encoder->coef32, encoder->coef16, true, pick_stream(encoder->device, stream));
+	return cudaPeekAtLastError() == cudaSuccess ? PYROWAVE_SUCCESS : PYROWAVE_ERROR_GENERIC;
+}
+
+pyrowave_result pyrowave_cuda_encoder_read_debug(pyrowave_encoder encoder, const pyrowave_cuda_encoder_debug *d)
+{
+	if (!encoder || !d || !encoder->allocated)
+		return PYROWAVE_ERROR_INVALID_ARGUMENT;
+	if (cudaDeviceSynchronize() != cudaSuccess)
+		return PYROWAVE_ERROR_GENERIC;
+	const Geometry &g = encoder->g;
+	const size_t n8 = size_t(g.block_count_8x8), n32 = size_t(g.block_count_32x32);
+	if (d->code_words)
+		cudaMemcpy(d->code_words, encoder->code_words, n8 * 4, cudaMemcpyDeviceToHost);
+	if (d->rd_cost)
+		cudaMemcpy(d->rd_cost, encoder->rd_cost, n32 * 32, cudaMemcpyDeviceToHost);
+	if (d->rd_bucket)
+		cudaMemcpy(d->rd_bucket, encoder->rd_bucket, n32 * 16, cudaMemcpyDeviceToHost);
+	if (d->rd_dist)
+		cudaMemcpy(d->rd_dist, encoder->rd_dist, n32 * 64, cudaMemcpyDeviceToHost);
+	if (d->histogram)
+		cudaMemcpy(d->histogram, encoder->rc->histogram, kHistSize * 4, cudaMemcpyDeviceToHost);
+	if (d->consumed)
+		cudaMemcpy(d->consumed, &encoder->rc->consumed, 4, cudaMemcpyDeviceToHost);
+	if (d->quant)
+		cudaMemcpy(d->quant, encoder->quant, n32 * 4, cudaMemcpyDeviceToHost);
+	if (d->block_meta)
+		cudaMemcpy(d->block_meta, encoder->block_meta, n32 * 8, cudaMemcpyDeviceToHost);
+	if (d->error_flags)
+		cudaMemcpy(d->error_flags, &encoder->rc->error, 4, cudaMemcpyDeviceToHost);
+	return cudaGetLastError() == cudaSuccess ? PYROWAVE_SUCCESS : PYROWAVE_ERROR_GENERIC;
+}
+
+pyrowave_result pyrowave_cuda_decoder_decode(pyrowave_decoder decoder, const pyrowave_cuda_planes *planes,
+                                             pyrowave_cuda_stream stream)
+{
+	if (!decoder || !planes)
+		return PYROWAVE_ERROR_INVALID_ARGUMENT;
+	pyrowave_result r = decoder->allocate();
+	if (r != PYROWAVE_SUCCESS)
+		return r;
+	PlaneOutput out = {};
+	for (int p = 0; p < 3; p++)
+	{
+		if (!planes->data[p] || planes->row_stride_in_bytes[p] < size_t(decoder->g.plane_width[p]) ||
+		    planes->row_stride_in_bytes[p] > 0x7fffffffu)
+			return PYROWAVE_ERROR_INVALID_ARGUMENT;
+		out.data[p] = static_cast<uint8_t *>(planes->data[p]);
+		out.pitch[p] = int32_t(planes->row_stride_in_bytes[p]);
+	}
+	return decoder->decode_parsed(out, pick_stream(decoder->device, stream));
+}
+
+pyrowave_result pyrowave_cuda_decoder_decode_blocks(pyrowave_decoder decoder, const uint32_t *block_meta,
+                                                    const uint32_t *words, size_t num_words,
+                                                    const pyrowave_cuda_planes *planes, pyrowave_cuda_stream stream)
+{
+	if (!decoder || !block_meta || !words || !planes || num_words > 0xffffffffu)
+		return PYROWAVE_ERROR_INVALID_ARGUMENT;
+	pyrowave_result r = decoder->allocate();
+	if (r != PYROWAVE_SUCCESS)
+		return r;
+	PlaneOutput out = {};
+	for (int p = 0; p < 3; p++)
+	{
+		if (!planes->data[p] || planes->row_stride_in_bytes[p] < size_t(decoder->g.plane_width[p]) ||
+		    planes->row_stride_in_bytes[p] > 0x7fffffffu)
+			return PYROWAVE_ERROR_INVALID_ARGUMENT;
+		out.data[p] = static_cast<uint8_t *>(planes->data[p]);
+		out.pitch[p] = int32_t(planes->row_stride_in_bytes[p]);
+	}
+	DecodeInput in = {};
+	in.offsets = nullptr;
+	in.block_meta = block_meta;
+	in.payload = words;
+	in.payload_words = uint32_t(num_words);
+	in.jobs = decoder->jobs_d;
+	in.coef32 = decoder->coef32;
+	in.coef16 = decoder->coef16;
+	decoder->run(in, out, pick_stream(decoder->device, stream), true);
+	return cudaPeekAtLastError() == cudaSuccess ? PYROWAVE_SUCCESS : PYROWAVE_ERROR_GENERIC;
+}
+
+pyrowave_result pyrowave_cuda_decoder_read_wavelet(pyrowave_decoder decoder, float *pyramid, pyrowave_cuda_stream stream)
+{
+	if (!decoder || !pyramid || !decoder->allocated)
+		return PYROWAVE_ERROR_INVALID_ARGUMENT;
+	launch_pyramid_io(decoder->g, pyramid, decoder->coef32, decoder->coef16, true, pick_stream(decoder->device, stream));
+	return cudaPeekAtLastError() == cudaSuccess ? PYROWAVE_SUCCESS : PYROWAVE_ERROR_GENERIC;
+}
+
+pyrowave_result pyrowave_cuda_decoder_decode_pyramid(pyrowave_decoder decoder, const float *pyramid,
+                                                     const pyrowave_cuda_planes *planes, pyrowave_cuda_stream stream)
+{
+	if (!decoder || !pyramid || !planes)
+		return PYROWAVE_ERROR_INVALID_ARGUMENT;
+	pyrowave_result r = decoder->allocate();
+	if (r != PYROWAVE_SUCCESS)
+		return r;
+	PlaneOutput out = {};
+	for (int p = 0; p < 3; p++)
+	{
+		if (!planes->data[p] || planes->row_stride_in_bytes[p] < size_t(decoder->g.plane_width[p]))
+			return PYROWAVE_ERROR_INVALID_ARGUMENT;
+		out.data[p] = static_cast<uint8_t *>(planes->data[p]);
+		out.pitch[p] = int32_t(planes->row_stride_in_bytes[p]);
+	}
+	cudaStream_t s = pick_stream(decoder->device, stream);
+	launch_pyramid_io(decoder->g, const_cast<float *>(pyramid), decoder->coef32, decoder->coef16, false, s);
+	DecodeInput in = {};
+	in.jobs = decoder->jobs_d;
+	in.coef32 = decoder->coef32;
+	in.coef16 = decoder->coef16;
+	decoder->run(in, out, s, false);
+	return cudaPeekAtLastError() == cudaSuccess ? PYROWAVE_SUCCESS : PYROWAVE_ERROR_GENERIC;
+}
+}

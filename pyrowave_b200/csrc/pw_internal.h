@@ -1,0 +1,156 @@
+// Internal definitions shared by the host library and the sm_100a kernels.
+//
+// Frame geometry follows the bitstream definition (bitstream.md:99-152 and the
+// block index order at :472-511 of the reference). Device layout chosen here:
+//   * every band is a row-major 2D array whose pitch and row count are padded to
+//     multiples of 32, so every 8x8 and 32x32 block is addressable without
+//     bounds checks; the forward transform writes zeros into the padding, which
+//     reproduces the reference quantiser's clamp-to-border sampling;
+//   * levels are stored in FP32 or FP16 (per-level mask), each in its own buffer;
+//   * the encoder emits the packetized bitstream directly: a 2-word sequence
+//     header followed by the coded 32x32 blocks in block index order, placed by
+//     a device prefix scan instead of the reference's atomic allocation.
+#pragma once
+
+#include <cstddef>
+#include <cstdint>
+
+#include <cuda_fp16.h>
+#include <cuda_runtime.h>
+
+namespace pw
+{
+constexpr int kLevels = 5;
+constexpr int kComponents = 3;
+constexpr int kAlignment = 32;
+constexpr int kMinImageSize = 128;
+constexpr int kBuckets = 128;
+constexpr int kSubdivisions = 16;
+constexpr int kHistSize = kBuckets * kSubdivisions;
+constexpr int kMaxBlockWords = 1024; // a 32x32 block can need at most ~640 words
+constexpr int kQPlanesOffset = 16;
+constexpr int kQuantScaleOffset = 20;
+constexpr int kMaxScaleExp = 4;
+
+// Magnitudes are clamped below 2^15 after scaling, keeping the statistics of an
+// 8x8 block within 16 entries (q = 0..14 plus "drop all"). Real 8-bit content
+// stays far below this (the reference's own table has 15 entries).
+constexpr float kMaxScaledMagnitude = 32767.0f;
+
+struct BandDesc
+{
+	int32_t present;          // transmitted band (LL only at the last level)
+	int64_t offset;           // element offset of the band in its level's storage buffer
+	int32_t block8_offset;    // first global 8x8 block index
+	int32_t block8_stride;    // 8x8 blocks per row
+	int32_t block32_offset;   // first global 32x32 block index
+	int32_t block32_stride;   // 32x32 blocks per row
+	float quant_resolution;   // 1 / decode_quant(encode_quant(1 / resolution)): quantiser scale
+	float rdo_scale;          // CSF distortion weight / 256
+	uint32_t quant_code;      // encode_quant(1 / resolution): the 32x32 header's quant code
+};
+
+struct LevelDesc
+{
+	int32_t width, height;    // band size at this level
+	int32_t pitch, rows;      // padded to multiples of 32
+	int32_t tiles_x, tiles_y; // 32x32 band tiles
+	int32_t blocks8_x, blocks8_y;
+	int32_t fp16;             // 1: coefficients of this level are stored as FP16
+};
+
+struct Geometry
+{
+	int32_t width, height, chroma444;
+	int32_t aligned_width, aligned_height;
+	int32_t block_count_8x8, block_count_32x32;
+	int32_t blocks_per_subdivision, subdivision_shift;
+	int32_t plane_width[3], plane_height[3];
+	LevelDesc level[kLevels];
+	BandDesc band[kComponents][kLevels][4];
+	int64_t storage_elems32, storage_elems16;
+};
+
+// Which band a 32x32 block (in block index order) belongs to: packed
+// level | comp << 3 | band << 5 | bx << 8 | by << 20.
+__host__ __device__ inline uint32_t pack_job(int level, int comp, int band, int bx, int by)
+{
+	return uint32_t(level) | (uint32_t(comp) << 3) | (uint32_t(band) << 5) | (uint32_t(bx) << 8) | (uint32_t(by) << 20);
+}
+__host__ __device__ inline void unpack_job(uint32_t j, int &level, int &comp, int &band, int &bx, int &by)
+{
+	level = int(j & 7u);
+	comp = int((j >> 3) & 3u);
+	band = int((j >> 5) & 3u);
+	bx = int((j >> 8) & 0xfffu);
+	by = int(j >> 20);
+}
+
+// Rate-control scratch, one per encoder instance (device memory).
+struct RateControlState
+{
+	uint32_t histogram[kHistSize]; // savings per (bucket, subdivision)
+	uint32_t consumed;             // words at quant 0
+	uint32_t error;                // nonzero when a consistency check failed
+	uint32_t total_words;          // coded words after rate control (blocks only)
+	uint32_t non_zero_blocks;
+	int32_t xstar;                 // first partially applied bucket*16+subdivision (-1 none)
+	uint32_t block_cut;            // ops of blocks >= this in the partial subdivision are not applied
+	uint32_t sequence;
+	uint32_t pad;
+};
+
+// Buffers the encode kernels read and write.
+struct EncodeBuffers
+{
+	float *coef32;
+	__half *coef16;
+	uint32_t *code_words;   // per 8x8: q=0 code word (plane codes | Q planes << 16 | scale << 20)
+	uint16_t *rd_cost;      // per 32x32 x 16: words when quantised by q
+	uint8_t *rd_bucket;     // per 32x32 x 16: bucket index of the step to q
+	float *rd_dist;         // per 32x32 x 16: summed distortion
+	RateControlState *rc;
+	int32_t *quant;         // per 32x32: chosen quant drop
+	uint32_t *block_meta;   // per 32x32: {offset_u32 relative to the first block word, num_words}
+	uint32_t *stream;       // packetized output: 2-word sequence header, then blocks
+	uint32_t stream_capacity_words;
+	const uint32_t *jobs;   // per 32x32: pack_job(...)
+};
+
+struct PlaneInput
+{
+	const uint8_t *data[3];
+	int32_t pitch[3];   // bytes between rows
+	int32_t xstride[3]; // bytes between samples (2 for the interleaved CbCr plane of NV12)
+};
+
+struct PlaneOutput
+{
+	uint8_t *data[3];
+	int32_t pitch[3];
+};
+
+struct DecodeInput
+{
+	const uint32_t *offsets;    // per 32x32 block, UINT32_MAX = missing (reference format), or nullptr
+	const uint32_t *block_meta; // alternatively {offset, num_words} pairs; num_words == 0 = missing
+	const uint32_t *payload;    // concatenated block words
+	uint32_t payload_words;
+	const uint32_t *jobs;
+	float *coef32;
+	__half *coef16;
+};
+
+// Host-side kernel launchers (implemented in the .cu files).
+void launch_dwt_forward_level(const Geometry &g, int level, const PlaneInput &in, const EncodeBuffers &buf,
+                              bool fused_quant, cudaStream_t stream);
+void launch_quant_pretransformed(const Geometry &g, const EncodeBuffers &buf, cudaStream_t stream);
+void launch_resolve(const Geometry &g, const EncodeBuffers &buf, uint32_t target_words, uint32_t sequence,
+                    cudaStream_t stream);
+void launch_pack(const Geometry &g, const EncodeBuffers &buf, cudaStream_t stream);
+void launch_dequant(const Geometry &g, const DecodeInput &in, cudaStream_t stream);
+void launch_idwt_level(const Geometry &g, int level, const DecodeInput &in, const PlaneOutput &out,
+                       cudaStream_t stream);
+void launch_pyramid_io(const Geometry &g, float *canonical, float *coef32, __half *coef16, bool to_canonical,
+                       cudaStream_t stream);
+} // namespace pw
