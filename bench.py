@@ -1,0 +1,474 @@
+#!/usr/bin/env python3
+"""PyroWave B200 benchmark: microseconds per frame, encode + decode, 1080p 4:2:0 at 400000 bytes.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference] [--config 1080p|4k|4k444|720p]
+
+One step = encode one frame and decode it again, on one GPU. Inputs are 16
+seeded synthetic frames (gradient + band-limited noise + flat rectangles, the
+generator in pyrowave_b200/synth.py) that stand in for the reference's private
+game clips.
+
+value : device-resident encode + decode (input planes already in HBM, decode
+        from the encoder's device bitstream), timed per step with CUDA events on
+        the library's stream; L2 is flushed (a 256 MiB write) between steps.
+e2e   : the same frames through the reference-facing C API with host buffers:
+        pyrowave_encoder_encode_cpu_synchronous (H2D inside), compute_num_packets
+        + packetize (D2H), pyrowave_decoder_push_packet (host parse) and
+        pyrowave_decoder_decode_cpu_buffer_synchronous (H2D payload, D2H planes).
+Multi-GPU: one process per GPU (torchrun), independent replicas ("scaling":
+"weak"): each rank codes its own frames; time = max over ranks.
+--impl reference: the reference algorithm's CPU restatement (oracle/) on all
+host cores, same workload and metric (the reference's own Vulkan path has no
+device it can run on here).
+"""
+from __future__ import annotations
+
+import argparse
+import concurrent.futures
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+CONFIGS = {
+    "1080p": dict(width=1920, height=1080, chroma444=False, budget=400000, seeds=list(range(1, 17)), rects=40, lines=0),
+    "4k": dict(width=3840, height=2160, chroma444=False, budget=1200000, seeds=list(range(1, 17)), rects=40, lines=0),
+    "4k444": dict(width=3840, height=2160, chroma444=True, budget=1200000, seeds=list(range(1, 5)), rects=200, lines=40),
+    "720p": dict(width=1280, height=720, chroma444=False, budget=150000, seeds=[0], rects=40, lines=0),
+}
+
+KERNELS_PER_STEP = 13  # 5 forward levels, resolve, pack, dequant, 5 inverse levels
+
+
+def dist_info():
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return ws, rank, local
+
+
+def make_frames(cfg):
+    from pyrowave_b200 import synth
+
+    return [synth.synth_frame(cfg["width"], cfg["height"], cfg["chroma444"], s, cfg["rects"], cfg["lines"])
+            for s in cfg["seeds"]]
+
+
+def algorithmic_bytes(cfg, fp16_mask):
+    """Minimal bytes per frame of each kernel: every input byte read once, every output byte written once."""
+    w, h, c444 = cfg["width"], cfg["height"], cfg["chroma444"]
+    aw = max((w + 31) // 32 * 32, 128)
+    ah = max((h + 31) // 32 * 32, 128)
+    planes = [(w, h)] + ([(w, h)] * 2 if c444 else [(w // 2, h // 2)] * 2)
+
+    def band_bytes(level):
+        return ((aw // 2) >> level) * ((ah // 2) >> level) * (2 if (fp16_mask >> level) & 1 else 4)
+
+    out = {}
+    transmitted = 0
+    for level in range(5):
+        fin = fout = 0
+        for c in range(3):
+            first = 0 if (c == 0 or c444) else 1
+            if level < first:
+                continue
+            src = planes[c][0] * planes[c][1] if level == first else band_bytes(level - 1)
+            fin += src + 4 * band_bytes(level)            # forward: read input, write LL, HL, LH, HH
+            fout += 4 * band_bytes(level) + src           # inverse: read 4 bands, write LL(level-1) or the plane
+            transmitted += (4 if level == 4 else 3) * band_bytes(level)
+        out[f"dwt{level}"] = fin
+        out[f"idwt{level}"] = fout
+    blocks8 = 0
+    for level in range(5):
+        bw, bh = (aw // 2) >> level, (ah // 2) >> level
+        ncomp = 3 if (level > 0 or c444) else 1
+        blocks8 += ((bw + 7) // 8) * ((bh + 7) // 8) * (4 if level == 4 else 3) * ncomp
+    out["pack"] = transmitted + 4 * blocks8 + cfg["budget"]
+    out["dequant"] = cfg["budget"] + transmitted
+    # The DWT stage as a whole: 8-bit planes read once, transmitted coefficients written once.
+    out["dwt_stage"] = sum(x * y for x, y in planes) + transmitted
+    return out
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled every 200 ms."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+              "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+              "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index: int):
+        self.gpu_index = gpu_index
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.gpu_index), f"--query-gpu={self.FIELDS}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except Exception:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        time.sleep(0.3)
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in self.lines:
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                mx = float(parts[2])
+            except ValueError:
+                continue
+            for n, v in zip(names, parts[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(n)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": mx, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def measured_peak():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        with open(p) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+# ---------------------------------------------------------------------------
+def run_ours(args, cfg, ws, rank, local):
+    import torch
+
+    from pyrowave_b200 import capi
+
+    torch.cuda.set_device(local)
+    if ws > 1:
+        import torch.distributed as dist
+        from datetime import timedelta
+
+        dist.init_process_group("nccl", timeout=timedelta(seconds=120), device_id=torch.device("cuda", local))
+    frames = make_frames(cfg)
+    w, h, c444, budget = cfg["width"], cfg["height"], cfg["chroma444"], cfg["budget"]
+    chroma = capi.CHROMA_444 if c444 else capi.CHROMA_420
+
+    dev = capi.Device()
+    enc = capi.Encoder(dev, w, h, chroma, args.fp16_mask)
+    dec = capi.Decoder(dev, w, h, chroma, args.fp16_mask)
+    stream = torch.cuda.Stream()
+    sid = stream.cuda_stream
+
+    d_frames = [[torch.from_numpy(p).cuda() for p in f] for f in frames]
+    d_out = [torch.empty(p.shape, dtype=torch.uint8, device="cuda") for p in frames[0]]
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
+    torch.cuda.synchronize()
+
+    def step(i):
+        f = d_frames[i % len(d_frames)]
+        enc.encode_device([p.data_ptr() for p in f], [p.stride(0) for p in f], budget, sid)
+        s, m, cap = enc.device_bitstream()
+        dec.decode_blocks(m, s + 8, cap - 2, [p.data_ptr() for p in d_out], [p.stride(0) for p in d_out], sid)
+
+    for i in range(args.warmup):
+        step(i)
+    torch.cuda.synchronize()
+    # Sanity: the last warm-up frame decodes to a sensible picture.
+    size = enc.size()
+    assert 8 < size <= budget, size
+
+    dev.set_stage_timing(True)
+    dev.report_performance_stats(reset=True)
+    sampler = ClockSampler(local)
+    if ws > 1:
+        torch.distributed.barrier()
+    torch.cuda.synchronize()
+    sampler.start()
+    starts = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+    ends = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+    for i in range(args.steps):
+        with torch.cuda.stream(stream):
+            flush.fill_(i & 0xFF)  # evict the previous frame from the 126 MB L2
+            starts[i].record(stream)
+        step(args.warmup + i)
+        with torch.cuda.stream(stream):
+            ends[i].record(stream)
+    torch.cuda.synchronize()
+    if ws > 1:
+        torch.distributed.barrier()
+    clocks = sampler.stop()
+    step_ms = [s.elapsed_time(e) for s, e in zip(starts, ends)]
+    total_ms = float(sum(step_ms))
+    stage_lines = dev.report_performance_stats(reset=True)
+    dev.set_stage_timing(False)
+    stages = {}
+    for line in stage_lines:
+        tag, rest = line.split(":", 1)
+        stages[tag.strip()] = float(rest.split("ms")[0])
+
+    # Same timed loop without stage events, to report their overhead.
+    torch.cuda.synchronize()
+    plain = []
+    for i in range(args.steps):
+        with torch.cuda.stream(stream):
+            flush.fill_(i & 0xFF)
+            starts[i].record(stream)
+        step(i)
+        with torch.cuda.stream(stream):
+            ends[i].record(stream)
+    torch.cuda.synchronize()
+    plain_ms = float(sum(s.elapsed_time(e) for s, e in zip(starts, ends)))
+
+    if ws > 1:
+        t = torch.tensor([total_ms, plain_ms], device="cuda")
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+        total_ms, plain_ms = float(t[0]), float(t[1])
+
+    frames_total = args.steps * ws
+    us_per_frame = total_ms * 1e3 / frames_total
+
+    # Roofline of the dominant kernel.
+    alg = algorithmic_bytes(cfg, args.fp16_mask)
+    peak, peak_kind = measured_peak()
+    kernel_stages = {k: v for k, v in stages.items() if k in alg}
+    dom = max(kernel_stages, key=kernel_stages.get) if kernel_stages else None
+    roofline = None
+    if dom:
+        ms = kernel_stages[dom]
+        achieved = alg[dom] / (ms * 1e-3) / 1e9
+        roofline = {"bound": "hbm", "kernel": dom, "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
+                    "frac": round(achieved / peak, 4), "traffic": _ncu_traffic(dom, cfg), "peak_source": peak_kind,
+                    "algorithmic_bytes": alg[dom], "avg_launch_us": round(ms * 1e3, 2)}
+    dwt_ms = sum(v for k, v in stages.items() if k.startswith("dwt"))
+    dwt_stage = {"us": round(dwt_ms * 1e3, 2), "algorithmic_bytes": alg["dwt_stage"],
+                 "achieved_gbs": round(alg["dwt_stage"] / (dwt_ms * 1e-3) / 1e9, 1) if dwt_ms else None}
+    if dwt_ms:
+        dwt_stage["frac_of_peak"] = round(dwt_stage["achieved_gbs"] / peak, 4)
+
+    e2e = run_e2e(args, cfg, frames, dev) if rank == 0 or ws > 1 else None
+    if ws > 1:
+        t = torch.tensor([e2e["total_s"]], device="cuda", dtype=torch.float64)
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+        e2e["total_s"] = float(t[0])
+    cpu = None
+    if rank == 0 and ws == 1 and not args.no_cpu_baseline:
+        cpu = cpu_baseline(cfg, frames, args.cpu_seconds)
+
+    if rank == 0:
+        line = {
+            "metric": f"us/frame enc+dec {cfg['width']}x{cfg['height']} {'4:4:4' if c444 else '4:2:0'} @ {budget} B",
+            "value": round(us_per_frame, 3),
+            "unit": "us/frame",
+            "n_gpus": ws,
+            "steps": args.steps,
+            "warmup": args.warmup,
+            "ms_per_step": round(total_ms / args.steps, 4),
+            "higher_is_better": False,
+            "scaling": "weak",
+            "vs_baseline": None,
+            "dtype": "f32" if args.fp16_mask == 0 else f"f32 (fp16 storage mask {args.fp16_mask:#x})",
+            "data": "synthetic (seeded gradient + band-limited noise + rectangles, 16 frames)",
+            "config": {"workload": f"encode+decode {cfg['width']}x{cfg['height']} "
+                                   f"{'4:4:4' if c444 else '4:2:0'} 8-bit, {budget}-byte budget",
+                       "frames": len(frames), "budget_bytes": budget, "fp16_level_mask": args.fp16_mask,
+                       "l2": "flushed between steps (256 MiB write)", "parallelism": f"replicas x{ws}"},
+            "e2e": {"value": round(e2e["total_s"] * 1e6 / (e2e["frames"] * ws), 2), "unit": "us/frame",
+                    "h2d_bytes_per_step": e2e["h2d"], "d2h_bytes_per_step": e2e["d2h"]},
+            "gpu_launches": KERNELS_PER_STEP * args.steps,
+            "roofline": roofline,
+            "dwt_stage": dwt_stage,
+            "stages_us": {k: round(v * 1e3, 2) for k, v in stages.items()},
+            "stage_event_overhead_us": round((total_ms - plain_ms) * 1e3 / args.steps, 2),
+            "value_without_stage_events": round(plain_ms * 1e3 / frames_total, 3),
+            "bytes_per_frame": size,
+            "clocks": clocks,
+            "cpu_baseline": cpu,
+        }
+        print(json.dumps(line), flush=True)
+    if ws > 1:
+        torch.distributed.barrier()
+        torch.distributed.destroy_process_group()
+
+
+def _ncu_traffic(kernel, cfg):
+    """DRAM bytes per launch of `kernel` from the committed ncu summary, if present."""
+    p = os.path.join(ROOT, "profiles", "ncu_traffic.json")
+    try:
+        with open(p) as f:
+            d = json.load(f)
+        key = f"{cfg['width']}x{cfg['height']}{'_444' if cfg['chroma444'] else ''}:{kernel}"
+        return d.get(key)
+    except Exception:
+        return None
+
+
+def run_e2e(args, cfg, frames, dev):
+    """Encode + decode through the C API with host (pinned) buffers."""
+    import torch
+
+    from pyrowave_b200 import capi
+
+    w, h, c444, budget = cfg["width"], cfg["height"], cfg["chroma444"], cfg["budget"]
+    chroma = capi.CHROMA_444 if c444 else capi.CHROMA_420
+    enc = capi.Encoder(dev, w, h, chroma, args.fp16_mask)
+    dec = capi.Decoder(dev, w, h, chroma, args.fp16_mask)
+    pinned = [[torch.from_numpy(p).pin_memory().numpy() for p in f] for f in frames]
+    out = [torch.empty(p.shape, dtype=torch.uint8).pin_memory().numpy() for p in frames[0]]
+    bitstream = torch.empty(budget, dtype=torch.uint8).pin_memory().numpy()
+    boundary = 8192
+
+    def step(i):
+        f = pinned[i % len(pinned)]
+        capi.check(enc.encode_cpu(f, budget), "encode_cpu_synchronous")
+        n = enc.compute_num_packets(boundary)
+        packets = (capi.Packet * max(n, 1))()
+        got = capi.c_size_t()
+        capi.check(enc.L.pyrowave_encoder_packetize(enc.h, packets, boundary, capi.ctypes.byref(got),
+                                                    capi.ctypes.c_void_p(bitstream.ctypes.data), budget), "packetize")
+        total = 0
+        for k in range(got.value):
+            off, sz = packets[k].offset, packets[k].size
+            capi.check(dec.push_packet(bitstream[off:off + sz]), "push_packet")
+            total += sz
+        code, _ = dec.decode_cpu(out)
+        capi.check(code, "decode_cpu_buffer_synchronous")
+        return total
+
+    for i in range(max(args.warmup, 3)):
+        step(i)
+    n = max(args.steps, 5)
+    t0 = time.perf_counter()
+    total_bytes = 0
+    for i in range(n):
+        total_bytes += step(i)
+    t1 = time.perf_counter()
+    planes_bytes = sum(p.nbytes for p in frames[0])
+    blocks32 = enc.layout().block_count_32x32
+    avg_stream = total_bytes // n
+    return {"total_s": t1 - t0, "frames": n,
+            "h2d": planes_bytes + avg_stream + 4 * blocks32,
+            "d2h": planes_bytes + budget + 8 * blocks32 + 8}
+
+
+def cpu_baseline(cfg, frames, seconds):
+    """The oracle (the reference algorithm restated in C++) on all host cores."""
+    import oracle as O
+
+    cores = os.cpu_count() or 1
+    w, h, c444, budget = cfg["width"], cfg["height"], cfg["chroma444"], cfg["budget"]
+
+    def one(f):
+        o = O.Oracle(w, h, c444)
+        o.encode(f, budget, O.MODE_F32)
+        stream, packets = o.packetize(8192, budget + 64)
+        p = o.parser()
+        for off, sz in packets:
+            p.push(stream[off:off + sz].tobytes())
+        offs, payload = p.get()
+        o.idwt(o.dequant(offs, payload, O.MODE_F32), O.MODE_F32)
+
+    done = 0
+    t0 = time.perf_counter()
+    with concurrent.futures.ThreadPoolExecutor(max_workers=cores) as ex:
+        while time.perf_counter() - t0 < seconds:
+            list(ex.map(one, [frames[(done + k) % len(frames)] for k in range(cores)]))
+            done += cores
+    dt = time.perf_counter() - t0
+    return {"value": round(dt * 1e6 / done, 1), "unit": "us/frame", "cores": cores, "kind": "port",
+            "sample": f"{done} frames encoded+decoded on {cores} threads in {dt:.1f} s (oracle restatement, FP32)"}
+
+
+def run_reference(args, cfg, ws, rank):
+    if rank != 0:
+        return
+    frames = make_frames(cfg)
+    cores = os.cpu_count() or 1
+    import oracle as O
+
+    w, h, c444, budget = cfg["width"], cfg["height"], cfg["chroma444"], cfg["budget"]
+
+    def one(f):
+        o = O.Oracle(w, h, c444)
+        o.encode(f, budget, O.MODE_REF16)
+        stream, packets = o.packetize(8192, budget + 64)
+        p = o.parser()
+        for off, sz in packets:
+            p.push(stream[off:off + sz].tobytes())
+        offs, payload = p.get()
+        o.idwt(o.dequant(offs, payload, O.MODE_REF16), O.MODE_REF16)
+
+    per_step = cores  # one frame per host thread per step
+    with concurrent.futures.ThreadPoolExecutor(max_workers=cores) as ex:
+        for i in range(args.warmup):
+            list(ex.map(one, [frames[(i * per_step + k) % len(frames)] for k in range(per_step)]))
+        t0 = time.perf_counter()
+        for i in range(args.steps):
+            list(ex.map(one, [frames[(i * per_step + k) % len(frames)] for k in range(per_step)]))
+        dt = time.perf_counter() - t0
+    us = dt * 1e6 / (args.steps * per_step)
+    line = {
+        "impl": "reference",
+        "metric": f"us/frame enc+dec {cfg['width']}x{cfg['height']} {'4:4:4' if c444 else '4:2:0'} @ {budget} B",
+        "value": round(us, 1), "unit": "us/frame", "n_gpus": ws, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": round(dt * 1e3 / args.steps, 3), "higher_is_better": False, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32 (fp16 staging, the reference's default precision)",
+        "data": "synthetic (seeded gradient + band-limited noise + rectangles)",
+        "config": {"workload": f"encode+decode {cfg['width']}x{cfg['height']} {'4:4:4' if c444 else '4:2:0'} 8-bit, "
+                               f"{budget}-byte budget", "frames": len(frames)},
+        "cpu_baseline": {"value": round(us, 1), "unit": "us/frame", "cores": cores, "kind": "port",
+                         "sample": f"{args.steps * per_step} frames, {per_step} per step on {cores} threads "
+                                   "(the reference's Vulkan path needs a graphics stack: unavailable on this box)"},
+        "e2e": {"value": round(us, 1), "unit": "us/frame", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=200)
+    ap.add_argument("--warmup", type=int, default=10)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--config", default="1080p", choices=sorted(CONFIGS))
+    ap.add_argument("--fp16-mask", type=lambda s: int(s, 0), default=0)
+    ap.add_argument("--cpu-seconds", type=float, default=10.0)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    if args.warmup < 3:
+        args.warmup = 3
+    ws, rank, local = dist_info()
+    cfg = CONFIGS[args.config]
+    if args.impl == "reference":
+        if args.steps > 50:
+            args.steps = 20  # each reference step is a full frame per host core
+        run_reference(args, cfg, ws, rank)
+        return
+    run_ours(args, cfg, ws, rank, local)
+
+
+if __name__ == "__main__":
+    main()

@@ -40,6 +40,12 @@ typedef struct pyrowave_cuda_layout
 	uint32_t fp16_level_mask;  /* bit L set: level L coefficients stored as FP16 */
 } pyrowave_cuda_layout;
 
+/* Per-kernel GPU timing with CUDA events recorded on the launching stream
+ * ("dwt0".."dwt4", "resolve", "pack", "dequant", "idwt4".."idwt0"), reported
+ * through pyrowave_device_report_performance_stats. Off by default (also
+ * enabled by the environment variable PYROWAVE_STAGE_TIMING=1). */
+PYROWAVE_PUBLIC_API pyrowave_result pyrowave_cuda_device_set_stage_timing(pyrowave_device device, bool enable);
+
 /* Coefficient storage precision per decomposition level. Default 0 (FP32 at
  * every level); 0x3 matches the reference's default precision layout (FP16 for
  * levels 0-1). Must be called before the first encode / decode. */

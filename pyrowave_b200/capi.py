@@ -47,7 +47,7 @@ API_SYMBOLS = [
     "pyrowave_decoder_push_packet", "pyrowave_decoder_decode_is_ready", "pyrowave_decoder_decode_gpu_buffer",
     "pyrowave_decoder_decode_cpu_buffer_synchronous", "pyrowave_decoder_destroy",
     # CUDA extension
-    "pyrowave_cuda_encoder_set_precision", "pyrowave_cuda_decoder_set_precision", "pyrowave_cuda_encoder_get_layout",
+    "pyrowave_cuda_device_set_stage_timing", "pyrowave_cuda_encoder_set_precision", "pyrowave_cuda_decoder_set_precision", "pyrowave_cuda_encoder_get_layout",
     "pyrowave_cuda_decoder_get_layout", "pyrowave_cuda_encoder_encode", "pyrowave_cuda_encoder_get_device_bitstream",
     "pyrowave_cuda_encoder_get_size", "pyrowave_cuda_encoder_encode_pre_transformed",
     "pyrowave_cuda_encoder_read_wavelet", "pyrowave_cuda_encoder_read_debug", "pyrowave_cuda_decoder_decode",
@@ -145,6 +145,7 @@ def lib():
     L.pyrowave_decoder_decode_is_ready.restype = c_bool
     L.pyrowave_decoder_decode_cpu_buffer_synchronous.argtypes = [c_void_p, POINTER(CpuBuffer)]
     L.pyrowave_decoder_decode_gpu_buffer.argtypes = [c_void_p, c_void_p, c_void_p, c_void_p]
+    L.pyrowave_cuda_device_set_stage_timing.argtypes = [c_void_p, c_bool]
     L.pyrowave_cuda_encoder_set_precision.argtypes = [c_void_p, c_uint32]
     L.pyrowave_cuda_decoder_set_precision.argtypes = [c_void_p, c_uint32]
     L.pyrowave_cuda_encoder_get_layout.argtypes = [c_void_p, POINTER(CudaLayout)]
@@ -163,9 +164,7 @@ def lib():
     L.pyrowave_cuda_decoder_read_wavelet.argtypes = [c_void_p, c_void_p, c_void_p]
     L.pyrowave_cuda_decoder_decode_pyramid.argtypes = [c_void_p, c_void_p, POINTER(CudaPlanes), c_void_p]
     for name in API_SYMBOLS:
-        fn = getattr(L, name)
-        if fn.restype is ctypes.c_int and name not in ("pyrowave_get_api_version",):
-            fn.restype = c_int
+        getattr(L, name)  # every declared entry point must resolve
     _lib = L
     return L
 
@@ -202,6 +201,9 @@ class Device:
 
     def __del__(self):
         self.close()
+
+    def set_stage_timing(self, enable: bool):
+        check(self.L.pyrowave_cuda_device_set_stage_timing(self.h, enable), "set_stage_timing")
 
     def report_performance_stats(self, reset: bool = True):
         out = []

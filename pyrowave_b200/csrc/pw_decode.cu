@@ -32,8 +32,9 @@ __device__ __forceinline__ void store_coef(float *c32, __half *c16, bool fp16, i
 
 // One 32x32 block per 128-thread CTA; thread = one 4x2 sub-block (the
 // reference's mapping, wavelet_dequant.comp:222-238).
-__global__ void __launch_bounds__(128) dequant_kernel(Geometry g, DecodeInput in)
+__global__ void __launch_bounds__(128) dequant_kernel(const Geometry *__restrict__ gp, DecodeInput in)
 {
+	const Geometry &g = *gp;
 	__shared__ uint32_t s_plane_off[16];
 	__shared__ uint32_t s_sign_base;
 	__shared__ uint32_t s_sig[4];
@@ -183,8 +184,9 @@ struct IdwtShared
 };
 
 // One inverse level for a 64x64 output tile (32x32 band tile) of one component.
-__global__ void __launch_bounds__(kIdwtThreads) idwt_kernel(Geometry g, int level, DecodeInput in, PlaneOutput out)
+__global__ void __launch_bounds__(kIdwtThreads) idwt_kernel(const Geometry *__restrict__ gp, int level, DecodeInput in, PlaneOutput out)
 {
+	const Geometry &g = *gp;
 	__shared__ IdwtShared sh;
 	const int comp = (level == 0 && !g.chroma444) ? 0 : int(blockIdx.y);
 	const LevelDesc &L = g.level[level];
@@ -209,15 +211,91 @@ __global__ void __launch_bounds__(kIdwtThreads) idwt_kernel(Geometry g, int leve
 	__syncthreads();
 
 	const bool f16 = L.fp16 != 0;
-	for (int k = threadIdx.x; k < 4 * kBandTile * kBandTile; k += kIdwtThreads)
+	const int64_t boff[4] = {g.band[comp][level][0].offset, g.band[comp][level][1].offset,
+	                         g.band[comp][level][2].offset, g.band[comp][level][3].offset};
+	// Interior tiles read every band sample at its own position: rows of 40
+	// samples from 4 before the tile (16-byte aligned), 10 vectors per row, all
+	// loads in flight at once. Edge tiles use the mirrored index tables.
+	const int bx0 = tx * 32 - 2, by0 = ty * 32 - 2;
+	const bool interior = bx0 - 2 >= 0 && by0 >= 0 && bx0 + 38 <= nx && by0 + kBandTile <= ny;
+	if (interior)
 	{
-		const int b = k / (kBandTile * kBandTile);
-		const int r = k - b * kBandTile * kBandTile;
-		const int i = r / kBandTile, j = r - i * kBandTile;
-		const int yy = (b >> 1) ? sh.yh[i] : sh.yl[i];
-		const int xx = (b & 1) ? sh.xh[j] : sh.xl[j];
-		const BandDesc &B = g.band[comp][level][b];
-		sh.band[b][i][j] = load_coef(in.coef32, in.coef16, f16, B.offset + int64_t(yy) * L.pitch + xx);
+		constexpr int kVecPerRow = 10;
+		constexpr int kVecs = 4 * kBandTile * kVecPerRow; // 1440
+		constexpr int kIters = (kVecs + kIdwtThreads - 1) / kIdwtThreads;
+		float4 v[kIters];
+#pragma unroll
+		for (int u = 0; u < kIters; u++)
+		{
+			const int k = threadIdx.x + u * kIdwtThreads;
+			const int b = k / (kBandTile * kVecPerRow);
+			const int r = k - b * kBandTile * kVecPerRow;
+			const int i = r / kVecPerRow, j = r - i * kVecPerRow;
+			if (k >= kVecs)
+			{
+				v[u] = make_float4(0.f, 0.f, 0.f, 0.f);
+				continue;
+			}
+			const int64_t idx = boff[b] + int64_t(by0 + i) * L.pitch + (bx0 - 2) + 4 * j;
+			if (f16)
+			{
+				uint2 hv = __ldg(reinterpret_cast<const uint2 *>(in.coef16 + idx));
+				float2 a = __half22float2(*reinterpret_cast<__half2 *>(&hv.x));
+				float2 c = __half22float2(*reinterpret_cast<__half2 *>(&hv.y));
+				v[u] = make_float4(a.x, a.y, c.x, c.y);
+			}
+			else
+				v[u] = __ldg(reinterpret_cast<const float4 *>(in.coef32 + idx));
+		}
+#pragma unroll
+		for (int u = 0; u < kIters; u++)
+		{
+			const int k = threadIdx.x + u * kIdwtThreads;
+			if (k >= kVecs)
+				continue;
+			const int b = k / (kBandTile * kVecPerRow);
+			const int r = k - b * kBandTile * kVecPerRow;
+			const int i = r / kVecPerRow, j = r - i * kVecPerRow;
+			const float vals[4] = {v[u].x, v[u].y, v[u].z, v[u].w};
+#pragma unroll
+			for (int e = 0; e < 4; e++)
+			{
+				const int col = 4 * j + e - 2;
+				if (col >= 0 && col < kBandTile)
+					sh.band[b][i][col] = vals[e];
+			}
+		}
+	}
+	else
+	{
+		constexpr int kN = 4 * kBandTile * kBandTile;
+		for (int base = threadIdx.x; base < kN; base += kIdwtThreads * 8)
+		{
+			float v[8];
+#pragma unroll
+			for (int u = 0; u < 8; u++)
+			{
+				const int k = base + u * kIdwtThreads;
+				const int b = k / (kBandTile * kBandTile);
+				const int r = k - b * kBandTile * kBandTile;
+				const int i = r / kBandTile, j = r - i * kBandTile;
+				const int yy = (b >> 1) ? sh.yh[i] : sh.yl[i];
+				const int xx = (b & 1) ? sh.xh[j] : sh.xl[j];
+				v[u] = k < kN ? load_coef(in.coef32, in.coef16, f16, boff[b & 3] + int64_t(yy) * L.pitch + xx) : 0.0f;
+			}
+#pragma unroll
+			for (int u = 0; u < 8; u++)
+			{
+				const int k = base + u * kIdwtThreads;
+				if (k < kN)
+				{
+					const int b = k / (kBandTile * kBandTile);
+					const int r = k - b * kBandTile * kBandTile;
+					const int i = r / kBandTile, j = r - i * kBandTile;
+					sh.band[b][i][j] = v[u];
+				}
+			}
+		}
 	}
 	__syncthreads();
 
@@ -260,19 +338,28 @@ __global__ void __launch_bounds__(kIdwtThreads) idwt_kernel(Geometry g, int leve
 		if (final_level)
 		{
 			const int pw = g.plane_width[comp], ph = g.plane_height[comp];
+			uint8_t *const plane = comp == 0 ? out.data[0] : (comp == 1 ? out.data[1] : out.data[2]);
+			const int opitch = comp == 0 ? out.pitch[0] : (comp == 1 ? out.pitch[1] : out.pitch[2]);
 			if (gy < ph)
 			{
-				uint8_t *dst = out.data[comp] + size_t(gy) * out.pitch[comp];
+				uint8_t *dst = plane + size_t(gy) * opitch;
+				uint32_t packed[4] = {0, 0, 0, 0};
 #pragma unroll
 				for (int jj = 4; jj < 20; jj++)
 				{
-					const int gx = gx0 + jj - 4;
-					if (gx < pw)
-					{
-						float f = __fadd_rn(e[jj], 0.5f);
-						f = fminf(fmaxf(f, 0.0f), 1.0f);
-						dst[gx] = uint8_t(int(__fadd_rn(__fmul_rn(f, 255.0f), 0.5f)));
-					}
+					float f = __fadd_rn(e[jj], 0.5f);
+					f = fminf(fmaxf(f, 0.0f), 1.0f);
+					const uint32_t u = uint32_t(int(__fadd_rn(__fmul_rn(f, 255.0f), 0.5f)));
+					packed[(jj - 4) >> 2] |= u << (8 * ((jj - 4) & 3));
+				}
+				if (gx0 + 16 <= pw && (reinterpret_cast<uintptr_t>(dst + gx0) & 15u) == 0)
+					*reinterpret_cast<uint4 *>(dst + gx0) = make_uint4(packed[0], packed[1], packed[2], packed[3]);
+				else
+				{
+#pragma unroll
+					for (int jj = 0; jj < 16; jj++)
+						if (gx0 + jj < pw)
+							dst[gx0 + jj] = uint8_t(packed[jj >> 2] >> (8 * (jj & 3)));
 				}
 			}
 		}
@@ -283,12 +370,38 @@ __global__ void __launch_bounds__(kIdwtThreads) idwt_kernel(Geometry g, int leve
 			const bool pf16 = P.fp16 != 0;
 			if (gy < P.height)
 			{
-#pragma unroll
-				for (int jj = 4; jj < 20; jj++)
+				const int64_t base = B.offset + int64_t(gy) * P.pitch + gx0;
+				if (gx0 + 16 <= P.width)
 				{
-					const int gx = gx0 + jj - 4;
-					if (gx < P.width)
-						store_coef(in.coef32, in.coef16, pf16, B.offset + int64_t(gy) * P.pitch + gx, e[jj]);
+					if (pf16)
+					{
+						uint32_t hw[8];
+#pragma unroll
+						for (int k = 0; k < 8; k++)
+						{
+							__half2 h2 = __floats2half2_rn(e[4 + 2 * k], e[5 + 2 * k]);
+							hw[k] = *reinterpret_cast<uint32_t *>(&h2);
+						}
+						*reinterpret_cast<uint4 *>(in.coef16 + base) = make_uint4(hw[0], hw[1], hw[2], hw[3]);
+						*reinterpret_cast<uint4 *>(in.coef16 + base + 8) = make_uint4(hw[4], hw[5], hw[6], hw[7]);
+					}
+					else
+					{
+#pragma unroll
+						for (int k = 0; k < 4; k++)
+							*reinterpret_cast<float4 *>(in.coef32 + base + 4 * k) =
+							    make_float4(e[4 + 4 * k], e[5 + 4 * k], e[6 + 4 * k], e[7 + 4 * k]);
+					}
+				}
+				else
+				{
+#pragma unroll
+					for (int jj = 4; jj < 20; jj++)
+					{
+						const int gx = gx0 + jj - 4;
+						if (gx < P.width)
+							store_coef(in.coef32, in.coef16, pf16, B.offset + int64_t(gy) * P.pitch + gx, e[jj]);
+					}
 				}
 			}
 		}
@@ -303,9 +416,10 @@ struct BandList
 };
 
 // Canonical pyramid (all transmitted bands, band-major, unpadded) <-> padded storage.
-__global__ void pyramid_io_kernel(Geometry g, BandList list, float *canonical, float *coef32, __half *coef16,
+__global__ void pyramid_io_kernel(const Geometry *__restrict__ gp, BandList list, float *canonical, float *coef32, __half *coef16,
                                   int to_canonical)
 {
+	const Geometry &g = *gp;
 	const int k = blockIdx.y;
 	const int comp = list.comp[k], level = list.level[k], band = list.band[k];
 	const LevelDesc &L = g.level[level];
@@ -329,19 +443,19 @@ __global__ void pyramid_io_kernel(Geometry g, BandList list, float *canonical, f
 }
 } // namespace
 
-void launch_dequant(const Geometry &g, const DecodeInput &in, cudaStream_t stream)
+void launch_dequant(const Geometry &g, const Geometry *gd, const DecodeInput &in, cudaStream_t stream)
 {
-	dequant_kernel<<<g.block_count_32x32, 128, 0, stream>>>(g, in);
+	dequant_kernel<<<g.block_count_32x32, 128, 0, stream>>>(gd, in);
 }
 
-void launch_idwt_level(const Geometry &g, int level, const DecodeInput &in, const PlaneOutput &out, cudaStream_t stream)
+void launch_idwt_level(const Geometry &g, const Geometry *gd, int level, const DecodeInput &in, const PlaneOutput &out, cudaStream_t stream)
 {
 	const LevelDesc &L = g.level[level];
 	dim3 grid(L.tiles_x * L.tiles_y, (level == 0 && !g.chroma444) ? 1 : 3);
-	idwt_kernel<<<grid, kIdwtThreads, 0, stream>>>(g, level, in, out);
+	idwt_kernel<<<grid, kIdwtThreads, 0, stream>>>(gd, level, in, out);
 }
 
-void launch_pyramid_io(const Geometry &g, float *canonical, float *coef32, __half *coef16, bool to_canonical,
+void launch_pyramid_io(const Geometry &g, const Geometry *gd, float *canonical, float *coef32, __half *coef16, bool to_canonical,
                        cudaStream_t stream)
 {
 	BandList list = {};
@@ -360,6 +474,6 @@ void launch_pyramid_io(const Geometry &g, float *canonical, float *coef32, __hal
 				canon += int64_t(g.level[level].width) * g.level[level].height;
 			}
 	dim3 grid(64, list.count);
-	pyramid_io_kernel<<<grid, 256, 0, stream>>>(g, list, canonical, coef32, coef16, to_canonical ? 1 : 0);
+	pyramid_io_kernel<<<grid, 256, 0, stream>>>(gd, list, canonical, coef32, coef16, to_canonical ? 1 : 0);
 }
 } // namespace pw

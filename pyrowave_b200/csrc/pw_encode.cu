@@ -137,6 +137,19 @@ __device__ void quant_analyze_block(const float *tile, int tile_pitch, bool acti
 	if (sub != 0 && sub > msb)
 		d_lo = drop;
 
+	// compute_square_error (wavelet_quant.comp:113-128) reconstructs each value
+	// quantised at q as trunc((floor(|v| / 2^q) + 0.5) * 2^q) when nonzero. With
+	// m = int(|v|) (|v| < 2^15), floor(|v| / 2^q) = m >> q and, for q >= 1, the
+	// reconstruction is the integer ((m >> q) << q) + 2^(q-1): the same values,
+	// computed without floating-point rounding steps.
+	uint32_t mag[8];
+	float av[8];
+#pragma unroll
+	for (int i = 0; i < 8; i++)
+	{
+		av[i] = fabsf(v[i]);
+		mag[i] = uint32_t(int(av[i]));
+	}
 	const int warp_msb = __reduce_max_sync(0xffffffffu, max(msb, 0));
 	for (int q = 1; q <= warp_msb; q++)
 	{
@@ -146,13 +159,10 @@ __device__ void quant_analyze_block(const float *tile, int tile_pitch, bool acti
 #pragma unroll
 		for (int i = 0; i < 8; i++)
 		{
-			float a = fabsf(v[i]);
-			float iv = floorf(ldexpf(a, -q));
-			nsig += iv != 0.0f ? 1 : 0;
-			if (iv != 0.0f)
-				iv = __fadd_rn(iv, 0.5f);
-			iv = truncf(ldexpf(iv, q));
-			float err = __fsub_rn(a, iv);
+			const uint32_t iv = mag[i] >> q;
+			nsig += iv != 0u ? 1 : 0;
+			const float recon = iv != 0u ? float((iv << q) + (1u << (q - 1))) : 0.0f;
+			float err = __fsub_rn(av[i], recon);
 			float sq = __fmul_rn(err, err);
 			if (i < 4)
 				e0 = (i == 0) ? sq : __fadd_rn(e0, sq);
@@ -279,9 +289,10 @@ struct DwtShared
 
 // One forward level for one 32x32 band tile of one component (64x64 input
 // samples). grid.x = tile, grid.y = component index among those at this level.
-__global__ void __launch_bounds__(kDwtThreads) dwt_forward_kernel(Geometry g, int level, PlaneInput in,
+__global__ void __launch_bounds__(kDwtThreads) dwt_forward_kernel(const Geometry *__restrict__ gp, int level, PlaneInput in,
                                                                    EncodeBuffers buf, int fused)
 {
+	const Geometry &g = *gp;
 	__shared__ DwtShared sh;
 	const int comp = (level == 0 && !g.chroma444) ? 0 : int(blockIdx.y);
 	const LevelDesc &L = g.level[level];
@@ -312,15 +323,67 @@ __global__ void __launch_bounds__(kDwtThreads) dwt_forward_kernel(Geometry g, in
 	}
 	__syncthreads();
 
+	// Tile load. A tile whose 72x72 window lies inside the source maps every
+	// sample to itself: load whole rows with vector loads, all in flight at
+	// once. Edge tiles go through the mirrored index tables in batches of
+	// independent loads.
+	const int x0 = tx * 64 - 4, y0 = ty * 64 - 4;
+	const bool interior = x0 >= 0 && y0 >= 0 && x0 + kTileIn <= res_w && y0 + kTileIn <= res_h;
+	constexpr int kVecPerRow = kTileIn / 4;                // 18 vectors of 4 samples
+	constexpr int kVecs = kVecPerRow * kTileIn;            // 1296
+	constexpr int kVecIters = (kVecs + kDwtThreads - 1) / kDwtThreads;
 	if (from_plane)
 	{
-		const uint8_t *p = in.data[comp];
-		const int pitch = in.pitch[comp], xs = in.xstride[comp];
-		for (int k = threadIdx.x; k < kTileIn * kTileIn; k += kDwtThreads)
+		const uint8_t *p = comp == 0 ? in.data[0] : (comp == 1 ? in.data[1] : in.data[2]);
+		const int pitch = comp == 0 ? in.pitch[0] : (comp == 1 ? in.pitch[1] : in.pitch[2]);
+		const int xs = comp == 0 ? in.xstride[0] : (comp == 1 ? in.xstride[1] : in.xstride[2]);
+		const bool vec_ok = interior && xs == 1 && ((reinterpret_cast<uintptr_t>(p) | uintptr_t(pitch)) & 3u) == 0;
+		if (vec_ok)
 		{
-			int i = k / kTileIn, j = k - i * kTileIn;
-			float f = __fdiv_rn(float(p[size_t(sh.yidx[i]) * pitch + size_t(sh.xidx[j]) * xs]), 255.0f);
-			sh.in[i][j] = __fsub_rn(f, 0.5f);
+			uint32_t v[kVecIters];
+#pragma unroll
+			for (int u = 0; u < kVecIters; u++)
+			{
+				const int k = threadIdx.x + u * kDwtThreads;
+				const int i = k / kVecPerRow, j = k - i * kVecPerRow;
+				v[u] = k < kVecs ? __ldg(reinterpret_cast<const uint32_t *>(p + size_t(y0 + i) * pitch + x0) + j) : 0u;
+			}
+#pragma unroll
+			for (int u = 0; u < kVecIters; u++)
+			{
+				const int k = threadIdx.x + u * kDwtThreads;
+				if (k < kVecs)
+				{
+					const int i = k / kVecPerRow, j = k - i * kVecPerRow;
+#pragma unroll
+					for (int b = 0; b < 4; b++)
+						sh.in[i][4 * j + b] = __fsub_rn(__fdiv_rn(float((v[u] >> (8 * b)) & 0xffu), 255.0f), 0.5f);
+				}
+			}
+		}
+		else
+		{
+			for (int base = threadIdx.x; base < kTileIn * kTileIn; base += kDwtThreads * 8)
+			{
+				uint32_t v[8];
+#pragma unroll
+				for (int u = 0; u < 8; u++)
+				{
+					const int k = base + u * kDwtThreads;
+					const int i = k / kTileIn, j = k - i * kTileIn;
+					v[u] = k < kTileIn * kTileIn ? p[size_t(sh.yidx[i]) * pitch + size_t(sh.xidx[j]) * xs] : 0u;
+				}
+#pragma unroll
+				for (int u = 0; u < 8; u++)
+				{
+					const int k = base + u * kDwtThreads;
+					if (k < kTileIn * kTileIn)
+					{
+						const int i = k / kTileIn, j = k - i * kTileIn;
+						sh.in[i][j] = __fsub_rn(__fdiv_rn(float(v[u]), 255.0f), 0.5f);
+					}
+				}
+			}
 		}
 	}
 	else
@@ -328,11 +391,66 @@ __global__ void __launch_bounds__(kDwtThreads) dwt_forward_kernel(Geometry g, in
 		const LevelDesc &P = g.level[level - 1];
 		const BandDesc &B = g.band[comp][level - 1][0];
 		const bool f16 = P.fp16 != 0;
-		for (int k = threadIdx.x; k < kTileIn * kTileIn; k += kDwtThreads)
+		if (interior)
 		{
-			int i = k / kTileIn, j = k - i * kTileIn;
-			int64_t idx = B.offset + int64_t(sh.yidx[i]) * P.pitch + sh.xidx[j];
-			sh.in[i][j] = load_coef(buf.coef32, buf.coef16, f16, idx);
+			float4 v[kVecIters];
+#pragma unroll
+			for (int u = 0; u < kVecIters; u++)
+			{
+				const int k = threadIdx.x + u * kDwtThreads;
+				const int i = k / kVecPerRow, j = k - i * kVecPerRow;
+				const int64_t idx = B.offset + int64_t(y0 + i) * P.pitch + x0 + 4 * j;
+				if (k >= kVecs)
+					v[u] = make_float4(0.f, 0.f, 0.f, 0.f);
+				else if (f16)
+				{
+					uint2 hv = __ldg(reinterpret_cast<const uint2 *>(buf.coef16 + idx));
+					float2 a = __half22float2(*reinterpret_cast<__half2 *>(&hv.x));
+					float2 b = __half22float2(*reinterpret_cast<__half2 *>(&hv.y));
+					v[u] = make_float4(a.x, a.y, b.x, b.y);
+				}
+				else
+					v[u] = __ldg(reinterpret_cast<const float4 *>(buf.coef32 + idx));
+			}
+#pragma unroll
+			for (int u = 0; u < kVecIters; u++)
+			{
+				const int k = threadIdx.x + u * kDwtThreads;
+				if (k < kVecs)
+				{
+					const int i = k / kVecPerRow, j = k - i * kVecPerRow;
+					sh.in[i][4 * j + 0] = v[u].x;
+					sh.in[i][4 * j + 1] = v[u].y;
+					sh.in[i][4 * j + 2] = v[u].z;
+					sh.in[i][4 * j + 3] = v[u].w;
+				}
+			}
+		}
+		else
+		{
+			for (int base = threadIdx.x; base < kTileIn * kTileIn; base += kDwtThreads * 8)
+			{
+				float v[8];
+#pragma unroll
+				for (int u = 0; u < 8; u++)
+				{
+					const int k = base + u * kDwtThreads;
+					const int i = k / kTileIn, j = k - i * kTileIn;
+					v[u] = k < kTileIn * kTileIn
+					           ? load_coef(buf.coef32, buf.coef16, f16, B.offset + int64_t(sh.yidx[i]) * P.pitch + sh.xidx[j])
+					           : 0.0f;
+				}
+#pragma unroll
+				for (int u = 0; u < 8; u++)
+				{
+					const int k = base + u * kDwtThreads;
+					if (k < kTileIn * kTileIn)
+					{
+						const int i = k / kTileIn, j = k - i * kTileIn;
+						sh.in[i][j] = v[u];
+					}
+				}
+			}
 		}
 	}
 	__syncthreads();
@@ -431,8 +549,9 @@ __global__ void __launch_bounds__(kDwtThreads) dwt_forward_kernel(Geometry g, in
 // Quantiser over a pyramid already in storage (the reference's
 // Encoder::encode_pre_transformed, pyrowave_encoder.cpp:1138-1151).
 // Two 32x32 blocks per CTA.
-__global__ void __launch_bounds__(256) quant_pretransformed_kernel(Geometry g, EncodeBuffers buf)
+__global__ void __launch_bounds__(256) quant_pretransformed_kernel(const Geometry *__restrict__ gp, EncodeBuffers buf)
 {
+	const Geometry &g = *gp;
 	__shared__ float tile[2][32][kBandPitch];
 	__shared__ QuantGroupShared q[2];
 	const int grp = threadIdx.x >> 7, t = threadIdx.x & 127;
@@ -492,6 +611,68 @@ __device__ __forceinline__ uint32_t block_exclusive_scan_1024(uint32_t v, uint32
 	return base + x - v;
 }
 
+// The 16 RD entries of one 32x32 block: words at quant 0..15 and buckets.
+struct BlockRD
+{
+	uint32_t cost[16];
+	uint32_t bucket[16];
+};
+
+__device__ __forceinline__ void load_block_rd(const EncodeBuffers &buf, int blk, BlockRD &rd)
+{
+	const uint4 c0 = __ldg(reinterpret_cast<const uint4 *>(buf.rd_cost + size_t(blk) * 16));
+	const uint4 c1 = __ldg(reinterpret_cast<const uint4 *>(buf.rd_cost + size_t(blk) * 16) + 1);
+	const uint4 bb = __ldg(reinterpret_cast<const uint4 *>(buf.rd_bucket + size_t(blk) * 16));
+	const uint32_t cw[8] = {c0.x, c0.y, c0.z, c0.w, c1.x, c1.y, c1.z, c1.w};
+	const uint32_t bw[4] = {bb.x, bb.y, bb.z, bb.w};
+#pragma unroll
+	for (int i = 0; i < 8; i++)
+	{
+		rd.cost[2 * i] = cw[i] & 0xffffu;
+		rd.cost[2 * i + 1] = cw[i] >> 16;
+	}
+#pragma unroll
+	for (int i = 0; i < 16; i++)
+		rd.bucket[i] = (bw[i >> 2] >> (8 * (i & 3))) & 0xffu;
+}
+
+// Saving of the block's RD operation that sits in bucket bk (0 if none).
+__device__ __forceinline__ uint32_t op_saving_at_bucket(const EncodeBuffers &buf, int blk, uint32_t bk)
+{
+	BlockRD rd;
+	load_block_rd(buf, blk, rd);
+	uint32_t sv = 0;
+#pragma unroll
+	for (int l = 1; l < 16; l++)
+		if (rd.bucket[l] == bk && sv == 0)
+			sv = rd.cost[l - 1] - rd.cost[l];
+	return sv;
+}
+
+// Quant of a block: its largest applied RD step. Steps are applied when their
+// (bucket, subdivision) slot precedes x*, or equals it and the block precedes the cut.
+__device__ __forceinline__ uint32_t block_words(const EncodeBuffers &buf, int blk, int sdiv, int xstar, uint32_t cut,
+                                                int &q)
+{
+	BlockRD rd;
+	load_block_rd(buf, blk, rd);
+	q = 0;
+#pragma unroll
+	for (int l = 1; l < 16; l++)
+	{
+		const uint32_t saving = rd.cost[l - 1] - rd.cost[l];
+		const int x = int(rd.bucket[l]) * kSubdivisions + sdiv;
+		if (saving != 0 && (x < xstar || (x == xstar && uint32_t(blk) < cut)))
+			q = l;
+	}
+	uint32_t words = rd.cost[0];
+#pragma unroll
+	for (int l = 1; l < 16; l++)
+		if (q == l)
+			words = rd.cost[l];
+	return words;
+}
+
 // Exact-rate resolve (analyze_rate_control_finalize.comp + resolve_rate_control.comp).
 //
 // The reference walks all 2048 (bucket, subdivision) slots; for each slot with
@@ -501,9 +682,10 @@ __device__ __forceinline__ uint32_t block_exclusive_scan_1024(uint32_t v, uint32
 // not at all, and x* up to the first operation whose exclusive prefix reaches
 // its requirement. This kernel computes x* and that cut, then gives every
 // block its quant (the largest applied step), its word count and its offset.
-__global__ void __launch_bounds__(1024) resolve_kernel(Geometry g, EncodeBuffers buf, uint32_t target_words,
+__global__ void __launch_bounds__(1024) resolve_kernel(const Geometry *__restrict__ gp, EncodeBuffers buf, uint32_t target_words,
                                                       uint32_t sequence)
 {
+	const Geometry &g = *gp;
 	__shared__ uint32_t scan[kHistSize];
 	__shared__ uint32_t warp_sums[32];
 	__shared__ int s_xstar;
@@ -535,73 +717,55 @@ __global__ void __launch_bounds__(1024) resolve_kernel(Geometry g, EncodeBuffers
 	__syncthreads();
 	const int xstar = s_xstar;
 
+	// Each thread owns a contiguous run of blocks, so every pass below needs
+	// only one block-wide scan.
+	const int xstar_sdiv = xstar & (kSubdivisions - 1);
 	if (xstar >= 0)
 	{
 		const int64_t required = need - (xstar > 0 ? int64_t(scan[xstar - 1]) : 0);
-		const int sdiv = xstar & (kSubdivisions - 1);
 		const uint32_t bk = uint32_t(xstar >> 4);
-		const int start = sdiv * nbps;
+		const int start = xstar_sdiv * nbps;
 		const int end = min(start + nbps, nblocks);
-		uint32_t carry = 0;
-		for (int base = start; base < end; base += 1024)
+		const int per = (end - start + 1023) / 1024;
+		const int b0 = start + t * per, b1 = min(b0 + per, end);
+		uint32_t local = 0;
+		for (int blk = b0; blk < b1; blk++)
+			local += op_saving_at_bucket(buf, blk, bk);
+		uint32_t tot;
+		uint32_t ex = block_exclusive_scan_1024(local, warp_sums, tot);
+		for (int blk = b0; blk < b1; blk++)
 		{
-			const int blk = base + t;
-			uint32_t sv = 0;
-			if (blk < end)
+			const uint32_t sv = op_saving_at_bucket(buf, blk, bk);
+			if (sv != 0 && int64_t(ex) >= required)
 			{
-				const uint16_t *cost = buf.rd_cost + size_t(blk) * 16;
-				const uint8_t *bucket = buf.rd_bucket + size_t(blk) * 16;
-				for (int l = 1; l < 16; l++)
-					if (bucket[l] == bk)
-					{
-						sv = uint32_t(cost[l - 1]) - uint32_t(cost[l]);
-						break;
-					}
-			}
-			uint32_t tot;
-			uint32_t ex = block_exclusive_scan_1024(sv, warp_sums, tot);
-			if (sv != 0 && int64_t(carry) + int64_t(ex) >= required)
 				atomicMin(&s_cut, uint32_t(blk));
-			carry += tot;
+				break;
+			}
+			ex += sv;
 		}
 	}
 	__syncthreads();
 	const uint32_t cut = s_cut;
 
-	uint32_t carry = 0, non_zero = 0;
-	for (int base = 0; base < nblocks; base += 1024)
+	const int per = (nblocks + 1023) / 1024;
+	const int b0 = min(t * per, nblocks), b1 = min(b0 + per, nblocks);
+	uint32_t local = 0, local_nz = 0;
+	for (int blk = b0; blk < b1; blk++)
 	{
-		const int blk = base + t;
-		uint32_t words = 0;
-		int q = 0;
-		if (blk < nblocks)
-		{
-			const uint16_t *cost = buf.rd_cost + size_t(blk) * 16;
-			const uint8_t *bucket = buf.rd_bucket + size_t(blk) * 16;
-			const int sdiv = blk >> g.subdivision_shift;
-			for (int l = 1; l < 16; l++)
-			{
-				uint32_t saving = uint32_t(cost[l - 1]) - uint32_t(cost[l]);
-				if (saving == 0)
-					continue;
-				int x = int(bucket[l]) * kSubdivisions + sdiv;
-				if (x < xstar || (x == xstar && uint32_t(blk) < cut))
-					q = l;
-			}
-			words = cost[q];
-		}
-		uint32_t tot;
-		uint32_t ex = block_exclusive_scan_1024(words, warp_sums, tot);
-		if (blk < nblocks)
-		{
-			buf.quant[blk] = q;
-			buf.block_meta[2 * blk + 0] = carry + ex;
-			buf.block_meta[2 * blk + 1] = words;
-		}
-		uint32_t nz = __syncthreads_count(words != 0);
-		non_zero += nz;
-		carry += tot;
+		int q;
+		const uint32_t words = block_words(buf, blk, blk >> g.subdivision_shift, xstar, cut, q);
+		buf.quant[blk] = q;
+		buf.block_meta[2 * blk + 0] = local;
+		buf.block_meta[2 * blk + 1] = words;
+		local += words;
+		local_nz += words != 0 ? 1u : 0u;
 	}
+	uint32_t carry;
+	const uint32_t base = block_exclusive_scan_1024(local, warp_sums, carry);
+	for (int blk = b0; blk < b1; blk++)
+		buf.block_meta[2 * blk + 0] += base;
+	uint32_t non_zero;
+	block_exclusive_scan_1024(local_nz, warp_sums, non_zero);
 
 	if (t == 0)
 	{
@@ -621,8 +785,9 @@ __global__ void __launch_bounds__(1024) resolve_kernel(Geometry g, EncodeBuffers
 // ---------------------------------------------------------------------------
 // Block packing: one 32x32 block per 128-thread CTA, assembled in shared
 // memory and written as whole words at its prefix-scanned offset.
-__global__ void __launch_bounds__(128) pack_kernel(Geometry g, EncodeBuffers buf)
+__global__ void __launch_bounds__(128) pack_kernel(const Geometry *__restrict__ gp, EncodeBuffers buf)
 {
+	const Geometry &g = *gp;
 	__shared__ uint32_t pkt[kMaxBlockWords];
 	__shared__ uint32_t s_ballot[4];
 	__shared__ uint32_t s_bytes[16];
@@ -775,27 +940,27 @@ __global__ void __launch_bounds__(128) pack_kernel(Geometry g, EncodeBuffers buf
 }
 } // namespace
 
-void launch_dwt_forward_level(const Geometry &g, int level, const PlaneInput &in, const EncodeBuffers &buf,
+void launch_dwt_forward_level(const Geometry &g, const Geometry *gd, int level, const PlaneInput &in, const EncodeBuffers &buf,
                               bool fused_quant, cudaStream_t stream)
 {
 	const LevelDesc &L = g.level[level];
 	dim3 grid(L.tiles_x * L.tiles_y, (level == 0 && !g.chroma444) ? 1 : 3);
-	dwt_forward_kernel<<<grid, kDwtThreads, 0, stream>>>(g, level, in, buf, fused_quant ? 1 : 0);
+	dwt_forward_kernel<<<grid, kDwtThreads, 0, stream>>>(gd, level, in, buf, fused_quant ? 1 : 0);
 }
 
-void launch_quant_pretransformed(const Geometry &g, const EncodeBuffers &buf, cudaStream_t stream)
+void launch_quant_pretransformed(const Geometry &g, const Geometry *gd, const EncodeBuffers &buf, cudaStream_t stream)
 {
-	quant_pretransformed_kernel<<<(g.block_count_32x32 + 1) / 2, 256, 0, stream>>>(g, buf);
+	quant_pretransformed_kernel<<<(g.block_count_32x32 + 1) / 2, 256, 0, stream>>>(gd, buf);
 }
 
-void launch_resolve(const Geometry &g, const EncodeBuffers &buf, uint32_t target_words, uint32_t sequence,
+void launch_resolve(const Geometry &g, const Geometry *gd, const EncodeBuffers &buf, uint32_t target_words, uint32_t sequence,
                     cudaStream_t stream)
 {
-	resolve_kernel<<<1, 1024, 0, stream>>>(g, buf, target_words, sequence);
+	resolve_kernel<<<1, 1024, 0, stream>>>(gd, buf, target_words, sequence);
 }
 
-void launch_pack(const Geometry &g, const EncodeBuffers &buf, cudaStream_t stream)
+void launch_pack(const Geometry &g, const Geometry *gd, const EncodeBuffers &buf, cudaStream_t stream)
 {
-	pack_kernel<<<g.block_count_32x32, 128, 0, stream>>>(g, buf);
+	pack_kernel<<<g.block_count_32x32, 128, 0, stream>>>(gd, buf);
 }
 } // namespace pw

@@ -31,6 +31,30 @@ namespace
 {
 int align_up(int v, int a) { return (v + a - 1) & ~(a - 1); }
 
+// CUDA error reporting: failures are logged to stderr when PYROWAVE_DEBUG is
+// set (the reference logs through Granite only with VULKAN_DEBUG,
+// pyrowave_c.cpp:17-29).
+bool debug_enabled()
+{
+	static const bool on = [] {
+		const char *e = getenv("PYROWAVE_DEBUG");
+		return e && atoi(e) != 0;
+	}();
+	return on;
+}
+
+bool cuda_ok(cudaError_t e, const char *what)
+{
+	if (e == cudaSuccess)
+		return true;
+	if (debug_enabled())
+		fprintf(stderr, "pyrowave: %s failed: %s\n", what, cudaGetErrorString(e));
+	return false;
+}
+
+// Consumes (and reports) the error state left by preceding kernel launches.
+bool launches_ok(const char *what) { return cuda_ok(cudaGetLastError(), what); }
+
 uint32_t float_bits(float f)
 {
 	uint32_t u;
@@ -274,45 +298,56 @@ namespace
 // pyrowave_encoder.cpp:277,335,411,486,591; surfaced by report_performance_stats).
 struct StageEvents
 {
-	static constexpr int kMax = 8;
+	static constexpr int kMax = 16;
 	cudaEvent_t ev[kMax + 1] = {};
 	const char *tags[kMax] = {};
 	int count = 0;
 	bool pending = false;
 	bool created = false;
 
+	// Outside stream capture: create the events once timing is on.
+	void prepare(pyrowave_device_opaque *dev)
+	{
+		if (!dev->stage_timing || created)
+			return;
+		for (auto &e : ev)
+			cuda_ok(cudaEventCreate(&e), "cudaEventCreate");
+		created = true;
+	}
+	// Inside stream capture the records become event-record graph nodes
+	// (cudaEventRecordExternal), replayed with every launch of the graph.
 	void begin(pyrowave_device_opaque *dev, cudaStream_t s)
 	{
-		if (!dev->stage_timing)
+		if (!dev->stage_timing || !created)
 			return;
-		if (!created)
-		{
-			for (auto &e : ev)
-				cudaEventCreate(&e);
-			created = true;
-		}
 		count = 0;
-		cudaEventRecord(ev[0], s);
+		cuda_ok(cudaEventRecordWithFlags(ev[0], s, cudaEventRecordExternal), "cudaEventRecordWithFlags");
 	}
 	void mark(pyrowave_device_opaque *dev, cudaStream_t s, const char *tag)
 	{
-		if (!dev->stage_timing || count >= kMax)
+		if (!dev->stage_timing || !created || count >= kMax)
 			return;
 		tags[count++] = tag;
-		cudaEventRecord(ev[count], s);
-		pending = true;
+		cuda_ok(cudaEventRecordWithFlags(ev[count], s, cudaEventRecordExternal), "cudaEventRecordWithFlags");
+	}
+	// The events of the captured sequence were launched (they are graph nodes).
+	void launched(pyrowave_device_opaque *dev)
+	{
+		if (dev->stage_timing && created && count > 0)
+			pending = true;
 	}
 	void collect(pyrowave_device_opaque *dev)
 	{
 		if (!pending)
 			return;
 		pending = false;
-		cudaEventSynchronize(ev[count]);
+		if (!cuda_ok(cudaEventSynchronize(ev[count]), "cudaEventSynchronize"))
+			return;
 		for (int i = 0; i < count; i++)
 		{
 			float ms = 0.0f;
-			cudaEventElapsedTime(&ms, ev[i], ev[i + 1]);
-			dev->add_time(tags[i], ms);
+			if (cuda_ok(cudaEventElapsedTime(&ms, ev[i], ev[i + 1]), "cudaEventElapsedTime"))
+				dev->add_time(tags[i], ms);
 		}
 	}
 	void destroy()
@@ -325,6 +360,82 @@ struct StageEvents
 };
 } // namespace
 
+namespace
+{
+// A kernel node of a captured graph, with the launch parameters it was
+// captured with; its arguments are replaced per call.
+struct KernelNode
+{
+	cudaGraphNode_t node = nullptr;
+	cudaKernelNodeParams params = {};
+};
+
+// The node the last captured operation on `s` created.
+bool last_captured_node(cudaStream_t s, KernelNode &kn)
+{
+	cudaStreamCaptureStatus st;
+	const cudaGraphNode_t *deps = nullptr;
+	size_t n = 0;
+	if (!cuda_ok(cudaStreamGetCaptureInfo(s, &st, nullptr, nullptr, &deps, &n), "cudaStreamGetCaptureInfo") ||
+	    st != cudaStreamCaptureStatusActive || n == 0)
+		return false;
+	kn.node = deps[n - 1];
+	return cuda_ok(cudaGraphKernelNodeGetParams(kn.node, &kn.params), "cudaGraphKernelNodeGetParams");
+}
+
+// Replace the arguments of a kernel node in an instantiated graph; the types
+// of `args` must be exactly the kernel's parameter types.
+template <typename... A> bool set_kernel_args(cudaGraphExec_t exec, const KernelNode &kn, A &...args)
+{
+	void *arr[] = {static_cast<void *>(&args)...};
+	cudaKernelNodeParams p = kn.params;
+	p.kernelParams = arr;
+	p.extra = nullptr;
+	return cuda_ok(cudaGraphExecKernelNodeSetParams(exec, kn.node, &p), "cudaGraphExecKernelNodeSetParams");
+}
+
+// One encode or decode sequence captured as a CUDA graph: a single launch
+// per frame instead of one per kernel.
+struct CapturedGraph
+{
+	cudaGraph_t graph = nullptr;
+	cudaGraphExec_t exec = nullptr;
+	uint64_t key = ~0ull;
+	bool valid() const { return exec != nullptr; }
+	void destroy()
+	{
+		if (exec)
+			cudaGraphExecDestroy(exec);
+		if (graph)
+			cudaGraphDestroy(graph);
+		exec = nullptr;
+		graph = nullptr;
+		key = ~0ull;
+	}
+	bool begin(cudaStream_t s)
+	{
+		destroy();
+		launches_ok("work queued before graph capture");
+		return cuda_ok(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal), "cudaStreamBeginCapture");
+	}
+	bool end(cudaStream_t s, uint64_t k)
+	{
+		if (!cuda_ok(cudaStreamEndCapture(s, &graph), "cudaStreamEndCapture"))
+		{
+			graph = nullptr;
+			return false;
+		}
+		if (!cuda_ok(cudaGraphInstantiate(&exec, graph, 0), "cudaGraphInstantiate"))
+		{
+			exec = nullptr;
+			return false;
+		}
+		key = k;
+		return true;
+	}
+};
+} // namespace
+
 struct pyrowave_encoder_opaque
 {
 	pyrowave_device device = nullptr;
@@ -333,6 +444,8 @@ struct pyrowave_encoder_opaque
 	uint32_t fp16_mask = 0;
 	bool allocated = false;
 
+	Geometry *g_dev = nullptr;          // device copy of g read by the kernels
+	Geometry *g_dev_override = nullptr; // per-call copy for encode_pre_transformed
 	float *coef32 = nullptr;
 	__half *coef16 = nullptr;
 	uint32_t *code_words = nullptr;
@@ -357,6 +470,9 @@ struct pyrowave_encoder_opaque
 	bool has_device_frame = false;
 	uint32_t sequence_count = 0;
 	StageEvents timing;
+	CapturedGraph graph;
+	KernelNode node_dwt[kLevels];
+	KernelNode node_resolve;
 
 	EncodeBuffers buffers() const
 	{
@@ -380,6 +496,8 @@ struct pyrowave_encoder_opaque
 	{
 		if (device)
 			cudaStreamSynchronize(device->stream);
+		dev_free(g_dev);
+		dev_free(g_dev_override);
 		dev_free(coef32);
 		dev_free(coef16);
 		dev_free(code_words);
@@ -398,9 +516,27 @@ struct pyrowave_encoder_opaque
 		host_free(h_total);
 		if (done)
 			cudaEventDestroy(done);
+		done = nullptr;
 		timing.destroy();
+		graph.destroy();
+		g_dev = g_dev_override = nullptr;
 		coef32 = nullptr;
 		coef16 = nullptr;
+		code_words = nullptr;
+		rd_cost = nullptr;
+		rd_bucket = nullptr;
+		rd_dist = nullptr;
+		rc = nullptr;
+		quant = nullptr;
+		block_meta = nullptr;
+		stream_buf = nullptr;
+		stream_capacity = 0;
+		jobs_d = nullptr;
+		for (auto &p : in_planes)
+			p = nullptr;
+		h_meta = h_stream = h_total = nullptr;
+		h_stream_capacity = 0;
+		has_frame = has_device_frame = false;
 		allocated = false;
 	}
 
@@ -411,6 +547,8 @@ struct pyrowave_encoder_opaque
 		if (!build_geometry(g, jobs, g.width, g.height, g.chroma444 != 0, fp16_mask))
 			return PYROWAVE_ERROR_INVALID_ARGUMENT;
 		bool ok = true;
+		g_dev = dev_alloc<Geometry>(1, ok);
+		g_dev_override = dev_alloc<Geometry>(1, ok);
 		coef32 = dev_alloc<float>(size_t(g.storage_elems32), ok);
 		coef16 = dev_alloc<__half>(size_t(g.storage_elems16), ok);
 		code_words = dev_alloc<uint32_t>(size_t(g.block_count_8x8), ok);
@@ -431,6 +569,7 @@ struct pyrowave_encoder_opaque
 			return PYROWAVE_ERROR_OUT_OF_DEVICE_MEMORY;
 		}
 		cudaMemcpy(jobs_d, jobs.data(), jobs.size() * 4, cudaMemcpyHostToDevice);
+		cudaMemcpy(g_dev, &g, sizeof(Geometry), cudaMemcpyHostToDevice);
 		allocated = true;
 		return PYROWAVE_SUCCESS;
 	}
@@ -499,17 +638,60 @@ struct pyrowave_encoder_opaque
 		sequence_count = (sequence_count + 1) & 7u;
 		EncodeBuffers b = buffers();
 		timing.collect(device);
-		timing.begin(device, s);
-		cudaMemsetAsync(rc, 0, sizeof(RateControlState), s);
-		for (int level = 0; level < kLevels; level++)
-			launch_dwt_forward_level(g, level, in, b, true, s);
-		timing.mark(device, s, "DWT+Quant+Analyze");
-		launch_resolve(g, b, target_words, sequence_count, s);
-		timing.mark(device, s, "Resolve");
-		launch_pack(g, b, s);
-		timing.mark(device, s, "Packing");
-		if (cudaPeekAtLastError() != cudaSuccess)
+		timing.prepare(device);
+		const uint64_t key = uint64_t(stream_capacity) | (device->stage_timing ? (1ull << 40) : 0ull);
+		if (!graph.valid() || graph.key != key)
+		{
+			// Capture the frame's kernel sequence once (pyrowave_encoder.cpp:1153-1183:
+			// clear, DWT + quant + analyze per level, resolve, pack).
+			if (!graph.begin(s))
+				return PYROWAVE_ERROR_GENERIC;
+			bool ok = true;
+			timing.begin(device, s);
+			cudaMemsetAsync(rc, 0, sizeof(RateControlState), s);
+			static const char *const dwt_tags[kLevels] = {"dwt0", "dwt1", "dwt2", "dwt3", "dwt4"};
+			for (int level = 0; level < kLevels; level++)
+			{
+				launch_dwt_forward_level(g, g_dev, level, in, b, true, s);
+				ok = ok && last_captured_node(s, node_dwt[level]);
+				timing.mark(device, s, dwt_tags[level]);
+			}
+			launch_resolve(g, g_dev, b, target_words, sequence_count, s);
+			ok = ok && last_captured_node(s, node_resolve);
+			timing.mark(device, s, "resolve");
+			launch_pack(g, g_dev, b, s);
+			timing.mark(device, s, "pack");
+			ok = graph.end(s, key) && ok;
+			if (!ok)
+			{
+				graph.destroy();
+				(void)cudaGetLastError();
+				return PYROWAVE_ERROR_GENERIC;
+			}
+		}
+		else
+		{
+			const Geometry *gd = g_dev;
+			PlaneInput pin = in;
+			int fused = 1;
+			uint32_t tw = target_words, seq = sequence_count;
+			bool ok = true;
+			for (int level = 0; level < kLevels; level++)
+			{
+				int lv = level;
+				ok = ok && set_kernel_args(graph.exec, node_dwt[level], gd, lv, pin, b, fused);
+			}
+			ok = ok && set_kernel_args(graph.exec, node_resolve, gd, b, tw, seq);
+			if (!ok)
+			{
+				graph.destroy();
+				(void)cudaGetLastError();
+				return PYROWAVE_ERROR_GENERIC;
+			}
+		}
+		if (!cuda_ok(cudaGraphLaunch(graph.exec, s), "cudaGraphLaunch"))
 			return PYROWAVE_ERROR_GENERIC;
+		timing.launched(device);
 		has_device_frame = true;
 		return PYROWAVE_SUCCESS;
 	}
@@ -545,6 +727,7 @@ struct pyrowave_decoder_opaque
 	uint32_t fp16_mask = 0;
 	bool allocated = false;
 
+	Geometry *g_dev = nullptr;
 	float *coef32 = nullptr;
 	__half *coef16 = nullptr;
 	uint32_t *jobs_d = nullptr;
@@ -556,6 +739,9 @@ struct pyrowave_decoder_opaque
 	uint32_t *h_upload = nullptr;
 	size_t h_upload_capacity = 0;
 	StageEvents timing;
+	CapturedGraph graph_full, graph_idwt;
+	KernelNode node_dequant;
+	KernelNode node_idwt_full[kLevels], node_idwt_only[kLevels];
 
 	// Parser state (pyrowave_decoder.cpp:24-39).
 	std::vector<uint32_t> offsets;
@@ -670,6 +856,7 @@ struct pyrowave_decoder_opaque
 	{
 		if (device)
 			cudaStreamSynchronize(device->stream);
+		dev_free(g_dev);
 		dev_free(coef32);
 		dev_free(coef16);
 		dev_free(jobs_d);
@@ -679,6 +866,17 @@ struct pyrowave_decoder_opaque
 			dev_free(p);
 		host_free(h_upload);
 		timing.destroy();
+		graph_full.destroy();
+		graph_idwt.destroy();
+		g_dev = nullptr;
+		coef32 = nullptr;
+		coef16 = nullptr;
+		jobs_d = offsets_d = payload_d = nullptr;
+		payload_capacity = 0;
+		for (auto &p : out_planes)
+			p = nullptr;
+		h_upload = nullptr;
+		h_upload_capacity = 0;
 		allocated = false;
 	}
 
@@ -689,6 +887,7 @@ struct pyrowave_decoder_opaque
 		if (!build_geometry(g, jobs, g.width, g.height, g.chroma444 != 0, fp16_mask))
 			return PYROWAVE_ERROR_INVALID_ARGUMENT;
 		bool ok = true;
+		g_dev = dev_alloc<Geometry>(1, ok);
 		coef32 = dev_alloc<float>(size_t(g.storage_elems32), ok);
 		coef16 = dev_alloc<__half>(size_t(g.storage_elems16), ok);
 		jobs_d = dev_alloc<uint32_t>(jobs.size(), ok);
@@ -699,6 +898,7 @@ struct pyrowave_decoder_opaque
 			return PYROWAVE_ERROR_OUT_OF_DEVICE_MEMORY;
 		}
 		cudaMemcpy(jobs_d, jobs.data(), jobs.size() * 4, cudaMemcpyHostToDevice);
+		cudaMemcpy(g_dev, &g, sizeof(Geometry), cudaMemcpyHostToDevice);
 		if (offsets.size() != size_t(g.block_count_32x32))
 		{
 			offsets.assign(size_t(g.block_count_32x32), UINT32_MAX);
@@ -750,19 +950,66 @@ struct pyrowave_decoder_opaque
 	}
 
 	// Dequantise + inverse transform (pyrowave_decoder.cpp:796-830).
-	void run(const DecodeInput &in, const PlaneOutput &out, cudaStream_t s, bool dequant)
+	// Dequantise + inverse transform (pyrowave_decoder.cpp:796-830), as one graph launch.
+	bool run(const DecodeInput &in, const PlaneOutput &out, cudaStream_t s, bool dequant)
 	{
 		timing.collect(device);
-		timing.begin(device, s);
-		if (dequant)
+		timing.prepare(device);
+		CapturedGraph &graph = dequant ? graph_full : graph_idwt;
+		const uint64_t key = device->stage_timing ? 1ull : 0ull;
+		if (!graph.valid() || graph.key != key)
 		{
-			launch_dequant(g, in, s);
-			timing.mark(device, s, "Dequant");
+			if (!graph.begin(s))
+				return false;
+			bool ok = true;
+			timing.begin(device, s);
+			if (dequant)
+			{
+				launch_dequant(g, g_dev, in, s);
+				ok = ok && last_captured_node(s, node_dequant);
+				timing.mark(device, s, "dequant");
+			}
+			static const char *const idwt_tags[kLevels] = {"idwt0", "idwt1", "idwt2", "idwt3", "idwt4"};
+			for (int level = kLevels - 1; level >= 0; level--)
+			{
+				launch_idwt_level(g, g_dev, level, in, out, s);
+				ok = ok && last_captured_node(s, dequant ? node_idwt_full[level] : node_idwt_only[level]);
+				timing.mark(device, s, idwt_tags[level]);
+			}
+			ok = graph.end(s, key) && ok;
+			if (!ok)
+			{
+				graph.destroy();
+				(void)cudaGetLastError();
+				return false;
+			}
 		}
-		for (int level = kLevels - 1; level >= 0; level--)
-			launch_idwt_level(g, level, in, out, s);
-		timing.mark(device, s, "iDWT");
+		else
+		{
+			const Geometry *gd = g_dev;
+			DecodeInput din = in;
+			PlaneOutput pout = out;
+			bool ok = true;
+			if (dequant)
+				ok = set_kernel_args(graph.exec, node_dequant, gd, din);
+			for (int level = 0; level < kLevels; level++)
+			{
+				int lv = level;
+				ok = ok && set_kernel_args(graph.exec, dequant ? node_idwt_full[level] : node_idwt_only[level], gd, lv,
+				                           din, pout);
+			}
+			if (!ok)
+			{
+				graph.destroy();
+				(void)cudaGetLastError();
+				return false;
+			}
+		}
+		if (!cuda_ok(cudaGraphLaunch(graph.exec, s), "cudaGraphLaunch"))
+			return false;
+		timing.launched(device);
 		decoded_frame_for_current_sequence = true;
+		return true;
 	}
 
 	// Upload the parsed frame and decode it.
@@ -785,8 +1032,9 @@ struct pyrowave_decoder_opaque
 		in.jobs = jobs_d;
 		in.coef32 = coef32;
 		in.coef16 = coef16;
-		run(in, out, s, true);
-		return cudaPeekAtLastError() == cudaSuccess ? PYROWAVE_SUCCESS : PYROWAVE_ERROR_GENERIC;
+		if (!run(in, out, s, true))
+			return PYROWAVE_ERROR_GENERIC;
+		return launches_ok("kernel launch") ? PYROWAVE_SUCCESS : PYROWAVE_ERROR_GENERIC;
 	}
 };
 
@@ -936,6 +1184,14 @@ pyrowave_result pyrowave_device_set_queue_type(pyrowave_device device, VkQueueFl
 }
 
 bool pyrowave_device_confirm_interop_support(pyrowave_device) { return false; }
+
+pyrowave_result pyrowave_cuda_device_set_stage_timing(pyrowave_device device, bool enable)
+{
+	if (!device)
+		return PYROWAVE_ERROR_INVALID_ARGUMENT;
+	device->stage_timing = enable;
+	return PYROWAVE_SUCCESS;
+}
 
 void pyrowave_device_destroy(pyrowave_device device)
 {
@@ -1405,11 +1661,14 @@ pyrowave_result pyrowave_cuda_encoder_encode_pre_transformed(pyrowave_encoder en
 	encoder->sequence_count = (encoder->sequence_count + 1) & 7u;
 	EncodeBuffers b = encoder->buffers();
 	cudaMemsetAsync(encoder->rc, 0, sizeof(RateControlState), s);
-	launch_pyramid_io(g, const_cast<float *>(pyramid), encoder->coef32, encoder->coef16, false, s);
-	launch_quant_pretransformed(g, b, s);
-	launch_resolve(g, b, target_words, encoder->sequence_count, s);
-	launch_pack(g, b, s);
-	if (cudaPeekAtLastError() != cudaSuccess)
+	cudaMemcpyAsync(encoder->g_dev_override, &g, sizeof(Geometry), cudaMemcpyHostToDevice, s);
+	cudaStreamSynchronize(s); // the host copy of the override geometry is a local
+	Geometry *gd = encoder->g_dev_override;
+	launch_pyramid_io(g, gd, const_cast<float *>(pyramid), encoder->coef32, encoder->coef16, false, s);
+	launch_quant_pretransformed(g, gd, b, s);
+	launch_resolve(g, gd, b, target_words, encoder->sequence_count, s);
+	launch_pack(g, gd, b, s);
+	if (!launches_ok("kernel launch"))
 		return PYROWAVE_ERROR_GENERIC;
 	encoder->has_device_frame = true;
 	return encoder->queue_readback(s);
@@ -1419,8 +1678,9 @@ pyrowave_result pyrowave_cuda_encoder_read_wavelet(pyrowave_encoder encoder, flo
 {
 	if (!encoder || !pyramid || !encoder->allocated)
 		return PYROWAVE_ERROR_INVALID_ARGUMENT;
-	launch_pyramid_io(encoder->g, pyramid, encoder->coef32, encoder->coef16, true, pick_stream(encoder->device, stream));
-	return cudaPeekAtLastError() == cudaSuccess ? PYROWAVE_SUCCESS : PYROWAVE_ERROR_GENERIC;
+	launch_pyramid_io(encoder->g, encoder->g_dev, pyramid, encoder->coef32, encoder->coef16, true,
+	                  pick_stream(encoder->device, stream));
+	return launches_ok("kernel launch") ? PYROWAVE_SUCCESS : PYROWAVE_ERROR_GENERIC;
 }
 
 pyrowave_result pyrowave_cuda_encoder_read_debug(pyrowave_encoder encoder, const pyrowave_cuda_encoder_debug *d)
@@ -1498,16 +1758,18 @@ pyrowave_result pyrowave_cuda_decoder_decode_blocks(pyrowave_decoder decoder, co
 	in.jobs = decoder->jobs_d;
 	in.coef32 = decoder->coef32;
 	in.coef16 = decoder->coef16;
-	decoder->run(in, out, pick_stream(decoder->device, stream), true);
-	return cudaPeekAtLastError() == cudaSuccess ? PYROWAVE_SUCCESS : PYROWAVE_ERROR_GENERIC;
+	if (!decoder->run(in, out, pick_stream(decoder->device, stream), true))
+		return PYROWAVE_ERROR_GENERIC;
+	return launches_ok("kernel launch") ? PYROWAVE_SUCCESS : PYROWAVE_ERROR_GENERIC;
 }
 
 pyrowave_result pyrowave_cuda_decoder_read_wavelet(pyrowave_decoder decoder, float *pyramid, pyrowave_cuda_stream stream)
 {
 	if (!decoder || !pyramid || !decoder->allocated)
 		return PYROWAVE_ERROR_INVALID_ARGUMENT;
-	launch_pyramid_io(decoder->g, pyramid, decoder->coef32, decoder->coef16, true, pick_stream(decoder->device, stream));
-	return cudaPeekAtLastError() == cudaSuccess ? PYROWAVE_SUCCESS : PYROWAVE_ERROR_GENERIC;
+	launch_pyramid_io(decoder->g, decoder->g_dev, pyramid, decoder->coef32, decoder->coef16, true,
+	                  pick_stream(decoder->device, stream));
+	return launches_ok("kernel launch") ? PYROWAVE_SUCCESS : PYROWAVE_ERROR_GENERIC;
 }
 
 pyrowave_result pyrowave_cuda_decoder_decode_pyramid(pyrowave_decoder decoder, const float *pyramid,
@@ -1527,12 +1789,13 @@ pyrowave_result pyrowave_cuda_decoder_decode_pyramid(pyrowave_decoder decoder, c
 		out.pitch[p] = int32_t(planes->row_stride_in_bytes[p]);
 	}
 	cudaStream_t s = pick_stream(decoder->device, stream);
-	launch_pyramid_io(decoder->g, const_cast<float *>(pyramid), decoder->coef32, decoder->coef16, false, s);
+	launch_pyramid_io(decoder->g, decoder->g_dev, const_cast<float *>(pyramid), decoder->coef32, decoder->coef16, false, s);
 	DecodeInput in = {};
 	in.jobs = decoder->jobs_d;
 	in.coef32 = decoder->coef32;
 	in.coef16 = decoder->coef16;
-	decoder->run(in, out, s, false);
-	return cudaPeekAtLastError() == cudaSuccess ? PYROWAVE_SUCCESS : PYROWAVE_ERROR_GENERIC;
+	if (!decoder->run(in, out, s, false))
+		return PYROWAVE_ERROR_GENERIC;
+	return launches_ok("kernel launch") ? PYROWAVE_SUCCESS : PYROWAVE_ERROR_GENERIC;
 }
 }

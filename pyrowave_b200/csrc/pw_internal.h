@@ -142,15 +142,15 @@ struct DecodeInput
 };
 
 // Host-side kernel launchers (implemented in the .cu files).
-void launch_dwt_forward_level(const Geometry &g, int level, const PlaneInput &in, const EncodeBuffers &buf,
+void launch_dwt_forward_level(const Geometry &g, const Geometry *gd, int level, const PlaneInput &in, const EncodeBuffers &buf,
                               bool fused_quant, cudaStream_t stream);
-void launch_quant_pretransformed(const Geometry &g, const EncodeBuffers &buf, cudaStream_t stream);
-void launch_resolve(const Geometry &g, const EncodeBuffers &buf, uint32_t target_words, uint32_t sequence,
+void launch_quant_pretransformed(const Geometry &g, const Geometry *gd, const EncodeBuffers &buf, cudaStream_t stream);
+void launch_resolve(const Geometry &g, const Geometry *gd, const EncodeBuffers &buf, uint32_t target_words, uint32_t sequence,
                     cudaStream_t stream);
-void launch_pack(const Geometry &g, const EncodeBuffers &buf, cudaStream_t stream);
-void launch_dequant(const Geometry &g, const DecodeInput &in, cudaStream_t stream);
-void launch_idwt_level(const Geometry &g, int level, const DecodeInput &in, const PlaneOutput &out,
+void launch_pack(const Geometry &g, const Geometry *gd, const EncodeBuffers &buf, cudaStream_t stream);
+void launch_dequant(const Geometry &g, const Geometry *gd, const DecodeInput &in, cudaStream_t stream);
+void launch_idwt_level(const Geometry &g, const Geometry *gd, int level, const DecodeInput &in, const PlaneOutput &out,
                        cudaStream_t stream);
-void launch_pyramid_io(const Geometry &g, float *canonical, float *coef32, __half *coef16, bool to_canonical,
+void launch_pyramid_io(const Geometry &g, const Geometry *gd, float *canonical, float *coef32, __half *coef16, bool to_canonical,
                        cudaStream_t stream);
 } // namespace pw
