@@ -17,7 +17,7 @@ struct PayloadReader
 {
 	const uint32_t *words;
 	uint32_t nwords;
-	__device__ __forceinline__ uint32_t w32(uint32_t i) const { return i < nwords ? __ldg(words + i) : 0u; }
+	__device__ __forceinline__ uint32_t w32(uint32_t i) const { return i < nwords ? __ldcg(words + i) : 0u; }
 	__device__ __forceinline__ uint32_t u8(uint32_t i) const { return (w32(i >> 2) >> (8u * (i & 3u))) & 0xffu; }
 	__device__ __forceinline__ uint32_t u16(uint32_t i) const { return (w32(i >> 1) >> (16u * (i & 1u))) & 0xffffu; }
 };
@@ -32,28 +32,30 @@ __device__ __forceinline__ void store_coef(float *c32, __half *c16, bool fp16, i
 
 // One 32x32 block per 128-thread CTA; thread = one 4x2 sub-block (the
 // reference's mapping, wavelet_dequant.comp:222-238).
-__global__ void __launch_bounds__(128) dequant_kernel(const Geometry *__restrict__ gp, DecodeInput in)
+__global__ void __launch_bounds__(128) dequant_kernel(const BlockParams p, const DecodeInput in)
 {
-	const Geometry &g = *gp;
 	__shared__ uint32_t s_plane_off[16];
 	__shared__ uint32_t s_sign_base;
 	__shared__ uint32_t s_sig[4];
+	pdl_trigger();
 	const int blk = blockIdx.x;
-	int level, comp, band, bx32, by32;
-	unpack_job(in.jobs[blk], level, comp, band, bx32, by32);
-	const LevelDesc &L = g.level[level];
-	const BandDesc &B = g.band[comp][level][band];
+	const int k = find_band(p, blk);
+	const BandEntry &B = p.band[k];
+	const LevelDesc &L = p.level[B.level];
+	const int rel = blk - B.block32_offset;
+	const int by32 = rel / B.block32_stride, bx32 = rel - by32 * B.block32_stride;
 	const bool f16 = L.fp16 != 0;
 	const int t = threadIdx.x, lane = t & 31;
 	const int sub = t & 7, lx = (t >> 3) & 3, ly = t >> 5;
 	const int grp = ly * 4 + lx;
 	const int ox = bx32 * 32 + lx * 8 + sub_x(sub), oy = by32 * 32 + ly * 8 + sub_y(sub);
+	pdl_wait();
 
 	uint32_t off;
 	if (in.offsets)
-		off = in.offsets[blk];
+		off = __ldcg(in.offsets + blk);
 	else
-		off = in.block_meta[2 * blk + 1] ? in.block_meta[2 * blk] : 0xffffffffu;
+		off = __ldcg(in.block_meta + 2 * blk + 1) ? __ldcg(in.block_meta + 2 * blk) : 0xffffffffu;
 
 	if (off == 0xffffffffu)
 	{
@@ -74,18 +76,19 @@ __global__ void __launch_bounds__(128) dequant_kernel(const Geometry *__restrict
 		uint32_t cw = 0, qb = 0;
 		if ((ballot >> t) & 1u)
 		{
-			uint32_t local = uint32_t(__popc(ballot & ((1u << t) - 1u)));
+			const uint32_t local = uint32_t(__popc(ballot & ((1u << t) - 1u)));
 			cw = rd.u16(off * 2 + 4 + local);
 			qb = rd.u8(off * 4 + 8 + n * 2 + local) & 0xfu;
 		}
-		uint32_t lsbs = cw & 0x5555u, msbs = cw & 0xaaaau;
+		const uint32_t lsbs = cw & 0x5555u;
+		uint32_t msbs = cw & 0xaaaau;
 		msbs |= msbs >> 1;
-		uint32_t cost = uint32_t(__popc(lsbs) + __popc(msbs)) + qb * 8u;
+		const uint32_t cost = uint32_t(__popc(lsbs) + __popc(msbs)) + qb * 8u;
 		uint32_t inc = cost;
 #pragma unroll
 		for (int o = 1; o < 16; o *= 2)
 		{
-			uint32_t y = __shfl_up_sync(0x0000ffffu, inc, o);
+			const uint32_t y = __shfl_up_sync(0x0000ffffu, inc, o);
 			if (t >= o)
 				inc += y;
 		}
@@ -112,15 +115,16 @@ __global__ void __launch_bounds__(128) dequant_kernel(const Geometry *__restrict
 			const uint32_t lsbs = cw & 0x5555u;
 			uint32_t msbs = cw & 0xaaaau;
 			msbs |= msbs >> 1;
-			uint32_t byte_offset = uint32_t(__popc(lsbs & mask) + __popc(msbs & mask)) + qb * uint32_t(sub) + s_plane_off[grp];
+			uint32_t byte_offset =
+			    uint32_t(__popc(lsbs & mask) + __popc(msbs & mask)) + qb * uint32_t(sub) + s_plane_off[grp];
 			const int planes = int(qb + ((cw >> (2 * sub)) & 3u));
 			uint32_t dec[8] = {0, 0, 0, 0, 0, 0, 0, 0};
-			for (int p = planes - 1; p >= 0; p--)
+			for (int pl = planes - 1; pl >= 0; pl--)
 			{
-				uint32_t pl = rd.u8(byte_offset++);
+				const uint32_t bits = rd.u8(byte_offset++);
 #pragma unroll
 				for (int i = 0; i < 8; i++)
-					dec[i] |= ((pl >> i) & 1u) << p;
+					dec[i] |= ((bits >> i) & 1u) << pl;
 			}
 #pragma unroll
 			for (int i = 0; i < 8; i++)
@@ -146,7 +150,7 @@ __global__ void __launch_bounds__(128) dequant_kernel(const Geometry *__restrict
 #pragma unroll
 	for (int o = 1; o < 32; o *= 2)
 	{
-		uint32_t y = __shfl_up_sync(0xffffffffu, inc, o);
+		const uint32_t y = __shfl_up_sync(0xffffffffu, inc, o);
 		if (lane >= o)
 			inc += y;
 	}
@@ -161,7 +165,7 @@ __global__ void __launch_bounds__(128) dequant_kernel(const Geometry *__restrict
 	{
 		if (v[i] != 0.0f)
 		{
-			uint32_t bit = (rd.w32(bitpos >> 5) >> (bitpos & 31u)) & 1u;
+			const uint32_t bit = (rd.w32(bitpos >> 5) >> (bitpos & 31u)) & 1u;
 			if (bit)
 				v[i] = -v[i];
 			bitpos++;
@@ -184,16 +188,18 @@ struct IdwtShared
 };
 
 // One inverse level for a 64x64 output tile (32x32 band tile) of one component.
-__global__ void __launch_bounds__(kIdwtThreads) idwt_kernel(const Geometry *__restrict__ gp, int level, DecodeInput in, PlaneOutput out)
+__global__ void __launch_bounds__(kIdwtThreads) idwt_kernel(const LevelParams p, const DecodeInput in,
+                                                             const PlaneOutput out)
 {
-	const Geometry &g = *gp;
 	__shared__ IdwtShared sh;
-	const int comp = (level == 0 && !g.chroma444) ? 0 : int(blockIdx.y);
-	const LevelDesc &L = g.level[level];
+	pdl_trigger();
+	const int level = p.level;
+	const int comp = (level == 0 && !p.chroma444) ? 0 : int(blockIdx.y);
+	const LevelDesc &L = p.L;
 	const int tile = blockIdx.x;
 	const int tx = tile % L.tiles_x, ty = tile / L.tiles_x;
 	const int nx = L.width, ny = L.height;
-	const bool final_level = level == 0 || (level == 1 && comp != 0 && !g.chroma444);
+	const bool final_level = level == 0 || (level == 1 && comp != 0 && !p.chroma444);
 
 	for (int k = threadIdx.x; k < 4 * kBandTile; k += kIdwtThreads)
 	{
@@ -208,11 +214,12 @@ __global__ void __launch_bounds__(kIdwtThreads) idwt_kernel(const Geometry *__re
 		else
 			sh.yh[j] = inv_index_high(py, ny);
 	}
-	__syncthreads();
-
 	const bool f16 = L.fp16 != 0;
-	const int64_t boff[4] = {g.band[comp][level][0].offset, g.band[comp][level][1].offset,
-	                         g.band[comp][level][2].offset, g.band[comp][level][3].offset};
+	const int64_t o0 = p.band[comp][0].offset, o1 = p.band[comp][1].offset, o2 = p.band[comp][2].offset,
+	              o3 = p.band[comp][3].offset;
+	__syncthreads();
+	pdl_wait();
+
 	// Interior tiles read every band sample at its own position: rows of 40
 	// samples from 4 before the tile (16-byte aligned), 10 vectors per row, all
 	// loads in flight at once. Edge tiles use the mirrored index tables.
@@ -236,16 +243,17 @@ __global__ void __launch_bounds__(kIdwtThreads) idwt_kernel(const Geometry *__re
 				v[u] = make_float4(0.f, 0.f, 0.f, 0.f);
 				continue;
 			}
-			const int64_t idx = boff[b] + int64_t(by0 + i) * L.pitch + (bx0 - 2) + 4 * j;
+			const int64_t bo = b == 0 ? o0 : (b == 1 ? o1 : (b == 2 ? o2 : o3));
+			const int64_t idx = bo + int64_t(by0 + i) * L.pitch + (bx0 - 2) + 4 * j;
 			if (f16)
 			{
-				uint2 hv = __ldg(reinterpret_cast<const uint2 *>(in.coef16 + idx));
-				float2 a = __half22float2(*reinterpret_cast<__half2 *>(&hv.x));
-				float2 c = __half22float2(*reinterpret_cast<__half2 *>(&hv.y));
+				uint2 hv = __ldcg(reinterpret_cast<const uint2 *>(in.coef16 + idx));
+				const float2 a = __half22float2(*reinterpret_cast<__half2 *>(&hv.x));
+				const float2 c = __half22float2(*reinterpret_cast<__half2 *>(&hv.y));
 				v[u] = make_float4(a.x, a.y, c.x, c.y);
 			}
 			else
-				v[u] = __ldg(reinterpret_cast<const float4 *>(in.coef32 + idx));
+				v[u] = __ldcg(reinterpret_cast<const float4 *>(in.coef32 + idx));
 		}
 #pragma unroll
 		for (int u = 0; u < kIters; u++)
@@ -281,7 +289,10 @@ __global__ void __launch_bounds__(kIdwtThreads) idwt_kernel(const Geometry *__re
 				const int i = r / kBandTile, j = r - i * kBandTile;
 				const int yy = (b >> 1) ? sh.yh[i] : sh.yl[i];
 				const int xx = (b & 1) ? sh.xh[j] : sh.xl[j];
-				v[u] = k < kN ? load_coef(in.coef32, in.coef16, f16, boff[b & 3] + int64_t(yy) * L.pitch + xx) : 0.0f;
+				const int64_t bo = b == 0 ? o0 : (b == 1 ? o1 : (b == 2 ? o2 : o3));
+				v[u] = k < kN ? (f16 ? __half2float(__ldcg(in.coef16 + bo + int64_t(yy) * L.pitch + xx))
+				                     : __ldcg(in.coef32 + bo + int64_t(yy) * L.pitch + xx))
+				              : 0.0f;
 			}
 #pragma unroll
 			for (int u = 0; u < 8; u++)
@@ -337,7 +348,7 @@ __global__ void __launch_bounds__(kIdwtThreads) idwt_kernel(const Geometry *__re
 		const int gx0 = tx * 64 + seg * 16;
 		if (final_level)
 		{
-			const int pw = g.plane_width[comp], ph = g.plane_height[comp];
+			const int pw = p.plane_width[comp], ph = p.plane_height[comp];
 			uint8_t *const plane = comp == 0 ? out.data[0] : (comp == 1 ? out.data[1] : out.data[2]);
 			const int opitch = comp == 0 ? out.pitch[0] : (comp == 1 ? out.pitch[1] : out.pitch[2]);
 			if (gy < ph)
@@ -365,12 +376,12 @@ __global__ void __launch_bounds__(kIdwtThreads) idwt_kernel(const Geometry *__re
 		}
 		else
 		{
-			const LevelDesc &P = g.level[level - 1];
-			const BandDesc &B = g.band[comp][level - 1][0];
+			const LevelDesc &P = p.P;
+			const int64_t ll = comp == 0 ? p.prev_ll[0] : (comp == 1 ? p.prev_ll[1] : p.prev_ll[2]);
 			const bool pf16 = P.fp16 != 0;
 			if (gy < P.height)
 			{
-				const int64_t base = B.offset + int64_t(gy) * P.pitch + gx0;
+				const int64_t base = ll + int64_t(gy) * P.pitch + gx0;
 				if (gx0 + 16 <= P.width)
 				{
 					if (pf16)
@@ -400,7 +411,7 @@ __global__ void __launch_bounds__(kIdwtThreads) idwt_kernel(const Geometry *__re
 					{
 						const int gx = gx0 + jj - 4;
 						if (gx < P.width)
-							store_coef(in.coef32, in.coef16, pf16, B.offset + int64_t(gy) * P.pitch + gx, e[jj]);
+							store_coef(in.coef32, in.coef16, pf16, ll + int64_t(gy) * P.pitch + gx, e[jj]);
 					}
 				}
 			}
@@ -408,32 +419,26 @@ __global__ void __launch_bounds__(kIdwtThreads) idwt_kernel(const Geometry *__re
 	}
 }
 
-struct BandList
-{
-	int32_t count;
-	int32_t comp[48], level[48], band[48];
-	int64_t canon[48];
-};
-
 // Canonical pyramid (all transmitted bands, band-major, unpadded) <-> padded storage.
-__global__ void pyramid_io_kernel(const Geometry *__restrict__ gp, BandList list, float *canonical, float *coef32, __half *coef16,
+__global__ void pyramid_io_kernel(const BlockParams p, float *canonical, float *coef32, __half *coef16,
                                   int to_canonical)
 {
-	const Geometry &g = *gp;
 	const int k = blockIdx.y;
-	const int comp = list.comp[k], level = list.level[k], band = list.band[k];
-	const LevelDesc &L = g.level[level];
-	const BandDesc &B = g.band[comp][level][band];
+	const BandEntry &B = p.band[k];
+	const LevelDesc &L = p.level[B.level];
+	int64_t canon = 0;
+	for (int j = 0; j < k; j++)
+		canon += int64_t(p.level[p.band[j].level].width) * p.level[p.band[j].level].height;
 	const int64_t n = int64_t(L.width) * L.height;
 	for (int64_t i = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; i < n; i += int64_t(gridDim.x) * blockDim.x)
 	{
 		const int y = int(i / L.width), x = int(i - int64_t(y) * L.width);
 		const int64_t s = B.offset + int64_t(y) * L.pitch + x;
 		if (to_canonical)
-			canonical[list.canon[k] + i] = L.fp16 ? __half2float(coef16[s]) : coef32[s];
+			canonical[canon + i] = L.fp16 ? __half2float(coef16[s]) : coef32[s];
 		else
 		{
-			float v = canonical[list.canon[k] + i];
+			const float v = canonical[canon + i];
 			if (L.fp16)
 				coef16[s] = __float2half_rn(v);
 			else
@@ -443,37 +448,26 @@ __global__ void pyramid_io_kernel(const Geometry *__restrict__ gp, BandList list
 }
 } // namespace
 
-void launch_dequant(const Geometry &g, const Geometry *gd, const DecodeInput &in, cudaStream_t stream)
+void launch_dequant(const BlockParams &p, const DecodeInput &in, bool programmatic, cudaStream_t stream)
 {
-	dequant_kernel<<<g.block_count_32x32, 128, 0, stream>>>(gd, in);
+	LaunchConfig lc(dim3(p.block_count_32x32), dim3(128), stream, programmatic);
+	cudaLaunchKernelEx(&lc.cfg, dequant_kernel, p, in);
 }
 
-void launch_idwt_level(const Geometry &g, const Geometry *gd, int level, const DecodeInput &in, const PlaneOutput &out, cudaStream_t stream)
-{
-	const LevelDesc &L = g.level[level];
-	dim3 grid(L.tiles_x * L.tiles_y, (level == 0 && !g.chroma444) ? 1 : 3);
-	idwt_kernel<<<grid, kIdwtThreads, 0, stream>>>(gd, level, in, out);
-}
-
-void launch_pyramid_io(const Geometry &g, const Geometry *gd, float *canonical, float *coef32, __half *coef16, bool to_canonical,
+void launch_idwt_level(const LevelParams &p, const DecodeInput &in, const PlaneOutput &out, bool programmatic,
                        cudaStream_t stream)
 {
-	BandList list = {};
-	int64_t canon = 0;
-	for (int level = kLevels - 1; level >= 0; level--)
-		for (int comp = 0; comp < kComponents; comp++)
-			for (int band = 0; band < 4; band++)
-			{
-				if (!g.band[comp][level][band].present)
-					continue;
-				list.comp[list.count] = comp;
-				list.level[list.count] = level;
-				list.band[list.count] = band;
-				list.canon[list.count] = canon;
-				list.count++;
-				canon += int64_t(g.level[level].width) * g.level[level].height;
-			}
-	dim3 grid(64, list.count);
-	pyramid_io_kernel<<<grid, 256, 0, stream>>>(gd, list, canonical, coef32, coef16, to_canonical ? 1 : 0);
+	const dim3 grid(p.L.tiles_x * p.L.tiles_y, (p.level == 0 && !p.chroma444) ? 1 : 3);
+	LaunchConfig lc(grid, dim3(kIdwtThreads), stream, programmatic);
+	cudaLaunchKernelEx(&lc.cfg, idwt_kernel, p, in, out);
 }
+
+void launch_pyramid_io(const BlockParams &p, float *canonical, float *coef32, __half *coef16, bool to_canonical,
+                       cudaStream_t stream)
+{
+	pyramid_io_kernel<<<dim3(64, p.nbands), 256, 0, stream>>>(p, canonical, coef32, coef16, to_canonical ? 1 : 0);
+}
+
+const void *kernel_dequant() { return reinterpret_cast<const void *>(&dequant_kernel); }
+const void *kernel_idwt() { return reinterpret_cast<const void *>(&idwt_kernel); }
 } // namespace pw

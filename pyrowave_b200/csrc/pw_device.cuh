@@ -105,6 +105,29 @@ template <int N> __device__ __forceinline__ void lift_inverse(float (&e)[N])
 
 __device__ __forceinline__ float round_to_half(float v) { return __half2float(__float2half_rn(v)); }
 
+// Programmatic dependent launch (sm_90+ griddepcontrol): let the next kernel
+// of the sequence start its prologue now / wait until the previous kernel of
+// the sequence has completed and its writes are visible. Without a
+// programmatic predecessor both are no-ops.
+__device__ __forceinline__ void pdl_trigger() { asm volatile("griddepcontrol.launch_dependents;" ::: "memory"); }
+__device__ __forceinline__ void pdl_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
+
+// Band of a 32x32 block (block index order): the last band whose first block
+// is <= blk, then the block's position in it.
+__device__ __forceinline__ int find_band(const BlockParams &p, int blk)
+{
+	int lo = 0, hi = p.nbands - 1;
+	while (lo < hi)
+	{
+		const int mid = (lo + hi + 1) >> 1;
+		if (p.band[mid].block32_offset <= blk)
+			lo = mid;
+		else
+			hi = mid - 1;
+	}
+	return lo;
+}
+
 __device__ __forceinline__ float load_coef(const float *c32, const __half *c16, bool fp16, int64_t idx)
 {
 	return fp16 ? __half2float(c16[idx]) : c32[idx];

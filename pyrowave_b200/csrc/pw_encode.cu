@@ -33,16 +33,15 @@ struct QuantGroupShared
 //
 // Thread t of the 128-thread group owns one 4x2 sub-block: sub = t & 7,
 // 8x8 column lx = (t >> 3) & 3, 8x8 row ly = t >> 5 (one warp per 8x8 row),
-// exactly the reference's mapping (wavelet_quant.comp:294-306).
+// the reference's mapping (wavelet_quant.comp:294-306).
 //
 // Every thread of the CTA must call this the same number of times (it contains
 // __syncthreads); `active` is false for groups without a block this round.
-__device__ void quant_analyze_block(const float *tile, int tile_pitch, bool active, int t, QuantGroupShared &sh,
-                                    const Geometry &g, int level, int comp, int band, int bx32, int by32,
-                                    const EncodeBuffers &buf)
+__device__ __forceinline__ void quant_analyze_block(const float *tile, int tile_pitch, bool active, int t,
+                                                    QuantGroupShared &sh, const LevelDesc &L, const BandParam &B,
+                                                    int subdivision_shift, int bx32, int by32,
+                                                    const EncodeBuffers &buf)
 {
-	const LevelDesc &L = g.level[level];
-	const BandDesc &B = g.band[comp][level][band];
 	const int sub = t & 7, lx = (t >> 3) & 3, ly = t >> 5;
 	const int lane = threadIdx.x & 31;
 	const int x8 = bx32 * 4 + lx, y8 = by32 * 4 + ly;
@@ -94,10 +93,21 @@ __device__ void quant_analyze_block(const float *tile, int tile_pitch, bool acti
 		shifted0 >>= qp0;
 	}
 	cost_early0 += find_msb(uint32_t(shifted0)) + 1;
+	// compute_square_error (wavelet_quant.comp:113-128) reconstructs each value
+	// quantised at q as trunc((floor(|v| / 2^q) + 0.5) * 2^q) when nonzero. With
+	// m = int(|v|) (|v| < 2^15), floor(|v| / 2^q) = m >> q and, for q >= 1, the
+	// reconstruction is the integer ((m >> q) << q) + 2^(q-1): the same values,
+	// computed without floating-point rounding steps.
+	uint32_t mag[8];
+	float av[8];
 	int nsig0 = 0;
 #pragma unroll
 	for (int i = 0; i < 8; i++)
-		nsig0 += (fabsf(v[i]) >= 1.0f) ? 1 : 0;
+	{
+		av[i] = fabsf(v[i]);
+		mag[i] = uint32_t(int(av[i]));
+		nsig0 += mag[i] != 0u ? 1 : 0;
+	}
 	int csum0 = max(cost_early0 - 1, 0) * 8 + nsig0;
 	csum0 += __shfl_xor_sync(0xffffffffu, csum0, 1);
 	csum0 += __shfl_xor_sync(0xffffffffu, csum0, 2);
@@ -137,19 +147,6 @@ __device__ void quant_analyze_block(const float *tile, int tile_pitch, bool acti
 	if (sub != 0 && sub > msb)
 		d_lo = drop;
 
-	// compute_square_error (wavelet_quant.comp:113-128) reconstructs each value
-	// quantised at q as trunc((floor(|v| / 2^q) + 0.5) * 2^q) when nonzero. With
-	// m = int(|v|) (|v| < 2^15), floor(|v| / 2^q) = m >> q and, for q >= 1, the
-	// reconstruction is the integer ((m >> q) << q) + 2^(q-1): the same values,
-	// computed without floating-point rounding steps.
-	uint32_t mag[8];
-	float av[8];
-#pragma unroll
-	for (int i = 0; i < 8; i++)
-	{
-		av[i] = fabsf(v[i]);
-		mag[i] = uint32_t(int(av[i]));
-	}
 	const int warp_msb = __reduce_max_sync(0xffffffffu, max(msb, 0));
 	for (int q = 1; q <= warp_msb; q++)
 	{
@@ -162,8 +159,8 @@ __device__ void quant_analyze_block(const float *tile, int tile_pitch, bool acti
 			const uint32_t iv = mag[i] >> q;
 			nsig += iv != 0u ? 1 : 0;
 			const float recon = iv != 0u ? float((iv << q) + (1u << (q - 1))) : 0.0f;
-			float err = __fsub_rn(av[i], recon);
-			float sq = __fmul_rn(err, err);
+			const float err = __fsub_rn(av[i], recon);
+			const float sq = __fmul_rn(err, err);
 			if (i < 4)
 				e0 = (i == 0) ? sq : __fadd_rn(e0, sq);
 			else
@@ -174,12 +171,12 @@ __device__ void quant_analyze_block(const float *tile, int tile_pitch, bool acti
 		se = __fadd_rn(se, __shfl_xor_sync(0xffffffffu, se, 2));
 		se = __fadd_rn(se, __shfl_xor_sync(0xffffffffu, se, 4));
 
-		int m = msb - q;
+		const int m = msb - q;
 		int shifted = block4x2_max >> q;
 		int ce = shifted > 0 ? 1 : 0;
 		if (m >= 3)
 		{
-			int qp = m - 2;
+			const int qp = m - 2;
 			ce = qp + 1;
 			shifted >>= qp;
 		}
@@ -191,7 +188,7 @@ __device__ void quant_analyze_block(const float *tile, int tile_pitch, bool acti
 
 		if (q <= msb)
 		{
-			float d = __half2float(__float2half_rn(fminf(se, 60000.0f)));
+			const float d = __half2float(__float2half_rn(fminf(se, 60000.0f)));
 			if (q == sub)
 			{
 				d_lo = d;
@@ -238,14 +235,14 @@ __device__ void quant_analyze_block(const float *tile, int tile_pitch, bool acti
 	if (active && t < 16)
 	{
 		const int i = t;
-		float d = __fadd_rn(__fadd_rn(sh.dist[0][i], sh.dist[1][i]), __fadd_rn(sh.dist[2][i], sh.dist[3][i]));
+		const float d = __fadd_rn(__fadd_rn(sh.dist[0][i], sh.dist[1][i]), __fadd_rn(sh.dist[2][i], sh.dist[3][i]));
 		uint32_t c = sh.cost[0][i] + sh.cost[1][i] + sh.cost[2][i] + sh.cost[3][i];
 		if (c != 0)
 			c += 64;
-		uint32_t rate = (c + 31) >> 5;
+		const uint32_t rate = (c + 31) >> 5;
 		const unsigned m16 = 0x0000ffffu;
-		float d0 = __shfl_sync(m16, d, 0);
-		uint32_t r0 = __shfl_sync(m16, rate, 0);
+		const float d0 = __shfl_sync(m16, d, 0);
+		const uint32_t r0 = __shfl_sync(m16, rate, 0);
 		uint32_t bk = bucket_index(d, float(rate), d0, float(r0));
 		if (i == 0)
 			bk = 0;
@@ -254,11 +251,11 @@ __device__ void quant_analyze_block(const float *tile, int tile_pitch, bool acti
 #pragma unroll
 		for (int off = 1; off < 16; off *= 2)
 		{
-			uint32_t up = __shfl_up_sync(m16, bk, off) + uint32_t(off);
+			const uint32_t up = __shfl_up_sync(m16, bk, off) + uint32_t(off);
 			if (i >= off)
 				bk = max(bk, up);
 		}
-		uint32_t rate_prev = __shfl_up_sync(m16, rate, 1);
+		const uint32_t rate_prev = __shfl_up_sync(m16, rate, 1);
 		const uint32_t block_index = uint32_t(B.block32_offset + by32 * B.block32_stride + bx32);
 		buf.rd_cost[block_index * 16 + i] = uint16_t(rate);
 		buf.rd_bucket[block_index * 16 + i] = uint8_t(bk);
@@ -267,10 +264,10 @@ __device__ void quant_analyze_block(const float *tile, int tile_pitch, bool acti
 			atomicAdd(&buf.rc->consumed, rate);
 		else
 		{
-			uint32_t saving = rate_prev - rate;
+			const uint32_t saving = rate_prev - rate;
 			if (saving != 0)
 			{
-				uint32_t subdivision = block_index >> g.subdivision_shift;
+				const uint32_t subdivision = block_index >> subdivision_shift;
 				atomicAdd(&buf.rc->histogram[bk * kSubdivisions + subdivision], saving);
 			}
 		}
@@ -287,31 +284,37 @@ struct DwtShared
 	QuantGroupShared q[2];
 };
 
+__device__ __forceinline__ float unorm8_centered(uint32_t u)
+{
+	return __fsub_rn(__fdiv_rn(float(u), 255.0f), 0.5f);
+}
+
 // One forward level for one 32x32 band tile of one component (64x64 input
 // samples). grid.x = tile, grid.y = component index among those at this level.
-__global__ void __launch_bounds__(kDwtThreads) dwt_forward_kernel(const Geometry *__restrict__ gp, int level, PlaneInput in,
-                                                                   EncodeBuffers buf, int fused)
+__global__ void __launch_bounds__(kDwtThreads) dwt_forward_kernel(const LevelParams p, const PlaneInput in,
+                                                                   const EncodeBuffers buf, const int fused)
 {
-	const Geometry &g = *gp;
 	__shared__ DwtShared sh;
-	const int comp = (level == 0 && !g.chroma444) ? 0 : int(blockIdx.y);
-	const LevelDesc &L = g.level[level];
+	pdl_trigger();
+	const int level = p.level;
+	const int comp = (level == 0 && !p.chroma444) ? 0 : int(blockIdx.y);
+	const LevelDesc &L = p.L;
 	const int tile = blockIdx.x;
 	const int tx = tile % L.tiles_x, ty = tile / L.tiles_x;
-	const bool from_plane = level == 0 || (level == 1 && comp != 0 && !g.chroma444);
+	const bool from_plane = level == 0 || (level == 1 && comp != 0 && !p.chroma444);
 
 	int res_w, res_h, al_w, al_h;
 	if (from_plane)
 	{
-		res_w = g.plane_width[comp];
-		res_h = g.plane_height[comp];
-		al_w = level == 0 ? g.aligned_width : g.aligned_width >> 1;
-		al_h = level == 0 ? g.aligned_height : g.aligned_height >> 1;
+		res_w = p.plane_width[comp];
+		res_h = p.plane_height[comp];
+		al_w = level == 0 ? p.aligned_width : p.aligned_width >> 1;
+		al_h = level == 0 ? p.aligned_height : p.aligned_height >> 1;
 	}
 	else
 	{
-		res_w = al_w = g.level[level - 1].width;
-		res_h = al_h = g.level[level - 1].height;
+		res_w = al_w = p.P.width;
+		res_h = al_h = p.P.height;
 	}
 
 	for (int k = threadIdx.x; k < 2 * kTileIn; k += kDwtThreads)
@@ -322,6 +325,7 @@ __global__ void __launch_bounds__(kDwtThreads) dwt_forward_kernel(const Geometry
 			sh.yidx[k - kTileIn] = fwd_index(ty * 64 - 4 + (k - kTileIn), res_h, al_h);
 	}
 	__syncthreads();
+	pdl_wait();
 
 	// Tile load. A tile whose 72x72 window lies inside the source maps every
 	// sample to itself: load whole rows with vector loads, all in flight at
@@ -329,15 +333,15 @@ __global__ void __launch_bounds__(kDwtThreads) dwt_forward_kernel(const Geometry
 	// independent loads.
 	const int x0 = tx * 64 - 4, y0 = ty * 64 - 4;
 	const bool interior = x0 >= 0 && y0 >= 0 && x0 + kTileIn <= res_w && y0 + kTileIn <= res_h;
-	constexpr int kVecPerRow = kTileIn / 4;                // 18 vectors of 4 samples
-	constexpr int kVecs = kVecPerRow * kTileIn;            // 1296
+	constexpr int kVecPerRow = kTileIn / 4;     // 18 vectors of 4 samples
+	constexpr int kVecs = kVecPerRow * kTileIn; // 1296
 	constexpr int kVecIters = (kVecs + kDwtThreads - 1) / kDwtThreads;
 	if (from_plane)
 	{
-		const uint8_t *p = comp == 0 ? in.data[0] : (comp == 1 ? in.data[1] : in.data[2]);
+		const uint8_t *src = comp == 0 ? in.data[0] : (comp == 1 ? in.data[1] : in.data[2]);
 		const int pitch = comp == 0 ? in.pitch[0] : (comp == 1 ? in.pitch[1] : in.pitch[2]);
 		const int xs = comp == 0 ? in.xstride[0] : (comp == 1 ? in.xstride[1] : in.xstride[2]);
-		const bool vec_ok = interior && xs == 1 && ((reinterpret_cast<uintptr_t>(p) | uintptr_t(pitch)) & 3u) == 0;
+		const bool vec_ok = interior && xs == 1 && ((reinterpret_cast<uintptr_t>(src) | uintptr_t(pitch)) & 3u) == 0;
 		if (vec_ok)
 		{
 			uint32_t v[kVecIters];
@@ -346,7 +350,7 @@ __global__ void __launch_bounds__(kDwtThreads) dwt_forward_kernel(const Geometry
 			{
 				const int k = threadIdx.x + u * kDwtThreads;
 				const int i = k / kVecPerRow, j = k - i * kVecPerRow;
-				v[u] = k < kVecs ? __ldg(reinterpret_cast<const uint32_t *>(p + size_t(y0 + i) * pitch + x0) + j) : 0u;
+				v[u] = k < kVecs ? __ldg(reinterpret_cast<const uint32_t *>(src + size_t(y0 + i) * pitch + x0) + j) : 0u;
 			}
 #pragma unroll
 			for (int u = 0; u < kVecIters; u++)
@@ -357,7 +361,7 @@ __global__ void __launch_bounds__(kDwtThreads) dwt_forward_kernel(const Geometry
 					const int i = k / kVecPerRow, j = k - i * kVecPerRow;
 #pragma unroll
 					for (int b = 0; b < 4; b++)
-						sh.in[i][4 * j + b] = __fsub_rn(__fdiv_rn(float((v[u] >> (8 * b)) & 0xffu), 255.0f), 0.5f);
+						sh.in[i][4 * j + b] = unorm8_centered((v[u] >> (8 * b)) & 0xffu);
 				}
 			}
 		}
@@ -371,7 +375,7 @@ __global__ void __launch_bounds__(kDwtThreads) dwt_forward_kernel(const Geometry
 				{
 					const int k = base + u * kDwtThreads;
 					const int i = k / kTileIn, j = k - i * kTileIn;
-					v[u] = k < kTileIn * kTileIn ? p[size_t(sh.yidx[i]) * pitch + size_t(sh.xidx[j]) * xs] : 0u;
+					v[u] = k < kTileIn * kTileIn ? src[size_t(sh.yidx[i]) * pitch + size_t(sh.xidx[j]) * xs] : 0u;
 				}
 #pragma unroll
 				for (int u = 0; u < 8; u++)
@@ -380,7 +384,7 @@ __global__ void __launch_bounds__(kDwtThreads) dwt_forward_kernel(const Geometry
 					if (k < kTileIn * kTileIn)
 					{
 						const int i = k / kTileIn, j = k - i * kTileIn;
-						sh.in[i][j] = __fsub_rn(__fdiv_rn(float(v[u]), 255.0f), 0.5f);
+						sh.in[i][j] = unorm8_centered(v[u]);
 					}
 				}
 			}
@@ -388,8 +392,8 @@ __global__ void __launch_bounds__(kDwtThreads) dwt_forward_kernel(const Geometry
 	}
 	else
 	{
-		const LevelDesc &P = g.level[level - 1];
-		const BandDesc &B = g.band[comp][level - 1][0];
+		const LevelDesc &P = p.P;
+		const int64_t ll = comp == 0 ? p.prev_ll[0] : (comp == 1 ? p.prev_ll[1] : p.prev_ll[2]);
 		const bool f16 = P.fp16 != 0;
 		if (interior)
 		{
@@ -399,18 +403,18 @@ __global__ void __launch_bounds__(kDwtThreads) dwt_forward_kernel(const Geometry
 			{
 				const int k = threadIdx.x + u * kDwtThreads;
 				const int i = k / kVecPerRow, j = k - i * kVecPerRow;
-				const int64_t idx = B.offset + int64_t(y0 + i) * P.pitch + x0 + 4 * j;
+				const int64_t idx = ll + int64_t(y0 + i) * P.pitch + x0 + 4 * j;
 				if (k >= kVecs)
 					v[u] = make_float4(0.f, 0.f, 0.f, 0.f);
 				else if (f16)
 				{
-					uint2 hv = __ldg(reinterpret_cast<const uint2 *>(buf.coef16 + idx));
-					float2 a = __half22float2(*reinterpret_cast<__half2 *>(&hv.x));
-					float2 b = __half22float2(*reinterpret_cast<__half2 *>(&hv.y));
+					uint2 hv = __ldcg(reinterpret_cast<const uint2 *>(buf.coef16 + idx));
+					const float2 a = __half22float2(*reinterpret_cast<__half2 *>(&hv.x));
+					const float2 b = __half22float2(*reinterpret_cast<__half2 *>(&hv.y));
 					v[u] = make_float4(a.x, a.y, b.x, b.y);
 				}
 				else
-					v[u] = __ldg(reinterpret_cast<const float4 *>(buf.coef32 + idx));
+					v[u] = __ldcg(reinterpret_cast<const float4 *>(buf.coef32 + idx));
 			}
 #pragma unroll
 			for (int u = 0; u < kVecIters; u++)
@@ -437,7 +441,7 @@ __global__ void __launch_bounds__(kDwtThreads) dwt_forward_kernel(const Geometry
 					const int k = base + u * kDwtThreads;
 					const int i = k / kTileIn, j = k - i * kTileIn;
 					v[u] = k < kTileIn * kTileIn
-					           ? load_coef(buf.coef32, buf.coef16, f16, B.offset + int64_t(sh.yidx[i]) * P.pitch + sh.xidx[j])
+					           ? load_coef(buf.coef32, buf.coef16, f16, ll + int64_t(sh.yidx[i]) * P.pitch + sh.xidx[j])
 					           : 0.0f;
 				}
 #pragma unroll
@@ -509,10 +513,10 @@ __global__ void __launch_bounds__(kDwtThreads) dwt_forward_kernel(const Geometry
 	// Store all four bands (LL feeds the next level).
 	{
 		const int r = threadIdx.x >> 3, c4 = (threadIdx.x & 7) * 4;
+#pragma unroll
 		for (int b = 0; b < 4; b++)
 		{
-			const BandDesc &B = g.band[comp][level][b];
-			const int64_t idx = B.offset + int64_t(ty * 32 + r) * L.pitch + tx * 32 + c4;
+			const int64_t idx = p.band[comp][b].offset + int64_t(ty * 32 + r) * L.pitch + tx * 32 + c4;
 			if (L.fp16)
 			{
 				__half2 h0 = __floats2half2_rn(bands[b][r][c4 + 0], bands[b][r][c4 + 1]);
@@ -542,37 +546,48 @@ __global__ void __launch_bounds__(kDwtThreads) dwt_forward_kernel(const Geometry
 		const int bi = round * 2 + grp;
 		const bool active = bi < nb;
 		const int band = active ? first_band + bi : first_band;
-		quant_analyze_block(&bands[band][0][0], kBandPitch, active, t, sh.q[grp], g, level, comp, band, tx, ty, buf);
+		quant_analyze_block(&bands[band][0][0], kBandPitch, active, t, sh.q[grp], L, p.band[comp][band],
+		                    p.subdivision_shift, tx, ty, buf);
 	}
 }
 
 // Quantiser over a pyramid already in storage (the reference's
 // Encoder::encode_pre_transformed, pyrowave_encoder.cpp:1138-1151).
 // Two 32x32 blocks per CTA.
-__global__ void __launch_bounds__(256) quant_pretransformed_kernel(const Geometry *__restrict__ gp, EncodeBuffers buf)
+__global__ void __launch_bounds__(256) quant_pretransformed_kernel(const BlockParams p, const EncodeBuffers buf)
 {
-	const Geometry &g = *gp;
 	__shared__ float tile[2][32][kBandPitch];
 	__shared__ QuantGroupShared q[2];
+	pdl_trigger();
 	const int grp = threadIdx.x >> 7, t = threadIdx.x & 127;
 	const int b = blockIdx.x * 2 + grp;
-	const bool active = b < g.block_count_32x32;
-	int level = 0, comp = 0, band = 1, bx = 0, by = 0;
-	if (active)
-		unpack_job(buf.jobs[b], level, comp, band, bx, by);
+	const bool active = b < p.block_count_32x32;
+	const int k = active ? find_band(p, b) : 0;
+	const BandEntry &E = p.band[k];
+	const LevelDesc &L = p.level[E.level];
+	const int rel = b - E.block32_offset;
+	const int by = rel / E.block32_stride, bx = rel - by * E.block32_stride;
+	pdl_wait();
 	if (active)
 	{
-		const LevelDesc &L = g.level[level];
-		const BandDesc &B = g.band[comp][level][band];
-		for (int k = t; k < 1024; k += 128)
+		for (int i = t; i < 1024; i += 128)
 		{
-			int r = k >> 5, c = k & 31;
-			int64_t idx = B.offset + int64_t(by * 32 + r) * L.pitch + bx * 32 + c;
+			const int r = i >> 5, c = i & 31;
+			const int64_t idx = E.offset + int64_t(by * 32 + r) * L.pitch + bx * 32 + c;
 			tile[grp][r][c] = load_coef(buf.coef32, buf.coef16, L.fp16 != 0, idx);
 		}
 	}
 	__syncthreads();
-	quant_analyze_block(&tile[grp][0][0], kBandPitch, active, t, q[grp], g, level, comp, band, bx, by, buf);
+	BandParam B;
+	B.offset = E.offset;
+	B.block8_offset = E.block8_offset;
+	B.block8_stride = E.block8_stride;
+	B.block32_offset = E.block32_offset;
+	B.block32_stride = E.block32_stride;
+	B.quant_resolution = E.quant_resolution;
+	B.rdo_scale = E.rdo_scale;
+	B.quant_code = E.quant_code;
+	quant_analyze_block(&tile[grp][0][0], kBandPitch, active, t, q[grp], L, B, p.subdivision_shift, bx, by, buf);
 }
 
 // ---------------------------------------------------------------------------
@@ -585,7 +600,7 @@ __device__ __forceinline__ uint32_t block_exclusive_scan_1024(uint32_t v, uint32
 #pragma unroll
 	for (int off = 1; off < 32; off *= 2)
 	{
-		uint32_t y = __shfl_up_sync(0xffffffffu, x, off);
+		const uint32_t y = __shfl_up_sync(0xffffffffu, x, off);
 		if (lane >= off)
 			x += y;
 	}
@@ -598,14 +613,14 @@ __device__ __forceinline__ uint32_t block_exclusive_scan_1024(uint32_t v, uint32
 #pragma unroll
 		for (int off = 1; off < 32; off *= 2)
 		{
-			uint32_t y = __shfl_up_sync(0xffffffffu, s, off);
+			const uint32_t y = __shfl_up_sync(0xffffffffu, s, off);
 			if (lane >= off)
 				s += y;
 		}
 		warp_sums[lane] = s;
 	}
 	__syncthreads();
-	uint32_t base = warp == 0 ? 0u : warp_sums[warp - 1];
+	const uint32_t base = warp == 0 ? 0u : warp_sums[warp - 1];
 	total = warp_sums[31];
 	__syncthreads();
 	return base + x - v;
@@ -620,9 +635,9 @@ struct BlockRD
 
 __device__ __forceinline__ void load_block_rd(const EncodeBuffers &buf, int blk, BlockRD &rd)
 {
-	const uint4 c0 = __ldg(reinterpret_cast<const uint4 *>(buf.rd_cost + size_t(blk) * 16));
-	const uint4 c1 = __ldg(reinterpret_cast<const uint4 *>(buf.rd_cost + size_t(blk) * 16) + 1);
-	const uint4 bb = __ldg(reinterpret_cast<const uint4 *>(buf.rd_bucket + size_t(blk) * 16));
+	const uint4 c0 = __ldcg(reinterpret_cast<const uint4 *>(buf.rd_cost + size_t(blk) * 16));
+	const uint4 c1 = __ldcg(reinterpret_cast<const uint4 *>(buf.rd_cost + size_t(blk) * 16) + 1);
+	const uint4 bb = __ldcg(reinterpret_cast<const uint4 *>(buf.rd_bucket + size_t(blk) * 16));
 	const uint32_t cw[8] = {c0.x, c0.y, c0.z, c0.w, c1.x, c1.y, c1.z, c1.w};
 	const uint32_t bw[4] = {bb.x, bb.y, bb.z, bb.w};
 #pragma unroll
@@ -682,22 +697,23 @@ __device__ __forceinline__ uint32_t block_words(const EncodeBuffers &buf, int bl
 // not at all, and x* up to the first operation whose exclusive prefix reaches
 // its requirement. This kernel computes x* and that cut, then gives every
 // block its quant (the largest applied step), its word count and its offset.
-__global__ void __launch_bounds__(1024) resolve_kernel(const Geometry *__restrict__ gp, EncodeBuffers buf, uint32_t target_words,
-                                                      uint32_t sequence)
+__global__ void __launch_bounds__(1024) resolve_kernel(const ResolveParams p, const EncodeBuffers buf)
 {
-	const Geometry &g = *gp;
 	__shared__ uint32_t scan[kHistSize];
 	__shared__ uint32_t warp_sums[32];
 	__shared__ int s_xstar;
 	__shared__ uint32_t s_cut;
+	pdl_trigger();
 	RateControlState *rc = buf.rc;
 	const int t = threadIdx.x;
-	const int nblocks = g.block_count_32x32;
-	const int nbps = g.blocks_per_subdivision;
+	const int nblocks = p.block_count_32x32;
+	const int nbps = p.blocks_per_subdivision;
+	pdl_wait();
 
-	uint32_t a = rc->histogram[2 * t], b = rc->histogram[2 * t + 1];
+	const uint32_t a = __ldcg(&rc->histogram[2 * t]), b = __ldcg(&rc->histogram[2 * t + 1]);
+	const uint32_t consumed = __ldcg(&rc->consumed);
 	uint32_t total;
-	uint32_t excl = block_exclusive_scan_1024(a + b, warp_sums, total);
+	const uint32_t excl = block_exclusive_scan_1024(a + b, warp_sums, total);
 	scan[2 * t] = excl + a;
 	scan[2 * t + 1] = excl + a + b;
 	if (t == 0)
@@ -707,7 +723,7 @@ __global__ void __launch_bounds__(1024) resolve_kernel(const Geometry *__restric
 	}
 	__syncthreads();
 
-	const int64_t need = int64_t(rc->consumed) - int64_t(target_words);
+	const int64_t need = int64_t(consumed) - int64_t(p.target_words);
 	if (need > 0)
 	{
 		for (int x = 2 * t; x < 2 * t + 2; x++)
@@ -719,15 +735,14 @@ __global__ void __launch_bounds__(1024) resolve_kernel(const Geometry *__restric
 
 	// Each thread owns a contiguous run of blocks, so every pass below needs
 	// only one block-wide scan.
-	const int xstar_sdiv = xstar & (kSubdivisions - 1);
 	if (xstar >= 0)
 	{
 		const int64_t required = need - (xstar > 0 ? int64_t(scan[xstar - 1]) : 0);
 		const uint32_t bk = uint32_t(xstar >> 4);
-		const int start = xstar_sdiv * nbps;
+		const int start = (xstar & (kSubdivisions - 1)) * nbps;
 		const int end = min(start + nbps, nblocks);
-		const int per = (end - start + 1023) / 1024;
-		const int b0 = start + t * per, b1 = min(b0 + per, end);
+		const int per = max(end - start + 1023, 0) / 1024;
+		const int b0 = min(start + t * per, max(end, start)), b1 = min(b0 + per, end);
 		uint32_t local = 0;
 		for (int blk = b0; blk < b1; blk++)
 			local += op_saving_at_bucket(buf, blk, bk);
@@ -753,7 +768,7 @@ __global__ void __launch_bounds__(1024) resolve_kernel(const Geometry *__restric
 	for (int blk = b0; blk < b1; blk++)
 	{
 		int q;
-		const uint32_t words = block_words(buf, blk, blk >> g.subdivision_shift, xstar, cut, q);
+		const uint32_t words = block_words(buf, blk, blk >> p.subdivision_shift, xstar, cut, q);
 		buf.quant[blk] = q;
 		buf.block_meta[2 * blk + 0] = local;
 		buf.block_meta[2 * blk + 1] = words;
@@ -773,55 +788,57 @@ __global__ void __launch_bounds__(1024) resolve_kernel(const Geometry *__restric
 		rc->non_zero_blocks = non_zero;
 		rc->xstar = xstar;
 		rc->block_cut = cut;
-		rc->sequence = sequence & 7u;
+		rc->sequence = p.sequence & 7u;
 		if (2 + carry > buf.stream_capacity_words)
 			rc->error |= 1u;
 		// Start-of-frame sequence header (bitstream.md:250-265).
-		buf.stream[0] = uint32_t(g.width - 1) | (uint32_t(g.height - 1) << 14) | ((sequence & 7u) << 28) | (1u << 31);
-		buf.stream[1] = (non_zero & 0xffffffu) | (uint32_t(g.chroma444 ? 1 : 0) << 26);
+		buf.stream[0] = uint32_t(p.width - 1) | (uint32_t(p.height - 1) << 14) | ((p.sequence & 7u) << 28) | (1u << 31);
+		buf.stream[1] = (non_zero & 0xffffffu) | (uint32_t(p.chroma444 ? 1 : 0) << 26);
 	}
 }
 
 // ---------------------------------------------------------------------------
 // Block packing: one 32x32 block per 128-thread CTA, assembled in shared
 // memory and written as whole words at its prefix-scanned offset.
-__global__ void __launch_bounds__(128) pack_kernel(const Geometry *__restrict__ gp, EncodeBuffers buf)
+__global__ void __launch_bounds__(128) pack_kernel(const BlockParams p, const EncodeBuffers buf)
 {
-	const Geometry &g = *gp;
 	__shared__ uint32_t pkt[kMaxBlockWords];
 	__shared__ uint32_t s_ballot[4];
 	__shared__ uint32_t s_bytes[16];
 	__shared__ uint32_t s_sig[4];
+	pdl_trigger();
 	const int blk = blockIdx.x;
-	const uint32_t words = buf.block_meta[2 * blk + 1];
-	if (words == 0)
-		return;
-	const uint32_t offset = buf.block_meta[2 * blk + 0];
-	const int quant = buf.quant[blk];
-	int level, comp, band, bx32, by32;
-	unpack_job(buf.jobs[blk], level, comp, band, bx32, by32);
-	const LevelDesc &L = g.level[level];
-	const BandDesc &B = g.band[comp][level][band];
-
+	const int k = find_band(p, blk);
+	const BandEntry &B = p.band[k];
+	const LevelDesc &L = p.level[B.level];
+	const int rel = blk - B.block32_offset;
+	const int by32 = rel / B.block32_stride, bx32 = rel - by32 * B.block32_stride;
 	const int t = threadIdx.x, lane = t & 31;
 	const int sub = t & 7, lx = (t >> 3) & 3, ly = t >> 5;
 	const int grp = ly * 4 + lx;
 	const int x8 = bx32 * 4 + lx, y8 = by32 * 4 + ly;
 	const bool in_range = x8 < L.blocks8_x && y8 < L.blocks8_y;
-	const uint32_t cw0 = in_range ? buf.code_words[B.block8_offset + y8 * B.block8_stride + x8] : 0u;
+	const int ox = bx32 * 32 + lx * 8 + sub_x(sub), oy = by32 * 32 + ly * 8 + sub_y(sub);
+	pdl_wait();
+
+	const uint32_t words = __ldcg(&buf.block_meta[2 * blk + 1]);
+	if (words == 0)
+		return;
+	const uint32_t offset = __ldcg(&buf.block_meta[2 * blk + 0]);
+	const int quant = __ldcg(&buf.quant[blk]);
+	const uint32_t cw0 = in_range ? __ldcg(&buf.code_words[B.block8_offset + y8 * B.block8_stride + x8]) : 0u;
 	const uint32_t cw = quantize_code_word(cw0, quant);
 	const bool active = (cw & 0xffffu) != 0;
 
 	// Re-quantise this sub-block exactly as the quantiser did.
 	const float qs = __fdiv_rn(1.0f, decode_quant_scale((cw0 >> kQuantScaleOffset) & 0xfu));
-	const int ox = bx32 * 32 + lx * 8 + sub_x(sub), oy = by32 * 32 + ly * 8 + sub_y(sub);
 	uint32_t mag[8];
 	uint32_t neg = 0;
 #pragma unroll
 	for (int i = 0; i < 8; i++)
 	{
-		float c = load_coef(buf.coef32, buf.coef16, L.fp16 != 0,
-		                    B.offset + int64_t(oy + (i & 1)) * L.pitch + ox + (i >> 1));
+		const int64_t idx = B.offset + int64_t(oy + (i & 1)) * L.pitch + ox + (i >> 1);
+		const float c = L.fp16 ? __half2float(__ldcg(buf.coef16 + idx)) : __ldcg(buf.coef32 + idx);
 		float v = __fmul_rn(__fmul_rn(c, B.quant_resolution), qs);
 		v = fminf(fmaxf(v, -kMaxScaledMagnitude), kMaxScaledMagnitude);
 		mag[i] = uint32_t(abs(int(v)));
@@ -851,7 +868,7 @@ __global__ void __launch_bounds__(128) pack_kernel(const Geometry *__restrict__ 
 #pragma unroll
 	for (int off = 1; off < 32; off *= 2)
 	{
-		uint32_t y = __shfl_up_sync(0xffffffffu, inc, off);
+		const uint32_t y = __shfl_up_sync(0xffffffffu, inc, off);
 		if (lane >= off)
 			inc += y;
 	}
@@ -862,23 +879,24 @@ __global__ void __launch_bounds__(128) pack_kernel(const Geometry *__restrict__ 
 #pragma unroll
 	for (int off = 1; off < 8; off *= 2)
 	{
-		uint32_t y = __shfl_up_sync(0xffffffffu, pinc, off);
+		const uint32_t y = __shfl_up_sync(0xffffffffu, pinc, off);
 		if (sub >= off)
 			pinc += y;
 	}
 	const uint32_t sub_plane_offset = pinc - planes;
-	for (int w = t; w < int(words); w += 128)
+	for (int w = t; w < int(words) && w < kMaxBlockWords; w += 128)
 		pkt[w] = 0u;
 	__syncthreads();
 
 	const uint32_t ballot = s_ballot[0] | (s_ballot[1] << 4) | (s_ballot[2] << 8) | (s_ballot[3] << 12);
 	const uint32_t n = uint32_t(__popc(ballot));
 	uint32_t excl_bytes = 0, total_bytes = 0;
-	for (int k = 0; k < 16; k++)
+#pragma unroll
+	for (int g16 = 0; g16 < 16; g16++)
 	{
-		if (k < grp)
-			excl_bytes += s_bytes[k];
-		total_bytes += s_bytes[k];
+		if (g16 < grp)
+			excl_bytes += s_bytes[g16];
+		total_bytes += s_bytes[g16];
 	}
 	uint32_t sig_base = 0;
 	for (int w = 0; w < ly; w++)
@@ -889,26 +907,26 @@ __global__ void __launch_bounds__(128) pack_kernel(const Geometry *__restrict__ 
 	uint8_t *bytes = reinterpret_cast<uint8_t *>(pkt);
 	if (t == 0)
 	{
-		pkt[0] = (ballot & 0xffffu) | (words << 16) | ((buf.rc->sequence & 7u) << 28);
+		pkt[0] = (ballot & 0xffffu) | (words << 16) | ((__ldcg(&buf.rc->sequence) & 7u) << 28);
 		pkt[1] = modify_quant_code(B.quant_code, quant) | (uint32_t(blk) << 8);
 	}
 	if (active && sub == 0)
 	{
-		uint32_t compact = uint32_t(__popc(ballot & ((1u << grp) - 1u)));
+		const uint32_t compact = uint32_t(__popc(ballot & ((1u << grp) - 1u)));
 		bytes[8 + 2 * compact + 0] = uint8_t(cw);
 		bytes[8 + 2 * compact + 1] = uint8_t(cw >> 8);
 		bytes[8 + 2 * n + compact] = uint8_t(cw >> 16);
 	}
 	const uint32_t plane_base = 8 + 3 * n + excl_bytes + sub_plane_offset;
-	for (uint32_t p = 0; p < planes; p++)
+	for (uint32_t pl = 0; pl < planes; pl++)
 	{
-		const uint32_t bit = uint32_t(quant) + planes - 1u - p; // most significant plane first
+		const uint32_t bit = uint32_t(quant) + planes - 1u - pl; // most significant plane first
 		uint32_t by = 0;
 #pragma unroll
 		for (int i = 0; i < 8; i++)
 			by |= ((mag[i] >> bit) & 1u) << i;
-		if (plane_base + p < uint32_t(kMaxBlockWords) * 4)
-			bytes[plane_base + p] = uint8_t(by);
+		if (plane_base + pl < uint32_t(kMaxBlockWords) * 4)
+			bytes[plane_base + pl] = uint8_t(by);
 	}
 	__syncthreads();
 
@@ -929,38 +947,57 @@ __global__ void __launch_bounds__(128) pack_kernel(const Geometry *__restrict__ 
 	// The word count must match the rate-control estimate the offsets were built from.
 	const uint32_t bits = 8 * (3 * n + total_bytes) + total_sig;
 	const uint32_t expect = (bits + 31) / 32 + 2;
-	if (t == 0 && (expect != words || words > uint32_t(kMaxBlockWords) ||
-	               2 + offset + words > buf.stream_capacity_words))
+	const bool fits = words <= uint32_t(kMaxBlockWords) && 2 + offset + words <= buf.stream_capacity_words;
+	if (t == 0 && (expect != words || !fits))
 		atomicOr(&buf.rc->error, 2u);
-	if (words > uint32_t(kMaxBlockWords) || 2 + offset + words > buf.stream_capacity_words)
+	if (!fits)
 		return;
 	uint32_t *dst = buf.stream + 2 + offset;
 	for (int w = t; w < int(words); w += 128)
 		dst[w] = pkt[w];
 }
+
 } // namespace
 
-void launch_dwt_forward_level(const Geometry &g, const Geometry *gd, int level, const PlaneInput &in, const EncodeBuffers &buf,
-                              bool fused_quant, cudaStream_t stream)
+LaunchConfig::LaunchConfig(dim3 grid, dim3 block, cudaStream_t stream, bool programmatic)
 {
-	const LevelDesc &L = g.level[level];
-	dim3 grid(L.tiles_x * L.tiles_y, (level == 0 && !g.chroma444) ? 1 : 3);
-	dwt_forward_kernel<<<grid, kDwtThreads, 0, stream>>>(gd, level, in, buf, fused_quant ? 1 : 0);
+	cfg = {};
+	cfg.gridDim = grid;
+	cfg.blockDim = block;
+	cfg.dynamicSmemBytes = 0;
+	cfg.stream = stream;
+	attr.id = cudaLaunchAttributeProgrammaticStreamSerialization;
+	attr.val.programmaticStreamSerializationAllowed = 1;
+	cfg.attrs = programmatic ? &attr : nullptr;
+	cfg.numAttrs = programmatic ? 1 : 0;
 }
 
-void launch_quant_pretransformed(const Geometry &g, const Geometry *gd, const EncodeBuffers &buf, cudaStream_t stream)
+void launch_dwt_forward_level(const LevelParams &p, const PlaneInput &in, const EncodeBuffers &buf, bool fused_quant,
+                              bool programmatic, cudaStream_t stream)
 {
-	quant_pretransformed_kernel<<<(g.block_count_32x32 + 1) / 2, 256, 0, stream>>>(gd, buf);
+	const dim3 grid(p.L.tiles_x * p.L.tiles_y, (p.level == 0 && !p.chroma444) ? 1 : 3);
+	LaunchConfig lc(grid, dim3(kDwtThreads), stream, programmatic);
+	cudaLaunchKernelEx(&lc.cfg, dwt_forward_kernel, p, in, buf, fused_quant ? 1 : 0);
 }
 
-void launch_resolve(const Geometry &g, const Geometry *gd, const EncodeBuffers &buf, uint32_t target_words, uint32_t sequence,
-                    cudaStream_t stream)
+void launch_quant_pretransformed(const BlockParams &p, const EncodeBuffers &buf, cudaStream_t stream)
 {
-	resolve_kernel<<<1, 1024, 0, stream>>>(gd, buf, target_words, sequence);
+	LaunchConfig lc(dim3((p.block_count_32x32 + 1) / 2), dim3(256), stream, true);
+	cudaLaunchKernelEx(&lc.cfg, quant_pretransformed_kernel, p, buf);
 }
 
-void launch_pack(const Geometry &g, const Geometry *gd, const EncodeBuffers &buf, cudaStream_t stream)
+void launch_resolve(const ResolveParams &p, const EncodeBuffers &buf, cudaStream_t stream)
 {
-	pack_kernel<<<g.block_count_32x32, 128, 0, stream>>>(gd, buf);
+	LaunchConfig lc(dim3(1), dim3(1024), stream, true);
+	cudaLaunchKernelEx(&lc.cfg, resolve_kernel, p, buf);
 }
+
+void launch_pack(const BlockParams &p, const EncodeBuffers &buf, cudaStream_t stream)
+{
+	LaunchConfig lc(dim3(p.block_count_32x32), dim3(128), stream, true);
+	cudaLaunchKernelEx(&lc.cfg, pack_kernel, p, buf);
+}
+
+const void *kernel_dwt_forward() { return reinterpret_cast<const void *>(&dwt_forward_kernel); }
+const void *kernel_resolve() { return reinterpret_cast<const void *>(&resolve_kernel); }
 } // namespace pw

@@ -270,6 +270,91 @@ struct StageTimer
 } // namespace
 
 // ---------------------------------------------------------------------------
+// Kernel parameter blocks derived from the geometry.
+namespace pw
+{
+static BandParam band_param(const Geometry &g, int comp, int level, int band)
+{
+	const BandDesc &B = g.band[comp][level][band];
+	BandParam p = {};
+	p.offset = B.offset;
+	p.block8_offset = B.block8_offset;
+	p.block8_stride = B.block8_stride;
+	p.block32_offset = B.block32_offset;
+	p.block32_stride = B.block32_stride;
+	p.quant_resolution = B.quant_resolution;
+	p.rdo_scale = B.rdo_scale;
+	p.quant_code = B.quant_code;
+	return p;
+}
+
+LevelParams make_level_params(const Geometry &g, int level)
+{
+	LevelParams p = {};
+	p.L = g.level[level];
+	p.P = level > 0 ? g.level[level - 1] : g.level[0];
+	p.level = level;
+	p.chroma444 = g.chroma444;
+	p.subdivision_shift = g.subdivision_shift;
+	p.width = g.width;
+	p.height = g.height;
+	p.aligned_width = g.aligned_width;
+	p.aligned_height = g.aligned_height;
+	for (int c = 0; c < 3; c++)
+	{
+		p.plane_width[c] = g.plane_width[c];
+		p.plane_height[c] = g.plane_height[c];
+		p.prev_ll[c] = level > 0 ? g.band[c][level - 1][0].offset : 0;
+		for (int b = 0; b < 4; b++)
+			p.band[c][b] = band_param(g, c, level, b);
+	}
+	return p;
+}
+
+BlockParams make_block_params(const Geometry &g)
+{
+	BlockParams p = {};
+	for (int level = 0; level < kLevels; level++)
+		p.level[level] = g.level[level];
+	p.block_count_32x32 = g.block_count_32x32;
+	p.subdivision_shift = g.subdivision_shift;
+	for (int level = kLevels - 1; level >= 0; level--)
+		for (int comp = 0; comp < kComponents; comp++)
+			for (int band = 0; band < 4; band++)
+			{
+				const BandDesc &B = g.band[comp][level][band];
+				if (!B.present || p.nbands >= kMaxBands)
+					continue;
+				BandEntry &e = p.band[p.nbands++];
+				e.offset = B.offset;
+				e.block32_offset = B.block32_offset;
+				e.block32_stride = B.block32_stride;
+				e.block8_offset = B.block8_offset;
+				e.block8_stride = B.block8_stride;
+				e.quant_resolution = B.quant_resolution;
+				e.quant_code = B.quant_code;
+				e.rdo_scale = B.rdo_scale;
+				e.level = level;
+			}
+	return p;
+}
+
+ResolveParams make_resolve_params(const Geometry &g, uint32_t target_words, uint32_t sequence)
+{
+	ResolveParams p = {};
+	p.block_count_32x32 = g.block_count_32x32;
+	p.blocks_per_subdivision = g.blocks_per_subdivision;
+	p.subdivision_shift = g.subdivision_shift;
+	p.width = g.width;
+	p.height = g.height;
+	p.chroma444 = g.chroma444;
+	p.target_words = target_words;
+	p.sequence = sequence;
+	return p;
+}
+} // namespace pw
+
+// ---------------------------------------------------------------------------
 struct pyrowave_device_opaque
 {
 	int cuda_device = 0;
@@ -444,8 +529,8 @@ struct pyrowave_encoder_opaque
 	uint32_t fp16_mask = 0;
 	bool allocated = false;
 
-	Geometry *g_dev = nullptr;          // device copy of g read by the kernels
-	Geometry *g_dev_override = nullptr; // per-call copy for encode_pre_transformed
+	LevelParams lp[kLevels] = {}; // kernel parameter blocks derived from g
+	BlockParams bp = {};
 	float *coef32 = nullptr;
 	__half *coef16 = nullptr;
 	uint32_t *code_words = nullptr;
@@ -496,8 +581,6 @@ struct pyrowave_encoder_opaque
 	{
 		if (device)
 			cudaStreamSynchronize(device->stream);
-		dev_free(g_dev);
-		dev_free(g_dev_override);
 		dev_free(coef32);
 		dev_free(coef16);
 		dev_free(code_words);
@@ -519,7 +602,6 @@ struct pyrowave_encoder_opaque
 		done = nullptr;
 		timing.destroy();
 		graph.destroy();
-		g_dev = g_dev_override = nullptr;
 		coef32 = nullptr;
 		coef16 = nullptr;
 		code_words = nullptr;
@@ -546,9 +628,10 @@ struct pyrowave_encoder_opaque
 			return PYROWAVE_SUCCESS;
 		if (!build_geometry(g, jobs, g.width, g.height, g.chroma444 != 0, fp16_mask))
 			return PYROWAVE_ERROR_INVALID_ARGUMENT;
+		for (int level = 0; level < kLevels; level++)
+			lp[level] = make_level_params(g, level);
+		bp = make_block_params(g);
 		bool ok = true;
-		g_dev = dev_alloc<Geometry>(1, ok);
-		g_dev_override = dev_alloc<Geometry>(1, ok);
 		coef32 = dev_alloc<float>(size_t(g.storage_elems32), ok);
 		coef16 = dev_alloc<__half>(size_t(g.storage_elems16), ok);
 		code_words = dev_alloc<uint32_t>(size_t(g.block_count_8x8), ok);
@@ -569,7 +652,6 @@ struct pyrowave_encoder_opaque
 			return PYROWAVE_ERROR_OUT_OF_DEVICE_MEMORY;
 		}
 		cudaMemcpy(jobs_d, jobs.data(), jobs.size() * 4, cudaMemcpyHostToDevice);
-		cudaMemcpy(g_dev, &g, sizeof(Geometry), cudaMemcpyHostToDevice);
 		allocated = true;
 		return PYROWAVE_SUCCESS;
 	}
@@ -650,16 +732,17 @@ struct pyrowave_encoder_opaque
 			timing.begin(device, s);
 			cudaMemsetAsync(rc, 0, sizeof(RateControlState), s);
 			static const char *const dwt_tags[kLevels] = {"dwt0", "dwt1", "dwt2", "dwt3", "dwt4"};
+			const bool pdl = !device->stage_timing; // event nodes between kernels break programmatic edges
 			for (int level = 0; level < kLevels; level++)
 			{
-				launch_dwt_forward_level(g, g_dev, level, in, b, true, s);
+				launch_dwt_forward_level(lp[level], in, b, true, pdl && level > 0, s);
 				ok = ok && last_captured_node(s, node_dwt[level]);
 				timing.mark(device, s, dwt_tags[level]);
 			}
-			launch_resolve(g, g_dev, b, target_words, sequence_count, s);
+			launch_resolve(make_resolve_params(g, target_words, sequence_count), b, s);
 			ok = ok && last_captured_node(s, node_resolve);
 			timing.mark(device, s, "resolve");
-			launch_pack(g, g_dev, b, s);
+			launch_pack(bp, b, s);
 			timing.mark(device, s, "pack");
 			ok = graph.end(s, key) && ok;
 			if (!ok)
@@ -671,17 +754,13 @@ struct pyrowave_encoder_opaque
 		}
 		else
 		{
-			const Geometry *gd = g_dev;
 			PlaneInput pin = in;
 			int fused = 1;
-			uint32_t tw = target_words, seq = sequence_count;
+			ResolveParams rp = make_resolve_params(g, target_words, sequence_count);
 			bool ok = true;
 			for (int level = 0; level < kLevels; level++)
-			{
-				int lv = level;
-				ok = ok && set_kernel_args(graph.exec, node_dwt[level], gd, lv, pin, b, fused);
-			}
-			ok = ok && set_kernel_args(graph.exec, node_resolve, gd, b, tw, seq);
+				ok = ok && set_kernel_args(graph.exec, node_dwt[level], lp[level], pin, b, fused);
+			ok = ok && set_kernel_args(graph.exec, node_resolve, rp, b);
 			if (!ok)
 			{
 				graph.destroy();
@@ -727,7 +806,8 @@ struct pyrowave_decoder_opaque
 	uint32_t fp16_mask = 0;
 	bool allocated = false;
 
-	Geometry *g_dev = nullptr;
+	LevelParams lp[kLevels] = {};
+	BlockParams bp = {};
 	float *coef32 = nullptr;
 	__half *coef16 = nullptr;
 	uint32_t *jobs_d = nullptr;
@@ -856,7 +936,6 @@ struct pyrowave_decoder_opaque
 	{
 		if (device)
 			cudaStreamSynchronize(device->stream);
-		dev_free(g_dev);
 		dev_free(coef32);
 		dev_free(coef16);
 		dev_free(jobs_d);
@@ -868,7 +947,6 @@ struct pyrowave_decoder_opaque
 		timing.destroy();
 		graph_full.destroy();
 		graph_idwt.destroy();
-		g_dev = nullptr;
 		coef32 = nullptr;
 		coef16 = nullptr;
 		jobs_d = offsets_d = payload_d = nullptr;
@@ -886,8 +964,10 @@ struct pyrowave_decoder_opaque
 			return PYROWAVE_SUCCESS;
 		if (!build_geometry(g, jobs, g.width, g.height, g.chroma444 != 0, fp16_mask))
 			return PYROWAVE_ERROR_INVALID_ARGUMENT;
+		for (int level = 0; level < kLevels; level++)
+			lp[level] = make_level_params(g, level);
+		bp = make_block_params(g);
 		bool ok = true;
-		g_dev = dev_alloc<Geometry>(1, ok);
 		coef32 = dev_alloc<float>(size_t(g.storage_elems32), ok);
 		coef16 = dev_alloc<__half>(size_t(g.storage_elems16), ok);
 		jobs_d = dev_alloc<uint32_t>(jobs.size(), ok);
@@ -898,7 +978,6 @@ struct pyrowave_decoder_opaque
 			return PYROWAVE_ERROR_OUT_OF_DEVICE_MEMORY;
 		}
 		cudaMemcpy(jobs_d, jobs.data(), jobs.size() * 4, cudaMemcpyHostToDevice);
-		cudaMemcpy(g_dev, &g, sizeof(Geometry), cudaMemcpyHostToDevice);
 		if (offsets.size() != size_t(g.block_count_32x32))
 		{
 			offsets.assign(size_t(g.block_count_32x32), UINT32_MAX);
@@ -963,16 +1042,17 @@ struct pyrowave_decoder_opaque
 				return false;
 			bool ok = true;
 			timing.begin(device, s);
+			const bool pdl = !device->stage_timing; // event nodes between kernels break programmatic edges
 			if (dequant)
 			{
-				launch_dequant(g, g_dev, in, s);
+				launch_dequant(bp, in, false, s);
 				ok = ok && last_captured_node(s, node_dequant);
 				timing.mark(device, s, "dequant");
 			}
 			static const char *const idwt_tags[kLevels] = {"idwt0", "idwt1", "idwt2", "idwt3", "idwt4"};
 			for (int level = kLevels - 1; level >= 0; level--)
 			{
-				launch_idwt_level(g, g_dev, level, in, out, s);
+				launch_idwt_level(lp[level], in, out, pdl && (dequant || level < kLevels - 1), s);
 				ok = ok && last_captured_node(s, dequant ? node_idwt_full[level] : node_idwt_only[level]);
 				timing.mark(device, s, idwt_tags[level]);
 			}
@@ -986,18 +1066,14 @@ struct pyrowave_decoder_opaque
 		}
 		else
 		{
-			const Geometry *gd = g_dev;
 			DecodeInput din = in;
 			PlaneOutput pout = out;
 			bool ok = true;
 			if (dequant)
-				ok = set_kernel_args(graph.exec, node_dequant, gd, din);
+				ok = set_kernel_args(graph.exec, node_dequant, bp, din);
 			for (int level = 0; level < kLevels; level++)
-			{
-				int lv = level;
-				ok = ok && set_kernel_args(graph.exec, dequant ? node_idwt_full[level] : node_idwt_only[level], gd, lv,
+				ok = ok && set_kernel_args(graph.exec, dequant ? node_idwt_full[level] : node_idwt_only[level], lp[level],
 				                           din, pout);
-			}
 			if (!ok)
 			{
 				graph.destroy();
@@ -1660,14 +1736,12 @@ pyrowave_result pyrowave_cuda_encoder_encode_pre_transformed(pyrowave_encoder en
 	apply_quant_scale_override(g, quant_scale);
 	encoder->sequence_count = (encoder->sequence_count + 1) & 7u;
 	EncodeBuffers b = encoder->buffers();
+	const BlockParams bp = make_block_params(g);
 	cudaMemsetAsync(encoder->rc, 0, sizeof(RateControlState), s);
-	cudaMemcpyAsync(encoder->g_dev_override, &g, sizeof(Geometry), cudaMemcpyHostToDevice, s);
-	cudaStreamSynchronize(s); // the host copy of the override geometry is a local
-	Geometry *gd = encoder->g_dev_override;
-	launch_pyramid_io(g, gd, const_cast<float *>(pyramid), encoder->coef32, encoder->coef16, false, s);
-	launch_quant_pretransformed(g, gd, b, s);
-	launch_resolve(g, gd, b, target_words, encoder->sequence_count, s);
-	launch_pack(g, gd, b, s);
+	launch_pyramid_io(bp, const_cast<float *>(pyramid), encoder->coef32, encoder->coef16, false, s);
+	launch_quant_pretransformed(bp, b, s);
+	launch_resolve(make_resolve_params(g, target_words, encoder->sequence_count), b, s);
+	launch_pack(bp, b, s);
 	if (!launches_ok("kernel launch"))
 		return PYROWAVE_ERROR_GENERIC;
 	encoder->has_device_frame = true;
@@ -1678,8 +1752,7 @@ pyrowave_result pyrowave_cuda_encoder_read_wavelet(pyrowave_encoder encoder, flo
 {
 	if (!encoder || !pyramid || !encoder->allocated)
 		return PYROWAVE_ERROR_INVALID_ARGUMENT;
-	launch_pyramid_io(encoder->g, encoder->g_dev, pyramid, encoder->coef32, encoder->coef16, true,
-	                  pick_stream(encoder->device, stream));
+	launch_pyramid_io(encoder->bp, pyramid, encoder->coef32, encoder->coef16, true, pick_stream(encoder->device, stream));
 	return launches_ok("kernel launch") ? PYROWAVE_SUCCESS : PYROWAVE_ERROR_GENERIC;
 }
 
@@ -1767,8 +1840,7 @@ pyrowave_result pyrowave_cuda_decoder_read_wavelet(pyrowave_decoder decoder, flo
 {
 	if (!decoder || !pyramid || !decoder->allocated)
 		return PYROWAVE_ERROR_INVALID_ARGUMENT;
-	launch_pyramid_io(decoder->g, decoder->g_dev, pyramid, decoder->coef32, decoder->coef16, true,
-	                  pick_stream(decoder->device, stream));
+	launch_pyramid_io(decoder->bp, pyramid, decoder->coef32, decoder->coef16, true, pick_stream(decoder->device, stream));
 	return launches_ok("kernel launch") ? PYROWAVE_SUCCESS : PYROWAVE_ERROR_GENERIC;
 }
 
@@ -1789,7 +1861,7 @@ pyrowave_result pyrowave_cuda_decoder_decode_pyramid(pyrowave_decoder decoder, c
 		out.pitch[p] = int32_t(planes->row_stride_in_bytes[p]);
 	}
 	cudaStream_t s = pick_stream(decoder->device, stream);
-	launch_pyramid_io(decoder->g, decoder->g_dev, const_cast<float *>(pyramid), decoder->coef32, decoder->coef16, false, s);
+	launch_pyramid_io(decoder->bp, const_cast<float *>(pyramid), decoder->coef32, decoder->coef16, false, s);
 	DecodeInput in = {};
 	in.jobs = decoder->jobs_d;
 	in.coef32 = decoder->coef32;

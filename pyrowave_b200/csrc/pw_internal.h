@@ -141,16 +141,91 @@ struct DecodeInput
 	__half *coef16;
 };
 
-// Host-side kernel launchers (implemented in the .cu files).
-void launch_dwt_forward_level(const Geometry &g, const Geometry *gd, int level, const PlaneInput &in, const EncodeBuffers &buf,
-                              bool fused_quant, cudaStream_t stream);
-void launch_quant_pretransformed(const Geometry &g, const Geometry *gd, const EncodeBuffers &buf, cudaStream_t stream);
-void launch_resolve(const Geometry &g, const Geometry *gd, const EncodeBuffers &buf, uint32_t target_words, uint32_t sequence,
-                    cudaStream_t stream);
-void launch_pack(const Geometry &g, const Geometry *gd, const EncodeBuffers &buf, cudaStream_t stream);
-void launch_dequant(const Geometry &g, const Geometry *gd, const DecodeInput &in, cudaStream_t stream);
-void launch_idwt_level(const Geometry &g, const Geometry *gd, int level, const DecodeInput &in, const PlaneOutput &out,
+// ---------------------------------------------------------------------------
+// Kernel parameter blocks. Everything a kernel needs about the frame layout
+// arrives by value with the launch, so no kernel starts with a chain of
+// dependent loads of layout metadata.
+struct BandParam
+{
+	int64_t offset;                       // storage offset of the band (elements)
+	int32_t block8_offset, block8_stride; // global 8x8 numbering
+	int32_t block32_offset, block32_stride;
+	float quant_resolution, rdo_scale;
+	uint32_t quant_code, pad;
+};
+
+// One forward or inverse level.
+struct LevelParams
+{
+	LevelDesc L;            // this level
+	LevelDesc P;            // the finer level (level - 1): forward input LL / inverse output LL
+	int32_t level, chroma444, subdivision_shift;
+	int32_t width, height, aligned_width, aligned_height;
+	int32_t plane_width[3], plane_height[3];
+	int64_t prev_ll[3];     // offset of LL at level - 1 per component
+	BandParam band[3][4];   // this level's four bands per component
+};
+
+// One transmitted band, for kernels that walk the 32x32 blocks of all bands.
+struct BandEntry
+{
+	int64_t offset;
+	int32_t block32_offset;
+	int32_t block32_stride;
+	int32_t block8_offset, block8_stride;
+	float quant_resolution;
+	uint32_t quant_code;
+	float rdo_scale;
+	int32_t level;
+};
+
+constexpr int kMaxBands = 48;
+struct BlockParams
+{
+	LevelDesc level[kLevels];
+	int32_t nbands, block_count_32x32, subdivision_shift, pad;
+	BandEntry band[kMaxBands]; // in block index order
+};
+
+struct ResolveParams
+{
+	int32_t block_count_32x32, blocks_per_subdivision, subdivision_shift;
+	int32_t width, height, chroma444;
+	uint32_t target_words, sequence;
+};
+
+// cudaLaunchKernelEx configuration, optionally marked as a programmatic
+// dependent launch of the preceding kernel on the stream.
+struct LaunchConfig
+{
+	cudaLaunchConfig_t cfg;
+	cudaLaunchAttribute attr;
+	LaunchConfig(dim3 grid, dim3 block, cudaStream_t stream, bool programmatic);
+	LaunchConfig(const LaunchConfig &) = delete;
+};
+
+LevelParams make_level_params(const Geometry &g, int level);
+BlockParams make_block_params(const Geometry &g);
+ResolveParams make_resolve_params(const Geometry &g, uint32_t target_words, uint32_t sequence);
+
+// Host-side kernel launchers (implemented in the .cu files). Every launch but
+// the first of a sequence may start early (programmatic dependent launch):
+// kernels wait for their predecessor with griddepcontrol before touching
+// global memory.
+void launch_dwt_forward_level(const LevelParams &p, const PlaneInput &in, const EncodeBuffers &buf, bool fused_quant,
+                              bool programmatic, cudaStream_t stream);
+void launch_quant_pretransformed(const BlockParams &p, const EncodeBuffers &buf, cudaStream_t stream);
+void launch_resolve(const ResolveParams &p, const EncodeBuffers &buf, cudaStream_t stream);
+void launch_pack(const BlockParams &p, const EncodeBuffers &buf, cudaStream_t stream);
+void launch_dequant(const BlockParams &p, const DecodeInput &in, bool programmatic, cudaStream_t stream);
+void launch_idwt_level(const LevelParams &p, const DecodeInput &in, const PlaneOutput &out, bool programmatic,
                        cudaStream_t stream);
-void launch_pyramid_io(const Geometry &g, const Geometry *gd, float *canonical, float *coef32, __half *coef16, bool to_canonical,
+void launch_pyramid_io(const BlockParams &p, float *canonical, float *coef32, __half *coef16, bool to_canonical,
                        cudaStream_t stream);
+
+// Kernel entry points, for patching captured graph nodes.
+const void *kernel_dwt_forward();
+const void *kernel_resolve();
+const void *kernel_dequant();
+const void *kernel_idwt();
 } // namespace pw
