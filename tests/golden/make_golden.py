@@ -6,7 +6,7 @@ Requires oracle/_ref/libref_bitstream.so, i.e. the reference's Granite-free
 bitstream code (metal/pyrowave_bitstream.cpp) compiled in place by
 `make -C oracle`. The reference has no stored golden vectors of its own, so
 these fixtures record what its block layout, packetizer, packet parser and
-quant-code helpers produce on deterministic inputs. tests/test_golden.py then
+quant-code helpers produce on deterministic inputs. tests/test_oracle_pinning.py then
 pins the oracle against them on machines without the reference tree.
 """
 from __future__ import annotations
