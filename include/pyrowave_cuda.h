@@ -132,6 +132,48 @@ PYROWAVE_PUBLIC_API pyrowave_result pyrowave_cuda_decoder_decode_pyramid(pyrowav
                                                                          const pyrowave_cuda_planes *planes,
                                                                          pyrowave_cuda_stream stream);
 
+/* Largest FP32 coefficient storage pyrowave_cuda_decode_blocks_static accepts:
+ * 32 MiB, enough for 4:2:0 frames up to 2560x1440 (1920x1080 needs 17.7 MB;
+ * 1920x1080 4:4:4 and 3840x2160 do not fit). */
+#define PYROWAVE_CUDA_STATIC_DECODE_SCRATCH_BYTES (32u << 20)
+
+/* Decode coded blocks already in device memory (same block_meta / words
+ * format as pyrowave_cuda_decoder_decode_blocks) into device planes, without
+ * a decoder object and without allocating any memory, host or device.
+ *
+ * There is no counterpart in the reference: its decoder always owns buffers
+ * it allocates. This entry point is for callers that cannot allocate when
+ * they decode: a process whose device memory is fully budgeted up front, a
+ * real-time thread that must not enter an allocator, or an application that
+ * hands its CUDA memory to its own arena and wants no other owner on the GPU.
+ *
+ * Scratch: the coefficient pyramid is kept in one fixed device array of
+ * PYROWAVE_CUDA_STATIC_DECODE_SCRATCH_BYTES inside this library, reserved by
+ * CUDA when the library's device code is loaded on a device. Frames whose
+ * coefficient storage is larger are rejected with
+ * PYROWAVE_ERROR_INVALID_ARGUMENT. Nothing in the array has to start at zero:
+ * every coefficient the inverse transform reads is written earlier in the
+ * same call (a missing block decodes as zeros).
+ *
+ * First call: on each device, the first call (with that device current)
+ * looks up the array's device address once. Make that first call before any
+ * stream capture is in progress, for example with a small decode at start-up.
+ *
+ * Overlapping calls race: every call on a device uses the same array, so two
+ * calls whose work can overlap on the GPU (different streams without an event
+ * between them, or concurrent host threads) corrupt each other's output.
+ * Issue the calls in one stream, or order them with events.
+ *
+ * width, height and chroma follow pyrowave_decoder_create's rules; planes
+ * follow pyrowave_cuda_decoder_decode_blocks. Work is queued on `stream`
+ * (0: the legacy default stream); the call does not wait for it. */
+PYROWAVE_PUBLIC_API pyrowave_result pyrowave_cuda_decode_blocks_static(int width, int height,
+                                                                       pyrowave_chroma_subsampling chroma,
+                                                                       const uint32_t *block_meta,
+                                                                       const uint32_t *words, size_t num_words,
+                                                                       const pyrowave_cuda_planes *planes,
+                                                                       pyrowave_cuda_stream stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -52,7 +52,11 @@ API_SYMBOLS = [
     "pyrowave_cuda_encoder_get_size", "pyrowave_cuda_encoder_encode_pre_transformed",
     "pyrowave_cuda_encoder_read_wavelet", "pyrowave_cuda_encoder_read_debug", "pyrowave_cuda_decoder_decode",
     "pyrowave_cuda_decoder_decode_blocks", "pyrowave_cuda_decoder_read_wavelet", "pyrowave_cuda_decoder_decode_pyramid",
+    "pyrowave_cuda_decode_blocks_static",
 ]
+
+# Coefficient storage limit of pyrowave_cuda_decode_blocks_static (PYROWAVE_CUDA_STATIC_DECODE_SCRATCH_BYTES).
+STATIC_DECODE_SCRATCH_BYTES = 32 << 20
 
 
 class PyrowaveError(RuntimeError):
@@ -163,6 +167,8 @@ def lib():
                                                       c_void_p]
     L.pyrowave_cuda_decoder_read_wavelet.argtypes = [c_void_p, c_void_p, c_void_p]
     L.pyrowave_cuda_decoder_decode_pyramid.argtypes = [c_void_p, c_void_p, POINTER(CudaPlanes), c_void_p]
+    L.pyrowave_cuda_decode_blocks_static.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_int, c_void_p, c_void_p,
+                                                     c_size_t, POINTER(CudaPlanes), c_void_p]
     for name in API_SYMBOLS:
         getattr(L, name)  # every declared entry point must resolve
     _lib = L
@@ -408,3 +414,15 @@ class Decoder:
     def read_wavelet(self, pyramid_dev_ptr: int, stream: int = 0):
         check(self.L.pyrowave_cuda_decoder_read_wavelet(self.h, c_void_p(pyramid_dev_ptr), c_void_p(stream)),
               "decoder_read_wavelet")
+
+
+def decode_blocks_static(width: int, height: int, chroma: int, meta_ptr: int, words_ptr: int, num_words: int,
+                         plane_ptrs, strides, stream: int = 0) -> int:
+    """pyrowave_cuda_decode_blocks_static: decode device-resident blocks with no decoder object and no
+    allocation. Returns the pyrowave_result code."""
+    cp = CudaPlanes()
+    for i in range(3):
+        cp.data[i] = plane_ptrs[i]
+        cp.row_stride_in_bytes[i] = strides[i]
+    return lib().pyrowave_cuda_decode_blocks_static(width, height, chroma, c_void_p(meta_ptr), c_void_p(words_ptr),
+                                                    num_words, ctypes.byref(cp), c_void_p(stream))

@@ -471,3 +471,95 @@ void launch_pyramid_io(const BlockParams &p, float *canonical, float *coef32, __
 const void *kernel_dequant() { return reinterpret_cast<const void *>(&dequant_kernel); }
 const void *kernel_idwt() { return reinterpret_cast<const void *>(&idwt_kernel); }
 } // namespace pw
+
+// ---------------------------------------------------------------------------
+// Decode without allocation (pyrowave_cuda_decode_blocks_static).
+//
+// The coefficient pyramid of the decode lives in one file-scope device array
+// instead of memory owned by a decoder object. CUDA reserves the array when
+// this library's device code is loaded on a device; its address is looked up
+// once per device and then passed to the dequantiser and inverse-transform
+// kernels in place of a decoder's storage buffer.
+#include "pyrowave_cuda.h"
+
+#include <mutex>
+
+namespace
+{
+constexpr size_t kStaticScratchBytes = PYROWAVE_CUDA_STATIC_DECODE_SCRATCH_BYTES;
+static __device__ __align__(256) float g_static_pyramid[kStaticScratchBytes / sizeof(float)];
+
+constexpr int kMaxStaticDevices = 64;
+std::mutex g_static_lock;
+float *g_static_pyramid_ptr[kMaxStaticDevices]; // per device ordinal; null until looked up
+
+// Address of the array on the current device (null on failure).
+float *static_pyramid_on_current_device()
+{
+	int dev = -1;
+	if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kMaxStaticDevices)
+	{
+		(void)cudaGetLastError();
+		return nullptr;
+	}
+	std::lock_guard<std::mutex> hold(g_static_lock);
+	if (!g_static_pyramid_ptr[dev])
+	{
+		float *ptr = nullptr;
+		if (cudaGetSymbolAddress((void **)&ptr, g_static_pyramid) != cudaSuccess || !ptr)
+		{
+			(void)cudaGetLastError();
+			return nullptr;
+		}
+		g_static_pyramid_ptr[dev] = ptr;
+	}
+	return g_static_pyramid_ptr[dev];
+}
+} // namespace
+
+extern "C" pyrowave_result pyrowave_cuda_decode_blocks_static(int width, int height,
+                                                              pyrowave_chroma_subsampling chroma,
+                                                              const uint32_t *block_meta, const uint32_t *words,
+                                                              size_t num_words, const pyrowave_cuda_planes *planes,
+                                                              pyrowave_cuda_stream stream)
+{
+	using namespace pw;
+	// Frame rules of pyrowave_decoder_create, buffer rules of pyrowave_cuda_decoder_decode_blocks.
+	if (width <= 0 || height <= 0)
+		return PYROWAVE_ERROR_INVALID_ARGUMENT;
+	if (chroma != PYROWAVE_CHROMA_SUBSAMPLING_420 && chroma != PYROWAVE_CHROMA_SUBSAMPLING_444)
+		return PYROWAVE_ERROR_INVALID_ARGUMENT;
+	if (chroma == PYROWAVE_CHROMA_SUBSAMPLING_420 && ((width & 1) || (height & 1)))
+		return PYROWAVE_ERROR_INVALID_ARGUMENT;
+	if (!block_meta || !words || !planes || num_words > 0xffffffffu)
+		return PYROWAVE_ERROR_INVALID_ARGUMENT;
+	Geometry g;
+	if (!make_geometry(g, width, height, chroma == PYROWAVE_CHROMA_SUBSAMPLING_444, 0))
+		return PYROWAVE_ERROR_INVALID_ARGUMENT;
+	if (size_t(g.storage_elems32) * sizeof(float) > kStaticScratchBytes)
+		return PYROWAVE_ERROR_INVALID_ARGUMENT;
+	PlaneOutput out = {};
+	for (int p = 0; p < 3; p++)
+	{
+		if (!planes->data[p] || planes->row_stride_in_bytes[p] < size_t(g.plane_width[p]) ||
+		    planes->row_stride_in_bytes[p] > 0x7fffffffu)
+			return PYROWAVE_ERROR_INVALID_ARGUMENT;
+		out.data[p] = static_cast<uint8_t *>(planes->data[p]);
+		out.pitch[p] = int32_t(planes->row_stride_in_bytes[p]);
+	}
+	float *scratch = static_pyramid_on_current_device();
+	if (!scratch)
+		return PYROWAVE_ERROR_GENERIC;
+
+	DecodeInput in = {};
+	in.block_meta = block_meta;
+	in.payload = words;
+	in.payload_words = uint32_t(num_words);
+	in.coef32 = scratch;
+	in.coef16 = nullptr; // every level is FP32 here
+	const cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
+	launch_dequant(make_block_params(g), in, false, s);
+	for (int level = kLevels - 1; level >= 0; level--)
+		launch_idwt_level(make_level_params(g, level), in, out, true, s);
+	return cudaGetLastError() == cudaSuccess ? PYROWAVE_SUCCESS : PYROWAVE_ERROR_GENERIC;
+}

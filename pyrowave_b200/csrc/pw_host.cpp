@@ -114,7 +114,8 @@ float rdo_distortion_scale(int level, int comp, int band, bool chroma444)
 bool has_level(int comp, int level, bool chroma444) { return !(level == 0 && comp != 0 && !chroma444); }
 
 // Frame geometry, padded band storage and the block tables.
-bool build_geometry(Geometry &g, std::vector<uint32_t> &jobs, int width, int height, bool chroma444, uint32_t fp16_mask)
+// Layout only: band sizes, storage offsets and block numbering (no job table).
+bool build_geometry(Geometry &g, int width, int height, bool chroma444, uint32_t fp16_mask)
 {
 	if (width <= 0 || height <= 0 || width > 16384 || height > 16384)
 		return false;
@@ -162,7 +163,6 @@ bool build_geometry(Geometry &g, std::vector<uint32_t> &jobs, int width, int hei
 	g.storage_elems16 = off16;
 
 	// Block index order (bitstream.md:472-511): level 4 -> 0, component, band.
-	jobs.clear();
 	int count8 = 0, count32 = 0;
 	for (int level = kLevels - 1; level >= 0; level--)
 		for (int comp = 0; comp < kComponents; comp++)
@@ -182,10 +182,7 @@ bool build_geometry(Geometry &g, std::vector<uint32_t> &jobs, int width, int hei
 				B.quant_code = encode_quant(1.0f / qr);
 				B.quant_resolution = 1.0f / decode_quant(B.quant_code);
 				B.rdo_scale = rdo_distortion_scale(level, comp, band, chroma444) * (1.0f / 256.0f);
-				int by32n = (L.height + 31) / 32;
-				for (int by = 0; by < by32n; by++)
-					for (int bx = 0; bx < B.block32_stride; bx++)
-						jobs.push_back(pack_job(level, comp, band, bx, by));
+				const int by32n = (L.height + 31) / 32;
 				count32 += B.block32_stride * by32n;
 				count8 += L.blocks8_x * L.blocks8_y;
 			}
@@ -202,6 +199,27 @@ bool build_geometry(Geometry &g, std::vector<uint32_t> &jobs, int width, int hei
 	}
 	g.blocks_per_subdivision = pot;
 	g.subdivision_shift = shift;
+	return true;
+}
+
+// Layout plus the per-32x32 job table in block index order.
+bool build_geometry(Geometry &g, std::vector<uint32_t> &jobs, int width, int height, bool chroma444, uint32_t fp16_mask)
+{
+	if (!build_geometry(g, width, height, chroma444, fp16_mask))
+		return false;
+	jobs.clear();
+	for (int level = kLevels - 1; level >= 0; level--)
+		for (int comp = 0; comp < kComponents; comp++)
+			for (int band = 0; band < 4; band++)
+			{
+				const BandDesc &B = g.band[comp][level][band];
+				if (!B.present)
+					continue;
+				const int by32n = (g.level[level].height + 31) / 32;
+				for (int by = 0; by < by32n; by++)
+					for (int bx = 0; bx < B.block32_stride; bx++)
+						jobs.push_back(pack_job(level, comp, band, bx, by));
+			}
 	return true;
 }
 
@@ -351,6 +369,11 @@ ResolveParams make_resolve_params(const Geometry &g, uint32_t target_words, uint
 	p.target_words = target_words;
 	p.sequence = sequence;
 	return p;
+}
+
+bool make_geometry(Geometry &g, int width, int height, bool chroma444, uint32_t fp16_mask)
+{
+	return build_geometry(g, width, height, chroma444, fp16_mask);
 }
 } // namespace pw
 

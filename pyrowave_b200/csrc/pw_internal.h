@@ -204,6 +204,8 @@ struct LaunchConfig
 	LaunchConfig(const LaunchConfig &) = delete;
 };
 
+// Frame layout without the job table; allocates nothing.
+bool make_geometry(Geometry &g, int width, int height, bool chroma444, uint32_t fp16_mask);
 LevelParams make_level_params(const Geometry &g, int level);
 BlockParams make_block_params(const Geometry &g);
 ResolveParams make_resolve_params(const Geometry &g, uint32_t target_words, uint32_t sequence);
