@@ -22,6 +22,49 @@ struct PayloadReader
 	__device__ __forceinline__ uint32_t u16(uint32_t i) const { return (w32(i >> 1) >> (16u * (i & 1u))) & 0xffffu; }
 };
 
+// A block's words staged in shared memory: words [base, base + count) of the
+// payload come from `s`, anything else from the bounds-checked global reader,
+// so reads of a malformed block behave exactly as with PayloadReader alone.
+struct StagedReader
+{
+	const uint32_t *s;
+	uint32_t base, count;
+	PayloadReader g;
+	__device__ __forceinline__ uint32_t w32(uint32_t i) const
+	{
+		const uint32_t r = i - base;
+		return r < count ? s[r] : g.w32(i);
+	}
+	__device__ __forceinline__ uint32_t u8(uint32_t i) const { return (w32(i >> 2) >> (8u * (i & 3u))) & 0xffu; }
+	__device__ __forceinline__ uint32_t u16(uint32_t i) const { return (w32(i >> 1) >> (16u * (i & 1u))) & 0xffffu; }
+};
+
+constexpr uint32_t kSpeculativeWords = 128; // staged with the header when the block size is not yet known
+
+// s[i] = payload word off + i for i in [begin, end), by 128 threads with up to
+// eight loads per thread in flight together.
+__device__ __forceinline__ void stage_words(uint32_t *s, const PayloadReader &g, uint32_t off, uint32_t begin,
+                                            uint32_t end, int t)
+{
+	for (uint32_t base = begin + uint32_t(t); base < end; base += 128 * 8)
+	{
+		uint32_t v[8];
+#pragma unroll
+		for (int u = 0; u < 8; u++)
+		{
+			const uint32_t i = base + 128u * u;
+			v[u] = i < end ? g.w32(off + i) : 0u;
+		}
+#pragma unroll
+		for (int u = 0; u < 8; u++)
+		{
+			const uint32_t i = base + 128u * u;
+			if (i < end)
+				s[i] = v[u];
+		}
+	}
+}
+
 __device__ __forceinline__ void store_coef(float *c32, __half *c16, bool fp16, int64_t idx, float v)
 {
 	if (fp16)
@@ -34,6 +77,7 @@ __device__ __forceinline__ void store_coef(float *c32, __half *c16, bool fp16, i
 // reference's mapping, wavelet_dequant.comp:222-238).
 __global__ void __launch_bounds__(128) dequant_kernel(const BlockParams p, const DecodeInput in)
 {
+	__shared__ uint32_t s_words[kMaxBlockWords];
 	__shared__ uint32_t s_plane_off[16];
 	__shared__ uint32_t s_sign_base;
 	__shared__ uint32_t s_sig[4];
@@ -51,11 +95,15 @@ __global__ void __launch_bounds__(128) dequant_kernel(const BlockParams p, const
 	const int ox = bx32 * 32 + lx * 8 + sub_x(sub), oy = by32 * 32 + ly * 8 + sub_y(sub);
 	pdl_wait();
 
-	uint32_t off;
+	uint32_t off, words = 0;
 	if (in.offsets)
 		off = __ldcg(in.offsets + blk);
 	else
-		off = __ldcg(in.block_meta + 2 * blk + 1) ? __ldcg(in.block_meta + 2 * blk) : 0xffffffffu;
+	{
+		const uint2 m = __ldcg(reinterpret_cast<const uint2 *>(in.block_meta) + blk);
+		off = m.y ? m.x : 0xffffffffu;
+		words = m.y;
+	}
 
 	if (off == 0xffffffffu)
 	{
@@ -66,7 +114,27 @@ __global__ void __launch_bounds__(128) dequant_kernel(const BlockParams p, const
 		return;
 	}
 
-	const PayloadReader rd{in.payload, in.payload_words};
+	// Stage the block's words in shared memory with all loads in flight at
+	// once; every read below is then a shared-memory read. With only an offset
+	// table the size comes from the block header, so the first
+	// kSpeculativeWords are fetched together with it.
+	const PayloadReader grd{in.payload, in.payload_words};
+	uint32_t staged;
+	if (in.offsets)
+	{
+		stage_words(s_words, grd, off, 0, kSpeculativeWords, t);
+		__syncthreads();
+		words = (s_words[0] >> 16) & 0xfffu;
+		staged = min(max(words, kSpeculativeWords), uint32_t(kMaxBlockWords));
+		stage_words(s_words, grd, off, kSpeculativeWords, staged, t);
+	}
+	else
+	{
+		staged = min(words, uint32_t(kMaxBlockWords));
+		stage_words(s_words, grd, off, 0, staged, t);
+	}
+	__syncthreads();
+	const StagedReader rd{s_words, off, staged, grd};
 	const uint32_t ballot = rd.w32(off) & 0xffffu;
 	const uint32_t q_code = rd.w32(off + 1) & 0xffu;
 	const uint32_t n = uint32_t(__popc(ballot));
@@ -277,11 +345,12 @@ __global__ void __launch_bounds__(kIdwtThreads) idwt_kernel(const LevelParams p,
 	else
 	{
 		constexpr int kN = 4 * kBandTile * kBandTile;
-		for (int base = threadIdx.x; base < kN; base += kIdwtThreads * 8)
+		constexpr int kIdwtGen = (kN + kIdwtThreads - 1) / kIdwtThreads; // every load in flight at once
+		for (int base = threadIdx.x; base < kN; base += kIdwtThreads * kIdwtGen)
 		{
-			float v[8];
+			float v[kIdwtGen];
 #pragma unroll
-			for (int u = 0; u < 8; u++)
+			for (int u = 0; u < kIdwtGen; u++)
 			{
 				const int k = base + u * kIdwtThreads;
 				const int b = k / (kBandTile * kBandTile);
@@ -295,7 +364,7 @@ __global__ void __launch_bounds__(kIdwtThreads) idwt_kernel(const LevelParams p,
 				              : 0.0f;
 			}
 #pragma unroll
-			for (int u = 0; u < 8; u++)
+			for (int u = 0; u < kIdwtGen; u++)
 			{
 				const int k = base + u * kIdwtThreads;
 				if (k < kN)

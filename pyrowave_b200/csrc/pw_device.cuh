@@ -112,6 +112,18 @@ __device__ __forceinline__ float round_to_half(float v) { return __half2float(__
 __device__ __forceinline__ void pdl_trigger() { asm volatile("griddepcontrol.launch_dependents;" ::: "memory"); }
 __device__ __forceinline__ void pdl_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
 
+// GPU-scope acquire load / release store of a 64-bit word (flags between CTAs).
+__device__ __forceinline__ unsigned long long ld_acquire_u64(const unsigned long long *p)
+{
+	unsigned long long v;
+	asm volatile("ld.acquire.gpu.global.u64 %0, [%1];" : "=l"(v) : "l"(p) : "memory");
+	return v;
+}
+__device__ __forceinline__ void st_release_u64(unsigned long long *p, unsigned long long v)
+{
+	asm volatile("st.release.gpu.global.u64 [%0], %1;" ::"l"(p), "l"(v) : "memory");
+}
+
 // Band of a 32x32 block (block index order): the last band whose first block
 // is <= blk, then the block's position in it.
 __device__ __forceinline__ int find_band(const BlockParams &p, int blk)

@@ -20,6 +20,8 @@ constexpr int kTileIn = 72;  // 64 input samples + 4-sample apron on each side
 constexpr int kInPitch = 73; // odd pitch: conflict-free column walks
 constexpr int kHPitch = 65;
 constexpr int kBandPitch = 33;
+// Loads per thread of an edge tile gathered through the index tables: all in flight at once.
+constexpr int kDwtGen = (kTileIn * kTileIn + kDwtThreads - 1) / kDwtThreads;
 
 // Reduction scratch of one 128-thread quantiser group (one 32x32 block).
 struct QuantGroupShared
@@ -291,7 +293,7 @@ __device__ __forceinline__ float unorm8_centered(uint32_t u)
 
 // One forward level for one 32x32 band tile of one component (64x64 input
 // samples). grid.x = tile, grid.y = component index among those at this level.
-__global__ void __launch_bounds__(kDwtThreads) dwt_forward_kernel(const LevelParams p, const PlaneInput in,
+__global__ void __launch_bounds__(kDwtThreads, 4) dwt_forward_kernel(const LevelParams p, const PlaneInput in,
                                                                    const EncodeBuffers buf, const int fused)
 {
 	__shared__ DwtShared sh;
@@ -367,18 +369,18 @@ __global__ void __launch_bounds__(kDwtThreads) dwt_forward_kernel(const LevelPar
 		}
 		else
 		{
-			for (int base = threadIdx.x; base < kTileIn * kTileIn; base += kDwtThreads * 8)
+			for (int base = threadIdx.x; base < kTileIn * kTileIn; base += kDwtThreads * kDwtGen)
 			{
-				uint32_t v[8];
+				uint32_t v[kDwtGen];
 #pragma unroll
-				for (int u = 0; u < 8; u++)
+				for (int u = 0; u < kDwtGen; u++)
 				{
 					const int k = base + u * kDwtThreads;
 					const int i = k / kTileIn, j = k - i * kTileIn;
 					v[u] = k < kTileIn * kTileIn ? src[size_t(sh.yidx[i]) * pitch + size_t(sh.xidx[j]) * xs] : 0u;
 				}
 #pragma unroll
-				for (int u = 0; u < 8; u++)
+				for (int u = 0; u < kDwtGen; u++)
 				{
 					const int k = base + u * kDwtThreads;
 					if (k < kTileIn * kTileIn)
@@ -432,11 +434,11 @@ __global__ void __launch_bounds__(kDwtThreads) dwt_forward_kernel(const LevelPar
 		}
 		else
 		{
-			for (int base = threadIdx.x; base < kTileIn * kTileIn; base += kDwtThreads * 8)
+			for (int base = threadIdx.x; base < kTileIn * kTileIn; base += kDwtThreads * kDwtGen)
 			{
-				float v[8];
+				float v[kDwtGen];
 #pragma unroll
-				for (int u = 0; u < 8; u++)
+				for (int u = 0; u < kDwtGen; u++)
 				{
 					const int k = base + u * kDwtThreads;
 					const int i = k / kTileIn, j = k - i * kTileIn;
@@ -445,7 +447,7 @@ __global__ void __launch_bounds__(kDwtThreads) dwt_forward_kernel(const LevelPar
 					           : 0.0f;
 				}
 #pragma unroll
-				for (int u = 0; u < 8; u++)
+				for (int u = 0; u < kDwtGen; u++)
 				{
 					const int k = base + u * kDwtThreads;
 					if (k < kTileIn * kTileIn)
@@ -593,14 +595,14 @@ __global__ void __launch_bounds__(256) quant_pretransformed_kernel(const BlockPa
 // ---------------------------------------------------------------------------
 // Block-wide (1024 threads) exclusive scan; returns the exclusive prefix and
 // the block total.
-__device__ __forceinline__ uint32_t block_exclusive_scan_1024(uint32_t v, uint32_t *warp_sums, uint32_t &total)
+template <typename T> __device__ __forceinline__ T block_exclusive_scan_1024(T v, T *warp_sums, T &total)
 {
 	const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-	uint32_t x = v;
+	T x = v;
 #pragma unroll
 	for (int off = 1; off < 32; off *= 2)
 	{
-		const uint32_t y = __shfl_up_sync(0xffffffffu, x, off);
+		const T y = __shfl_up_sync(0xffffffffu, x, off);
 		if (lane >= off)
 			x += y;
 	}
@@ -609,82 +611,86 @@ __device__ __forceinline__ uint32_t block_exclusive_scan_1024(uint32_t v, uint32
 	__syncthreads();
 	if (warp == 0)
 	{
-		uint32_t s = warp_sums[lane];
+		T s = warp_sums[lane];
 #pragma unroll
 		for (int off = 1; off < 32; off *= 2)
 		{
-			const uint32_t y = __shfl_up_sync(0xffffffffu, s, off);
+			const T y = __shfl_up_sync(0xffffffffu, s, off);
 			if (lane >= off)
 				s += y;
 		}
 		warp_sums[lane] = s;
 	}
 	__syncthreads();
-	const uint32_t base = warp == 0 ? 0u : warp_sums[warp - 1];
+	const T base = warp == 0 ? T(0) : warp_sums[warp - 1];
 	total = warp_sums[31];
 	__syncthreads();
 	return base + x - v;
 }
 
-// The 16 RD entries of one 32x32 block: words at quant 0..15 and buckets.
-struct BlockRD
+// The RD row of one 32x32 block as stored: 16 u16 word counts (quant 0..15)
+// and 16 u8 buckets, 48 bytes in three 16-byte loads.
+struct RawRD
 {
-	uint32_t cost[16];
-	uint32_t bucket[16];
+	uint4 c0, c1, bb;
 };
 
-__device__ __forceinline__ void load_block_rd(const EncodeBuffers &buf, int blk, BlockRD &rd)
+__device__ __forceinline__ RawRD load_raw_rd(const EncodeBuffers &buf, int blk)
 {
-	const uint4 c0 = __ldcg(reinterpret_cast<const uint4 *>(buf.rd_cost + size_t(blk) * 16));
-	const uint4 c1 = __ldcg(reinterpret_cast<const uint4 *>(buf.rd_cost + size_t(blk) * 16) + 1);
-	const uint4 bb = __ldcg(reinterpret_cast<const uint4 *>(buf.rd_bucket + size_t(blk) * 16));
-	const uint32_t cw[8] = {c0.x, c0.y, c0.z, c0.w, c1.x, c1.y, c1.z, c1.w};
-	const uint32_t bw[4] = {bb.x, bb.y, bb.z, bb.w};
-#pragma unroll
-	for (int i = 0; i < 8; i++)
-	{
-		rd.cost[2 * i] = cw[i] & 0xffffu;
-		rd.cost[2 * i + 1] = cw[i] >> 16;
-	}
-#pragma unroll
-	for (int i = 0; i < 16; i++)
-		rd.bucket[i] = (bw[i >> 2] >> (8 * (i & 3))) & 0xffu;
+	RawRD r;
+	r.c0 = __ldcg(reinterpret_cast<const uint4 *>(buf.rd_cost + size_t(blk) * 16));
+	r.c1 = __ldcg(reinterpret_cast<const uint4 *>(buf.rd_cost + size_t(blk) * 16) + 1);
+	r.bb = __ldcg(reinterpret_cast<const uint4 *>(buf.rd_bucket + size_t(blk) * 16));
+	return r;
 }
 
-// Saving of the block's RD operation that sits in bucket bk (0 if none).
-__device__ __forceinline__ uint32_t op_saving_at_bucket(const EncodeBuffers &buf, int blk, uint32_t bk)
+__device__ __forceinline__ uint32_t u4_word(const uint4 &v, int i)
 {
-	BlockRD rd;
-	load_block_rd(buf, blk, rd);
+	return i == 0 ? v.x : (i == 1 ? v.y : (i == 2 ? v.z : v.w));
+}
+
+// Word count at quant l (l is a compile-time index after unrolling).
+__device__ __forceinline__ uint32_t rd_cost_at(const RawRD &r, int l)
+{
+	const uint32_t w = l < 8 ? u4_word(r.c0, l >> 1) : u4_word(r.c1, (l - 8) >> 1);
+	return (w >> (16 * (l & 1))) & 0xffffu;
+}
+
+__device__ __forceinline__ uint32_t rd_bucket_at(const RawRD &r, int l)
+{
+	return (u4_word(r.bb, l >> 2) >> (8 * (l & 3))) & 0xffu;
+}
+
+// Saving of the block's RD operation in bucket bk (0 if none). Buckets of one
+// block strictly increase with the step, so at most one step matches.
+__device__ __forceinline__ uint32_t op_saving_at_bucket(const RawRD &r, uint32_t bk)
+{
 	uint32_t sv = 0;
 #pragma unroll
 	for (int l = 1; l < 16; l++)
-		if (rd.bucket[l] == bk && sv == 0)
-			sv = rd.cost[l - 1] - rd.cost[l];
+		if (rd_bucket_at(r, l) == bk)
+			sv = rd_cost_at(r, l - 1) - rd_cost_at(r, l);
 	return sv;
 }
 
 // Quant of a block: its largest applied RD step. Steps are applied when their
 // (bucket, subdivision) slot precedes x*, or equals it and the block precedes the cut.
-__device__ __forceinline__ uint32_t block_words(const EncodeBuffers &buf, int blk, int sdiv, int xstar, uint32_t cut,
-                                                int &q)
+__device__ __forceinline__ uint32_t block_words(const RawRD &r, int blk, int sdiv, int xstar, uint32_t cut, int &q)
 {
-	BlockRD rd;
-	load_block_rd(buf, blk, rd);
 	q = 0;
+	uint32_t words = rd_cost_at(r, 0);
 #pragma unroll
 	for (int l = 1; l < 16; l++)
 	{
-		const uint32_t saving = rd.cost[l - 1] - rd.cost[l];
-		const int x = int(rd.bucket[l]) * kSubdivisions + sdiv;
+		const uint32_t cost = rd_cost_at(r, l);
+		const uint32_t saving = rd_cost_at(r, l - 1) - cost;
+		const int x = int(rd_bucket_at(r, l)) * kSubdivisions + sdiv;
 		if (saving != 0 && (x < xstar || (x == xstar && uint32_t(blk) < cut)))
+		{
 			q = l;
+			words = cost;
+		}
 	}
-	uint32_t words = rd.cost[0];
-#pragma unroll
-	for (int l = 1; l < 16; l++)
-		if (q == l)
-			words = rd.cost[l];
 	return words;
 }
 
@@ -695,32 +701,83 @@ __device__ __forceinline__ uint32_t block_words(const EncodeBuffers &buf, int bl
 // stays below need - savings_of_earlier_slots. Every slot before the first slot
 // x* whose inclusive prefix reaches `need` is applied in full, slots after x*
 // not at all, and x* up to the first operation whose exclusive prefix reaches
-// its requirement. This kernel computes x* and that cut, then gives every
-// block its quant (the largest applied step), its word count and its offset.
+// its requirement (the cut).
+//
+// The blocks are split into slices of consecutive blocks, one 1024-thread CTA
+// each. Every CTA scans the histogram for x* itself; a CTA whose slice meets
+// the x* subdivision also finds the cut (from the savings of that subdivision
+// up to the end of its slice). It then gives its blocks their quant (the
+// largest applied step), word counts and offsets: the slice's own scan plus
+// the totals the preceding slices publish.
+constexpr int kOwnBatch = 2;           // RD rows per thread with their loads in flight together
+constexpr int kSliceWaitSpins = 1 << 20; // bounded wait for one preceding slice's total
+
+// Calls f(blk, row) for blocks [b0, b1) in order, the first kOwnBatch rows from
+// `first`, the rest loaded kOwnBatch at a time.
+template <typename F>
+__device__ __forceinline__ void for_rows(const EncodeBuffers &buf, int b0, int b1, const RawRD (&first)[kOwnBatch],
+                                         F f)
+{
+#pragma unroll
+	for (int i = 0; i < kOwnBatch; i++)
+		if (b0 + i < b1)
+			f(b0 + i, first[i]);
+	for (int base = b0 + kOwnBatch; base < b1; base += kOwnBatch)
+	{
+		RawRD r[kOwnBatch];
+#pragma unroll
+		for (int i = 0; i < kOwnBatch; i++)
+			if (base + i < b1)
+				r[i] = load_raw_rd(buf, base + i);
+#pragma unroll
+		for (int i = 0; i < kOwnBatch; i++)
+			if (base + i < b1)
+				f(base + i, r[i]);
+	}
+}
+
+__device__ __forceinline__ void load_rows(const EncodeBuffers &buf, int b0, int b1, RawRD (&r)[kOwnBatch])
+{
+#pragma unroll
+	for (int i = 0; i < kOwnBatch; i++)
+		if (b0 + i < b1)
+			r[i] = load_raw_rd(buf, b0 + i);
+}
+
 __global__ void __launch_bounds__(1024) resolve_kernel(const ResolveParams p, const EncodeBuffers buf)
 {
 	__shared__ uint32_t scan[kHistSize];
 	__shared__ uint32_t warp_sums[32];
+	__shared__ unsigned long long warp_sums64[32];
 	__shared__ int s_xstar;
 	__shared__ uint32_t s_cut;
-	pdl_trigger();
+	__shared__ unsigned long long s_base;
 	RateControlState *rc = buf.rc;
 	const int t = threadIdx.x;
 	const int nblocks = p.block_count_32x32;
-	const int nbps = p.blocks_per_subdivision;
+	const int slice = blockIdx.x, nslices = gridDim.x;
+	const int per_slice = (nblocks + nslices - 1) / nslices;
+	const int s0 = min(slice * per_slice, nblocks), s1 = min(s0 + per_slice, nblocks);
+	const int per = (s1 - s0 + 1023) / 1024;
+	const int b0 = min(s0 + t * per, s1), b1 = min(b0 + per, s1);
+	// Every quantiser has finished once the wait returns. The packer is released
+	// only then, because it reads their output before its own wait.
 	pdl_wait();
+	pdl_trigger();
 
+	RawRD own[kOwnBatch];
+	load_rows(buf, b0, b1, own);
 	const uint32_t a = __ldcg(&rc->histogram[2 * t]), b = __ldcg(&rc->histogram[2 * t + 1]);
 	const uint32_t consumed = __ldcg(&rc->consumed);
-	uint32_t total;
-	const uint32_t excl = block_exclusive_scan_1024(a + b, warp_sums, total);
-	scan[2 * t] = excl + a;
-	scan[2 * t + 1] = excl + a + b;
 	if (t == 0)
 	{
 		s_xstar = -1;
 		s_cut = 0xffffffffu;
 	}
+	uint32_t total;
+	const uint32_t excl = block_exclusive_scan_1024(a + b, warp_sums, total);
+	scan[2 * t] = excl + a;
+	scan[2 * t + 1] = excl + a + b;
 	__syncthreads();
 
 	const int64_t need = int64_t(consumed) - int64_t(p.target_words);
@@ -733,64 +790,96 @@ __global__ void __launch_bounds__(1024) resolve_kernel(const ResolveParams p, co
 	__syncthreads();
 	const int xstar = s_xstar;
 
-	// Each thread owns a contiguous run of blocks, so every pass below needs
-	// only one block-wide scan.
-	if (xstar >= 0)
+	const int start = xstar >= 0 ? (xstar & (kSubdivisions - 1)) * p.blocks_per_subdivision : 0;
+	const int end = xstar >= 0 ? min(start + p.blocks_per_subdivision, nblocks) : 0;
+	if (xstar >= 0 && s0 < end && s1 > start)
 	{
+		// The cut, as far as this slice needs it: scan the savings at bucket b*
+		// of the x* subdivision's blocks up to the end of the slice.
 		const int64_t required = need - (xstar > 0 ? int64_t(scan[xstar - 1]) : 0);
 		const uint32_t bk = uint32_t(xstar >> 4);
-		const int start = (xstar & (kSubdivisions - 1)) * nbps;
-		const int end = min(start + nbps, nblocks);
-		const int per = max(end - start + 1023, 0) / 1024;
-		const int b0 = min(start + t * per, max(end, start)), b1 = min(b0 + per, end);
+		const int c1 = min(end, s1);
+		const int cper = (c1 - start + 1023) / 1024;
+		const int c0 = min(start + t * cper, c1), c0e = min(c0 + cper, c1);
+		RawRD r0[kOwnBatch];
+		load_rows(buf, c0, c0e, r0);
 		uint32_t local = 0;
-		for (int blk = b0; blk < b1; blk++)
-			local += op_saving_at_bucket(buf, blk, bk);
+		for_rows(buf, c0, c0e, r0, [&](int, const RawRD &r) { local += op_saving_at_bucket(r, bk); });
 		uint32_t tot;
 		uint32_t ex = block_exclusive_scan_1024(local, warp_sums, tot);
-		for (int blk = b0; blk < b1; blk++)
-		{
-			const uint32_t sv = op_saving_at_bucket(buf, blk, bk);
-			if (sv != 0 && int64_t(ex) >= required)
+		bool found = false;
+		for_rows(buf, c0, c0e, r0, [&](int blk, const RawRD &r) {
+			const uint32_t sv = op_saving_at_bucket(r, bk);
+			if (!found && sv != 0 && int64_t(ex) >= required)
 			{
 				atomicMin(&s_cut, uint32_t(blk));
-				break;
+				found = true;
 			}
 			ex += sv;
-		}
+		});
+		__syncthreads();
+		if (t == 0 && s_cut != 0xffffffffu)
+			rc->block_cut = s_cut; // every slice that reaches the cut finds the same block
 	}
-	__syncthreads();
 	const uint32_t cut = s_cut;
 
-	const int per = (nblocks + 1023) / 1024;
-	const int b0 = min(t * per, nblocks), b1 = min(b0 + per, nblocks);
-	uint32_t local = 0, local_nz = 0;
-	for (int blk = b0; blk < b1; blk++)
-	{
+	// Word counts of this thread's run, the slice scan, then the slice's base
+	// from the totals of the preceding slices.
+	unsigned long long local = 0; // words << 32 | non-empty blocks << 1
+	for_rows(buf, b0, b1, own, [&](int blk, const RawRD &r) {
 		int q;
-		const uint32_t words = block_words(buf, blk, blk >> p.subdivision_shift, xstar, cut, q);
-		buf.quant[blk] = q;
-		buf.block_meta[2 * blk + 0] = local;
-		buf.block_meta[2 * blk + 1] = words;
-		local += words;
-		local_nz += words != 0 ? 1u : 0u;
-	}
-	uint32_t carry;
-	const uint32_t base = block_exclusive_scan_1024(local, warp_sums, carry);
-	for (int blk = b0; blk < b1; blk++)
-		buf.block_meta[2 * blk + 0] += base;
-	uint32_t non_zero;
-	block_exclusive_scan_1024(local_nz, warp_sums, non_zero);
-
+		const uint32_t w = block_words(r, blk, blk >> p.subdivision_shift, xstar, cut, q);
+		local += (uint64_t(w) << 32) | (uint64_t(w != 0 ? 1 : 0) << 1);
+	});
+	unsigned long long slice_sum;
+	const unsigned long long run_excl = block_exclusive_scan_1024(local, warp_sums64, slice_sum);
 	if (t == 0)
+		st_release_u64(&rc->slice_total[slice], slice_sum | 1ull);
+	unsigned long long pred = 0;
+	if (t < slice)
 	{
-		rc->total_words = carry;
-		rc->non_zero_blocks = non_zero;
+		// Every slice CTA is resident (the grid is at most kMaxResolveSlices
+		// CTAs and the packer launches only after all of them started), so the
+		// wait ends; it is bounded all the same.
+		unsigned long long v;
+		int spins = 0;
+		while (((v = ld_acquire_u64(&rc->slice_total[t])) & 1ull) == 0ull)
+		{
+			if (++spins > kSliceWaitSpins)
+			{
+				atomicOr(&rc->error, kErrorSliceWait);
+				v = 1ull;
+				break;
+			}
+			__nanosleep(64);
+		}
+		pred = v & ~1ull;
+	}
+	unsigned long long base_total;
+	(void)block_exclusive_scan_1024(pred, warp_sums64, base_total);
+	if (t == 0)
+		s_base = base_total;
+	__syncthreads();
+	unsigned long long pos = s_base + run_excl;
+	for_rows(buf, b0, b1, own, [&](int blk, const RawRD &r) {
+		int q;
+		const uint32_t w = block_words(r, blk, blk >> p.subdivision_shift, xstar, cut, q);
+		buf.quant[blk] = q;
+		*reinterpret_cast<uint2 *>(buf.block_meta + 2 * size_t(blk)) = make_uint2(uint32_t(pos >> 32), w);
+		pos += uint64_t(w) << 32;
+	});
+
+	if (t == 0 && slice == nslices - 1)
+	{
+		const unsigned long long all = s_base + slice_sum;
+		const uint32_t total_words = uint32_t(all >> 32);
+		const uint32_t non_zero = uint32_t(all & 0xffffffffull) >> 1;
 		rc->xstar = xstar;
-		rc->block_cut = cut;
 		rc->sequence = p.sequence & 7u;
-		if (2 + carry > buf.stream_capacity_words)
-			rc->error |= 1u;
+		rc->total_words = total_words;
+		rc->non_zero_blocks = non_zero;
+		if (2 + uint64_t(total_words) > buf.stream_capacity_words)
+			atomicOr(&rc->error, kErrorStreamCapacity);
 		// Start-of-frame sequence header (bitstream.md:250-265).
 		buf.stream[0] = uint32_t(p.width - 1) | (uint32_t(p.height - 1) << 14) | ((p.sequence & 7u) << 28) | (1u << 31);
 		buf.stream[1] = (non_zero & 0xffffffu) | (uint32_t(p.chroma444 ? 1 : 0) << 26);
@@ -819,14 +908,26 @@ __global__ void __launch_bounds__(128) pack_kernel(const BlockParams p, const En
 	const int x8 = bx32 * 4 + lx, y8 = by32 * 4 + ly;
 	const bool in_range = x8 < L.blocks8_x && y8 < L.blocks8_y;
 	const int ox = bx32 * 32 + lx * 8 + sub_x(sub), oy = by32 * 32 + ly * 8 + sub_y(sub);
+
+	// The resolve kernel releases this grid only after every quantiser has
+	// finished, so coefficients and code words can be fetched before the wait;
+	// only the rate-control decisions come from the resolve kernel itself.
+	const uint32_t cw0 = in_range ? __ldcg(&buf.code_words[B.block8_offset + y8 * B.block8_stride + x8]) : 0u;
+	float coef[8];
+#pragma unroll
+	for (int i = 0; i < 8; i++)
+	{
+		const int64_t idx = B.offset + int64_t(oy + (i & 1)) * L.pitch + ox + (i >> 1);
+		coef[i] = L.fp16 ? __half2float(__ldcg(buf.coef16 + idx)) : __ldcg(buf.coef32 + idx);
+	}
 	pdl_wait();
 
-	const uint32_t words = __ldcg(&buf.block_meta[2 * blk + 1]);
+	const uint2 meta = __ldcg(reinterpret_cast<const uint2 *>(buf.block_meta) + blk);
+	const int quant = __ldcg(&buf.quant[blk]);
+	const uint32_t words = meta.y;
 	if (words == 0)
 		return;
-	const uint32_t offset = __ldcg(&buf.block_meta[2 * blk + 0]);
-	const int quant = __ldcg(&buf.quant[blk]);
-	const uint32_t cw0 = in_range ? __ldcg(&buf.code_words[B.block8_offset + y8 * B.block8_stride + x8]) : 0u;
+	const uint32_t offset = meta.x;
 	const uint32_t cw = quantize_code_word(cw0, quant);
 	const bool active = (cw & 0xffffu) != 0;
 
@@ -837,8 +938,7 @@ __global__ void __launch_bounds__(128) pack_kernel(const BlockParams p, const En
 #pragma unroll
 	for (int i = 0; i < 8; i++)
 	{
-		const int64_t idx = B.offset + int64_t(oy + (i & 1)) * L.pitch + ox + (i >> 1);
-		const float c = L.fp16 ? __half2float(__ldcg(buf.coef16 + idx)) : __ldcg(buf.coef32 + idx);
+		const float c = coef[i];
 		float v = __fmul_rn(__fmul_rn(c, B.quant_resolution), qs);
 		v = fminf(fmaxf(v, -kMaxScaledMagnitude), kMaxScaledMagnitude);
 		mag[i] = uint32_t(abs(int(v)));
@@ -949,7 +1049,7 @@ __global__ void __launch_bounds__(128) pack_kernel(const BlockParams p, const En
 	const uint32_t expect = (bits + 31) / 32 + 2;
 	const bool fits = words <= uint32_t(kMaxBlockWords) && 2 + offset + words <= buf.stream_capacity_words;
 	if (t == 0 && (expect != words || !fits))
-		atomicOr(&buf.rc->error, 2u);
+		atomicOr(&buf.rc->error, kErrorWordCount);
 	if (!fits)
 		return;
 	uint32_t *dst = buf.stream + 2 + offset;
@@ -988,7 +1088,8 @@ void launch_quant_pretransformed(const BlockParams &p, const EncodeBuffers &buf,
 
 void launch_resolve(const ResolveParams &p, const EncodeBuffers &buf, cudaStream_t stream)
 {
-	LaunchConfig lc(dim3(1), dim3(1024), stream, true);
+	const int slices = std::min((p.block_count_32x32 + 1023) / 1024, kMaxResolveSlices);
+	LaunchConfig lc(dim3(std::max(slices, 1)), dim3(1024), stream, true);
 	cudaLaunchKernelEx(&lc.cfg, resolve_kernel, p, buf);
 }
 

@@ -336,6 +336,9 @@ BlockParams make_block_params(const Geometry &g)
 		p.level[level] = g.level[level];
 	p.block_count_32x32 = g.block_count_32x32;
 	p.subdivision_shift = g.subdivision_shift;
+	p.width = g.width;
+	p.height = g.height;
+	p.chroma444 = g.chroma444;
 	for (int level = kLevels - 1; level >= 0; level--)
 		for (int comp = 0; comp < kComponents; comp++)
 			for (int band = 0; band < 4; band++)

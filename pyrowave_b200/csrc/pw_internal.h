@@ -86,7 +86,11 @@ __host__ __device__ inline void unpack_job(uint32_t j, int &level, int &comp, in
 	by = int(j >> 20);
 }
 
-// Rate-control scratch, one per encoder instance (device memory).
+// The resolve kernel splits the blocks into at most this many slices, one CTA each.
+constexpr int kMaxResolveSlices = 128;
+
+// Rate-control scratch, one per encoder instance (device memory), cleared
+// before every frame.
 struct RateControlState
 {
 	uint32_t histogram[kHistSize]; // savings per (bucket, subdivision)
@@ -98,7 +102,14 @@ struct RateControlState
 	uint32_t block_cut;            // ops of blocks >= this in the partial subdivision are not applied
 	uint32_t sequence;
 	uint32_t pad;
+	// Per resolve slice: words << 32 | non-empty blocks << 1 | 1 once published.
+	unsigned long long slice_total[kMaxResolveSlices];
 };
+
+// Error bits of RateControlState::error.
+constexpr uint32_t kErrorStreamCapacity = 1u; // the coded frame does not fit the stream buffer
+constexpr uint32_t kErrorWordCount = 2u;      // a packed block's size differs from the rate-control estimate
+constexpr uint32_t kErrorSliceWait = 4u;      // a resolve slice gave up waiting for a preceding slice's total
 
 // Buffers the encode kernels read and write.
 struct EncodeBuffers
@@ -183,7 +194,8 @@ constexpr int kMaxBands = 48;
 struct BlockParams
 {
 	LevelDesc level[kLevels];
-	int32_t nbands, block_count_32x32, subdivision_shift, pad;
+	int32_t nbands, block_count_32x32, subdivision_shift;
+	int32_t width, height, chroma444; // frame size and chroma format (sequence header)
 	BandEntry band[kMaxBands]; // in block index order
 };
 
