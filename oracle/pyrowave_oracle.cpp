@@ -3,8 +3,11 @@
 // A line-by-line CPU restatement of the reference's encode/decode path. Every
 // function cites the reference file:line it follows. Arithmetic conventions,
 // chosen so that the CUDA implementation can be compared bit for bit:
-//   * FP32 operations are separate IEEE round-to-nearest operations, no FMA
-//     contraction (build with -ffp-contract=off), no fast-math.
+//   * FP32 operations are IEEE round-to-nearest operations with no implicit
+//     contraction (build with -ffp-contract=off), no fast-math. Where a shader
+//     statement is a multiply-add (a lifting step x += c * (a + b), the squared
+//     sums of dot()), it is one fused multiply-add (std::fmaf), which is what
+//     an FMA-capable GPU compiles those statements to.
 //   * Subgroup float reductions use the xor-butterfly order (lanes 1,2,4,8).
 //   * FP16 conversions are IEEE round-to-nearest-even.
 //   * The rate-control bucket index uses the exactly rounded value of
@@ -228,17 +231,17 @@ template <> struct Lift<float>
 	static float add(float a, float b) { return a + b; }
 	static void fwd(float *e, int len)
 	{
-		for (int j = 1; j + 1 < len; j += 2) { float t = e[j - 1] + e[j + 1]; t = ALPHA * t; e[j] = e[j] + t; }
-		for (int j = 2; j + 1 < len; j += 2) { float t = e[j - 1] + e[j + 1]; t = BETA * t; e[j] = e[j] + t; }
-		for (int j = 3; j + 1 < len; j += 2) { float t = e[j - 1] + e[j + 1]; t = GAMMA * t; e[j] = e[j] + t; }
-		for (int j = 4; j + 1 < len; j += 2) { float t = e[j - 1] + e[j + 1]; t = DELTA * t; e[j] = e[j] + t; }
+		for (int j = 1; j + 1 < len; j += 2) e[j] = std::fmaf(ALPHA, e[j - 1] + e[j + 1], e[j]);
+		for (int j = 2; j + 1 < len; j += 2) e[j] = std::fmaf(BETA, e[j - 1] + e[j + 1], e[j]);
+		for (int j = 3; j + 1 < len; j += 2) e[j] = std::fmaf(GAMMA, e[j - 1] + e[j + 1], e[j]);
+		for (int j = 4; j + 1 < len; j += 2) e[j] = std::fmaf(DELTA, e[j - 1] + e[j + 1], e[j]);
 	}
 	static void inv(float *e, int len)
 	{
-		for (int j = 2; j + 1 < len; j += 2) { float t = e[j - 1] + e[j + 1]; t = DELTA * t; e[j] = e[j] - t; }
-		for (int j = 3; j + 1 < len; j += 2) { float t = e[j - 1] + e[j + 1]; t = GAMMA * t; e[j] = e[j] - t; }
-		for (int j = 4; j + 1 < len; j += 2) { float t = e[j - 1] + e[j + 1]; t = BETA * t; e[j] = e[j] - t; }
-		for (int j = 5; j + 1 < len; j += 2) { float t = e[j - 1] + e[j + 1]; t = ALPHA * t; e[j] = e[j] - t; }
+		for (int j = 2; j + 1 < len; j += 2) e[j] = std::fmaf(-DELTA, e[j - 1] + e[j + 1], e[j]);
+		for (int j = 3; j + 1 < len; j += 2) e[j] = std::fmaf(-GAMMA, e[j - 1] + e[j + 1], e[j]);
+		for (int j = 4; j + 1 < len; j += 2) e[j] = std::fmaf(-BETA, e[j - 1] + e[j + 1], e[j]);
+		for (int j = 5; j + 1 < len; j += 2) e[j] = std::fmaf(-ALPHA, e[j - 1] + e[j + 1], e[j]);
 	}
 	static float low_scale() { return INV_KF; }
 	static float high_scale() { return KF; }
@@ -588,9 +591,9 @@ float butterfly16(const float v[16])
 float dot4(const float *e)
 {
 	float s = e[0] * e[0];
-	s = s + e[1] * e[1];
-	s = s + e[2] * e[2];
-	s = s + e[3] * e[3];
+	s = std::fmaf(e[1], e[1], s);
+	s = std::fmaf(e[2], e[2], s);
+	s = std::fmaf(e[3], e[3], s);
 	return s;
 }
 

@@ -1,10 +1,11 @@
 // Device helpers shared by the sm_100a kernels.
 //
 // Floating point conventions (mirrored by the CPU oracle, which is how the two
-// are compared bit for bit): every FP32 operation is a separate IEEE
-// round-to-nearest operation (the library is built with --fmad=false and the
-// lifting steps are written with explicit _rn intrinsics), reductions use the
-// xor-butterfly order, FP16 rounding is round-to-nearest-even.
+// are compared bit for bit): every FP32 operation is an IEEE round-to-nearest
+// operation written out with explicit _rn intrinsics; the library is built with
+// --fmad=false, so the only fused multiply-adds are the explicit ones (lifting
+// updates and squared sums). Reductions use the xor-butterfly order, FP16
+// rounding is round-to-nearest-even.
 #pragma once
 
 #include "pw_internal.h"
@@ -56,17 +57,14 @@ __device__ __forceinline__ int inv_index_high(int p, int n)
 	return mirrored_repeat(q + 1 >= n ? p + 1 : p, n);
 }
 
+// One lifting update v +/- c * (a + b): a rounded add, then one fused multiply-add.
 __device__ __forceinline__ float lift_add(float v, float c, float a, float b)
 {
-	float t = __fadd_rn(a, b);
-	t = __fmul_rn(c, t);
-	return __fadd_rn(v, t);
+	return __fmaf_rn(c, __fadd_rn(a, b), v);
 }
 __device__ __forceinline__ float lift_sub(float v, float c, float a, float b)
 {
-	float t = __fadd_rn(a, b);
-	t = __fmul_rn(c, t);
-	return __fsub_rn(v, t);
+	return __fmaf_rn(-c, __fadd_rn(a, b), v);
 }
 
 // Forward lifting over a register window e[0..N); window position j has the

@@ -128,13 +128,13 @@ __device__ __forceinline__ void quant_analyze_block(const float *tile, int tile_
 	float drop;
 	{
 		float s0 = __fmul_rn(v[0], v[0]);
-		s0 = __fadd_rn(s0, __fmul_rn(v[1], v[1]));
-		s0 = __fadd_rn(s0, __fmul_rn(v[2], v[2]));
-		s0 = __fadd_rn(s0, __fmul_rn(v[3], v[3]));
+		s0 = __fmaf_rn(v[1], v[1], s0);
+		s0 = __fmaf_rn(v[2], v[2], s0);
+		s0 = __fmaf_rn(v[3], v[3], s0);
 		float s1 = __fmul_rn(v[4], v[4]);
-		s1 = __fadd_rn(s1, __fmul_rn(v[5], v[5]));
-		s1 = __fadd_rn(s1, __fmul_rn(v[6], v[6]));
-		s1 = __fadd_rn(s1, __fmul_rn(v[7], v[7]));
+		s1 = __fmaf_rn(v[5], v[5], s1);
+		s1 = __fmaf_rn(v[6], v[6], s1);
+		s1 = __fmaf_rn(v[7], v[7], s1);
 		drop = __fmul_rn(__fadd_rn(s0, s1), iqs);
 		drop = __fadd_rn(drop, __shfl_xor_sync(0xffffffffu, drop, 1));
 		drop = __fadd_rn(drop, __shfl_xor_sync(0xffffffffu, drop, 2));
@@ -153,20 +153,27 @@ __device__ __forceinline__ void quant_analyze_block(const float *tile, int tile_
 	for (int q = 1; q <= warp_msb; q++)
 	{
 		// compute_square_error + compute_quant_stats at q (wavelet_quant.comp:113-165).
+		// floor(|v| / 2^q) in float arithmetic, exactly: scale by 2^-q, then
+		// truncate by adding 2^23 with round-toward-zero and subtracting it again
+		// (the quotient is below 2^15). The reconstruction fl * 2^q + 2^(q-1) is
+		// an exact integer, so err equals the integer formulation above.
+		const float pq = __int_as_float((127 + q) << 23);
+		const float ipq = __int_as_float((127 - q) << 23);
+		const float hq = __int_as_float((126 + q) << 23);
 		int nsig = 0;
 		float e0 = 0.0f, e1 = 0.0f;
 #pragma unroll
 		for (int i = 0; i < 8; i++)
 		{
-			const uint32_t iv = mag[i] >> q;
-			nsig += iv != 0u ? 1 : 0;
-			const float recon = iv != 0u ? float((iv << q) + (1u << (q - 1))) : 0.0f;
+			const float fl = __fsub_rn(__fadd_rz(__fmul_rn(av[i], ipq), 8388608.0f), 8388608.0f);
+			const bool sig = fl != 0.0f;
+			nsig += sig ? 1 : 0;
+			const float recon = sig ? __fmaf_rn(fl, pq, hq) : 0.0f;
 			const float err = __fsub_rn(av[i], recon);
-			const float sq = __fmul_rn(err, err);
 			if (i < 4)
-				e0 = (i == 0) ? sq : __fadd_rn(e0, sq);
+				e0 = (i == 0) ? __fmul_rn(err, err) : __fmaf_rn(err, err, e0);
 			else
-				e1 = (i == 4) ? sq : __fadd_rn(e1, sq);
+				e1 = (i == 4) ? __fmul_rn(err, err) : __fmaf_rn(err, err, e1);
 		}
 		float se = __fmul_rn(__fmul_rn(__fadd_rn(e0, e1), rdo), iqs);
 		se = __fadd_rn(se, __shfl_xor_sync(0xffffffffu, se, 1));
@@ -284,6 +291,7 @@ struct DwtShared
 	float in[kTileIn][kInPitch]; // input tile, later the four 32x32 band tiles
 	float h[kTileIn][kHPitch];   // after horizontal lifting: low in 0..31, high in 32..63
 	QuantGroupShared q[2];
+	float unorm[256];            // unorm8_centered(u) for every byte value
 };
 
 __device__ __forceinline__ float unorm8_centered(uint32_t u)
@@ -326,6 +334,9 @@ __global__ void __launch_bounds__(kDwtThreads, 4) dwt_forward_kernel(const Level
 		else
 			sh.yidx[k - kTileIn] = fwd_index(ty * 64 - 4 + (k - kTileIn), res_h, al_h);
 	}
+	if (from_plane)
+		for (int u = threadIdx.x; u < 256; u += kDwtThreads)
+			sh.unorm[u] = unorm8_centered(uint32_t(u));
 	__syncthreads();
 	pdl_wait();
 
@@ -363,7 +374,7 @@ __global__ void __launch_bounds__(kDwtThreads, 4) dwt_forward_kernel(const Level
 					const int i = k / kVecPerRow, j = k - i * kVecPerRow;
 #pragma unroll
 					for (int b = 0; b < 4; b++)
-						sh.in[i][4 * j + b] = unorm8_centered((v[u] >> (8 * b)) & 0xffu);
+						sh.in[i][4 * j + b] = sh.unorm[(v[u] >> (8 * b)) & 0xffu];
 				}
 			}
 		}
@@ -386,7 +397,7 @@ __global__ void __launch_bounds__(kDwtThreads, 4) dwt_forward_kernel(const Level
 					if (k < kTileIn * kTileIn)
 					{
 						const int i = k / kTileIn, j = k - i * kTileIn;
-						sh.in[i][j] = unorm8_centered(v[u]);
+						sh.in[i][j] = sh.unorm[v[u] & 0xffu];
 					}
 				}
 			}
