@@ -244,7 +244,6 @@ __global__ void __launch_bounds__(128) dequant_kernel(const BlockParams p, const
 		store_coef(in.coef32, in.coef16, f16, B.offset + int64_t(oy + (i & 1)) * L.pitch + ox + (i >> 1), v[i]);
 }
 
-constexpr int kIdwtThreads = 256;
 constexpr int kBandTile = 36; // 32 band samples + 2 on each side
 constexpr int kBandTilePitch = 37;
 
@@ -256,9 +255,15 @@ struct IdwtShared
 };
 
 // One inverse level for a 64x64 output tile (32x32 band tile) of one component.
-__global__ void __launch_bounds__(kIdwtThreads) idwt_kernel(const LevelParams p, const DecodeInput in,
-                                                             const PlaneOutput out)
+// Large levels run 256-thread CTAs, several per SM; small levels (fewer tiles
+// than SMs) run 1024-thread CTAs whose lifting items cover half as many
+// outputs, shortening every serial phase.
+template <int kThreads>
+__global__ void __launch_bounds__(kThreads) idwt_kernel(const LevelParams p, const DecodeInput in, const PlaneOutput out)
 {
+	constexpr int kOut = kThreads >= 1024 ? 8 : 16; // outputs per lifting item
+	constexpr int kSegs = 64 / kOut;
+	constexpr int kWin = kOut + 8;
 	__shared__ IdwtShared sh;
 	pdl_trigger();
 	const int level = p.level;
@@ -269,7 +274,7 @@ __global__ void __launch_bounds__(kIdwtThreads) idwt_kernel(const LevelParams p,
 	const int nx = L.width, ny = L.height;
 	const bool final_level = level == 0 || (level == 1 && comp != 0 && !p.chroma444);
 
-	for (int k = threadIdx.x; k < 4 * kBandTile; k += kIdwtThreads)
+	for (int k = threadIdx.x; k < 4 * kBandTile; k += kThreads)
 	{
 		const int j = k % kBandTile, which = k / kBandTile;
 		const int px = tx * 32 - 2 + j, py = ty * 32 - 2 + j;
@@ -297,12 +302,12 @@ __global__ void __launch_bounds__(kIdwtThreads) idwt_kernel(const LevelParams p,
 	{
 		constexpr int kVecPerRow = 10;
 		constexpr int kVecs = 4 * kBandTile * kVecPerRow; // 1440
-		constexpr int kIters = (kVecs + kIdwtThreads - 1) / kIdwtThreads;
+		constexpr int kIters = (kVecs + kThreads - 1) / kThreads;
 		float4 v[kIters];
 #pragma unroll
 		for (int u = 0; u < kIters; u++)
 		{
-			const int k = threadIdx.x + u * kIdwtThreads;
+			const int k = threadIdx.x + u * kThreads;
 			const int b = k / (kBandTile * kVecPerRow);
 			const int r = k - b * kBandTile * kVecPerRow;
 			const int i = r / kVecPerRow, j = r - i * kVecPerRow;
@@ -326,7 +331,7 @@ __global__ void __launch_bounds__(kIdwtThreads) idwt_kernel(const LevelParams p,
 #pragma unroll
 		for (int u = 0; u < kIters; u++)
 		{
-			const int k = threadIdx.x + u * kIdwtThreads;
+			const int k = threadIdx.x + u * kThreads;
 			if (k >= kVecs)
 				continue;
 			const int b = k / (kBandTile * kVecPerRow);
@@ -345,14 +350,14 @@ __global__ void __launch_bounds__(kIdwtThreads) idwt_kernel(const LevelParams p,
 	else
 	{
 		constexpr int kN = 4 * kBandTile * kBandTile;
-		constexpr int kIdwtGen = (kN + kIdwtThreads - 1) / kIdwtThreads; // every load in flight at once
-		for (int base = threadIdx.x; base < kN; base += kIdwtThreads * kIdwtGen)
+		constexpr int kIdwtGen = (kN + kThreads - 1) / kThreads; // every load in flight at once
+		for (int base = threadIdx.x; base < kN; base += kThreads * kIdwtGen)
 		{
 			float v[kIdwtGen];
 #pragma unroll
 			for (int u = 0; u < kIdwtGen; u++)
 			{
-				const int k = base + u * kIdwtThreads;
+				const int k = base + u * kThreads;
 				const int b = k / (kBandTile * kBandTile);
 				const int r = k - b * kBandTile * kBandTile;
 				const int i = r / kBandTile, j = r - i * kBandTile;
@@ -366,7 +371,7 @@ __global__ void __launch_bounds__(kIdwtThreads) idwt_kernel(const LevelParams p,
 #pragma unroll
 			for (int u = 0; u < kIdwtGen; u++)
 			{
-				const int k = base + u * kIdwtThreads;
+				const int k = base + u * kThreads;
 				if (k < kN)
 				{
 					const int b = k / (kBandTile * kBandTile);
@@ -379,42 +384,43 @@ __global__ void __launch_bounds__(kIdwtThreads) idwt_kernel(const LevelParams p,
 	}
 	__syncthreads();
 
-	// Vertical lifting: 36 band columns x {horizontal low: LL/LH, horizontal high: HL/HH} x 4 segments.
-	for (int item = threadIdx.x; item < kBandTile * 2 * 4; item += kIdwtThreads)
+	// Vertical lifting: 36 band columns x {horizontal low: LL/LH, horizontal high: HL/HH} x kSegs segments.
+	for (int item = threadIdx.x; item < kBandTile * 2 * kSegs; item += kThreads)
 	{
 		const int col = item % kBandTile;
 		const int which = (item / kBandTile) & 1;
 		const int seg = item / (2 * kBandTile);
 		const int b_low = which ? 1 : 0, b_high = which ? 3 : 2;
-		float e[24];
+		float e[kWin];
 #pragma unroll
-		for (int jj = 0; jj < 24; jj++)
+		for (int jj = 0; jj < kWin; jj++)
 		{
-			const int q = seg * 16 + jj;
+			const int q = seg * kOut + jj;
 			const int i = q >> 1;
 			e[jj] = (q & 1) ? __fmul_rn(sh.band[b_high][i][col], kInvK) : __fmul_rn(sh.band[b_low][i][col], kK);
 		}
 		lift_inverse(e);
 #pragma unroll
-		for (int jj = 4; jj < 20; jj++)
-			sh.v[which][seg * 16 + jj - 4][col] = e[jj];
+		for (int jj = 4; jj < 4 + kOut; jj++)
+			sh.v[which][seg * kOut + jj - 4][col] = e[jj];
 	}
 	__syncthreads();
 
-	// Horizontal lifting: 64 output rows x 4 segments of 16 outputs.
+	// Horizontal lifting: 64 output rows x kSegs segments of kOut outputs.
+	for (int item = threadIdx.x; item < 64 * kSegs; item += kThreads)
 	{
-		const int row = threadIdx.x & 63, seg = threadIdx.x >> 6;
-		float e[24];
+		const int row = item & 63, seg = item >> 6;
+		float e[kWin];
 #pragma unroll
-		for (int jj = 0; jj < 24; jj++)
+		for (int jj = 0; jj < kWin; jj++)
 		{
-			const int q = seg * 16 + jj;
+			const int q = seg * kOut + jj;
 			const int i = q >> 1;
 			e[jj] = (q & 1) ? __fmul_rn(sh.v[1][row][i], kInvK) : __fmul_rn(sh.v[0][row][i], kK);
 		}
 		lift_inverse(e);
 		const int gy = ty * 64 + row;
-		const int gx0 = tx * 64 + seg * 16;
+		const int gx0 = tx * 64 + seg * kOut;
 		if (final_level)
 		{
 			const int pw = p.plane_width[comp], ph = p.plane_height[comp];
@@ -423,21 +429,29 @@ __global__ void __launch_bounds__(kIdwtThreads) idwt_kernel(const LevelParams p,
 			if (gy < ph)
 			{
 				uint8_t *dst = plane + size_t(gy) * opitch;
-				uint32_t packed[4] = {0, 0, 0, 0};
+				uint32_t packed[kOut / 4];
 #pragma unroll
-				for (int jj = 4; jj < 20; jj++)
+				for (int w = 0; w < kOut / 4; w++)
+					packed[w] = 0;
+#pragma unroll
+				for (int jj = 4; jj < 4 + kOut; jj++)
 				{
 					float f = __fadd_rn(e[jj], 0.5f);
 					f = fminf(fmaxf(f, 0.0f), 1.0f);
 					const uint32_t u = uint32_t(int(__fadd_rn(__fmul_rn(f, 255.0f), 0.5f)));
 					packed[(jj - 4) >> 2] |= u << (8 * ((jj - 4) & 3));
 				}
-				if (gx0 + 16 <= pw && (reinterpret_cast<uintptr_t>(dst + gx0) & 15u) == 0)
-					*reinterpret_cast<uint4 *>(dst + gx0) = make_uint4(packed[0], packed[1], packed[2], packed[3]);
+				if (gx0 + kOut <= pw && (reinterpret_cast<uintptr_t>(dst + gx0) & (kOut - 1)) == 0)
+				{
+					if constexpr (kOut == 16)
+						*reinterpret_cast<uint4 *>(dst + gx0) = make_uint4(packed[0], packed[1], packed[2], packed[3]);
+					else
+						*reinterpret_cast<uint2 *>(dst + gx0) = make_uint2(packed[0], packed[1]);
+				}
 				else
 				{
 #pragma unroll
-					for (int jj = 0; jj < 16; jj++)
+					for (int jj = 0; jj < kOut; jj++)
 						if (gx0 + jj < pw)
 							dst[gx0 + jj] = uint8_t(packed[jj >> 2] >> (8 * (jj & 3)));
 				}
@@ -451,24 +465,27 @@ __global__ void __launch_bounds__(kIdwtThreads) idwt_kernel(const LevelParams p,
 			if (gy < P.height)
 			{
 				const int64_t base = ll + int64_t(gy) * P.pitch + gx0;
-				if (gx0 + 16 <= P.width)
+				if (gx0 + kOut <= P.width)
 				{
 					if (pf16)
 					{
-						uint32_t hw[8];
 #pragma unroll
-						for (int k = 0; k < 8; k++)
+						for (int v = 0; v < kOut / 8; v++)
 						{
-							__half2 h2 = __floats2half2_rn(e[4 + 2 * k], e[5 + 2 * k]);
-							hw[k] = *reinterpret_cast<uint32_t *>(&h2);
+							uint32_t hw[4];
+#pragma unroll
+							for (int k = 0; k < 4; k++)
+							{
+								__half2 h2 = __floats2half2_rn(e[4 + 8 * v + 2 * k], e[5 + 8 * v + 2 * k]);
+								hw[k] = *reinterpret_cast<uint32_t *>(&h2);
+							}
+							*reinterpret_cast<uint4 *>(in.coef16 + base + 8 * v) = make_uint4(hw[0], hw[1], hw[2], hw[3]);
 						}
-						*reinterpret_cast<uint4 *>(in.coef16 + base) = make_uint4(hw[0], hw[1], hw[2], hw[3]);
-						*reinterpret_cast<uint4 *>(in.coef16 + base + 8) = make_uint4(hw[4], hw[5], hw[6], hw[7]);
 					}
 					else
 					{
 #pragma unroll
-						for (int k = 0; k < 4; k++)
+						for (int k = 0; k < kOut / 4; k++)
 							*reinterpret_cast<float4 *>(in.coef32 + base + 4 * k) =
 							    make_float4(e[4 + 4 * k], e[5 + 4 * k], e[6 + 4 * k], e[7 + 4 * k]);
 					}
@@ -476,7 +493,7 @@ __global__ void __launch_bounds__(kIdwtThreads) idwt_kernel(const LevelParams p,
 				else
 				{
 #pragma unroll
-					for (int jj = 4; jj < 20; jj++)
+					for (int jj = 4; jj < 4 + kOut; jj++)
 					{
 						const int gx = gx0 + jj - 4;
 						if (gx < P.width)
@@ -527,8 +544,16 @@ void launch_idwt_level(const LevelParams &p, const DecodeInput &in, const PlaneO
                        cudaStream_t stream)
 {
 	const dim3 grid(p.L.tiles_x * p.L.tiles_y, (p.level == 0 && !p.chroma444) ? 1 : 3);
-	LaunchConfig lc(grid, dim3(kIdwtThreads), stream, programmatic);
-	cudaLaunchKernelEx(&lc.cfg, idwt_kernel, p, in, out);
+	if (int(grid.x * grid.y) < kSmallLevelTiles)
+	{
+		LaunchConfig lc(grid, dim3(1024), stream, programmatic);
+		cudaLaunchKernelEx(&lc.cfg, idwt_kernel<1024>, p, in, out);
+	}
+	else
+	{
+		LaunchConfig lc(grid, dim3(256), stream, programmatic);
+		cudaLaunchKernelEx(&lc.cfg, idwt_kernel<256>, p, in, out);
+	}
 }
 
 void launch_pyramid_io(const BlockParams &p, float *canonical, float *coef32, __half *coef16, bool to_canonical,
@@ -537,8 +562,6 @@ void launch_pyramid_io(const BlockParams &p, float *canonical, float *coef32, __
 	pyramid_io_kernel<<<dim3(64, p.nbands), 256, 0, stream>>>(p, canonical, coef32, coef16, to_canonical ? 1 : 0);
 }
 
-const void *kernel_dequant() { return reinterpret_cast<const void *>(&dequant_kernel); }
-const void *kernel_idwt() { return reinterpret_cast<const void *>(&idwt_kernel); }
 } // namespace pw
 
 // ---------------------------------------------------------------------------

@@ -15,13 +15,10 @@ namespace pw
 {
 namespace
 {
-constexpr int kDwtThreads = 256;
 constexpr int kTileIn = 72;  // 64 input samples + 4-sample apron on each side
 constexpr int kInPitch = 73; // odd pitch: conflict-free column walks
 constexpr int kHPitch = 65;
 constexpr int kBandPitch = 33;
-// Loads per thread of an edge tile gathered through the index tables: all in flight at once.
-constexpr int kDwtGen = (kTileIn * kTileIn + kDwtThreads - 1) / kDwtThreads;
 
 // Reduction scratch of one 128-thread quantiser group (one 32x32 block).
 struct QuantGroupShared
@@ -33,18 +30,24 @@ struct QuantGroupShared
 // ---------------------------------------------------------------------------
 // Quantiser + RD analysis of one 32x32 block held in shared memory.
 //
-// Thread t of the 128-thread group owns one 4x2 sub-block: sub = t & 7,
-// 8x8 column lx = (t >> 3) & 3, 8x8 row ly = t >> 5 (one warp per 8x8 row),
-// the reference's mapping (wavelet_quant.comp:294-306).
+// A group of 128 * S threads handles the block. Thread t owns one 4x2
+// sub-block, sub = t & 7, in 8x8 column lx = (t >> 3) & 3 and 8x8 row
+// ly = (t >> 5) & 3 (one warp per 8x8 row, the reference's mapping,
+// wavelet_quant.comp:294-306), and the statistics of every S-th quant level
+// starting at 1 + (t >> 7): with S = 2 two threads share a sub-block's levels,
+// halving the serial loop. Each level's values are computed by exactly one
+// thread, in the same order, so the results do not depend on S.
 //
 // Every thread of the CTA must call this the same number of times (it contains
 // __syncthreads); `active` is false for groups without a block this round.
+template <int S>
 __device__ __forceinline__ void quant_analyze_block(const float *tile, int tile_pitch, bool active, int t,
                                                     QuantGroupShared &sh, const LevelDesc &L, const BandParam &B,
                                                     int subdivision_shift, int bx32, int by32,
                                                     const EncodeBuffers &buf)
 {
-	const int sub = t & 7, lx = (t >> 3) & 3, ly = t >> 5;
+	const int sub = t & 7, lx = (t >> 3) & 3, ly = (t >> 5) & 3;
+	const int r = t >> 7; // quant levels q with (q - 1) % S == r are this thread's
 	const int lane = threadIdx.x & 31;
 	const int x8 = bx32 * 4 + lx, y8 = by32 * 4 + ly;
 	const bool in_range = active && x8 < L.blocks8_x && y8 < L.blocks8_y;
@@ -150,7 +153,7 @@ __device__ __forceinline__ void quant_analyze_block(const float *tile, int tile_
 		d_lo = drop;
 
 	const int warp_msb = __reduce_max_sync(0xffffffffu, max(msb, 0));
-	for (int q = 1; q <= warp_msb; q++)
+	for (int q = 1 + r; q <= warp_msb; q += S)
 	{
 		// compute_square_error + compute_quant_stats at q (wavelet_quant.comp:113-165).
 		// floor(|v| / 2^q) in float arithmetic, exactly: scale by 2^-q, then
@@ -230,14 +233,23 @@ __device__ __forceinline__ void quant_analyze_block(const float *tile, int tile_
 	c_lo += __shfl_xor_sync(0xffffffffu, c_lo, 16);
 	c_hi += __shfl_xor_sync(0xffffffffu, c_hi, 8);
 	c_hi += __shfl_xor_sync(0xffffffffu, c_hi, 16);
+	// The thread that computed level sub (level 0: residue 0) and sub + 8 stores them.
+	const bool own_lo = sub == 0 ? r == 0 : (sub - 1) % S == r;
+	const bool own_hi = (sub + 7) % S == r;
 	if (lane < 8)
 	{
-		sh.dist[ly][sub] = d_lo;
-		sh.dist[ly][sub + 8] = d_hi;
-		sh.cost[ly][sub] = c_lo;
-		sh.cost[ly][sub + 8] = c_hi;
+		if (own_lo)
+		{
+			sh.dist[ly][sub] = d_lo;
+			sh.cost[ly][sub] = c_lo;
+		}
+		if (own_hi)
+		{
+			sh.dist[ly][sub + 8] = d_hi;
+			sh.cost[ly][sub + 8] = c_hi;
+		}
 	}
-	if (in_range && sub == 0)
+	if (in_range && sub == 0 && r == 0)
 		buf.code_words[B.block8_offset + y8 * B.block8_stride + x8] = cw;
 	__syncthreads();
 
@@ -290,7 +302,7 @@ struct DwtShared
 	int yidx[kTileIn];
 	float in[kTileIn][kInPitch]; // input tile, later the four 32x32 band tiles
 	float h[kTileIn][kHPitch];   // after horizontal lifting: low in 0..31, high in 32..63
-	QuantGroupShared q[2];
+	QuantGroupShared q[4];
 	float unorm[256];            // unorm8_centered(u) for every byte value
 };
 
@@ -299,11 +311,29 @@ __device__ __forceinline__ float unorm8_centered(uint32_t u)
 	return __fsub_rn(__fdiv_rn(float(u), 255.0f), 0.5f);
 }
 
+// Work split of the forward level for a CTA of kThreads threads. Large levels
+// run many 256-thread CTAs per SM; the small levels, with fewer tiles than
+// SMs, run 1024-thread CTAs that cut every serial phase: shorter lifting
+// windows per thread and all bands quantised in one round with two threads per
+// 4x2 sub-block.
+template <int kThreads> struct DwtSplit
+{
+	static constexpr int kSegPairs = kThreads >= 1024 ? 4 : 8; // output pairs per lifting item
+	static constexpr int kSegs = 32 / kSegPairs;                // items per row / column
+	static constexpr int kWin = 2 * kSegPairs + 8;              // lifting window (4 apron samples each side)
+	static constexpr int kQSplit = kThreads >= 1024 ? 2 : 1;    // threads per 4x2 sub-block in the quantiser
+	static constexpr int kGroupThreads = 128 * kQSplit;         // threads per quantised 32x32 block
+	static constexpr int kGroups = kThreads / kGroupThreads;    // 32x32 blocks quantised at once
+	static constexpr int kGen = (kTileIn * kTileIn + kThreads - 1) / kThreads; // edge-tile loads per thread
+};
+
 // One forward level for one 32x32 band tile of one component (64x64 input
 // samples). grid.x = tile, grid.y = component index among those at this level.
-__global__ void __launch_bounds__(kDwtThreads, 4) dwt_forward_kernel(const LevelParams p, const PlaneInput in,
-                                                                   const EncodeBuffers buf, const int fused)
+template <int kThreads>
+__global__ void __launch_bounds__(kThreads, kThreads >= 1024 ? 1 : 4)
+    dwt_forward_kernel(const LevelParams p, const PlaneInput in, const EncodeBuffers buf, const int fused)
 {
+	using Split = DwtSplit<kThreads>;
 	__shared__ DwtShared sh;
 	pdl_trigger();
 	const int level = p.level;
@@ -327,7 +357,7 @@ __global__ void __launch_bounds__(kDwtThreads, 4) dwt_forward_kernel(const Level
 		res_h = al_h = p.P.height;
 	}
 
-	for (int k = threadIdx.x; k < 2 * kTileIn; k += kDwtThreads)
+	for (int k = threadIdx.x; k < 2 * kTileIn; k += kThreads)
 	{
 		if (k < kTileIn)
 			sh.xidx[k] = fwd_index(tx * 64 - 4 + k, res_w, al_w);
@@ -335,7 +365,7 @@ __global__ void __launch_bounds__(kDwtThreads, 4) dwt_forward_kernel(const Level
 			sh.yidx[k - kTileIn] = fwd_index(ty * 64 - 4 + (k - kTileIn), res_h, al_h);
 	}
 	if (from_plane)
-		for (int u = threadIdx.x; u < 256; u += kDwtThreads)
+		for (int u = threadIdx.x; u < 256; u += kThreads)
 			sh.unorm[u] = unorm8_centered(uint32_t(u));
 	__syncthreads();
 	pdl_wait();
@@ -348,7 +378,7 @@ __global__ void __launch_bounds__(kDwtThreads, 4) dwt_forward_kernel(const Level
 	const bool interior = x0 >= 0 && y0 >= 0 && x0 + kTileIn <= res_w && y0 + kTileIn <= res_h;
 	constexpr int kVecPerRow = kTileIn / 4;     // 18 vectors of 4 samples
 	constexpr int kVecs = kVecPerRow * kTileIn; // 1296
-	constexpr int kVecIters = (kVecs + kDwtThreads - 1) / kDwtThreads;
+	constexpr int kVecIters = (kVecs + kThreads - 1) / kThreads;
 	if (from_plane)
 	{
 		const uint8_t *src = comp == 0 ? in.data[0] : (comp == 1 ? in.data[1] : in.data[2]);
@@ -361,14 +391,14 @@ __global__ void __launch_bounds__(kDwtThreads, 4) dwt_forward_kernel(const Level
 #pragma unroll
 			for (int u = 0; u < kVecIters; u++)
 			{
-				const int k = threadIdx.x + u * kDwtThreads;
+				const int k = threadIdx.x + u * kThreads;
 				const int i = k / kVecPerRow, j = k - i * kVecPerRow;
 				v[u] = k < kVecs ? __ldg(reinterpret_cast<const uint32_t *>(src + size_t(y0 + i) * pitch + x0) + j) : 0u;
 			}
 #pragma unroll
 			for (int u = 0; u < kVecIters; u++)
 			{
-				const int k = threadIdx.x + u * kDwtThreads;
+				const int k = threadIdx.x + u * kThreads;
 				if (k < kVecs)
 				{
 					const int i = k / kVecPerRow, j = k - i * kVecPerRow;
@@ -380,20 +410,20 @@ __global__ void __launch_bounds__(kDwtThreads, 4) dwt_forward_kernel(const Level
 		}
 		else
 		{
-			for (int base = threadIdx.x; base < kTileIn * kTileIn; base += kDwtThreads * kDwtGen)
+			for (int base = threadIdx.x; base < kTileIn * kTileIn; base += kThreads * Split::kGen)
 			{
-				uint32_t v[kDwtGen];
+				uint32_t v[Split::kGen];
 #pragma unroll
-				for (int u = 0; u < kDwtGen; u++)
+				for (int u = 0; u < Split::kGen; u++)
 				{
-					const int k = base + u * kDwtThreads;
+					const int k = base + u * kThreads;
 					const int i = k / kTileIn, j = k - i * kTileIn;
 					v[u] = k < kTileIn * kTileIn ? src[size_t(sh.yidx[i]) * pitch + size_t(sh.xidx[j]) * xs] : 0u;
 				}
 #pragma unroll
-				for (int u = 0; u < kDwtGen; u++)
+				for (int u = 0; u < Split::kGen; u++)
 				{
-					const int k = base + u * kDwtThreads;
+					const int k = base + u * kThreads;
 					if (k < kTileIn * kTileIn)
 					{
 						const int i = k / kTileIn, j = k - i * kTileIn;
@@ -414,7 +444,7 @@ __global__ void __launch_bounds__(kDwtThreads, 4) dwt_forward_kernel(const Level
 #pragma unroll
 			for (int u = 0; u < kVecIters; u++)
 			{
-				const int k = threadIdx.x + u * kDwtThreads;
+				const int k = threadIdx.x + u * kThreads;
 				const int i = k / kVecPerRow, j = k - i * kVecPerRow;
 				const int64_t idx = ll + int64_t(y0 + i) * P.pitch + x0 + 4 * j;
 				if (k >= kVecs)
@@ -432,7 +462,7 @@ __global__ void __launch_bounds__(kDwtThreads, 4) dwt_forward_kernel(const Level
 #pragma unroll
 			for (int u = 0; u < kVecIters; u++)
 			{
-				const int k = threadIdx.x + u * kDwtThreads;
+				const int k = threadIdx.x + u * kThreads;
 				if (k < kVecs)
 				{
 					const int i = k / kVecPerRow, j = k - i * kVecPerRow;
@@ -445,22 +475,22 @@ __global__ void __launch_bounds__(kDwtThreads, 4) dwt_forward_kernel(const Level
 		}
 		else
 		{
-			for (int base = threadIdx.x; base < kTileIn * kTileIn; base += kDwtThreads * kDwtGen)
+			for (int base = threadIdx.x; base < kTileIn * kTileIn; base += kThreads * Split::kGen)
 			{
-				float v[kDwtGen];
+				float v[Split::kGen];
 #pragma unroll
-				for (int u = 0; u < kDwtGen; u++)
+				for (int u = 0; u < Split::kGen; u++)
 				{
-					const int k = base + u * kDwtThreads;
+					const int k = base + u * kThreads;
 					const int i = k / kTileIn, j = k - i * kTileIn;
 					v[u] = k < kTileIn * kTileIn
 					           ? load_coef(buf.coef32, buf.coef16, f16, ll + int64_t(sh.yidx[i]) * P.pitch + sh.xidx[j])
 					           : 0.0f;
 				}
 #pragma unroll
-				for (int u = 0; u < kDwtGen; u++)
+				for (int u = 0; u < Split::kGen; u++)
 				{
-					const int k = base + u * kDwtThreads;
+					const int k = base + u * kThreads;
 					if (k < kTileIn * kTileIn)
 					{
 						const int i = k / kTileIn, j = k - i * kTileIn;
@@ -472,41 +502,43 @@ __global__ void __launch_bounds__(kDwtThreads, 4) dwt_forward_kernel(const Level
 	}
 	__syncthreads();
 
-	// Horizontal lifting: 72 rows x 4 segments of 8 output pairs.
-	for (int item = threadIdx.x; item < kTileIn * 4; item += kDwtThreads)
+	// Horizontal lifting: 72 rows x kSegs segments of kSegPairs output pairs.
+	constexpr int kSegPairs = Split::kSegPairs, kWin = Split::kWin;
+	for (int item = threadIdx.x; item < kTileIn * Split::kSegs; item += kThreads)
 	{
 		const int row = item % kTileIn, seg = item / kTileIn;
-		float e[24];
+		float e[kWin];
 #pragma unroll
-		for (int j = 0; j < 24; j++)
-			e[j] = sh.in[row][seg * 16 + j];
+		for (int j = 0; j < kWin; j++)
+			e[j] = sh.in[row][seg * 2 * kSegPairs + j];
 		lift_forward(e);
 #pragma unroll
-		for (int k = 0; k < 8; k++)
+		for (int k = 0; k < kSegPairs; k++)
 		{
-			sh.h[row][seg * 8 + k] = __fmul_rn(e[4 + 2 * k], kInvK);
-			sh.h[row][32 + seg * 8 + k] = __fmul_rn(e[5 + 2 * k], kK);
+			sh.h[row][seg * kSegPairs + k] = __fmul_rn(e[4 + 2 * k], kInvK);
+			sh.h[row][32 + seg * kSegPairs + k] = __fmul_rn(e[5 + 2 * k], kK);
 		}
 	}
 	__syncthreads();
 
-	// Vertical lifting: 64 columns x 4 segments. Columns 0..31 hold the
+	// Vertical lifting: 64 columns x kSegs segments. Columns 0..31 hold the
 	// horizontal low band (-> LL, LH), 32..63 the high band (-> HL, HH).
 	float(*bands)[32][kBandPitch] = reinterpret_cast<float(*)[32][kBandPitch]>(&sh.in[0][0]);
+	for (int item = threadIdx.x; item < 64 * Split::kSegs; item += kThreads)
 	{
-		const int col = threadIdx.x & 63, seg = threadIdx.x >> 6;
-		float e[24];
+		const int col = item & 63, seg = item >> 6;
+		float e[kWin];
 #pragma unroll
-		for (int j = 0; j < 24; j++)
-			e[j] = sh.h[seg * 16 + j][col];
+		for (int j = 0; j < kWin; j++)
+			e[j] = sh.h[seg * 2 * kSegPairs + j][col];
 		lift_forward(e);
 		const int c = col & 31;
 		const int b_low = col < 32 ? 0 : 1, b_high = col < 32 ? 2 : 3;
 		const int gx = tx * 32 + c;
 #pragma unroll
-		for (int k = 0; k < 8; k++)
+		for (int k = 0; k < kSegPairs; k++)
 		{
-			const int r = seg * 8 + k;
+			const int r = seg * kSegPairs + k;
 			const int gy = ty * 32 + r;
 			float lo = __fmul_rn(e[4 + 2 * k], kInvK);
 			float hi = __fmul_rn(e[5 + 2 * k], kK);
@@ -523,58 +555,57 @@ __global__ void __launch_bounds__(kDwtThreads, 4) dwt_forward_kernel(const Level
 	}
 	__syncthreads();
 
-	// Store all four bands (LL feeds the next level).
+	// Store all four bands (LL feeds the next level): 4 x 32 rows x 8 vectors.
+	for (int item = threadIdx.x; item < 4 * 256; item += kThreads)
 	{
-		const int r = threadIdx.x >> 3, c4 = (threadIdx.x & 7) * 4;
-#pragma unroll
-		for (int b = 0; b < 4; b++)
+		const int b = item >> 8, r = (item >> 3) & 31, c4 = (item & 7) * 4;
+		const int64_t idx = p.band[comp][b].offset + int64_t(ty * 32 + r) * L.pitch + tx * 32 + c4;
+		if (L.fp16)
 		{
-			const int64_t idx = p.band[comp][b].offset + int64_t(ty * 32 + r) * L.pitch + tx * 32 + c4;
-			if (L.fp16)
-			{
-				__half2 h0 = __floats2half2_rn(bands[b][r][c4 + 0], bands[b][r][c4 + 1]);
-				__half2 h1 = __floats2half2_rn(bands[b][r][c4 + 2], bands[b][r][c4 + 3]);
-				uint2 u;
-				u.x = *reinterpret_cast<uint32_t *>(&h0);
-				u.y = *reinterpret_cast<uint32_t *>(&h1);
-				*reinterpret_cast<uint2 *>(buf.coef16 + idx) = u;
-			}
-			else
-			{
-				float4 f = make_float4(bands[b][r][c4 + 0], bands[b][r][c4 + 1], bands[b][r][c4 + 2], bands[b][r][c4 + 3]);
-				*reinterpret_cast<float4 *>(buf.coef32 + idx) = f;
-			}
+			__half2 h0 = __floats2half2_rn(bands[b][r][c4 + 0], bands[b][r][c4 + 1]);
+			__half2 h1 = __floats2half2_rn(bands[b][r][c4 + 2], bands[b][r][c4 + 3]);
+			uint2 u;
+			u.x = *reinterpret_cast<uint32_t *>(&h0);
+			u.y = *reinterpret_cast<uint32_t *>(&h1);
+			*reinterpret_cast<uint2 *>(buf.coef16 + idx) = u;
+		}
+		else
+		{
+			float4 f = make_float4(bands[b][r][c4 + 0], bands[b][r][c4 + 1], bands[b][r][c4 + 2], bands[b][r][c4 + 3]);
+			*reinterpret_cast<float4 *>(buf.coef32 + idx) = f;
 		}
 	}
 
 	if (!fused)
 		return;
 
-	// Quantise the transmitted bands of this tile: HL, LH, HH (+ LL at the last level).
+	// Quantise the transmitted bands of this tile: HL, LH, HH (+ LL at the last
+	// level), kGroups bands per round.
 	const int first_band = level == kLevels - 1 ? 0 : 1;
 	const int nb = 4 - first_band;
-	const int grp = threadIdx.x >> 7, t = threadIdx.x & 127;
-	for (int round = 0; round < 2; round++)
+	const int grp = threadIdx.x / Split::kGroupThreads, t = threadIdx.x % Split::kGroupThreads;
+	for (int round = 0; round * Split::kGroups < nb; round++)
 	{
-		const int bi = round * 2 + grp;
+		const int bi = round * Split::kGroups + grp;
 		const bool active = bi < nb;
 		const int band = active ? first_band + bi : first_band;
-		quant_analyze_block(&bands[band][0][0], kBandPitch, active, t, sh.q[grp], L, p.band[comp][band],
-		                    p.subdivision_shift, tx, ty, buf);
+		quant_analyze_block<Split::kQSplit>(&bands[band][0][0], kBandPitch, active, t, sh.q[grp], L,
+		                                    p.band[comp][band], p.subdivision_shift, tx, ty, buf);
 	}
 }
 
 // Quantiser over a pyramid already in storage (the reference's
 // Encoder::encode_pre_transformed, pyrowave_encoder.cpp:1138-1151).
 // Two 32x32 blocks per CTA.
-__global__ void __launch_bounds__(256) quant_pretransformed_kernel(const BlockParams p, const EncodeBuffers buf)
+__global__ void __launch_bounds__(256) quant_pretransformed_kernel(const BlockParams p, const EncodeBuffers buf,
+                                                                   const int nblocks)
 {
 	__shared__ float tile[2][32][kBandPitch];
 	__shared__ QuantGroupShared q[2];
 	pdl_trigger();
 	const int grp = threadIdx.x >> 7, t = threadIdx.x & 127;
 	const int b = blockIdx.x * 2 + grp;
-	const bool active = b < p.block_count_32x32;
+	const bool active = b < nblocks;
 	const int k = active ? find_band(p, b) : 0;
 	const BandEntry &E = p.band[k];
 	const LevelDesc &L = p.level[E.level];
@@ -600,7 +631,7 @@ __global__ void __launch_bounds__(256) quant_pretransformed_kernel(const BlockPa
 	B.quant_resolution = E.quant_resolution;
 	B.rdo_scale = E.rdo_scale;
 	B.quant_code = E.quant_code;
-	quant_analyze_block(&tile[grp][0][0], kBandPitch, active, t, q[grp], L, B, p.subdivision_shift, bx, by, buf);
+	quant_analyze_block<1>(&tile[grp][0][0], kBandPitch, active, t, q[grp], L, B, p.subdivision_shift, bx, by, buf);
 }
 
 // ---------------------------------------------------------------------------
@@ -1087,14 +1118,24 @@ void launch_dwt_forward_level(const LevelParams &p, const PlaneInput &in, const 
                               bool programmatic, cudaStream_t stream)
 {
 	const dim3 grid(p.L.tiles_x * p.L.tiles_y, (p.level == 0 && !p.chroma444) ? 1 : 3);
-	LaunchConfig lc(grid, dim3(kDwtThreads), stream, programmatic);
-	cudaLaunchKernelEx(&lc.cfg, dwt_forward_kernel, p, in, buf, fused_quant ? 1 : 0);
+	const int f = fused_quant ? 1 : 0;
+	if (int(grid.x * grid.y) < kSmallLevelTiles)
+	{
+		LaunchConfig lc(grid, dim3(1024), stream, programmatic);
+		cudaLaunchKernelEx(&lc.cfg, dwt_forward_kernel<1024>, p, in, buf, f);
+	}
+	else
+	{
+		LaunchConfig lc(grid, dim3(256), stream, programmatic);
+		cudaLaunchKernelEx(&lc.cfg, dwt_forward_kernel<256>, p, in, buf, f);
+	}
 }
 
-void launch_quant_pretransformed(const BlockParams &p, const EncodeBuffers &buf, cudaStream_t stream)
+void launch_quant_pretransformed(const BlockParams &p, const EncodeBuffers &buf, int nblocks, bool programmatic,
+                                 cudaStream_t stream)
 {
-	LaunchConfig lc(dim3((p.block_count_32x32 + 1) / 2), dim3(256), stream, true);
-	cudaLaunchKernelEx(&lc.cfg, quant_pretransformed_kernel, p, buf);
+	LaunchConfig lc(dim3((nblocks + 1) / 2), dim3(256), stream, programmatic);
+	cudaLaunchKernelEx(&lc.cfg, quant_pretransformed_kernel, p, buf, nblocks);
 }
 
 void launch_resolve(const ResolveParams &p, const EncodeBuffers &buf, cudaStream_t stream)
@@ -1110,6 +1151,4 @@ void launch_pack(const BlockParams &p, const EncodeBuffers &buf, cudaStream_t st
 	cudaLaunchKernelEx(&lc.cfg, pack_kernel, p, buf);
 }
 
-const void *kernel_dwt_forward() { return reinterpret_cast<const void *>(&dwt_forward_kernel); }
-const void *kernel_resolve() { return reinterpret_cast<const void *>(&resolve_kernel); }
 } // namespace pw

@@ -583,6 +583,8 @@ struct pyrowave_encoder_opaque
 	StageEvents timing;
 	CapturedGraph graph;
 	KernelNode node_dwt[kLevels];
+	int small_level = kLevels; // levels >= this are quantised by one launch after the transform
+	int small_blocks = 0;      // 32x32 blocks of those levels (a prefix in block index order)
 	KernelNode node_resolve;
 
 	EncodeBuffers buffers() const
@@ -657,6 +659,20 @@ struct pyrowave_encoder_opaque
 		for (int level = 0; level < kLevels; level++)
 			lp[level] = make_level_params(g, level);
 		bp = make_block_params(g);
+		// The small levels are the coarsest ones; their blocks come first in
+		// block index order (level 4 -> 0), so one launch over a prefix of the
+		// blocks quantises all of them.
+		small_level = kLevels;
+		for (int level = kLevels - 1; level >= 0; level--)
+		{
+			const int tiles = g.level[level].tiles_x * g.level[level].tiles_y * ((level == 0 && !g.chroma444) ? 1 : 3);
+			if (tiles >= kSmallLevelTiles)
+				break;
+			small_level = level;
+		}
+		small_blocks = small_level == kLevels ? 0
+		               : small_level == 0     ? g.block_count_32x32
+		                                      : g.band[0][small_level - 1][1].block32_offset;
 		bool ok = true;
 		coef32 = dev_alloc<float>(size_t(g.storage_elems32), ok);
 		coef16 = dev_alloc<__half>(size_t(g.storage_elems16), ok);
@@ -761,9 +777,14 @@ struct pyrowave_encoder_opaque
 			const bool pdl = !device->stage_timing; // event nodes between kernels break programmatic edges
 			for (int level = 0; level < kLevels; level++)
 			{
-				launch_dwt_forward_level(lp[level], in, b, true, pdl && level > 0, s);
+				launch_dwt_forward_level(lp[level], in, b, level < small_level, pdl && level > 0, s);
 				ok = ok && last_captured_node(s, node_dwt[level]);
 				timing.mark(device, s, dwt_tags[level]);
+			}
+			if (small_blocks > 0)
+			{
+				launch_quant_pretransformed(bp, b, small_blocks, pdl, s);
+				timing.mark(device, s, "quant");
 			}
 			launch_resolve(make_resolve_params(g, target_words, sequence_count), b, s);
 			ok = ok && last_captured_node(s, node_resolve);
@@ -781,11 +802,13 @@ struct pyrowave_encoder_opaque
 		else
 		{
 			PlaneInput pin = in;
-			int fused = 1;
 			ResolveParams rp = make_resolve_params(g, target_words, sequence_count);
 			bool ok = true;
 			for (int level = 0; level < kLevels; level++)
+			{
+				int fused = level < small_level ? 1 : 0;
 				ok = ok && set_kernel_args(graph.exec, node_dwt[level], lp[level], pin, b, fused);
+			}
 			ok = ok && set_kernel_args(graph.exec, node_resolve, rp, b);
 			if (!ok)
 			{
@@ -1765,7 +1788,7 @@ pyrowave_result pyrowave_cuda_encoder_encode_pre_transformed(pyrowave_encoder en
 	const BlockParams bp = make_block_params(g);
 	cudaMemsetAsync(encoder->rc, 0, sizeof(RateControlState), s);
 	launch_pyramid_io(bp, const_cast<float *>(pyramid), encoder->coef32, encoder->coef16, false, s);
-	launch_quant_pretransformed(bp, b, s);
+	launch_quant_pretransformed(bp, b, bp.block_count_32x32, true, s);
 	launch_resolve(make_resolve_params(g, target_words, encoder->sequence_count), b, s);
 	launch_pack(bp, b, s);
 	if (!launches_ok("kernel launch"))

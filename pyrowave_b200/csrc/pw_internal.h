@@ -226,9 +226,16 @@ ResolveParams make_resolve_params(const Geometry &g, uint32_t target_words, uint
 // the first of a sequence may start early (programmatic dependent launch):
 // kernels wait for their predecessor with griddepcontrol before touching
 // global memory.
+// Levels with fewer tiles than this (all components) are "small": their
+// transforms run 1024-thread CTAs, and the encoder quantises their bands in one
+// launch across the whole GPU after the last level instead of inside the
+// transform of each level.
+constexpr int kSmallLevelTiles = 256;
 void launch_dwt_forward_level(const LevelParams &p, const PlaneInput &in, const EncodeBuffers &buf, bool fused_quant,
                               bool programmatic, cudaStream_t stream);
-void launch_quant_pretransformed(const BlockParams &p, const EncodeBuffers &buf, cudaStream_t stream);
+// Quantise and analyse the first nblocks 32x32 blocks (block index order) from storage.
+void launch_quant_pretransformed(const BlockParams &p, const EncodeBuffers &buf, int nblocks, bool programmatic,
+                                 cudaStream_t stream);
 void launch_resolve(const ResolveParams &p, const EncodeBuffers &buf, cudaStream_t stream);
 void launch_pack(const BlockParams &p, const EncodeBuffers &buf, cudaStream_t stream);
 void launch_dequant(const BlockParams &p, const DecodeInput &in, bool programmatic, cudaStream_t stream);
@@ -237,9 +244,4 @@ void launch_idwt_level(const LevelParams &p, const DecodeInput &in, const PlaneO
 void launch_pyramid_io(const BlockParams &p, float *canonical, float *coef32, __half *coef16, bool to_canonical,
                        cudaStream_t stream);
 
-// Kernel entry points, for patching captured graph nodes.
-const void *kernel_dwt_forward();
-const void *kernel_resolve();
-const void *kernel_dequant();
-const void *kernel_idwt();
 } // namespace pw
