@@ -75,14 +75,14 @@ __device__ __forceinline__ void store_coef(float *c32, __half *c16, bool fp16, i
 
 // One 32x32 block per 128-thread CTA; thread = one 4x2 sub-block (the
 // reference's mapping, wavelet_dequant.comp:222-238).
-__global__ void __launch_bounds__(128) dequant_kernel(const BlockParams p, const DecodeInput in)
+__global__ void __launch_bounds__(128) dequant_kernel(const BlockParams p, const DecodeInput in, const int first)
 {
 	__shared__ uint32_t s_words[kMaxBlockWords];
 	__shared__ uint32_t s_plane_off[16];
 	__shared__ uint32_t s_sign_base;
 	__shared__ uint32_t s_sig[4];
 	pdl_trigger();
-	const int blk = blockIdx.x;
+	const int blk = first + int(blockIdx.x);
 	const int k = find_band(p, blk);
 	const BandEntry &B = p.band[k];
 	const LevelDesc &L = p.level[B.level];
@@ -534,10 +534,11 @@ __global__ void pyramid_io_kernel(const BlockParams p, float *canonical, float *
 }
 } // namespace
 
-void launch_dequant(const BlockParams &p, const DecodeInput &in, bool programmatic, cudaStream_t stream)
+void launch_dequant(const BlockParams &p, const DecodeInput &in, int first, int count, bool programmatic,
+                    cudaStream_t stream)
 {
-	LaunchConfig lc(dim3(p.block_count_32x32), dim3(128), stream, programmatic);
-	cudaLaunchKernelEx(&lc.cfg, dequant_kernel, p, in);
+	LaunchConfig lc(dim3(count), dim3(128), stream, programmatic);
+	cudaLaunchKernelEx(&lc.cfg, dequant_kernel, p, in, first);
 }
 
 void launch_idwt_level(const LevelParams &p, const DecodeInput &in, const PlaneOutput &out, bool programmatic,
@@ -650,7 +651,7 @@ extern "C" pyrowave_result pyrowave_cuda_decode_blocks_static(int width, int hei
 	in.coef32 = scratch;
 	in.coef16 = nullptr; // every level is FP32 here
 	const cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
-	launch_dequant(make_block_params(g), in, false, s);
+	launch_dequant(make_block_params(g), in, 0, g.block_count_32x32, false, s);
 	for (int level = kLevels - 1; level >= 0; level--)
 		launch_idwt_level(make_level_params(g, level), in, out, true, s);
 	return cudaGetLastError() == cudaSuccess ? PYROWAVE_SUCCESS : PYROWAVE_ERROR_GENERIC;

@@ -595,15 +595,17 @@ __global__ void __launch_bounds__(kThreads, kThreads >= 1024 ? 1 : 4)
 }
 
 // Quantiser over a pyramid already in storage (the reference's
-// Encoder::encode_pre_transformed, pyrowave_encoder.cpp:1138-1151).
-// Two 32x32 blocks per CTA.
-__global__ void __launch_bounds__(256) quant_pretransformed_kernel(const BlockParams p, const EncodeBuffers buf,
-                                                                   const int nblocks)
+// Encoder::encode_pre_transformed, pyrowave_encoder.cpp:1138-1151, and the
+// small levels of a frame). Two 32x32 blocks per CTA, 128 * S threads each.
+template <int S>
+__global__ void __launch_bounds__(256 * S) quant_pretransformed_kernel(const BlockParams p, const EncodeBuffers buf,
+                                                                       const int nblocks)
 {
+	constexpr int kGroupThreads = 128 * S;
 	__shared__ float tile[2][32][kBandPitch];
 	__shared__ QuantGroupShared q[2];
 	pdl_trigger();
-	const int grp = threadIdx.x >> 7, t = threadIdx.x & 127;
+	const int grp = threadIdx.x / kGroupThreads, t = threadIdx.x % kGroupThreads;
 	const int b = blockIdx.x * 2 + grp;
 	const bool active = b < nblocks;
 	const int k = active ? find_band(p, b) : 0;
@@ -614,11 +616,25 @@ __global__ void __launch_bounds__(256) quant_pretransformed_kernel(const BlockPa
 	pdl_wait();
 	if (active)
 	{
-		for (int i = t; i < 1024; i += 128)
+		// The block's 32 rows as 8 vectors of 4 each, every load in flight at once.
+		for (int i = t; i < 256; i += kGroupThreads)
 		{
-			const int r = i >> 5, c = i & 31;
-			const int64_t idx = E.offset + int64_t(by * 32 + r) * L.pitch + bx * 32 + c;
-			tile[grp][r][c] = load_coef(buf.coef32, buf.coef16, L.fp16 != 0, idx);
+			const int r = i >> 3, c4 = (i & 7) * 4;
+			const int64_t idx = E.offset + int64_t(by * 32 + r) * L.pitch + bx * 32 + c4;
+			float4 f;
+			if (L.fp16)
+			{
+				const uint2 hv = __ldcg(reinterpret_cast<const uint2 *>(buf.coef16 + idx));
+				const float2 a = __half22float2(*reinterpret_cast<const __half2 *>(&hv.x));
+				const float2 c = __half22float2(*reinterpret_cast<const __half2 *>(&hv.y));
+				f = make_float4(a.x, a.y, c.x, c.y);
+			}
+			else
+				f = __ldcg(reinterpret_cast<const float4 *>(buf.coef32 + idx));
+			tile[grp][r][c4 + 0] = f.x;
+			tile[grp][r][c4 + 1] = f.y;
+			tile[grp][r][c4 + 2] = f.z;
+			tile[grp][r][c4 + 3] = f.w;
 		}
 	}
 	__syncthreads();
@@ -631,7 +647,7 @@ __global__ void __launch_bounds__(256) quant_pretransformed_kernel(const BlockPa
 	B.quant_resolution = E.quant_resolution;
 	B.rdo_scale = E.rdo_scale;
 	B.quant_code = E.quant_code;
-	quant_analyze_block<1>(&tile[grp][0][0], kBandPitch, active, t, q[grp], L, B, p.subdivision_shift, bx, by, buf);
+	quant_analyze_block<S>(&tile[grp][0][0], kBandPitch, active, t, q[grp], L, B, p.subdivision_shift, bx, by, buf);
 }
 
 // ---------------------------------------------------------------------------
@@ -931,7 +947,7 @@ __global__ void __launch_bounds__(1024) resolve_kernel(const ResolveParams p, co
 // ---------------------------------------------------------------------------
 // Block packing: one 32x32 block per 128-thread CTA, assembled in shared
 // memory and written as whole words at its prefix-scanned offset.
-__global__ void __launch_bounds__(128) pack_kernel(const BlockParams p, const EncodeBuffers buf)
+__global__ void __launch_bounds__(128, 12) pack_kernel(const BlockParams p, const EncodeBuffers buf)
 {
 	__shared__ uint32_t pkt[kMaxBlockWords];
 	__shared__ uint32_t s_ballot[4];
@@ -1134,8 +1150,8 @@ void launch_dwt_forward_level(const LevelParams &p, const PlaneInput &in, const 
 void launch_quant_pretransformed(const BlockParams &p, const EncodeBuffers &buf, int nblocks, bool programmatic,
                                  cudaStream_t stream)
 {
-	LaunchConfig lc(dim3((nblocks + 1) / 2), dim3(256), stream, programmatic);
-	cudaLaunchKernelEx(&lc.cfg, quant_pretransformed_kernel, p, buf, nblocks);
+	LaunchConfig lc(dim3((nblocks + 1) / 2), dim3(512), stream, programmatic);
+	cudaLaunchKernelEx(&lc.cfg, quant_pretransformed_kernel<2>, p, buf, nblocks);
 }
 
 void launch_resolve(const ResolveParams &p, const EncodeBuffers &buf, cudaStream_t stream)

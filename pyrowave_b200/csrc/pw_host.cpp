@@ -223,6 +223,24 @@ bool build_geometry(Geometry &g, std::vector<uint32_t> &jobs, int width, int hei
 	return true;
 }
 
+// The small levels (fewer than kSmallLevelTiles tiles) are the coarsest ones;
+// their blocks come first in block index order (level 4 -> 0), so they are
+// the prefix [0, blocks) of the blocks.
+void small_level_split(const Geometry &g, int &level_out, int &blocks)
+{
+	level_out = kLevels;
+	for (int level = kLevels - 1; level >= 0; level--)
+	{
+		const int tiles = g.level[level].tiles_x * g.level[level].tiles_y * ((level == 0 && !g.chroma444) ? 1 : 3);
+		if (tiles >= kSmallLevelTiles)
+			break;
+		level_out = level;
+	}
+	blocks = level_out == kLevels ? 0
+	         : level_out == 0     ? g.block_count_32x32
+	                              : g.band[0][level_out - 1][1].block32_offset;
+}
+
 // Per-band resolution override of encode_pre_transformed (pyrowave_encoder.cpp:449,251).
 void apply_quant_scale_override(Geometry &g, float quant_scale)
 {
@@ -536,7 +554,7 @@ struct CapturedGraph
 			graph = nullptr;
 			return false;
 		}
-		if (!cuda_ok(cudaGraphInstantiate(&exec, graph, 0), "cudaGraphInstantiate"))
+		if (!cuda_ok(cudaGraphInstantiate(&exec, graph, cudaGraphInstantiateFlagUseNodePriority), "cudaGraphInstantiate"))
 		{
 			exec = nullptr;
 			return false;
@@ -659,20 +677,7 @@ struct pyrowave_encoder_opaque
 		for (int level = 0; level < kLevels; level++)
 			lp[level] = make_level_params(g, level);
 		bp = make_block_params(g);
-		// The small levels are the coarsest ones; their blocks come first in
-		// block index order (level 4 -> 0), so one launch over a prefix of the
-		// blocks quantises all of them.
-		small_level = kLevels;
-		for (int level = kLevels - 1; level >= 0; level--)
-		{
-			const int tiles = g.level[level].tiles_x * g.level[level].tiles_y * ((level == 0 && !g.chroma444) ? 1 : 3);
-			if (tiles >= kSmallLevelTiles)
-				break;
-			small_level = level;
-		}
-		small_blocks = small_level == kLevels ? 0
-		               : small_level == 0     ? g.block_count_32x32
-		                                      : g.band[0][small_level - 1][1].block32_offset;
+		small_level_split(g, small_level, small_blocks);
 		bool ok = true;
 		coef32 = dev_alloc<float>(size_t(g.storage_elems32), ok);
 		coef16 = dev_alloc<__half>(size_t(g.storage_elems16), ok);
@@ -1094,7 +1099,7 @@ struct pyrowave_decoder_opaque
 			const bool pdl = !device->stage_timing; // event nodes between kernels break programmatic edges
 			if (dequant)
 			{
-				launch_dequant(bp, in, false, s);
+				launch_dequant(bp, in, 0, g.block_count_32x32, false, s);
 				ok = ok && last_captured_node(s, node_dequant);
 				timing.mark(device, s, "dequant");
 			}
@@ -1119,7 +1124,10 @@ struct pyrowave_decoder_opaque
 			PlaneOutput pout = out;
 			bool ok = true;
 			if (dequant)
-				ok = set_kernel_args(graph.exec, node_dequant, bp, din);
+			{
+				int first = 0;
+				ok = set_kernel_args(graph.exec, node_dequant, bp, din, first);
+			}
 			for (int level = 0; level < kLevels; level++)
 				ok = ok && set_kernel_args(graph.exec, dequant ? node_idwt_full[level] : node_idwt_only[level], lp[level],
 				                           din, pout);
@@ -1229,7 +1237,11 @@ pyrowave_result pyrowave_create_default_device(pyrowave_device *device)
 	if (!dev)
 		return PYROWAVE_ERROR_OUT_OF_HOST_MEMORY;
 	cudaGetDevice(&dev->cuda_device);
-	if (cudaStreamCreateWithFlags(&dev->stream, cudaStreamNonBlocking) != cudaSuccess)
+	// The library's own stream runs at the highest priority, so its kernels go
+	// first when other work shares the GPU.
+	int least = 0, greatest = 0;
+	cudaDeviceGetStreamPriorityRange(&least, &greatest);
+	if (cudaStreamCreateWithPriority(&dev->stream, cudaStreamNonBlocking, greatest) != cudaSuccess)
 	{
 		delete dev;
 		return PYROWAVE_ERROR_GENERIC;

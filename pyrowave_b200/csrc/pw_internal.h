@@ -238,7 +238,9 @@ void launch_quant_pretransformed(const BlockParams &p, const EncodeBuffers &buf,
                                  cudaStream_t stream);
 void launch_resolve(const ResolveParams &p, const EncodeBuffers &buf, cudaStream_t stream);
 void launch_pack(const BlockParams &p, const EncodeBuffers &buf, cudaStream_t stream);
-void launch_dequant(const BlockParams &p, const DecodeInput &in, bool programmatic, cudaStream_t stream);
+// Dequantise blocks [first, first + count) (block index order).
+void launch_dequant(const BlockParams &p, const DecodeInput &in, int first, int count, bool programmatic,
+                    cudaStream_t stream);
 void launch_idwt_level(const LevelParams &p, const DecodeInput &in, const PlaneOutput &out, bool programmatic,
                        cudaStream_t stream);
 void launch_pyramid_io(const BlockParams &p, float *canonical, float *coef32, __half *coef16, bool to_canonical,
