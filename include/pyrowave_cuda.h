@@ -174,6 +174,57 @@ PYROWAVE_PUBLIC_API pyrowave_result pyrowave_cuda_decode_blocks_static(int width
                                                                        const pyrowave_cuda_planes *planes,
                                                                        pyrowave_cuda_stream stream);
 
+/* ------------------------------------------------------------------------
+ * Batched form: encode (and optionally decode) many frames of any sizes,
+ * chroma formats and budgets with one CUDA graph launch per call: every stage
+ * runs once over all frames' tiles or blocks. Each frame's bitstream is
+ * identical to what a pyrowave_encoder of the same size produces for the same
+ * input and budget on its n-th call. No counterpart in the reference. */
+typedef struct pyrowave_cuda_batch_opaque *pyrowave_cuda_batch;
+
+typedef struct pyrowave_cuda_batch_frame_info
+{
+	int width, height;
+	pyrowave_chroma_subsampling chroma;
+	size_t maximum_bitstream_size; /* largest per-call budget of this frame, bytes */
+} pyrowave_cuda_batch_frame_info;
+
+/* Create a batch of `count` frame slots (at most 256). Device memory is
+ * allocated here, once. */
+PYROWAVE_PUBLIC_API pyrowave_result pyrowave_cuda_batch_create(pyrowave_device device,
+                                                               const pyrowave_cuda_batch_frame_info *frames,
+                                                               uint32_t count, pyrowave_cuda_batch *batch);
+PYROWAVE_PUBLIC_API void pyrowave_cuda_batch_destroy(pyrowave_cuda_batch batch);
+
+/* Encode frame i from inputs[i] within budgets[i] bytes (<= its maximum) for
+ * every slot; when `outputs` is not NULL, also decode every frame's new
+ * bitstream into outputs[i]. Queued on `stream` (NULL: the device's stream);
+ * the call does not wait. A call may overwrite the previous call's results. */
+PYROWAVE_PUBLIC_API pyrowave_result pyrowave_cuda_batch_encode(pyrowave_cuda_batch batch,
+                                                               const pyrowave_cuda_planes *inputs,
+                                                               const size_t *budgets,
+                                                               const pyrowave_cuda_planes *outputs,
+                                                               pyrowave_cuda_stream stream);
+
+/* Device view of frame i's last bitstream (as pyrowave_cuda_encoder_get_device_bitstream). */
+PYROWAVE_PUBLIC_API pyrowave_result pyrowave_cuda_batch_get_device_bitstream(pyrowave_cuda_batch batch, uint32_t index,
+                                                                             const uint32_t **stream,
+                                                                             const uint32_t **block_meta);
+
+/* Bytes of every frame's last bitstream (waits for the last call). */
+PYROWAVE_PUBLIC_API pyrowave_result pyrowave_cuda_batch_get_sizes(pyrowave_cuda_batch batch, size_t *bytes);
+
+/* Choose the batch's CTA shapes by timing the candidates on these inputs (the
+ * batch's autotuner) and keep the fastest: which coarse levels are transformed
+ * first and quantised together afterwards, and below how many tiles a level
+ * runs 1024-thread CTAs. The bitstreams do not depend on the choice, and the
+ * tuning calls do not advance the frames' sequence numbers. Waits. */
+PYROWAVE_PUBLIC_API pyrowave_result pyrowave_cuda_batch_autotune(pyrowave_cuda_batch batch,
+                                                                 const pyrowave_cuda_planes *inputs,
+                                                                 const size_t *budgets,
+                                                                 const pyrowave_cuda_planes *outputs,
+                                                                 pyrowave_cuda_stream stream);
+
 #ifdef __cplusplus
 }
 #endif

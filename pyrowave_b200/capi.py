@@ -8,6 +8,7 @@ from __future__ import annotations
 
 import ctypes
 import os
+import weakref
 from ctypes import (POINTER, Structure, c_bool, c_float, c_int, c_int32, c_size_t, c_uint8, c_uint16, c_uint32,
                     c_void_p)
 
@@ -53,6 +54,8 @@ API_SYMBOLS = [
     "pyrowave_cuda_encoder_read_wavelet", "pyrowave_cuda_encoder_read_debug", "pyrowave_cuda_decoder_decode",
     "pyrowave_cuda_decoder_decode_blocks", "pyrowave_cuda_decoder_read_wavelet", "pyrowave_cuda_decoder_decode_pyramid",
     "pyrowave_cuda_decode_blocks_static",
+    "pyrowave_cuda_batch_create", "pyrowave_cuda_batch_destroy", "pyrowave_cuda_batch_encode",
+    "pyrowave_cuda_batch_get_device_bitstream", "pyrowave_cuda_batch_get_sizes", "pyrowave_cuda_batch_autotune",
 ]
 
 # Coefficient storage limit of pyrowave_cuda_decode_blocks_static (PYROWAVE_CUDA_STATIC_DECODE_SCRATCH_BYTES).
@@ -100,6 +103,11 @@ class CudaEncoderDebug(Structure):
     _fields_ = [("code_words", c_void_p), ("rd_cost", c_void_p), ("rd_bucket", c_void_p), ("rd_dist", c_void_p),
                 ("histogram", c_void_p), ("consumed", c_void_p), ("quant", c_void_p), ("block_meta", c_void_p),
                 ("error_flags", c_void_p)]
+
+
+class BatchFrameInfo(Structure):
+    _fields_ = [("width", ctypes.c_int), ("height", ctypes.c_int), ("chroma", ctypes.c_int),
+                ("maximum_bitstream_size", c_size_t)]
 
 
 MESSAGE_CB = ctypes.CFUNCTYPE(None, c_void_p, ctypes.c_char_p)
@@ -169,6 +177,15 @@ def lib():
     L.pyrowave_cuda_decoder_decode_pyramid.argtypes = [c_void_p, c_void_p, POINTER(CudaPlanes), c_void_p]
     L.pyrowave_cuda_decode_blocks_static.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_int, c_void_p, c_void_p,
                                                      c_size_t, POINTER(CudaPlanes), c_void_p]
+    L.pyrowave_cuda_batch_create.argtypes = [c_void_p, POINTER(BatchFrameInfo), c_uint32, POINTER(c_void_p)]
+    L.pyrowave_cuda_batch_destroy.argtypes = [c_void_p]
+    L.pyrowave_cuda_batch_destroy.restype = None
+    L.pyrowave_cuda_batch_encode.argtypes = [c_void_p, POINTER(CudaPlanes), POINTER(c_size_t), POINTER(CudaPlanes),
+                                             c_void_p]
+    L.pyrowave_cuda_batch_get_device_bitstream.argtypes = [c_void_p, c_uint32, POINTER(c_void_p), POINTER(c_void_p)]
+    L.pyrowave_cuda_batch_get_sizes.argtypes = [c_void_p, POINTER(c_size_t)]
+    L.pyrowave_cuda_batch_autotune.argtypes = [c_void_p, POINTER(CudaPlanes), POINTER(c_size_t), POINTER(CudaPlanes),
+                                               c_void_p]
     for name in API_SYMBOLS:
         getattr(L, name)  # every declared entry point must resolve
     _lib = L
@@ -199,9 +216,17 @@ class Device:
         h = c_void_p()
         check(self.L.pyrowave_create_default_device(ctypes.byref(h)), "pyrowave_create_default_device")
         self.h = h
+        self._children = weakref.WeakSet()
+
+    def adopt(self, child):
+        """Encoders, decoders and batches made on this device: closed before it."""
+        self._children.add(child)
 
     def close(self):
         if self.h:
+            # The C API requires every object of a device to be destroyed first.
+            for child in list(self._children):
+                child.close()
             self.L.pyrowave_device_destroy(self.h)
             self.h = None
 
@@ -247,6 +272,7 @@ class Encoder:
     def __init__(self, device: Device, width: int, height: int, chroma: int = CHROMA_420, fp16_level_mask: int = 0):
         self.L = lib()
         self.device = device
+        device.adopt(self)
         info = EncoderCreateInfo(device.h, width, height, chroma)
         h = c_void_p()
         check(self.L.pyrowave_encoder_create(ctypes.byref(info), ctypes.byref(h)), "pyrowave_encoder_create")
@@ -346,6 +372,7 @@ class Decoder:
     def __init__(self, device: Device, width: int, height: int, chroma: int = CHROMA_420, fp16_level_mask: int = 0):
         self.L = lib()
         self.device = device
+        device.adopt(self)
         info = DecoderCreateInfo(device.h, width, height, chroma, False)
         h = c_void_p()
         check(self.L.pyrowave_decoder_create(ctypes.byref(info), ctypes.byref(h)), "pyrowave_decoder_create")
@@ -426,3 +453,60 @@ def decode_blocks_static(width: int, height: int, chroma: int, meta_ptr: int, wo
         cp.row_stride_in_bytes[i] = strides[i]
     return lib().pyrowave_cuda_decode_blocks_static(width, height, chroma, c_void_p(meta_ptr), c_void_p(words_ptr),
                                                     num_words, ctypes.byref(cp), c_void_p(stream))
+
+
+def _planes_array(plane_ptr_lists, stride_lists):
+    arr = (CudaPlanes * len(plane_ptr_lists))()
+    for i, (ptrs, strides) in enumerate(zip(plane_ptr_lists, stride_lists)):
+        for p in range(3):
+            arr[i].data[p] = ptrs[p]
+            arr[i].row_stride_in_bytes[p] = strides[p]
+    return arr
+
+
+class Batch:
+    """pyrowave_cuda_batch: many frames of any sizes through one graph launch per call."""
+
+    def __init__(self, device: Device, frames):
+        """frames: list of (width, height, chroma, maximum_bitstream_size)."""
+        self.L = lib()
+        self.device = device
+        device.adopt(self)
+        infos = (BatchFrameInfo * len(frames))(*[BatchFrameInfo(w, h, c, m) for w, h, c, m in frames])
+        h = c_void_p()
+        check(self.L.pyrowave_cuda_batch_create(device.h, infos, len(frames), ctypes.byref(h)), "batch_create")
+        self.h = h
+        self.count = len(frames)
+
+    def close(self):
+        if self.h:
+            self.L.pyrowave_cuda_batch_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        self.close()
+
+    def _args(self, inputs, input_strides, budgets, outputs, output_strides):
+        ins = _planes_array(inputs, input_strides)
+        outs = _planes_array(outputs, output_strides) if outputs is not None else None
+        b = (c_size_t * self.count)(*budgets)
+        return ins, b, outs
+
+    def encode(self, inputs, input_strides, budgets, outputs=None, output_strides=None, stream: int = 0) -> int:
+        ins, b, outs = self._args(inputs, input_strides, budgets, outputs, output_strides)
+        return self.L.pyrowave_cuda_batch_encode(self.h, ins, b, outs, c_void_p(stream))
+
+    def autotune(self, inputs, input_strides, budgets, outputs=None, output_strides=None, stream: int = 0) -> int:
+        ins, b, outs = self._args(inputs, input_strides, budgets, outputs, output_strides)
+        return self.L.pyrowave_cuda_batch_autotune(self.h, ins, b, outs, c_void_p(stream))
+
+    def device_bitstream(self, index: int):
+        s, m = c_void_p(), c_void_p()
+        check(self.L.pyrowave_cuda_batch_get_device_bitstream(self.h, index, ctypes.byref(s), ctypes.byref(m)),
+              "batch_get_device_bitstream")
+        return s.value, m.value
+
+    def sizes(self):
+        out = (c_size_t * self.count)()
+        check(self.L.pyrowave_cuda_batch_get_sizes(self.h, out), "batch_get_sizes")
+        return list(out)

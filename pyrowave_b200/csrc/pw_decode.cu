@@ -75,14 +75,13 @@ __device__ __forceinline__ void store_coef(float *c32, __half *c16, bool fp16, i
 
 // One 32x32 block per 128-thread CTA; thread = one 4x2 sub-block (the
 // reference's mapping, wavelet_dequant.comp:222-238).
-__global__ void __launch_bounds__(128) dequant_kernel(const BlockParams p, const DecodeInput in, const int first)
+__device__ __forceinline__ void dequant_body(const BlockParams &p, const DecodeInput &in, const int blk)
 {
 	__shared__ uint32_t s_words[kMaxBlockWords];
 	__shared__ uint32_t s_plane_off[16];
 	__shared__ uint32_t s_sign_base;
 	__shared__ uint32_t s_sig[4];
 	pdl_trigger();
-	const int blk = first + int(blockIdx.x);
 	const int k = find_band(p, blk);
 	const BandEntry &B = p.band[k];
 	const LevelDesc &L = p.level[B.level];
@@ -244,6 +243,24 @@ __global__ void __launch_bounds__(128) dequant_kernel(const BlockParams p, const
 		store_coef(in.coef32, in.coef16, f16, B.offset + int64_t(oy + (i & 1)) * L.pitch + ox + (i >> 1), v[i]);
 }
 
+__global__ void __launch_bounds__(128) dequant_kernel(const BlockParams p, const DecodeInput in, const int first)
+{
+	dequant_body(p, in, first + int(blockIdx.x));
+}
+
+// Batched form: one CTA per (frame, block), decoding the frame's own bitstream.
+__global__ void __launch_bounds__(128) dequant_batch_kernel(const BatchFrame *frames, const uint32_t *cta_map)
+{
+	__shared__ BlockParams s_p;
+	__shared__ DecodeInput s_in;
+	int f, local;
+	batch_item(cta_map, f, local);
+	load_params(s_p, frames[f].bp);
+	load_params(s_in, frames[f].di);
+	__syncthreads();
+	dequant_body(s_p, s_in, local);
+}
+
 constexpr int kBandTile = 36; // 32 band samples + 2 on each side
 constexpr int kBandTilePitch = 37;
 
@@ -259,7 +276,8 @@ struct IdwtShared
 // than SMs) run 1024-thread CTAs whose lifting items cover half as many
 // outputs, shortening every serial phase.
 template <int kThreads>
-__global__ void __launch_bounds__(kThreads) idwt_kernel(const LevelParams p, const DecodeInput in, const PlaneOutput out)
+__device__ __forceinline__ void idwt_body(const LevelParams &p, const DecodeInput &in, const PlaneOutput &out,
+                                          const int tile, const int comp_index)
 {
 	constexpr int kOut = kThreads >= 1024 ? 8 : 16; // outputs per lifting item
 	constexpr int kSegs = 64 / kOut;
@@ -267,9 +285,8 @@ __global__ void __launch_bounds__(kThreads) idwt_kernel(const LevelParams p, con
 	__shared__ IdwtShared sh;
 	pdl_trigger();
 	const int level = p.level;
-	const int comp = (level == 0 && !p.chroma444) ? 0 : int(blockIdx.y);
+	const int comp = (level == 0 && !p.chroma444) ? 0 : comp_index;
 	const LevelDesc &L = p.L;
-	const int tile = blockIdx.x;
 	const int tx = tile % L.tiles_x, ty = tile / L.tiles_x;
 	const int nx = L.width, ny = L.height;
 	const bool final_level = level == 0 || (level == 1 && comp != 0 && !p.chroma444);
@@ -505,6 +522,30 @@ __global__ void __launch_bounds__(kThreads) idwt_kernel(const LevelParams p, con
 	}
 }
 
+template <int kThreads>
+__global__ void __launch_bounds__(kThreads) idwt_kernel(const LevelParams p, const DecodeInput in, const PlaneOutput out)
+{
+	idwt_body<kThreads>(p, in, out, int(blockIdx.x), int(blockIdx.y));
+}
+
+// Batched form: one CTA per (frame, component, tile) of this level.
+template <int kThreads>
+__global__ void __launch_bounds__(kThreads) idwt_batch_kernel(const BatchFrame *frames, const BatchFrameIO *io,
+                                                              const uint32_t *cta_map, const int level)
+{
+	__shared__ LevelParams s_p;
+	__shared__ DecodeInput s_in;
+	__shared__ PlaneOutput s_out;
+	int f, local;
+	batch_item(cta_map, f, local);
+	load_params(s_p, frames[f].lp[level]);
+	load_params(s_in, frames[f].di);
+	load_params(s_out, io[f].out);
+	__syncthreads();
+	const int ntiles = s_p.L.tiles_x * s_p.L.tiles_y;
+	idwt_body<kThreads>(s_p, s_in, s_out, local % ntiles, local / ntiles);
+}
+
 // Canonical pyramid (all transmitted bands, band-major, unpadded) <-> padded storage.
 __global__ void pyramid_io_kernel(const BlockParams p, float *canonical, float *coef32, __half *coef16,
                                   int to_canonical)
@@ -561,6 +602,28 @@ void launch_pyramid_io(const BlockParams &p, float *canonical, float *coef32, __
                        cudaStream_t stream)
 {
 	pyramid_io_kernel<<<dim3(64, p.nbands), 256, 0, stream>>>(p, canonical, coef32, coef16, to_canonical ? 1 : 0);
+}
+
+void launch_dequant_batch(const BatchFrame *frames, const uint32_t *cta_map, int nctas, bool programmatic,
+                          cudaStream_t stream)
+{
+	LaunchConfig lc(dim3(nctas), dim3(128), stream, programmatic);
+	cudaLaunchKernelEx(&lc.cfg, dequant_batch_kernel, frames, cta_map);
+}
+
+void launch_idwt_batch(const BatchFrame *frames, const BatchFrameIO *io, const uint32_t *cta_map, int nctas, int level,
+                       bool large_ctas, bool programmatic, cudaStream_t stream)
+{
+	if (large_ctas)
+	{
+		LaunchConfig lc(dim3(nctas), dim3(1024), stream, programmatic);
+		cudaLaunchKernelEx(&lc.cfg, idwt_batch_kernel<1024>, frames, io, cta_map, level);
+	}
+	else
+	{
+		LaunchConfig lc(dim3(nctas), dim3(256), stream, programmatic);
+		cudaLaunchKernelEx(&lc.cfg, idwt_batch_kernel<256>, frames, io, cta_map, level);
+	}
 }
 
 } // namespace pw

@@ -122,6 +122,25 @@ __device__ __forceinline__ void st_release_u64(unsigned long long *p, unsigned l
 	asm volatile("st.release.gpu.global.u64 [%0], %1;" ::"l"(p), "l"(v) : "memory");
 }
 
+// Cooperative copy of a parameter struct from global to shared memory (the
+// caller synchronises before use).
+template <typename T> __device__ __forceinline__ void load_params(T &dst, const T &src)
+{
+	static_assert(sizeof(T) % 4 == 0, "parameter structs are word multiples");
+	const uint32_t *s = reinterpret_cast<const uint32_t *>(&src);
+	uint32_t *d = reinterpret_cast<uint32_t *>(&dst);
+	for (int i = int(threadIdx.x); i < int(sizeof(T) / 4); i += int(blockDim.x))
+		d[i] = __ldg(s + i);
+}
+
+// Frame and work item of this CTA in a batched launch (batch_cta() words).
+__device__ __forceinline__ void batch_item(const uint32_t *cta_map, int &frame, int &local)
+{
+	const uint32_t m = __ldg(cta_map + blockIdx.x);
+	frame = int(m >> 24);
+	local = int(m & 0xffffffu);
+}
+
 // Band of a 32x32 block (block index order): the last band whose first block
 // is <= blk, then the block's position in it.
 __device__ __forceinline__ int find_band(const BlockParams &p, int blk)

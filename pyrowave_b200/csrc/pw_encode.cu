@@ -328,18 +328,18 @@ template <int kThreads> struct DwtSplit
 };
 
 // One forward level for one 32x32 band tile of one component (64x64 input
-// samples). grid.x = tile, grid.y = component index among those at this level.
+// samples): `tile` in row-major tile order, `comp_index` the component among
+// those at this level. Run by every thread of a kThreads-thread CTA.
 template <int kThreads>
-__global__ void __launch_bounds__(kThreads, kThreads >= 1024 ? 1 : 4)
-    dwt_forward_kernel(const LevelParams p, const PlaneInput in, const EncodeBuffers buf, const int fused)
+__device__ __forceinline__ void dwt_forward_body(const LevelParams &p, const PlaneInput &in, const EncodeBuffers &buf,
+                                                 const int fused, const int tile, const int comp_index)
 {
 	using Split = DwtSplit<kThreads>;
 	__shared__ DwtShared sh;
 	pdl_trigger();
 	const int level = p.level;
-	const int comp = (level == 0 && !p.chroma444) ? 0 : int(blockIdx.y);
+	const int comp = (level == 0 && !p.chroma444) ? 0 : comp_index;
 	const LevelDesc &L = p.L;
-	const int tile = blockIdx.x;
 	const int tx = tile % L.tiles_x, ty = tile / L.tiles_x;
 	const bool from_plane = level == 0 || (level == 1 && comp != 0 && !p.chroma444);
 
@@ -594,19 +594,45 @@ __global__ void __launch_bounds__(kThreads, kThreads >= 1024 ? 1 : 4)
 	}
 }
 
+template <int kThreads>
+__global__ void __launch_bounds__(kThreads, kThreads >= 1024 ? 1 : 4)
+    dwt_forward_kernel(const LevelParams p, const PlaneInput in, const EncodeBuffers buf, const int fused)
+{
+	dwt_forward_body<kThreads>(p, in, buf, fused, int(blockIdx.x), int(blockIdx.y));
+}
+
+// Batched form: one CTA per (frame, component, tile) of this level.
+template <int kThreads>
+__global__ void __launch_bounds__(kThreads, kThreads >= 1024 ? 1 : 4)
+    dwt_forward_batch_kernel(const BatchFrame *frames, const BatchFrameIO *io, const uint32_t *cta_map, const int level,
+                             const int fused)
+{
+	__shared__ LevelParams s_p;
+	__shared__ PlaneInput s_in;
+	__shared__ EncodeBuffers s_buf;
+	int f, local;
+	batch_item(cta_map, f, local);
+	load_params(s_p, frames[f].lp[level]);
+	load_params(s_in, io[f].in);
+	load_params(s_buf, frames[f].eb);
+	__syncthreads();
+	const int ntiles = s_p.L.tiles_x * s_p.L.tiles_y;
+	dwt_forward_body<kThreads>(s_p, s_in, s_buf, fused, local % ntiles, local / ntiles);
+}
+
 // Quantiser over a pyramid already in storage (the reference's
 // Encoder::encode_pre_transformed, pyrowave_encoder.cpp:1138-1151, and the
 // small levels of a frame). Two 32x32 blocks per CTA, 128 * S threads each.
 template <int S>
-__global__ void __launch_bounds__(256 * S) quant_pretransformed_kernel(const BlockParams p, const EncodeBuffers buf,
-                                                                       const int nblocks)
+__device__ __forceinline__ void quant_blocks_body(const BlockParams &p, const EncodeBuffers &buf, const int nblocks,
+                                                  const int pair)
 {
 	constexpr int kGroupThreads = 128 * S;
 	__shared__ float tile[2][32][kBandPitch];
 	__shared__ QuantGroupShared q[2];
 	pdl_trigger();
 	const int grp = threadIdx.x / kGroupThreads, t = threadIdx.x % kGroupThreads;
-	const int b = blockIdx.x * 2 + grp;
+	const int b = pair * 2 + grp;
 	const bool active = b < nblocks;
 	const int k = active ? find_band(p, b) : 0;
 	const BandEntry &E = p.band[k];
@@ -648,6 +674,27 @@ __global__ void __launch_bounds__(256 * S) quant_pretransformed_kernel(const Blo
 	B.rdo_scale = E.rdo_scale;
 	B.quant_code = E.quant_code;
 	quant_analyze_block<S>(&tile[grp][0][0], kBandPitch, active, t, q[grp], L, B, p.subdivision_shift, bx, by, buf);
+}
+
+template <int S>
+__global__ void __launch_bounds__(256 * S) quant_pretransformed_kernel(const BlockParams p, const EncodeBuffers buf,
+                                                                       const int nblocks)
+{
+	quant_blocks_body<S>(p, buf, nblocks, int(blockIdx.x));
+}
+
+// Batched form: one CTA per pair of blocks among each frame's small-level blocks.
+template <int S>
+__global__ void __launch_bounds__(256 * S) quant_blocks_batch_kernel(const BatchFrame *frames, const uint32_t *cta_map)
+{
+	__shared__ BlockParams s_p;
+	__shared__ EncodeBuffers s_buf;
+	int f, local;
+	batch_item(cta_map, f, local);
+	load_params(s_p, frames[f].bp);
+	load_params(s_buf, frames[f].eb);
+	__syncthreads();
+	quant_blocks_body<S>(s_p, s_buf, frames[f].small_blocks, local);
 }
 
 // ---------------------------------------------------------------------------
@@ -802,7 +849,8 @@ __device__ __forceinline__ void load_rows(const EncodeBuffers &buf, int b0, int 
 			r[i] = load_raw_rd(buf, b0 + i);
 }
 
-__global__ void __launch_bounds__(1024) resolve_kernel(const ResolveParams p, const EncodeBuffers buf)
+__device__ __forceinline__ void resolve_body(const ResolveParams &p, const EncodeBuffers &buf, const int slice,
+                                             const int nslices)
 {
 	__shared__ uint32_t scan[kHistSize];
 	__shared__ uint32_t warp_sums[32];
@@ -813,7 +861,6 @@ __global__ void __launch_bounds__(1024) resolve_kernel(const ResolveParams p, co
 	RateControlState *rc = buf.rc;
 	const int t = threadIdx.x;
 	const int nblocks = p.block_count_32x32;
-	const int slice = blockIdx.x, nslices = gridDim.x;
 	const int per_slice = (nblocks + nslices - 1) / nslices;
 	const int s0 = min(slice * per_slice, nblocks), s1 = min(s0 + per_slice, nblocks);
 	const int per = (s1 - s0 + 1023) / 1024;
@@ -944,17 +991,35 @@ __global__ void __launch_bounds__(1024) resolve_kernel(const ResolveParams p, co
 	}
 }
 
+__global__ void __launch_bounds__(1024) resolve_kernel(const ResolveParams p, const EncodeBuffers buf)
+{
+	resolve_body(p, buf, int(blockIdx.x), int(gridDim.x));
+}
+
+// Batched form: one CTA per (frame, slice).
+__global__ void __launch_bounds__(1024) resolve_batch_kernel(const BatchFrame *frames, const BatchFrameIO *io,
+                                                             const uint32_t *cta_map)
+{
+	__shared__ ResolveParams s_p;
+	__shared__ EncodeBuffers s_buf;
+	int f, local;
+	batch_item(cta_map, f, local);
+	load_params(s_p, io[f].rp);
+	load_params(s_buf, frames[f].eb);
+	__syncthreads();
+	resolve_body(s_p, s_buf, local, frames[f].slices);
+}
+
 // ---------------------------------------------------------------------------
 // Block packing: one 32x32 block per 128-thread CTA, assembled in shared
 // memory and written as whole words at its prefix-scanned offset.
-__global__ void __launch_bounds__(128, 12) pack_kernel(const BlockParams p, const EncodeBuffers buf)
+__device__ __forceinline__ void pack_body(const BlockParams &p, const EncodeBuffers &buf, const int blk)
 {
 	__shared__ uint32_t pkt[kMaxBlockWords];
 	__shared__ uint32_t s_ballot[4];
 	__shared__ uint32_t s_bytes[16];
 	__shared__ uint32_t s_sig[4];
 	pdl_trigger();
-	const int blk = blockIdx.x;
 	const int k = find_band(p, blk);
 	const BandEntry &B = p.band[k];
 	const LevelDesc &L = p.level[B.level];
@@ -1115,6 +1180,24 @@ __global__ void __launch_bounds__(128, 12) pack_kernel(const BlockParams p, cons
 		dst[w] = pkt[w];
 }
 
+__global__ void __launch_bounds__(128, 12) pack_kernel(const BlockParams p, const EncodeBuffers buf)
+{
+	pack_body(p, buf, int(blockIdx.x));
+}
+
+// Batched form: one CTA per (frame, block).
+__global__ void __launch_bounds__(128, 12) pack_batch_kernel(const BatchFrame *frames, const uint32_t *cta_map)
+{
+	__shared__ BlockParams s_p;
+	__shared__ EncodeBuffers s_buf;
+	int f, local;
+	batch_item(cta_map, f, local);
+	load_params(s_p, frames[f].bp);
+	load_params(s_buf, frames[f].eb);
+	__syncthreads();
+	pack_body(s_p, s_buf, local);
+}
+
 } // namespace
 
 LaunchConfig::LaunchConfig(dim3 grid, dim3 block, cudaStream_t stream, bool programmatic)
@@ -1165,6 +1248,42 @@ void launch_pack(const BlockParams &p, const EncodeBuffers &buf, cudaStream_t st
 {
 	LaunchConfig lc(dim3(p.block_count_32x32), dim3(128), stream, true);
 	cudaLaunchKernelEx(&lc.cfg, pack_kernel, p, buf);
+}
+
+void launch_dwt_forward_batch(const BatchFrame *frames, const BatchFrameIO *io, const uint32_t *cta_map, int nctas,
+                              int level, bool fused_quant, bool large_ctas, bool programmatic, cudaStream_t stream)
+{
+	const int f = fused_quant ? 1 : 0;
+	if (large_ctas)
+	{
+		LaunchConfig lc(dim3(nctas), dim3(1024), stream, programmatic);
+		cudaLaunchKernelEx(&lc.cfg, dwt_forward_batch_kernel<1024>, frames, io, cta_map, level, f);
+	}
+	else
+	{
+		LaunchConfig lc(dim3(nctas), dim3(256), stream, programmatic);
+		cudaLaunchKernelEx(&lc.cfg, dwt_forward_batch_kernel<256>, frames, io, cta_map, level, f);
+	}
+}
+
+void launch_quant_blocks_batch(const BatchFrame *frames, const uint32_t *cta_map, int nctas, bool programmatic,
+                               cudaStream_t stream)
+{
+	LaunchConfig lc(dim3(nctas), dim3(512), stream, programmatic);
+	cudaLaunchKernelEx(&lc.cfg, quant_blocks_batch_kernel<2>, frames, cta_map);
+}
+
+void launch_resolve_batch(const BatchFrame *frames, const BatchFrameIO *io, const uint32_t *cta_map, int nctas,
+                          cudaStream_t stream)
+{
+	LaunchConfig lc(dim3(nctas), dim3(1024), stream, true);
+	cudaLaunchKernelEx(&lc.cfg, resolve_batch_kernel, frames, io, cta_map);
+}
+
+void launch_pack_batch(const BatchFrame *frames, const uint32_t *cta_map, int nctas, cudaStream_t stream)
+{
+	LaunchConfig lc(dim3(nctas), dim3(128), stream, true);
+	cudaLaunchKernelEx(&lc.cfg, pack_batch_kernel, frames, cta_map);
 }
 
 } // namespace pw

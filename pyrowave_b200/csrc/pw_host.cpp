@@ -1932,3 +1932,444 @@ pyrowave_result pyrowave_cuda_decoder_decode_pyramid(pyrowave_decoder decoder, c
 	return launches_ok("kernel launch") ? PYROWAVE_SUCCESS : PYROWAVE_ERROR_GENERIC;
 }
 }
+
+// ---------------------------------------------------------------------------
+// Batched form. Every frame of the batch owns the same buffers an encoder
+// owns; the kernels of each stage run once over all frames, mapped CTA by CTA
+// through per-stage tables of batch_cta() words. A call is one CUDA graph
+// launch: upload of the per-call table, rate-control clear, the stages.
+namespace
+{
+// CTA shape choices of one batch (the autotuner's search space).
+struct BatchShape
+{
+	int small_level = kLevels; // levels >= this: transform only, quantised after the last level
+	int large_below = 0;       // other levels (forward and inverse) run 1024-thread CTAs when they have fewer tiles
+	bool operator==(const BatchShape &o) const { return small_level == o.small_level && large_below == o.large_below; }
+};
+} // namespace
+
+struct pyrowave_cuda_batch_opaque
+{
+	pyrowave_device device = nullptr;
+	int count = 0;
+	std::vector<Geometry> geo;
+	std::vector<uint32_t> capacity_words; // stream buffer per frame
+	std::vector<uint32_t> sequence;
+	std::vector<BatchFrame> frames_h;
+	std::vector<void *> owned; // device allocations
+	BatchFrame *frames_d = nullptr;
+	BatchFrameIO *io_d = nullptr;
+	BatchFrameIO *io_h[2] = {};
+	cudaEvent_t io_free[2] = {};
+	int slot = 0;
+	RateControlState *rc_d = nullptr;
+	uint32_t *h_totals = nullptr; // {error, total_words} per frame
+	cudaStream_t last_stream = nullptr;
+	bool has_result = false;
+
+	// CTA maps, one device array, per-stage ranges.
+	uint32_t *maps_d = nullptr;
+	std::vector<uint32_t> maps_h;
+	int level_off[kLevels] = {}, level_n[kLevels] = {};
+	int quant_off = 0, quant_n = 0, resolve_off = 0, resolve_n = 0, block_off = 0, block_n = 0;
+	int level_tiles[kLevels] = {}; // all frames' tiles per level
+
+	BatchShape shape;
+	CapturedGraph graphs[2][2]; // [slot][with decode]
+
+	template <typename T> T *alloc(size_t n, bool &ok)
+	{
+		T *p = dev_alloc<T>(n, ok);
+		if (p)
+			owned.push_back(p);
+		return p;
+	}
+
+	~pyrowave_cuda_batch_opaque()
+	{
+		if (device)
+			cudaStreamSynchronize(device->stream);
+		if (last_stream)
+			cudaStreamSynchronize(last_stream);
+		for (auto &row : graphs)
+			for (auto &gr : row)
+				gr.destroy();
+		for (void *p : owned)
+			dev_free(p);
+		for (int i = 0; i < 2; i++)
+		{
+			host_free(io_h[i]);
+			if (io_free[i])
+				cudaEventDestroy(io_free[i]);
+		}
+		host_free(h_totals);
+	}
+
+	void build_maps()
+	{
+		maps_h.clear();
+		for (int level = 0; level < kLevels; level++)
+		{
+			level_off[level] = int(maps_h.size());
+			for (int f = 0; f < count; f++)
+			{
+				const LevelDesc &L = geo[f].level[level];
+				const int ncomp = (level == 0 && !geo[f].chroma444) ? 1 : 3;
+				for (int i = 0; i < L.tiles_x * L.tiles_y * ncomp; i++)
+					maps_h.push_back(batch_cta(f, i));
+			}
+			level_n[level] = int(maps_h.size()) - level_off[level];
+			level_tiles[level] = level_n[level];
+		}
+		quant_off = int(maps_h.size());
+		for (int f = 0; f < count; f++)
+			for (int i = 0; i < (frames_h[f].small_blocks + 1) / 2; i++)
+				maps_h.push_back(batch_cta(f, i));
+		quant_n = int(maps_h.size()) - quant_off;
+		resolve_off = int(maps_h.size());
+		for (int f = 0; f < count; f++)
+			for (int i = 0; i < frames_h[f].slices; i++)
+				maps_h.push_back(batch_cta(f, i));
+		resolve_n = int(maps_h.size()) - resolve_off;
+		block_off = int(maps_h.size());
+		for (int f = 0; f < count; f++)
+			for (int i = 0; i < frames_h[f].block_count; i++)
+				maps_h.push_back(batch_cta(f, i));
+		block_n = int(maps_h.size()) - block_off;
+	}
+
+	// Per-frame blocks of the levels >= small_level (a prefix in block index order).
+	void apply_shape(const BatchShape &s)
+	{
+		shape = s;
+		for (int f = 0; f < count; f++)
+		{
+			const Geometry &g = geo[f];
+			frames_h[f].small_blocks = s.small_level >= kLevels ? 0
+			                           : s.small_level == 0     ? g.block_count_32x32
+			                                                    : g.band[0][s.small_level - 1][1].block32_offset;
+		}
+		for (auto &row : graphs)
+			for (auto &gr : row)
+				gr.destroy();
+	}
+
+	// Upload the frame table and the CTA maps (after apply_shape).
+	bool upload(cudaStream_t s)
+	{
+		build_maps();
+		bool ok = true;
+		if (!frames_d)
+			frames_d = alloc<BatchFrame>(size_t(count), ok);
+		if (maps_d)
+		{
+			dev_free(maps_d);
+			owned.erase(std::find(owned.begin(), owned.end(), static_cast<void *>(maps_d)));
+		}
+		maps_d = alloc<uint32_t>(maps_h.size(), ok);
+		if (!ok)
+			return false;
+		return cuda_ok(cudaMemcpyAsync(frames_d, frames_h.data(), sizeof(BatchFrame) * size_t(count),
+		                               cudaMemcpyHostToDevice, s), "cudaMemcpyAsync") &&
+		       cuda_ok(cudaMemcpyAsync(maps_d, maps_h.data(), maps_h.size() * 4, cudaMemcpyHostToDevice, s),
+		               "cudaMemcpyAsync") &&
+		       cuda_ok(cudaStreamSynchronize(s), "cudaStreamSynchronize");
+	}
+
+	bool large(int level) const { return level >= shape.small_level || level_tiles[level] < shape.large_below; }
+
+	// The stages of one call, captured into graphs[slot][decode].
+	bool capture(int slot_index, bool decode, cudaStream_t s)
+	{
+		CapturedGraph &graph = graphs[slot_index][decode ? 1 : 0];
+		if (graph.valid())
+			return true;
+		if (!graph.begin(s))
+			return false;
+		bool ok = cuda_ok(cudaMemcpyAsync(io_d, io_h[slot_index], sizeof(BatchFrameIO) * size_t(count),
+		                                  cudaMemcpyHostToDevice, s), "cudaMemcpyAsync");
+		ok = ok && cuda_ok(cudaMemsetAsync(rc_d, 0, sizeof(RateControlState) * size_t(count), s), "cudaMemsetAsync");
+		for (int level = 0; level < kLevels; level++)
+			launch_dwt_forward_batch(frames_d, io_d, maps_d + level_off[level], level_n[level], level,
+			                         level < shape.small_level, large(level), level > 0, s);
+		if (quant_n > 0)
+			launch_quant_blocks_batch(frames_d, maps_d + quant_off, quant_n, true, s);
+		launch_resolve_batch(frames_d, io_d, maps_d + resolve_off, resolve_n, s);
+		launch_pack_batch(frames_d, maps_d + block_off, block_n, s);
+		if (decode)
+		{
+			launch_dequant_batch(frames_d, maps_d + block_off, block_n, true, s);
+			for (int level = kLevels - 1; level >= 0; level--)
+				launch_idwt_batch(frames_d, io_d, maps_d + level_off[level], level_n[level], level, large(level), true,
+				                  s);
+		}
+		ok = launches_ok("kernel launch") && ok;
+		ok = graph.end(s, 0) && ok;
+		if (!ok)
+			graph.destroy();
+		return ok;
+	}
+
+	pyrowave_result run(const pyrowave_cuda_planes *inputs, const size_t *budgets, const pyrowave_cuda_planes *outputs,
+	                    cudaStream_t s)
+	{
+		// Validate everything before touching any state.
+		for (int f = 0; f < count; f++)
+		{
+			const Geometry &g = geo[f];
+			for (int p = 0; p < 3; p++)
+			{
+				if (!inputs[f].data[p] || inputs[f].row_stride_in_bytes[p] < size_t(g.plane_width[p]) ||
+				    inputs[f].row_stride_in_bytes[p] > 0x7fffffffu)
+					return PYROWAVE_ERROR_INVALID_ARGUMENT;
+				if (outputs && (!outputs[f].data[p] || outputs[f].row_stride_in_bytes[p] < size_t(g.plane_width[p]) ||
+				                outputs[f].row_stride_in_bytes[p] > 0x7fffffffu))
+					return PYROWAVE_ERROR_INVALID_ARGUMENT;
+			}
+			const uint64_t target = uint64_t(budgets[f]) & ~uint64_t(3);
+			if (target == 0 || target > 0xffffffffull || (target >= 8 ? (target - 8) / 4 : target / 4) + 2 >
+			                                                 capacity_words[f])
+				return PYROWAVE_ERROR_INVALID_ARGUMENT;
+		}
+		const int k = slot;
+		slot ^= 1;
+		// The pinned table of this slot was last read by the call before the previous one.
+		if (!cuda_ok(cudaEventSynchronize(io_free[k]), "cudaEventSynchronize"))
+			return PYROWAVE_ERROR_GENERIC;
+		for (int f = 0; f < count; f++)
+		{
+			BatchFrameIO &io = io_h[k][f];
+			io = {};
+			for (int p = 0; p < 3; p++)
+			{
+				io.in.data[p] = static_cast<const uint8_t *>(inputs[f].data[p]);
+				io.in.pitch[p] = int32_t(inputs[f].row_stride_in_bytes[p]);
+				io.in.xstride[p] = 1;
+				if (outputs)
+				{
+					io.out.data[p] = static_cast<uint8_t *>(outputs[f].data[p]);
+					io.out.pitch[p] = int32_t(outputs[f].row_stride_in_bytes[p]);
+				}
+			}
+			const uint64_t target = uint64_t(budgets[f]) & ~uint64_t(3);
+			sequence[f] = (sequence[f] + 1) & 7u;
+			io.rp = make_resolve_params(geo[f], uint32_t((target >= 8 ? target - 8 : target) / 4), sequence[f]);
+		}
+		if (!capture(k, outputs != nullptr, s))
+			return PYROWAVE_ERROR_GENERIC;
+		if (!cuda_ok(cudaGraphLaunch(graphs[k][outputs ? 1 : 0].exec, s), "cudaGraphLaunch") ||
+		    !cuda_ok(cudaEventRecord(io_free[k], s), "cudaEventRecord"))
+			return PYROWAVE_ERROR_GENERIC;
+		// {error, total_words} of every frame, for get_sizes.
+		if (!cuda_ok(cudaMemcpy2DAsync(h_totals, 8, &rc_d[0].error, sizeof(RateControlState), 8, size_t(count),
+		                               cudaMemcpyDeviceToHost, s),
+		             "cudaMemcpy2DAsync"))
+			return PYROWAVE_ERROR_GENERIC;
+		last_stream = s;
+		has_result = true;
+		return PYROWAVE_SUCCESS;
+	}
+};
+
+extern "C" {
+
+pyrowave_result pyrowave_cuda_batch_create(pyrowave_device device, const pyrowave_cuda_batch_frame_info *frames,
+                                           uint32_t count, pyrowave_cuda_batch *batch)
+{
+	if (!device || !frames || !batch || count == 0 || count > uint32_t(kMaxBatchFrames))
+		return PYROWAVE_ERROR_INVALID_ARGUMENT;
+	for (uint32_t f = 0; f < count; f++)
+	{
+		const auto &fi = frames[f];
+		if (fi.width <= 0 || fi.height <= 0)
+			return PYROWAVE_ERROR_INVALID_ARGUMENT;
+		if (fi.chroma != PYROWAVE_CHROMA_SUBSAMPLING_420 && fi.chroma != PYROWAVE_CHROMA_SUBSAMPLING_444)
+			return PYROWAVE_ERROR_INVALID_ARGUMENT;
+		if (fi.chroma == PYROWAVE_CHROMA_SUBSAMPLING_420 && ((fi.width & 1) || (fi.height & 1)))
+			return PYROWAVE_ERROR_INVALID_ARGUMENT;
+		const uint64_t target = uint64_t(fi.maximum_bitstream_size) & ~uint64_t(3);
+		if (target == 0 || target > 0xffffffffull)
+			return PYROWAVE_ERROR_INVALID_ARGUMENT;
+	}
+	auto *b = new (std::nothrow) pyrowave_cuda_batch_opaque;
+	if (!b)
+		return PYROWAVE_ERROR_OUT_OF_HOST_MEMORY;
+	b->device = device;
+	b->count = int(count);
+	b->geo.resize(count);
+	b->frames_h.resize(count);
+	b->capacity_words.resize(count);
+	b->sequence.assign(count, 0);
+	bool ok = true;
+	b->rc_d = b->alloc<RateControlState>(count, ok);
+	for (uint32_t f = 0; f < count && ok; f++)
+	{
+		const auto &fi = frames[f];
+		Geometry &g = b->geo[f];
+		if (!make_geometry(g, fi.width, fi.height, fi.chroma == PYROWAVE_CHROMA_SUBSAMPLING_444, 0))
+		{
+			delete b;
+			return PYROWAVE_ERROR_INVALID_ARGUMENT;
+		}
+		const uint64_t target = uint64_t(fi.maximum_bitstream_size) & ~uint64_t(3);
+		b->capacity_words[f] = uint32_t((target >= 8 ? target - 8 : target) / 4) + 2;
+		BatchFrame &fr = b->frames_h[f];
+		fr = {};
+		for (int level = 0; level < kLevels; level++)
+			fr.lp[level] = make_level_params(g, level);
+		fr.bp = make_block_params(g);
+		const size_t n8 = size_t(g.block_count_8x8), n32 = size_t(g.block_count_32x32);
+		EncodeBuffers &eb = fr.eb;
+		eb.coef32 = b->alloc<float>(size_t(g.storage_elems32), ok);
+		eb.coef16 = nullptr;
+		eb.code_words = b->alloc<uint32_t>(n8, ok);
+		eb.rd_cost = b->alloc<uint16_t>(n32 * 16, ok);
+		eb.rd_bucket = b->alloc<uint8_t>(n32 * 16, ok);
+		eb.rd_dist = b->alloc<float>(n32 * 16, ok);
+		eb.rc = b->rc_d ? b->rc_d + f : nullptr;
+		eb.quant = b->alloc<int32_t>(n32, ok);
+		eb.block_meta = b->alloc<uint32_t>(n32 * 2, ok);
+		eb.stream = b->alloc<uint32_t>(b->capacity_words[f], ok);
+		eb.stream_capacity_words = b->capacity_words[f];
+		eb.jobs = nullptr;
+		DecodeInput &di = fr.di;
+		di.offsets = nullptr;
+		di.block_meta = eb.block_meta;
+		di.payload = eb.stream ? eb.stream + 2 : nullptr;
+		di.payload_words = b->capacity_words[f] - 2;
+		di.coef32 = eb.coef32;
+		di.coef16 = nullptr;
+		fr.block_count = g.block_count_32x32;
+		fr.slices = std::max(1, std::min((g.block_count_32x32 + 1023) / 1024, kMaxResolveSlices));
+	}
+	b->io_d = b->alloc<BatchFrameIO>(count, ok);
+	for (int i = 0; i < 2 && ok; i++)
+	{
+		b->io_h[i] = host_alloc<BatchFrameIO>(count, ok);
+		ok = ok && cudaEventCreateWithFlags(&b->io_free[i], cudaEventDisableTiming) == cudaSuccess;
+	}
+	b->h_totals = host_alloc<uint32_t>(size_t(count) * 2, ok);
+	if (!ok)
+	{
+		(void)cudaGetLastError();
+		delete b;
+		return PYROWAVE_ERROR_OUT_OF_DEVICE_MEMORY;
+	}
+	// Default shape: the single-frame rule applied to the batch's tile counts.
+	BatchShape shape;
+	int tiles[kLevels] = {};
+	for (int f = 0; f < b->count; f++)
+		for (int level = 0; level < kLevels; level++)
+			tiles[level] += b->geo[f].level[level].tiles_x * b->geo[f].level[level].tiles_y *
+			                ((level == 0 && !b->geo[f].chroma444) ? 1 : 3);
+	for (int level = kLevels - 1; level >= 0 && tiles[level] < kSmallLevelTiles; level--)
+		shape.small_level = level;
+	shape.large_below = kSmallLevelTiles;
+	b->apply_shape(shape);
+	if (!b->upload(device->stream))
+	{
+		delete b;
+		return PYROWAVE_ERROR_GENERIC;
+	}
+	*batch = b;
+	return PYROWAVE_SUCCESS;
+}
+
+void pyrowave_cuda_batch_destroy(pyrowave_cuda_batch batch) { delete batch; }
+
+pyrowave_result pyrowave_cuda_batch_encode(pyrowave_cuda_batch batch, const pyrowave_cuda_planes *inputs,
+                                           const size_t *budgets, const pyrowave_cuda_planes *outputs,
+                                           pyrowave_cuda_stream stream)
+{
+	if (!batch || !inputs || !budgets)
+		return PYROWAVE_ERROR_INVALID_ARGUMENT;
+	return batch->run(inputs, budgets, outputs, pick_stream(batch->device, stream));
+}
+
+pyrowave_result pyrowave_cuda_batch_get_device_bitstream(pyrowave_cuda_batch batch, uint32_t index,
+                                                         const uint32_t **stream, const uint32_t **block_meta)
+{
+	if (!batch || index >= uint32_t(batch->count) || !stream || !block_meta)
+		return PYROWAVE_ERROR_INVALID_ARGUMENT;
+	*stream = batch->frames_h[index].eb.stream;
+	*block_meta = batch->frames_h[index].eb.block_meta;
+	return PYROWAVE_SUCCESS;
+}
+
+pyrowave_result pyrowave_cuda_batch_get_sizes(pyrowave_cuda_batch batch, size_t *bytes)
+{
+	if (!batch || !bytes || !batch->has_result)
+		return PYROWAVE_ERROR_INVALID_ARGUMENT;
+	if (!cuda_ok(cudaStreamSynchronize(batch->last_stream), "cudaStreamSynchronize"))
+		return PYROWAVE_ERROR_GENERIC;
+	for (int f = 0; f < batch->count; f++)
+	{
+		if (batch->h_totals[2 * f] != 0)
+			return PYROWAVE_ERROR_GENERIC; // device-side consistency check failed
+		bytes[f] = 8 + size_t(batch->h_totals[2 * f + 1]) * 4;
+	}
+	return PYROWAVE_SUCCESS;
+}
+
+pyrowave_result pyrowave_cuda_batch_autotune(pyrowave_cuda_batch batch, const pyrowave_cuda_planes *inputs,
+                                             const size_t *budgets, const pyrowave_cuda_planes *outputs,
+                                             pyrowave_cuda_stream stream)
+{
+	if (!batch || !inputs || !budgets)
+		return PYROWAVE_ERROR_INVALID_ARGUMENT;
+	cudaStream_t s = pick_stream(batch->device, stream);
+	const std::vector<uint32_t> sequence = batch->sequence; // tuning calls do not count
+	cudaEvent_t e0 = nullptr, e1 = nullptr;
+	if (!cuda_ok(cudaEventCreate(&e0), "cudaEventCreate") || !cuda_ok(cudaEventCreate(&e1), "cudaEventCreate"))
+		return PYROWAVE_ERROR_GENERIC;
+	// Candidates: where the transform-only suffix of levels starts, and below how
+	// many tiles a level runs 1024-thread CTAs. Each is timed over a few calls.
+	static const int kLargeBelow[] = {0, 148, 256, 512, 1024, 4096};
+	BatchShape best = batch->shape;
+	float best_ms = 0.0f;
+	bool have_best = false;
+	pyrowave_result r = PYROWAVE_SUCCESS;
+	for (int small = kLevels; small >= 1 && r == PYROWAVE_SUCCESS; small--)
+		for (int lb : kLargeBelow)
+		{
+			BatchShape cand;
+			cand.small_level = small;
+			cand.large_below = lb;
+			batch->apply_shape(cand);
+			if (!batch->upload(s))
+			{
+				r = PYROWAVE_ERROR_GENERIC;
+				break;
+			}
+			for (int w = 0; w < 2 && r == PYROWAVE_SUCCESS; w++)
+				r = batch->run(inputs, budgets, outputs, s);
+			if (r != PYROWAVE_SUCCESS)
+				break;
+			cudaEventRecord(e0, s);
+			for (int it = 0; it < 4 && r == PYROWAVE_SUCCESS; it++)
+				r = batch->run(inputs, budgets, outputs, s);
+			cudaEventRecord(e1, s);
+			float ms = 0.0f;
+			if (r != PYROWAVE_SUCCESS || !cuda_ok(cudaEventSynchronize(e1), "cudaEventSynchronize") ||
+			    !cuda_ok(cudaEventElapsedTime(&ms, e0, e1), "cudaEventElapsedTime"))
+			{
+				r = r != PYROWAVE_SUCCESS ? r : PYROWAVE_ERROR_GENERIC;
+				break;
+			}
+			if (!have_best || ms < best_ms)
+			{
+				best_ms = ms;
+				best = cand;
+				have_best = true;
+			}
+		}
+	cudaEventDestroy(e0);
+	cudaEventDestroy(e1);
+	batch->apply_shape(best);
+	batch->sequence = sequence;
+	if (!batch->upload(s))
+		return PYROWAVE_ERROR_GENERIC;
+	return r;
+}
+}

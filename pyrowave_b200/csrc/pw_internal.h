@@ -222,6 +222,34 @@ LevelParams make_level_params(const Geometry &g, int level);
 BlockParams make_block_params(const Geometry &g);
 ResolveParams make_resolve_params(const Geometry &g, uint32_t target_words, uint32_t sequence);
 
+// ---------------------------------------------------------------------------
+// Batched form: the frames of a batch (any sizes and chroma formats) go
+// through every stage in one launch per stage. Each frame's fixed parameters
+// sit in a device table of BatchFrame, its per-call inputs in BatchFrameIO;
+// each launch maps its CTAs to (frame, work item of that frame) through a
+// table of batch_cta() words.
+struct BatchFrame
+{
+	LevelParams lp[kLevels];
+	BlockParams bp;
+	EncodeBuffers eb;
+	DecodeInput di;      // decodes the frame's own bitstream (eb.block_meta, eb.stream + 2)
+	int32_t block_count;  // 32x32 blocks
+	int32_t slices;       // resolve CTAs
+	int32_t small_blocks; // blocks of the levels the batch quantises after the transform
+	int32_t pad;
+};
+
+struct BatchFrameIO
+{
+	PlaneInput in;
+	PlaneOutput out;
+	ResolveParams rp; // target words and sequence number of this call
+};
+
+__host__ __device__ inline uint32_t batch_cta(int frame, int local) { return (uint32_t(frame) << 24) | uint32_t(local); }
+constexpr int kMaxBatchFrames = 256;
+
 // Host-side kernel launchers (implemented in the .cu files). Every launch but
 // the first of a sequence may start early (programmatic dependent launch):
 // kernels wait for their predecessor with griddepcontrol before touching
@@ -245,5 +273,19 @@ void launch_idwt_level(const LevelParams &p, const DecodeInput &in, const PlaneO
                        cudaStream_t stream);
 void launch_pyramid_io(const BlockParams &p, float *canonical, float *coef32, __half *coef16, bool to_canonical,
                        cudaStream_t stream);
+
+// Batched launchers: `cta_map` holds one batch_cta() word per CTA.
+// large_ctas selects the 1024-thread variant of a level.
+void launch_dwt_forward_batch(const BatchFrame *frames, const BatchFrameIO *io, const uint32_t *cta_map, int nctas,
+                              int level, bool fused_quant, bool large_ctas, bool programmatic, cudaStream_t stream);
+void launch_quant_blocks_batch(const BatchFrame *frames, const uint32_t *cta_map, int nctas, bool programmatic,
+                               cudaStream_t stream);
+void launch_resolve_batch(const BatchFrame *frames, const BatchFrameIO *io, const uint32_t *cta_map, int nctas,
+                          cudaStream_t stream);
+void launch_pack_batch(const BatchFrame *frames, const uint32_t *cta_map, int nctas, cudaStream_t stream);
+void launch_dequant_batch(const BatchFrame *frames, const uint32_t *cta_map, int nctas, bool programmatic,
+                          cudaStream_t stream);
+void launch_idwt_batch(const BatchFrame *frames, const BatchFrameIO *io, const uint32_t *cta_map, int nctas, int level,
+                       bool large_ctas, bool programmatic, cudaStream_t stream);
 
 } // namespace pw
