@@ -292,6 +292,9 @@ def run_ours(args, cfg, ws, rank, local):
     batched = None
     if rank == 0 and ws == 1 and not args.no_batch:
         batched = run_batched(iters=10)
+    serving = None
+    if rank == 0 and ws == 1 and args.serve_seconds > 0:
+        serving = run_serving(args.serve_seconds)
 
     if rank == 0:
         line = {
@@ -323,6 +326,7 @@ def run_ours(args, cfg, ws, rank, local):
             "clocks": clocks,
             "cpu_baseline": cpu,
             "batched": batched,
+            "serving": serving,
         }
         print(json.dumps(line), flush=True)
     if ws > 1:
@@ -415,6 +419,83 @@ def run_batched(iters: int, frames_n: int = 64, seed: int = 7):
     batch.close()
     dev.close()
     return result
+
+
+def run_serving(seconds: float, streams_n: int = 32, pool_bytes: int = 16 << 30, seed: int = 11):
+    """Serving loop: streams_n streams with seeded Poisson frame arrivals at 60
+    or 120 fps, sizes from the batched set (4:2:0 and 4:4:4), budgets 150-250
+    Mbit/s; every frame is encoded and decoded on the device. Reports latency
+    percentiles (submit to completion) and the aggregate frame rate."""
+    import torch
+
+    from pyrowave_b200 import capi, synth
+
+    rng = np.random.default_rng(seed)
+    dev = capi.Device()
+    server = capi.Server(dev, memory_pool_bytes=pool_bytes, max_in_flight=16)
+    streams = []
+    content = {}
+    refused = 0
+    for i in range(streams_n):
+        w, h = BATCH_SIZES[int(rng.integers(len(BATCH_SIZES)))]
+        c444 = bool(rng.integers(2))
+        fps = 60.0 if rng.integers(2) == 0 else 120.0
+        budget = int(rng.uniform(150e6, 250e6) / 8 / fps) & ~3
+        code, sid = server.open_stream(w, h, capi.CHROMA_444 if c444 else capi.CHROMA_420, budget)
+        if code != capi.PYROWAVE_SUCCESS:
+            refused += 1
+            continue
+        key = (w, h, c444)
+        if key not in content:
+            content[key] = [torch.from_numpy(p).cuda() for p in synth.synth_frame(w, h, c444, 2000 + len(content))]
+        inp = content[key]
+        out = [torch.empty_like(p) for p in inp]
+        streams.append(dict(sid=sid, fps=fps, budget=budget, inp=([p.data_ptr() for p in inp],
+                                                                  [p.stride(0) for p in inp]),
+                            out=([p.data_ptr() for p in out], [p.stride(0) for p in out]), keep=out,
+                            next=float(rng.exponential(1.0 / fps))))
+    # Warm up every stream once (first-use allocation and graph capture).
+    for s in streams:
+        server.submit(s["sid"], *s["inp"], s["budget"], *s["out"])
+    got = 0
+    while got < len(streams):
+        got += len(server.poll(timeout_us=100000))
+    server.stats(reset=True)
+    start = time.perf_counter()
+    submitted = completed = 0
+    nbytes = 0
+    while True:
+        now = time.perf_counter() - start
+        if now >= seconds:
+            break
+        for s in streams:
+            while s["next"] <= now:
+                server.submit(s["sid"], *s["inp"], s["budget"], *s["out"])
+                submitted += 1
+                s["next"] += float(rng.exponential(1.0 / s["fps"]))
+        for _, _, result, b, _ in server.poll(timeout_us=0):
+            completed += 1
+            nbytes += b
+        time.sleep(0.0002)
+    while completed < submitted:
+        for _, _, result, b, _ in server.poll(timeout_us=100000):
+            completed += 1
+            nbytes += b
+    elapsed = time.perf_counter() - start
+    p50, p99, frames = server.stats()
+    server.close()
+    dev.close()
+    offered = sum(s["fps"] for s in streams)
+    return {
+        "workload": f"{streams_n} streams, Poisson arrivals at 60/120 fps, sizes {len(BATCH_SIZES)}-way mixed, "
+                    f"4:2:0 and 4:4:4, budgets 150-250 Mbit/s, {pool_bytes >> 30} GiB state pool, "
+                    f"{seconds:g} s",
+        "streams_admitted": len(streams), "streams_refused": refused,
+        "offered_frames_per_s": round(offered, 1),
+        "frames_per_s": round(completed / elapsed, 1),
+        "p50_latency_us": round(p50, 1), "p99_latency_us": round(p99, 1),
+        "frames": int(frames), "mean_bytes": round(nbytes / max(completed, 1), 1),
+    }
 
 
 def _ncu_traffic(kernel, cfg):
@@ -561,6 +642,8 @@ def main():
     ap.add_argument("--cpu-seconds", type=float, default=10.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-batch", action="store_true", help="skip the batched-form measurement")
+    ap.add_argument("--serve-seconds", type=float, default=10.0,
+                    help="duration of the serving-loop measurement (0: skip)")
     ap.add_argument("--l2", default="rotate", choices=["rotate", "flush"],
                     help="rotate: distinct inputs larger than L2; flush: 256 MiB write between steps")
     args = ap.parse_args()

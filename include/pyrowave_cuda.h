@@ -225,6 +225,67 @@ PYROWAVE_PUBLIC_API pyrowave_result pyrowave_cuda_batch_autotune(pyrowave_cuda_b
                                                                  const pyrowave_cuda_planes *outputs,
                                                                  pyrowave_cuda_stream stream);
 
+/* ------------------------------------------------------------------------
+ * Serving loop: continuous batching of encode + decode requests from many
+ * video streams on one GPU. No counterpart in the reference.
+ *
+ * Each open stream owns device-resident encoder and decoder state, reserved
+ * from a memory pool when the stream is opened (admission by memory: a stream
+ * that does not fit is refused with PYROWAVE_ERROR_OUT_OF_DEVICE_MEMORY until
+ * others close). Submitted frames are queued; a dispatcher thread starts every
+ * frame whose stream is idle as soon as one of `max_in_flight` CUDA streams is
+ * free, so the kernels of different requests overlap on the device. Frames of
+ * one stream run in submission order; each result is the same as encoding and
+ * decoding that stream alone. */
+typedef struct pyrowave_cuda_server_opaque *pyrowave_cuda_server;
+
+typedef struct pyrowave_cuda_server_info
+{
+	size_t memory_pool_bytes; /* device memory for per-stream state */
+	uint32_t max_in_flight;   /* frames on the GPU at once (1..64) */
+} pyrowave_cuda_server_info;
+
+typedef struct pyrowave_cuda_server_completion
+{
+	uint64_t request_id;
+	uint32_t stream_id;
+	int32_t result;           /* pyrowave_result of the request */
+	size_t bytes;             /* bitstream bytes of the frame */
+	double latency_us;        /* submit to completion, host clock */
+} pyrowave_cuda_server_completion;
+
+PYROWAVE_PUBLIC_API pyrowave_result pyrowave_cuda_server_create(pyrowave_device device,
+                                                                const pyrowave_cuda_server_info *info,
+                                                                pyrowave_cuda_server *server);
+/* Waits for every submitted frame, then frees everything. */
+PYROWAVE_PUBLIC_API void pyrowave_cuda_server_destroy(pyrowave_cuda_server server);
+
+PYROWAVE_PUBLIC_API pyrowave_result pyrowave_cuda_server_open_stream(pyrowave_cuda_server server, int width, int height,
+                                                                     pyrowave_chroma_subsampling chroma,
+                                                                     size_t maximum_bitstream_size,
+                                                                     uint32_t *stream_id);
+/* Releases the stream's memory once its queued frames have finished. */
+PYROWAVE_PUBLIC_API pyrowave_result pyrowave_cuda_server_close_stream(pyrowave_cuda_server server, uint32_t stream_id);
+
+/* Queue one frame: encode `input` (device planes) within `budget` bytes, then
+ * decode the new bitstream into `output` (device planes, may be NULL). Both
+ * buffers must stay valid until the completion is reported. Thread-safe. */
+PYROWAVE_PUBLIC_API pyrowave_result pyrowave_cuda_server_submit(pyrowave_cuda_server server, uint32_t stream_id,
+                                                                const pyrowave_cuda_planes *input, size_t budget,
+                                                                const pyrowave_cuda_planes *output,
+                                                                uint64_t *request_id);
+
+/* Up to `capacity` finished requests; waits up to timeout_us for the first. */
+PYROWAVE_PUBLIC_API pyrowave_result pyrowave_cuda_server_poll(pyrowave_cuda_server server,
+                                                              pyrowave_cuda_server_completion *completions,
+                                                              uint32_t capacity, uint32_t *count,
+                                                              uint32_t timeout_us);
+
+/* Latency percentiles (microseconds) and count of the requests finished since
+ * the last reset. */
+PYROWAVE_PUBLIC_API pyrowave_result pyrowave_cuda_server_stats(pyrowave_cuda_server server, double *p50_us,
+                                                               double *p99_us, uint64_t *frames, bool reset);
+
 #ifdef __cplusplus
 }
 #endif

@@ -56,6 +56,9 @@ API_SYMBOLS = [
     "pyrowave_cuda_decode_blocks_static",
     "pyrowave_cuda_batch_create", "pyrowave_cuda_batch_destroy", "pyrowave_cuda_batch_encode",
     "pyrowave_cuda_batch_get_device_bitstream", "pyrowave_cuda_batch_get_sizes", "pyrowave_cuda_batch_autotune",
+    "pyrowave_cuda_server_create", "pyrowave_cuda_server_destroy", "pyrowave_cuda_server_open_stream",
+    "pyrowave_cuda_server_close_stream", "pyrowave_cuda_server_submit", "pyrowave_cuda_server_poll",
+    "pyrowave_cuda_server_stats",
 ]
 
 # Coefficient storage limit of pyrowave_cuda_decode_blocks_static (PYROWAVE_CUDA_STATIC_DECODE_SCRATCH_BYTES).
@@ -108,6 +111,15 @@ class CudaEncoderDebug(Structure):
 class BatchFrameInfo(Structure):
     _fields_ = [("width", ctypes.c_int), ("height", ctypes.c_int), ("chroma", ctypes.c_int),
                 ("maximum_bitstream_size", c_size_t)]
+
+
+class ServerInfo(Structure):
+    _fields_ = [("memory_pool_bytes", c_size_t), ("max_in_flight", c_uint32)]
+
+
+class ServerCompletion(Structure):
+    _fields_ = [("request_id", ctypes.c_uint64), ("stream_id", c_uint32), ("result", c_int32), ("bytes", c_size_t),
+                ("latency_us", ctypes.c_double)]
 
 
 MESSAGE_CB = ctypes.CFUNCTYPE(None, c_void_p, ctypes.c_char_p)
@@ -186,6 +198,17 @@ def lib():
     L.pyrowave_cuda_batch_get_sizes.argtypes = [c_void_p, POINTER(c_size_t)]
     L.pyrowave_cuda_batch_autotune.argtypes = [c_void_p, POINTER(CudaPlanes), POINTER(c_size_t), POINTER(CudaPlanes),
                                                c_void_p]
+    L.pyrowave_cuda_server_create.argtypes = [c_void_p, POINTER(ServerInfo), POINTER(c_void_p)]
+    L.pyrowave_cuda_server_destroy.argtypes = [c_void_p]
+    L.pyrowave_cuda_server_destroy.restype = None
+    L.pyrowave_cuda_server_open_stream.argtypes = [c_void_p, c_int, c_int, c_int, c_size_t, POINTER(c_uint32)]
+    L.pyrowave_cuda_server_close_stream.argtypes = [c_void_p, c_uint32]
+    L.pyrowave_cuda_server_submit.argtypes = [c_void_p, c_uint32, POINTER(CudaPlanes), c_size_t, POINTER(CudaPlanes),
+                                              POINTER(ctypes.c_uint64)]
+    L.pyrowave_cuda_server_poll.argtypes = [c_void_p, POINTER(ServerCompletion), c_uint32, POINTER(c_uint32),
+                                            c_uint32]
+    L.pyrowave_cuda_server_stats.argtypes = [c_void_p, POINTER(ctypes.c_double), POINTER(ctypes.c_double),
+                                             POINTER(ctypes.c_uint64), c_bool]
     for name in API_SYMBOLS:
         getattr(L, name)  # every declared entry point must resolve
     _lib = L
@@ -510,3 +533,55 @@ class Batch:
         out = (c_size_t * self.count)()
         check(self.L.pyrowave_cuda_batch_get_sizes(self.h, out), "batch_get_sizes")
         return list(out)
+
+
+class Server:
+    """pyrowave_cuda_server: continuous batching of encode + decode requests from many streams."""
+
+    def __init__(self, device: Device, memory_pool_bytes: int, max_in_flight: int = 8):
+        self.L = lib()
+        self.device = device
+        device.adopt(self)
+        info = ServerInfo(memory_pool_bytes, max_in_flight)
+        h = c_void_p()
+        check(self.L.pyrowave_cuda_server_create(device.h, ctypes.byref(info), ctypes.byref(h)), "server_create")
+        self.h = h
+
+    def close(self):
+        if self.h:
+            self.L.pyrowave_cuda_server_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        self.close()
+
+    def open_stream(self, width: int, height: int, chroma: int, maximum_bitstream_size: int):
+        """Returns (result code, stream id)."""
+        sid = c_uint32()
+        code = self.L.pyrowave_cuda_server_open_stream(self.h, width, height, chroma, maximum_bitstream_size,
+                                                       ctypes.byref(sid))
+        return code, sid.value
+
+    def close_stream(self, stream_id: int) -> int:
+        return self.L.pyrowave_cuda_server_close_stream(self.h, stream_id)
+
+    def submit(self, stream_id: int, in_ptrs, in_strides, budget: int, out_ptrs=None, out_strides=None):
+        ins = _planes_array([in_ptrs], [in_strides])
+        outs = _planes_array([out_ptrs], [out_strides]) if out_ptrs is not None else None
+        rid = ctypes.c_uint64()
+        check(self.L.pyrowave_cuda_server_submit(self.h, stream_id, ins, budget, outs, ctypes.byref(rid)),
+              "server_submit")
+        return rid.value
+
+    def poll(self, capacity: int = 256, timeout_us: int = 0):
+        arr = (ServerCompletion * capacity)()
+        n = c_uint32()
+        check(self.L.pyrowave_cuda_server_poll(self.h, arr, capacity, ctypes.byref(n), timeout_us), "server_poll")
+        return [(arr[i].request_id, arr[i].stream_id, arr[i].result, arr[i].bytes, arr[i].latency_us)
+                for i in range(n.value)]
+
+    def stats(self, reset: bool = False):
+        p50, p99, frames = ctypes.c_double(), ctypes.c_double(), ctypes.c_uint64()
+        check(self.L.pyrowave_cuda_server_stats(self.h, ctypes.byref(p50), ctypes.byref(p99), ctypes.byref(frames),
+                                                reset), "server_stats")
+        return p50.value, p99.value, frames.value
