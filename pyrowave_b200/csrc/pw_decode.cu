@@ -186,12 +186,35 @@ __device__ __forceinline__ void dequant_body(const BlockParams &p, const DecodeI
 			    uint32_t(__popc(lsbs & mask) + __popc(msbs & mask)) + qb * uint32_t(sub) + s_plane_off[grp];
 			const int planes = int(qb + ((cw >> (2 * sub)) & 3u));
 			uint32_t dec[8] = {0, 0, 0, 0, 0, 0, 0, 0};
-			for (int pl = planes - 1; pl >= 0; pl--)
+			if (planes <= 16)
 			{
-				const uint32_t bits = rd.u8(byte_offset++);
+				// Plane bytes (most significant first) as the rows of two 8x8 bit
+				// matrices; transposed, byte i holds coefficient i's magnitude bits.
+				unsigned long long lo = 0, hi = 0;
+				for (int pl = planes - 1; pl >= 0; pl--)
+				{
+					const unsigned long long bits = rd.u8(byte_offset++);
+					if (pl < 8)
+						lo |= bits << (8 * pl);
+					else
+						hi |= bits << (8 * (pl - 8));
+				}
+				lo = transpose8x8(lo);
+				hi = transpose8x8(hi);
 #pragma unroll
 				for (int i = 0; i < 8; i++)
-					dec[i] |= ((bits >> i) & 1u) << pl;
+					dec[i] = uint32_t((lo >> (8 * i)) & 0xffu) | (uint32_t((hi >> (8 * i)) & 0xffu) << 8);
+			}
+			else
+			{
+				// Only a malformed header gives more than 16 planes.
+				for (int pl = planes - 1; pl >= 0; pl--)
+				{
+					const uint32_t bits = rd.u8(byte_offset++);
+#pragma unroll
+					for (int i = 0; i < 8; i++)
+						dec[i] |= ((bits >> i) & 1u) << pl;
+				}
 			}
 #pragma unroll
 			for (int i = 0; i < 8; i++)

@@ -122,6 +122,18 @@ __device__ __forceinline__ void st_release_u64(unsigned long long *p, unsigned l
 	asm volatile("st.release.gpu.global.u64 [%0], %1;" ::"l"(p), "l"(v) : "memory");
 }
 
+// 8x8 bit-matrix transpose: bit j of byte i of the input becomes bit i of byte
+// j of the output (three swap stages of 1, 2 and 4 bit-square blocks).
+__device__ __forceinline__ unsigned long long transpose8x8(unsigned long long x)
+{
+	unsigned long long t = (x ^ (x >> 7)) & 0x00AA00AA00AA00AAull;
+	x = x ^ t ^ (t << 7);
+	t = (x ^ (x >> 14)) & 0x0000CCCC0000CCCCull;
+	x = x ^ t ^ (t << 14);
+	t = (x ^ (x >> 28)) & 0x00000000F0F0F0F0ull;
+	return x ^ t ^ (t << 28);
+}
+
 // Cooperative copy of a parameter struct from global to shared memory (the
 // caller synchronises before use).
 template <typename T> __device__ __forceinline__ void load_params(T &dst, const T &src)

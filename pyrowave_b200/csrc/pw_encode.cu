@@ -103,15 +103,13 @@ __device__ __forceinline__ void quant_analyze_block(const float *tile, int tile_
 	// m = int(|v|) (|v| < 2^15), floor(|v| / 2^q) = m >> q and, for q >= 1, the
 	// reconstruction is the integer ((m >> q) << q) + 2^(q-1): the same values,
 	// computed without floating-point rounding steps.
-	uint32_t mag[8];
 	float av[8];
 	int nsig0 = 0;
 #pragma unroll
 	for (int i = 0; i < 8; i++)
 	{
 		av[i] = fabsf(v[i]);
-		mag[i] = uint32_t(int(av[i]));
-		nsig0 += mag[i] != 0u ? 1 : 0;
+		nsig0 += av[i] >= 1.0f ? 1 : 0; // int(|v|) != 0
 	}
 	int csum0 = max(cost_early0 - 1, 0) * 8 + nsig0;
 	csum0 += __shfl_xor_sync(0xffffffffu, csum0, 1);
@@ -325,7 +323,12 @@ template <int kThreads> struct DwtSplit
 	static constexpr int kGroupThreads = 128 * kQSplit;         // threads per quantised 32x32 block
 	static constexpr int kGroups = kThreads / kGroupThreads;    // 32x32 blocks quantised at once
 	static constexpr int kGen = (kTileIn * kTileIn + kThreads - 1) / kThreads; // edge-tile loads per thread
+	static constexpr int kMinBlocks = kThreads >= 1024 ? 1 : (kThreads >= 384 ? 2 : 4); // CTAs per SM to fit
 };
+
+// CTA size of the large levels (several CTAs per SM). 384-thread CTAs, which
+// quantise the three high bands of a tile in one round, measured no faster.
+constexpr int kLargeLevelThreads = 256;
 
 // One forward level for one 32x32 band tile of one component (64x64 input
 // samples): `tile` in row-major tile order, `comp_index` the component among
@@ -595,7 +598,7 @@ __device__ __forceinline__ void dwt_forward_body(const LevelParams &p, const Pla
 }
 
 template <int kThreads>
-__global__ void __launch_bounds__(kThreads, kThreads >= 1024 ? 1 : 4)
+__global__ void __launch_bounds__(kThreads, DwtSplit<kThreads>::kMinBlocks)
     dwt_forward_kernel(const LevelParams p, const PlaneInput in, const EncodeBuffers buf, const int fused)
 {
 	dwt_forward_body<kThreads>(p, in, buf, fused, int(blockIdx.x), int(blockIdx.y));
@@ -603,7 +606,7 @@ __global__ void __launch_bounds__(kThreads, kThreads >= 1024 ? 1 : 4)
 
 // Batched form: one CTA per (frame, component, tile) of this level.
 template <int kThreads>
-__global__ void __launch_bounds__(kThreads, kThreads >= 1024 ? 1 : 4)
+__global__ void __launch_bounds__(kThreads, DwtSplit<kThreads>::kMinBlocks)
     dwt_forward_batch_kernel(const BatchFrame *frames, const BatchFrameIO *io, const uint32_t *cta_map, const int level,
                              const int fused)
 {
@@ -1141,15 +1144,26 @@ __device__ __forceinline__ void pack_body(const BlockParams &p, const EncodeBuff
 		bytes[8 + 2 * n + compact] = uint8_t(cw >> 16);
 	}
 	const uint32_t plane_base = 8 + 3 * n + excl_bytes + sub_plane_offset;
-	for (uint32_t pl = 0; pl < planes; pl++)
+	if (planes != 0)
 	{
-		const uint32_t bit = uint32_t(quant) + planes - 1u - pl; // most significant plane first
-		uint32_t by = 0;
+		// Bit plane k of the 8 magnitudes is byte k of the transposed bit matrix
+		// whose byte i holds the magnitude of coefficient i (low and high 8 bits).
+		unsigned long long lo = 0, hi = 0;
 #pragma unroll
 		for (int i = 0; i < 8; i++)
-			by |= ((mag[i] >> bit) & 1u) << i;
-		if (plane_base + pl < uint32_t(kMaxBlockWords) * 4)
-			bytes[plane_base + pl] = uint8_t(by);
+		{
+			lo |= (unsigned long long)(mag[i] & 0xffu) << (8 * i);
+			hi |= (unsigned long long)((mag[i] >> 8) & 0xffu) << (8 * i);
+		}
+		lo = transpose8x8(lo);
+		hi = transpose8x8(hi);
+		for (uint32_t pl = 0; pl < planes; pl++)
+		{
+			const uint32_t bit = uint32_t(quant) + planes - 1u - pl; // most significant plane first
+			const uint32_t by = bit < 8 ? uint32_t(lo >> (8 * bit)) : (bit < 16 ? uint32_t(hi >> (8 * (bit - 8))) : 0u);
+			if (plane_base + pl < uint32_t(kMaxBlockWords) * 4)
+				bytes[plane_base + pl] = uint8_t(by);
+		}
 	}
 	__syncthreads();
 
@@ -1225,8 +1239,8 @@ void launch_dwt_forward_level(const LevelParams &p, const PlaneInput &in, const 
 	}
 	else
 	{
-		LaunchConfig lc(grid, dim3(256), stream, programmatic);
-		cudaLaunchKernelEx(&lc.cfg, dwt_forward_kernel<256>, p, in, buf, f);
+		LaunchConfig lc(grid, dim3(kLargeLevelThreads), stream, programmatic);
+		cudaLaunchKernelEx(&lc.cfg, dwt_forward_kernel<kLargeLevelThreads>, p, in, buf, f);
 	}
 }
 
@@ -1261,8 +1275,8 @@ void launch_dwt_forward_batch(const BatchFrame *frames, const BatchFrameIO *io, 
 	}
 	else
 	{
-		LaunchConfig lc(dim3(nctas), dim3(256), stream, programmatic);
-		cudaLaunchKernelEx(&lc.cfg, dwt_forward_batch_kernel<256>, frames, io, cta_map, level, f);
+		LaunchConfig lc(dim3(nctas), dim3(kLargeLevelThreads), stream, programmatic);
+		cudaLaunchKernelEx(&lc.cfg, dwt_forward_batch_kernel<kLargeLevelThreads>, frames, io, cta_map, level, f);
 	}
 }
 
