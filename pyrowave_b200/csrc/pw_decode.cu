@@ -107,9 +107,8 @@ __device__ __forceinline__ void dequant_body(const BlockParams &p, const DecodeI
 	if (off == 0xffffffffu)
 	{
 		// Missing block: all coefficients are zero (wavelet_dequant.comp:242-248).
-#pragma unroll
-		for (int i = 0; i < 8; i++)
-			store_coef(in.coef32, in.coef16, f16, B.offset + int64_t(oy + (i & 1)) * L.pitch + ox + (i >> 1), 0.0f);
+		const float zero[8] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+		store_subblock(in.coef32, in.coef16, f16, B.offset + int64_t(oy) * L.pitch + ox, L.pitch, zero);
 		return;
 	}
 
@@ -250,20 +249,21 @@ __device__ __forceinline__ void dequant_body(const BlockParams &p, const DecodeI
 	uint32_t bitpos = s_sign_base + inc - nsig;
 	for (int w = 0; w < ly; w++)
 		bitpos += s_sig[w];
+	// This thread's (at most 8) sign bits are consecutive: one 64-bit window.
+	const uint32_t sw = bitpos >> 5, sh = bitpos & 31u;
+	const uint64_t window = (uint64_t(rd.w32(sw + 1)) << 32 | rd.w32(sw)) >> sh;
+	int nth = 0;
 #pragma unroll
 	for (int i = 0; i < 8; i++)
 	{
 		if (v[i] != 0.0f)
 		{
-			const uint32_t bit = (rd.w32(bitpos >> 5) >> (bitpos & 31u)) & 1u;
-			if (bit)
+			if ((window >> nth) & 1u)
 				v[i] = -v[i];
-			bitpos++;
+			nth++;
 		}
 	}
-#pragma unroll
-	for (int i = 0; i < 8; i++)
-		store_coef(in.coef32, in.coef16, f16, B.offset + int64_t(oy + (i & 1)) * L.pitch + ox + (i >> 1), v[i]);
+	store_subblock(in.coef32, in.coef16, f16, B.offset + int64_t(oy) * L.pitch + ox, L.pitch, v);
 }
 
 __global__ void __launch_bounds__(128) dequant_kernel(const BlockParams p, const DecodeInput in, const int first)

@@ -134,6 +134,53 @@ __device__ __forceinline__ unsigned long long transpose8x8(unsigned long long x)
 	return x ^ t ^ (t << 28);
 }
 
+// The 8 coefficients of a 4x2 sub-block in the quantiser's order (i = 2 * column
+// + row) as two 4-wide row vectors: idx is the element index of (row 0, column
+// 0), a multiple of 4 (the sub-block starts on a 4-column boundary of a
+// 32-aligned band row), pitch the row pitch in elements.
+__device__ __forceinline__ void load_subblock(const float *c32, const __half *c16, bool fp16, int64_t idx, int pitch,
+                                              float (&c)[8])
+{
+	float4 r0, r1;
+	if (fp16)
+	{
+		const uint2 a = __ldcg(reinterpret_cast<const uint2 *>(c16 + idx));
+		const uint2 b = __ldcg(reinterpret_cast<const uint2 *>(c16 + idx + pitch));
+		const float2 a0 = __half22float2(*reinterpret_cast<const __half2 *>(&a.x));
+		const float2 a1 = __half22float2(*reinterpret_cast<const __half2 *>(&a.y));
+		const float2 b0 = __half22float2(*reinterpret_cast<const __half2 *>(&b.x));
+		const float2 b1 = __half22float2(*reinterpret_cast<const __half2 *>(&b.y));
+		r0 = make_float4(a0.x, a0.y, a1.x, a1.y);
+		r1 = make_float4(b0.x, b0.y, b1.x, b1.y);
+	}
+	else
+	{
+		r0 = __ldcg(reinterpret_cast<const float4 *>(c32 + idx));
+		r1 = __ldcg(reinterpret_cast<const float4 *>(c32 + idx + pitch));
+	}
+	c[0] = r0.x, c[2] = r0.y, c[4] = r0.z, c[6] = r0.w;
+	c[1] = r1.x, c[3] = r1.y, c[5] = r1.z, c[7] = r1.w;
+}
+
+__device__ __forceinline__ void store_subblock(float *c32, __half *c16, bool fp16, int64_t idx, int pitch,
+                                               const float (&c)[8])
+{
+	if (fp16)
+	{
+		const __half2 a0 = __floats2half2_rn(c[0], c[2]), a1 = __floats2half2_rn(c[4], c[6]);
+		const __half2 b0 = __floats2half2_rn(c[1], c[3]), b1 = __floats2half2_rn(c[5], c[7]);
+		*reinterpret_cast<uint2 *>(c16 + idx) =
+		    make_uint2(*reinterpret_cast<const uint32_t *>(&a0), *reinterpret_cast<const uint32_t *>(&a1));
+		*reinterpret_cast<uint2 *>(c16 + idx + pitch) =
+		    make_uint2(*reinterpret_cast<const uint32_t *>(&b0), *reinterpret_cast<const uint32_t *>(&b1));
+	}
+	else
+	{
+		*reinterpret_cast<float4 *>(c32 + idx) = make_float4(c[0], c[2], c[4], c[6]);
+		*reinterpret_cast<float4 *>(c32 + idx + pitch) = make_float4(c[1], c[3], c[5], c[7]);
+	}
+}
+
 // Cooperative copy of a parameter struct from global to shared memory (the
 // caller synchronises before use).
 template <typename T> __device__ __forceinline__ void load_params(T &dst, const T &src)
@@ -177,18 +224,20 @@ __device__ __forceinline__ float load_coef(const float *c32, const __half *c16, 
 // ---------------------------------------------------------------------------
 // Quantiser helpers (reference: dwt_quant_scale.h, wavelet_quant.comp,
 // block_packing.comp, pyrowave_common.hpp:124-145).
+// code / 8 + 0.25 (the division by 8 is exact, so it is a multiplication).
 __device__ __forceinline__ float decode_quant_scale(uint32_t code)
 {
-	return __fadd_rn(__fdiv_rn(float(code), 8.0f), 0.25f);
+	return __fadd_rn(__fmul_rn(float(code), 0.125f), 0.25f);
 }
 
 // Custom FP quant code of the 32x32 header: (8+m) * 2^(20+e) / 2^23 with
-// e = 4 - (code >> 3), written as an exact ldexp.
+// e = 4 - (code >> 3): an exact product with the power of two 2^(e-3)
+// (e - 3 is within [-30, 1], a normal exponent).
 __device__ __forceinline__ float decode_quant(uint32_t code)
 {
-	int e = kMaxScaleExp - int(code >> 3);
-	int m = int(code & 7u);
-	return ldexpf(float(8 + m), e - 3);
+	const int e = kMaxScaleExp - int(code >> 3);
+	const int m = int(code & 7u);
+	return __fmul_rn(float(8 + m), __int_as_float((127 + e - 3) << 23));
 }
 
 __device__ __forceinline__ int find_msb(uint32_t v) { return v ? 31 - __clz(v) : -1; }

@@ -1022,6 +1022,7 @@ __device__ __forceinline__ void pack_body(const BlockParams &p, const EncodeBuff
 	__shared__ uint32_t s_ballot[4];
 	__shared__ uint32_t s_bytes[16];
 	__shared__ uint32_t s_sig[4];
+	__shared__ float s_inv_scale[16];
 	pdl_trigger();
 	const int k = find_band(p, blk);
 	const BandEntry &B = p.band[k];
@@ -1034,18 +1035,16 @@ __device__ __forceinline__ void pack_body(const BlockParams &p, const EncodeBuff
 	const int x8 = bx32 * 4 + lx, y8 = by32 * 4 + ly;
 	const bool in_range = x8 < L.blocks8_x && y8 < L.blocks8_y;
 	const int ox = bx32 * 32 + lx * 8 + sub_x(sub), oy = by32 * 32 + ly * 8 + sub_y(sub);
+	// 1 / (code / 8 + 0.25) for every 4-bit scale code, as the quantiser computed it.
+	if (t < 16)
+		s_inv_scale[t] = __fdiv_rn(1.0f, decode_quant_scale(uint32_t(t)));
 
 	// The resolve kernel releases this grid only after every quantiser has
 	// finished, so coefficients and code words can be fetched before the wait;
 	// only the rate-control decisions come from the resolve kernel itself.
 	const uint32_t cw0 = in_range ? __ldcg(&buf.code_words[B.block8_offset + y8 * B.block8_stride + x8]) : 0u;
 	float coef[8];
-#pragma unroll
-	for (int i = 0; i < 8; i++)
-	{
-		const int64_t idx = B.offset + int64_t(oy + (i & 1)) * L.pitch + ox + (i >> 1);
-		coef[i] = L.fp16 ? __half2float(__ldcg(buf.coef16 + idx)) : __ldcg(buf.coef32 + idx);
-	}
+	load_subblock(buf.coef32, buf.coef16, L.fp16 != 0, B.offset + int64_t(oy) * L.pitch + ox, L.pitch, coef);
 	pdl_wait();
 
 	const uint2 meta = __ldcg(reinterpret_cast<const uint2 *>(buf.block_meta) + blk);
@@ -1056,9 +1055,10 @@ __device__ __forceinline__ void pack_body(const BlockParams &p, const EncodeBuff
 	const uint32_t offset = meta.x;
 	const uint32_t cw = quantize_code_word(cw0, quant);
 	const bool active = (cw & 0xffffu) != 0;
+	__syncthreads(); // s_inv_scale
 
 	// Re-quantise this sub-block exactly as the quantiser did.
-	const float qs = __fdiv_rn(1.0f, decode_quant_scale((cw0 >> kQuantScaleOffset) & 0xfu));
+	const float qs = s_inv_scale[(cw0 >> kQuantScaleOffset) & 0xfu];
 	uint32_t mag[8];
 	uint32_t neg = 0;
 #pragma unroll
@@ -1116,14 +1116,17 @@ __device__ __forceinline__ void pack_body(const BlockParams &p, const EncodeBuff
 
 	const uint32_t ballot = s_ballot[0] | (s_ballot[1] << 4) | (s_ballot[2] << 8) | (s_ballot[3] << 12);
 	const uint32_t n = uint32_t(__popc(ballot));
-	uint32_t excl_bytes = 0, total_bytes = 0;
+	// Plane bytes before this 8x8 and in total: a 16-lane inclusive scan in every warp.
+	uint32_t scan_bytes = s_bytes[lane & 15];
 #pragma unroll
-	for (int g16 = 0; g16 < 16; g16++)
+	for (int off = 1; off < 16; off *= 2)
 	{
-		if (g16 < grp)
-			excl_bytes += s_bytes[g16];
-		total_bytes += s_bytes[g16];
+		const uint32_t y = __shfl_up_sync(0xffffffffu, scan_bytes, off, 16);
+		if ((lane & 15) >= off)
+			scan_bytes += y;
 	}
+	const uint32_t total_bytes = __shfl_sync(0xffffffffu, scan_bytes, 15);
+	const uint32_t excl_bytes = __shfl_sync(0xffffffffu, scan_bytes, grp) - s_bytes[grp];
 	uint32_t sig_base = 0;
 	for (int w = 0; w < ly; w++)
 		sig_base += s_sig[w];
@@ -1168,15 +1171,28 @@ __device__ __forceinline__ void pack_body(const BlockParams &p, const EncodeBuff
 	__syncthreads();
 
 	// Sign bits of significant coefficients, in coefficient order, after the planes.
-	uint32_t bitpos = (8 + 3 * n + total_bytes) * 8 + sig_excl;
-#pragma unroll
-	for (int i = 0; i < 8; i++)
+	// This thread's sign bits are consecutive in the stream: gather them (sign
+	// of each significant coefficient, in order) and OR them in with at most two
+	// word updates.
 	{
-		if ((sig >> i) & 1u)
+		const uint32_t bitpos = (8 + 3 * n + total_bytes) * 8 + sig_excl;
+		uint32_t bits = 0;
+		int k = 0;
+#pragma unroll
+		for (int i = 0; i < 8; i++)
 		{
-			if (((neg >> i) & 1u) && (bitpos >> 5) < uint32_t(kMaxBlockWords))
-				atomicOr(&pkt[bitpos >> 5], 1u << (bitpos & 31u));
-			bitpos++;
+			if ((sig >> i) & 1u)
+			{
+				bits |= ((neg >> i) & 1u) << k;
+				k++;
+			}
+		}
+		const uint32_t w = bitpos >> 5, sh = bitpos & 31u;
+		if (bits != 0 && w < uint32_t(kMaxBlockWords))
+		{
+			atomicOr(&pkt[w], bits << sh);
+			if (sh != 0 && (bits >> (32u - sh)) != 0 && w + 1 < uint32_t(kMaxBlockWords))
+				atomicOr(&pkt[w + 1], bits >> (32u - sh));
 		}
 	}
 	__syncthreads();
