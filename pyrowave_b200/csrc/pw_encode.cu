@@ -158,24 +158,27 @@ __device__ __forceinline__ void quant_analyze_block(const float *tile, int tile_
 		// truncate by adding 2^23 with round-toward-zero and subtracting it again
 		// (the quotient is below 2^15). The reconstruction fl * 2^q + 2^(q-1) is
 		// an exact integer, so err equals the integer formulation above.
+		// With sg = min(fl, 1) (1 when significant), the error is
+		// |v| - fl * 2^q - sg * 2^(q-1): two fused multiply-adds whose exact
+		// results are representable, so they round to themselves.
 		const float pq = __int_as_float((127 + q) << 23);
 		const float ipq = __int_as_float((127 - q) << 23);
 		const float hq = __int_as_float((126 + q) << 23);
-		int nsig = 0;
+		float nsig_f = 0.0f;
 		float e0 = 0.0f, e1 = 0.0f;
 #pragma unroll
 		for (int i = 0; i < 8; i++)
 		{
 			const float fl = __fsub_rn(__fadd_rz(__fmul_rn(av[i], ipq), 8388608.0f), 8388608.0f);
-			const bool sig = fl != 0.0f;
-			nsig += sig ? 1 : 0;
-			const float recon = sig ? __fmaf_rn(fl, pq, hq) : 0.0f;
-			const float err = __fsub_rn(av[i], recon);
+			const float sg = fminf(fl, 1.0f);
+			nsig_f = __fadd_rn(nsig_f, sg);
+			const float err = __fmaf_rn(-sg, hq, __fmaf_rn(-fl, pq, av[i]));
 			if (i < 4)
 				e0 = (i == 0) ? __fmul_rn(err, err) : __fmaf_rn(err, err, e0);
 			else
 				e1 = (i == 4) ? __fmul_rn(err, err) : __fmaf_rn(err, err, e1);
 		}
+		const int nsig = int(nsig_f);
 		float se = __fmul_rn(__fmul_rn(__fadd_rn(e0, e1), rdo), iqs);
 		se = __fadd_rn(se, __shfl_xor_sync(0xffffffffu, se, 1));
 		se = __fadd_rn(se, __shfl_xor_sync(0xffffffffu, se, 2));
