@@ -154,25 +154,24 @@ __device__ __forceinline__ void quant_analyze_block(const float *tile, int tile_
 	for (int q = 1 + r; q <= warp_msb; q += S)
 	{
 		// compute_square_error + compute_quant_stats at q (wavelet_quant.comp:113-165).
-		// floor(|v| / 2^q) in float arithmetic, exactly: scale by 2^-q, then
-		// truncate by adding 2^23 with round-toward-zero and subtracting it again
-		// (the quotient is below 2^15). The reconstruction fl * 2^q + 2^(q-1) is
-		// an exact integer, so err equals the integer formulation above.
-		// With sg = min(fl, 1) (1 when significant), the error is
-		// |v| - fl * 2^q - sg * 2^(q-1): two fused multiply-adds whose exact
-		// results are representable, so they round to themselves.
-		const float pq = __int_as_float((127 + q) << 23);
-		const float ipq = __int_as_float((127 - q) << 23);
+		// R = floor(|v| / 2^q) * 2^q in float arithmetic, exactly: adding
+		// M = 2^(23+q) with round-toward-zero keeps the multiples of 2^q (the
+		// spacing of floats in [M, 2M), and |v| < 2^15 < M), and subtracting M
+		// again is exact. The reconstruction R + 2^(q-1) is an exact integer, so
+		// err equals the integer formulation above. With sg = min(R, 1) (1 when
+		// significant), err = (|v| - R) - sg * 2^(q-1): the difference and the
+		// fused multiply-add are exact, so they round to themselves.
 		const float hq = __int_as_float((126 + q) << 23);
+		const float mq = __int_as_float((150 + q) << 23);
 		float nsig_f = 0.0f;
 		float e0 = 0.0f, e1 = 0.0f;
 #pragma unroll
 		for (int i = 0; i < 8; i++)
 		{
-			const float fl = __fsub_rn(__fadd_rz(__fmul_rn(av[i], ipq), 8388608.0f), 8388608.0f);
-			const float sg = fminf(fl, 1.0f);
+			const float R = __fsub_rn(__fadd_rz(av[i], mq), mq);
+			const float sg = fminf(R, 1.0f);
 			nsig_f = __fadd_rn(nsig_f, sg);
-			const float err = __fmaf_rn(-sg, hq, __fmaf_rn(-fl, pq, av[i]));
+			const float err = __fmaf_rn(-sg, hq, __fsub_rn(av[i], R));
 			if (i < 4)
 				e0 = (i == 0) ? __fmul_rn(err, err) : __fmaf_rn(err, err, e0);
 			else
