@@ -1,0 +1,55 @@
+"""Per-subband transform error against an FP64 evaluation of the same lifting.
+
+The quantiser maps a band's coefficients onto steps of 1 / quant_resolution
+(pyrowave_encoder.cpp:107-172); a coefficient error below half a step cannot
+move a value across a quantiser decision on its own. The kernels are bit-exact
+with the oracle's F32 mode (tests/test_gpu_parity.py), so the oracle's F32 and
+FP16-storage pyramids are the kernels' pyramids; these tests run on the CPU.
+"""
+import numpy as np
+import pytest
+
+import oracle as O
+from pyrowave_b200 import synth
+
+
+def _band_ratios(w, h, c444, mask, seed):
+    """{(comp, level, band): max |err| / (half a quantiser step)} of the F32-mode
+    transform with FP16 storage of the levels in `mask`, against FP64."""
+    planes = synth.synth_frame(w, h, c444, seed)
+    o = O.Oracle(w, h, c444, mask)
+    ref = O.Oracle(w, h, c444).dwt(planes, O.MODE_F64)
+    got = o.dwt(planes, O.MODE_F32).astype(np.float64)
+    offs = o.band_offsets()
+    qr, _ = o.quant_tables()
+    out = {}
+    for c in range(3):
+        for level in range(5):
+            n = (o.aligned_width >> (level + 1)) * (o.aligned_height >> (level + 1))
+            for band in range(4):
+                off = int(offs[c, level, band])
+                if off < 0:
+                    continue
+                err = float(np.abs(got[off:off + n] - ref[off:off + n]).max())
+                out[(c, level, band)] = err / (0.5 / float(qr[c, level, band]))
+    return out
+
+
+@pytest.mark.parametrize("w,h,c444,seed", [(1920, 1080, False, 1), (1280, 720, False, 0), (640, 360, True, 5)])
+def test_fp32_lifting_far_below_half_step(w, h, c444, seed):
+    """FP32 lifting with FP32 storage: every subband's error is under 1% of half a step."""
+    ratios = _band_ratios(w, h, c444, 0, seed)
+    worst = max(ratios.items(), key=lambda kv: kv[1])
+    assert worst[1] < 0.01, worst
+
+
+def test_fp16_storage_exceeds_half_step():
+    """FP16 storage of level 0, level 1 or both (the reference's precision 1
+    stores levels 0-1 in FP16) puts some subband of 1080p 4:2:0 past half a
+    step, through the rounded LL that feeds the deeper levels; so the library
+    stores FP32 unless a caller opts in with pyrowave_cuda_*_set_precision.
+    The level-0 bands themselves stay below half a step."""
+    for mask in (1, 2, 3):
+        ratios = _band_ratios(1920, 1080, False, mask, 1)
+        assert max(ratios.values()) > 0.5, mask
+        assert max(v for (c, level, b), v in ratios.items() if level == 0) < 0.5, mask
