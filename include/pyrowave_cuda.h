@@ -48,7 +48,12 @@ PYROWAVE_PUBLIC_API pyrowave_result pyrowave_cuda_device_set_stage_timing(pyrowa
 
 /* Coefficient storage precision per decomposition level. Default 0 (FP32 at
  * every level); 0x3 matches the reference's default precision layout (FP16 for
- * levels 0-1). Must be called before the first encode / decode. */
+ * levels 0-1). Must be called before the first encode / decode.
+ * PYROWAVE_CUDA_PRECISION_STAGE16 added to the mask also rounds every lifting
+ * input and output to FP16, as the reference's precision 1 stages its shared
+ * memory in FP16 (dwt_common.h:45-47); 0x3 | STAGE16 reproduces that precision
+ * (pyrowave_common.cpp:133-157). Encoder and decoder of one stream should agree. */
+#define PYROWAVE_CUDA_PRECISION_STAGE16 0x100u
 PYROWAVE_PUBLIC_API pyrowave_result pyrowave_cuda_encoder_set_precision(pyrowave_encoder encoder, uint32_t fp16_level_mask);
 PYROWAVE_PUBLIC_API pyrowave_result pyrowave_cuda_decoder_set_precision(pyrowave_decoder decoder, uint32_t fp16_level_mask);
 

@@ -29,6 +29,12 @@ PYROWAVE_ERROR_NOT_IMPLEMENTED = -6
 CHROMA_420 = 0
 CHROMA_444 = 1
 
+# Precision flag of pyrowave_cuda_*_set_precision: lifting staged through FP16
+# as in the reference's precision 1; REFERENCE_PRECISION adds FP16 storage of
+# levels 0-1, which together reproduce that precision.
+PRECISION_STAGE16 = 0x100
+REFERENCE_PRECISION = PRECISION_STAGE16 | 0x3
+
 FORMAT_NV12 = 0
 FORMAT_YUV420P = 1
 FORMAT_YUV444P = 2

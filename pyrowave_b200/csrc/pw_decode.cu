@@ -377,7 +377,13 @@ __device__ __forceinline__ void idwt_body(const LevelParams &p, const DecodeInpu
 			const int b = k / (kBandTile * kVecPerRow);
 			const int r = k - b * kBandTile * kVecPerRow;
 			const int i = r / kVecPerRow, j = r - i * kVecPerRow;
-			const float vals[4] = {v[u].x, v[u].y, v[u].z, v[u].w};
+			float vals[4] = {v[u].x, v[u].y, v[u].z, v[u].w};
+			if (L.stage16)
+			{
+#pragma unroll
+				for (int e = 0; e < 4; e++)
+					vals[e] = round_to_half(vals[e]);
+			}
 #pragma unroll
 			for (int e = 0; e < 4; e++)
 			{
@@ -417,7 +423,7 @@ __device__ __forceinline__ void idwt_body(const LevelParams &p, const DecodeInpu
 					const int b = k / (kBandTile * kBandTile);
 					const int r = k - b * kBandTile * kBandTile;
 					const int i = r / kBandTile, j = r - i * kBandTile;
-					sh.band[b][i][j] = v[u];
+					sh.band[b][i][j] = L.stage16 ? round_to_half(v[u]) : v[u];
 				}
 			}
 		}
@@ -442,7 +448,7 @@ __device__ __forceinline__ void idwt_body(const LevelParams &p, const DecodeInpu
 		lift_inverse(e);
 #pragma unroll
 		for (int jj = 4; jj < 4 + kOut; jj++)
-			sh.v[which][seg * kOut + jj - 4][col] = e[jj];
+			sh.v[which][seg * kOut + jj - 4][col] = L.stage16 ? round_to_half(e[jj]) : e[jj];
 	}
 	__syncthreads();
 
@@ -459,6 +465,12 @@ __device__ __forceinline__ void idwt_body(const LevelParams &p, const DecodeInpu
 			e[jj] = (q & 1) ? __fmul_rn(sh.v[1][row][i], kInvK) : __fmul_rn(sh.v[0][row][i], kK);
 		}
 		lift_inverse(e);
+		if (L.stage16)
+		{
+#pragma unroll
+			for (int jj = 4; jj < 4 + kOut; jj++)
+				e[jj] = round_to_half(e[jj]);
+		}
 		const int gy = ty * 64 + row;
 		const int gx0 = tx * 64 + seg * kOut;
 		if (final_level)

@@ -371,7 +371,10 @@ __device__ __forceinline__ void dwt_forward_body(const LevelParams &p, const Pla
 	}
 	if (from_plane)
 		for (int u = threadIdx.x; u < 256; u += kThreads)
-			sh.unorm[u] = unorm8_centered(uint32_t(u));
+		{
+			const float f = unorm8_centered(uint32_t(u));
+			sh.unorm[u] = L.stage16 ? round_to_half(f) : f;
+		}
 	__syncthreads();
 	pdl_wait();
 
@@ -520,8 +523,14 @@ __device__ __forceinline__ void dwt_forward_body(const LevelParams &p, const Pla
 #pragma unroll
 		for (int k = 0; k < kSegPairs; k++)
 		{
-			sh.h[row][seg * kSegPairs + k] = __fmul_rn(e[4 + 2 * k], kInvK);
-			sh.h[row][32 + seg * kSegPairs + k] = __fmul_rn(e[5 + 2 * k], kK);
+			float lo = __fmul_rn(e[4 + 2 * k], kInvK), hi = __fmul_rn(e[5 + 2 * k], kK);
+			if (L.stage16)
+			{
+				lo = round_to_half(lo);
+				hi = round_to_half(hi);
+			}
+			sh.h[row][seg * kSegPairs + k] = lo;
+			sh.h[row][32 + seg * kSegPairs + k] = hi;
 		}
 	}
 	__syncthreads();
@@ -549,7 +558,7 @@ __device__ __forceinline__ void dwt_forward_body(const LevelParams &p, const Pla
 			float hi = __fmul_rn(e[5 + 2 * k], kK);
 			if (gx >= L.width || gy >= L.height)
 				lo = hi = 0.0f;
-			else if (L.fp16)
+			else if (L.fp16 || L.stage16)
 			{
 				lo = round_to_half(lo);
 				hi = round_to_half(hi);

@@ -142,6 +142,7 @@ bool build_geometry(Geometry &g, int width, int height, bool chroma444, uint32_t
 		L.blocks8_x = (L.width + 7) / 8;
 		L.blocks8_y = (L.height + 7) / 8;
 		L.fp16 = (fp16_mask >> level) & 1u;
+		L.stage16 = (fp16_mask & PYROWAVE_CUDA_PRECISION_STAGE16) ? 1 : 0;
 	}
 
 	// Storage: every band of every (component, level) that exists, LL included.
@@ -1209,7 +1210,7 @@ pyrowave_result fill_layout(const Geometry &g, uint32_t mask, pyrowave_cuda_layo
 				if (g.band[comp][level][band].present)
 					n += size_t(g.level[level].width) * g.level[level].height;
 	layout->pyramid_size = n;
-	layout->fp16_level_mask = mask;
+	layout->fp16_level_mask = mask & 0x1fu;
 	return PYROWAVE_SUCCESS;
 }
 } // namespace
@@ -1696,7 +1697,7 @@ void pyrowave_decoder_destroy(pyrowave_decoder decoder)
 // --- CUDA extension ----------------------------------------------------------
 pyrowave_result pyrowave_cuda_encoder_set_precision(pyrowave_encoder encoder, uint32_t fp16_level_mask)
 {
-	if (!encoder || (fp16_level_mask & ~0x1fu))
+	if (!encoder || (fp16_level_mask & ~(0x1fu | PYROWAVE_CUDA_PRECISION_STAGE16)))
 		return PYROWAVE_ERROR_INVALID_ARGUMENT;
 	if (encoder->allocated && fp16_level_mask != encoder->fp16_mask)
 		encoder->release();
@@ -1706,7 +1707,7 @@ pyrowave_result pyrowave_cuda_encoder_set_precision(pyrowave_encoder encoder, ui
 
 pyrowave_result pyrowave_cuda_decoder_set_precision(pyrowave_decoder decoder, uint32_t fp16_level_mask)
 {
-	if (!decoder || (fp16_level_mask & ~0x1fu))
+	if (!decoder || (fp16_level_mask & ~(0x1fu | PYROWAVE_CUDA_PRECISION_STAGE16)))
 		return PYROWAVE_ERROR_INVALID_ARGUMENT;
 	if (decoder->allocated && fp16_level_mask != decoder->fp16_mask)
 		decoder->release();

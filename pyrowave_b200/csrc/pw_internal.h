@@ -57,6 +57,7 @@ struct LevelDesc
 	int32_t tiles_x, tiles_y; // 32x32 band tiles
 	int32_t blocks8_x, blocks8_y;
 	int32_t fp16;             // 1: coefficients of this level are stored as FP16
+	int32_t stage16;          // 1: lifting inputs and outputs rounded to FP16 (reference precision 1)
 };
 
 struct Geometry

@@ -142,6 +142,52 @@ def test_encode_decode_bit_exact(device, case):
     assert not errors, "\n".join(errors)
 
 
+@pytest.mark.parametrize("w,h,c444,budget,seed", [(1920, 1080, False, 400000, 1), (1920, 1080, False, 400000, 2),
+                                                  (200, 128, True, 30000, 6)])
+def test_reference_precision_bit_exact(device, w, h, c444, budget, seed):
+    """REFERENCE_PRECISION (FP16 lifting stages, FP16 levels 0-1) against the
+    oracle's restatement of the reference's precision 1: pyramid, packets and
+    decoded planes bit for bit, hence the same PSNR at the same budget."""
+    import torch
+
+    chroma = capi.CHROMA_444 if c444 else capi.CHROMA_420
+    planes = synth.synth_frame(w, h, c444, seed)
+    mode = capi.REFERENCE_PRECISION
+    enc = capi.Encoder(device, w, h, chroma, mode)
+    o = O.Oracle(w, h, c444, 3)
+    d = _to_dev(planes)
+    enc.encode_device([p.data_ptr() for p in d], [p.stride(0) for p in d], budget)
+    pyr = torch.zeros(enc.layout().pyramid_size, dtype=torch.float32, device="cuda")
+    enc.read_wavelet(pyr.data_ptr())
+    torch.cuda.synchronize()
+    ref_pyr = o.dwt(planes, O.MODE_REF16)
+    errors = [_mismatch("dwt bits", pyr.cpu().numpy().view(np.uint32), ref_pyr.view(np.uint32))]
+
+    assert enc.encode_cpu(planes, budget) == capi.PYROWAVE_SUCCESS
+    stream, packets = enc.packetize(8192, budget)
+    o.encode_pyramid(ref_pyr, budget, sequence=2)
+    ostream, opackets = o.packetize(8192, budget)
+    total = sum(p[1] for p in packets)
+    assert total <= budget
+    errors.append(_mismatch("packets", np.array(packets, np.int64).reshape(-1, 2), opackets))
+    errors.append(_mismatch("stream bytes", stream[:total], ostream[:total]))
+
+    dec = capi.Decoder(device, w, h, chroma, mode)
+    for off, sz in packets:
+        assert dec.push_packet(stream[off:off + sz]) == capi.PYROWAVE_SUCCESS
+    code, out = dec.decode_cpu()
+    assert code == capi.PYROWAVE_SUCCESS
+    p = o.parser()
+    for off, sz in packets:
+        assert p.push(stream[off:off + sz].tobytes())
+    offs, payload = p.get()
+    oout = o.idwt(o.dequant(offs, payload, O.MODE_REF16), O.MODE_REF16)
+    for i in range(3):
+        errors.append(_mismatch(f"decoded plane {i}", out[i], oout[i]))
+    errors = [e for e in errors if e]
+    assert not errors, "\n".join(errors)
+
+
 @pytest.mark.parametrize("w,h,c444", [(1280, 720, False), (640, 480, True)])
 def test_dwt_accuracy_vs_fp64(device, w, h, c444):
     """The FP32 transform stays within 1e-5 of an FP64 evaluation of the same lifting."""
