@@ -295,6 +295,9 @@ def run_ours(args, cfg, ws, rank, local):
     serving = None
     if rank == 0 and ws == 1 and args.serve_seconds > 0:
         serving = run_serving(args.serve_seconds)
+    secondary = None
+    if rank == 0 and ws == 1 and not args.no_configs:
+        secondary = run_secondary(steps=30, warmup=5)
 
     if rank == 0:
         line = {
@@ -327,6 +330,7 @@ def run_ours(args, cfg, ws, rank, local):
             "cpu_baseline": cpu,
             "batched": batched,
             "serving": serving,
+            "configs": secondary,
         }
         print(json.dumps(line), flush=True)
     if ws > 1:
@@ -498,6 +502,98 @@ def run_serving(seconds: float, streams_n: int = 32, pool_bytes: int = 16 << 30,
     }
 
 
+SECONDARY = [
+    # (name, config, budget, precision mask)
+    ("720p", "720p", 150000, 0),
+    ("1080p_fp16_storage", "1080p", 400000, 0x3),
+    ("1080p_reference_precision", "1080p", 400000, 0x103),
+    ("4k", "4k", 1200000, 0),
+    ("4k_fp16_storage", "4k", 1200000, 0x3),
+    ("4k444_600000", "4k444", 600000, 0),
+    ("4k444_1200000", "4k444", 1200000, 0),
+    ("4k444_2400000", "4k444", 2400000, 0),
+]
+
+
+def measure_config(dev, cfg, budget, mask, steps, warmup):
+    """Device-resident encode + decode of one configuration: us/frame over
+    `steps` frames (inputs rotated through more than twice L2), then the same
+    steps with per-kernel events for per-stage us and GB/s (algorithmic bytes)."""
+    import torch
+
+    from pyrowave_b200 import capi
+
+    w, h, c444 = cfg["width"], cfg["height"], cfg["chroma444"]
+    chroma = capi.CHROMA_444 if c444 else capi.CHROMA_420
+    base = [[torch.from_numpy(p).cuda() for p in f] for f in make_frames(dict(cfg, seeds=cfg["seeds"][:2]))]
+    frame_bytes = sum(p.numel() for p in base[0])
+    n = max(len(base), -(-2 * (126 << 20) // frame_bytes))
+    nb = len(base)
+    frames = [[torch.roll(p, shifts=(3 * (i // nb), 5 * (i // nb)), dims=(0, 1)).contiguous() if i >= nb else p
+               for p in base[i % nb]] for i in range(n)]
+    out = [torch.empty_like(p) for p in base[0]]
+    enc = capi.Encoder(dev, w, h, chroma, mask)
+    dec = capi.Decoder(dev, w, h, chroma, mask)
+    stream = torch.cuda.Stream()
+    sid = stream.cuda_stream
+    sizes = []
+
+    def step(i):
+        f = frames[i % len(frames)]
+        enc.encode_device([p.data_ptr() for p in f], [p.stride(0) for p in f], budget, sid)
+        s, m, cap = enc.device_bitstream()
+        dec.decode_blocks(m, s + 8, cap - 2, [p.data_ptr() for p in out], [p.stride(0) for p in out], sid)
+
+    for i in range(warmup):
+        step(i)
+        torch.cuda.synchronize()
+        sizes.append(enc.size())
+
+    def timed():
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        e0.record(stream)
+        for i in range(steps):
+            step(i)
+        e1.record(stream)
+        e1.synchronize()
+        return e0.elapsed_time(e1) / steps
+
+    ms = timed()
+    dev.set_stage_timing(True)
+    dev.report_performance_stats(reset=True)
+    timed()
+    stages = {}
+    for line in dev.report_performance_stats(reset=True):
+        tag, rest = line.split(":", 1)
+        stages[tag.strip()] = float(rest.split("ms")[0])
+    dev.set_stage_timing(False)
+    alg = algorithmic_bytes(dict(cfg, budget=budget), mask & 0x1F)
+    dwt_ms = sum(v for k, v in stages.items() if k.startswith("dwt"))
+    enc.close()
+    dec.close()
+    return {
+        "workload": f"encode+decode {w}x{h} {'4:4:4' if c444 else '4:2:0'} 8-bit, {budget}-byte budget",
+        "precision_mask": hex(mask), "us_per_frame": round(ms * 1e3, 2),
+        "bytes_per_frame": max(sizes), "within_budget": all(0 < s <= budget for s in sizes),
+        "stages_us": {k: round(v * 1e3, 2) for k, v in stages.items()},
+        "stages_gbs": {k: round(alg[k] / (v * 1e-3) / 1e9, 1) for k, v in stages.items() if k in alg and v > 0},
+        "dwt_stage_gbs": round(alg["dwt_stage"] / (dwt_ms * 1e-3) / 1e9, 1) if dwt_ms else None,
+        "note": "stage times carry one event pair per kernel (launch gaps included)",
+    }
+
+
+def run_secondary(steps, warmup):
+    from pyrowave_b200 import capi
+
+    dev = capi.Device()
+    out = {}
+    for name, cfg_name, budget, mask in SECONDARY:
+        out[name] = measure_config(dev, CONFIGS[cfg_name], budget, mask, steps, warmup)
+    dev.close()
+    return out
+
+
 def _ncu_traffic(kernel, cfg):
     """DRAM bytes per launch of `kernel` from the committed ncu summary, if present."""
     p = os.path.join(ROOT, "profiles", "ncu_traffic.json")
@@ -642,6 +738,8 @@ def main():
     ap.add_argument("--cpu-seconds", type=float, default=10.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-batch", action="store_true", help="skip the batched-form measurement")
+    ap.add_argument("--no-configs", action="store_true",
+                    help="skip the other configurations (720p, FP16 storage, reference precision, 4K, 4K 4:4:4 sweep)")
     ap.add_argument("--serve-seconds", type=float, default=10.0,
                     help="duration of the serving-loop measurement (0: skip)")
     ap.add_argument("--l2", default="rotate", choices=["rotate", "flush"],

@@ -1296,7 +1296,7 @@ void pyrowave_device_report_performance_stats(pyrowave_device device, pyrowave_m
 	for (auto &t : device->timers)
 	{
 		char msg[256];
-		snprintf(msg, sizeof(msg), "%s: %.3f ms per frame\n", t.tag, t.frames ? t.total_ms / double(t.frames) : 0.0);
+		snprintf(msg, sizeof(msg), "%s: %.4f ms per frame\n", t.tag, t.frames ? t.total_ms / double(t.frames) : 0.0);
 		cb(userdata, msg);
 	}
 	if (reset)
