@@ -292,6 +292,9 @@ def run_ours(args, cfg, ws, rank, local):
     batched = None
     if rank == 0 and ws == 1 and not args.no_batch:
         batched = run_batched(iters=10)
+    packet_decode = None
+    if rank == 0 and ws == 1 and not args.no_configs:
+        packet_decode = run_packet_decode(cfg, frames)
     serving = None
     if rank == 0 and ws == 1 and args.serve_seconds > 0:
         serving = run_serving(args.serve_seconds)
@@ -331,6 +334,7 @@ def run_ours(args, cfg, ws, rank, local):
             "batched": batched,
             "serving": serving,
             "configs": secondary,
+            "device_packet_decode": packet_decode,
         }
         print(json.dumps(line), flush=True)
     if ws > 1:
@@ -339,6 +343,54 @@ def run_ours(args, cfg, ws, rank, local):
 
 
 BATCH_SIZES = [(1280, 720), (1366, 768), (1920, 1080), (2560, 1080), (2560, 1440), (3840, 2160)]
+
+
+def run_packet_decode(cfg, frames, steps: int = 50, boundary: int = 8192):
+    """Decode from received packets already in device memory: assembly on the
+    GPU (pyrowave_cuda_decoder_decode_packets) against decoding the encoder's
+    device-resident blocks (pyrowave_cuda_decoder_decode_blocks), us per frame."""
+    import torch
+
+    from pyrowave_b200 import capi
+
+    w, h, c444, budget = cfg["width"], cfg["height"], cfg["chroma444"], cfg["budget"]
+    chroma = capi.CHROMA_444 if c444 else capi.CHROMA_420
+    dev = capi.Device()
+    enc = capi.Encoder(dev, w, h, chroma)
+    dec = capi.Decoder(dev, w, h, chroma)
+    assert enc.encode_cpu(frames[0], budget) == capi.PYROWAVE_SUCCESS
+    stream_bytes, packets = enc.packetize(boundary, budget)
+    total = sum(sz for _, sz in packets)
+    d_data = torch.from_numpy(np.ascontiguousarray(stream_bytes[:total])).cuda()
+    d_desc = torch.from_numpy(np.array(packets, np.int64).reshape(-1)).cuda()
+    out = [torch.empty(p.shape, dtype=torch.uint8, device="cuda") for p in frames[0]]
+    ptrs, strides = [t.data_ptr() for t in out], [t.stride(0) for t in out]
+    s, m, cap = enc.device_bitstream()
+    stream = torch.cuda.Stream()
+
+    def timed(fn):
+        for _ in range(5):
+            fn()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(steps):
+            fn()
+        e1.record(stream)
+        e1.synchronize()
+        return e0.elapsed_time(e1) * 1e3 / steps
+
+    packets_us = timed(lambda: capi.check(dec.decode_packets(d_data.data_ptr(), total, d_desc.data_ptr(), len(packets),
+                                                             ptrs, strides, stream.cuda_stream), "decode_packets"))
+    st = dec.packet_status()
+    blocks_us = timed(lambda: dec.decode_blocks(m, s + 8, cap - 2, ptrs, strides, stream.cuda_stream))
+    enc.close()
+    dec.close()
+    dev.close()
+    return {"workload": f"decode {w}x{h} {'4:4:4' if c444 else '4:2:0'} from {len(packets)} packets of "
+                        f"<= {boundary} B in device memory ({total} B)",
+            "us_per_frame": round(packets_us, 2), "decode_blocks_us_per_frame": round(blocks_us, 2),
+            "complete": bool(st.decoded_blocks >= st.total_blocks), "invalid_packets": int(st.invalid_packets)}
 
 
 def run_batched(iters: int, frames_n: int = 64, seed: int = 7):

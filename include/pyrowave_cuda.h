@@ -128,6 +128,41 @@ PYROWAVE_PUBLIC_API pyrowave_result pyrowave_cuda_decoder_decode_blocks(pyrowave
                                                                         const pyrowave_cuda_planes *planes,
                                                                         pyrowave_cuda_stream stream);
 
+/* Assemble a frame from received packets on the GPU and decode it: the
+ * device-side counterpart of pyrowave_decoder_clear, then
+ * pyrowave_decoder_push_packet for every packet in order
+ * (pyrowave_decoder.cpp:126-262), then pyrowave_decoder_decode_gpu_buffer.
+ * `data` holds the packets in device memory (4-byte aligned, at most 4 GiB);
+ * `packets` is a device array of `count` {offset, size} byte ranges of `data`,
+ * in push order, each offset a multiple of 4. The sequence rules of the
+ * reference parser apply (a newer sequence restarts the frame, packets of an
+ * older one are ignored from that point of the packet on, the first copy of a
+ * block wins); blocks not received decode as zero. A packet the host parser
+ * would reject keeps what it added before the fault, as push_packet does,
+ * except that a block announcing fewer than two words is left missing. Nothing
+ * waits: the outcome is read with pyrowave_cuda_decoder_get_packet_status. */
+typedef struct pyrowave_cuda_packet_status
+{
+	uint32_t decoded_blocks;  /* distinct blocks of the assembled frame */
+	uint32_t total_blocks;    /* blocks its sequence header announced (the layout's count without one) */
+	uint32_t sequence;        /* 3-bit sequence of the frame, 0xffffffff when no packet was accepted */
+	uint32_t invalid_packets; /* packets pyrowave_decoder_push_packet would have rejected */
+} pyrowave_cuda_packet_status;
+
+PYROWAVE_PUBLIC_API pyrowave_result pyrowave_cuda_decoder_decode_packets(pyrowave_decoder decoder, const void *data,
+                                                                         size_t data_size,
+                                                                         const pyrowave_packet *packets,
+                                                                         uint32_t count,
+                                                                         const pyrowave_cuda_planes *planes,
+                                                                         pyrowave_cuda_stream stream);
+
+/* Outcome of the last pyrowave_cuda_decoder_decode_packets (waits for it).
+ * The frame was complete when decoded_blocks >= total_blocks; the reference's
+ * partial-frame rule (pyrowave_decoder_decode_is_ready with
+ * allow_partial_frame) accepts more than half. */
+PYROWAVE_PUBLIC_API pyrowave_result pyrowave_cuda_decoder_get_packet_status(pyrowave_decoder decoder,
+                                                                            pyrowave_cuda_packet_status *status);
+
 /* Copy the last decode's dequantised pyramid (canonical layout, device memory). */
 PYROWAVE_PUBLIC_API pyrowave_result pyrowave_cuda_decoder_read_wavelet(pyrowave_decoder decoder, float *pyramid,
                                                                        pyrowave_cuda_stream stream);

@@ -59,6 +59,7 @@ API_SYMBOLS = [
     "pyrowave_cuda_encoder_get_size", "pyrowave_cuda_encoder_encode_pre_transformed",
     "pyrowave_cuda_encoder_read_wavelet", "pyrowave_cuda_encoder_read_debug", "pyrowave_cuda_decoder_decode",
     "pyrowave_cuda_decoder_decode_blocks", "pyrowave_cuda_decoder_read_wavelet", "pyrowave_cuda_decoder_decode_pyramid",
+    "pyrowave_cuda_decoder_decode_packets", "pyrowave_cuda_decoder_get_packet_status",
     "pyrowave_cuda_decode_blocks_static",
     "pyrowave_cuda_batch_create", "pyrowave_cuda_batch_destroy", "pyrowave_cuda_batch_encode",
     "pyrowave_cuda_batch_get_device_bitstream", "pyrowave_cuda_batch_get_sizes", "pyrowave_cuda_batch_autotune",
@@ -96,6 +97,11 @@ class RateControl(Structure):
 
 class Packet(Structure):
     _fields_ = [("offset", c_size_t), ("size", c_size_t)]
+
+
+class PacketStatus(Structure):
+    _fields_ = [("decoded_blocks", c_uint32), ("total_blocks", c_uint32), ("sequence", c_uint32),
+                ("invalid_packets", c_uint32)]
 
 
 class CudaPlanes(Structure):
@@ -192,6 +198,9 @@ def lib():
     L.pyrowave_cuda_decoder_decode_blocks.argtypes = [c_void_p, c_void_p, c_void_p, c_size_t, POINTER(CudaPlanes),
                                                       c_void_p]
     L.pyrowave_cuda_decoder_read_wavelet.argtypes = [c_void_p, c_void_p, c_void_p]
+    L.pyrowave_cuda_decoder_decode_packets.argtypes = [c_void_p, c_void_p, c_size_t, c_void_p, c_uint32,
+                                                       POINTER(CudaPlanes), c_void_p]
+    L.pyrowave_cuda_decoder_get_packet_status.argtypes = [c_void_p, POINTER(PacketStatus)]
     L.pyrowave_cuda_decoder_decode_pyramid.argtypes = [c_void_p, c_void_p, POINTER(CudaPlanes), c_void_p]
     L.pyrowave_cuda_decode_blocks_static.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_int, c_void_p, c_void_p,
                                                      c_size_t, POINTER(CudaPlanes), c_void_p]
@@ -458,6 +467,22 @@ class Decoder:
             cp.row_stride_in_bytes[i] = strides[i]
         check(self.L.pyrowave_cuda_decoder_decode_blocks(self.h, c_void_p(meta_ptr), c_void_p(words_ptr), num_words,
                                                          ctypes.byref(cp), c_void_p(stream)), "decode_blocks")
+
+    def decode_packets(self, data_ptr: int, data_size: int, packets_ptr: int, count: int, plane_ptrs, strides,
+                       stream: int = 0) -> int:
+        """pyrowave_cuda_decoder_decode_packets: assemble a frame from device-resident packets
+        ({offset, size} u64 pairs at packets_ptr) on the GPU and decode it. Returns the result code."""
+        cp = CudaPlanes()
+        for i in range(3):
+            cp.data[i] = plane_ptrs[i]
+            cp.row_stride_in_bytes[i] = strides[i]
+        return self.L.pyrowave_cuda_decoder_decode_packets(self.h, c_void_p(data_ptr), data_size, c_void_p(packets_ptr),
+                                                           count, ctypes.byref(cp), c_void_p(stream))
+
+    def packet_status(self) -> PacketStatus:
+        st = PacketStatus()
+        check(self.L.pyrowave_cuda_decoder_get_packet_status(self.h, ctypes.byref(st)), "get_packet_status")
+        return st
 
     def decode_pyramid(self, pyramid_ptr: int, plane_ptrs, strides, stream: int = 0):
         cp = CudaPlanes()

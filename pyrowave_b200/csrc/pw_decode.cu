@@ -95,7 +95,13 @@ __device__ __forceinline__ void dequant_body(const BlockParams &p, const DecodeI
 	pdl_wait();
 
 	uint32_t off, words = 0;
-	if (in.offsets)
+	const bool sized_by_header = in.offsets || in.keys;
+	if (in.keys)
+	{
+		const unsigned long long key = __ldcg(in.keys + blk);
+		off = key == ~0ull ? 0xffffffffu : uint32_t(key & 0x3fffffffull);
+	}
+	else if (in.offsets)
 		off = __ldcg(in.offsets + blk);
 	else
 	{
@@ -118,7 +124,7 @@ __device__ __forceinline__ void dequant_body(const BlockParams &p, const DecodeI
 	// kSpeculativeWords are fetched together with it.
 	const PayloadReader grd{in.payload, in.payload_words};
 	uint32_t staged;
-	if (in.offsets)
+	if (sized_by_header)
 	{
 		stage_words(s_words, grd, off, 0, kSpeculativeWords, t);
 		__syncthreads();

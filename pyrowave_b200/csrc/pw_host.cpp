@@ -878,6 +878,20 @@ struct pyrowave_decoder_opaque
 	KernelNode node_dequant;
 	KernelNode node_idwt_full[kLevels], node_idwt_only[kLevels];
 
+	// Device-side packet assembly (pw_packets.cu): per-packet tables, grown on demand.
+	uint32_t *pk_tables = nullptr;
+	uint8_t *pk_state = nullptr;
+	uint32_t *pk_summaries = nullptr;
+	size_t pk_capacity = 0; // packets
+	uint32_t *pk_items = nullptr;
+	size_t pk_items_capacity = 0; // words
+	unsigned long long *pk_first = nullptr;
+	PacketStatus *pk_status = nullptr;
+	PacketStatus *pk_status_h = nullptr;
+	uint32_t *pk_counter = nullptr;
+	cudaEvent_t pk_done = nullptr;
+	bool pk_pending = false;
+
 	// Parser state (pyrowave_decoder.cpp:24-39).
 	std::vector<uint32_t> offsets;
 	std::vector<uint32_t> payload;
@@ -999,6 +1013,28 @@ struct pyrowave_decoder_opaque
 		for (auto &p : out_planes)
 			dev_free(p);
 		host_free(h_upload);
+		dev_free(pk_tables);
+		dev_free(pk_state);
+		dev_free(pk_summaries);
+		dev_free(pk_items);
+		dev_free(pk_first);
+		dev_free(pk_status);
+		dev_free(pk_counter);
+		host_free(pk_status_h);
+		if (pk_done)
+			cudaEventDestroy(pk_done);
+		pk_tables = nullptr;
+		pk_state = nullptr;
+		pk_summaries = nullptr;
+		pk_items = nullptr;
+		pk_items_capacity = 0;
+		pk_first = nullptr;
+		pk_status = nullptr;
+		pk_counter = nullptr;
+		pk_status_h = nullptr;
+		pk_done = nullptr;
+		pk_capacity = 0;
+		pk_pending = false;
 		timing.destroy();
 		graph_full.destroy();
 		graph_idwt.destroy();
@@ -1147,6 +1183,76 @@ struct pyrowave_decoder_opaque
 	}
 
 	// Upload the parsed frame and decode it.
+	// Assemble the frame from packets in device memory on the GPU, then decode it.
+	pyrowave_result decode_packets(const void *data, size_t data_bytes, const pyrowave_packet *packets, uint32_t count,
+	                               const PlaneOutput &out, cudaStream_t s)
+	{
+		bool ok = true;
+		if (!pk_first)
+		{
+			pk_first = dev_alloc<unsigned long long>(size_t(g.block_count_32x32), ok);
+			pk_status = dev_alloc<PacketStatus>(1, ok);
+			pk_counter = dev_alloc<uint32_t>(1, ok);
+			pk_status_h = host_alloc<PacketStatus>(1, ok);
+			if (ok && cudaMemset(pk_counter, 0, sizeof(uint32_t)) != cudaSuccess)
+				ok = false;
+			if (ok && cudaEventCreateWithFlags(&pk_done, cudaEventDisableTiming) != cudaSuccess)
+				ok = false;
+		}
+		if (ok && count > pk_capacity)
+		{
+			cudaStreamSynchronize(s);
+			dev_free(pk_tables);
+			dev_free(pk_state);
+			dev_free(pk_summaries);
+			const size_t cap = std::max<size_t>(count, 256);
+			pk_tables = dev_alloc<uint32_t>(cap * 18, ok);
+			pk_state = dev_alloc<uint8_t>(cap, ok);
+			pk_summaries = dev_alloc<uint32_t>(cap * 8, ok);
+			pk_capacity = ok ? cap : 0;
+		}
+		const size_t data_words = (data_bytes + 3) / 4;
+		if (ok && data_words > pk_items_capacity)
+		{
+			cudaStreamSynchronize(s);
+			dev_free(pk_items);
+			const size_t cap = std::max<size_t>(data_words, 1 << 16);
+			pk_items = dev_alloc<uint32_t>(cap, ok);
+			pk_items_capacity = ok ? cap : 0;
+		}
+		if (!ok)
+			return PYROWAVE_ERROR_OUT_OF_DEVICE_MEMORY;
+		PacketParams pp = {};
+		pp.data = static_cast<const uint32_t *>(data);
+		pp.data_bytes = data_bytes;
+		pp.packets = reinterpret_cast<const unsigned long long *>(packets);
+		pp.count = int32_t(count);
+		pp.width = g.width;
+		pp.height = g.height;
+		pp.chroma444 = g.chroma444;
+		pp.block_count = g.block_count_32x32;
+		pp.tables = pk_tables;
+		pp.state_before = pk_state;
+		pp.summaries = pk_summaries;
+		pp.items = pk_items;
+		pp.first = pk_first;
+		pp.counter = pk_counter;
+		pp.status = pk_status;
+		launch_packet_assembly(pp, s);
+		DecodeInput in = {};
+		in.keys = pk_first;
+		in.payload = pp.data;
+		in.payload_words = uint32_t(data_bytes / 4);
+		in.jobs = jobs_d;
+		in.coef32 = coef32;
+		in.coef16 = coef16;
+		if (!run(in, out, s, true))
+			return PYROWAVE_ERROR_GENERIC;
+		cudaEventRecord(pk_done, s);
+		pk_pending = true;
+		return launches_ok("kernel launch") ? PYROWAVE_SUCCESS : PYROWAVE_ERROR_GENERIC;
+	}
+
 	pyrowave_result decode_parsed(const PlaneOutput &out, cudaStream_t s)
 	{
 		pyrowave_result r = ensure_payload(payload.size());
@@ -1898,6 +2004,45 @@ pyrowave_result pyrowave_cuda_decoder_decode_blocks(pyrowave_decoder decoder, co
 	return launches_ok("kernel launch") ? PYROWAVE_SUCCESS : PYROWAVE_ERROR_GENERIC;
 }
 
+pyrowave_result pyrowave_cuda_decoder_decode_packets(pyrowave_decoder decoder, const void *data, size_t data_size,
+                                                     const pyrowave_packet *packets, uint32_t count,
+                                                     const pyrowave_cuda_planes *planes, pyrowave_cuda_stream stream)
+{
+	if (!decoder || !data || !packets || !planes || count == 0 || count > uint32_t(kMaxPackets) ||
+	    data_size > 0xffffffffull || (reinterpret_cast<uintptr_t>(data) & 3u) != 0 ||
+	    (reinterpret_cast<uintptr_t>(packets) & 7u) != 0)
+		return PYROWAVE_ERROR_INVALID_ARGUMENT;
+	pyrowave_result r = decoder->allocate();
+	if (r != PYROWAVE_SUCCESS)
+		return r;
+	PlaneOutput out = {};
+	for (int p = 0; p < 3; p++)
+	{
+		if (!planes->data[p] || planes->row_stride_in_bytes[p] < size_t(decoder->g.plane_width[p]) ||
+		    planes->row_stride_in_bytes[p] > 0x7fffffffu)
+			return PYROWAVE_ERROR_INVALID_ARGUMENT;
+		out.data[p] = static_cast<uint8_t *>(planes->data[p]);
+		out.pitch[p] = int32_t(planes->row_stride_in_bytes[p]);
+	}
+	return decoder->decode_packets(data, data_size, packets, count, out, pick_stream(decoder->device, stream));
+}
+
+pyrowave_result pyrowave_cuda_decoder_get_packet_status(pyrowave_decoder decoder, pyrowave_cuda_packet_status *status)
+{
+	if (!decoder || !status || !decoder->pk_pending)
+		return PYROWAVE_ERROR_INVALID_ARGUMENT;
+	if (!cuda_ok(cudaEventSynchronize(decoder->pk_done), "cudaEventSynchronize") ||
+	    !cuda_ok(cudaMemcpy(decoder->pk_status_h, decoder->pk_status, sizeof(PacketStatus), cudaMemcpyDeviceToHost),
+	             "cudaMemcpy"))
+		return PYROWAVE_ERROR_GENERIC;
+	const PacketStatus &st = *decoder->pk_status_h;
+	status->decoded_blocks = st.decoded_blocks;
+	status->total_blocks = st.total_blocks;
+	status->sequence = st.sequence;
+	status->invalid_packets = st.invalid_packets;
+	return PYROWAVE_SUCCESS;
+}
+
 pyrowave_result pyrowave_cuda_decoder_read_wavelet(pyrowave_decoder decoder, float *pyramid, pyrowave_cuda_stream stream)
 {
 	if (!decoder || !pyramid || !decoder->allocated)
@@ -2236,6 +2381,7 @@ pyrowave_result pyrowave_cuda_batch_create(pyrowave_device device, const pyrowav
 		eb.jobs = nullptr;
 		DecodeInput &di = fr.di;
 		di.offsets = nullptr;
+		di.keys = nullptr;
 		di.block_meta = eb.block_meta;
 		di.payload = eb.stream ? eb.stream + 2 : nullptr;
 		di.payload_words = b->capacity_words[f] - 2;

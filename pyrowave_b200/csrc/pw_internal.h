@@ -146,6 +146,7 @@ struct DecodeInput
 {
 	const uint32_t *offsets;    // per 32x32 block, UINT32_MAX = missing (reference format), or nullptr
 	const uint32_t *block_meta; // alternatively {offset, num_words} pairs; num_words == 0 = missing
+	const unsigned long long *keys; // alternatively packet-assembly keys: word offset in the low 30 bits, ~0 = missing
 	const uint32_t *payload;    // concatenated block words
 	uint32_t payload_words;
 	const uint32_t *jobs;
@@ -274,6 +275,37 @@ void launch_idwt_level(const LevelParams &p, const DecodeInput &in, const PlaneO
                        cudaStream_t stream);
 void launch_pyramid_io(const BlockParams &p, float *canonical, float *coef32, __half *coef16, bool to_canonical,
                        cudaStream_t stream);
+
+// Device-side packet assembly (pw_packets.cu). The first four fields of
+// PacketStatus are the public pyrowave_cuda_packet_status.
+struct PacketStatus
+{
+	uint32_t decoded_blocks;  // distinct blocks kept
+	uint32_t total_blocks;    // blocks the frame's sequence header announced, else the layout's count
+	uint32_t sequence;        // 3-bit sequence of the assembled frame, 0xffffffff: none
+	uint32_t invalid_packets; // packets the host parser would reject
+	uint32_t restart_packet, restart_item; // position of the last restart
+	uint32_t pad[2];
+};
+
+struct PacketParams
+{
+	const uint32_t *data;             // the received packets (device memory, 4-byte aligned)
+	unsigned long long data_bytes;
+	const unsigned long long *packets; // {offset, size} in bytes per packet (pyrowave_packet), device memory
+	int32_t count;
+	int32_t width, height, chroma444, block_count;
+	uint32_t *tables;                 // count x 9 x {state | error << 4 | restart << 8, total}
+	uint8_t *state_before;            // count
+	uint32_t *summaries;              // count x 8 words: each packet's item summary
+	uint32_t *items;                  // data_bytes / 4: packet p's item positions at its own first word on
+	unsigned long long *first;        // block_count: smallest (packet, item, word offset) key, ~0 = missing
+	uint32_t *counter;                // CTAs of the table pass done (zero between calls)
+	PacketStatus *status;
+};
+
+constexpr int kMaxPackets = 1 << 20;
+void launch_packet_assembly(const PacketParams &pp, cudaStream_t stream);
 
 // Batched launchers: `cta_map` holds one batch_cta() word per CTA.
 // large_ctas selects the 1024-thread variant of a level.
