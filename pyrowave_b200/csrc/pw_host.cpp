@@ -853,6 +853,49 @@ struct pyrowave_encoder_opaque
 	}
 };
 
+// Growable array of 32-bit words in page-locked host memory: the parser's
+// payload, uploaded without a staging copy when the caller waits for the decode.
+struct PinnedWords
+{
+	uint32_t *ptr = nullptr;
+	size_t n = 0, cap = 0;
+	PinnedWords() = default;
+	PinnedWords(const PinnedWords &) = delete;
+	PinnedWords &operator=(const PinnedWords &) = delete;
+	~PinnedWords()
+	{
+		if (ptr)
+			cudaFreeHost(ptr);
+	}
+	size_t size() const { return n; }
+	bool empty() const { return n == 0; }
+	uint32_t *data() { return ptr; }
+	const uint32_t *data() const { return ptr; }
+	void clear() { n = 0; }
+	bool reserve(size_t c)
+	{
+		if (c <= cap)
+			return true;
+		uint32_t *np = nullptr;
+		if (cudaHostAlloc(reinterpret_cast<void **>(&np), c * 4, cudaHostAllocDefault) != cudaSuccess)
+			return false;
+		if (n)
+			memcpy(np, ptr, n * 4);
+		if (ptr)
+			cudaFreeHost(ptr);
+		ptr = np;
+		cap = c;
+		return true;
+	}
+	bool resize(size_t m)
+	{
+		if (m > cap && !reserve(std::max(m, cap * 2)))
+			return false;
+		n = m;
+		return true;
+	}
+};
+
 struct pyrowave_decoder_opaque
 {
 	pyrowave_device device = nullptr;
@@ -894,7 +937,7 @@ struct pyrowave_decoder_opaque
 
 	// Parser state (pyrowave_decoder.cpp:24-39).
 	std::vector<uint32_t> offsets;
-	std::vector<uint32_t> payload;
+	PinnedWords payload;
 	int decoded_blocks = 0;
 	int total_blocks_in_sequence = 0;
 	uint32_t last_seq = UINT32_MAX;
@@ -921,8 +964,9 @@ struct pyrowave_decoder_opaque
 		if (payload_words < 2)
 			return false;
 		size_t base = payload.size();
-		payload.resize(base + payload_words);
-		memcpy(&payload[base], data, size_t(payload_words) * 4);
+		if (!payload.resize(base + payload_words))
+			return false;
+		memcpy(payload.data() + base, data, size_t(payload_words) * 4);
 		return true;
 	}
 
@@ -1253,18 +1297,27 @@ struct pyrowave_decoder_opaque
 		return launches_ok("kernel launch") ? PYROWAVE_SUCCESS : PYROWAVE_ERROR_GENERIC;
 	}
 
-	pyrowave_result decode_parsed(const PlaneOutput &out, cudaStream_t s)
+	// `waits`: the caller synchronizes with `s` before the parser can change,
+	// so the payload is uploaded straight from the parser's page-locked array;
+	// otherwise it is staged first.
+	pyrowave_result decode_parsed(const PlaneOutput &out, cudaStream_t s, bool waits = false)
 	{
 		pyrowave_result r = ensure_payload(payload.size());
 		if (r != PYROWAVE_SUCCESS)
 			return r;
 		const size_t nb = size_t(g.block_count_32x32);
 		memcpy(h_upload, offsets.data(), nb * 4);
-		if (!payload.empty())
-			memcpy(h_upload + nb, payload.data(), payload.size() * 4);
 		cudaMemcpyAsync(offsets_d, h_upload, nb * 4, cudaMemcpyHostToDevice, s);
 		if (!payload.empty())
-			cudaMemcpyAsync(payload_d, h_upload + nb, payload.size() * 4, cudaMemcpyHostToDevice, s);
+		{
+			const uint32_t *src = payload.data();
+			if (!waits)
+			{
+				memcpy(h_upload + nb, payload.data(), payload.size() * 4);
+				src = h_upload + nb;
+			}
+			cudaMemcpyAsync(payload_d, src, payload.size() * 4, cudaMemcpyHostToDevice, s);
+		}
 		DecodeInput in = {};
 		in.offsets = offsets_d;
 		in.payload = payload_d;
@@ -1578,11 +1631,23 @@ pyrowave_result pyrowave_encoder_encode_cpu_synchronous(pyrowave_encoder encoder
 		{
 			int w, h;
 			plane_dims(chroma, g.width, g.height, p, w, h);
-			cudaMemcpy2DAsync(encoder->in_planes[p], encoder->in_pitch[p], buffers->data[p],
-			                  buffers->row_stride_in_bytes[p], size_t(w), size_t(h), cudaMemcpyHostToDevice, s);
+			const size_t stride = buffers->row_stride_in_bytes[p];
 			in.data[p] = encoder->in_planes[p];
-			in.pitch[p] = encoder->in_pitch[p];
 			in.xstride[p] = 1;
+			if (stride <= size_t(encoder->in_pitch[p]))
+			{
+				// One linear copy (row padding included) at the source's own pitch:
+				// a pitched copy of narrow rows runs far below the link's bandwidth.
+				cudaMemcpyAsync(encoder->in_planes[p], buffers->data[p], stride * size_t(h - 1) + size_t(w),
+				                cudaMemcpyHostToDevice, s);
+				in.pitch[p] = int32_t(stride);
+			}
+			else
+			{
+				cudaMemcpy2DAsync(encoder->in_planes[p], encoder->in_pitch[p], buffers->data[p], stride, size_t(w),
+				                  size_t(h), cudaMemcpyHostToDevice, s);
+				in.pitch[p] = encoder->in_pitch[p];
+			}
 		}
 	}
 	r = encoder->enqueue(in, rate_control, s);
@@ -1772,20 +1837,29 @@ pyrowave_result pyrowave_decoder_decode_cpu_buffer_synchronous(pyrowave_decoder 
 		return r;
 	cudaStream_t s = decoder->device->stream;
 	PlaneOutput out = {};
+	bool linear[3];
 	for (int p = 0; p < 3; p++)
 	{
+		int w, h;
+		plane_dims(chroma, g.width, g.height, p, w, h);
+		// Unpadded host rows: decode at that pitch and copy back in one piece
+		// (a pitched copy of narrow rows runs far below the link's bandwidth).
+		linear[p] = buffers->row_stride_in_bytes[p] == size_t(w);
 		out.data[p] = decoder->out_planes[p];
-		out.pitch[p] = decoder->out_pitch[p];
+		out.pitch[p] = linear[p] ? int32_t(w) : decoder->out_pitch[p];
 	}
-	r = decoder->decode_parsed(out, s);
+	r = decoder->decode_parsed(out, s, true);
 	if (r != PYROWAVE_SUCCESS)
 		return r;
 	for (int p = 0; p < 3; p++)
 	{
 		int w, h;
 		plane_dims(chroma, g.width, g.height, p, w, h);
-		cudaMemcpy2DAsync(buffers->data[p], buffers->row_stride_in_bytes[p], decoder->out_planes[p],
-		                  decoder->out_pitch[p], size_t(w), size_t(h), cudaMemcpyDeviceToHost, s);
+		if (linear[p])
+			cudaMemcpyAsync(buffers->data[p], decoder->out_planes[p], size_t(w) * size_t(h), cudaMemcpyDeviceToHost, s);
+		else
+			cudaMemcpy2DAsync(buffers->data[p], buffers->row_stride_in_bytes[p], decoder->out_planes[p],
+			                  decoder->out_pitch[p], size_t(w), size_t(h), cudaMemcpyDeviceToHost, s);
 	}
 	if (cudaStreamSynchronize(s) != cudaSuccess)
 		return PYROWAVE_ERROR_GENERIC;
