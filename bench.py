@@ -682,9 +682,10 @@ def run_e2e(args, cfg, frames, dev):
         capi.check(enc.L.pyrowave_encoder_packetize(enc.h, packets, boundary, capi.ctypes.byref(got),
                                                     capi.ctypes.c_void_p(bitstream.ctypes.data), budget), "packetize")
         total = 0
+        base = bitstream.ctypes.data
         for k in range(got.value):
             off, sz = packets[k].offset, packets[k].size
-            capi.check(dec.push_packet(bitstream[off:off + sz]), "push_packet")
+            capi.check(dec.push_packet_ptr(base + off, sz), "push_packet")
             total += sz
         code, _ = dec.decode_cpu(out)
         capi.check(code, "decode_cpu_buffer_synchronous")

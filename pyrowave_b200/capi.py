@@ -441,6 +441,10 @@ class Decoder:
             return self.L.pyrowave_decoder_push_packet(self.h, None, 0)
         return self.L.pyrowave_decoder_push_packet(self.h, _ptr(buf), buf.size)
 
+    def push_packet_ptr(self, ptr: int, size: int) -> int:
+        """pyrowave_decoder_push_packet on `size` bytes at host address `ptr` (no copy in Python)."""
+        return self.L.pyrowave_decoder_push_packet(self.h, c_void_p(ptr), size)
+
     def is_ready(self, allow_partial: bool = False) -> bool:
         return bool(self.L.pyrowave_decoder_decode_is_ready(self.h, allow_partial))
 

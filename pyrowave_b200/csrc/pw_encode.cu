@@ -712,11 +712,11 @@ __global__ void __launch_bounds__(256 * S) quant_blocks_batch_kernel(const Batch
 }
 
 // ---------------------------------------------------------------------------
-// Block-wide (1024 threads) exclusive scan; returns the exclusive prefix and
-// the block total.
-template <typename T> __device__ __forceinline__ T block_exclusive_scan_1024(T v, T *warp_sums, T &total)
+// Block-wide exclusive scan (blockDim.x a multiple of 32, at most 1024);
+// returns the exclusive prefix and the block total.
+template <typename T> __device__ __forceinline__ T block_exclusive_scan(T v, T *warp_sums, T &total)
 {
-	const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+	const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
 	T x = v;
 #pragma unroll
 	for (int off = 1; off < 32; off *= 2)
@@ -730,7 +730,7 @@ template <typename T> __device__ __forceinline__ T block_exclusive_scan_1024(T v
 	__syncthreads();
 	if (warp == 0)
 	{
-		T s = warp_sums[lane];
+		T s = lane < nwarps ? warp_sums[lane] : T(0);
 #pragma unroll
 		for (int off = 1; off < 32; off *= 2)
 		{
@@ -742,7 +742,7 @@ template <typename T> __device__ __forceinline__ T block_exclusive_scan_1024(T v
 	}
 	__syncthreads();
 	const T base = warp == 0 ? T(0) : warp_sums[warp - 1];
-	total = warp_sums[31];
+	total = warp_sums[nwarps - 1];
 	__syncthreads();
 	return base + x - v;
 }
@@ -873,11 +873,12 @@ __device__ __forceinline__ void resolve_body(const ResolveParams &p, const Encod
 	__shared__ uint32_t s_cut;
 	__shared__ unsigned long long s_base;
 	RateControlState *rc = buf.rc;
-	const int t = threadIdx.x;
+	const int t = threadIdx.x, nthreads = blockDim.x;
 	const int nblocks = p.block_count_32x32;
-	const int per_slice = (nblocks + nslices - 1) / nslices;
-	const int s0 = min(slice * per_slice, nblocks), s1 = min(s0 + per_slice, nblocks);
-	const int per = (s1 - s0 + 1023) / 1024;
+	// Slice = one rate-control subdivision: only the slice of the x*
+	// subdivision depends on the cut.
+	const int s0 = min(slice * p.blocks_per_subdivision, nblocks), s1 = min(s0 + p.blocks_per_subdivision, nblocks);
+	const int per = (s1 - s0 + nthreads - 1) / nthreads;
 	const int b0 = min(s0 + t * per, s1), b1 = min(b0 + per, s1);
 	// Every quantiser has finished once the wait returns. The packer is released
 	// only then, because it reads their output before its own wait.
@@ -886,7 +887,17 @@ __device__ __forceinline__ void resolve_body(const ResolveParams &p, const Encod
 
 	RawRD own[kOwnBatch];
 	load_rows(buf, b0, b1, own);
-	const uint32_t a = __ldcg(&rc->histogram[2 * t]), b = __ldcg(&rc->histogram[2 * t + 1]);
+	// The histogram: kHistSize / nthreads consecutive slots per thread.
+	const int hper = kHistSize / nthreads, h0 = t * hper;
+	uint32_t hv[kHistSize / 256];
+	uint32_t hsum = 0;
+#pragma unroll
+	for (int i = 0; i < kHistSize / 256; i++)
+		if (i < hper)
+		{
+			hv[i] = __ldcg(&rc->histogram[h0 + i]);
+			hsum += hv[i];
+		}
 	const uint32_t consumed = __ldcg(&rc->consumed);
 	if (t == 0)
 	{
@@ -894,15 +905,20 @@ __device__ __forceinline__ void resolve_body(const ResolveParams &p, const Encod
 		s_cut = 0xffffffffu;
 	}
 	uint32_t total;
-	const uint32_t excl = block_exclusive_scan_1024(a + b, warp_sums, total);
-	scan[2 * t] = excl + a;
-	scan[2 * t + 1] = excl + a + b;
+	uint32_t run = block_exclusive_scan(hsum, warp_sums, total);
+#pragma unroll
+	for (int i = 0; i < kHistSize / 256; i++)
+		if (i < hper)
+		{
+			run += hv[i];
+			scan[h0 + i] = run;
+		}
 	__syncthreads();
 
 	const int64_t need = int64_t(consumed) - int64_t(p.target_words);
 	if (need > 0)
 	{
-		for (int x = 2 * t; x < 2 * t + 2; x++)
+		for (int x = h0; x < h0 + hper; x++)
 			if (int64_t(scan[x]) >= need && (x == 0 || int64_t(scan[x - 1]) < need))
 				s_xstar = x;
 	}
@@ -918,14 +934,14 @@ __device__ __forceinline__ void resolve_body(const ResolveParams &p, const Encod
 		const int64_t required = need - (xstar > 0 ? int64_t(scan[xstar - 1]) : 0);
 		const uint32_t bk = uint32_t(xstar >> 4);
 		const int c1 = min(end, s1);
-		const int cper = (c1 - start + 1023) / 1024;
+		const int cper = (c1 - start + nthreads - 1) / nthreads;
 		const int c0 = min(start + t * cper, c1), c0e = min(c0 + cper, c1);
 		RawRD r0[kOwnBatch];
 		load_rows(buf, c0, c0e, r0);
 		uint32_t local = 0;
 		for_rows(buf, c0, c0e, r0, [&](int, const RawRD &r) { local += op_saving_at_bucket(r, bk); });
 		uint32_t tot;
-		uint32_t ex = block_exclusive_scan_1024(local, warp_sums, tot);
+		uint32_t ex = block_exclusive_scan(local, warp_sums, tot);
 		bool found = false;
 		for_rows(buf, c0, c0e, r0, [&](int blk, const RawRD &r) {
 			const uint32_t sv = op_saving_at_bucket(r, bk);
@@ -951,7 +967,7 @@ __device__ __forceinline__ void resolve_body(const ResolveParams &p, const Encod
 		local += (uint64_t(w) << 32) | (uint64_t(w != 0 ? 1 : 0) << 1);
 	});
 	unsigned long long slice_sum;
-	const unsigned long long run_excl = block_exclusive_scan_1024(local, warp_sums64, slice_sum);
+	const unsigned long long run_excl = block_exclusive_scan(local, warp_sums64, slice_sum);
 	if (t == 0)
 		st_release_u64(&rc->slice_total[slice], slice_sum | 1ull);
 	unsigned long long pred = 0;
@@ -975,7 +991,7 @@ __device__ __forceinline__ void resolve_body(const ResolveParams &p, const Encod
 		pred = v & ~1ull;
 	}
 	unsigned long long base_total;
-	(void)block_exclusive_scan_1024(pred, warp_sums64, base_total);
+	(void)block_exclusive_scan(pred, warp_sums64, base_total);
 	if (t == 0)
 		s_base = base_total;
 	__syncthreads();
@@ -1005,13 +1021,13 @@ __device__ __forceinline__ void resolve_body(const ResolveParams &p, const Encod
 	}
 }
 
-__global__ void __launch_bounds__(1024) resolve_kernel(const ResolveParams p, const EncodeBuffers buf)
+__global__ void __launch_bounds__(kResolveThreads) resolve_kernel(const ResolveParams p, const EncodeBuffers buf)
 {
 	resolve_body(p, buf, int(blockIdx.x), int(gridDim.x));
 }
 
 // Batched form: one CTA per (frame, slice).
-__global__ void __launch_bounds__(1024) resolve_batch_kernel(const BatchFrame *frames, const BatchFrameIO *io,
+__global__ void __launch_bounds__(kResolveThreads) resolve_batch_kernel(const BatchFrame *frames, const BatchFrameIO *io,
                                                              const uint32_t *cta_map)
 {
 	__shared__ ResolveParams s_p;
@@ -1280,8 +1296,8 @@ void launch_quant_pretransformed(const BlockParams &p, const EncodeBuffers &buf,
 
 void launch_resolve(const ResolveParams &p, const EncodeBuffers &buf, cudaStream_t stream)
 {
-	const int slices = std::min((p.block_count_32x32 + 1023) / 1024, kMaxResolveSlices);
-	LaunchConfig lc(dim3(std::max(slices, 1)), dim3(1024), stream, true);
+	const int slices = resolve_slices(p.block_count_32x32, p.blocks_per_subdivision);
+	LaunchConfig lc(dim3(slices), dim3(kResolveThreads), stream, true);
 	cudaLaunchKernelEx(&lc.cfg, resolve_kernel, p, buf);
 }
 
@@ -1317,7 +1333,7 @@ void launch_quant_blocks_batch(const BatchFrame *frames, const uint32_t *cta_map
 void launch_resolve_batch(const BatchFrame *frames, const BatchFrameIO *io, const uint32_t *cta_map, int nctas,
                           cudaStream_t stream)
 {
-	LaunchConfig lc(dim3(nctas), dim3(1024), stream, true);
+	LaunchConfig lc(dim3(nctas), dim3(kResolveThreads), stream, true);
 	cudaLaunchKernelEx(&lc.cfg, resolve_batch_kernel, frames, io, cta_map);
 }
 

@@ -2462,7 +2462,7 @@ pyrowave_result pyrowave_cuda_batch_create(pyrowave_device device, const pyrowav
 		di.coef32 = eb.coef32;
 		di.coef16 = nullptr;
 		fr.block_count = g.block_count_32x32;
-		fr.slices = std::max(1, std::min((g.block_count_32x32 + 1023) / 1024, kMaxResolveSlices));
+		fr.slices = resolve_slices(g.block_count_32x32, g.blocks_per_subdivision);
 	}
 	b->io_d = b->alloc<BatchFrameIO>(count, ok);
 	for (int i = 0; i < 2 && ok; i++)

@@ -87,8 +87,15 @@ __host__ __device__ inline void unpack_job(uint32_t j, int &level, int &comp, in
 	by = int(j >> 20);
 }
 
-// The resolve kernel splits the blocks into at most this many slices, one CTA each.
+// The resolve kernel runs one kResolveThreads-thread CTA per rate-control
+// subdivision (at most 16 of them; room for kMaxResolveSlices totals).
 constexpr int kMaxResolveSlices = 128;
+constexpr int kResolveThreads = 256;
+inline int resolve_slices(int blocks, int blocks_per_subdivision)
+{
+	const int n = (blocks + blocks_per_subdivision - 1) / blocks_per_subdivision;
+	return n < 1 ? 1 : (n > kMaxResolveSlices ? kMaxResolveSlices : n);
+}
 
 // Rate-control scratch, one per encoder instance (device memory), cleared
 // before every frame.
