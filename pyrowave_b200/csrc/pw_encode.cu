@@ -875,9 +875,10 @@ __device__ __forceinline__ void resolve_body(const ResolveParams &p, const Encod
 	RateControlState *rc = buf.rc;
 	const int t = threadIdx.x, nthreads = blockDim.x;
 	const int nblocks = p.block_count_32x32;
-	// Slice = one rate-control subdivision: only the slice of the x*
-	// subdivision depends on the cut.
-	const int s0 = min(slice * p.blocks_per_subdivision, nblocks), s1 = min(s0 + p.blocks_per_subdivision, nblocks);
+	// Slices are rate-control subdivisions, or 1024-block parts of larger
+	// ones: only the slices of the x* subdivision depend on the cut.
+	const int slice_blocks = resolve_slice_blocks(nblocks, p.blocks_per_subdivision);
+	const int s0 = min(slice * slice_blocks, nblocks), s1 = min(s0 + slice_blocks, nblocks);
 	const int per = (s1 - s0 + nthreads - 1) / nthreads;
 	const int b0 = min(s0 + t * per, s1), b1 = min(b0 + per, s1);
 	// Every quantiser has finished once the wait returns. The packer is released
@@ -1021,13 +1022,14 @@ __device__ __forceinline__ void resolve_body(const ResolveParams &p, const Encod
 	}
 }
 
-__global__ void __launch_bounds__(kResolveThreads) resolve_kernel(const ResolveParams p, const EncodeBuffers buf)
+template <int kThreads>
+__global__ void __launch_bounds__(kThreads) resolve_kernel(const ResolveParams p, const EncodeBuffers buf)
 {
 	resolve_body(p, buf, int(blockIdx.x), int(gridDim.x));
 }
 
 // Batched form: one CTA per (frame, slice).
-__global__ void __launch_bounds__(kResolveThreads) resolve_batch_kernel(const BatchFrame *frames, const BatchFrameIO *io,
+__global__ void __launch_bounds__(kResolveBatchThreads) resolve_batch_kernel(const BatchFrame *frames, const BatchFrameIO *io,
                                                              const uint32_t *cta_map)
 {
 	__shared__ ResolveParams s_p;
@@ -1297,8 +1299,22 @@ void launch_quant_pretransformed(const BlockParams &p, const EncodeBuffers &buf,
 void launch_resolve(const ResolveParams &p, const EncodeBuffers &buf, cudaStream_t stream)
 {
 	const int slices = resolve_slices(p.block_count_32x32, p.blocks_per_subdivision);
-	LaunchConfig lc(dim3(slices), dim3(kResolveThreads), stream, true);
-	cudaLaunchKernelEx(&lc.cfg, resolve_kernel, p, buf);
+	// One thread per block of a slice, 256 to 1024 per CTA.
+	if (p.blocks_per_subdivision >= 1024)
+	{
+		LaunchConfig lc(dim3(slices), dim3(1024), stream, true);
+		cudaLaunchKernelEx(&lc.cfg, resolve_kernel<1024>, p, buf);
+	}
+	else if (p.blocks_per_subdivision >= 512)
+	{
+		LaunchConfig lc(dim3(slices), dim3(512), stream, true);
+		cudaLaunchKernelEx(&lc.cfg, resolve_kernel<512>, p, buf);
+	}
+	else
+	{
+		LaunchConfig lc(dim3(slices), dim3(256), stream, true);
+		cudaLaunchKernelEx(&lc.cfg, resolve_kernel<256>, p, buf);
+	}
 }
 
 void launch_pack(const BlockParams &p, const EncodeBuffers &buf, cudaStream_t stream)
@@ -1333,7 +1349,7 @@ void launch_quant_blocks_batch(const BatchFrame *frames, const uint32_t *cta_map
 void launch_resolve_batch(const BatchFrame *frames, const BatchFrameIO *io, const uint32_t *cta_map, int nctas,
                           cudaStream_t stream)
 {
-	LaunchConfig lc(dim3(nctas), dim3(kResolveThreads), stream, true);
+	LaunchConfig lc(dim3(nctas), dim3(kResolveBatchThreads), stream, true);
 	cudaLaunchKernelEx(&lc.cfg, resolve_batch_kernel, frames, io, cta_map);
 }
 

@@ -87,14 +87,24 @@ __host__ __device__ inline void unpack_job(uint32_t j, int &level, int &comp, in
 	by = int(j >> 20);
 }
 
-// The resolve kernel runs one kResolveThreads-thread CTA per rate-control
-// subdivision (at most 16 of them; room for kMaxResolveSlices totals).
+// The resolve kernel runs one CTA per slice of blocks: a rate-control
+// subdivision, or a 1024-block part of a larger one (subdivisions hold a power
+// of two of blocks), one thread per block of the slice between 256 and 1024;
+// the batched form always uses 1024.
 constexpr int kMaxResolveSlices = 128;
-constexpr int kResolveThreads = 256;
+constexpr int kResolveBatchThreads = 1024;
+__host__ __device__ inline int resolve_slice_blocks(int blocks, int blocks_per_subdivision)
+{
+	int per = 1024; // a power of two, at least blocks / kMaxResolveSlices
+	while (per * kMaxResolveSlices < blocks)
+		per *= 2;
+	return blocks_per_subdivision < per ? blocks_per_subdivision : per;
+}
 inline int resolve_slices(int blocks, int blocks_per_subdivision)
 {
-	const int n = (blocks + blocks_per_subdivision - 1) / blocks_per_subdivision;
-	return n < 1 ? 1 : (n > kMaxResolveSlices ? kMaxResolveSlices : n);
+	const int per = resolve_slice_blocks(blocks, blocks_per_subdivision);
+	const int n = (blocks + per - 1) / per;
+	return n < 1 ? 1 : n;
 }
 
 // Rate-control scratch, one per encoder instance (device memory), cleared
