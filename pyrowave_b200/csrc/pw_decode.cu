@@ -292,12 +292,20 @@ __global__ void __launch_bounds__(128) dequant_batch_kernel(const BatchFrame *fr
 
 constexpr int kBandTile = 36; // 32 band samples + 2 on each side
 constexpr int kBandTilePitch = 37;
+// Band tiles are stored as rows of 40 samples from 4 before the tile (16-byte
+// aligned in the band, so an interior tile is one TMA box per band): band
+// sample j of the tile (0 = 2 before it) is at column j + kBandCol0.
+constexpr int kBandRow = 40;
+constexpr int kBandCol0 = 2;
+constexpr uint32_t kBandBoxBytes = kBandTile * kBandRow * 4;
+constexpr uint32_t kTmaMaxPolls = 1u << 20; // bounded wait for a tile load
 
 struct IdwtShared
 {
 	int yl[kBandTile], yh[kBandTile], xl[kBandTile], xh[kBandTile];
-	float band[4][kBandTile][kBandTilePitch];
+	alignas(128) float band[4][kBandTile][kBandRow];
 	float v[2][64][kBandTilePitch]; // after vertical lifting: [horizontal low/high][output row][band column]
+	uint64_t tile_bar;             // completion of the TMA tile loads
 };
 
 // One inverse level for a 64x64 output tile (32x32 band tile) of one component.
@@ -336,15 +344,45 @@ __device__ __forceinline__ void idwt_body(const LevelParams &p, const DecodeInpu
 	const bool f16 = L.fp16 != 0;
 	const int64_t o0 = p.band[comp][0].offset, o1 = p.band[comp][1].offset, o2 = p.band[comp][2].offset,
 	              o3 = p.band[comp][3].offset;
+	// Interior tiles read every band sample at its own position: rows of 40
+	// samples from 4 before the tile (16-byte aligned). Interior FP32 tiles of a
+	// decoder with tensor maps take one TMA box per band (barrier and maps made
+	// ready before the dependency wait); other interior tiles load 10 vectors per
+	// row, all in flight at once. Edge tiles use the mirrored index tables.
+	const int bx0 = tx * 32 - 2, by0 = ty * 32 - 2;
+	const bool interior = bx0 - 2 >= 0 && by0 >= 0 && bx0 + 38 <= nx && by0 + kBandTile <= ny;
+	const CUtensorMap *tmaps = in.tmaps ? in.tmaps + (level * kComponents + comp) * 4 : nullptr;
+	const bool use_tma = kThreads == 256 && interior && tmaps && !f16 && !L.stage16;
+	if (use_tma && threadIdx.x == 0)
+	{
+		mbarrier_init(&sh.tile_bar, 1);
+#pragma unroll
+		for (int b = 0; b < 4; b++)
+			prefetch_tensor_map(tmaps + b);
+	}
 	__syncthreads();
 	pdl_wait();
 
-	// Interior tiles read every band sample at its own position: rows of 40
-	// samples from 4 before the tile (16-byte aligned), 10 vectors per row, all
-	// loads in flight at once. Edge tiles use the mirrored index tables.
-	const int bx0 = tx * 32 - 2, by0 = ty * 32 - 2;
-	const bool interior = bx0 - 2 >= 0 && by0 >= 0 && bx0 + 38 <= nx && by0 + kBandTile <= ny;
-	if (interior)
+	if (use_tma)
+	{
+		if (threadIdx.x == 0)
+		{
+			mbarrier_expect_tx(&sh.tile_bar, 4 * kBandBoxBytes);
+#pragma unroll
+			for (int b = 0; b < 4; b++)
+				tma_load_2d(&sh.band[b][0][0], tmaps + b, bx0 - kBandCol0, by0, &sh.tile_bar);
+		}
+		if (!mbarrier_wait(&sh.tile_bar, 0, kTmaMaxPolls))
+		{
+			// Give up on this tile: record it, and keep the CTA alive (its shared
+			// memory is the copy's destination) for one more bounded wait.
+			if (threadIdx.x == 0 && in.error)
+				atomicOr(in.error, kDecodeErrorTileWait);
+			(void)mbarrier_wait(&sh.tile_bar, 0, kTmaMaxPolls);
+			return;
+		}
+	}
+	else if (interior)
 	{
 		constexpr int kVecPerRow = 10;
 		constexpr int kVecs = 4 * kBandTile * kVecPerRow; // 1440
@@ -383,20 +421,15 @@ __device__ __forceinline__ void idwt_body(const LevelParams &p, const DecodeInpu
 			const int b = k / (kBandTile * kVecPerRow);
 			const int r = k - b * kBandTile * kVecPerRow;
 			const int i = r / kVecPerRow, j = r - i * kVecPerRow;
-			float vals[4] = {v[u].x, v[u].y, v[u].z, v[u].w};
+			float4 f = v[u];
 			if (L.stage16)
 			{
-#pragma unroll
-				for (int e = 0; e < 4; e++)
-					vals[e] = round_to_half(vals[e]);
+				f.x = round_to_half(f.x);
+				f.y = round_to_half(f.y);
+				f.z = round_to_half(f.z);
+				f.w = round_to_half(f.w);
 			}
-#pragma unroll
-			for (int e = 0; e < 4; e++)
-			{
-				const int col = 4 * j + e - 2;
-				if (col >= 0 && col < kBandTile)
-					sh.band[b][i][col] = vals[e];
-			}
+			*reinterpret_cast<float4 *>(&sh.band[b][i][4 * j]) = f;
 		}
 	}
 	else
@@ -429,7 +462,7 @@ __device__ __forceinline__ void idwt_body(const LevelParams &p, const DecodeInpu
 					const int b = k / (kBandTile * kBandTile);
 					const int r = k - b * kBandTile * kBandTile;
 					const int i = r / kBandTile, j = r - i * kBandTile;
-					sh.band[b][i][j] = L.stage16 ? round_to_half(v[u]) : v[u];
+					sh.band[b][i][j + kBandCol0] = L.stage16 ? round_to_half(v[u]) : v[u];
 				}
 			}
 		}
@@ -449,7 +482,8 @@ __device__ __forceinline__ void idwt_body(const LevelParams &p, const DecodeInpu
 		{
 			const int q = seg * kOut + jj;
 			const int i = q >> 1;
-			e[jj] = (q & 1) ? __fmul_rn(sh.band[b_high][i][col], kInvK) : __fmul_rn(sh.band[b_low][i][col], kK);
+			e[jj] = (q & 1) ? __fmul_rn(sh.band[b_high][i][col + kBandCol0], kInvK)
+			                : __fmul_rn(sh.band[b_low][i][col + kBandCol0], kK);
 		}
 		lift_inverse(e);
 #pragma unroll
@@ -563,15 +597,21 @@ __device__ __forceinline__ void idwt_body(const LevelParams &p, const DecodeInpu
 	}
 }
 
-template <int kThreads>
-__global__ void __launch_bounds__(kThreads) idwt_kernel(const LevelParams p, const DecodeInput in, const PlaneOutput out)
+// 256-thread CTAs: three per SM (80 registers) for levels of about one wave,
+// four per SM (64 registers) for levels of several waves, each measured the
+// faster of the two there; 1024-thread CTAs keep 32 registers.
+template <int kThreads> constexpr int kIdwtMinBlocks = kThreads >= 1024 ? 2 : 3;
+constexpr int kIdwtManyTiles = 2 * 148 * 4; // levels with at least this many tiles use four CTAs per SM
+
+template <int kThreads, int kMinBlocks = kIdwtMinBlocks<kThreads>>
+__global__ void __launch_bounds__(kThreads, kMinBlocks) idwt_kernel(const LevelParams p, const DecodeInput in, const PlaneOutput out)
 {
 	idwt_body<kThreads>(p, in, out, int(blockIdx.x), int(blockIdx.y));
 }
 
 // Batched form: one CTA per (frame, component, tile) of this level.
 template <int kThreads>
-__global__ void __launch_bounds__(kThreads) idwt_batch_kernel(const BatchFrame *frames, const BatchFrameIO *io,
+__global__ void __launch_bounds__(kThreads, kIdwtMinBlocks<kThreads>) idwt_batch_kernel(const BatchFrame *frames, const BatchFrameIO *io,
                                                               const uint32_t *cta_map, const int level)
 {
 	__shared__ LevelParams s_p;
@@ -632,10 +672,15 @@ void launch_idwt_level(const LevelParams &p, const DecodeInput &in, const PlaneO
 		LaunchConfig lc(grid, dim3(1024), stream, programmatic);
 		cudaLaunchKernelEx(&lc.cfg, idwt_kernel<1024>, p, in, out);
 	}
-	else
+	else if (int(grid.x * grid.y) < kIdwtManyTiles)
 	{
 		LaunchConfig lc(grid, dim3(256), stream, programmatic);
 		cudaLaunchKernelEx(&lc.cfg, idwt_kernel<256>, p, in, out);
+	}
+	else
+	{
+		LaunchConfig lc(grid, dim3(256), stream, programmatic);
+		cudaLaunchKernelEx(&lc.cfg, idwt_kernel<256, 4>, p, in, out);
 	}
 }
 

@@ -110,6 +110,55 @@ __device__ __forceinline__ float round_to_half(float v) { return __half2float(__
 __device__ __forceinline__ void pdl_trigger() { asm volatile("griddepcontrol.launch_dependents;" ::: "memory"); }
 __device__ __forceinline__ void pdl_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
 
+// Tensor-memory-access (TMA) tile loads into shared memory, completed on an
+// mbarrier. Plain CTA-local loads: no cluster multicast.
+__device__ __forceinline__ uint32_t smem_addr(const void *p) { return uint32_t(__cvta_generic_to_shared(p)); }
+
+__device__ __forceinline__ void mbarrier_init(uint64_t *bar, uint32_t count)
+{
+	asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_addr(bar)), "r"(count) : "memory");
+	asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+}
+
+__device__ __forceinline__ void mbarrier_expect_tx(uint64_t *bar, uint32_t bytes)
+{
+	asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_addr(bar)), "r"(bytes) : "memory");
+}
+
+// Waits for phase `parity` of the barrier to complete, at most `max_polls`
+// polls (each a bounded hardware wait); false when it gave up.
+__device__ __forceinline__ bool mbarrier_wait(uint64_t *bar, uint32_t parity, uint32_t max_polls)
+{
+	const uint32_t a = smem_addr(bar);
+	for (uint32_t i = 0; i < max_polls; i++)
+	{
+		uint32_t done;
+		asm volatile("{\n\t.reg .pred p;\n\t"
+		             "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+		             "selp.u32 %0, 1, 0, p;\n\t}"
+		             : "=r"(done)
+		             : "r"(a), "r"(parity)
+		             : "memory");
+		if (done)
+			return true;
+	}
+	return false;
+}
+
+__device__ __forceinline__ void prefetch_tensor_map(const void *tensor_map)
+{
+	asm volatile("prefetch.tensormap [%0];" ::"l"(tensor_map) : "memory");
+}
+
+// 2D tile load: the box of the tensor map at (x, y) (x * element size a
+// multiple of 16 bytes) into shared memory at dst (16-byte aligned).
+__device__ __forceinline__ void tma_load_2d(void *dst, const void *tensor_map, int x, int y, uint64_t *bar)
+{
+	asm volatile("cp.async.bulk.tensor.2d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3}], [%4];"
+	             ::"r"(smem_addr(dst)), "l"(tensor_map), "r"(x), "r"(y), "r"(smem_addr(bar))
+	             : "memory");
+}
+
 // GPU-scope acquire load / release store of a 64-bit word (flags between CTAs).
 __device__ __forceinline__ unsigned long long ld_acquire_u64(const unsigned long long *p)
 {

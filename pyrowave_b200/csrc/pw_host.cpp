@@ -12,6 +12,8 @@
 //   decode sequence         pyrowave_decoder.cpp:796-830
 #include "pw_internal.h"
 
+#include <cudaTypedefs.h>
+
 #include "pyrowave.h"
 #include "pyrowave_cuda.h"
 
@@ -896,6 +898,50 @@ struct PinnedWords
 	}
 };
 
+// TMA maps of every FP32 band of a frame, [level][component][band]: 2D
+// (pitch x rows samples), boxes of the inverse transform's band tiles (40 x 36
+// samples). Only levels large enough to have interior tiles are used by the
+// kernels. False when the driver offers no tensor-map encoder.
+bool build_band_tensor_maps(const Geometry &g, const LevelParams (&lp)[kLevels], float *coef32,
+                            std::vector<CUtensorMap> &maps)
+{
+	static PFN_cuTensorMapEncodeTiled_v12000 encode = [] {
+		void *fn = nullptr;
+		cudaDriverEntryPointQueryResult q;
+		if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &fn, cudaEnableDefault, &q) != cudaSuccess ||
+		    q != cudaDriverEntryPointSuccess)
+			fn = nullptr;
+		return reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(fn);
+	}();
+	if (!encode || !coef32)
+		return false;
+	maps.assign(size_t(kLevels) * kComponents * 4, CUtensorMap{});
+	for (int level = 0; level < kLevels; level++)
+	{
+		const LevelDesc &L = lp[level].L;
+		if (L.fp16 || L.pitch < 40 || L.rows < 36)
+			continue;
+		for (int comp = 0; comp < kComponents; comp++)
+		{
+			if (level == 0 && comp != 0 && !g.chroma444)
+				continue;
+			for (int band = 0; band < 4; band++)
+			{
+				const cuuint64_t dims[2] = {cuuint64_t(L.pitch), cuuint64_t(L.rows)};
+				const cuuint64_t strides[1] = {cuuint64_t(L.pitch) * 4};
+				const cuuint32_t box[2] = {40, 36};
+				const cuuint32_t elem[2] = {1, 1};
+				if (encode(&maps[(size_t(level) * kComponents + comp) * 4 + band], CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 2,
+				           coef32 + lp[level].band[comp][band].offset, dims, strides, box, elem,
+				           CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+				           CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) != CUDA_SUCCESS)
+					return false;
+			}
+		}
+	}
+	return true;
+}
+
 struct pyrowave_decoder_opaque
 {
 	pyrowave_device device = nullptr;
@@ -921,6 +967,8 @@ struct pyrowave_decoder_opaque
 	KernelNode node_dequant;
 	KernelNode node_idwt_full[kLevels], node_idwt_only[kLevels];
 
+	CUtensorMap *tmaps_d = nullptr; // TMA maps of the FP32 bands (inverse transform tile loads)
+	uint32_t *error_d = nullptr;     // kDecodeError* bits
 	// Device-side packet assembly (pw_packets.cu): per-packet tables, grown on demand.
 	uint32_t *pk_tables = nullptr;
 	uint8_t *pk_state = nullptr;
@@ -1062,6 +1110,10 @@ struct pyrowave_decoder_opaque
 		dev_free(pk_summaries);
 		dev_free(pk_items);
 		dev_free(pk_first);
+		dev_free(tmaps_d);
+		dev_free(error_d);
+		tmaps_d = nullptr;
+		error_d = nullptr;
 		dev_free(pk_status);
 		dev_free(pk_counter);
 		host_free(pk_status_h);
@@ -1113,6 +1165,21 @@ struct pyrowave_decoder_opaque
 			return PYROWAVE_ERROR_OUT_OF_DEVICE_MEMORY;
 		}
 		cudaMemcpy(jobs_d, jobs.data(), jobs.size() * 4, cudaMemcpyHostToDevice);
+		error_d = dev_alloc<uint32_t>(1, ok);
+		if (error_d)
+			cudaMemset(error_d, 0, sizeof(uint32_t));
+		std::vector<CUtensorMap> maps;
+		if (build_band_tensor_maps(g, lp, coef32, maps))
+		{
+			tmaps_d = dev_alloc<CUtensorMap>(maps.size(), ok);
+			if (tmaps_d)
+				cudaMemcpy(tmaps_d, maps.data(), maps.size() * sizeof(CUtensorMap), cudaMemcpyHostToDevice);
+		}
+		if (!ok)
+		{
+			release();
+			return PYROWAVE_ERROR_OUT_OF_DEVICE_MEMORY;
+		}
 		if (offsets.size() != size_t(g.block_count_32x32))
 		{
 			offsets.assign(size_t(g.block_count_32x32), UINT32_MAX);
@@ -1165,8 +1232,11 @@ struct pyrowave_decoder_opaque
 
 	// Dequantise + inverse transform (pyrowave_decoder.cpp:796-830).
 	// Dequantise + inverse transform (pyrowave_decoder.cpp:796-830), as one graph launch.
-	bool run(const DecodeInput &in, const PlaneOutput &out, cudaStream_t s, bool dequant)
+	bool run(const DecodeInput &in_args, const PlaneOutput &out, cudaStream_t s, bool dequant)
 	{
+		DecodeInput in = in_args;
+		in.tmaps = tmaps_d;
+		in.error = error_d;
 		timing.collect(device);
 		timing.prepare(device);
 		CapturedGraph &graph = dequant ? graph_full : graph_idwt;
@@ -2456,6 +2526,8 @@ pyrowave_result pyrowave_cuda_batch_create(pyrowave_device device, const pyrowav
 		DecodeInput &di = fr.di;
 		di.offsets = nullptr;
 		di.keys = nullptr;
+		di.tmaps = nullptr;
+		di.error = nullptr;
 		di.block_meta = eb.block_meta;
 		di.payload = eb.stream ? eb.stream + 2 : nullptr;
 		di.payload_words = b->capacity_words[f] - 2;

@@ -15,6 +15,7 @@
 #include <cstddef>
 #include <cstdint>
 
+#include <cuda.h>
 #include <cuda_fp16.h>
 #include <cuda_runtime.h>
 
@@ -124,6 +125,9 @@ struct RateControlState
 	unsigned long long slice_total[kMaxResolveSlices];
 };
 
+// Error bits of a decoder's error word.
+constexpr uint32_t kDecodeErrorTileWait = 1u; // an inverse-transform tile load did not complete in time
+
 // Error bits of RateControlState::error.
 constexpr uint32_t kErrorStreamCapacity = 1u; // the coded frame does not fit the stream buffer
 constexpr uint32_t kErrorWordCount = 2u;      // a packed block's size differs from the rate-control estimate
@@ -164,6 +168,8 @@ struct DecodeInput
 	const uint32_t *offsets;    // per 32x32 block, UINT32_MAX = missing (reference format), or nullptr
 	const uint32_t *block_meta; // alternatively {offset, num_words} pairs; num_words == 0 = missing
 	const unsigned long long *keys; // alternatively packet-assembly keys: word offset in the low 30 bits, ~0 = missing
+	const CUtensorMap *tmaps;   // per (level, component, band) TMA maps of FP32 bands, or nullptr
+	uint32_t *error;            // kDecodeError* bits, or nullptr
 	const uint32_t *payload;    // concatenated block words
 	uint32_t payload_words;
 	const uint32_t *jobs;
