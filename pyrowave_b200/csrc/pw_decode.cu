@@ -610,8 +610,8 @@ __global__ void __launch_bounds__(kThreads, kMinBlocks) idwt_kernel(const LevelP
 }
 
 // Batched form: one CTA per (frame, component, tile) of this level.
-template <int kThreads>
-__global__ void __launch_bounds__(kThreads, kIdwtMinBlocks<kThreads>) idwt_batch_kernel(const BatchFrame *frames, const BatchFrameIO *io,
+template <int kThreads, int kMinBlocks = kIdwtMinBlocks<kThreads>>
+__global__ void __launch_bounds__(kThreads, kMinBlocks) idwt_batch_kernel(const BatchFrame *frames, const BatchFrameIO *io,
                                                               const uint32_t *cta_map, const int level)
 {
 	__shared__ LevelParams s_p;
@@ -705,10 +705,15 @@ void launch_idwt_batch(const BatchFrame *frames, const BatchFrameIO *io, const u
 		LaunchConfig lc(dim3(nctas), dim3(1024), stream, programmatic);
 		cudaLaunchKernelEx(&lc.cfg, idwt_batch_kernel<1024>, frames, io, cta_map, level);
 	}
-	else
+	else if (nctas < kIdwtManyTiles)
 	{
 		LaunchConfig lc(dim3(nctas), dim3(256), stream, programmatic);
 		cudaLaunchKernelEx(&lc.cfg, idwt_batch_kernel<256>, frames, io, cta_map, level);
+	}
+	else
+	{
+		LaunchConfig lc(dim3(nctas), dim3(256), stream, programmatic);
+		cudaLaunchKernelEx(&lc.cfg, idwt_batch_kernel<256, 4>, frames, io, cta_map, level);
 	}
 }
 

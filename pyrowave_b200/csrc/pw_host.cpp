@@ -2528,6 +2528,13 @@ pyrowave_result pyrowave_cuda_batch_create(pyrowave_device device, const pyrowav
 		di.keys = nullptr;
 		di.tmaps = nullptr;
 		di.error = nullptr;
+		std::vector<CUtensorMap> maps;
+		if (ok && build_band_tensor_maps(g, fr.lp, eb.coef32, maps))
+		{
+			CUtensorMap *m = b->alloc<CUtensorMap>(maps.size(), ok);
+			if (m && cudaMemcpy(m, maps.data(), maps.size() * sizeof(CUtensorMap), cudaMemcpyHostToDevice) == cudaSuccess)
+				di.tmaps = m;
+		}
 		di.block_meta = eb.block_meta;
 		di.payload = eb.stream ? eb.stream + 2 : nullptr;
 		di.payload_words = b->capacity_words[f] - 2;
