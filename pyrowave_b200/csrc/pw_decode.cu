@@ -314,7 +314,7 @@ struct IdwtShared
 // outputs, shortening every serial phase.
 template <int kThreads>
 __device__ __forceinline__ void idwt_body(const LevelParams &p, const DecodeInput &in, const PlaneOutput &out,
-                                          const int tile, const int comp_index)
+                                          const LevelBandMaps *maps, const int tile, const int comp_index)
 {
 	constexpr int kOut = kThreads >= 1024 ? 8 : 16; // outputs per lifting item
 	constexpr int kSegs = 64 / kOut;
@@ -351,7 +351,7 @@ __device__ __forceinline__ void idwt_body(const LevelParams &p, const DecodeInpu
 	// row, all in flight at once. Edge tiles use the mirrored index tables.
 	const int bx0 = tx * 32 - 2, by0 = ty * 32 - 2;
 	const bool interior = bx0 - 2 >= 0 && by0 >= 0 && bx0 + 38 <= nx && by0 + kBandTile <= ny;
-	const CUtensorMap *tmaps = in.tmaps ? in.tmaps + (level * kComponents + comp) * 4 : nullptr;
+	const CUtensorMap *tmaps = (maps && ((maps->valid >> comp) & 1u)) ? &maps->band[comp][0] : nullptr;
 	const bool use_tma = kThreads == 256 && interior && tmaps && !f16 && !L.stage16;
 	if (use_tma && threadIdx.x == 0)
 	{
@@ -372,7 +372,8 @@ __device__ __forceinline__ void idwt_body(const LevelParams &p, const DecodeInpu
 			for (int b = 0; b < 4; b++)
 				tma_load_2d(&sh.band[b][0][0], tmaps + b, bx0 - kBandCol0, by0, &sh.tile_bar);
 		}
-		if (!mbarrier_wait(&sh.tile_bar, 0, kTmaMaxPolls))
+		const bool done = mbarrier_wait(&sh.tile_bar, 0, kTmaMaxPolls);
+		if (__syncthreads_or(!done))
 		{
 			// Give up on this tile: record it, and keep the CTA alive (its shared
 			// memory is the copy's destination) for one more bounded wait.
@@ -604,9 +605,10 @@ template <int kThreads> constexpr int kIdwtMinBlocks = kThreads >= 1024 ? 2 : 3;
 constexpr int kIdwtManyTiles = 2 * 148 * 4; // levels with at least this many tiles use four CTAs per SM
 
 template <int kThreads, int kMinBlocks = kIdwtMinBlocks<kThreads>>
-__global__ void __launch_bounds__(kThreads, kMinBlocks) idwt_kernel(const LevelParams p, const DecodeInput in, const PlaneOutput out)
+__global__ void __launch_bounds__(kThreads, kMinBlocks) idwt_kernel(const LevelParams p, const DecodeInput in, const PlaneOutput out,
+                                                                     const __grid_constant__ LevelBandMaps maps)
 {
-	idwt_body<kThreads>(p, in, out, int(blockIdx.x), int(blockIdx.y));
+	idwt_body<kThreads>(p, in, out, &maps, int(blockIdx.x), int(blockIdx.y));
 }
 
 // Batched form: one CTA per (frame, component, tile) of this level.
@@ -624,7 +626,7 @@ __global__ void __launch_bounds__(kThreads, kMinBlocks) idwt_batch_kernel(const 
 	load_params(s_out, io[f].out);
 	__syncthreads();
 	const int ntiles = s_p.L.tiles_x * s_p.L.tiles_y;
-	idwt_body<kThreads>(s_p, s_in, s_out, local % ntiles, local / ntiles);
+	idwt_body<kThreads>(s_p, s_in, s_out, nullptr, local % ntiles, local / ntiles);
 }
 
 // Canonical pyramid (all transmitted bands, band-major, unpadded) <-> padded storage.
@@ -663,24 +665,27 @@ void launch_dequant(const BlockParams &p, const DecodeInput &in, int first, int 
 	cudaLaunchKernelEx(&lc.cfg, dequant_kernel, p, in, first);
 }
 
-void launch_idwt_level(const LevelParams &p, const DecodeInput &in, const PlaneOutput &out, bool programmatic,
-                       cudaStream_t stream)
+void launch_idwt_level(const LevelParams &p, const DecodeInput &in, const PlaneOutput &out, const LevelBandMaps *maps,
+                       bool programmatic, cudaStream_t stream)
 {
 	const dim3 grid(p.L.tiles_x * p.L.tiles_y, (p.level == 0 && !p.chroma444) ? 1 : 3);
+	LevelBandMaps m = {};
+	if (maps)
+		m = *maps;
 	if (int(grid.x * grid.y) < kSmallLevelTiles)
 	{
 		LaunchConfig lc(grid, dim3(1024), stream, programmatic);
-		cudaLaunchKernelEx(&lc.cfg, idwt_kernel<1024>, p, in, out);
+		cudaLaunchKernelEx(&lc.cfg, idwt_kernel<1024>, p, in, out, m);
 	}
 	else if (int(grid.x * grid.y) < kIdwtManyTiles)
 	{
 		LaunchConfig lc(grid, dim3(256), stream, programmatic);
-		cudaLaunchKernelEx(&lc.cfg, idwt_kernel<256>, p, in, out);
+		cudaLaunchKernelEx(&lc.cfg, idwt_kernel<256>, p, in, out, m);
 	}
 	else
 	{
 		LaunchConfig lc(grid, dim3(256), stream, programmatic);
-		cudaLaunchKernelEx(&lc.cfg, idwt_kernel<256, 4>, p, in, out);
+		cudaLaunchKernelEx(&lc.cfg, idwt_kernel<256, 4>, p, in, out, m);
 	}
 }
 
@@ -807,6 +812,6 @@ extern "C" pyrowave_result pyrowave_cuda_decode_blocks_static(int width, int hei
 	const cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
 	launch_dequant(make_block_params(g), in, 0, g.block_count_32x32, false, s);
 	for (int level = kLevels - 1; level >= 0; level--)
-		launch_idwt_level(make_level_params(g, level), in, out, true, s);
+		launch_idwt_level(make_level_params(g, level), in, out, nullptr, true, s);
 	return cudaGetLastError() == cudaSuccess ? PYROWAVE_SUCCESS : PYROWAVE_ERROR_GENERIC;
 }

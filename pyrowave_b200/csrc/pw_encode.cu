@@ -16,7 +16,12 @@ namespace pw
 namespace
 {
 constexpr int kTileIn = 72;  // 64 input samples + 4-sample apron on each side
-constexpr int kInPitch = 73; // odd pitch: conflict-free column walks
+// Rows of 76 samples: 16-byte aligned, so the horizontal lifting reads its
+// window as float4 vectors without bank conflicts (76 = 4 * 19, 19 odd), and an
+// interior tile of a level above 0 is one TMA box (72 rows of 76 samples).
+constexpr int kInPitch = 76;
+constexpr uint32_t kInBoxBytes = kTileIn * kInPitch * 4;
+constexpr uint32_t kTmaMaxPolls = 1u << 20; // bounded wait for a tile load
 constexpr int kHPitch = 65;
 constexpr int kBandPitch = 33;
 
@@ -300,10 +305,11 @@ struct DwtShared
 {
 	int xidx[kTileIn];
 	int yidx[kTileIn];
-	float in[kTileIn][kInPitch]; // input tile, later the four 32x32 band tiles
+	alignas(128) float in[kTileIn][kInPitch]; // input tile, later the four 32x32 band tiles
 	float h[kTileIn][kHPitch];   // after horizontal lifting: low in 0..31, high in 32..63
 	QuantGroupShared q[4];
 	float unorm[256];            // unorm8_centered(u) for every byte value
+	uint64_t tile_bar;           // completion of the TMA tile load
 };
 
 __device__ __forceinline__ float unorm8_centered(uint32_t u)
@@ -337,7 +343,8 @@ constexpr int kLargeLevelThreads = 256;
 // those at this level. Run by every thread of a kThreads-thread CTA.
 template <int kThreads>
 __device__ __forceinline__ void dwt_forward_body(const LevelParams &p, const PlaneInput &in, const EncodeBuffers &buf,
-                                                 const int fused, const int tile, const int comp_index)
+                                                 const LevelInputMaps *maps, const int fused, const int tile,
+                                                 const int comp_index)
 {
 	using Split = DwtSplit<kThreads>;
 	__shared__ DwtShared sh;
@@ -375,15 +382,22 @@ __device__ __forceinline__ void dwt_forward_body(const LevelParams &p, const Pla
 			const float f = unorm8_centered(uint32_t(u));
 			sh.unorm[u] = L.stage16 ? round_to_half(f) : f;
 		}
-	__syncthreads();
-	pdl_wait();
-
 	// Tile load. A tile whose 72x72 window lies inside the source maps every
-	// sample to itself: load whole rows with vector loads, all in flight at
-	// once. Edge tiles go through the mirrored index tables in batches of
-	// independent loads.
+	// sample to itself: an FP32 level above 0 with a tensor map is one TMA box
+	// (barrier and map made ready before the dependency wait); otherwise whole
+	// rows are read with vector loads, all in flight at once. Edge tiles go
+	// through the mirrored index tables in batches of independent loads.
 	const int x0 = tx * 64 - 4, y0 = ty * 64 - 4;
 	const bool interior = x0 >= 0 && y0 >= 0 && x0 + kTileIn <= res_w && y0 + kTileIn <= res_h;
+	const CUtensorMap *tmap = (maps && ((maps->valid >> comp) & 1u)) ? &maps->comp[comp] : nullptr;
+	const bool use_tma = !from_plane && interior && tmap && !p.P.fp16;
+	if (use_tma && threadIdx.x == 0)
+	{
+		mbarrier_init(&sh.tile_bar, 1);
+		prefetch_tensor_map(tmap);
+	}
+	__syncthreads();
+	pdl_wait();
 	constexpr int kVecPerRow = kTileIn / 4;     // 18 vectors of 4 samples
 	constexpr int kVecs = kVecPerRow * kTileIn; // 1296
 	constexpr int kVecIters = (kVecs + kThreads - 1) / kThreads;
@@ -441,6 +455,24 @@ __device__ __forceinline__ void dwt_forward_body(const LevelParams &p, const Pla
 			}
 		}
 	}
+	else if (use_tma)
+	{
+		if (threadIdx.x == 0)
+		{
+			mbarrier_expect_tx(&sh.tile_bar, kInBoxBytes);
+			tma_load_2d(&sh.in[0][0], tmap, x0, y0, &sh.tile_bar);
+		}
+		const bool done = mbarrier_wait(&sh.tile_bar, 0, kTmaMaxPolls);
+		if (__syncthreads_or(!done))
+		{
+			// Give up on this tile: record it, and keep the CTA alive (its shared
+			// memory is the copy's destination) for one more bounded wait.
+			if (threadIdx.x == 0)
+				atomicOr(&buf.rc->error, kErrorTileWait);
+			(void)mbarrier_wait(&sh.tile_bar, 0, kTmaMaxPolls);
+			return;
+		}
+	}
 	else
 	{
 		const LevelDesc &P = p.P;
@@ -474,10 +506,7 @@ __device__ __forceinline__ void dwt_forward_body(const LevelParams &p, const Pla
 				if (k < kVecs)
 				{
 					const int i = k / kVecPerRow, j = k - i * kVecPerRow;
-					sh.in[i][4 * j + 0] = v[u].x;
-					sh.in[i][4 * j + 1] = v[u].y;
-					sh.in[i][4 * j + 2] = v[u].z;
-					sh.in[i][4 * j + 3] = v[u].w;
+					*reinterpret_cast<float4 *>(&sh.in[i][4 * j]) = v[u];
 				}
 			}
 		}
@@ -517,8 +546,14 @@ __device__ __forceinline__ void dwt_forward_body(const LevelParams &p, const Pla
 		const int row = item % kTileIn, seg = item / kTileIn;
 		float e[kWin];
 #pragma unroll
-		for (int j = 0; j < kWin; j++)
-			e[j] = sh.in[row][seg * 2 * kSegPairs + j];
+		for (int j = 0; j < kWin; j += 4)
+		{
+			const float4 q = *reinterpret_cast<const float4 *>(&sh.in[row][seg * 2 * kSegPairs + j]);
+			e[j] = q.x;
+			e[j + 1] = q.y;
+			e[j + 2] = q.z;
+			e[j + 3] = q.w;
+		}
 		lift_forward(e);
 #pragma unroll
 		for (int k = 0; k < kSegPairs; k++)
@@ -610,9 +645,10 @@ __device__ __forceinline__ void dwt_forward_body(const LevelParams &p, const Pla
 
 template <int kThreads>
 __global__ void __launch_bounds__(kThreads, DwtSplit<kThreads>::kMinBlocks)
-    dwt_forward_kernel(const LevelParams p, const PlaneInput in, const EncodeBuffers buf, const int fused)
+    dwt_forward_kernel(const LevelParams p, const PlaneInput in, const EncodeBuffers buf, const int fused,
+                       const __grid_constant__ LevelInputMaps maps)
 {
-	dwt_forward_body<kThreads>(p, in, buf, fused, int(blockIdx.x), int(blockIdx.y));
+	dwt_forward_body<kThreads>(p, in, buf, &maps, fused, int(blockIdx.x), int(blockIdx.y));
 }
 
 // Batched form: one CTA per (frame, component, tile) of this level.
@@ -631,7 +667,7 @@ __global__ void __launch_bounds__(kThreads, DwtSplit<kThreads>::kMinBlocks)
 	load_params(s_buf, frames[f].eb);
 	__syncthreads();
 	const int ntiles = s_p.L.tiles_x * s_p.L.tiles_y;
-	dwt_forward_body<kThreads>(s_p, s_in, s_buf, fused, local % ntiles, local / ntiles);
+	dwt_forward_body<kThreads>(s_p, s_in, s_buf, nullptr, fused, local % ntiles, local / ntiles);
 }
 
 // Quantiser over a pyramid already in storage (the reference's
@@ -1272,20 +1308,23 @@ LaunchConfig::LaunchConfig(dim3 grid, dim3 block, cudaStream_t stream, bool prog
 	cfg.numAttrs = programmatic ? 1 : 0;
 }
 
-void launch_dwt_forward_level(const LevelParams &p, const PlaneInput &in, const EncodeBuffers &buf, bool fused_quant,
-                              bool programmatic, cudaStream_t stream)
+void launch_dwt_forward_level(const LevelParams &p, const PlaneInput &in, const EncodeBuffers &buf,
+                              const LevelInputMaps *maps, bool fused_quant, bool programmatic, cudaStream_t stream)
 {
 	const dim3 grid(p.L.tiles_x * p.L.tiles_y, (p.level == 0 && !p.chroma444) ? 1 : 3);
 	const int f = fused_quant ? 1 : 0;
+	LevelInputMaps m = {};
+	if (maps)
+		m = *maps;
 	if (int(grid.x * grid.y) < kSmallLevelTiles)
 	{
 		LaunchConfig lc(grid, dim3(1024), stream, programmatic);
-		cudaLaunchKernelEx(&lc.cfg, dwt_forward_kernel<1024>, p, in, buf, f);
+		cudaLaunchKernelEx(&lc.cfg, dwt_forward_kernel<1024>, p, in, buf, f, m);
 	}
 	else
 	{
 		LaunchConfig lc(grid, dim3(kLargeLevelThreads), stream, programmatic);
-		cudaLaunchKernelEx(&lc.cfg, dwt_forward_kernel<kLargeLevelThreads>, p, in, buf, f);
+		cudaLaunchKernelEx(&lc.cfg, dwt_forward_kernel<kLargeLevelThreads>, p, in, buf, f, m);
 	}
 }
 

@@ -568,6 +568,90 @@ struct CapturedGraph
 };
 } // namespace
 
+PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder()
+{
+	static PFN_cuTensorMapEncodeTiled_v12000 encode = [] {
+		void *fn = nullptr;
+		cudaDriverEntryPointQueryResult q;
+		if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &fn, cudaEnableDefault, &q) != cudaSuccess ||
+		    q != cudaDriverEntryPointSuccess)
+			fn = nullptr;
+		return reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(fn);
+	}();
+	return encode;
+}
+
+// 2D FP32 tensor map over a padded band array (pitch x rows samples).
+bool encode_band_map(CUtensorMap &map, float *base, const LevelDesc &L, uint32_t box_w, uint32_t box_h)
+{
+	const auto encode = tensor_map_encoder();
+	const cuuint64_t dims[2] = {cuuint64_t(L.pitch), cuuint64_t(L.rows)};
+	const cuuint64_t strides[1] = {cuuint64_t(L.pitch) * 4};
+	const cuuint32_t box[2] = {box_w, box_h};
+	const cuuint32_t elem[2] = {1, 1};
+	return encode && encode(&map, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 2, base, dims, strides, box, elem,
+	                        CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+	                        CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+}
+
+// TMA maps of the forward transform's LL inputs, per level and component: the
+// LL of level - 1 as 72 rows of 76 samples, for FP32 levels large enough to
+// have interior tiles (valid bit set). All invalid when the driver offers no
+// tensor-map encoder; false when encoding a map fails.
+bool build_ll_tensor_maps(const Geometry &g, const LevelParams (&lp)[kLevels], float *coef32,
+                          LevelInputMaps (&maps)[kLevels])
+{
+	for (auto &m : maps)
+		m = LevelInputMaps{};
+	if (!tensor_map_encoder() || !coef32)
+		return true;
+	for (int level = 1; level < kLevels; level++)
+	{
+		const LevelDesc &P = lp[level].P;
+		if (P.fp16 || P.pitch < 76 || P.rows < 72)
+			continue;
+		for (int comp = 0; comp < kComponents; comp++)
+		{
+			if (level == 1 && comp != 0 && !g.chroma444)
+				continue; // 4:2:0 chroma enters at level 1 from its plane
+			if (!encode_band_map(maps[level].comp[comp], coef32 + lp[level].prev_ll[comp], P, 76, 72))
+				return false;
+			maps[level].valid |= 1u << comp;
+		}
+	}
+	return true;
+}
+
+// TMA maps of every FP32 band of a frame, per level, component and band: boxes
+// of the inverse transform's band tiles (40 x 36 samples), for levels large
+// enough to have interior tiles (valid bit set). All invalid when the driver
+// offers no tensor-map encoder; false when encoding a map fails.
+bool build_band_tensor_maps(const Geometry &g, const LevelParams (&lp)[kLevels], float *coef32,
+                            LevelBandMaps (&maps)[kLevels])
+{
+	for (auto &m : maps)
+		m = LevelBandMaps{};
+	if (!tensor_map_encoder() || !coef32)
+		return true;
+	for (int level = 0; level < kLevels; level++)
+	{
+		const LevelDesc &L = lp[level].L;
+		if (L.fp16 || L.pitch < 40 || L.rows < 36)
+			continue;
+		for (int comp = 0; comp < kComponents; comp++)
+		{
+			if (level == 0 && comp != 0 && !g.chroma444)
+				continue;
+			for (int band = 0; band < 4; band++)
+				if (!encode_band_map(maps[level].band[comp][band], coef32 + lp[level].band[comp][band].offset, L, 40,
+				                     36))
+					return false;
+			maps[level].valid |= 1u << comp;
+		}
+	}
+	return true;
+}
+
 struct pyrowave_encoder_opaque
 {
 	pyrowave_device device = nullptr;
@@ -590,6 +674,7 @@ struct pyrowave_encoder_opaque
 	uint32_t *stream_buf = nullptr;
 	uint32_t stream_capacity = 0;
 	uint32_t *jobs_d = nullptr;
+	LevelInputMaps in_maps[kLevels] = {}; // TMA maps of the forward transform's LL inputs
 	uint8_t *in_planes[3] = {};
 	int in_pitch[3] = {};
 
@@ -702,6 +787,9 @@ struct pyrowave_encoder_opaque
 			return PYROWAVE_ERROR_OUT_OF_DEVICE_MEMORY;
 		}
 		cudaMemcpy(jobs_d, jobs.data(), jobs.size() * 4, cudaMemcpyHostToDevice);
+		if (!build_ll_tensor_maps(g, lp, coef32, in_maps))
+			for (auto &m : in_maps)
+				m = LevelInputMaps{}; // plain loads throughout
 		allocated = true;
 		return PYROWAVE_SUCCESS;
 	}
@@ -785,7 +873,7 @@ struct pyrowave_encoder_opaque
 			const bool pdl = !device->stage_timing; // event nodes between kernels break programmatic edges
 			for (int level = 0; level < kLevels; level++)
 			{
-				launch_dwt_forward_level(lp[level], in, b, level < small_level, pdl && level > 0, s);
+				launch_dwt_forward_level(lp[level], in, b, &in_maps[level], level < small_level, pdl && level > 0, s);
 				ok = ok && last_captured_node(s, node_dwt[level]);
 				timing.mark(device, s, dwt_tags[level]);
 			}
@@ -815,7 +903,7 @@ struct pyrowave_encoder_opaque
 			for (int level = 0; level < kLevels; level++)
 			{
 				int fused = level < small_level ? 1 : 0;
-				ok = ok && set_kernel_args(graph.exec, node_dwt[level], lp[level], pin, b, fused);
+				ok = ok && set_kernel_args(graph.exec, node_dwt[level], lp[level], pin, b, fused, in_maps[level]);
 			}
 			ok = ok && set_kernel_args(graph.exec, node_resolve, rp, b);
 			if (!ok)
@@ -898,50 +986,6 @@ struct PinnedWords
 	}
 };
 
-// TMA maps of every FP32 band of a frame, [level][component][band]: 2D
-// (pitch x rows samples), boxes of the inverse transform's band tiles (40 x 36
-// samples). Only levels large enough to have interior tiles are used by the
-// kernels. False when the driver offers no tensor-map encoder.
-bool build_band_tensor_maps(const Geometry &g, const LevelParams (&lp)[kLevels], float *coef32,
-                            std::vector<CUtensorMap> &maps)
-{
-	static PFN_cuTensorMapEncodeTiled_v12000 encode = [] {
-		void *fn = nullptr;
-		cudaDriverEntryPointQueryResult q;
-		if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &fn, cudaEnableDefault, &q) != cudaSuccess ||
-		    q != cudaDriverEntryPointSuccess)
-			fn = nullptr;
-		return reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(fn);
-	}();
-	if (!encode || !coef32)
-		return false;
-	maps.assign(size_t(kLevels) * kComponents * 4, CUtensorMap{});
-	for (int level = 0; level < kLevels; level++)
-	{
-		const LevelDesc &L = lp[level].L;
-		if (L.fp16 || L.pitch < 40 || L.rows < 36)
-			continue;
-		for (int comp = 0; comp < kComponents; comp++)
-		{
-			if (level == 0 && comp != 0 && !g.chroma444)
-				continue;
-			for (int band = 0; band < 4; band++)
-			{
-				const cuuint64_t dims[2] = {cuuint64_t(L.pitch), cuuint64_t(L.rows)};
-				const cuuint64_t strides[1] = {cuuint64_t(L.pitch) * 4};
-				const cuuint32_t box[2] = {40, 36};
-				const cuuint32_t elem[2] = {1, 1};
-				if (encode(&maps[(size_t(level) * kComponents + comp) * 4 + band], CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 2,
-				           coef32 + lp[level].band[comp][band].offset, dims, strides, box, elem,
-				           CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
-				           CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) != CUDA_SUCCESS)
-					return false;
-			}
-		}
-	}
-	return true;
-}
-
 struct pyrowave_decoder_opaque
 {
 	pyrowave_device device = nullptr;
@@ -967,7 +1011,7 @@ struct pyrowave_decoder_opaque
 	KernelNode node_dequant;
 	KernelNode node_idwt_full[kLevels], node_idwt_only[kLevels];
 
-	CUtensorMap *tmaps_d = nullptr; // TMA maps of the FP32 bands (inverse transform tile loads)
+	LevelBandMaps band_maps[kLevels] = {}; // TMA maps of the FP32 bands (inverse transform tile loads)
 	uint32_t *error_d = nullptr;     // kDecodeError* bits
 	// Device-side packet assembly (pw_packets.cu): per-packet tables, grown on demand.
 	uint32_t *pk_tables = nullptr;
@@ -1110,9 +1154,7 @@ struct pyrowave_decoder_opaque
 		dev_free(pk_summaries);
 		dev_free(pk_items);
 		dev_free(pk_first);
-		dev_free(tmaps_d);
 		dev_free(error_d);
-		tmaps_d = nullptr;
 		error_d = nullptr;
 		dev_free(pk_status);
 		dev_free(pk_counter);
@@ -1168,13 +1210,9 @@ struct pyrowave_decoder_opaque
 		error_d = dev_alloc<uint32_t>(1, ok);
 		if (error_d)
 			cudaMemset(error_d, 0, sizeof(uint32_t));
-		std::vector<CUtensorMap> maps;
-		if (build_band_tensor_maps(g, lp, coef32, maps))
-		{
-			tmaps_d = dev_alloc<CUtensorMap>(maps.size(), ok);
-			if (tmaps_d)
-				cudaMemcpy(tmaps_d, maps.data(), maps.size() * sizeof(CUtensorMap), cudaMemcpyHostToDevice);
-		}
+		if (!build_band_tensor_maps(g, lp, coef32, band_maps))
+			for (auto &m : band_maps)
+				m = LevelBandMaps{}; // plain loads throughout
 		if (!ok)
 		{
 			release();
@@ -1235,7 +1273,6 @@ struct pyrowave_decoder_opaque
 	bool run(const DecodeInput &in_args, const PlaneOutput &out, cudaStream_t s, bool dequant)
 	{
 		DecodeInput in = in_args;
-		in.tmaps = tmaps_d;
 		in.error = error_d;
 		timing.collect(device);
 		timing.prepare(device);
@@ -1257,7 +1294,7 @@ struct pyrowave_decoder_opaque
 			static const char *const idwt_tags[kLevels] = {"idwt0", "idwt1", "idwt2", "idwt3", "idwt4"};
 			for (int level = kLevels - 1; level >= 0; level--)
 			{
-				launch_idwt_level(lp[level], in, out, pdl && (dequant || level < kLevels - 1), s);
+				launch_idwt_level(lp[level], in, out, &band_maps[level], pdl && (dequant || level < kLevels - 1), s);
 				ok = ok && last_captured_node(s, dequant ? node_idwt_full[level] : node_idwt_only[level]);
 				timing.mark(device, s, idwt_tags[level]);
 			}
@@ -1281,7 +1318,7 @@ struct pyrowave_decoder_opaque
 			}
 			for (int level = 0; level < kLevels; level++)
 				ok = ok && set_kernel_args(graph.exec, dequant ? node_idwt_full[level] : node_idwt_only[level], lp[level],
-				                           din, pout);
+				                           din, pout, band_maps[level]);
 			if (!ok)
 			{
 				graph.destroy();
@@ -2526,15 +2563,7 @@ pyrowave_result pyrowave_cuda_batch_create(pyrowave_device device, const pyrowav
 		DecodeInput &di = fr.di;
 		di.offsets = nullptr;
 		di.keys = nullptr;
-		di.tmaps = nullptr;
 		di.error = nullptr;
-		std::vector<CUtensorMap> maps;
-		if (ok && build_band_tensor_maps(g, fr.lp, eb.coef32, maps))
-		{
-			CUtensorMap *m = b->alloc<CUtensorMap>(maps.size(), ok);
-			if (m && cudaMemcpy(m, maps.data(), maps.size() * sizeof(CUtensorMap), cudaMemcpyHostToDevice) == cudaSuccess)
-				di.tmaps = m;
-		}
 		di.block_meta = eb.block_meta;
 		di.payload = eb.stream ? eb.stream + 2 : nullptr;
 		di.payload_words = b->capacity_words[f] - 2;

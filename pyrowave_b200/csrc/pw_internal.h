@@ -132,6 +132,7 @@ constexpr uint32_t kDecodeErrorTileWait = 1u; // an inverse-transform tile load 
 constexpr uint32_t kErrorStreamCapacity = 1u; // the coded frame does not fit the stream buffer
 constexpr uint32_t kErrorWordCount = 2u;      // a packed block's size differs from the rate-control estimate
 constexpr uint32_t kErrorSliceWait = 4u;      // a resolve slice gave up waiting for a preceding slice's total
+constexpr uint32_t kErrorTileWait = 8u;       // a forward-transform tile load did not complete in time
 
 // Buffers the encode kernels read and write.
 struct EncodeBuffers
@@ -148,6 +149,20 @@ struct EncodeBuffers
 	uint32_t *stream;       // packetized output: 2-word sequence header, then blocks
 	uint32_t stream_capacity_words;
 	const uint32_t *jobs;   // per 32x32: pack_job(...)
+};
+
+// TMA maps of one transform level, passed as kernel parameters (grid
+// constants): a map in global memory at an address that earlier held another
+// map can be served stale by the TMA unit's descriptor cache.
+struct alignas(64) LevelInputMaps // forward: the LL input (level - 1) per component
+{
+	CUtensorMap comp[kComponents];
+	uint32_t valid; // bit c: comp[c] is a map
+};
+struct alignas(64) LevelBandMaps // inverse: the four bands per component
+{
+	CUtensorMap band[kComponents][4];
+	uint32_t valid; // bit c: band[c][*] are maps
 };
 
 struct PlaneInput
@@ -168,7 +183,6 @@ struct DecodeInput
 	const uint32_t *offsets;    // per 32x32 block, UINT32_MAX = missing (reference format), or nullptr
 	const uint32_t *block_meta; // alternatively {offset, num_words} pairs; num_words == 0 = missing
 	const unsigned long long *keys; // alternatively packet-assembly keys: word offset in the low 30 bits, ~0 = missing
-	const CUtensorMap *tmaps;   // per (level, component, band) TMA maps of FP32 bands, or nullptr
 	uint32_t *error;            // kDecodeError* bits, or nullptr
 	const uint32_t *payload;    // concatenated block words
 	uint32_t payload_words;
@@ -284,7 +298,8 @@ constexpr int kMaxBatchFrames = 256;
 // launch across the whole GPU after the last level instead of inside the
 // transform of each level.
 constexpr int kSmallLevelTiles = 256;
-void launch_dwt_forward_level(const LevelParams &p, const PlaneInput &in, const EncodeBuffers &buf, bool fused_quant,
+void launch_dwt_forward_level(const LevelParams &p, const PlaneInput &in, const EncodeBuffers &buf,
+                              const LevelInputMaps *maps, bool fused_quant,
                               bool programmatic, cudaStream_t stream);
 // Quantise and analyse the first nblocks 32x32 blocks (block index order) from storage.
 void launch_quant_pretransformed(const BlockParams &p, const EncodeBuffers &buf, int nblocks, bool programmatic,
@@ -294,7 +309,8 @@ void launch_pack(const BlockParams &p, const EncodeBuffers &buf, cudaStream_t st
 // Dequantise blocks [first, first + count) (block index order).
 void launch_dequant(const BlockParams &p, const DecodeInput &in, int first, int count, bool programmatic,
                     cudaStream_t stream);
-void launch_idwt_level(const LevelParams &p, const DecodeInput &in, const PlaneOutput &out, bool programmatic,
+void launch_idwt_level(const LevelParams &p, const DecodeInput &in, const PlaneOutput &out, const LevelBandMaps *maps,
+                       bool programmatic,
                        cudaStream_t stream);
 void launch_pyramid_io(const BlockParams &p, float *canonical, float *coef32, __half *coef16, bool to_canonical,
                        cudaStream_t stream);

@@ -282,3 +282,36 @@ def test_4k_stability(device):
         code, out = dec.decode_cpu()
         assert code == capi.PYROWAVE_SUCCESS
         assert 40.0 < O.psnr(planes[0], out[0]) < 60.0
+
+
+def test_tensor_maps_follow_reused_addresses(device):
+    """Encoders and decoders created and destroyed in turn, with different
+    frame sizes, so the device addresses of their TMA tensor maps are reused
+    for maps of other buffers: every transform still reads its own buffers
+    (bit-exact pyramids and decoded planes)."""
+    import torch
+
+    shapes = [(1280, 720, False), (640, 480, True), (1920, 1080, False), (1280, 720, False), (960, 544, True)]
+    for k, (w, h, c444) in enumerate(shapes * 2):
+        chroma = capi.CHROMA_444 if c444 else capi.CHROMA_420
+        planes = synth.synth_frame(w, h, c444, 40 + k)
+        enc = capi.Encoder(device, w, h, chroma)
+        d = _to_dev(planes)
+        enc.encode_device([p.data_ptr() for p in d], [p.stride(0) for p in d], 60000)
+        pyr = torch.zeros(enc.layout().pyramid_size, dtype=torch.float32, device="cuda")
+        enc.read_wavelet(pyr.data_ptr())
+        torch.cuda.synchronize()
+        o = O.Oracle(w, h, c444)
+        ref = o.dwt(planes, O.MODE_F32)
+        err = _mismatch(f"dwt bits {w}x{h} #{k}", pyr.cpu().numpy().view(np.uint32), ref.view(np.uint32))
+        assert err is None, err
+        dec = capi.Decoder(device, w, h, chroma)
+        outs = [torch.zeros(pl.shape, dtype=torch.uint8, device="cuda") for pl in planes]
+        dec.decode_pyramid(pyr.data_ptr(), [t.data_ptr() for t in outs], [t.stride(0) for t in outs])
+        torch.cuda.synchronize()
+        want = o.idwt(ref, O.MODE_F32)
+        for i in range(3):
+            err = _mismatch(f"idwt plane {i} {w}x{h} #{k}", outs[i].cpu().numpy(), want[i])
+            assert err is None, err
+        enc.close()
+        dec.close()
