@@ -314,7 +314,7 @@ struct IdwtShared
 // outputs, shortening every serial phase.
 template <int kThreads>
 __device__ __forceinline__ void idwt_body(const LevelParams &p, const DecodeInput &in, const PlaneOutput &out,
-                                          const LevelBandMaps *maps, const int tile, const int comp_index)
+                                          const LevelTileMap *maps, const int tile, const int comp_index)
 {
 	constexpr int kOut = kThreads >= 1024 ? 8 : 16; // outputs per lifting item
 	constexpr int kSegs = 64 / kOut;
@@ -351,14 +351,11 @@ __device__ __forceinline__ void idwt_body(const LevelParams &p, const DecodeInpu
 	// row, all in flight at once. Edge tiles use the mirrored index tables.
 	const int bx0 = tx * 32 - 2, by0 = ty * 32 - 2;
 	const bool interior = bx0 - 2 >= 0 && by0 >= 0 && bx0 + 38 <= nx && by0 + kBandTile <= ny;
-	const CUtensorMap *tmaps = (maps && ((maps->valid >> comp) & 1u)) ? &maps->band[comp][0] : nullptr;
-	const bool use_tma = kThreads == 256 && interior && tmaps && !f16 && !L.stage16;
+	const bool use_tma = kThreads == 256 && interior && maps && ((maps->valid >> comp) & 1u) && !f16 && !L.stage16;
 	if (use_tma && threadIdx.x == 0)
 	{
 		mbarrier_init(&sh.tile_bar, 1);
-#pragma unroll
-		for (int b = 0; b < 4; b++)
-			prefetch_tensor_map(tmaps + b);
+		prefetch_tensor_map(&maps->map);
 	}
 	__syncthreads();
 	pdl_wait();
@@ -370,7 +367,7 @@ __device__ __forceinline__ void idwt_body(const LevelParams &p, const DecodeInpu
 			mbarrier_expect_tx(&sh.tile_bar, 4 * kBandBoxBytes);
 #pragma unroll
 			for (int b = 0; b < 4; b++)
-				tma_load_2d(&sh.band[b][0][0], tmaps + b, bx0 - kBandCol0, by0, &sh.tile_bar);
+				tma_load_2d(&sh.band[b][0][0], &maps->map, bx0 - kBandCol0, maps->row[comp][b] + by0, &sh.tile_bar);
 		}
 		const bool done = mbarrier_wait(&sh.tile_bar, 0, kTmaMaxPolls);
 		if (__syncthreads_or(!done))
@@ -606,7 +603,7 @@ constexpr int kIdwtManyTiles = 2 * 148 * 4; // levels with at least this many ti
 
 template <int kThreads, int kMinBlocks = kIdwtMinBlocks<kThreads>>
 __global__ void __launch_bounds__(kThreads, kMinBlocks) idwt_kernel(const LevelParams p, const DecodeInput in, const PlaneOutput out,
-                                                                     const __grid_constant__ LevelBandMaps maps)
+                                                                     const __grid_constant__ LevelTileMap maps)
 {
 	idwt_body<kThreads>(p, in, out, &maps, int(blockIdx.x), int(blockIdx.y));
 }
@@ -614,7 +611,8 @@ __global__ void __launch_bounds__(kThreads, kMinBlocks) idwt_kernel(const LevelP
 // Batched form: one CTA per (frame, component, tile) of this level.
 template <int kThreads, int kMinBlocks = kIdwtMinBlocks<kThreads>>
 __global__ void __launch_bounds__(kThreads, kMinBlocks) idwt_batch_kernel(const BatchFrame *frames, const BatchFrameIO *io,
-                                                              const uint32_t *cta_map, const int level)
+                                                              const uint32_t *cta_map, const int level,
+                                                              const __grid_constant__ BatchTileMaps maps)
 {
 	__shared__ LevelParams s_p;
 	__shared__ DecodeInput s_in;
@@ -626,7 +624,8 @@ __global__ void __launch_bounds__(kThreads, kMinBlocks) idwt_batch_kernel(const 
 	load_params(s_out, io[f].out);
 	__syncthreads();
 	const int ntiles = s_p.L.tiles_x * s_p.L.tiles_y;
-	idwt_body<kThreads>(s_p, s_in, s_out, nullptr, local % ntiles, local / ntiles);
+	idwt_body<kThreads>(s_p, s_in, s_out, f < kBatchTileMapFrames ? &maps.frame[f] : nullptr, local % ntiles,
+	                    local / ntiles);
 }
 
 // Canonical pyramid (all transmitted bands, band-major, unpadded) <-> padded storage.
@@ -665,11 +664,11 @@ void launch_dequant(const BlockParams &p, const DecodeInput &in, int first, int 
 	cudaLaunchKernelEx(&lc.cfg, dequant_kernel, p, in, first);
 }
 
-void launch_idwt_level(const LevelParams &p, const DecodeInput &in, const PlaneOutput &out, const LevelBandMaps *maps,
+void launch_idwt_level(const LevelParams &p, const DecodeInput &in, const PlaneOutput &out, const LevelTileMap *maps,
                        bool programmatic, cudaStream_t stream)
 {
 	const dim3 grid(p.L.tiles_x * p.L.tiles_y, (p.level == 0 && !p.chroma444) ? 1 : 3);
-	LevelBandMaps m = {};
+	LevelTileMap m = {};
 	if (maps)
 		m = *maps;
 	if (int(grid.x * grid.y) < kSmallLevelTiles)
@@ -703,22 +702,24 @@ void launch_dequant_batch(const BatchFrame *frames, const uint32_t *cta_map, int
 }
 
 void launch_idwt_batch(const BatchFrame *frames, const BatchFrameIO *io, const uint32_t *cta_map, int nctas, int level,
-                       bool large_ctas, bool programmatic, cudaStream_t stream)
+                       const BatchTileMaps *maps, bool large_ctas, bool programmatic, cudaStream_t stream)
 {
+	static const BatchTileMaps none = {};
+	const BatchTileMaps &m = maps ? *maps : none;
 	if (large_ctas)
 	{
 		LaunchConfig lc(dim3(nctas), dim3(1024), stream, programmatic);
-		cudaLaunchKernelEx(&lc.cfg, idwt_batch_kernel<1024>, frames, io, cta_map, level);
+		cudaLaunchKernelEx(&lc.cfg, idwt_batch_kernel<1024>, frames, io, cta_map, level, m);
 	}
 	else if (nctas < kIdwtManyTiles)
 	{
 		LaunchConfig lc(dim3(nctas), dim3(256), stream, programmatic);
-		cudaLaunchKernelEx(&lc.cfg, idwt_batch_kernel<256>, frames, io, cta_map, level);
+		cudaLaunchKernelEx(&lc.cfg, idwt_batch_kernel<256>, frames, io, cta_map, level, m);
 	}
 	else
 	{
 		LaunchConfig lc(dim3(nctas), dim3(256), stream, programmatic);
-		cudaLaunchKernelEx(&lc.cfg, idwt_batch_kernel<256, 4>, frames, io, cta_map, level);
+		cudaLaunchKernelEx(&lc.cfg, idwt_batch_kernel<256, 4>, frames, io, cta_map, level, m);
 	}
 }
 

@@ -343,7 +343,7 @@ constexpr int kLargeLevelThreads = 256;
 // those at this level. Run by every thread of a kThreads-thread CTA.
 template <int kThreads>
 __device__ __forceinline__ void dwt_forward_body(const LevelParams &p, const PlaneInput &in, const EncodeBuffers &buf,
-                                                 const LevelInputMaps *maps, const int fused, const int tile,
+                                                 const LevelTileMap *maps, const int fused, const int tile,
                                                  const int comp_index)
 {
 	using Split = DwtSplit<kThreads>;
@@ -389,8 +389,8 @@ __device__ __forceinline__ void dwt_forward_body(const LevelParams &p, const Pla
 	// through the mirrored index tables in batches of independent loads.
 	const int x0 = tx * 64 - 4, y0 = ty * 64 - 4;
 	const bool interior = x0 >= 0 && y0 >= 0 && x0 + kTileIn <= res_w && y0 + kTileIn <= res_h;
-	const CUtensorMap *tmap = (maps && ((maps->valid >> comp) & 1u)) ? &maps->comp[comp] : nullptr;
-	const bool use_tma = !from_plane && interior && tmap && !p.P.fp16;
+	const bool use_tma = !from_plane && interior && maps && ((maps->valid >> comp) & 1u) && !p.P.fp16;
+	const CUtensorMap *tmap = use_tma ? &maps->map : nullptr;
 	if (use_tma && threadIdx.x == 0)
 	{
 		mbarrier_init(&sh.tile_bar, 1);
@@ -460,7 +460,7 @@ __device__ __forceinline__ void dwt_forward_body(const LevelParams &p, const Pla
 		if (threadIdx.x == 0)
 		{
 			mbarrier_expect_tx(&sh.tile_bar, kInBoxBytes);
-			tma_load_2d(&sh.in[0][0], tmap, x0, y0, &sh.tile_bar);
+			tma_load_2d(&sh.in[0][0], tmap, x0, maps->row[comp][0] + y0, &sh.tile_bar);
 		}
 		const bool done = mbarrier_wait(&sh.tile_bar, 0, kTmaMaxPolls);
 		if (__syncthreads_or(!done))
@@ -646,7 +646,7 @@ __device__ __forceinline__ void dwt_forward_body(const LevelParams &p, const Pla
 template <int kThreads>
 __global__ void __launch_bounds__(kThreads, DwtSplit<kThreads>::kMinBlocks)
     dwt_forward_kernel(const LevelParams p, const PlaneInput in, const EncodeBuffers buf, const int fused,
-                       const __grid_constant__ LevelInputMaps maps)
+                       const __grid_constant__ LevelTileMap maps)
 {
 	dwt_forward_body<kThreads>(p, in, buf, &maps, fused, int(blockIdx.x), int(blockIdx.y));
 }
@@ -655,7 +655,7 @@ __global__ void __launch_bounds__(kThreads, DwtSplit<kThreads>::kMinBlocks)
 template <int kThreads>
 __global__ void __launch_bounds__(kThreads, DwtSplit<kThreads>::kMinBlocks)
     dwt_forward_batch_kernel(const BatchFrame *frames, const BatchFrameIO *io, const uint32_t *cta_map, const int level,
-                             const int fused)
+                             const int fused, const __grid_constant__ BatchTileMaps maps)
 {
 	__shared__ LevelParams s_p;
 	__shared__ PlaneInput s_in;
@@ -667,7 +667,8 @@ __global__ void __launch_bounds__(kThreads, DwtSplit<kThreads>::kMinBlocks)
 	load_params(s_buf, frames[f].eb);
 	__syncthreads();
 	const int ntiles = s_p.L.tiles_x * s_p.L.tiles_y;
-	dwt_forward_body<kThreads>(s_p, s_in, s_buf, nullptr, fused, local % ntiles, local / ntiles);
+	dwt_forward_body<kThreads>(s_p, s_in, s_buf, f < kBatchTileMapFrames ? &maps.frame[f] : nullptr, fused,
+	                           local % ntiles, local / ntiles);
 }
 
 // Quantiser over a pyramid already in storage (the reference's
@@ -1309,11 +1310,11 @@ LaunchConfig::LaunchConfig(dim3 grid, dim3 block, cudaStream_t stream, bool prog
 }
 
 void launch_dwt_forward_level(const LevelParams &p, const PlaneInput &in, const EncodeBuffers &buf,
-                              const LevelInputMaps *maps, bool fused_quant, bool programmatic, cudaStream_t stream)
+                              const LevelTileMap *maps, bool fused_quant, bool programmatic, cudaStream_t stream)
 {
 	const dim3 grid(p.L.tiles_x * p.L.tiles_y, (p.level == 0 && !p.chroma444) ? 1 : 3);
 	const int f = fused_quant ? 1 : 0;
-	LevelInputMaps m = {};
+	LevelTileMap m = {};
 	if (maps)
 		m = *maps;
 	if (int(grid.x * grid.y) < kSmallLevelTiles)
@@ -1363,18 +1364,21 @@ void launch_pack(const BlockParams &p, const EncodeBuffers &buf, cudaStream_t st
 }
 
 void launch_dwt_forward_batch(const BatchFrame *frames, const BatchFrameIO *io, const uint32_t *cta_map, int nctas,
-                              int level, bool fused_quant, bool large_ctas, bool programmatic, cudaStream_t stream)
+                              int level, const BatchTileMaps *maps, bool fused_quant, bool large_ctas,
+                              bool programmatic, cudaStream_t stream)
 {
 	const int f = fused_quant ? 1 : 0;
+	static const BatchTileMaps none = {};
+	const BatchTileMaps &m = maps ? *maps : none;
 	if (large_ctas)
 	{
 		LaunchConfig lc(dim3(nctas), dim3(1024), stream, programmatic);
-		cudaLaunchKernelEx(&lc.cfg, dwt_forward_batch_kernel<1024>, frames, io, cta_map, level, f);
+		cudaLaunchKernelEx(&lc.cfg, dwt_forward_batch_kernel<1024>, frames, io, cta_map, level, f, m);
 	}
 	else
 	{
 		LaunchConfig lc(dim3(nctas), dim3(kLargeLevelThreads), stream, programmatic);
-		cudaLaunchKernelEx(&lc.cfg, dwt_forward_batch_kernel<kLargeLevelThreads>, frames, io, cta_map, level, f);
+		cudaLaunchKernelEx(&lc.cfg, dwt_forward_batch_kernel<kLargeLevelThreads>, frames, io, cta_map, level, f, m);
 	}
 }
 

@@ -581,75 +581,78 @@ PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder()
 	return encode;
 }
 
-// 2D FP32 tensor map over a padded band array (pitch x rows samples).
-bool encode_band_map(CUtensorMap &map, float *base, const LevelDesc &L, uint32_t box_w, uint32_t box_h)
+// 2D FP32 tensor map over a frame's whole FP32 coefficient storage, viewed as
+// rows of `pitch` samples.
+bool encode_storage_map(CUtensorMap &map, float *coef32, int64_t storage_elems, int pitch, uint32_t box_w,
+                        uint32_t box_h)
 {
 	const auto encode = tensor_map_encoder();
-	const cuuint64_t dims[2] = {cuuint64_t(L.pitch), cuuint64_t(L.rows)};
-	const cuuint64_t strides[1] = {cuuint64_t(L.pitch) * 4};
+	const cuuint64_t dims[2] = {cuuint64_t(pitch), cuuint64_t(storage_elems / pitch)};
+	const cuuint64_t strides[1] = {cuuint64_t(pitch) * 4};
 	const cuuint32_t box[2] = {box_w, box_h};
 	const cuuint32_t elem[2] = {1, 1};
-	return encode && encode(&map, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 2, base, dims, strides, box, elem,
+	return encode && encode(&map, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 2, coef32, dims, strides, box, elem,
 	                        CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
 	                        CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
 }
 
-// TMA maps of the forward transform's LL inputs, per level and component: the
-// LL of level - 1 as 72 rows of 76 samples, for FP32 levels large enough to
-// have interior tiles (valid bit set). All invalid when the driver offers no
-// tensor-map encoder; false when encoding a map fails.
-bool build_ll_tensor_maps(const Geometry &g, const LevelParams (&lp)[kLevels], float *coef32,
-                          LevelInputMaps (&maps)[kLevels])
+// Per-level TMA maps of a frame. Forward level l reads its LL input (level
+// l - 1) as boxes of 72 rows x 76 samples; inverse level l reads its four bands
+// as boxes of 36 rows x 40 samples. A component's tiles use the map (valid bit)
+// when its level is FP32, large enough to have interior tiles, and each band it
+// reads starts on a row of the level's pitch; otherwise they use plain loads,
+// as do all tiles when the driver offers no tensor-map encoder.
+void build_tile_maps(const Geometry &g, const LevelParams (&lp)[kLevels], float *coef32, LevelTileMap (&fwd)[kLevels],
+                     LevelTileMap (&inv)[kLevels])
 {
-	for (auto &m : maps)
-		m = LevelInputMaps{};
-	if (!tensor_map_encoder() || !coef32)
-		return true;
-	for (int level = 1; level < kLevels; level++)
-	{
-		const LevelDesc &P = lp[level].P;
-		if (P.fp16 || P.pitch < 76 || P.rows < 72)
-			continue;
-		for (int comp = 0; comp < kComponents; comp++)
-		{
-			if (level == 1 && comp != 0 && !g.chroma444)
-				continue; // 4:2:0 chroma enters at level 1 from its plane
-			if (!encode_band_map(maps[level].comp[comp], coef32 + lp[level].prev_ll[comp], P, 76, 72))
-				return false;
-			maps[level].valid |= 1u << comp;
-		}
-	}
-	return true;
-}
-
-// TMA maps of every FP32 band of a frame, per level, component and band: boxes
-// of the inverse transform's band tiles (40 x 36 samples), for levels large
-// enough to have interior tiles (valid bit set). All invalid when the driver
-// offers no tensor-map encoder; false when encoding a map fails.
-bool build_band_tensor_maps(const Geometry &g, const LevelParams (&lp)[kLevels], float *coef32,
-                            LevelBandMaps (&maps)[kLevels])
-{
-	for (auto &m : maps)
-		m = LevelBandMaps{};
-	if (!tensor_map_encoder() || !coef32)
-		return true;
 	for (int level = 0; level < kLevels; level++)
 	{
-		const LevelDesc &L = lp[level].L;
-		if (L.fp16 || L.pitch < 40 || L.rows < 36)
-			continue;
-		for (int comp = 0; comp < kComponents; comp++)
+		fwd[level] = LevelTileMap{};
+		inv[level] = LevelTileMap{};
+	}
+	if (!tensor_map_encoder() || !coef32 || g.storage_elems32 <= 0)
+		return;
+	for (int level = 0; level < kLevels; level++)
+	{
+		const LevelParams &p = lp[level];
+		if (level > 0 && !p.P.fp16 && p.P.pitch >= 76 && p.P.rows >= 72)
 		{
-			if (level == 0 && comp != 0 && !g.chroma444)
-				continue;
-			for (int band = 0; band < 4; band++)
-				if (!encode_band_map(maps[level].band[comp][band], coef32 + lp[level].band[comp][band].offset, L, 40,
-				                     36))
-					return false;
-			maps[level].valid |= 1u << comp;
+			LevelTileMap &m = fwd[level];
+			uint32_t valid = 0;
+			for (int comp = 0; comp < kComponents; comp++)
+			{
+				if (level == 1 && comp != 0 && !g.chroma444)
+					continue; // 4:2:0 chroma enters at level 1 from its plane
+				if (p.prev_ll[comp] % p.P.pitch == 0)
+				{
+					m.row[comp][0] = int32_t(p.prev_ll[comp] / p.P.pitch);
+					valid |= 1u << comp;
+				}
+			}
+			if (valid && encode_storage_map(m.map, coef32, g.storage_elems32, p.P.pitch, 76, 72))
+				m.valid = valid;
+		}
+		if (!p.L.fp16 && p.L.pitch >= 40 && p.L.rows >= 36)
+		{
+			LevelTileMap &m = inv[level];
+			uint32_t valid = 0;
+			for (int comp = 0; comp < kComponents; comp++)
+			{
+				if (level == 0 && comp != 0 && !g.chroma444)
+					continue;
+				bool rows_ok = true;
+				for (int band = 0; band < 4; band++)
+				{
+					rows_ok = rows_ok && p.band[comp][band].offset % p.L.pitch == 0;
+					m.row[comp][band] = int32_t(p.band[comp][band].offset / p.L.pitch);
+				}
+				if (rows_ok)
+					valid |= 1u << comp;
+			}
+			if (valid && encode_storage_map(m.map, coef32, g.storage_elems32, p.L.pitch, 40, 36))
+				m.valid = valid;
 		}
 	}
-	return true;
 }
 
 struct pyrowave_encoder_opaque
@@ -674,7 +677,7 @@ struct pyrowave_encoder_opaque
 	uint32_t *stream_buf = nullptr;
 	uint32_t stream_capacity = 0;
 	uint32_t *jobs_d = nullptr;
-	LevelInputMaps in_maps[kLevels] = {}; // TMA maps of the forward transform's LL inputs
+	LevelTileMap in_maps[kLevels] = {}; // TMA maps of the forward transform's LL inputs
 	uint8_t *in_planes[3] = {};
 	int in_pitch[3] = {};
 
@@ -787,9 +790,10 @@ struct pyrowave_encoder_opaque
 			return PYROWAVE_ERROR_OUT_OF_DEVICE_MEMORY;
 		}
 		cudaMemcpy(jobs_d, jobs.data(), jobs.size() * 4, cudaMemcpyHostToDevice);
-		if (!build_ll_tensor_maps(g, lp, coef32, in_maps))
-			for (auto &m : in_maps)
-				m = LevelInputMaps{}; // plain loads throughout
+		{
+			LevelTileMap unused[kLevels];
+			build_tile_maps(g, lp, coef32, in_maps, unused);
+		}
 		allocated = true;
 		return PYROWAVE_SUCCESS;
 	}
@@ -1011,7 +1015,7 @@ struct pyrowave_decoder_opaque
 	KernelNode node_dequant;
 	KernelNode node_idwt_full[kLevels], node_idwt_only[kLevels];
 
-	LevelBandMaps band_maps[kLevels] = {}; // TMA maps of the FP32 bands (inverse transform tile loads)
+	LevelTileMap band_maps[kLevels] = {}; // TMA maps of the FP32 bands (inverse transform tile loads)
 	uint32_t *error_d = nullptr;     // kDecodeError* bits
 	// Device-side packet assembly (pw_packets.cu): per-packet tables, grown on demand.
 	uint32_t *pk_tables = nullptr;
@@ -1210,9 +1214,10 @@ struct pyrowave_decoder_opaque
 		error_d = dev_alloc<uint32_t>(1, ok);
 		if (error_d)
 			cudaMemset(error_d, 0, sizeof(uint32_t));
-		if (!build_band_tensor_maps(g, lp, coef32, band_maps))
-			for (auto &m : band_maps)
-				m = LevelBandMaps{}; // plain loads throughout
+		{
+			LevelTileMap unused[kLevels];
+			build_tile_maps(g, lp, coef32, unused, band_maps);
+		}
 		if (!ok)
 		{
 			release();
@@ -2301,6 +2306,9 @@ struct pyrowave_cuda_batch_opaque
 	int level_off[kLevels] = {}, level_n[kLevels] = {};
 	int quant_off = 0, quant_n = 0, resolve_off = 0, resolve_n = 0, block_off = 0, block_n = 0;
 	int level_tiles[kLevels] = {}; // all frames' tiles per level
+	// Per-level TMA maps of the first kBatchTileMapFrames frames (kernel parameters).
+	std::vector<BatchTileMaps> fwd_maps = std::vector<BatchTileMaps>(kLevels);
+	std::vector<BatchTileMaps> inv_maps = std::vector<BatchTileMaps>(kLevels);
 
 	BatchShape shape;
 	CapturedGraph graphs[2][2]; // [slot][with decode]
@@ -2418,7 +2426,7 @@ struct pyrowave_cuda_batch_opaque
 		                                  cudaMemcpyHostToDevice, s), "cudaMemcpyAsync");
 		ok = ok && cuda_ok(cudaMemsetAsync(rc_d, 0, sizeof(RateControlState) * size_t(count), s), "cudaMemsetAsync");
 		for (int level = 0; level < kLevels; level++)
-			launch_dwt_forward_batch(frames_d, io_d, maps_d + level_off[level], level_n[level], level,
+			launch_dwt_forward_batch(frames_d, io_d, maps_d + level_off[level], level_n[level], level, &fwd_maps[level],
 			                         level < shape.small_level, large(level), level > 0, s);
 		if (quant_n > 0)
 			launch_quant_blocks_batch(frames_d, maps_d + quant_off, quant_n, true, s);
@@ -2428,8 +2436,8 @@ struct pyrowave_cuda_batch_opaque
 		{
 			launch_dequant_batch(frames_d, maps_d + block_off, block_n, true, s);
 			for (int level = kLevels - 1; level >= 0; level--)
-				launch_idwt_batch(frames_d, io_d, maps_d + level_off[level], level_n[level], level, large(level), true,
-				                  s);
+				launch_idwt_batch(frames_d, io_d, maps_d + level_off[level], level_n[level], level, &inv_maps[level],
+				                  large(level), true, s);
 		}
 		ok = launches_ok("kernel launch") && ok;
 		ok = graph.end(s, 0) && ok;
@@ -2569,6 +2577,16 @@ pyrowave_result pyrowave_cuda_batch_create(pyrowave_device device, const pyrowav
 		di.payload_words = b->capacity_words[f] - 2;
 		di.coef32 = eb.coef32;
 		di.coef16 = nullptr;
+		if (ok && f < uint32_t(kBatchTileMapFrames))
+		{
+			LevelTileMap fwd[kLevels], inv[kLevels];
+			build_tile_maps(g, fr.lp, eb.coef32, fwd, inv);
+			for (int level = 0; level < kLevels; level++)
+			{
+				b->fwd_maps[level].frame[f] = fwd[level];
+				b->inv_maps[level].frame[f] = inv[level];
+			}
+		}
 		fr.block_count = g.block_count_32x32;
 		fr.slices = resolve_slices(g.block_count_32x32, g.blocks_per_subdivision);
 	}

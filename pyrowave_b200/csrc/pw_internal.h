@@ -151,18 +151,23 @@ struct EncodeBuffers
 	const uint32_t *jobs;   // per 32x32: pack_job(...)
 };
 
-// TMA maps of one transform level, passed as kernel parameters (grid
-// constants): a map in global memory at an address that earlier held another
-// map can be served stale by the TMA unit's descriptor cache.
-struct alignas(64) LevelInputMaps // forward: the LL input (level - 1) per component
+// TMA map of one transform level: the frame's FP32 coefficient storage viewed
+// as rows of one level's pitch, every band of that level starting on a row.
+// Passed as a kernel parameter (grid constant): a map in global memory at an
+// address that earlier held another map can be served stale by the TMA unit's
+// descriptor cache.
+struct alignas(64) LevelTileMap
 {
-	CUtensorMap comp[kComponents];
-	uint32_t valid; // bit c: comp[c] is a map
+	CUtensorMap map;
+	uint32_t valid;     // bit c: component c's interior tiles load through the map
+	int32_t row[3][4];  // first row of band b of component c (forward: the LL input, b = 0)
 };
-struct alignas(64) LevelBandMaps // inverse: the four bands per component
+// The batched form's maps of one level, per frame (frames past the table use
+// plain loads).
+constexpr int kBatchTileMapFrames = 64;
+struct alignas(64) BatchTileMaps
 {
-	CUtensorMap band[kComponents][4];
-	uint32_t valid; // bit c: band[c][*] are maps
+	LevelTileMap frame[kBatchTileMapFrames];
 };
 
 struct PlaneInput
@@ -299,7 +304,7 @@ constexpr int kMaxBatchFrames = 256;
 // transform of each level.
 constexpr int kSmallLevelTiles = 256;
 void launch_dwt_forward_level(const LevelParams &p, const PlaneInput &in, const EncodeBuffers &buf,
-                              const LevelInputMaps *maps, bool fused_quant,
+                              const LevelTileMap *maps, bool fused_quant,
                               bool programmatic, cudaStream_t stream);
 // Quantise and analyse the first nblocks 32x32 blocks (block index order) from storage.
 void launch_quant_pretransformed(const BlockParams &p, const EncodeBuffers &buf, int nblocks, bool programmatic,
@@ -309,7 +314,7 @@ void launch_pack(const BlockParams &p, const EncodeBuffers &buf, cudaStream_t st
 // Dequantise blocks [first, first + count) (block index order).
 void launch_dequant(const BlockParams &p, const DecodeInput &in, int first, int count, bool programmatic,
                     cudaStream_t stream);
-void launch_idwt_level(const LevelParams &p, const DecodeInput &in, const PlaneOutput &out, const LevelBandMaps *maps,
+void launch_idwt_level(const LevelParams &p, const DecodeInput &in, const PlaneOutput &out, const LevelTileMap *maps,
                        bool programmatic,
                        cudaStream_t stream);
 void launch_pyramid_io(const BlockParams &p, float *canonical, float *coef32, __half *coef16, bool to_canonical,
@@ -347,9 +352,11 @@ constexpr int kMaxPackets = 1 << 20;
 void launch_packet_assembly(const PacketParams &pp, cudaStream_t stream);
 
 // Batched launchers: `cta_map` holds one batch_cta() word per CTA.
-// large_ctas selects the 1024-thread variant of a level.
+// large_ctas selects the 1024-thread variant of a level; `maps` (may be null)
+// holds the level's per-frame TMA maps.
 void launch_dwt_forward_batch(const BatchFrame *frames, const BatchFrameIO *io, const uint32_t *cta_map, int nctas,
-                              int level, bool fused_quant, bool large_ctas, bool programmatic, cudaStream_t stream);
+                              int level, const BatchTileMaps *maps, bool fused_quant, bool large_ctas,
+                              bool programmatic, cudaStream_t stream);
 void launch_quant_blocks_batch(const BatchFrame *frames, const uint32_t *cta_map, int nctas, bool programmatic,
                                cudaStream_t stream);
 void launch_resolve_batch(const BatchFrame *frames, const BatchFrameIO *io, const uint32_t *cta_map, int nctas,
@@ -358,6 +365,6 @@ void launch_pack_batch(const BatchFrame *frames, const uint32_t *cta_map, int nc
 void launch_dequant_batch(const BatchFrame *frames, const uint32_t *cta_map, int nctas, bool programmatic,
                           cudaStream_t stream);
 void launch_idwt_batch(const BatchFrame *frames, const BatchFrameIO *io, const uint32_t *cta_map, int nctas, int level,
-                       bool large_ctas, bool programmatic, cudaStream_t stream);
+                       const BatchTileMaps *maps, bool large_ctas, bool programmatic, cudaStream_t stream);
 
 } // namespace pw

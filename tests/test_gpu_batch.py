@@ -135,3 +135,42 @@ def test_batch_validation(device):
     assert batch.encode(ptrs, strides, [4096]) == capi.PYROWAVE_SUCCESS
     assert batch.sizes()[0] <= 4096
     batch.close()
+
+
+def test_batch_frames_past_tensor_map_table(device):
+    """Frames past the batch's per-frame TMA map table (64 frames) load their
+    tiles with plain loads; both kinds match the single-frame path."""
+    import torch
+
+    big = (640, 360, True, 60000)
+    shapes = [big] + [(64, 64, False, 4096)] * 63 + [big, (1280, 720, False, 150000)]
+    planes = [synth.synth_frame(w, h, c444, 500 + i) for i, (w, h, c444, _) in enumerate(shapes)]
+    dev_planes = [[torch.from_numpy(p).cuda() for p in pl] for pl in planes]
+    infos = [(w, h, capi.CHROMA_444 if c444 else capi.CHROMA_420, b) for w, h, c444, b in shapes]
+    batch = capi.Batch(device, infos)
+    outs = [[torch.zeros_like(p) for p in pl] for pl in dev_planes]
+    in_ptrs, in_strides = _ptrs(dev_planes)
+    out_ptrs, out_strides = _ptrs(outs)
+    budgets = [b for *_, b in shapes]
+    assert batch.encode(in_ptrs, in_strides, budgets, out_ptrs, out_strides) == capi.PYROWAVE_SUCCESS
+    sizes = batch.sizes()
+    for i in (0, 64, 65):
+        w, h, c444, budget = shapes[i]
+        chroma = capi.CHROMA_444 if c444 else capi.CHROMA_420
+        enc = capi.Encoder(device, w, h, chroma)
+        pl = dev_planes[i]
+        enc.encode_device([p.data_ptr() for p in pl], [p.stride(0) for p in pl], budget)
+        torch.cuda.synchronize()
+        n = enc.size()
+        s, m, _ = enc.device_bitstream()
+        ref = _copy_device_words(s, n // 4)
+        dec = capi.Decoder(device, w, h, chroma)
+        ref_out = [torch.zeros_like(p) for p in pl]
+        dec.decode_blocks(m, s + 8, n // 4 - 2, [t.data_ptr() for t in ref_out], [t.stride(0) for t in ref_out])
+        torch.cuda.synchronize()
+        bs, _ = batch.device_bitstream(i)
+        assert sizes[i] == n
+        assert np.array_equal(_copy_device_words(bs, sizes[i] // 4), ref), f"frame {i}: bitstream differs"
+        for p in range(3):
+            assert np.array_equal(outs[i][p].cpu().numpy(), ref_out[p].cpu().numpy()), f"frame {i} plane {p}"
+    batch.close()
