@@ -601,21 +601,24 @@ bool encode_storage_map(CUtensorMap &map, float *coef32, int64_t storage_elems, 
 // as boxes of 36 rows x 40 samples. A component's tiles use the map (valid bit)
 // when its level is FP32, large enough to have interior tiles, and each band it
 // reads starts on a row of the level's pitch; otherwise they use plain loads,
-// as do all tiles when the driver offers no tensor-map encoder.
-void build_tile_maps(const Geometry &g, const LevelParams (&lp)[kLevels], float *coef32, LevelTileMap (&fwd)[kLevels],
-                     LevelTileMap (&inv)[kLevels])
+// as do all tiles when the driver offers no tensor-map encoder. Either table
+// may be null.
+void build_tile_maps(const Geometry &g, const LevelParams (&lp)[kLevels], float *coef32, LevelTileMap *fwd,
+                     LevelTileMap *inv)
 {
 	for (int level = 0; level < kLevels; level++)
 	{
-		fwd[level] = LevelTileMap{};
-		inv[level] = LevelTileMap{};
+		if (fwd)
+			fwd[level] = LevelTileMap{};
+		if (inv)
+			inv[level] = LevelTileMap{};
 	}
 	if (!tensor_map_encoder() || !coef32 || g.storage_elems32 <= 0)
 		return;
 	for (int level = 0; level < kLevels; level++)
 	{
 		const LevelParams &p = lp[level];
-		if (level > 0 && !p.P.fp16 && p.P.pitch >= 76 && p.P.rows >= 72)
+		if (fwd && level > 0 && !p.P.fp16 && p.P.pitch >= 76 && p.P.rows >= 72)
 		{
 			LevelTileMap &m = fwd[level];
 			uint32_t valid = 0;
@@ -632,7 +635,7 @@ void build_tile_maps(const Geometry &g, const LevelParams (&lp)[kLevels], float 
 			if (valid && encode_storage_map(m.map, coef32, g.storage_elems32, p.P.pitch, 76, 72))
 				m.valid = valid;
 		}
-		if (!p.L.fp16 && p.L.pitch >= 40 && p.L.rows >= 36)
+		if (inv && !p.L.fp16 && p.L.pitch >= 40 && p.L.rows >= 36)
 		{
 			LevelTileMap &m = inv[level];
 			uint32_t valid = 0;
@@ -790,10 +793,7 @@ struct pyrowave_encoder_opaque
 			return PYROWAVE_ERROR_OUT_OF_DEVICE_MEMORY;
 		}
 		cudaMemcpy(jobs_d, jobs.data(), jobs.size() * 4, cudaMemcpyHostToDevice);
-		{
-			LevelTileMap unused[kLevels];
-			build_tile_maps(g, lp, coef32, in_maps, unused);
-		}
+		build_tile_maps(g, lp, coef32, in_maps, nullptr);
 		allocated = true;
 		return PYROWAVE_SUCCESS;
 	}
@@ -1214,10 +1214,7 @@ struct pyrowave_decoder_opaque
 		error_d = dev_alloc<uint32_t>(1, ok);
 		if (error_d)
 			cudaMemset(error_d, 0, sizeof(uint32_t));
-		{
-			LevelTileMap unused[kLevels];
-			build_tile_maps(g, lp, coef32, unused, band_maps);
-		}
+		build_tile_maps(g, lp, coef32, nullptr, band_maps);
 		if (!ok)
 		{
 			release();
