@@ -25,7 +25,8 @@
  * the arithmetic stages follow the GLSL line by line and are pinned by the
  * reference's known-answer tests (pyrowave_c_test.cpp). The GLSL itself cannot
  * run on this machine (no Vulkan device), so the arithmetic is "restated, not
- * executed" -- see the parity section of DESIGN.md.
+ * executed": bit-exact agreement of the CUDA kernels with this restatement is
+ * what the GPU tests check.
  */
 #ifndef PYROWAVE_ORACLE_H_
 #define PYROWAVE_ORACLE_H_
