@@ -56,6 +56,25 @@ def dist_info():
     return ws, rank, local
 
 
+def max_over_ranks(values, ws, device="cpu"):
+    """Element-wise maximum of this rank's timings over all ranks; every rank
+    gets the result (one all-reduce, the same on every rank). With one rank the
+    values come back unchanged."""
+    if ws <= 1:
+        return [float(v) for v in values]
+    import torch
+
+    t = torch.tensor([float(v) for v in values], dtype=torch.float64, device=device)
+    torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+    return [float(x) for x in t.tolist()]
+
+
+def whole_job_us_per_frame(max_ms, steps, ws):
+    """Microseconds per frame of the whole job: every rank codes `steps`
+    frames, and the job takes as long as its slowest rank."""
+    return max_ms * 1e3 / (steps * ws)
+
+
 def make_frames(cfg):
     from pyrowave_b200 import synth
 
@@ -255,13 +274,10 @@ def run_ours(args, cfg, ws, rank, local):
         tag, rest = line.split(":", 1)
         stages[tag.strip()] = float(rest.split("ms")[0])
 
-    if ws > 1:
-        t = torch.tensor([total_ms, plain_ms], device="cuda")
-        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-        total_ms, plain_ms = float(t[0]), float(t[1])
+    total_ms, plain_ms = max_over_ranks([total_ms, plain_ms], ws, "cuda")
 
     frames_total = args.steps * ws
-    us_per_frame = plain_ms * 1e3 / frames_total
+    us_per_frame = whole_job_us_per_frame(plain_ms, args.steps, ws)
 
     # Roofline of the dominant kernel.
     alg = algorithmic_bytes(cfg, args.fp16_mask)
@@ -283,9 +299,7 @@ def run_ours(args, cfg, ws, rank, local):
 
     e2e = run_e2e(args, cfg, frames, dev) if rank == 0 or ws > 1 else None
     if ws > 1:
-        t = torch.tensor([e2e["total_s"]], device="cuda", dtype=torch.float64)
-        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-        e2e["total_s"] = float(t[0])
+        e2e["total_s"] = max_over_ranks([e2e["total_s"]], ws, "cuda")[0]
     cpu = None
     if rank == 0 and ws == 1 and not args.no_cpu_baseline:
         cpu = cpu_baseline(cfg, frames, args.cpu_seconds)
