@@ -721,22 +721,49 @@ def run_e2e(args, cfg, frames, dev):
             "d2h": planes_bytes + budget + 8 * blocks32 + 8}
 
 
-def cpu_baseline(cfg, frames, seconds):
-    """The oracle (the reference algorithm restated in C++) on all host cores."""
+def _oracle_frame(O, f, w, h, c444, budget, mode):
+    """One frame through the oracle (encode, packetize, parse, decode); seconds per stage."""
+    t = {}
+    o = O.Oracle(w, h, c444)
+    t0 = time.perf_counter()
+    pyr = o.dwt(f, mode)
+    t1 = time.perf_counter()
+    o.encode_pyramid(pyr, budget)
+    t2 = time.perf_counter()
+    stream, packets = o.packetize(8192, budget + 64)
+    t3 = time.perf_counter()
+    p = o.parser()
+    for off, sz in packets:
+        p.push(stream[off:off + sz].tobytes())
+    offs, payload = p.get()
+    t4 = time.perf_counter()
+    coef = o.dequant(offs, payload, mode)
+    t5 = time.perf_counter()
+    o.idwt(coef, mode)
+    t6 = time.perf_counter()
+    t.update(dwt=t1 - t0, quant_rate_pack=t2 - t1, packetize=t3 - t2, parse=t4 - t3, dequant=t5 - t4, idwt=t6 - t5)
+    return t
+
+
+def cpu_baseline(cfg, frames, seconds, single_frames: int = 3):
+    """The oracle (the reference algorithm restated in C++) on all host cores,
+    plus a single-thread pass over a few frames with per-stage times."""
     import oracle as O
 
     cores = os.cpu_count() or 1
     w, h, c444, budget = cfg["width"], cfg["height"], cfg["chroma444"], cfg["budget"]
 
     def one(f):
-        o = O.Oracle(w, h, c444)
-        o.encode(f, budget, O.MODE_F32)
-        stream, packets = o.packetize(8192, budget + 64)
-        p = o.parser()
-        for off, sz in packets:
-            p.push(stream[off:off + sz].tobytes())
-        offs, payload = p.get()
-        o.idwt(o.dequant(offs, payload, O.MODE_F32), O.MODE_F32)
+        return _oracle_frame(O, f, w, h, c444, budget, O.MODE_F32)
+
+    # Single thread: per-stage times (the first frame also warms the oracle's tables).
+    one(frames[0])
+    stages = {}
+    t0 = time.perf_counter()
+    for i in range(single_frames):
+        for k, v in one(frames[i % len(frames)]).items():
+            stages[k] = stages.get(k, 0.0) + v
+    single_us = (time.perf_counter() - t0) * 1e6 / single_frames
 
     done = 0
     t0 = time.perf_counter()
@@ -746,7 +773,10 @@ def cpu_baseline(cfg, frames, seconds):
             done += cores
     dt = time.perf_counter() - t0
     return {"value": round(dt * 1e6 / done, 1), "unit": "us/frame", "cores": cores, "kind": "port",
-            "sample": f"{done} frames encoded+decoded on {cores} threads in {dt:.1f} s (oracle restatement, FP32)"}
+            "sample": f"{done} frames encoded+decoded on {cores} threads in {dt:.1f} s (oracle restatement, FP32); "
+                      f"single thread: {single_frames} frames",
+            "single_thread_us_per_frame": round(single_us, 1),
+            "single_thread_stages_us": {k: round(v * 1e6 / single_frames, 1) for k, v in stages.items()}}
 
 
 def run_reference(args, cfg, ws, rank):
