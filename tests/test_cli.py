@@ -257,7 +257,7 @@ def test_container_errors(shim_tools, tmp_path):
 
 
 @pytest.mark.gpu
-def test_shipped_tools_round_trip_on_gpu(tmp_path):
+def test_shipped_tools_round_trip_on_gpu(gpu, tmp_path):
     """The built binaries against the CUDA library: same packets and decodes as the oracle."""
     tools = {t: os.path.join(lib_build.BIN, t) for t in lib_build.CLI_TOOLS}
     for exe in tools.values():
