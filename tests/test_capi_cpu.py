@@ -90,3 +90,20 @@ def test_vulkan_only_entry_points_report_not_implemented():
     assert L.pyrowave_create_device(None, ctypes.byref(h)) == capi.PYROWAVE_ERROR_NO_VULKAN
     assert not L.pyrowave_device_confirm_interop_support(None)
     assert not L.pyrowave_decoder_device_prefers_fragment_path(None)
+
+
+@pytest.mark.parametrize("lang, std", [("c", "c99"), ("c++", "c++11")])
+def test_public_headers_compile_and_link_for_c_and_cpp_callers(tmp_path, lang, std):
+    """A caller of the reference's C header keeps its source: both headers build
+    as pedantic C99 and C++11 and the program links against the library."""
+    src = tmp_path / "caller.c"
+    src.write_text('#include "pyrowave.h"\n#include "pyrowave_cuda.h"\n'
+                   "int main(void)\n{\n\tpyrowave_device d;\n\tuint32_t a, b, c;\n"
+                   "\tpyrowave_get_api_version(&a, &b, &c);\n"
+                   "\treturn pyrowave_create_default_device(&d) != PYROWAVE_SUCCESS;\n}\n")
+    compiler = "gcc" if lang == "c" else "g++"
+    r = subprocess.run([compiler, "-x", lang, f"-std={std}", "-Wall", "-Wextra", "-pedantic", "-Werror",
+                        "-I", os.path.join(ROOT, "include"), str(src), "-o", str(tmp_path / "caller"),
+                        "-L", os.path.dirname(capi.library_path()), "-l:libpyrowave-shared.so.0"],
+                       capture_output=True, text=True)
+    assert r.returncode == 0, r.stderr
