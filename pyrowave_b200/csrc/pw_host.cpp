@@ -424,6 +424,11 @@ struct pyrowave_device_opaque
 	}
 };
 
+namespace pw
+{
+int device_ordinal(const pyrowave_device_opaque *device) { return device ? device->cuda_device : 0; }
+} // namespace pw
+
 namespace
 {
 // Per-stage GPU timing with CUDA events (the reference's register_time_interval,

@@ -19,8 +19,14 @@
 #include <cuda_fp16.h>
 #include <cuda_runtime.h>
 
+struct pyrowave_device_opaque;
+
 namespace pw
 {
+// The CUDA device a pyrowave_device was created on. Library threads of their
+// own (the serving loop's dispatcher) make it current before any CUDA call.
+int device_ordinal(const pyrowave_device_opaque *device);
+
 constexpr int kLevels = 5;
 constexpr int kComponents = 3;
 constexpr int kAlignment = 32;

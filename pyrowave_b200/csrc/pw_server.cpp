@@ -150,6 +150,9 @@ struct pyrowave_cuda_server_opaque
 
 	void run()
 	{
+		// This thread starts with device 0 current; the slots' streams, the
+		// encoders and their buffers belong to the server's device.
+		cudaSetDevice(device_ordinal(device));
 		std::unique_lock<std::mutex> g(lock);
 		size_t rr = 0; // round-robin start among streams
 		while (!stop.load() || pending > 0)
