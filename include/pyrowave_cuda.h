@@ -322,7 +322,7 @@ PYROWAVE_PUBLIC_API pyrowave_result pyrowave_cuda_server_poll(pyrowave_cuda_serv
                                                               uint32_t timeout_us);
 
 /* Latency percentiles (microseconds) and count of the requests finished since
- * the last reset. */
+ * the last reset. The percentiles cover the most recent 2^20 of those requests. */
 PYROWAVE_PUBLIC_API pyrowave_result pyrowave_cuda_server_stats(pyrowave_cuda_server server, double *p50_us,
                                                                double *p99_us, uint64_t *frames, bool reset);
 

@@ -83,7 +83,12 @@ struct pyrowave_cuda_server_opaque
 	uint32_t next_stream = 1;
 	uint64_t next_request = 1;
 	std::deque<pyrowave_cuda_server_completion> completed;
-	std::vector<double> latencies; // since the last stats reset
+	// Latencies since the last stats reset: the most recent kLatencySamples in a
+	// ring, so a server that never resets its statistics stays bounded.
+	static constexpr size_t kLatencySamples = size_t(1) << 20;
+	std::vector<double> latencies;
+	size_t latency_next = 0;     // ring position once the ring is full
+	uint64_t finished_since_reset = 0;
 	std::mutex lock;
 	std::condition_variable wake, done_cv;
 	std::atomic<bool> stop{false};
@@ -141,7 +146,14 @@ struct pyrowave_cuda_server_opaque
 		}
 		c.latency_us = std::chrono::duration<double, std::micro>(Clock::now() - slot.req.submitted).count();
 		completed.push_back(c);
-		latencies.push_back(c.latency_us);
+		if (latencies.size() < kLatencySamples)
+			latencies.push_back(c.latency_us);
+		else
+		{
+			latencies[latency_next] = c.latency_us;
+			latency_next = (latency_next + 1) % kLatencySamples;
+		}
+		finished_since_reset++;
 		slot.busy = false;
 		vs.busy = false;
 		pending--;
@@ -379,11 +391,17 @@ pyrowave_result pyrowave_cuda_server_stats(pyrowave_cuda_server server, double *
 	if (!server)
 		return PYROWAVE_ERROR_INVALID_ARGUMENT;
 	std::vector<double> lat;
+	uint64_t finished = 0;
 	{
 		std::lock_guard<std::mutex> g(server->lock);
 		lat = server->latencies;
+		finished = server->finished_since_reset;
 		if (reset)
+		{
 			server->latencies.clear();
+			server->latency_next = 0;
+			server->finished_since_reset = 0;
+		}
 	}
 	std::sort(lat.begin(), lat.end());
 	auto pct = [&](double p) {
@@ -397,7 +415,7 @@ pyrowave_result pyrowave_cuda_server_stats(pyrowave_cuda_server server, double *
 	if (p99_us)
 		*p99_us = pct(0.99);
 	if (frames)
-		*frames = lat.size();
+		*frames = finished;
 	return PYROWAVE_SUCCESS;
 }
 }
