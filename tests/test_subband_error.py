@@ -53,3 +53,34 @@ def test_fp16_storage_exceeds_half_step():
         ratios = _band_ratios(1920, 1080, False, mask, 1)
         assert max(ratios.values()) > 0.5, mask
         assert max(v for (c, level, b), v in ratios.items() if level == 0) < 0.5, mask
+
+
+def _coded_psnr(w, h, c444, seed, budget, mode):
+    o = O.Oracle(w, h, c444)
+    planes = synth.synth_frame(w, h, c444, seed)
+    o.encode(planes, budget, mode)
+    stream, packets = o.packetize(budget + 64, budget + 64)
+    parser = o.parser()
+    for off, size in packets:
+        assert parser.push(stream[int(off):int(off) + int(size)].tobytes())
+    offs, payload = parser.get()
+    out = o.idwt(o.dequant(offs, payload, mode), mode)
+    return [O.psnr(a, b) for a, b in zip(planes, out)]
+
+
+def test_fp32_psnr_tracks_reference_precision():
+    """PSNR of the FP32 default against the reference precision (REF16) at the
+    same budget, 720p 4:2:0 at 150000 bytes, seeds 1-8. The modes take slightly
+    different rate-control steps, so single frames differ by a few hundredths
+    of a dB either way (measured: means per plane -0.003 / -0.019 / +0.018 dB,
+    single frames within 0.14 dB); this guards against a drift beyond that: the
+    mean per plane within 0.05 dB and every frame within 0.25 dB."""
+    import concurrent.futures
+
+    seeds = range(1, 9)
+    with concurrent.futures.ThreadPoolExecutor(8) as ex:
+        f32 = list(ex.map(lambda s: _coded_psnr(1280, 720, False, s, 150000, O.MODE_F32), seeds))
+        r16 = list(ex.map(lambda s: _coded_psnr(1280, 720, False, s, 150000, O.MODE_REF16), seeds))
+    d = np.array(f32) - np.array(r16)
+    assert np.abs(d.mean(axis=0)).max() <= 0.05, d.mean(axis=0)
+    assert np.abs(d).max() <= 0.25, d
