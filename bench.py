@@ -119,21 +119,25 @@ def algorithmic_bytes(cfg, fp16_mask):
 
 
 class ClockSampler:
-    """nvidia-smi clocks and throttle reasons sampled every 200 ms."""
+    """nvidia-smi clocks and throttle reasons, sampled every 50 ms with arrival
+    times, so that only the samples taken while the GPU runs the measured
+    workload (between mark_begin and mark_end) are summarised."""
 
     FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
               "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
               "clocks_event_reasons.sw_power_cap")
+    INTERVAL_MS = 50
 
     def __init__(self, gpu_index: int):
         self.gpu_index = gpu_index
         self.proc = None
-        self.lines = []
+        self.lines = []  # (arrival time, csv line)
+        self.begin = self.end = None
 
     def start(self):
         try:
             self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.gpu_index), f"--query-gpu={self.FIELDS}",
-                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                          "--format=csv,noheader,nounits", "-lms", str(self.INTERVAL_MS)],
                                          stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
             self.thread = threading.Thread(target=self._read, daemon=True)
             self.thread.start()
@@ -142,20 +146,39 @@ class ClockSampler:
 
     def _read(self):
         for line in self.proc.stdout:
-            self.lines.append(line.strip())
+            self.lines.append((time.perf_counter(), line.strip()))
+
+    def wait_ready(self, timeout: float = 3.0):
+        """Waits (bounded) for the first sample, so sampling runs before the load starts."""
+        t0 = time.perf_counter()
+        while self.proc is not None and not self.lines and time.perf_counter() - t0 < timeout:
+            time.sleep(0.01)
+
+    def mark_begin(self):
+        self.begin = time.perf_counter()
+
+    def mark_end(self):
+        self.end = time.perf_counter()
 
     def stop(self):
         if self.proc is None:
             return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
-        time.sleep(0.3)
+        time.sleep(2 * self.INTERVAL_MS / 1000)  # the sample in flight at mark_end
         self.proc.terminate()
         try:
             self.proc.wait(timeout=5)
         except Exception:
             self.proc.kill()
+        lines = list(self.lines)
+        in_region = lines
+        if self.begin is not None and self.end is not None:
+            # A sample printed up to one interval after mark_end was queried before it.
+            last = self.end + self.INTERVAL_MS / 1000
+            in_region = [(t, l) for t, l in lines if self.begin <= t <= last]
+        used = in_region if in_region else lines
         sm, mx, reasons = [], None, set()
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        for line in self.lines:
+        for _, line in used:
             parts = [p.strip() for p in line.split(",")]
             if len(parts) < 9:
                 continue
@@ -168,7 +191,8 @@ class ClockSampler:
                 if v.lower().startswith("active"):
                     reasons.add(n)
         return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": mx, "reasons": sorted(reasons),
-                "samples": len(sm)}
+                "samples": len(sm), "samples_under_load": len(in_region) if in_region is not lines else 0,
+                "interval_ms": self.INTERVAL_MS}
 
 
 def measured_peak():
@@ -258,15 +282,32 @@ def run_ours(args, cfg, ws, rank, local):
         return float(sum(s_.elapsed_time(e_) for s_, e_ in zip(starts, ends)))
 
     # Timed region 1: the headline number (no extra events between kernels).
+    # The clock samples cover it and about 0.3 s of the same untimed steps just
+    # before it (64 at a time, then a synchronize, so the queue stays short):
+    # the timed steps alone last too short for samples at 50 ms. The frame
+    # order continues through the load steps into the timed ones, so no timed
+    # frame is still in L2.
     sampler = ClockSampler(local)
     sampler.start()
-    plain_ms = timed_pass(args.warmup)
+    sampler.wait_ready()
+    sampler.mark_begin()
+    load_steps = 0
+    t_load = time.perf_counter()
+    while time.perf_counter() - t_load < 0.3:
+        for _ in range(64):
+            step(args.warmup + load_steps)
+            load_steps += 1
+        torch.cuda.synchronize()
+    first_timed = args.warmup + load_steps
+    plain_ms = timed_pass(first_timed)
+    sampler.mark_end()
     clocks = sampler.stop()
+    clocks["load_steps_before_timed"] = load_steps
     # Timed region 2: the same steps with a CUDA event after every kernel, for
     # the per-kernel durations behind the roofline.
     dev.set_stage_timing(True)
     dev.report_performance_stats(reset=True)
-    total_ms = timed_pass(args.warmup + args.steps)
+    total_ms = timed_pass(first_timed + args.steps)
     stage_lines = dev.report_performance_stats(reset=True)
     dev.set_stage_timing(False)
     stages = {}
