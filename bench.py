@@ -82,6 +82,18 @@ def make_frames(cfg):
             for s in cfg["seeds"]]
 
 
+def frames_fingerprint(frames):
+    """8-byte blake2b over the frames' own fingerprints, in order."""
+    import hashlib
+
+    from pyrowave_b200 import synth
+
+    h = hashlib.blake2b(digest_size=8)
+    for f in frames:
+        h.update(bytes.fromhex(synth.frame_hash(f)))
+    return h.hexdigest()
+
+
 def algorithmic_bytes(cfg, fp16_mask):
     """Minimal bytes per frame of each kernel: every input byte read once, every output byte written once."""
     w, h, c444 = cfg["width"], cfg["height"], cfg["chroma444"]
@@ -373,7 +385,8 @@ def run_ours(args, cfg, ws, rank, local):
             "data": "synthetic (seeded gradient + band-limited noise + rectangles, 16 frames)",
             "config": {"workload": f"encode+decode {cfg['width']}x{cfg['height']} "
                                    f"{'4:4:4' if c444 else '4:2:0'} 8-bit, {budget}-byte budget",
-                       "frames": len(frames), "budget_bytes": budget, "fp16_level_mask": args.fp16_mask,
+                       "frames": len(frames), "frames_fingerprint": frames_fingerprint(frames),
+                       "budget_bytes": budget, "fp16_level_mask": args.fp16_mask,
                        "l2": l2_note, "parallelism": f"replicas x{ws}"},
             "e2e": {"value": round(e2e["total_s"] * 1e6 / (e2e["frames"] * ws), 2), "unit": "us/frame",
                     "h2d_bytes_per_step": e2e["h2d"], "d2h_bytes_per_step": e2e["d2h"]},

@@ -126,7 +126,7 @@ def synth_frame(width: int, height: int, chroma444: bool, seed: int, rects: int 
 
 
 def frame_hash(planes) -> str:
-    """FNV-style fingerprint (blake2b, 8 bytes) of the three planes."""
+    """Fingerprint (8-byte blake2b, hex) of the three planes."""
     h = hashlib.blake2b(digest_size=8)
     for p in planes:
         h.update(np.ascontiguousarray(p).tobytes())

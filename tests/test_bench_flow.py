@@ -113,3 +113,4 @@ def test_run_ours_json_line(fake_gpu):
     assert line["gpu_launches"] == 14 * 20
     assert line["roofline"]["bound"] == "hbm" and line["roofline"]["frac"] > 0
     assert line["e2e"]["value"] == pytest.approx(0.004 * 1e6 / 10)
+    assert len(line["config"]["frames_fingerprint"]) == 16
