@@ -775,6 +775,18 @@ def run_e2e(args, cfg, frames, dev):
             "d2h": planes_bytes + budget + 8 * blocks32 + 8}
 
 
+def cpu_model() -> str:
+    """The host CPU's model name (Linux /proc/cpuinfo), or "unknown"."""
+    try:
+        with open("/proc/cpuinfo") as f:
+            for line in f:
+                if line.startswith("model name"):
+                    return line.split(":", 1)[1].strip()
+    except OSError:
+        pass
+    return "unknown"
+
+
 def _oracle_frame(O, f, w, h, c444, budget, mode):
     """One frame through the oracle (encode, packetize, parse, decode); seconds per stage."""
     t = {}
@@ -827,6 +839,7 @@ def cpu_baseline(cfg, frames, seconds, single_frames: int = 3):
             done += cores
     dt = time.perf_counter() - t0
     return {"value": round(dt * 1e6 / done, 1), "unit": "us/frame", "cores": cores, "kind": "port",
+            "cpu_model": cpu_model(),
             "sample": f"{done} frames encoded+decoded on {cores} threads in {dt:.1f} s (oracle restatement, FP32); "
                       f"single thread: {single_frames} frames",
             "single_thread_us_per_frame": round(single_us, 1),
@@ -871,6 +884,7 @@ def run_reference(args, cfg, ws, rank):
         "config": {"workload": f"encode+decode {cfg['width']}x{cfg['height']} {'4:4:4' if c444 else '4:2:0'} 8-bit, "
                                f"{budget}-byte budget", "frames": len(frames)},
         "cpu_baseline": {"value": round(us, 1), "unit": "us/frame", "cores": cores, "kind": "port",
+                         "cpu_model": cpu_model(),
                          "sample": f"{args.steps * per_step} frames, {per_step} per step on {cores} threads "
                                    "(the reference's Vulkan path needs a graphics stack: unavailable on this box)"},
         "e2e": {"value": round(us, 1), "unit": "us/frame", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
