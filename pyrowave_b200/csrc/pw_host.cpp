@@ -1703,7 +1703,8 @@ pyrowave_result pyrowave_encoder_encode_cpu_synchronous(pyrowave_encoder encoder
 		const size_t bpp = (num_planes == 2 && p == 1) ? 2 : 1;
 		if (buffers->row_stride_in_bytes[p] < size_t(w) * bpp)
 			return PYROWAVE_ERROR_INVALID_ARGUMENT;
-		if (buffers->row_stride_in_bytes[p] * size_t(h) > buffers->plane_size_in_bytes[p])
+		// stride * h > plane size, written so that an absurd stride cannot wrap around
+		if (h > 0 && buffers->row_stride_in_bytes[p] > buffers->plane_size_in_bytes[p] / size_t(h))
 			return PYROWAVE_ERROR_INVALID_ARGUMENT;
 		if (!buffers->data[p])
 			return PYROWAVE_ERROR_INVALID_ARGUMENT;
@@ -1938,7 +1939,8 @@ pyrowave_result pyrowave_decoder_decode_cpu_buffer_synchronous(pyrowave_decoder 
 		plane_dims(chroma, g.width, g.height, p, w, h);
 		if (buffers->row_stride_in_bytes[p] < size_t(w))
 			return PYROWAVE_ERROR_INVALID_ARGUMENT;
-		if (buffers->row_stride_in_bytes[p] * size_t(h) > buffers->plane_size_in_bytes[p])
+		// stride * h > plane size, written so that an absurd stride cannot wrap around
+		if (h > 0 && buffers->row_stride_in_bytes[p] > buffers->plane_size_in_bytes[p] / size_t(h))
 			return PYROWAVE_ERROR_INVALID_ARGUMENT;
 		if (!buffers->data[p])
 			return PYROWAVE_ERROR_INVALID_ARGUMENT;

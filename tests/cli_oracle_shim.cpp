@@ -53,7 +53,7 @@ bool planes_ok(const pyrowave_cpu_buffer *b, bool c444, int w, int h)
 		int pw, ph;
 		plane_dims(c444, w, h, p, pw, ph);
 		if (!b->data[p] || b->row_stride_in_bytes[p] < size_t(pw) ||
-		    b->row_stride_in_bytes[p] * size_t(ph) > b->plane_size_in_bytes[p])
+		    b->row_stride_in_bytes[p] > b->plane_size_in_bytes[p] / size_t(ph))
 			return false;
 	}
 	return true;
