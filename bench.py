@@ -94,6 +94,72 @@ def frames_fingerprint(frames):
     return h.hexdigest()
 
 
+def workload_config(cfg, frames, ws):
+    """The `config` object of both arms' JSON lines: the same keys and values for the same workload."""
+    c444 = cfg["chroma444"]
+    return {"workload": f"encode+decode {cfg['width']}x{cfg['height']} {'4:4:4' if c444 else '4:2:0'} 8-bit, "
+                        f"{cfg['budget']}-byte budget",
+            "frames": len(frames), "frames_fingerprint": frames_fingerprint(frames),
+            "budget_bytes": cfg["budget"], "parallelism": f"replicas x{ws}"}
+
+
+# How the numbers of this line are tied to the reference's behaviour.
+PARITY = {
+    "bitstream_layer": "block layout, packetize and packet parser pinned to the reference's own "
+                       "metal/pyrowave_bitstream.cpp, compiled from its tree (tests/test_oracle_pinning.py, "
+                       "tests/golden/)",
+    "shader_math": "DWT, quantiser and RD statistics, rate control, packing, dequantiser and inverse DWT: bit-exact "
+                   "with the oracle's restatement of the reference shaders at every stage, on the frames of every "
+                   "configuration of this line (tests/test_gpu_parity.py); the restatement itself is pinned only by "
+                   "the reference's known-answer tests (pyrowave_c_test.cpp:147-158,288-379,440-535), since the "
+                   "shaders need Vulkan, which no machine here has",
+    "reference_precision": "REFERENCE_PRECISION (FP16 staging + FP16 levels 0-1) is bit-exact with the oracle's "
+                           "restatement of the reference's precision 1, so its PSNR equals the restated "
+                           "reference's (tests/test_gpu_psnr.py)",
+}
+
+
+def psnr_delta(cfg, frames, budget, mask):
+    """Decoded PSNR of the given precision minus that of REFERENCE_PRECISION (the
+    reference's arithmetic) at the same budget, per plane: mean over the frames
+    and the frame with the largest difference."""
+    import torch
+
+    from pyrowave_b200 import capi
+
+    w, h, c444 = cfg["width"], cfg["height"], cfg["chroma444"]
+    chroma = capi.CHROMA_444 if c444 else capi.CHROMA_420
+    dev = capi.Device()
+
+    def coded(m):
+        enc = capi.Encoder(dev, w, h, chroma, m)
+        dec = capi.Decoder(dev, w, h, chroma, m)
+        res = []
+        for f in frames:
+            d = [torch.from_numpy(p).cuda() for p in f]
+            o = [torch.empty_like(p) for p in d]
+            enc.encode_device([p.data_ptr() for p in d], [p.stride(0) for p in d], budget)
+            s, mt, cap = enc.device_bitstream()
+            dec.decode_blocks(mt, s + 8, cap - 2, [p.data_ptr() for p in o], [p.stride(0) for p in o])
+            res.append([_psnr(a, b.cpu().numpy()) for a, b in zip(f, o)])
+        enc.close()
+        dec.close()
+        return np.array(res)
+
+    d = coded(mask) - coded(0x103)
+    dev.close()
+    worst = np.abs(d).max(axis=0)
+    return {"mask": hex(mask), "against": "REFERENCE_PRECISION (0x103)", "frames": len(frames),
+            "mean_y_cb_cr": [round(float(x), 4) for x in d.mean(axis=0)],
+            "worst_frame_y_cb_cr": [round(float(x), 4) for x in worst],
+            "within_0.02_db_mean": bool(np.abs(d.mean(axis=0)).max() <= 0.02)}
+
+
+def _psnr(a, b):
+    mse = float(np.mean((a.astype(np.float64) - b.astype(np.float64)) ** 2))
+    return 99.0 if mse == 0 else 10.0 * np.log10(255.0 ** 2 / mse)
+
+
 def algorithmic_bytes(cfg, fp16_mask):
     """Minimal bytes per frame of each kernel: every input byte read once, every output byte written once."""
     w, h, c444 = cfg["width"], cfg["height"], cfg["chroma444"]
@@ -275,23 +341,34 @@ def run_ours(args, cfg, ws, rank, local):
 
     starts = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
     ends = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+    wall = {}
 
     def timed_pass(first):
+        """Device milliseconds of `steps` steps. With rotated inputs (larger than
+        L2) one event pair spans all steps, so any gap between steps counts; with
+        an L2 flush between steps, the flushes are excluded by an event pair per
+        step. The host wall clock over the same region is kept as a cross-check."""
         if ws > 1:
             torch.distributed.barrier()
         torch.cuda.synchronize()
+        w0 = time.perf_counter()
         for i in range(args.steps):
             with torch.cuda.stream(stream):
                 if flush is not None:
                     flush.fill_(i & 0xFF)  # evict the previous frame from the 126 MB L2
-                starts[i].record(stream)
+                if flush is not None or i == 0:
+                    starts[i].record(stream)
             step(first + i)
             with torch.cuda.stream(stream):
-                ends[i].record(stream)
+                if flush is not None or i == args.steps - 1:
+                    ends[i].record(stream)
         torch.cuda.synchronize()
+        wall["ms"] = (time.perf_counter() - w0) * 1e3
         if ws > 1:
             torch.distributed.barrier()
-        return float(sum(s_.elapsed_time(e_) for s_, e_ in zip(starts, ends)))
+        if flush is not None:
+            return float(sum(s_.elapsed_time(e_) for s_, e_ in zip(starts, ends)))
+        return float(starts[0].elapsed_time(ends[args.steps - 1]))
 
     # Timed region 1: the headline number (no extra events between kernels).
     # The clock samples cover it and about 0.3 s of the same untimed steps just
@@ -312,6 +389,7 @@ def run_ours(args, cfg, ws, rank, local):
         torch.cuda.synchronize()
     first_timed = args.warmup + load_steps
     plain_ms = timed_pass(first_timed)
+    plain_wall_ms = wall["ms"]
     sampler.mark_end()
     clocks = sampler.stop()
     clocks["load_steps_before_timed"] = load_steps
@@ -353,6 +431,9 @@ def run_ours(args, cfg, ws, rank, local):
     e2e = run_e2e(args, cfg, frames, dev) if rank == 0 or ws > 1 else None
     if ws > 1:
         e2e["total_s"] = max_over_ranks([e2e["total_s"]], ws, "cuda")[0]
+    psnr = None
+    if rank == 0 and not args.no_configs:
+        psnr = psnr_delta(cfg, frames, budget, args.fp16_mask)
     cpu = None
     if rank == 0 and ws == 1 and not args.no_cpu_baseline:
         cpu = cpu_baseline(cfg, frames, args.cpu_seconds)
@@ -383,13 +464,14 @@ def run_ours(args, cfg, ws, rank, local):
             "vs_baseline": None,
             "dtype": "f32" if args.fp16_mask == 0 else f"f32 (fp16 storage mask {args.fp16_mask:#x})",
             "data": "synthetic (seeded gradient + band-limited noise + rectangles, 16 frames)",
-            "config": {"workload": f"encode+decode {cfg['width']}x{cfg['height']} "
-                                   f"{'4:4:4' if c444 else '4:2:0'} 8-bit, {budget}-byte budget",
-                       "frames": len(frames), "frames_fingerprint": frames_fingerprint(frames),
-                       "budget_bytes": budget, "fp16_level_mask": args.fp16_mask,
-                       "l2": l2_note, "parallelism": f"replicas x{ws}"},
+            "config": workload_config(cfg, frames, ws),
+            "l2": l2_note,
+            "wall_us_per_frame": round(plain_wall_ms * 1e3 / args.steps, 3),
             "e2e": {"value": round(e2e["total_s"] * 1e6 / (e2e["frames"] * ws), 2), "unit": "us/frame",
-                    "h2d_bytes_per_step": e2e["h2d"], "d2h_bytes_per_step": e2e["d2h"]},
+                    "h2d_bytes_per_step": e2e["h2d"], "d2h_bytes_per_step": e2e["d2h"],
+                    "method": e2e["method"], "breakdown_us": e2e["breakdown_us"]},
+            "parity": PARITY,
+            "psnr_delta_db": psnr,
             "gpu_launches": len(stages) * args.steps,  # one stage-timing tag per kernel launch
             "roofline": roofline,
             "dwt_stage": dwt_stage,
@@ -545,11 +627,15 @@ def run_batched(iters: int, frames_n: int = 64, seed: int = 7):
     return result
 
 
-def run_serving(seconds: float, streams_n: int = 32, pool_bytes: int = 16 << 30, seed: int = 11):
+def run_serving(seconds: float, streams_n: int = 32, pool_bytes: int = 16 << 30, seed: int = 11,
+                saturation_seconds: float = 15.0, outstanding: int = 3):
     """Serving loop: streams_n streams with seeded Poisson frame arrivals at 60
     or 120 fps, sizes from the batched set (4:2:0 and 4:4:4), budgets 150-250
     Mbit/s; every frame is encoded and decoded on the device. Reports latency
-    percentiles (submit to completion) and the aggregate frame rate."""
+    percentiles (submit to completion) and the aggregate frame rate at the
+    offered load, then a saturation point: every stream keeps `outstanding`
+    frames submitted at all times (offered load above capacity), which gives
+    the loop's capacity and its latency there."""
     import torch
 
     from pyrowave_b200 import capi, synth
@@ -579,11 +665,14 @@ def run_serving(seconds: float, streams_n: int = 32, pool_bytes: int = 16 << 30,
                             out=([p.data_ptr() for p in out], [p.stride(0) for p in out]), keep=out,
                             next=float(rng.exponential(1.0 / fps))))
     # Warm up every stream once (first-use allocation and graph capture).
-    for s in streams:
-        server.submit(s["sid"], *s["inp"], s["budget"], *s["out"])
+    for st in streams:
+        server.submit(st["sid"], *st["inp"], st["budget"], *st["out"])
     got = 0
     while got < len(streams):
         got += len(server.poll(timeout_us=100000))
+    failures = 0
+
+    # Offered load: Poisson arrivals.
     server.stats(reset=True)
     start = time.perf_counter()
     submitted = completed = 0
@@ -592,24 +681,42 @@ def run_serving(seconds: float, streams_n: int = 32, pool_bytes: int = 16 << 30,
         now = time.perf_counter() - start
         if now >= seconds:
             break
-        for s in streams:
-            while s["next"] <= now:
-                server.submit(s["sid"], *s["inp"], s["budget"], *s["out"])
+        for st in streams:
+            while st["next"] <= now:
+                server.submit(st["sid"], *st["inp"], st["budget"], *st["out"])
                 submitted += 1
-                s["next"] += float(rng.exponential(1.0 / s["fps"]))
+                st["next"] += float(rng.exponential(1.0 / st["fps"]))
         for _, _, result, b, _ in server.poll(timeout_us=0):
             completed += 1
             nbytes += b
+            failures += result != capi.PYROWAVE_SUCCESS
         time.sleep(0.0002)
     while completed < submitted:
         for _, _, result, b, _ in server.poll(timeout_us=100000):
             completed += 1
             nbytes += b
+            failures += result != capi.PYROWAVE_SUCCESS
     elapsed = time.perf_counter() - start
-    p50, p99, frames = server.stats()
+    p50, p99, frames = server.stats(reset=True)
+    offered = sum(st["fps"] for st in streams)
+
+    # Saturation: a closed loop with `outstanding` frames per stream.
+    by_sid = {st["sid"]: st for st in streams}
+    sat_done = 0
+    for st in streams:
+        for _ in range(outstanding):
+            server.submit(st["sid"], *st["inp"], st["budget"], *st["out"])
+    t0 = time.perf_counter()
+    while time.perf_counter() - t0 < saturation_seconds:
+        for _, sid, result, _, _ in server.poll(timeout_us=1000):
+            sat_done += 1
+            failures += result != capi.PYROWAVE_SUCCESS
+            st = by_sid[sid]
+            server.submit(sid, *st["inp"], st["budget"], *st["out"])
+    sat_elapsed = time.perf_counter() - t0
+    s50, s99, _ = server.stats(reset=True)
     server.close()
     dev.close()
-    offered = sum(s["fps"] for s in streams)
     return {
         "workload": f"{streams_n} streams, Poisson arrivals at 60/120 fps, sizes {len(BATCH_SIZES)}-way mixed, "
                     f"4:2:0 and 4:4:4, budgets 150-250 Mbit/s, {pool_bytes >> 30} GiB state pool, "
@@ -619,6 +726,11 @@ def run_serving(seconds: float, streams_n: int = 32, pool_bytes: int = 16 << 30,
         "frames_per_s": round(completed / elapsed, 1),
         "p50_latency_us": round(p50, 1), "p99_latency_us": round(p99, 1),
         "frames": int(frames), "mean_bytes": round(nbytes / max(completed, 1), 1),
+        "failed_requests": int(failures),
+        "saturation": {"method": f"closed loop, {outstanding} frames outstanding per stream, "
+                                 f"{saturation_seconds:g} s",
+                       "frames_per_s": round(sat_done / sat_elapsed, 1),
+                       "p50_latency_us": round(s50, 1), "p99_latency_us": round(s99, 1)},
     }
 
 
@@ -692,6 +804,9 @@ def measure_config(dev, cfg, budget, mask, steps, warmup):
     dwt_ms = sum(v for k, v in stages.items() if k.startswith("dwt"))
     enc.close()
     dec.close()
+    psnr = None
+    if mask != 0x103:
+        psnr = psnr_delta(cfg, [[p.cpu().numpy() for p in f] for f in base], budget, mask)
     return {
         "workload": f"encode+decode {w}x{h} {'4:4:4' if c444 else '4:2:0'} 8-bit, {budget}-byte budget",
         "precision_mask": hex(mask), "us_per_frame": round(ms * 1e3, 2),
@@ -699,6 +814,7 @@ def measure_config(dev, cfg, budget, mask, steps, warmup):
         "stages_us": {k: round(v * 1e3, 2) for k, v in stages.items()},
         "stages_gbs": {k: round(alg[k] / (v * 1e-3) / 1e9, 1) for k, v in stages.items() if k in alg and v > 0},
         "dwt_stage_gbs": round(alg["dwt_stage"] / (dwt_ms * 1e-3) / 1e9, 1) if dwt_ms else None,
+        "psnr_delta_db": psnr,
         "note": "stage times carry one event pair per kernel (launch gaps included)",
     }
 
@@ -727,52 +843,103 @@ def _ncu_traffic(kernel, cfg):
 
 
 def run_e2e(args, cfg, frames, dev):
-    """Encode + decode through the C API with host (pinned) buffers."""
+    """Encode + decode through the reference-facing C API with host (pinned)
+    buffers: pyrowave_encoder_encode_cpu_synchronous (input planes uploaded
+    inside), compute_num_packets + packetize (the frame read back), one
+    pyrowave_decoder_push_packet of the whole packetized frame (the parser
+    walks the concatenated packets, as the reference's does) and
+    pyrowave_decoder_decode_cpu_buffer_synchronous (payload uploaded, planes
+    read back).
+
+    The timed run keeps two encoder/decoder pairs on two devices (two CUDA
+    streams): the encode of frame i+1, which returns without waiting
+    (pyrowave.h:445-447), is issued before frame i is packetized and decoded,
+    so one frame's copies and kernels overlap the other's. A sequential pass
+    with one pair gives the per-call breakdown."""
     import torch
 
     from pyrowave_b200 import capi
 
     w, h, c444, budget = cfg["width"], cfg["height"], cfg["chroma444"], cfg["budget"]
     chroma = capi.CHROMA_444 if c444 else capi.CHROMA_420
-    enc = capi.Encoder(dev, w, h, chroma, args.fp16_mask)
-    dec = capi.Decoder(dev, w, h, chroma, args.fp16_mask)
+    devs = [dev, capi.Device()]
+    pairs = [(capi.Encoder(d, w, h, chroma, args.fp16_mask), capi.Decoder(d, w, h, chroma, args.fp16_mask))
+             for d in devs]
     pinned = [[torch.from_numpy(p).pin_memory().numpy() for p in f] for f in frames]
-    out = [torch.empty(p.shape, dtype=torch.uint8).pin_memory().numpy() for p in frames[0]]
-    bitstream = torch.empty(budget, dtype=torch.uint8).pin_memory().numpy()
+    outs = [[torch.empty(p.shape, dtype=torch.uint8).pin_memory().numpy() for p in frames[0]] for _ in pairs]
+    bitstreams = [torch.empty(budget, dtype=torch.uint8).pin_memory().numpy() for _ in pairs]
     boundary = 8192
+    packets = (capi.Packet * 4096)()
+    got = capi.c_size_t()
 
-    def step(i):
-        f = pinned[i % len(pinned)]
-        capi.check(enc.encode_cpu(f, budget), "encode_cpu_synchronous")
+    def encode(k, i):
+        capi.check(pairs[k][0].encode_cpu(pinned[i % len(pinned)], budget), "encode_cpu_synchronous")
+
+    def finish(k):
+        enc, dec = pairs[k]
+        bs = bitstreams[k]
         n = enc.compute_num_packets(boundary)
-        packets = (capi.Packet * max(n, 1))()
-        got = capi.c_size_t()
+        assert n <= len(packets)
         capi.check(enc.L.pyrowave_encoder_packetize(enc.h, packets, boundary, capi.ctypes.byref(got),
-                                                    capi.ctypes.c_void_p(bitstream.ctypes.data), budget), "packetize")
-        total = 0
-        base = bitstream.ctypes.data
-        for k in range(got.value):
-            off, sz = packets[k].offset, packets[k].size
-            capi.check(dec.push_packet_ptr(base + off, sz), "push_packet")
-            total += sz
-        code, _ = dec.decode_cpu(out)
+                                                    capi.ctypes.c_void_p(bs.ctypes.data), budget), "packetize")
+        total = packets[got.value - 1].offset + packets[got.value - 1].size
+        t_pk = time.perf_counter()
+        capi.check(dec.push_packet_ptr(bs.ctypes.data, total), "push_packet")
+        t_push = time.perf_counter()
+        code, _ = dec.decode_cpu(outs[k])
         capi.check(code, "decode_cpu_buffer_synchronous")
-        return total
+        return total, t_pk, t_push
 
-    for i in range(max(args.warmup, 3)):
-        step(i)
-    n = max(args.steps, 5)
-    t0 = time.perf_counter()
+    # Sequential pass with one pair: per-call host times.
+    for i in range(3):
+        encode(0, i)
+        finish(0)
+    nseq = max(args.steps // 4, 10)
+    acc = dict(encode=0.0, packetize=0.0, push_packet=0.0, decode=0.0)
+    t_all = time.perf_counter()
+    for i in range(nseq):
+        t0 = time.perf_counter()
+        encode(0, i)
+        t1 = time.perf_counter()
+        _, t_pk, t_push = finish(0)
+        t2 = time.perf_counter()
+        acc["encode"] += t1 - t0
+        acc["packetize"] += t_pk - t1
+        acc["push_packet"] += t_push - t_pk
+        acc["decode"] += t2 - t_push
+    seq_us = (time.perf_counter() - t_all) * 1e6 / nseq
+    breakdown = {k: round(v * 1e6 / nseq, 1) for k, v in acc.items()}
+    breakdown["sequential_total"] = round(seq_us, 1)
+    breakdown["notes"] = ("encode: upload + launch, returns without waiting; packetize: waits for the encode, "
+                          "reads the frame back, cuts packets; push_packet: host parse of the whole frame; "
+                          "decode: payload upload, dequantise + inverse DWT, planes read back")
+
+    # Timed run: two pairs alternating, frame i+1 encoding while frame i finishes.
+    for i in range(4):
+        encode(i & 1, i)
+        finish(i & 1)
+    n = max(args.steps, 10)
     total_bytes = 0
+    t0 = time.perf_counter()
+    encode(0, 0)
     for i in range(n):
-        total_bytes += step(i)
+        if i + 1 < n:
+            encode((i + 1) & 1, i + 1)
+        total_bytes += finish(i & 1)[0]
     t1 = time.perf_counter()
+    blocks32 = pairs[0][0].layout().block_count_32x32
+    for enc, dec in pairs:
+        enc.close()
+        dec.close()
+    devs[1].close()
     planes_bytes = sum(p.nbytes for p in frames[0])
-    blocks32 = enc.layout().block_count_32x32
     avg_stream = total_bytes // n
     return {"total_s": t1 - t0, "frames": n,
             "h2d": planes_bytes + avg_stream + 4 * blocks32,
-            "d2h": planes_bytes + budget + 8 * blocks32 + 8}
+            "d2h": planes_bytes + budget + 8 * blocks32 + 8,
+            "method": "two encoder/decoder pairs on two CUDA streams, frame i+1's encode issued before frame i "
+                      "is packetized and decoded; one push_packet per frame",
+            "breakdown_us": breakdown}
 
 
 def cpu_model() -> str:
@@ -881,8 +1048,7 @@ def run_reference(args, cfg, ws, rank):
         "ms_per_step": round(dt * 1e3 / args.steps, 3), "higher_is_better": False, "scaling": "weak",
         "vs_baseline": None, "dtype": "f32 (fp16 staging, the reference's default precision)",
         "data": "synthetic (seeded gradient + band-limited noise + rectangles)",
-        "config": {"workload": f"encode+decode {cfg['width']}x{cfg['height']} {'4:4:4' if c444 else '4:2:0'} 8-bit, "
-                               f"{budget}-byte budget", "frames": len(frames)},
+        "config": workload_config(cfg, frames, ws),
         "cpu_baseline": {"value": round(us, 1), "unit": "us/frame", "cores": cores, "kind": "port",
                          "cpu_model": cpu_model(),
                          "sample": f"{args.steps * per_step} frames, {per_step} per step on {cores} threads "
@@ -905,7 +1071,7 @@ def main():
     ap.add_argument("--no-batch", action="store_true", help="skip the batched-form measurement")
     ap.add_argument("--no-configs", action="store_true",
                     help="skip the other configurations (720p, FP16 storage, reference precision, 4K, 4K 4:4:4 sweep)")
-    ap.add_argument("--serve-seconds", type=float, default=10.0,
+    ap.add_argument("--serve-seconds", type=float, default=60.0,
                     help="duration of the serving-loop measurement (0: skip)")
     ap.add_argument("--l2", default="rotate", choices=["rotate", "flush"],
                     help="rotate: distinct inputs larger than L2; flush: 256 MiB write between steps")

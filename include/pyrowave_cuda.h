@@ -163,6 +163,18 @@ PYROWAVE_PUBLIC_API pyrowave_result pyrowave_cuda_decoder_decode_packets(pyrowav
 PYROWAVE_PUBLIC_API pyrowave_result pyrowave_cuda_decoder_get_packet_status(pyrowave_decoder decoder,
                                                                             pyrowave_cuda_packet_status *status);
 
+/* Outcome of the decoder's last decode on the GPU (any of pyrowave_cuda_decoder_decode,
+ * _decode_blocks, _decode_packets, _decode_pyramid; waits for it). The inverse
+ * transform loads interior tiles with the tensor-memory accelerator and gives
+ * up a tile whose load does not complete within a bounded wait; such a frame
+ * is not valid. Returns PYROWAVE_ERROR_GENERIC and sets bit 0 of *error_bits
+ * (may be NULL) when that happened, PYROWAVE_SUCCESS otherwise.
+ * pyrowave_decoder_decode_cpu_buffer_synchronous and
+ * pyrowave_cuda_decoder_get_packet_status report the same condition through
+ * their own result. No counterpart in the reference (its Vulkan decode has no
+ * bounded waits). */
+PYROWAVE_PUBLIC_API pyrowave_result pyrowave_cuda_decoder_get_error(pyrowave_decoder decoder, uint32_t *error_bits);
+
 /* Copy the last decode's dequantised pyramid (canonical layout, device memory). */
 PYROWAVE_PUBLIC_API pyrowave_result pyrowave_cuda_decoder_read_wavelet(pyrowave_decoder decoder, float *pyramid,
                                                                        pyrowave_cuda_stream stream);
@@ -195,9 +207,14 @@ PYROWAVE_PUBLIC_API pyrowave_result pyrowave_cuda_decoder_decode_pyramid(pyrowav
  * every coefficient the inverse transform reads is written earlier in the
  * same call (a missing block decodes as zeros).
  *
- * First call: on each device, the first call (with that device current)
- * looks up the array's device address once. Make that first call before any
- * stream capture is in progress, for example with a small decode at start-up.
+ * Device address: every call looks up the array's address on the current
+ * device (cudaGetSymbolAddress), which allocates nothing once the library's
+ * device code is loaded there. With lazy module loading, the CUDA default,
+ * the first call on a device is where CUDA loads that code and reserves the
+ * array: that call can fail, with PYROWAVE_ERROR_OUT_OF_DEVICE_MEMORY when
+ * the device has no room for it. Make that first call before any stream
+ * capture is in progress, for example with a small decode at start-up. After
+ * a device reset the next call looks the array up again.
  *
  * Overlapping calls race: every call on a device uses the same array, so two
  * calls whose work can overlap on the GPU (different streams without an event
@@ -269,14 +286,18 @@ PYROWAVE_PUBLIC_API pyrowave_result pyrowave_cuda_batch_autotune(pyrowave_cuda_b
  * Serving loop: continuous batching of encode + decode requests from many
  * video streams on one GPU. No counterpart in the reference.
  *
- * Each open stream owns device-resident encoder and decoder state, reserved
- * from a memory pool when the stream is opened (admission by memory: a stream
- * that does not fit is refused with PYROWAVE_ERROR_OUT_OF_DEVICE_MEMORY until
- * others close). Submitted frames are queued; a dispatcher thread starts every
- * frame whose stream is idle as soon as one of `max_in_flight` CUDA streams is
- * free, so the kernels of different requests overlap on the device. Frames of
- * one stream run in submission order; each result is the same as encoding and
- * decoding that stream alone. */
+ * Each stream's state is a device-resident working set: an encoder and a
+ * decoder with their buffers, which stays on the device between the stream's
+ * frames. Requests are admitted by memory: a frame whose stream has no working
+ * set starts only once the memory pool has room for one, after releasing the
+ * working sets of idle streams (least recently used first) if needed; until
+ * then it waits in its stream's queue while other requests run. Submitted
+ * frames are queued per stream; a dispatcher thread starts every frame whose
+ * stream is idle as soon as one of `max_in_flight` CUDA streams is free and
+ * admission allows, so the kernels of different requests overlap on the
+ * device. Frames of one stream run in submission order; each result is the
+ * same as encoding and decoding that stream alone, also when its working set
+ * was released and created again between frames. */
 typedef struct pyrowave_cuda_server_opaque *pyrowave_cuda_server;
 
 typedef struct pyrowave_cuda_server_info
@@ -300,6 +321,9 @@ PYROWAVE_PUBLIC_API pyrowave_result pyrowave_cuda_server_create(pyrowave_device 
 /* Waits for every submitted frame, then frees everything. */
 PYROWAVE_PUBLIC_API void pyrowave_cuda_server_destroy(pyrowave_cuda_server server);
 
+/* Opens a stream. PYROWAVE_ERROR_OUT_OF_DEVICE_MEMORY when one working set
+ * of this frame size and budget is larger than the whole pool; no memory is
+ * taken until the stream's first frame is admitted. */
 PYROWAVE_PUBLIC_API pyrowave_result pyrowave_cuda_server_open_stream(pyrowave_cuda_server server, int width, int height,
                                                                      pyrowave_chroma_subsampling chroma,
                                                                      size_t maximum_bitstream_size,
@@ -309,7 +333,10 @@ PYROWAVE_PUBLIC_API pyrowave_result pyrowave_cuda_server_close_stream(pyrowave_c
 
 /* Queue one frame: encode `input` (device planes) within `budget` bytes, then
  * decode the new bitstream into `output` (device planes, may be NULL). Both
- * buffers must stay valid until the completion is reported. Thread-safe. */
+ * buffers must stay valid until the completion is reported. Thread-safe.
+ * Finished requests wait for pyrowave_cuda_server_poll: with 2^20 requests
+ * queued, running or finished but not yet polled, submit refuses more with
+ * PYROWAVE_ERROR_OUT_OF_HOST_MEMORY. */
 PYROWAVE_PUBLIC_API pyrowave_result pyrowave_cuda_server_submit(pyrowave_cuda_server server, uint32_t stream_id,
                                                                 const pyrowave_cuda_planes *input, size_t budget,
                                                                 const pyrowave_cuda_planes *output,
@@ -320,6 +347,11 @@ PYROWAVE_PUBLIC_API pyrowave_result pyrowave_cuda_server_poll(pyrowave_cuda_serv
                                                               pyrowave_cuda_server_completion *completions,
                                                               uint32_t capacity, uint32_t *count,
                                                               uint32_t timeout_us);
+
+/* Pool bytes held by working sets now and at most so far, and how many
+ * working sets were released to admit another stream's frame. */
+PYROWAVE_PUBLIC_API pyrowave_result pyrowave_cuda_server_get_memory(pyrowave_cuda_server server, size_t *used_bytes,
+                                                                    size_t *peak_bytes, uint64_t *releases);
 
 /* Latency percentiles (microseconds) and count of the requests finished since
  * the last reset. The percentiles cover the most recent 2^20 of those requests. */

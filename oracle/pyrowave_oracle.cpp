@@ -281,7 +281,7 @@ template <typename T> struct Plane
 	T at(int x, int y) const { return data[size_t(y) * size_t(width) + size_t(x)]; }
 };
 
-// One forward level (dwt.comp:307-346): H lifting on every needed row, then V
+// One forward level (dwt.comp:195-233): H lifting on every needed row, then V
 // lifting on every column. Returns LL, HL, LH, HH of size (aligned/2)^2.
 // round16: reference precision-1 FP16 staging (dwt_common.h:44-47).
 template <typename T>
@@ -1783,7 +1783,7 @@ int oracle_parser_total_blocks(const oracle_parser *p) { return p->total_blocks_
 
 // pyrowave_decoder.cpp:280-381: dequant every band. Storage rounding: F32 mode
 // follows the level mask; REF16 mode stores levels 0-1 in FP16 (the reference's
-// precision 1 images, pyrowave_common.cpp:354-378).
+// precision 1 images, pyrowave_common.cpp:133-170).
 int oracle_dequant(const oracle_codec *c, const uint32_t *offsets, const uint32_t *payload, size_t payload_words, int mode,
                    float *out)
 {

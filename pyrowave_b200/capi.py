@@ -60,12 +60,12 @@ API_SYMBOLS = [
     "pyrowave_cuda_encoder_read_wavelet", "pyrowave_cuda_encoder_read_debug", "pyrowave_cuda_decoder_decode",
     "pyrowave_cuda_decoder_decode_blocks", "pyrowave_cuda_decoder_read_wavelet", "pyrowave_cuda_decoder_decode_pyramid",
     "pyrowave_cuda_decoder_decode_packets", "pyrowave_cuda_decoder_get_packet_status",
-    "pyrowave_cuda_decode_blocks_static",
+    "pyrowave_cuda_decoder_get_error", "pyrowave_cuda_decode_blocks_static",
     "pyrowave_cuda_batch_create", "pyrowave_cuda_batch_destroy", "pyrowave_cuda_batch_encode",
     "pyrowave_cuda_batch_get_device_bitstream", "pyrowave_cuda_batch_get_sizes", "pyrowave_cuda_batch_autotune",
     "pyrowave_cuda_server_create", "pyrowave_cuda_server_destroy", "pyrowave_cuda_server_open_stream",
     "pyrowave_cuda_server_close_stream", "pyrowave_cuda_server_submit", "pyrowave_cuda_server_poll",
-    "pyrowave_cuda_server_stats",
+    "pyrowave_cuda_server_stats", "pyrowave_cuda_server_get_memory",
 ]
 
 # Coefficient storage limit of pyrowave_cuda_decode_blocks_static (PYROWAVE_CUDA_STATIC_DECODE_SCRATCH_BYTES).
@@ -201,6 +201,7 @@ def lib():
     L.pyrowave_cuda_decoder_decode_packets.argtypes = [c_void_p, c_void_p, c_size_t, c_void_p, c_uint32,
                                                        POINTER(CudaPlanes), c_void_p]
     L.pyrowave_cuda_decoder_get_packet_status.argtypes = [c_void_p, POINTER(PacketStatus)]
+    L.pyrowave_cuda_decoder_get_error.argtypes = [c_void_p, POINTER(c_uint32)]
     L.pyrowave_cuda_decoder_decode_pyramid.argtypes = [c_void_p, c_void_p, POINTER(CudaPlanes), c_void_p]
     L.pyrowave_cuda_decode_blocks_static.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_int, c_void_p, c_void_p,
                                                      c_size_t, POINTER(CudaPlanes), c_void_p]
@@ -224,6 +225,8 @@ def lib():
                                             c_uint32]
     L.pyrowave_cuda_server_stats.argtypes = [c_void_p, POINTER(ctypes.c_double), POINTER(ctypes.c_double),
                                              POINTER(ctypes.c_uint64), c_bool]
+    L.pyrowave_cuda_server_get_memory.argtypes = [c_void_p, POINTER(c_size_t), POINTER(c_size_t),
+                                                  POINTER(ctypes.c_uint64)]
     for name in API_SYMBOLS:
         getattr(L, name)  # every declared entry point must resolve
     _lib = L
@@ -483,6 +486,12 @@ class Decoder:
         return self.L.pyrowave_cuda_decoder_decode_packets(self.h, c_void_p(data_ptr), data_size, c_void_p(packets_ptr),
                                                            count, ctypes.byref(cp), c_void_p(stream))
 
+    def error(self):
+        """pyrowave_cuda_decoder_get_error: (result code, error bits) of the last decode (waits for it)."""
+        bits = c_uint32(0)
+        code = self.L.pyrowave_cuda_decoder_get_error(self.h, ctypes.byref(bits))
+        return code, int(bits.value)
+
     def packet_status(self) -> PacketStatus:
         st = PacketStatus()
         check(self.L.pyrowave_cuda_decoder_get_packet_status(self.h, ctypes.byref(st)), "get_packet_status")
@@ -614,6 +623,13 @@ class Server:
         check(self.L.pyrowave_cuda_server_poll(self.h, arr, capacity, ctypes.byref(n), timeout_us), "server_poll")
         return [(arr[i].request_id, arr[i].stream_id, arr[i].result, arr[i].bytes, arr[i].latency_us)
                 for i in range(n.value)]
+
+    def memory(self):
+        """(pool bytes in use, peak, working sets released to admit other streams' frames)."""
+        used, peak, rel = c_size_t(), c_size_t(), ctypes.c_uint64()
+        check(self.L.pyrowave_cuda_server_get_memory(self.h, ctypes.byref(used), ctypes.byref(peak),
+                                                     ctypes.byref(rel)), "server_get_memory")
+        return used.value, peak.value, rel.value
 
     def stats(self, reset: bool = False):
         p50, p99, frames = ctypes.c_double(), ctypes.c_double(), ctypes.c_uint64()

@@ -74,8 +74,11 @@ __device__ __forceinline__ void store_coef(float *c32, __half *c16, bool fp16, i
 }
 
 // One 32x32 block per 128-thread CTA; thread = one 4x2 sub-block (the
-// reference's mapping, wavelet_dequant.comp:222-238).
-__device__ __forceinline__ void dequant_body(const BlockParams &p, const DecodeInput &in, const int blk)
+// reference's mapping, wavelet_dequant.comp:222-238). The CTA with
+// `clear_error` set clears the decode's error word: every inverse level runs
+// after the dequantiser has completed, so the clear precedes any error report.
+__device__ __forceinline__ void dequant_body(const BlockParams &p, const DecodeInput &in, const int blk,
+                                             const bool clear_error)
 {
 	__shared__ uint32_t s_words[kMaxBlockWords];
 	__shared__ uint32_t s_plane_off[16];
@@ -93,6 +96,8 @@ __device__ __forceinline__ void dequant_body(const BlockParams &p, const DecodeI
 	const int grp = ly * 4 + lx;
 	const int ox = bx32 * 32 + lx * 8 + sub_x(sub), oy = by32 * 32 + ly * 8 + sub_y(sub);
 	pdl_wait();
+	if (clear_error && t == 0 && in.error)
+		*in.error = 0u;
 
 	uint32_t off, words = 0;
 	const bool sized_by_header = in.offsets || in.keys;
@@ -274,7 +279,7 @@ __device__ __forceinline__ void dequant_body(const BlockParams &p, const DecodeI
 
 __global__ void __launch_bounds__(128) dequant_kernel(const BlockParams p, const DecodeInput in, const int first)
 {
-	dequant_body(p, in, first + int(blockIdx.x));
+	dequant_body(p, in, first + int(blockIdx.x), blockIdx.x == 0);
 }
 
 // Batched form: one CTA per (frame, block), decoding the frame's own bitstream.
@@ -287,7 +292,7 @@ __global__ void __launch_bounds__(128) dequant_batch_kernel(const BatchFrame *fr
 	load_params(s_p, frames[f].bp);
 	load_params(s_in, frames[f].di);
 	__syncthreads();
-	dequant_body(s_p, s_in, local);
+	dequant_body(s_p, s_in, local, local == 0);
 }
 
 constexpr int kBandTile = 36; // 32 band samples + 2 on each side
@@ -369,7 +374,7 @@ __device__ __forceinline__ void idwt_body(const LevelParams &p, const DecodeInpu
 			for (int b = 0; b < 4; b++)
 				tma_load_2d(&sh.band[b][0][0], &maps->map, bx0 - kBandCol0, maps->row[comp][b] + by0, &sh.tile_bar);
 		}
-		const bool done = mbarrier_wait(&sh.tile_bar, 0, kTmaMaxPolls);
+		const bool done = mbarrier_wait(&sh.tile_bar, 0, kTmaMaxPolls) && !maps->test_fail_wait;
 		if (__syncthreads_or(!done))
 		{
 			// Give up on this tile: record it, and keep the CTA alive (its shared
@@ -729,44 +734,33 @@ void launch_idwt_batch(const BatchFrame *frames, const BatchFrameIO *io, const u
 // Decode without allocation (pyrowave_cuda_decode_blocks_static).
 //
 // The coefficient pyramid of the decode lives in one file-scope device array
-// instead of memory owned by a decoder object. CUDA reserves the array when
-// this library's device code is loaded on a device; its address is looked up
-// once per device and then passed to the dequantiser and inverse-transform
-// kernels in place of a decoder's storage buffer.
+// instead of memory owned by a decoder object. In host code the array's name
+// only stands in for it: the device address is looked up with
+// cudaGetSymbolAddress, with the caller's device current, on every call. The
+// lookup allocates nothing once this library's device code is loaded on the
+// device; with lazy module loading (the CUDA default) the first lookup on a
+// device is where CUDA reserves the array, so it can fail there for lack of
+// memory. Looking it up each time keeps a device reset (which unloads the
+// module and may move the array) from leaving a stale address behind.
 #include "pyrowave_cuda.h"
-
-#include <mutex>
 
 namespace
 {
 constexpr size_t kStaticScratchBytes = PYROWAVE_CUDA_STATIC_DECODE_SCRATCH_BYTES;
 static __device__ __align__(256) float g_static_pyramid[kStaticScratchBytes / sizeof(float)];
 
-constexpr int kMaxStaticDevices = 64;
-std::mutex g_static_lock;
-float *g_static_pyramid_ptr[kMaxStaticDevices]; // per device ordinal; null until looked up
-
-// Address of the array on the current device (null on failure).
-float *static_pyramid_on_current_device()
+// Device address of the array on the current device, or the failure.
+pyrowave_result static_pyramid_on_current_device(float *&ptr)
 {
-	int dev = -1;
-	if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kMaxStaticDevices)
+	ptr = nullptr;
+	const cudaError_t e = cudaGetSymbolAddress(reinterpret_cast<void **>(&ptr), g_static_pyramid);
+	if (e != cudaSuccess || !ptr)
 	{
 		(void)cudaGetLastError();
-		return nullptr;
+		ptr = nullptr;
+		return e == cudaErrorMemoryAllocation ? PYROWAVE_ERROR_OUT_OF_DEVICE_MEMORY : PYROWAVE_ERROR_GENERIC;
 	}
-	std::lock_guard<std::mutex> hold(g_static_lock);
-	if (!g_static_pyramid_ptr[dev])
-	{
-		float *ptr = nullptr;
-		if (cudaGetSymbolAddress((void **)&ptr, g_static_pyramid) != cudaSuccess || !ptr)
-		{
-			(void)cudaGetLastError();
-			return nullptr;
-		}
-		g_static_pyramid_ptr[dev] = ptr;
-	}
-	return g_static_pyramid_ptr[dev];
+	return PYROWAVE_SUCCESS;
 }
 } // namespace
 
@@ -800,9 +794,10 @@ extern "C" pyrowave_result pyrowave_cuda_decode_blocks_static(int width, int hei
 		out.data[p] = static_cast<uint8_t *>(planes->data[p]);
 		out.pitch[p] = int32_t(planes->row_stride_in_bytes[p]);
 	}
-	float *scratch = static_pyramid_on_current_device();
-	if (!scratch)
-		return PYROWAVE_ERROR_GENERIC;
+	float *scratch = nullptr;
+	const pyrowave_result looked_up = static_pyramid_on_current_device(scratch);
+	if (looked_up != PYROWAVE_SUCCESS)
+		return looked_up;
 
 	DecodeInput in = {};
 	in.block_meta = block_meta;

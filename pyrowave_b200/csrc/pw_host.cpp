@@ -659,6 +659,8 @@ void build_tile_maps(const Geometry &g, const LevelParams (&lp)[kLevels], float 
 			}
 			if (valid && encode_storage_map(m.map, coef32, g.storage_elems32, p.L.pitch, 40, 36))
 				m.valid = valid;
+			const char *fail = getenv("PYROWAVE_TEST_FAIL_TILE_WAIT");
+			m.test_fail_wait = fail && atoi(fail) != 0 ? 1u : 0u;
 		}
 	}
 }
@@ -952,6 +954,16 @@ struct pyrowave_encoder_opaque
 	}
 };
 
+namespace pw
+{
+uint32_t encoder_frames(const pyrowave_encoder_opaque *encoder) { return encoder ? encoder->sequence_count : 0; }
+void encoder_set_frames(pyrowave_encoder_opaque *encoder, uint32_t frames)
+{
+	if (encoder)
+		encoder->sequence_count = frames & 7u;
+}
+} // namespace pw
+
 // Growable array of 32-bit words in page-locked host memory: the parser's
 // payload, uploaded without a staging copy when the caller waits for the decode.
 struct PinnedWords
@@ -1021,7 +1033,10 @@ struct pyrowave_decoder_opaque
 	KernelNode node_idwt_full[kLevels], node_idwt_only[kLevels];
 
 	LevelTileMap band_maps[kLevels] = {}; // TMA maps of the FP32 bands (inverse transform tile loads)
-	uint32_t *error_d = nullptr;     // kDecodeError* bits
+	uint32_t *error_d = nullptr;     // kDecodeError* bits of the last decode (cleared by each decode)
+	uint32_t *h_error = nullptr;     // page-locked copy of error_d
+	cudaEvent_t decode_done = nullptr; // recorded after every decode launch
+	bool decode_pending = false;
 	// Device-side packet assembly (pw_packets.cu): per-packet tables, grown on demand.
 	uint32_t *pk_tables = nullptr;
 	uint8_t *pk_state = nullptr;
@@ -1165,6 +1180,12 @@ struct pyrowave_decoder_opaque
 		dev_free(pk_first);
 		dev_free(error_d);
 		error_d = nullptr;
+		host_free(h_error);
+		h_error = nullptr;
+		if (decode_done)
+			cudaEventDestroy(decode_done);
+		decode_done = nullptr;
+		decode_pending = false;
 		dev_free(pk_status);
 		dev_free(pk_counter);
 		host_free(pk_status_h);
@@ -1217,8 +1238,11 @@ struct pyrowave_decoder_opaque
 		}
 		cudaMemcpy(jobs_d, jobs.data(), jobs.size() * 4, cudaMemcpyHostToDevice);
 		error_d = dev_alloc<uint32_t>(1, ok);
+		h_error = host_alloc<uint32_t>(1, ok);
 		if (error_d)
 			cudaMemset(error_d, 0, sizeof(uint32_t));
+		if (ok && cudaEventCreateWithFlags(&decode_done, cudaEventDisableTiming) != cudaSuccess)
+			ok = false;
 		build_tile_maps(g, lp, coef32, nullptr, band_maps);
 		if (!ok)
 		{
@@ -1292,6 +1316,10 @@ struct pyrowave_decoder_opaque
 			bool ok = true;
 			timing.begin(device, s);
 			const bool pdl = !device->stage_timing; // event nodes between kernels break programmatic edges
+			// The dequantiser clears the error word before any inverse level runs;
+			// without it the graph starts with a clear of its own.
+			if (!dequant)
+				cudaMemsetAsync(error_d, 0, sizeof(uint32_t), s);
 			if (dequant)
 			{
 				launch_dequant(bp, in, 0, g.block_count_32x32, false, s);
@@ -1336,7 +1364,22 @@ struct pyrowave_decoder_opaque
 		if (!cuda_ok(cudaGraphLaunch(graph.exec, s), "cudaGraphLaunch"))
 			return false;
 		timing.launched(device);
+		cudaEventRecord(decode_done, s);
+		decode_pending = true;
 		decoded_frame_for_current_sequence = true;
+		return true;
+	}
+
+	// Error bits of the last decode (waits for it); 0 when none was launched.
+	bool last_error(uint32_t &bits)
+	{
+		bits = 0;
+		if (!decode_pending)
+			return true;
+		if (!cuda_ok(cudaEventSynchronize(decode_done), "cudaEventSynchronize") ||
+		    !cuda_ok(cudaMemcpy(h_error, error_d, sizeof(uint32_t), cudaMemcpyDeviceToHost), "cudaMemcpy"))
+			return false;
+		bits = *h_error;
 		return true;
 	}
 
@@ -1977,7 +2020,11 @@ pyrowave_result pyrowave_decoder_decode_cpu_buffer_synchronous(pyrowave_decoder 
 			cudaMemcpy2DAsync(buffers->data[p], buffers->row_stride_in_bytes[p], decoder->out_planes[p],
 			                  decoder->out_pitch[p], size_t(w), size_t(h), cudaMemcpyDeviceToHost, s);
 	}
+	cudaMemcpyAsync(decoder->h_error, decoder->error_d, sizeof(uint32_t), cudaMemcpyDeviceToHost, s);
 	if (cudaStreamSynchronize(s) != cudaSuccess)
+		return PYROWAVE_ERROR_GENERIC;
+	// A tile load of the inverse transform that did not complete in time.
+	if (*decoder->h_error != 0)
 		return PYROWAVE_ERROR_GENERIC;
 	return PYROWAVE_SUCCESS;
 }
@@ -2230,7 +2277,21 @@ pyrowave_result pyrowave_cuda_decoder_get_packet_status(pyrowave_decoder decoder
 	status->total_blocks = st.total_blocks;
 	status->sequence = st.sequence;
 	status->invalid_packets = st.invalid_packets;
+	uint32_t bits = 0;
+	if (!decoder->last_error(bits) || bits != 0)
+		return PYROWAVE_ERROR_GENERIC;
 	return PYROWAVE_SUCCESS;
+}
+
+pyrowave_result pyrowave_cuda_decoder_get_error(pyrowave_decoder decoder, uint32_t *error_bits)
+{
+	if (!decoder)
+		return PYROWAVE_ERROR_INVALID_ARGUMENT;
+	uint32_t bits = 0;
+	const bool ok = decoder->last_error(bits);
+	if (error_bits)
+		*error_bits = bits;
+	return ok && bits == 0 ? PYROWAVE_SUCCESS : PYROWAVE_ERROR_GENERIC;
 }
 
 pyrowave_result pyrowave_cuda_decoder_read_wavelet(pyrowave_decoder decoder, float *pyramid, pyrowave_cuda_stream stream)
@@ -2300,7 +2361,10 @@ struct pyrowave_cuda_batch_opaque
 	cudaEvent_t io_free[2] = {};
 	int slot = 0;
 	RateControlState *rc_d = nullptr;
-	uint32_t *h_totals = nullptr; // {error, total_words} per frame
+	// Per frame, the words of RateControlState from `error` to `decode_error`.
+	static constexpr int kTotalsWords =
+	    int((offsetof(RateControlState, decode_error) - offsetof(RateControlState, error)) / 4) + 1;
+	uint32_t *h_totals = nullptr;
 	cudaStream_t last_stream = nullptr;
 	bool has_result = false;
 
@@ -2500,9 +2564,9 @@ struct pyrowave_cuda_batch_opaque
 		if (!cuda_ok(cudaGraphLaunch(graphs[k][outputs ? 1 : 0].exec, s), "cudaGraphLaunch") ||
 		    !cuda_ok(cudaEventRecord(io_free[k], s), "cudaEventRecord"))
 			return PYROWAVE_ERROR_GENERIC;
-		// {error, total_words} of every frame, for get_sizes.
-		if (!cuda_ok(cudaMemcpy2DAsync(h_totals, 8, &rc_d[0].error, sizeof(RateControlState), 8, size_t(count),
-		                               cudaMemcpyDeviceToHost, s),
+		// {error, total_words, ..., decode_error} of every frame, for get_sizes.
+		if (!cuda_ok(cudaMemcpy2DAsync(h_totals, kTotalsWords * 4, &rc_d[0].error, sizeof(RateControlState),
+		                               kTotalsWords * 4, size_t(count), cudaMemcpyDeviceToHost, s),
 		             "cudaMemcpy2DAsync"))
 			return PYROWAVE_ERROR_GENERIC;
 		last_stream = s;
@@ -2575,7 +2639,7 @@ pyrowave_result pyrowave_cuda_batch_create(pyrowave_device device, const pyrowav
 		DecodeInput &di = fr.di;
 		di.offsets = nullptr;
 		di.keys = nullptr;
-		di.error = nullptr;
+		di.error = eb.rc ? &eb.rc->decode_error : nullptr;
 		di.block_meta = eb.block_meta;
 		di.payload = eb.stream ? eb.stream + 2 : nullptr;
 		di.payload_words = b->capacity_words[f] - 2;
@@ -2600,7 +2664,7 @@ pyrowave_result pyrowave_cuda_batch_create(pyrowave_device device, const pyrowav
 		b->io_h[i] = host_alloc<BatchFrameIO>(count, ok);
 		ok = ok && cudaEventCreateWithFlags(&b->io_free[i], cudaEventDisableTiming) == cudaSuccess;
 	}
-	b->h_totals = host_alloc<uint32_t>(size_t(count) * 2, ok);
+	b->h_totals = host_alloc<uint32_t>(size_t(count) * pyrowave_cuda_batch_opaque::kTotalsWords, ok);
 	if (!ok)
 	{
 		(void)cudaGetLastError();
@@ -2656,9 +2720,11 @@ pyrowave_result pyrowave_cuda_batch_get_sizes(pyrowave_cuda_batch batch, size_t 
 		return PYROWAVE_ERROR_GENERIC;
 	for (int f = 0; f < batch->count; f++)
 	{
-		if (batch->h_totals[2 * f] != 0)
-			return PYROWAVE_ERROR_GENERIC; // device-side consistency check failed
-		bytes[f] = 8 + size_t(batch->h_totals[2 * f + 1]) * 4;
+		const uint32_t *t = batch->h_totals + size_t(f) * pyrowave_cuda_batch_opaque::kTotalsWords;
+		// Encoder consistency check, or a decode tile load that did not complete in time.
+		if (t[0] != 0 || t[pyrowave_cuda_batch_opaque::kTotalsWords - 1] != 0)
+			return PYROWAVE_ERROR_GENERIC;
+		bytes[f] = 8 + size_t(t[1]) * 4;
 	}
 	return PYROWAVE_SUCCESS;
 }

@@ -20,12 +20,19 @@
 #include <cuda_runtime.h>
 
 struct pyrowave_device_opaque;
+struct pyrowave_encoder_opaque;
 
 namespace pw
 {
 // The CUDA device a pyrowave_device was created on. Library threads of their
 // own (the serving loop's dispatcher) make it current before any CUDA call.
 int device_ordinal(const pyrowave_device_opaque *device);
+
+// An encoder's frame counter (mod 8, the 3-bit sequence number of its last
+// frame). The serving loop carries a stream's counter over to a new encoder
+// when the stream's working set was released and is created again.
+uint32_t encoder_frames(const pyrowave_encoder_opaque *encoder);
+void encoder_set_frames(pyrowave_encoder_opaque *encoder, uint32_t frames);
 
 constexpr int kLevels = 5;
 constexpr int kComponents = 3;
@@ -126,7 +133,7 @@ struct RateControlState
 	int32_t xstar;                 // first partially applied bucket*16+subdivision (-1 none)
 	uint32_t block_cut;            // ops of blocks >= this in the partial subdivision are not applied
 	uint32_t sequence;
-	uint32_t pad;
+	uint32_t decode_error;         // kDecodeError* bits of the batched form's decode of this frame
 	// Per resolve slice: words << 32 | non-empty blocks << 1 | 1 once published.
 	unsigned long long slice_total[kMaxResolveSlices];
 };
@@ -167,6 +174,11 @@ struct alignas(64) LevelTileMap
 	CUtensorMap map;
 	uint32_t valid;     // bit c: component c's interior tiles load through the map
 	int32_t row[3][4];  // first row of band b of component c (forward: the LL input, b = 0)
+	// Fault injection for tests (inverse maps only): every tile load that
+	// completes is handled as if its bounded wait had run out, which exercises
+	// the error report without stalling the GPU. Set from the environment
+	// variable PYROWAVE_TEST_FAIL_TILE_WAIT=1 when a decoder builds its maps.
+	uint32_t test_fail_wait;
 };
 // The batched form's maps of one level, per frame (frames past the table use
 // plain loads).

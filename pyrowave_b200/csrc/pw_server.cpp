@@ -1,12 +1,16 @@
 // Serving loop: continuous batching of encode + decode requests from many
 // video streams on one GPU, built on the library's own C API.
 //
-// Each open stream owns a pyrowave_encoder and a pyrowave_decoder (their
-// device buffers are the stream's state). Streams are admitted against a
-// memory pool; requests wait in per-stream FIFO queues. A dispatcher thread
-// starts the head request of every idle stream as soon as one of the server's
-// CUDA streams is free and completes requests by polling one event per CUDA
-// stream, so requests that arrive while others run are admitted immediately
+// Each stream's device state is a working set: a pyrowave_encoder and a
+// pyrowave_decoder with their device buffers and captured graphs. It stays
+// resident between the stream's frames. Requests wait in per-stream FIFO
+// queues and are admitted by memory: a request whose stream has no working set
+// starts only when the pool has room for one, after releasing the working sets
+// of idle streams, least recently used first, if needed; otherwise it waits
+// until a running request completes. A dispatcher thread starts the head
+// request of every idle stream as soon as one of the server's CUDA streams is
+// free and admission allows, and completes requests by polling one event per
+// CUDA stream, so requests that arrive while others run are admitted at once
 // and their kernels overlap on the device.
 #include "pw_internal.h"
 
@@ -57,9 +61,14 @@ struct Request
 struct VideoStream
 {
 	uint32_t id = 0;
+	int width = 0, height = 0;
+	pyrowave_chroma_subsampling chroma = PYROWAVE_CHROMA_SUBSAMPLING_420;
+	// Working set (null while released); `bytes` is what it takes from the pool.
 	pyrowave_encoder encoder = nullptr;
 	pyrowave_decoder decoder = nullptr;
 	size_t bytes = 0;
+	uint32_t frames = 0;    // frames encoded (mod 8): carried over when the working set is re-created
+	uint64_t last_use = 0;  // admission tick of the last frame (least recently used release order)
 	std::deque<Request> queue;
 	bool busy = false;    // a frame of this stream is on the GPU
 	bool closing = false; // free once the queue drains
@@ -82,7 +91,14 @@ struct pyrowave_cuda_server_opaque
 	std::map<uint32_t, std::unique_ptr<VideoStream>> streams;
 	uint32_t next_stream = 1;
 	uint64_t next_request = 1;
+	uint64_t tick = 0;
+	size_t peak_used = 0;
+	uint64_t releases = 0; // working sets released to admit another stream's request
 	std::deque<pyrowave_cuda_server_completion> completed;
+	// Finished requests not yet polled plus requests not yet finished: submit
+	// refuses new requests beyond this, so a caller that never polls cannot grow
+	// the completion queue without bound.
+	static constexpr size_t kMaxOutstanding = size_t(1) << 20;
 	// Latencies since the last stats reset: the most recent kLatencySamples in a
 	// ring, so a server that never resets its statistics stays bounded.
 	static constexpr size_t kLatencySamples = size_t(1) << 20;
@@ -95,8 +111,12 @@ struct pyrowave_cuda_server_opaque
 	size_t pending = 0; // queued + in flight
 	std::thread dispatcher;
 
-	void free_stream(VideoStream &vs)
+	// Releases a stream's working set (its encoder and decoder) back to the pool.
+	void release_working_set(VideoStream &vs)
 	{
+		if (!vs.encoder && !vs.decoder)
+			return;
+		vs.frames = encoder_frames(vs.encoder);
 		if (vs.encoder)
 			pyrowave_encoder_destroy(vs.encoder);
 		if (vs.decoder)
@@ -106,9 +126,52 @@ struct pyrowave_cuda_server_opaque
 		used -= vs.bytes;
 	}
 
-	// Start a request on a free slot (called with the lock held).
+	// Admission by memory (called with the lock held): gives the stream a
+	// working set if it has none, releasing idle streams' working sets (least
+	// recently used first) while the pool lacks room. False: the request waits.
+	bool admit(VideoStream &vs)
+	{
+		if (vs.encoder)
+			return true;
+		while (used + vs.bytes > pool)
+		{
+			VideoStream *victim = nullptr;
+			for (auto &kv : streams)
+			{
+				VideoStream &o = *kv.second;
+				if (&o != &vs && o.encoder && !o.busy && (!victim || o.last_use < victim->last_use))
+					victim = &o;
+			}
+			if (!victim)
+				return false;
+			release_working_set(*victim);
+			releases++;
+		}
+		pyrowave_encoder_create_info ei = {device, vs.width, vs.height, vs.chroma};
+		pyrowave_decoder_create_info di = {};
+		di.device = device;
+		di.width = vs.width;
+		di.height = vs.height;
+		di.chroma = vs.chroma;
+		if (pyrowave_encoder_create(&ei, &vs.encoder) != PYROWAVE_SUCCESS ||
+		    pyrowave_decoder_create(&di, &vs.decoder) != PYROWAVE_SUCCESS)
+		{
+			if (vs.encoder)
+				pyrowave_encoder_destroy(vs.encoder);
+			vs.encoder = nullptr;
+			vs.decoder = nullptr;
+			return false;
+		}
+		encoder_set_frames(vs.encoder, vs.frames);
+		used += vs.bytes;
+		peak_used = std::max(peak_used, used);
+		return true;
+	}
+
+	// Start a request on a free slot (called with the lock held, after admit()).
 	void start(Slot &slot, VideoStream &vs)
 	{
+		vs.last_use = ++tick;
 		Request r = vs.queue.front();
 		vs.queue.pop_front();
 		vs.busy = true;
@@ -143,6 +206,9 @@ struct pyrowave_cuda_server_opaque
 			size_t bytes = 0;
 			c.result = pyrowave_cuda_encoder_get_size(vs.encoder, &bytes);
 			c.bytes = bytes;
+			// The decode's own outcome (its event completed with the slot's).
+			if (c.result == PYROWAVE_SUCCESS && slot.req.decode)
+				c.result = pyrowave_cuda_decoder_get_error(vs.decoder, nullptr);
 		}
 		c.latency_us = std::chrono::duration<double, std::micro>(Clock::now() - slot.req.submitted).count();
 		completed.push_back(c);
@@ -188,7 +254,7 @@ struct pyrowave_cuda_server_opaque
 				VideoStream &vs = *it->second;
 				if (vs.closing && !vs.busy && vs.queue.empty())
 				{
-					free_stream(vs);
+					release_working_set(vs);
 					it = streams.erase(it);
 					progress = true;
 				}
@@ -211,6 +277,8 @@ struct pyrowave_cuda_server_opaque
 					auto free_slot = std::find_if(slots.begin(), slots.end(), [](const Slot &s) { return !s.busy; });
 					if (free_slot == slots.end())
 						break;
+					if (!admit(vs))
+						continue; // no memory until a running request completes
 					start(*free_slot, vs);
 					progress = true;
 				}
@@ -274,7 +342,7 @@ void pyrowave_cuda_server_destroy(pyrowave_cuda_server server)
 	}
 	server->dispatcher.join();
 	for (auto &kv : server->streams)
-		server->free_stream(*kv.second);
+		server->release_working_set(*kv.second);
 	for (Slot &s : server->slots)
 	{
 		cudaStreamDestroy(s.stream);
@@ -300,27 +368,16 @@ pyrowave_result pyrowave_cuda_server_open_stream(pyrowave_cuda_server server, in
 		return PYROWAVE_ERROR_INVALID_ARGUMENT;
 	const size_t bytes = stream_state_bytes(g, size_t((target >= 8 ? target - 8 : target) / 4) + 2);
 	std::lock_guard<std::mutex> guard(server->lock);
-	if (server->used + bytes > server->pool)
+	// A stream whose working set can never fit the pool is refused; any other
+	// is opened, and its requests are admitted as memory allows.
+	if (bytes > server->pool)
 		return PYROWAVE_ERROR_OUT_OF_DEVICE_MEMORY;
 	auto vs = std::make_unique<VideoStream>();
-	pyrowave_encoder_create_info ei = {server->device, width, height, chroma};
-	pyrowave_decoder_create_info di = {};
-	di.device = server->device;
-	di.width = width;
-	di.height = height;
-	di.chroma = chroma;
-	pyrowave_result r = pyrowave_encoder_create(&ei, &vs->encoder);
-	if (r == PYROWAVE_SUCCESS)
-		r = pyrowave_decoder_create(&di, &vs->decoder);
-	if (r != PYROWAVE_SUCCESS)
-	{
-		if (vs->encoder)
-			pyrowave_encoder_destroy(vs->encoder);
-		return r;
-	}
+	vs->width = width;
+	vs->height = height;
+	vs->chroma = chroma;
 	vs->id = server->next_stream++;
 	vs->bytes = bytes;
-	server->used += bytes;
 	*stream_id = vs->id;
 	server->streams[vs->id] = std::move(vs);
 	return PYROWAVE_SUCCESS;
@@ -357,6 +414,8 @@ pyrowave_result pyrowave_cuda_server_submit(pyrowave_cuda_server server, uint32_
 	auto it = server->streams.find(stream_id);
 	if (it == server->streams.end() || it->second->closing)
 		return PYROWAVE_ERROR_INVALID_ARGUMENT;
+	if (server->pending + server->completed.size() >= pyrowave_cuda_server_opaque::kMaxOutstanding)
+		return PYROWAVE_ERROR_OUT_OF_HOST_MEMORY; // poll the finished requests first
 	r.id = server->next_request++;
 	it->second->queue.push_back(r);
 	server->pending++;
@@ -382,6 +441,21 @@ pyrowave_result pyrowave_cuda_server_poll(pyrowave_cuda_server server, pyrowave_
 		server->completed.pop_front();
 	}
 	*count = n;
+	return PYROWAVE_SUCCESS;
+}
+
+pyrowave_result pyrowave_cuda_server_get_memory(pyrowave_cuda_server server, size_t *used_bytes,
+                                                size_t *peak_bytes, uint64_t *releases)
+{
+	if (!server)
+		return PYROWAVE_ERROR_INVALID_ARGUMENT;
+	std::lock_guard<std::mutex> g(server->lock);
+	if (used_bytes)
+		*used_bytes = server->used;
+	if (peak_bytes)
+		*peak_bytes = server->peak_used;
+	if (releases)
+		*releases = server->releases;
 	return PYROWAVE_SUCCESS;
 }
 

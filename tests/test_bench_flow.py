@@ -23,17 +23,18 @@ if ROOT not in sys.path:
 import bench  # noqa: E402
 
 STEP_MS = 0.1
+_clock = [0.0]  # fake device time: every encode_device call (one step) takes STEP_MS
 
 
 class _Event:
     def __init__(self, enable_timing=False):
-        pass
+        self.t = 0.0
 
     def record(self, stream=None):
-        pass
+        self.t = _clock[0]
 
     def elapsed_time(self, other):
-        return STEP_MS
+        return other.t - self.t
 
 
 class _Stream:
@@ -48,6 +49,7 @@ class _Coder:
 
     def encode_device(self, *a):
         _Coder.calls += 1
+        _clock[0] += STEP_MS
 
     def device_bitstream(self):
         return 0, 0, 1000
@@ -84,7 +86,8 @@ def fake_gpu(monkeypatch):
     monkeypatch.setattr(capi, "Device", _Coder)
     monkeypatch.setattr(capi, "Encoder", _Coder)
     monkeypatch.setattr(capi, "Decoder", _Coder)
-    monkeypatch.setattr(bench, "run_e2e", lambda *a: {"total_s": 0.004, "frames": 10, "h2d": 55296, "d2h": 55296})
+    monkeypatch.setattr(bench, "run_e2e", lambda *a: {"total_s": 0.004, "frames": 10, "h2d": 55296, "d2h": 55296,
+                                                      "method": "stand-in", "breakdown_us": {}})
     monkeypatch.setattr(bench, "ClockSampler", _NoClocks)
 
 

@@ -1,22 +1,33 @@
-"""The batched form: frames of mixed sizes, chroma formats and budgets through
-one graph launch per call give the same bitstreams and decoded planes as the
-single-frame encoder and decoder, before and after autotuning."""
+"""The batched form against the oracle: frames of mixed sizes, chroma formats
+and budgets coded in one call give, frame by frame, the oracle's packetized
+bitstream and decoded planes, before and after autotuning.
+
+The main case is the batched benchmark's frame set: the six sizes 1280x720,
+1366x768, 1920x1080, 2560x1080, 2560x1440 and 3840x2160, in 4:2:0 and 4:4:4,
+with budgets drawn from 150-250 Mbit/s at 60 frames/s."""
+import concurrent.futures
+
 import numpy as np
 import pytest
 
+from oracle_codec import oracle_frame, words_as_bytes
 from pyrowave_b200 import capi, synth
 
 pytestmark = pytest.mark.gpu
 
-# (width, height, 4:4:4, budget)
-FRAMES = [
-    (1280, 720, False, 150000),
-    (130, 98, False, 20000),
-    (200, 128, True, 30000),
-    (640, 360, True, 60000),
-    (34, 30, False, 65536),
-    (1366, 768, False, 200000),
-]
+SIZES = [(1280, 720), (1366, 768), (1920, 1080), (2560, 1080), (2560, 1440), (3840, 2160)]
+
+
+def _frame_set():
+    rng = np.random.default_rng(17)
+    out = []
+    for c444 in (False, True):
+        for w, h in SIZES:
+            out.append((w, h, c444, int(rng.uniform(150e6, 250e6) / 8 / 60) & ~3))
+    return out
+
+
+FRAMES = _frame_set()
 
 
 @pytest.fixture(scope="module")
@@ -26,38 +37,8 @@ def device(gpu):
     dev.close()
 
 
-def _inputs(seed_base):
-    import torch
-
-    planes = [synth.synth_frame(w, h, c444, seed_base + i) for i, (w, h, c444, _) in enumerate(FRAMES)]
-    dev_planes = [[torch.from_numpy(p).cuda() for p in pl] for pl in planes]
-    return planes, dev_planes
-
-
 def _ptrs(tensors):
     return [[t.data_ptr() for t in ts] for ts in tensors], [[t.stride(0) for t in ts] for ts in tensors]
-
-
-def _reference(device, dev_planes, budgets, calls):
-    """Single-frame encoders run `calls` times (same budgets); returns the last stream bytes and decodes."""
-    import torch
-
-    streams, decoded = [], []
-    for (w, h, c444, _), pl, budget in zip(FRAMES, dev_planes, budgets):
-        chroma = capi.CHROMA_444 if c444 else capi.CHROMA_420
-        enc = capi.Encoder(device, w, h, chroma)
-        for _ in range(calls):
-            enc.encode_device([p.data_ptr() for p in pl], [p.stride(0) for p in pl], budget)
-        torch.cuda.synchronize()
-        n = enc.size()
-        s, m, _ = enc.device_bitstream()
-        streams.append(_copy_device_words(s, n // 4))
-        dec = capi.Decoder(device, w, h, chroma)
-        outs = [torch.zeros_like(p) for p in pl]
-        dec.decode_blocks(m, s + 8, n // 4 - 2, [t.data_ptr() for t in outs], [t.stride(0) for t in outs])
-        torch.cuda.synchronize()
-        decoded.append([t.cpu().numpy() for t in outs])
-    return streams, decoded
 
 
 class _DeviceWords:
@@ -74,12 +55,31 @@ def _copy_device_words(ptr, nwords):
     return t.cpu().numpy().view(np.uint32).copy()
 
 
-def test_batch_matches_single_frame(device):
+def _check_against_oracle(batch, frames, planes, outs, budgets, sequence, what):
+    """Every frame's bitstream and decoded planes equal the oracle's for the same
+    input, budget and sequence number (oracle runs in parallel threads)."""
+    sizes = batch.sizes()
+    with concurrent.futures.ThreadPoolExecutor(8) as ex:
+        want = list(ex.map(lambda i: oracle_frame(frames[i][0], frames[i][1], frames[i][2], planes[i], budgets[i],
+                                                  sequence), range(len(frames))))
+    for i, (data, decoded) in enumerate(want):
+        assert sizes[i] <= budgets[i]
+        assert sizes[i] == data.size, f"{what} frame {i}: {sizes[i]} bytes, oracle {data.size}"
+        s, _ = batch.device_bitstream(i)
+        got = words_as_bytes(_copy_device_words(s, sizes[i] // 4))
+        assert np.array_equal(got, data), f"{what} frame {i}: bitstream differs from the oracle"
+        if outs is not None:
+            for p in range(3):
+                assert np.array_equal(outs[i][p].cpu().numpy(), decoded[p]), f"{what} frame {i} plane {p}"
+
+
+def test_batch_matches_oracle(device):
     import torch
 
-    planes, dev_planes = _inputs(40)
+    planes = [synth.synth_frame(w, h, c444, 40 + i) for i, (w, h, c444, _) in enumerate(FRAMES)]
+    dev_planes = [[torch.from_numpy(p).cuda() for p in pl] for pl in planes]
     budgets = [b for *_, b in FRAMES]
-    infos = [(w, h, capi.CHROMA_444 if c444 else capi.CHROMA_420, 2 * b) for w, h, c444, b in FRAMES]
+    infos = [(w, h, capi.CHROMA_444 if c444 else capi.CHROMA_420, b) for w, h, c444, b in FRAMES]
     batch = capi.Batch(device, infos)
     outs = [[torch.full_like(p, 0x55) for p in pl] for pl in dev_planes]
     in_ptrs, in_strides = _ptrs(dev_planes)
@@ -88,27 +88,39 @@ def test_batch_matches_single_frame(device):
     for call, scale in enumerate([1.0, 0.6]):
         b = [int(x * scale) for x in budgets]
         assert batch.encode(in_ptrs, in_strides, b, out_ptrs, out_strides) == capi.PYROWAVE_SUCCESS
-        sizes = batch.sizes()
-        ref_streams, ref_decoded = _reference(device, dev_planes, b, call + 1)
-        for i in range(len(FRAMES)):
-            assert sizes[i] <= b[i]
-            s, _ = batch.device_bitstream(i)
-            got = _copy_device_words(s, sizes[i] // 4)
-            assert np.array_equal(got, ref_streams[i]), f"frame {i} call {call}: bitstream differs"
-            for p in range(3):
-                assert np.array_equal(outs[i][p].cpu().numpy(), ref_decoded[i][p]), f"frame {i} plane {p}"
+        torch.cuda.synchronize()
+        _check_against_oracle(batch, FRAMES, planes, outs, b, call + 1, f"call {call}")
 
-    # The autotuner may pick other CTA shapes; the next call's output is unchanged.
+    # The autotuner may pick other CTA shapes and does not advance the
+    # sequence numbers; the next call's output is unchanged.
     b = [int(x * 0.8) for x in budgets]
     assert batch.autotune(in_ptrs, in_strides, b, out_ptrs, out_strides) == capi.PYROWAVE_SUCCESS
     assert batch.encode(in_ptrs, in_strides, b, out_ptrs, out_strides) == capi.PYROWAVE_SUCCESS
-    sizes = batch.sizes()
-    ref_streams, ref_decoded = _reference(device, dev_planes, b, 3)
-    for i in range(len(FRAMES)):
-        s, _ = batch.device_bitstream(i)
-        assert np.array_equal(_copy_device_words(s, sizes[i] // 4), ref_streams[i]), f"frame {i} after autotune"
-        for p in range(3):
-            assert np.array_equal(outs[i][p].cpu().numpy(), ref_decoded[i][p])
+    torch.cuda.synchronize()
+    _check_against_oracle(batch, FRAMES, planes, outs, b, 3, "after autotune")
+
+    # Encode only (no outputs): the bitstreams alone.
+    assert batch.encode(in_ptrs, in_strides, budgets, None, None) == capi.PYROWAVE_SUCCESS
+    torch.cuda.synchronize()
+    _check_against_oracle(batch, FRAMES, planes, None, budgets, 4, "encode only")
+    batch.close()
+
+
+def test_batch_small_and_odd_frames(device):
+    """Frames below one 32x32 tile per band and odd sizes, mixed with a larger one."""
+    import torch
+
+    frames = [(34, 30, False, 65536), (130, 98, False, 20000), (200, 128, True, 30000), (640, 360, True, 60000)]
+    planes = [synth.synth_frame(w, h, c444, 70 + i) for i, (w, h, c444, _) in enumerate(frames)]
+    dev_planes = [[torch.from_numpy(p).cuda() for p in pl] for pl in planes]
+    batch = capi.Batch(device, [(w, h, capi.CHROMA_444 if c else capi.CHROMA_420, b) for w, h, c, b in frames])
+    outs = [[torch.zeros_like(p) for p in pl] for pl in dev_planes]
+    in_ptrs, in_strides = _ptrs(dev_planes)
+    out_ptrs, out_strides = _ptrs(outs)
+    budgets = [b for *_, b in frames]
+    assert batch.encode(in_ptrs, in_strides, budgets, out_ptrs, out_strides) == capi.PYROWAVE_SUCCESS
+    torch.cuda.synchronize()
+    _check_against_oracle(batch, frames, planes, outs, budgets, 1, "small frames")
     batch.close()
 
 
@@ -139,7 +151,7 @@ def test_batch_validation(device):
 
 def test_batch_frames_past_tensor_map_table(device):
     """Frames past the batch's per-frame TMA map table (64 frames) load their
-    tiles with plain loads; both kinds match the single-frame path."""
+    tiles with plain loads; both kinds give the oracle's bitstreams and planes."""
     import torch
 
     big = (640, 360, True, 60000)
@@ -153,24 +165,14 @@ def test_batch_frames_past_tensor_map_table(device):
     out_ptrs, out_strides = _ptrs(outs)
     budgets = [b for *_, b in shapes]
     assert batch.encode(in_ptrs, in_strides, budgets, out_ptrs, out_strides) == capi.PYROWAVE_SUCCESS
+    torch.cuda.synchronize()
     sizes = batch.sizes()
-    for i in (0, 64, 65):
+    for i in (0, 1, 63, 64, 65):
         w, h, c444, budget = shapes[i]
-        chroma = capi.CHROMA_444 if c444 else capi.CHROMA_420
-        enc = capi.Encoder(device, w, h, chroma)
-        pl = dev_planes[i]
-        enc.encode_device([p.data_ptr() for p in pl], [p.stride(0) for p in pl], budget)
-        torch.cuda.synchronize()
-        n = enc.size()
-        s, m, _ = enc.device_bitstream()
-        ref = _copy_device_words(s, n // 4)
-        dec = capi.Decoder(device, w, h, chroma)
-        ref_out = [torch.zeros_like(p) for p in pl]
-        dec.decode_blocks(m, s + 8, n // 4 - 2, [t.data_ptr() for t in ref_out], [t.stride(0) for t in ref_out])
-        torch.cuda.synchronize()
+        data, decoded = oracle_frame(w, h, c444, planes[i], budget, 1)
+        assert sizes[i] == data.size
         bs, _ = batch.device_bitstream(i)
-        assert sizes[i] == n
-        assert np.array_equal(_copy_device_words(bs, sizes[i] // 4), ref), f"frame {i}: bitstream differs"
+        assert np.array_equal(words_as_bytes(_copy_device_words(bs, sizes[i] // 4)), data), f"frame {i}"
         for p in range(3):
-            assert np.array_equal(outs[i][p].cpu().numpy(), ref_out[p].cpu().numpy()), f"frame {i} plane {p}"
+            assert np.array_equal(outs[i][p].cpu().numpy(), decoded[p]), f"frame {i} plane {p}"
     batch.close()

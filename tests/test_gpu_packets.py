@@ -1,12 +1,15 @@
 """Device-side packet assembly (pyrowave_cuda_decoder_decode_packets) against the
-host parser (pyrowave_decoder_clear + pyrowave_decoder_push_packet per packet +
-pyrowave_cuda_decoder_decode), whose sequence and first-copy rules follow the
-reference's pyrowave_decoder.cpp:154-262 and are checked against the oracle and
-the reference's own parser elsewhere. Decoded planes must be bit-identical, and
-the readiness and rejected-packet counts must agree."""
+oracle: the oracle parser (a restatement of pyrowave_decoder.cpp:126-262, itself
+pinned to the reference's own compiled parser) fed the same packets in the same
+order, then the oracle's dequantiser and inverse transform. Decoded planes must
+be bit-identical, and the readiness and rejected-packet counts must agree. The
+library's host parser (pyrowave_decoder_clear + pyrowave_decoder_push_packet per
+packet + pyrowave_cuda_decoder_decode) is held to the same answers."""
 import numpy as np
 import pytest
 
+import oracle as O
+from oracle_codec import oracle_decode
 from pyrowave_b200 import capi, synth
 
 pytestmark = pytest.mark.gpu
@@ -102,16 +105,25 @@ def test_device_assembly_matches_host_parser(device, w, h, c444, budget, boundar
     shapes = [p.shape for p in synth.synth_frame(w, h, c444, 3)]
     host = capi.Decoder(device, w, h, chroma)
     dev_dec = capi.Decoder(device, w, h, chroma)
+    o = O.Oracle(w, h, c444)
     rng = np.random.default_rng(5)
     for name, packets in _cases(pa, pb, rng).items():
-        h_planes, h_invalid, h_ready, h_partial = _host_decode(host, packets, shapes)
+        # The oracle: parser state, counts and decoded planes.
+        op = o.parser()
+        o_invalid = sum(not op.push(pkt) for pkt in packets)
+        o_ready, o_partial = op.ready(False), op.ready(True)
+        o_planes = oracle_decode(o, packets)
+
         d_planes, st = _device_decode(dev_dec, packets, shapes)
+        h_planes, h_invalid, h_ready, h_partial = _host_decode(host, packets, shapes)
         for i in range(3):
-            assert np.array_equal(h_planes[i], d_planes[i]), f"{name}: plane {i}"
-        assert st.invalid_packets == h_invalid, name
+            assert np.array_equal(d_planes[i], o_planes[i]), f"{name}: device plane {i} differs from the oracle"
+            assert np.array_equal(h_planes[i], o_planes[i]), f"{name}: host-parser plane {i} differs from the oracle"
+        assert st.invalid_packets == o_invalid == h_invalid, name
         ready = st.sequence != 0xffffffff and st.decoded_blocks >= st.total_blocks
         partial = st.sequence != 0xffffffff and (ready or st.decoded_blocks > st.total_blocks // 2)
-        assert (ready, partial) == (h_ready, h_partial), (name, st.decoded_blocks, st.total_blocks)
+        assert (ready, partial) == (o_ready, o_partial) == (h_ready, h_partial), \
+            (name, st.decoded_blocks, st.total_blocks)
 
 
 def test_device_assembly_misaligned_and_invalid_arguments(device):

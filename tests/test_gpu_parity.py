@@ -3,11 +3,18 @@
 Every stage of the path is compared bit for bit with the oracle's restatement
 of the reference algorithm on the same seeded frames:
 
-  DWT coefficients          wavelet_dwt.comp / wavelet_dwt.slang (forward lifting)
-  8x8 code words, RD table  wavelet_quant.comp (quantiser + per-32x32 RD data)
-  histogram, quant drops    analyze_rate_control.comp, resolve_rate_control.comp
-  block metadata, bytes     block_packing.comp + pyrowave_encoder.cpp:1085-1109
-  decoded planes            wavelet_dequant.comp + wavelet_idwt.comp
+  DWT coefficients          shaders/dwt.comp + dwt_common.h (forward lifting)
+  8x8 code words, RD table  shaders/wavelet_quant.comp (quantiser + per-32x32 RD data)
+  histogram, quant drops    shaders/analyze_rate_control.comp, resolve_rate_control.comp
+  block metadata, bytes     shaders/block_packing.comp + pyrowave_encoder.cpp:1085-1109
+  decoded planes            shaders/wavelet_dequant.comp + shaders/idwt.comp
+
+The cases include every configuration the benchmark reports: 1080p 4:2:0 at
+400000 bytes with FP32 storage (seeds from both ends of its 16-frame set),
+4K 4:2:0 at 1200000 bytes with FP32 and FP16 level 0-1 storage, and 4K 4:4:4
+with the dense generator (200 rectangles, 1-pixel lines) at 600000 and
+2400000 bytes. Each benchmark frame is pinned by its fingerprint, so these are
+the frames the benchmark codes.
 
 All calls go through the C-ABI library (libpyrowave-shared.so.0).
 """
@@ -19,21 +26,31 @@ from pyrowave_b200 import capi, synth
 
 pytestmark = pytest.mark.gpu
 
-# (width, height, 4:4:4, budget bytes, seed, FP16 level mask)
+# (width, height, 4:4:4, budget bytes, seed, FP16 level mask, rectangles, lines, frame fingerprint or None)
 CASES = [
-    (1280, 720, False, 150000, 0, 0),
-    (34, 30, False, 65536, 0, 0),
-    (34, 30, True, 65536, 0, 0),
-    (130, 98, False, 20000, 5, 0),
-    (200, 128, True, 30000, 6, 0),
-    (1000, 562, False, 60000, 7, 0x1F),
-    (1920, 1080, False, 400000, 1, 3),
-    (3840, 2160, True, 1200000, 3, 0),
+    (1280, 720, False, 150000, 0, 0, 40, 0, "ca29b7e9c4fab120"),
+    (34, 30, False, 65536, 0, 0, 40, 0, None),
+    (34, 30, True, 65536, 0, 0, 40, 0, None),
+    (130, 98, False, 20000, 5, 0, 40, 0, None),
+    (200, 128, True, 30000, 6, 0, 40, 0, None),
+    (1000, 562, False, 60000, 7, 0x1F, 40, 0, None),
+    (1920, 1080, False, 400000, 1, 3, 40, 0, "3ff3f07e40a6491f"),
+    # 1080p benchmark workload, FP32 storage (the headline configuration).
+    (1920, 1080, False, 400000, 1, 0, 40, 0, "3ff3f07e40a6491f"),
+    (1920, 1080, False, 400000, 8, 0, 40, 0, "0b14888ed34de5d9"),
+    (1920, 1080, False, 400000, 16, 0, 40, 0, "5a629d5f15facfa2"),
+    # 4K 4:2:0 benchmark workload, FP32 and FP16 (levels 0-1) storage.
+    (3840, 2160, False, 1200000, 1, 0, 40, 0, "141d31e7daf8c1a9"),
+    (3840, 2160, False, 1200000, 2, 3, 40, 0, "1f9bb18edb08fb69"),
+    # 4K 4:4:4 benchmark generator, budget sweep ends and middle.
+    (3840, 2160, True, 600000, 1, 0, 200, 40, "56a528decd878230"),
+    (3840, 2160, True, 1200000, 3, 0, 200, 40, "f2411da1edc69dc3"),
+    (3840, 2160, True, 2400000, 2, 0, 200, 40, "6f0c2e3064ec0195"),
 ]
 
 
 def _ids(c):
-    return f"{c[0]}x{c[1]}-{'444' if c[2] else '420'}-{c[3]}B-fp16mask{c[5]}"
+    return f"{c[0]}x{c[1]}-{'444' if c[2] else '420'}-{c[3]}B-seed{c[4]}-fp16mask{c[5]}" + ("-dense" if c[6] > 40 else "")
 
 
 @pytest.fixture(scope="module")
@@ -64,9 +81,11 @@ def _mismatch(name, got, want):
 def test_encode_decode_bit_exact(device, case):
     import torch
 
-    w, h, c444, budget, seed, fp16 = case
+    w, h, c444, budget, seed, fp16, rects, lines, fingerprint = case
     chroma = capi.CHROMA_444 if c444 else capi.CHROMA_420
-    planes = synth.synth_frame(w, h, c444, seed)
+    planes = synth.synth_frame(w, h, c444, seed, rects, lines)
+    if fingerprint:
+        assert synth.frame_hash(planes) == fingerprint, "not the benchmark's frame"
     enc = capi.Encoder(device, w, h, chroma, fp16)
     lay = enc.layout()
     o = O.Oracle(w, h, c444, fp16)
@@ -76,7 +95,7 @@ def test_encode_decode_bit_exact(device, case):
 
     # A different frame and budget first, so the second encode runs through the
     # per-call updates of the captured graph rather than its first capture.
-    other = _to_dev(synth.synth_frame(w, h, c444, seed + 100))
+    other = _to_dev(synth.synth_frame(w, h, c444, seed + 100, rects, lines))
     enc.encode_device([p.data_ptr() for p in other], [p.stride(0) for p in other], budget // 2)
     dplanes = _to_dev(planes)
     enc.encode_device([p.data_ptr() for p in dplanes], [p.stride(0) for p in dplanes], budget)
@@ -134,6 +153,7 @@ def test_encode_decode_bit_exact(device, case):
     outs = [torch.zeros(pl.shape, dtype=torch.uint8, device="cuda") for pl in planes]
     dec2 = capi.Decoder(device, w, h, chroma, fp16)
     dec2.decode_blocks(m, s + 8, total // 4 - 2, [t.data_ptr() for t in outs], [t.stride(0) for t in outs])
+    assert dec2.error() == (capi.PYROWAVE_SUCCESS, 0)
     torch.cuda.synchronize()
     for i in range(3):
         errors.append(_mismatch(f"device decode plane {i}", outs[i].cpu().numpy(), oout[i]))

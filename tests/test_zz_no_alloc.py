@@ -51,9 +51,11 @@ def test_static_decode_matches_decoder_decode_blocks(gpu):
     import torch
 
     dev = capi.Device()
-    # Two frames of different layouts, so the second call runs over whatever
-    # the first left in the shared array.
-    frames = [(1280, 720, capi.CHROMA_420, 150000, 1), (320, 240, capi.CHROMA_444, 30000, 2)]
+    # Frames of different layouts, so each call runs over whatever the one
+    # before it left in the shared array; the last is the largest documented
+    # frame that fits (2560x1440 4:2:0, close to the array's size).
+    frames = [(1280, 720, capi.CHROMA_420, 150000, 1), (320, 240, capi.CHROMA_444, 30000, 2),
+              (2560, 1440, capi.CHROMA_420, 500000, 3)]
     encoded = []
     for w, h, chroma, budget, seed in frames:
         enc = capi.Encoder(dev, w, h, chroma)
@@ -78,7 +80,7 @@ def test_static_decode_matches_decoder_decode_blocks(gpu):
         want.append([t.cpu().numpy() for t in out])
         dec.close()
 
-    # Two calls in a row on one stream, then compare both.
+    # The calls in a row on one stream, then compare each.
     got = []
     for enc, w, h, chroma, planes, meta, words, n in encoded:
         out = alloc(planes)
