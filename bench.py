@@ -819,6 +819,58 @@ def measure_config(dev, cfg, budget, mask, steps, warmup):
     }
 
 
+def measure_transform(dev, cfg, steps: int = 30):
+    """The forward transform alone (pyrowave_cuda_encoder_transform: five levels,
+    no quantiser) with an event after every level: per-level us and GB/s of
+    algorithmic bytes (8-bit input read once, all four bands written once per
+    level), and the stage as a whole (input planes read once, transmitted
+    coefficients written once) against the measured HBM peak."""
+    import torch
+
+    from pyrowave_b200 import capi
+
+    w, h, c444 = cfg["width"], cfg["height"], cfg["chroma444"]
+    chroma = capi.CHROMA_444 if c444 else capi.CHROMA_420
+    base = [[torch.from_numpy(p).cuda() for p in f] for f in make_frames(dict(cfg, seeds=cfg["seeds"][:1]))]
+    frame_bytes = sum(p.numel() for p in base[0])
+    n = max(1, -(-2 * (126 << 20) // frame_bytes))
+    frames = [[torch.roll(p, shifts=(3 * i, 5 * i), dims=(0, 1)).contiguous() if i else p for p in base[0]]
+              for i in range(n)]
+    enc = capi.Encoder(dev, w, h, chroma)
+    stream = torch.cuda.Stream()
+    for i in range(3):
+        f = frames[i % n]
+        enc.transform([p.data_ptr() for p in f], [p.stride(0) for p in f], stream.cuda_stream)
+    torch.cuda.synchronize()
+    dev.set_stage_timing(True)
+    dev.report_performance_stats(reset=True)
+    for i in range(steps):
+        f = frames[i % n]
+        enc.transform([p.data_ptr() for p in f], [p.stride(0) for p in f], stream.cuda_stream)
+        torch.cuda.synchronize()
+    stages = {}
+    for line in dev.report_performance_stats(reset=True):
+        tag, rest = line.split(":", 1)
+        stages[tag.strip()] = float(rest.split("ms")[0])
+    dev.set_stage_timing(False)
+    enc.close()
+    alg = algorithmic_bytes(cfg, 0)
+    peak, peak_kind = measured_peak()
+    levels = {k: v for k, v in stages.items() if k.startswith("xdwt")}
+    total_ms = sum(levels.values())
+    out = {"workload": f"forward transform alone, {w}x{h} {'4:4:4' if c444 else '4:2:0'}",
+           "levels_us": {k: round(v * 1e3, 2) for k, v in levels.items()},
+           "levels_gbs": {k: round(alg[k[1:]] / (v * 1e-3) / 1e9, 1) for k, v in levels.items() if v > 0},
+           "stage_us": round(total_ms * 1e3, 2), "peak_gbs": peak, "peak_source": peak_kind}
+    if total_ms:
+        out["stage_gbs"] = round(alg["dwt_stage"] / (total_ms * 1e-3) / 1e9, 1)
+        out["stage_frac_of_peak"] = round(out["stage_gbs"] / peak, 4)
+        l0 = levels.get("xdwt0")
+        if l0:
+            out["level0_frac_of_peak"] = round(alg["dwt0"] / (l0 * 1e-3) / 1e9 / peak, 4)
+    return out
+
+
 def run_secondary(steps, warmup):
     from pyrowave_b200 import capi
 
@@ -826,6 +878,8 @@ def run_secondary(steps, warmup):
     out = {}
     for name, cfg_name, budget, mask in SECONDARY:
         out[name] = measure_config(dev, CONFIGS[cfg_name], budget, mask, steps, warmup)
+    for name in ("1080p", "4k444"):
+        out[f"transform_only_{name}"] = measure_transform(dev, CONFIGS[name])
     dev.close()
     return out
 

@@ -90,6 +90,16 @@ PYROWAVE_PUBLIC_API pyrowave_result pyrowave_cuda_encoder_encode_pre_transformed
                                                                                  float quant_scale,
                                                                                  pyrowave_cuda_stream stream);
 
+/* The forward transform alone: the five CDF 9/7 levels of `planes` into the
+ * encoder's pyramid (read back with pyrowave_cuda_encoder_read_wavelet), with
+ * no quantiser, rate control or packing: the reference's DWT stage
+ * (pyrowave_encoder.cpp:490-594) by itself, for measuring it apart from the
+ * quantiser the encoder fuses into its large levels. With stage timing on, the
+ * levels report as "xdwt0".."xdwt4". Queued on `stream`; does not wait. */
+PYROWAVE_PUBLIC_API pyrowave_result pyrowave_cuda_encoder_transform(pyrowave_encoder encoder,
+                                                                   const pyrowave_cuda_planes *planes,
+                                                                   pyrowave_cuda_stream stream);
+
 /* Copy the last encode's wavelet pyramid (canonical layout, device memory). */
 PYROWAVE_PUBLIC_API pyrowave_result pyrowave_cuda_encoder_read_wavelet(pyrowave_encoder encoder, float *pyramid,
                                                                        pyrowave_cuda_stream stream);
@@ -230,6 +240,29 @@ PYROWAVE_PUBLIC_API pyrowave_result pyrowave_cuda_decode_blocks_static(int width
                                                                        const uint32_t *words, size_t num_words,
                                                                        const pyrowave_cuda_planes *planes,
                                                                        pyrowave_cuda_stream stream);
+
+/* ------------------------------------------------------------------------
+ * PSNR-HVS-M: the reference's perceptual quality metric (shaders/psnr_hvs_m.comp
+ * and its driver psnr.cpp:25-28,126-224,245-320: a port of Ponomarenko's
+ * PSNR-HVS-M with the reference's own contrast sensitivity function) of a
+ * distorted luma plane against its reference, on 8x8 windows at a stride of 4,
+ * for 16 viewing distances (height factors 1 + i/8, i = 0..15).
+ *
+ * pyrowave_cuda_psnr_hvs_m adds each factor's error sum, in fixed point with
+ * 2^-24 units, into `errors` (16 uint64_t in device memory, 8-byte aligned,
+ * zeroed by the caller; several frames may accumulate). Both planes are 8-bit,
+ * width x height, in device memory. Queued on `stream`; allocates nothing.
+ * pyrowave_psnr_hvs_m_pixels gives the pixel count one frame adds (64 per
+ * window, as the reference counts); pyrowave_psnr_hvs_m_from_errors turns
+ * host copies of the sums into dB, with the limited-range peak of 223/255
+ * unless full_range. */
+PYROWAVE_PUBLIC_API pyrowave_result pyrowave_cuda_psnr_hvs_m(int width, int height, const uint8_t *reference,
+                                                             size_t reference_stride, const uint8_t *distorted,
+                                                             size_t distorted_stride, uint64_t *errors,
+                                                             pyrowave_cuda_stream stream);
+PYROWAVE_PUBLIC_API uint64_t pyrowave_psnr_hvs_m_pixels(int width, int height);
+PYROWAVE_PUBLIC_API void pyrowave_psnr_hvs_m_from_errors(const uint64_t *errors, uint64_t total_pixels, bool full_range,
+                                                         double *psnr);
 
 /* ------------------------------------------------------------------------
  * Batched form: encode (and optionally decode) many frames of any sizes,

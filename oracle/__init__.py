@@ -58,6 +58,14 @@ def lib():
             getattr(L, name).argtypes = [c_void_p]
         L.oracle_pyramid_size.restype = c_size_t
         L.oracle_pyramid_size.argtypes = [c_void_p]
+        L.oracle_psnr_hvs_m.argtypes = [c_void_p, c_int, c_void_p, c_int, c_int, c_int, c_void_p]
+        L.oracle_psnr_hvs_m.restype = None
+        L.oracle_psnr_hvs_m_tables.argtypes = [c_int, c_void_p]
+        L.oracle_psnr_hvs_m_tables.restype = None
+        L.oracle_psnr_hvs_m_pixels.argtypes = [c_int, c_int]
+        L.oracle_psnr_hvs_m_pixels.restype = c_uint64
+        L.oracle_hvs_dct8.argtypes = [c_void_p, c_void_p]
+        L.oracle_hvs_dct8.restype = None
         L.oracle_block_info.argtypes = [c_void_p, c_void_p]
         L.oracle_block_mapping.argtypes = [c_void_p, c_void_p]
         L.oracle_band_offsets.argtypes = [c_void_p, c_void_p]
@@ -469,6 +477,43 @@ def ref_decode_quant(code: int) -> float:
 
 def ref_block_count_per_subdivision(n: int) -> int:
     return int(ref_lib().ref_block_count_per_subdivision(n))
+
+
+def psnr_hvs_m_errors(ref: np.ndarray, dist: np.ndarray) -> np.ndarray:
+    """Per height factor (1 + i/8, i = 0..15) fixed-point (2^-24) PSNR-HVS-M error
+    sums of a distorted luma plane against its reference (psnr_hvs_m.comp)."""
+    L = lib()
+    a = np.ascontiguousarray(ref, np.uint8)
+    b = np.ascontiguousarray(dist, np.uint8)
+    out = np.zeros(16, np.uint64)
+    L.oracle_psnr_hvs_m(_ptr(a), a.shape[1], _ptr(b), b.shape[1], a.shape[1], a.shape[0], _ptr(out))
+    return out
+
+
+def psnr_hvs_m_tables(height: int) -> np.ndarray:
+    """(16 factors, 3 tables {csf, mask, inv_mask}, 8, 8) floats of psnr.cpp's per-factor set-up."""
+    out = np.zeros(16 * 192, np.float32)
+    lib().oracle_psnr_hvs_m_tables(height, _ptr(out))
+    return out.reshape(16, 3, 8, 8)
+
+
+def psnr_hvs_m_pixels(width: int, height: int) -> int:
+    return int(lib().oracle_psnr_hvs_m_pixels(width, height))
+
+
+def hvs_dct8(x) -> np.ndarray:
+    a = np.ascontiguousarray(x, np.float32)
+    out = np.zeros(8, np.float32)
+    lib().oracle_hvs_dct8(_ptr(a), _ptr(out))
+    return out
+
+
+def psnr_hvs_m_db(errors: np.ndarray, pixels: int, full_range: bool = True) -> np.ndarray:
+    """psnr.cpp:220-240: 10 log10(pixels * peak / error) per height factor."""
+    peak = 1.0 if full_range else (223.0 * 223.0) / (255.0 * 255.0)
+    e = np.ldexp(errors.astype(np.float64), -24)
+    with np.errstate(divide="ignore"):
+        return 10.0 * np.log10(pixels * peak / e)
 
 
 def psnr(a: np.ndarray, b: np.ndarray) -> float:

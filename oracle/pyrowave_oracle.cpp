@@ -1825,3 +1825,250 @@ uint32_t oracle_bucket_index(float d, float cost, float d_base, float cost_base)
 	return bucket_index(d, cost, d_base, cost_base);
 }
 }
+
+// ---------------------------------------------------------------------------
+// PSNR-HVS-M of a luma plane against a reference luma plane: the reference's
+// quality metric (shaders/psnr_hvs_m.comp:1-225, a port of Ponomarenko's
+// psnrhvsm.m with its own contrast sensitivity function), with the host-side
+// tables of psnr.cpp:25-28 (CSF), 126-224 (per height factor: CSF, masking
+// coefficients and their inverses, the 8x8 windows at a stride of 4) and
+// 245-320 (16 height factors 1 + i/8, fixed-point 2^-24 error sums, the
+// 10*log10 of pixels * peak / error). Every floating-point operation is one
+// rounded IEEE operation in the written order (no contraction), so the CUDA
+// kernel can reproduce the sums bit for bit. Samples outside the plane read as
+// zero (a texel fetch with robust image access).
+namespace
+{
+constexpr int kHvsFactors = 16;
+
+struct HvsTables
+{
+	float csf[8][8];
+	float mask[8][8];
+	float inv_mask[8][8];
+};
+
+float hvs_contrast_sensitivity(float cpd) // psnr.cpp:25-28
+{
+	return 2.6f * (0.0192f + 0.114f * cpd) * std::exp(-std::pow(0.114f * cpd, 1.1f));
+}
+
+void hvs_tables(int height, int factor, HvsTables &t) // psnr.cpp:151-195
+{
+	const float height_factor = 1.0f + float(factor) / 8.0f;
+	const float pi = 3.14159265358979323846f;
+	const float nyquist_cpd = float(height) * height_factor * pi / 360.0f;
+	for (int y = 0; y < 8; y++)
+		for (int x = 0; x < 8; x++)
+		{
+			const float H = (float(x) + 0.5f) / 8.0f;
+			const float V = (float(y) + 0.5f) / 8.0f;
+			const float cpd = std::sqrt(H * H + V * V);
+			t.csf[y][x] = 2.6f * hvs_contrast_sensitivity(cpd * nyquist_cpd);
+		}
+	float max_csf = 0.0f;
+	for (auto &row : t.csf)
+		for (float v : row)
+			max_csf = std::max(max_csf, v);
+	float norm = 1.0f / max_csf;
+	norm *= norm;
+	for (int y = 0; y < 8; y++)
+		for (int x = 0; x < 8; x++)
+			t.mask[y][x] = t.csf[y][x] * t.csf[y][x] * norm;
+	t.mask[0][0] = 0.0f;
+	for (int y = 0; y < 8; y++)
+		for (int x = 0; x < 8; x++)
+			t.inv_mask[y][x] = (y || x) ? 1.0f / t.mask[y][x] : 0.0f;
+}
+
+void hvs_butterfly(float &a, float &b)
+{
+	const float pos = a + b, neg = a - b;
+	a = pos;
+	b = neg;
+}
+
+void hvs_rotate(float &a, float &b, float c, float s)
+{
+	const float pos = a * c + b * s, neg = b * c - a * s;
+	a = pos;
+	b = neg;
+}
+
+void hvs_dct8(float dct[8], float sig[8]) // psnr_hvs_m.comp:58-97
+{
+	const float c7 = 0.19509032201612833f, s7 = 0.9807852804032304f;
+	const float c6 = 0.38268343236508984f, s6 = 0.9238795325112867f;
+	const float c5 = 0.5555702330196023f, s5 = 0.8314696123025452f;
+	const float r1 = std::sqrt(1.0f / 8.0f), r2 = std::sqrt(2.0f / 8.0f);
+	hvs_butterfly(sig[0], sig[7]);
+	hvs_butterfly(sig[1], sig[6]);
+	hvs_butterfly(sig[2], sig[5]);
+	hvs_butterfly(sig[3], sig[4]);
+	hvs_butterfly(sig[0], sig[3]);
+	hvs_butterfly(sig[1], sig[2]);
+	hvs_butterfly(sig[0], sig[1]);
+	hvs_rotate(sig[2], sig[3], c6, s6);
+	hvs_rotate(sig[4], sig[7], c7, s7);
+	hvs_rotate(sig[5], sig[6], c5, s5);
+	hvs_butterfly(sig[4], sig[5]);
+	hvs_butterfly(sig[6], sig[7]);
+	hvs_butterfly(sig[5], sig[6]);
+	sig[0] *= r1;
+	sig[1] *= r1;
+	sig[2] *= r2;
+	sig[3] *= r2;
+	sig[4] *= r2;
+	sig[5] *= r1;
+	sig[6] *= r1;
+	sig[7] *= -r2;
+	dct[0] = sig[0];
+	dct[1] = sig[4];
+	dct[2] = sig[2];
+	dct[3] = sig[5];
+	dct[4] = sig[1];
+	dct[5] = sig[6];
+	dct[6] = sig[3];
+	dct[7] = sig[7];
+}
+
+void hvs_dct8x8(float dct[8][8], float sig[8][8]) // psnr_hvs_m.comp:155-171
+{
+	for (int row = 0; row < 8; row++)
+	{
+		float s[8];
+		memcpy(s, sig[row], sizeof(s));
+		hvs_dct8(dct[row], s);
+	}
+	for (int col = 0; col < 8; col++)
+	{
+		float s[8], d[8];
+		for (int i = 0; i < 8; i++)
+			s[i] = dct[i][col];
+		hvs_dct8(d, s);
+		for (int i = 0; i < 8; i++)
+			dct[i][col] = d[i];
+	}
+}
+
+float hvs_vari(float e, float e2, int count) // psnr_hvs_m.comp:104-107
+{
+	return std::max(e2 * float(count) - e * e, 0.0f) / float(count - 1);
+}
+
+// The factor-independent part of maskeff (psnr_hvs_m.comp:109-153): the ratio
+// of the quadrant variances to the block variance.
+float hvs_pop(float sig[8][8])
+{
+	float sum_e2[2][2], sum_e[2][2];
+	float sum_e2_total = 0.0f, sum_e_total = 0.0f;
+	for (int y = 0; y < 2; y++)
+		for (int x = 0; x < 2; x++)
+		{
+			sum_e2[y][x] = 0.0f;
+			sum_e[y][x] = 0.0f;
+			for (int suby = 0; suby < 4; suby++)
+				for (int subx = 0; subx < 4; subx++)
+				{
+					const float v = sig[y * 4 + suby][x * 4 + subx];
+					sum_e[y][x] += v;
+					sum_e2[y][x] += v * v;
+				}
+			sum_e_total += sum_e[y][x];
+			sum_e2_total += sum_e2[y][x];
+		}
+	float pop = hvs_vari(sum_e_total, sum_e2_total, 64);
+	if (pop != 0.0f)
+		pop = (hvs_vari(sum_e[0][0], sum_e2[0][0], 16) + hvs_vari(sum_e[1][0], sum_e2[1][0], 16) +
+		       hvs_vari(sum_e[0][1], sum_e2[0][1], 16) + hvs_vari(sum_e[1][1], sum_e2[1][1], 16)) /
+		      pop;
+	return pop;
+}
+
+float hvs_maskeff(const float dct[8][8], float pop, const HvsTables &t) // psnr_hvs_m.comp:109-153
+{
+	float m = 0.0f;
+	for (int y = 0; y < 8; y++)
+		for (int x = 0; x < 8; x++)
+			m += dct[y][x] * dct[y][x] * t.mask[y][x];
+	return std::sqrt(m * pop) / 32.0f;
+}
+
+float hvs_dct_error(const float a[8][8], const float b[8][8], float mask, const HvsTables &t) // :173-195
+{
+	float total = 0.0f;
+	for (int y = 0; y < 8; y++)
+		for (int x = 0; x < 8; x++)
+		{
+			float e = std::fabs(a[y][x] - b[y][x]);
+			const float masking = mask * t.inv_mask[y][x];
+			e = std::max(e - masking, 0.0f);
+			const float w = e * t.csf[y][x];
+			total += w * w;
+		}
+	return total;
+}
+
+void hvs_window(const uint8_t *plane, int stride, int w, int h, int x0, int y0, float sig[8][8])
+{
+	for (int y = 0; y < 8; y++)
+		for (int x = 0; x < 8; x++)
+		{
+			const int px = x0 + x, py = y0 + y;
+			sig[y][x] = (px < w && py < h) ? float(plane[size_t(py) * size_t(stride) + size_t(px)]) / 255.0f : 0.0f;
+		}
+}
+} // namespace
+
+extern "C" {
+void oracle_psnr_hvs_m_tables(int height, float *out)
+{
+	for (int f = 0; f < kHvsFactors; f++)
+	{
+		HvsTables t;
+		hvs_tables(height, f, t);
+		memcpy(out + size_t(f) * 192, &t, sizeof(t));
+	}
+}
+
+uint64_t oracle_psnr_hvs_m_pixels(int width, int height)
+{
+	const uint64_t bx = uint64_t((width - 1) / 4 + 1), by = uint64_t((height - 1) / 4 + 1);
+	return bx * by * 64;
+}
+
+// Adds each height factor's fixed-point error sum (2^-24 units) into errors[16]. psnr_hvs_m.comp:197-225
+void oracle_psnr_hvs_m(const uint8_t *ref, int ref_stride, const uint8_t *dist, int dist_stride, int width,
+                       int height, uint64_t *errors)
+{
+	HvsTables tables[kHvsFactors];
+	for (int f = 0; f < kHvsFactors; f++)
+		hvs_tables(height, f, tables[f]);
+	const int nbx = (width - 1) / 4 + 1, nby = (height - 1) / 4 + 1;
+	for (int by = 0; by < nby; by++)
+		for (int bx = 0; bx < nbx; bx++)
+		{
+			float sig[8][8], dct_a[8][8], dct_b[8][8];
+			hvs_window(ref, ref_stride, width, height, bx * 4, by * 4, sig);
+			const float pop_a = hvs_pop(sig);
+			hvs_dct8x8(dct_a, sig);
+			hvs_window(dist, dist_stride, width, height, bx * 4, by * 4, sig);
+			const float pop_b = hvs_pop(sig);
+			hvs_dct8x8(dct_b, sig);
+			for (int f = 0; f < kHvsFactors; f++)
+			{
+				const float mask = std::max(hvs_maskeff(dct_a, pop_a, tables[f]), hvs_maskeff(dct_b, pop_b, tables[f]));
+				const float e = hvs_dct_error(dct_a, dct_b, mask, tables[f]);
+				errors[f] += uint64_t(std::ldexp(e, 24));
+			}
+		}
+}
+
+// dct8 of psnr_hvs_m.comp, exposed for the test that pins it to the orthonormal DCT-II.
+void oracle_hvs_dct8(const float *in, float *out)
+{
+	float s[8];
+	memcpy(s, in, sizeof(s));
+	hvs_dct8(out, s);
+}
+}

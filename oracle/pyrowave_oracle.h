@@ -117,6 +117,16 @@ int oracle_dequant(const oracle_codec *codec, const uint32_t *offsets, const uin
 int oracle_idwt(oracle_codec *codec, const float *pyramid, int mode, uint8_t *const planes[3], const int strides[3]);
 int oracle_idwt_f64(oracle_codec *codec, const double *pyramid, uint8_t *const planes[3], const int strides[3]);
 
+/* PSNR-HVS-M (shaders/psnr_hvs_m.comp, psnr.cpp:25-28,126-224,245-320 of the
+ * reference): adds, per height factor 1 + i/8 (i = 0..15), the fixed-point
+ * (2^-24) error sum of every 8x8 window at a stride of 4 of the luma planes
+ * into errors[16]. Tables: 16 x {csf, mask, inv_mask} x 64 floats. */
+void oracle_psnr_hvs_m(const uint8_t *ref, int ref_stride, const uint8_t *dist, int dist_stride, int width,
+                       int height, uint64_t *errors);
+void oracle_psnr_hvs_m_tables(int height, float *out);
+uint64_t oracle_psnr_hvs_m_pixels(int width, int height);
+void oracle_hvs_dct8(const float *in, float *out);
+
 /* Helpers exposed for unit tests. */
 uint16_t oracle_float_to_half(float v);
 float oracle_half_to_float(uint16_t h);

@@ -57,10 +57,11 @@ API_SYMBOLS = [
     "pyrowave_cuda_device_set_stage_timing", "pyrowave_cuda_encoder_set_precision", "pyrowave_cuda_decoder_set_precision", "pyrowave_cuda_encoder_get_layout",
     "pyrowave_cuda_decoder_get_layout", "pyrowave_cuda_encoder_encode", "pyrowave_cuda_encoder_get_device_bitstream",
     "pyrowave_cuda_encoder_get_size", "pyrowave_cuda_encoder_encode_pre_transformed",
-    "pyrowave_cuda_encoder_read_wavelet", "pyrowave_cuda_encoder_read_debug", "pyrowave_cuda_decoder_decode",
+    "pyrowave_cuda_encoder_read_wavelet", "pyrowave_cuda_encoder_read_debug", "pyrowave_cuda_encoder_transform", "pyrowave_cuda_decoder_decode",
     "pyrowave_cuda_decoder_decode_blocks", "pyrowave_cuda_decoder_read_wavelet", "pyrowave_cuda_decoder_decode_pyramid",
     "pyrowave_cuda_decoder_decode_packets", "pyrowave_cuda_decoder_get_packet_status",
     "pyrowave_cuda_decoder_get_error", "pyrowave_cuda_decode_blocks_static",
+    "pyrowave_cuda_psnr_hvs_m", "pyrowave_psnr_hvs_m_pixels", "pyrowave_psnr_hvs_m_from_errors",
     "pyrowave_cuda_batch_create", "pyrowave_cuda_batch_destroy", "pyrowave_cuda_batch_encode",
     "pyrowave_cuda_batch_get_device_bitstream", "pyrowave_cuda_batch_get_sizes", "pyrowave_cuda_batch_autotune",
     "pyrowave_cuda_server_create", "pyrowave_cuda_server_destroy", "pyrowave_cuda_server_open_stream",
@@ -193,6 +194,7 @@ def lib():
     L.pyrowave_cuda_encoder_encode_pre_transformed.argtypes = [c_void_p, c_void_p, POINTER(RateControl), c_float,
                                                                c_void_p]
     L.pyrowave_cuda_encoder_read_wavelet.argtypes = [c_void_p, c_void_p, c_void_p]
+    L.pyrowave_cuda_encoder_transform.argtypes = [c_void_p, POINTER(CudaPlanes), c_void_p]
     L.pyrowave_cuda_encoder_read_debug.argtypes = [c_void_p, POINTER(CudaEncoderDebug)]
     L.pyrowave_cuda_decoder_decode.argtypes = [c_void_p, POINTER(CudaPlanes), c_void_p]
     L.pyrowave_cuda_decoder_decode_blocks.argtypes = [c_void_p, c_void_p, c_void_p, c_size_t, POINTER(CudaPlanes),
@@ -202,6 +204,11 @@ def lib():
                                                        POINTER(CudaPlanes), c_void_p]
     L.pyrowave_cuda_decoder_get_packet_status.argtypes = [c_void_p, POINTER(PacketStatus)]
     L.pyrowave_cuda_decoder_get_error.argtypes = [c_void_p, POINTER(c_uint32)]
+    L.pyrowave_cuda_psnr_hvs_m.argtypes = [c_int, c_int, c_void_p, c_size_t, c_void_p, c_size_t, c_void_p, c_void_p]
+    L.pyrowave_psnr_hvs_m_pixels.argtypes = [c_int, c_int]
+    L.pyrowave_psnr_hvs_m_pixels.restype = ctypes.c_uint64
+    L.pyrowave_psnr_hvs_m_from_errors.argtypes = [c_void_p, ctypes.c_uint64, c_bool, c_void_p]
+    L.pyrowave_psnr_hvs_m_from_errors.restype = None
     L.pyrowave_cuda_decoder_decode_pyramid.argtypes = [c_void_p, c_void_p, POINTER(CudaPlanes), c_void_p]
     L.pyrowave_cuda_decode_blocks_static.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_int, c_void_p, c_void_p,
                                                      c_size_t, POINTER(CudaPlanes), c_void_p]
@@ -366,6 +373,15 @@ class Encoder:
         check(self.L.pyrowave_cuda_encoder_encode(self.h, ctypes.byref(cp), ctypes.byref(rc), c_void_p(stream)),
               "pyrowave_cuda_encoder_encode")
 
+    def transform(self, plane_ptrs, strides, stream: int = 0):
+        """pyrowave_cuda_encoder_transform: the five forward levels alone (no quantiser)."""
+        cp = CudaPlanes()
+        for i in range(3):
+            cp.data[i] = plane_ptrs[i]
+            cp.row_stride_in_bytes[i] = strides[i]
+        check(self.L.pyrowave_cuda_encoder_transform(self.h, ctypes.byref(cp), c_void_p(stream)),
+              "pyrowave_cuda_encoder_transform")
+
     def encode_pre_transformed(self, pyramid_dev_ptr: int, budget: int, quant_scale: float = -1.0, stream: int = 0):
         rc = RateControl(budget)
         check(self.L.pyrowave_cuda_encoder_encode_pre_transformed(self.h, c_void_p(pyramid_dev_ptr), ctypes.byref(rc),
@@ -508,6 +524,21 @@ class Decoder:
     def read_wavelet(self, pyramid_dev_ptr: int, stream: int = 0):
         check(self.L.pyrowave_cuda_decoder_read_wavelet(self.h, c_void_p(pyramid_dev_ptr), c_void_p(stream)),
               "decoder_read_wavelet")
+
+
+def psnr_hvs_m(width: int, height: int, ref_ptr: int, ref_stride: int, dist_ptr: int, dist_stride: int,
+               errors_ptr: int, stream: int = 0) -> int:
+    """pyrowave_cuda_psnr_hvs_m: add the 16 fixed-point error sums into the device array at errors_ptr."""
+    return lib().pyrowave_cuda_psnr_hvs_m(width, height, c_void_p(ref_ptr), ref_stride, c_void_p(dist_ptr),
+                                          dist_stride, c_void_p(errors_ptr), c_void_p(stream))
+
+
+def psnr_hvs_m_db(errors, pixels: int, full_range: bool = True) -> np.ndarray:
+    """pyrowave_psnr_hvs_m_from_errors on host copies of the sums."""
+    e = np.ascontiguousarray(errors, np.uint64)
+    out = np.zeros(16, np.float64)
+    lib().pyrowave_psnr_hvs_m_from_errors(_ptr(e), pixels, full_range, _ptr(out))
+    return out
 
 
 def decode_blocks_static(width: int, height: int, chroma: int, meta_ptr: int, words_ptr: int, num_words: int,

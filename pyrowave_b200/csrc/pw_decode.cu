@@ -98,6 +98,8 @@ __device__ __forceinline__ void dequant_body(const BlockParams &p, const DecodeI
 	pdl_wait();
 	if (clear_error && t == 0 && in.error)
 		*in.error = 0u;
+	if (clear_error && in.state && t < int(sizeof(DecodeState) / 4))
+		reinterpret_cast<uint32_t *>(in.state)[t] = 0u;
 
 	uint32_t off, words = 0;
 	const bool sized_by_header = in.offsets || in.keys;
@@ -318,13 +320,13 @@ struct IdwtShared
 // than SMs) run 1024-thread CTAs whose lifting items cover half as many
 // outputs, shortening every serial phase.
 template <int kThreads>
-__device__ __forceinline__ void idwt_body(const LevelParams &p, const DecodeInput &in, const PlaneOutput &out,
-                                          const LevelTileMap *maps, const int tile, const int comp_index)
+__device__ __forceinline__ void idwt_body(IdwtShared &sh, const LevelParams &p, const DecodeInput &in,
+                                          const PlaneOutput &out, const LevelTileMap *maps, const int tile,
+                                          const int comp_index)
 {
 	constexpr int kOut = kThreads >= 1024 ? 8 : 16; // outputs per lifting item
 	constexpr int kSegs = 64 / kOut;
 	constexpr int kWin = kOut + 8;
-	__shared__ IdwtShared sh;
 	pdl_trigger();
 	const int level = p.level;
 	const int comp = (level == 0 && !p.chroma444) ? 0 : comp_index;
@@ -610,7 +612,8 @@ template <int kThreads, int kMinBlocks = kIdwtMinBlocks<kThreads>>
 __global__ void __launch_bounds__(kThreads, kMinBlocks) idwt_kernel(const LevelParams p, const DecodeInput in, const PlaneOutput out,
                                                                      const __grid_constant__ LevelTileMap maps)
 {
-	idwt_body<kThreads>(p, in, out, &maps, int(blockIdx.x), int(blockIdx.y));
+	__shared__ IdwtShared sh;
+	idwt_body<kThreads>(sh, p, in, out, &maps, int(blockIdx.x), int(blockIdx.y));
 }
 
 // Batched form: one CTA per (frame, component, tile) of this level.
@@ -629,8 +632,63 @@ __global__ void __launch_bounds__(kThreads, kMinBlocks) idwt_batch_kernel(const 
 	load_params(s_out, io[f].out);
 	__syncthreads();
 	const int ntiles = s_p.L.tiles_x * s_p.L.tiles_y;
-	idwt_body<kThreads>(s_p, s_in, s_out, f < kBatchTileMapFrames ? &maps.frame[f] : nullptr, local % ntiles,
+	__shared__ IdwtShared sh;
+	idwt_body<kThreads>(sh, s_p, s_in, s_out, f < kBatchTileMapFrames ? &maps.frame[f] : nullptr, local % ntiles,
 	                    local / ntiles);
+}
+
+// The small levels of one decode in one launch, coarsest first: every CTA
+// takes the next tile from the decode's ticket counter, and a level's tiles
+// wait for every tile of the coarser level (bounded; a wait that gives up sets
+// kDecodeErrorLevelWait). Taking tickets in order means a CTA only waits for
+// tiles that running CTAs hold.
+constexpr int kSmallInvThreads = 1024;
+constexpr uint32_t kInvLevelWaitSpins = 1u << 22;
+
+__global__ void __launch_bounds__(kSmallInvThreads, 1)
+    idwt_small_levels_kernel(const __grid_constant__ SmallInverseParams sp, const DecodeInput in, const PlaneOutput out)
+{
+	__shared__ IdwtShared sh;
+	__shared__ int s_item;
+	DecodeState *st = in.state;
+	// The dequantiser clears the decode's counters: take a ticket only after it completed.
+	pdl_wait();
+	if (threadIdx.x == 0)
+		s_item = int(atomicAdd(&st->ticket, 1u));
+	__syncthreads();
+	const int item = s_item;
+	int level = -1, local = 0;
+	for (int l = sp.last_level; l >= sp.first_level; l--)
+		if (item >= sp.item_first[l] && item < sp.item_first[l] + sp.ntiles[l])
+		{
+			level = l;
+			local = item - sp.item_first[l];
+		}
+	if (level < 0)
+		return;
+	if (level < sp.last_level && threadIdx.x == 0)
+	{
+		uint32_t spins = 0;
+		while (ld_acquire_u32(&st->level_done[level + 1]) < uint32_t(sp.ntiles[level + 1]))
+		{
+			if (++spins > kInvLevelWaitSpins)
+			{
+				atomicOr(&st->error, kDecodeErrorLevelWait);
+				break;
+			}
+			__nanosleep(32);
+		}
+	}
+	__syncthreads();
+	const LevelParams &p = sp.lp[level];
+	const int per_comp = p.L.tiles_x * p.L.tiles_y;
+	idwt_body<kSmallInvThreads>(sh, p, in, out, nullptr, local % per_comp, local / per_comp);
+	__syncthreads();
+	if (threadIdx.x == 0)
+	{
+		__threadfence();
+		atomicAdd(&st->level_done[level], 1u);
+	}
 }
 
 // Canonical pyramid (all transmitted bands, band-major, unpadded) <-> padded storage.
@@ -691,6 +749,16 @@ void launch_idwt_level(const LevelParams &p, const DecodeInput &in, const PlaneO
 		LaunchConfig lc(grid, dim3(256), stream, programmatic);
 		cudaLaunchKernelEx(&lc.cfg, idwt_kernel<256, 4>, p, in, out, m);
 	}
+}
+
+void launch_idwt_small_levels(const SmallInverseParams &sp, const DecodeInput &in, const PlaneOutput &out,
+                              bool programmatic, cudaStream_t stream)
+{
+	int items = 0;
+	for (int l = sp.first_level; l <= sp.last_level; l++)
+		items += sp.ntiles[l];
+	LaunchConfig lc(dim3(items), dim3(kSmallInvThreads), stream, programmatic);
+	cudaLaunchKernelEx(&lc.cfg, idwt_small_levels_kernel, sp, in, out);
 }
 
 void launch_pyramid_io(const BlockParams &p, float *canonical, float *coef32, __half *coef16, bool to_canonical,

@@ -159,6 +159,14 @@ __device__ __forceinline__ void tma_load_2d(void *dst, const void *tensor_map, i
 	             : "memory");
 }
 
+// GPU-scope acquire load of a 32-bit counter (work items finished by other CTAs).
+__device__ __forceinline__ uint32_t ld_acquire_u32(const uint32_t *p)
+{
+	uint32_t v;
+	asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+	return v;
+}
+
 // GPU-scope acquire load / release store of a 64-bit word (flags between CTAs).
 __device__ __forceinline__ unsigned long long ld_acquire_u64(const unsigned long long *p)
 {
@@ -265,9 +273,10 @@ __device__ __forceinline__ int find_band(const BlockParams &p, int blk)
 	return lo;
 }
 
+// One coefficient, read through L2 (other CTAs of the same launch may have written it).
 __device__ __forceinline__ float load_coef(const float *c32, const __half *c16, bool fp16, int64_t idx)
 {
-	return fp16 ? __half2float(c16[idx]) : c32[idx];
+	return fp16 ? __half2float(__ldcg(c16 + idx)) : __ldcg(c32 + idx);
 }
 
 // ---------------------------------------------------------------------------

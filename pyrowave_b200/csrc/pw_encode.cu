@@ -342,12 +342,11 @@ constexpr int kLargeLevelThreads = 256;
 // samples): `tile` in row-major tile order, `comp_index` the component among
 // those at this level. Run by every thread of a kThreads-thread CTA.
 template <int kThreads>
-__device__ __forceinline__ void dwt_forward_body(const LevelParams &p, const PlaneInput &in, const EncodeBuffers &buf,
-                                                 const LevelTileMap *maps, const int fused, const int tile,
-                                                 const int comp_index)
+__device__ __forceinline__ void dwt_forward_body(DwtShared &sh, const LevelParams &p, const PlaneInput &in,
+                                                 const EncodeBuffers &buf, const LevelTileMap *maps, const int fused,
+                                                 const int tile, const int comp_index)
 {
 	using Split = DwtSplit<kThreads>;
-	__shared__ DwtShared sh;
 	pdl_trigger();
 	const int level = p.level;
 	const int comp = (level == 0 && !p.chroma444) ? 0 : comp_index;
@@ -629,17 +628,33 @@ __device__ __forceinline__ void dwt_forward_body(const LevelParams &p, const Pla
 		return;
 
 	// Quantise the transmitted bands of this tile: HL, LH, HH (+ LL at the last
-	// level), kGroups bands per round.
+	// level), kGroups bands per round. With fused == kFusedSplitTail, a last
+	// round that would leave groups idle (HH after HL and LH in a 256-thread
+	// CTA) instead runs its band on the whole CTA with twice the threads per
+	// sub-block: same results, a shorter serial chain for levels of few waves.
 	const int first_band = level == kLevels - 1 ? 0 : 1;
 	const int nb = 4 - first_band;
 	const int grp = threadIdx.x / Split::kGroupThreads, t = threadIdx.x % Split::kGroupThreads;
-	for (int round = 0; round * Split::kGroups < nb; round++)
+	bool split_tail = false;
+	if constexpr (kThreads == kLargeLevelThreads)
+		split_tail = fused == kFusedSplitTail && (nb % Split::kGroups) != 0;
+	const int rounds = split_tail ? nb / Split::kGroups : (nb + Split::kGroups - 1) / Split::kGroups;
+	for (int round = 0; round < rounds; round++)
 	{
 		const int bi = round * Split::kGroups + grp;
 		const bool active = bi < nb;
 		const int band = active ? first_band + bi : first_band;
 		quant_analyze_block<Split::kQSplit>(&bands[band][0][0], kBandPitch, active, t, sh.q[grp], L,
 		                                    p.band[comp][band], p.subdivision_shift, tx, ty, buf);
+	}
+	if constexpr (kThreads == kLargeLevelThreads)
+	{
+		if (split_tail)
+		{
+			const int band = first_band + rounds * Split::kGroups;
+			quant_analyze_block<2 * Split::kQSplit>(&bands[band][0][0], kBandPitch, true, int(threadIdx.x), sh.q[0],
+			                                        L, p.band[comp][band], p.subdivision_shift, tx, ty, buf);
+		}
 	}
 }
 
@@ -648,7 +663,8 @@ __global__ void __launch_bounds__(kThreads, DwtSplit<kThreads>::kMinBlocks)
     dwt_forward_kernel(const LevelParams p, const PlaneInput in, const EncodeBuffers buf, const int fused,
                        const __grid_constant__ LevelTileMap maps)
 {
-	dwt_forward_body<kThreads>(p, in, buf, &maps, fused, int(blockIdx.x), int(blockIdx.y));
+	__shared__ DwtShared sh;
+	dwt_forward_body<kThreads>(sh, p, in, buf, &maps, fused, int(blockIdx.x), int(blockIdx.y));
 }
 
 // Batched form: one CTA per (frame, component, tile) of this level.
@@ -667,24 +683,26 @@ __global__ void __launch_bounds__(kThreads, DwtSplit<kThreads>::kMinBlocks)
 	load_params(s_buf, frames[f].eb);
 	__syncthreads();
 	const int ntiles = s_p.L.tiles_x * s_p.L.tiles_y;
-	dwt_forward_body<kThreads>(s_p, s_in, s_buf, f < kBatchTileMapFrames ? &maps.frame[f] : nullptr, fused,
+	__shared__ DwtShared sh;
+	dwt_forward_body<kThreads>(sh, s_p, s_in, s_buf, f < kBatchTileMapFrames ? &maps.frame[f] : nullptr, fused,
 	                           local % ntiles, local / ntiles);
 }
 
 // Quantiser over a pyramid already in storage (the reference's
 // Encoder::encode_pre_transformed, pyrowave_encoder.cpp:1138-1151, and the
-// small levels of a frame). Two 32x32 blocks per CTA, 128 * S threads each.
-template <int S>
-__device__ __forceinline__ void quant_blocks_body(const BlockParams &p, const EncodeBuffers &buf, const int nblocks,
-                                                  const int pair)
+// small levels of a frame). G 32x32 blocks per CTA, 128 * S threads each:
+// blocks first + item * G + group, those below `end`. `tile` holds G band
+// tiles of 32 x kBandPitch floats, `q` G reduction scratches.
+template <int S, int G>
+__device__ __forceinline__ void quant_blocks_body(const BlockParams &p, const EncodeBuffers &buf, const int first,
+                                                  const int end, const int item, float (*tile)[32][kBandPitch],
+                                                  QuantGroupShared *q)
 {
 	constexpr int kGroupThreads = 128 * S;
-	__shared__ float tile[2][32][kBandPitch];
-	__shared__ QuantGroupShared q[2];
 	pdl_trigger();
 	const int grp = threadIdx.x / kGroupThreads, t = threadIdx.x % kGroupThreads;
-	const int b = pair * 2 + grp;
-	const bool active = b < nblocks;
+	const int b = first + item * G + grp;
+	const bool active = b < end;
 	const int k = active ? find_band(p, b) : 0;
 	const BandEntry &E = p.band[k];
 	const LevelDesc &L = p.level[E.level];
@@ -731,7 +749,9 @@ template <int S>
 __global__ void __launch_bounds__(256 * S) quant_pretransformed_kernel(const BlockParams p, const EncodeBuffers buf,
                                                                        const int nblocks)
 {
-	quant_blocks_body<S>(p, buf, nblocks, int(blockIdx.x));
+	__shared__ float tile[2][32][kBandPitch];
+	__shared__ QuantGroupShared q[2];
+	quant_blocks_body<S, 2>(p, buf, 0, nblocks, int(blockIdx.x), tile, q);
 }
 
 // Batched form: one CTA per pair of blocks among each frame's small-level blocks.
@@ -740,12 +760,100 @@ __global__ void __launch_bounds__(256 * S) quant_blocks_batch_kernel(const Batch
 {
 	__shared__ BlockParams s_p;
 	__shared__ EncodeBuffers s_buf;
+	__shared__ float tile[2][32][kBandPitch];
+	__shared__ QuantGroupShared q[2];
 	int f, local;
 	batch_item(cta_map, f, local);
 	load_params(s_p, frames[f].bp);
 	load_params(s_buf, frames[f].eb);
 	__syncthreads();
-	quant_blocks_body<S>(s_p, s_buf, frames[f].small_blocks, local);
+	quant_blocks_body<S, 2>(s_p, s_buf, 0, frames[f].small_blocks, local, tile, q);
+}
+
+// ---------------------------------------------------------------------------
+// The small levels of one frame in one launch: for each level from the first
+// small one to the last, the transform of its tiles (input: the finer level's
+// LL), then the quantiser and RD analysis of its blocks. Every CTA takes the
+// next work item from a per-frame ticket counter, so an item that waits for
+// another (a level's transform for the finer level's; a level's quantiser for
+// its transform) only waits for items that running CTAs hold: the waits end
+// even when not every CTA of the grid is resident. The quantiser of a level
+// runs while the coarser levels transform. Waits are bounded; a wait that
+// gives up sets kErrorLevelWait.
+constexpr int kSmallThreads = 1024;
+constexpr int kSmallQuantGroups = kSmallThreads / 256; // 32x32 blocks per quantiser item (two threads per sub-block)
+constexpr uint32_t kLevelWaitSpins = 1u << 22;
+
+__device__ __forceinline__ void wait_count(const uint32_t *counter, uint32_t target, uint32_t *error)
+{
+	__shared__ int s_failed;
+	if (threadIdx.x == 0)
+	{
+		uint32_t spins = 0;
+		int failed = 0;
+		while (ld_acquire_u32(counter) < target)
+		{
+			if (++spins > kLevelWaitSpins)
+			{
+				atomicOr(error, kErrorLevelWait);
+				failed = 1;
+				break;
+			}
+			__nanosleep(32);
+		}
+		s_failed = failed;
+	}
+	__syncthreads();
+	(void)s_failed;
+}
+
+__global__ void __launch_bounds__(kSmallThreads, 1)
+    dwt_small_levels_kernel(const __grid_constant__ SmallLevelParams sp, const PlaneInput in, const EncodeBuffers buf)
+{
+	__shared__ DwtShared sh;
+	__shared__ int s_item;
+	if (threadIdx.x == 0)
+		s_item = int(atomicAdd(&buf.rc->small_ticket, 1u));
+	__syncthreads();
+	const int item = s_item;
+	int level = -1, kind = 0, local = 0;
+	for (int l = sp.first_level; l < kLevels; l++)
+		for (int k = 0; k < 2; k++)
+		{
+			const int i0 = sp.item_first[2 * l + k], i1 = sp.item_first[2 * l + k + 1];
+			if (item >= i0 && item < i1)
+			{
+				level = l;
+				kind = k;
+				local = item - i0;
+			}
+		}
+	if (level < 0)
+		return;
+	if (kind == 0)
+	{
+		// Transform: after every tile of the finer level (the first small level
+		// follows the previous launch through the dependency wait in the body).
+		if (level > sp.first_level)
+			wait_count(&buf.rc->level_done[level - 1], uint32_t(sp.ntiles[level - 1]), &buf.rc->error);
+		const LevelParams &p = sp.lp[level];
+		const int per_comp = p.L.tiles_x * p.L.tiles_y;
+		dwt_forward_body<kSmallThreads>(sh, p, in, buf, nullptr, 0, local % per_comp, local / per_comp);
+		__syncthreads();
+		if (threadIdx.x == 0)
+		{
+			__threadfence();
+			atomicAdd(&buf.rc->level_done[level], 1u);
+		}
+	}
+	else
+	{
+		// Quantiser: after every tile of its own level, four blocks per item.
+		wait_count(&buf.rc->level_done[level], uint32_t(sp.ntiles[level]), &buf.rc->error);
+		float(*tile)[32][kBandPitch] = reinterpret_cast<float(*)[32][kBandPitch]>(&sh.in[0][0]);
+		quant_blocks_body<2, kSmallQuantGroups>(sp.bp, buf, sp.block_first[level],
+		                                        sp.block_first[level] + sp.block_count[level], local, tile, sh.q);
+	}
 }
 
 // ---------------------------------------------------------------------------
@@ -1065,6 +1173,143 @@ __global__ void __launch_bounds__(kThreads) resolve_kernel(const ResolveParams p
 	resolve_body(p, buf, int(blockIdx.x), int(gridDim.x));
 }
 
+// The same resolve in one 1024-thread CTA, for frames of at most
+// kSingleResolveRows * 1024 blocks: every thread loads the RD rows of its run
+// of consecutive blocks once, into registers, together with two histogram
+// slots; the histogram scan, x*, the cut and the block offsets are then four
+// block-wide scans with no global round trip between them and no wait on
+// other CTAs. Results are those of resolve_body.
+constexpr int kSingleResolveRows = 4;
+constexpr int kSingleResolveThreads = 1024;
+
+__global__ void __launch_bounds__(kSingleResolveThreads, 1)
+    resolve_single_kernel(const ResolveParams p, const EncodeBuffers buf)
+{
+	__shared__ uint32_t scan[kHistSize];
+	__shared__ uint32_t warp_sums[32];
+	__shared__ unsigned long long warp_sums64[32];
+	__shared__ int s_xstar;
+	__shared__ uint32_t s_cut;
+	RateControlState *rc = buf.rc;
+	const int t = threadIdx.x;
+	const int n = p.block_count_32x32;
+	const int per = (n + kSingleResolveThreads - 1) / kSingleResolveThreads; // at most kSingleResolveRows
+	const int b0 = min(t * per, n), b1 = min(b0 + per, n);
+	// Every quantiser has finished once the wait returns; the packer is released only then.
+	pdl_wait();
+	pdl_trigger();
+
+	RawRD rows[kSingleResolveRows];
+#pragma unroll
+	for (int i = 0; i < kSingleResolveRows; i++)
+		if (b0 + i < b1)
+			rows[i] = load_raw_rd(buf, b0 + i);
+	static_assert(kHistSize == 2 * kSingleResolveThreads, "two histogram slots per thread");
+	const uint32_t h0 = __ldcg(&rc->histogram[2 * t]), h1 = __ldcg(&rc->histogram[2 * t + 1]);
+	const uint32_t consumed = __ldcg(&rc->consumed);
+	if (t == 0)
+	{
+		s_xstar = -1;
+		s_cut = 0xffffffffu;
+	}
+	uint32_t total;
+	const uint32_t run = block_exclusive_scan(h0 + h1, warp_sums, total);
+	scan[2 * t] = run + h0;
+	scan[2 * t + 1] = run + h0 + h1;
+	__syncthreads();
+
+	const int64_t need = int64_t(consumed) - int64_t(p.target_words);
+	if (need > 0)
+	{
+		for (int x = 2 * t; x < 2 * t + 2; x++)
+			if (int64_t(scan[x]) >= need && (x == 0 || int64_t(scan[x - 1]) < need))
+				s_xstar = x;
+	}
+	__syncthreads();
+	const int xstar = s_xstar;
+
+	if (xstar >= 0)
+	{
+		// The cut: exclusive prefix of the savings at bucket b* over the x*
+		// subdivision's blocks, in block order; the first operation whose
+		// prefix reaches the requirement is not applied, nor any after it.
+		const int start = (xstar & (kSubdivisions - 1)) * p.blocks_per_subdivision;
+		const int end = min(start + p.blocks_per_subdivision, n);
+		const int64_t required = need - (xstar > 0 ? int64_t(scan[xstar - 1]) : 0);
+		const uint32_t bk = uint32_t(xstar >> 4);
+		uint32_t sv[kSingleResolveRows];
+		uint32_t local = 0;
+#pragma unroll
+		for (int i = 0; i < kSingleResolveRows; i++)
+		{
+			const int blk = b0 + i;
+			sv[i] = (blk < b1 && blk >= start && blk < end) ? op_saving_at_bucket(rows[i], bk) : 0u;
+			local += sv[i];
+		}
+		uint32_t tot;
+		uint32_t ex = block_exclusive_scan(local, warp_sums, tot);
+		bool found = false;
+#pragma unroll
+		for (int i = 0; i < kSingleResolveRows; i++)
+		{
+			if (!found && sv[i] != 0 && int64_t(ex) >= required)
+			{
+				atomicMin(&s_cut, uint32_t(b0 + i));
+				found = true;
+			}
+			ex += sv[i];
+		}
+		__syncthreads();
+	}
+	const uint32_t cut = s_cut;
+
+	// Word counts, the block scan of offsets, the per-block decisions.
+	uint32_t w[kSingleResolveRows];
+	int q[kSingleResolveRows];
+	unsigned long long local = 0; // words << 32 | non-empty blocks << 1
+#pragma unroll
+	for (int i = 0; i < kSingleResolveRows; i++)
+	{
+		const int blk = b0 + i;
+		w[i] = 0;
+		q[i] = 0;
+		if (blk < b1)
+		{
+			w[i] = block_words(rows[i], blk, blk >> p.subdivision_shift, xstar, cut, q[i]);
+			local += (uint64_t(w[i]) << 32) | (uint64_t(w[i] != 0 ? 1 : 0) << 1);
+		}
+	}
+	unsigned long long all;
+	unsigned long long pos = block_exclusive_scan(local, warp_sums64, all);
+#pragma unroll
+	for (int i = 0; i < kSingleResolveRows; i++)
+	{
+		const int blk = b0 + i;
+		if (blk < b1)
+		{
+			buf.quant[blk] = q[i];
+			*reinterpret_cast<uint2 *>(buf.block_meta + 2 * size_t(blk)) = make_uint2(uint32_t(pos >> 32), w[i]);
+			pos += uint64_t(w[i]) << 32;
+		}
+	}
+	if (t == 0)
+	{
+		const uint32_t total_words = uint32_t(all >> 32);
+		const uint32_t non_zero = uint32_t(all & 0xffffffffull) >> 1;
+		if (cut != 0xffffffffu)
+			rc->block_cut = cut;
+		rc->xstar = xstar;
+		rc->sequence = p.sequence & 7u;
+		rc->total_words = total_words;
+		rc->non_zero_blocks = non_zero;
+		if (2 + uint64_t(total_words) > buf.stream_capacity_words)
+			atomicOr(&rc->error, kErrorStreamCapacity);
+		// Start-of-frame sequence header (bitstream.md:250-265).
+		buf.stream[0] = uint32_t(p.width - 1) | (uint32_t(p.height - 1) << 14) | ((p.sequence & 7u) << 28) | (1u << 31);
+		buf.stream[1] = (non_zero & 0xffffffu) | (uint32_t(p.chroma444 ? 1 : 0) << 26);
+	}
+}
+
 // Batched form: one CTA per (frame, slice).
 __global__ void __launch_bounds__(kResolveBatchThreads) resolve_batch_kernel(const BatchFrame *frames, const BatchFrameIO *io,
                                                              const uint32_t *cta_map)
@@ -1309,11 +1554,19 @@ LaunchConfig::LaunchConfig(dim3 grid, dim3 block, cudaStream_t stream, bool prog
 	cfg.numAttrs = programmatic ? 1 : 0;
 }
 
+int forward_fused_mode(const LevelParams &p, bool fused_quant)
+{
+	if (!fused_quant)
+		return 0;
+	const int tiles = p.L.tiles_x * p.L.tiles_y * ((p.level == 0 && !p.chroma444) ? 1 : 3);
+	return tiles < kSplitTailTiles ? kFusedSplitTail : 1;
+}
+
 void launch_dwt_forward_level(const LevelParams &p, const PlaneInput &in, const EncodeBuffers &buf,
                               const LevelTileMap *maps, bool fused_quant, bool programmatic, cudaStream_t stream)
 {
 	const dim3 grid(p.L.tiles_x * p.L.tiles_y, (p.level == 0 && !p.chroma444) ? 1 : 3);
-	const int f = fused_quant ? 1 : 0;
+	const int f = forward_fused_mode(p, fused_quant);
 	LevelTileMap m = {};
 	if (maps)
 		m = *maps;
@@ -1329,6 +1582,15 @@ void launch_dwt_forward_level(const LevelParams &p, const PlaneInput &in, const 
 	}
 }
 
+int small_level_items(const SmallLevelParams &sp) { return sp.item_first[2 * kLevels]; }
+
+void launch_dwt_small_levels(const SmallLevelParams &sp, const PlaneInput &in, const EncodeBuffers &buf,
+                             bool programmatic, cudaStream_t stream)
+{
+	LaunchConfig lc(dim3(small_level_items(sp)), dim3(kSmallThreads), stream, programmatic);
+	cudaLaunchKernelEx(&lc.cfg, dwt_small_levels_kernel, sp, in, buf);
+}
+
 void launch_quant_pretransformed(const BlockParams &p, const EncodeBuffers &buf, int nblocks, bool programmatic,
                                  cudaStream_t stream)
 {
@@ -1338,6 +1600,12 @@ void launch_quant_pretransformed(const BlockParams &p, const EncodeBuffers &buf,
 
 void launch_resolve(const ResolveParams &p, const EncodeBuffers &buf, cudaStream_t stream)
 {
+	if (p.block_count_32x32 <= kSingleResolveRows * kSingleResolveThreads)
+	{
+		LaunchConfig lc(dim3(1), dim3(kSingleResolveThreads), stream, true);
+		cudaLaunchKernelEx(&lc.cfg, resolve_single_kernel, p, buf);
+		return;
+	}
 	const int slices = resolve_slices(p.block_count_32x32, p.blocks_per_subdivision);
 	// One thread per block of a slice, 256 to 1024 per CTA.
 	if (p.blocks_per_subdivision >= 1024)

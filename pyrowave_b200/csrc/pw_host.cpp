@@ -381,6 +381,52 @@ BlockParams make_block_params(const Geometry &g)
 	return p;
 }
 
+SmallInverseParams make_small_inverse_params(const Geometry &g, int first_level)
+{
+	SmallInverseParams sp = {};
+	for (int level = 0; level < kLevels; level++)
+		sp.lp[level] = make_level_params(g, level);
+	sp.first_level = first_level;
+	sp.last_level = kLevels - 1;
+	int item = 0;
+	for (int level = kLevels - 1; level >= 0; level--)
+	{
+		const int ncomp = (level == 0 && !g.chroma444) ? 1 : 3;
+		sp.ntiles[level] = g.level[level].tiles_x * g.level[level].tiles_y * ncomp;
+		sp.item_first[level] = item;
+		if (level >= first_level)
+			item += sp.ntiles[level];
+	}
+	return sp;
+}
+
+SmallLevelParams make_small_level_params(const Geometry &g, int first_level)
+{
+	SmallLevelParams sp = {};
+	for (int level = 0; level < kLevels; level++)
+		sp.lp[level] = make_level_params(g, level);
+	sp.bp = make_block_params(g);
+	sp.first_level = first_level;
+	int item = 0;
+	for (int level = 0; level < kLevels; level++)
+	{
+		const int ncomp = (level == 0 && !g.chroma444) ? 1 : 3;
+		const int first = level == kLevels - 1 ? 0 : g.band[0][level][1].block32_offset;
+		const int end = level == 0 ? g.block_count_32x32 : g.band[0][level - 1][1].block32_offset;
+		sp.ntiles[level] = g.level[level].tiles_x * g.level[level].tiles_y * ncomp;
+		sp.block_first[level] = first;
+		sp.block_count[level] = end - first;
+		sp.item_first[2 * level] = item;
+		if (level >= first_level)
+			item += sp.ntiles[level];
+		sp.item_first[2 * level + 1] = item;
+		if (level >= first_level)
+			item += (sp.block_count[level] + 3) / 4;
+	}
+	sp.item_first[2 * kLevels] = item;
+	return sp;
+}
+
 ResolveParams make_resolve_params(const Geometry &g, uint32_t target_words, uint32_t sequence)
 {
 	ResolveParams p = {};
@@ -702,8 +748,10 @@ struct pyrowave_encoder_opaque
 	StageEvents timing;
 	CapturedGraph graph;
 	KernelNode node_dwt[kLevels];
-	int small_level = kLevels; // levels >= this are quantised by one launch after the transform
+	int small_level = kLevels; // levels >= this run in one launch: their transforms and quantisers
 	int small_blocks = 0;      // 32x32 blocks of those levels (a prefix in block index order)
+	SmallLevelParams small = {};
+	KernelNode node_small;
 	KernelNode node_resolve;
 
 	EncodeBuffers buffers() const
@@ -779,6 +827,7 @@ struct pyrowave_encoder_opaque
 			lp[level] = make_level_params(g, level);
 		bp = make_block_params(g);
 		small_level_split(g, small_level, small_blocks);
+		small = make_small_level_params(g, small_level);
 		bool ok = true;
 		coef32 = dev_alloc<float>(size_t(g.storage_elems32), ok);
 		coef16 = dev_alloc<__half>(size_t(g.storage_elems16), ok);
@@ -882,16 +931,17 @@ struct pyrowave_encoder_opaque
 			cudaMemsetAsync(rc, 0, sizeof(RateControlState), s);
 			static const char *const dwt_tags[kLevels] = {"dwt0", "dwt1", "dwt2", "dwt3", "dwt4"};
 			const bool pdl = !device->stage_timing; // event nodes between kernels break programmatic edges
-			for (int level = 0; level < kLevels; level++)
+			for (int level = 0; level < small_level; level++)
 			{
-				launch_dwt_forward_level(lp[level], in, b, &in_maps[level], level < small_level, pdl && level > 0, s);
+				launch_dwt_forward_level(lp[level], in, b, &in_maps[level], true, pdl && level > 0, s);
 				ok = ok && last_captured_node(s, node_dwt[level]);
 				timing.mark(device, s, dwt_tags[level]);
 			}
-			if (small_blocks > 0)
+			if (small_level < kLevels)
 			{
-				launch_quant_pretransformed(bp, b, small_blocks, pdl, s);
-				timing.mark(device, s, "quant");
+				launch_dwt_small_levels(small, in, b, pdl && small_level > 0, s);
+				ok = ok && last_captured_node(s, node_small);
+				timing.mark(device, s, "dwt_small");
 			}
 			launch_resolve(make_resolve_params(g, target_words, sequence_count), b, s);
 			ok = ok && last_captured_node(s, node_resolve);
@@ -911,11 +961,13 @@ struct pyrowave_encoder_opaque
 			PlaneInput pin = in;
 			ResolveParams rp = make_resolve_params(g, target_words, sequence_count);
 			bool ok = true;
-			for (int level = 0; level < kLevels; level++)
+			for (int level = 0; level < small_level; level++)
 			{
-				int fused = level < small_level ? 1 : 0;
+				int fused = forward_fused_mode(lp[level], true);
 				ok = ok && set_kernel_args(graph.exec, node_dwt[level], lp[level], pin, b, fused, in_maps[level]);
 			}
+			if (small_level < kLevels)
+				ok = ok && set_kernel_args(graph.exec, node_small, small, pin, b);
 			ok = ok && set_kernel_args(graph.exec, node_resolve, rp, b);
 			if (!ok)
 			{
@@ -1033,7 +1085,12 @@ struct pyrowave_decoder_opaque
 	KernelNode node_idwt_full[kLevels], node_idwt_only[kLevels];
 
 	LevelTileMap band_maps[kLevels] = {}; // TMA maps of the FP32 bands (inverse transform tile loads)
-	uint32_t *error_d = nullptr;     // kDecodeError* bits of the last decode (cleared by each decode)
+	int small_level = kLevels;            // levels >= this: one inverse launch (coarsest first)
+	int small_blocks = 0;
+	SmallInverseParams small = {};
+	KernelNode node_small_full, node_small_only;
+	DecodeState *state_d = nullptr;  // per-decode state: error bits and the small-levels launch's counters
+	uint32_t *error_d = nullptr;     // &state_d->error: kDecodeError* bits of the last decode (cleared by each decode)
 	uint32_t *h_error = nullptr;     // page-locked copy of error_d
 	cudaEvent_t decode_done = nullptr; // recorded after every decode launch
 	bool decode_pending = false;
@@ -1178,7 +1235,8 @@ struct pyrowave_decoder_opaque
 		dev_free(pk_summaries);
 		dev_free(pk_items);
 		dev_free(pk_first);
-		dev_free(error_d);
+		dev_free(state_d);
+		state_d = nullptr;
 		error_d = nullptr;
 		host_free(h_error);
 		h_error = nullptr;
@@ -1237,10 +1295,13 @@ struct pyrowave_decoder_opaque
 			return PYROWAVE_ERROR_OUT_OF_DEVICE_MEMORY;
 		}
 		cudaMemcpy(jobs_d, jobs.data(), jobs.size() * 4, cudaMemcpyHostToDevice);
-		error_d = dev_alloc<uint32_t>(1, ok);
+		state_d = dev_alloc<DecodeState>(1, ok);
+		error_d = state_d ? &state_d->error : nullptr;
 		h_error = host_alloc<uint32_t>(1, ok);
-		if (error_d)
-			cudaMemset(error_d, 0, sizeof(uint32_t));
+		if (state_d)
+			cudaMemset(state_d, 0, sizeof(DecodeState));
+		small_level_split(g, small_level, small_blocks);
+		small = make_small_inverse_params(g, small_level);
 		if (ok && cudaEventCreateWithFlags(&decode_done, cudaEventDisableTiming) != cudaSuccess)
 			ok = false;
 		build_tile_maps(g, lp, coef32, nullptr, band_maps);
@@ -1305,6 +1366,7 @@ struct pyrowave_decoder_opaque
 	{
 		DecodeInput in = in_args;
 		in.error = error_d;
+		in.state = state_d;
 		timing.collect(device);
 		timing.prepare(device);
 		CapturedGraph &graph = dequant ? graph_full : graph_idwt;
@@ -1316,20 +1378,28 @@ struct pyrowave_decoder_opaque
 			bool ok = true;
 			timing.begin(device, s);
 			const bool pdl = !device->stage_timing; // event nodes between kernels break programmatic edges
-			// The dequantiser clears the error word before any inverse level runs;
+			// The dequantiser clears the decode state before any inverse level runs;
 			// without it the graph starts with a clear of its own.
 			if (!dequant)
-				cudaMemsetAsync(error_d, 0, sizeof(uint32_t), s);
+				cudaMemsetAsync(state_d, 0, sizeof(DecodeState), s);
 			if (dequant)
 			{
 				launch_dequant(bp, in, 0, g.block_count_32x32, false, s);
 				ok = ok && last_captured_node(s, node_dequant);
 				timing.mark(device, s, "dequant");
 			}
-			static const char *const idwt_tags[kLevels] = {"idwt0", "idwt1", "idwt2", "idwt3", "idwt4"};
-			for (int level = kLevels - 1; level >= 0; level--)
+			// Programmatic launches follow a kernel only (not the clear of an inverse-only decode).
+			if (small_level < kLevels)
 			{
-				launch_idwt_level(lp[level], in, out, &band_maps[level], pdl && (dequant || level < kLevels - 1), s);
+				launch_idwt_small_levels(small, in, out, pdl && dequant, s);
+				ok = ok && last_captured_node(s, dequant ? node_small_full : node_small_only);
+				timing.mark(device, s, "idwt_small");
+			}
+			static const char *const idwt_tags[kLevels] = {"idwt0", "idwt1", "idwt2", "idwt3", "idwt4"};
+			for (int level = small_level - 1; level >= 0; level--)
+			{
+				launch_idwt_level(lp[level], in, out, &band_maps[level],
+				                  pdl && (dequant || small_level < kLevels || level < kLevels - 1), s);
 				ok = ok && last_captured_node(s, dequant ? node_idwt_full[level] : node_idwt_only[level]);
 				timing.mark(device, s, idwt_tags[level]);
 			}
@@ -1351,7 +1421,9 @@ struct pyrowave_decoder_opaque
 				int first = 0;
 				ok = set_kernel_args(graph.exec, node_dequant, bp, din, first);
 			}
-			for (int level = 0; level < kLevels; level++)
+			if (small_level < kLevels)
+				ok = ok && set_kernel_args(graph.exec, dequant ? node_small_full : node_small_only, small, din, pout);
+			for (int level = 0; level < small_level; level++)
 				ok = ok && set_kernel_args(graph.exec, dequant ? node_idwt_full[level] : node_idwt_only[level], lp[level],
 				                           din, pout, band_maps[level]);
 			if (!ok)
@@ -2151,6 +2223,43 @@ pyrowave_result pyrowave_cuda_encoder_encode_pre_transformed(pyrowave_encoder en
 		return PYROWAVE_ERROR_GENERIC;
 	encoder->has_device_frame = true;
 	return encoder->queue_readback(s);
+}
+
+pyrowave_result pyrowave_cuda_encoder_transform(pyrowave_encoder encoder, const pyrowave_cuda_planes *planes,
+                                                pyrowave_cuda_stream stream)
+{
+	if (!encoder || !planes)
+		return PYROWAVE_ERROR_INVALID_ARGUMENT;
+	pyrowave_result r = encoder->allocate();
+	if (r != PYROWAVE_SUCCESS)
+		return r;
+	const Geometry &g = encoder->g;
+	PlaneInput in = {};
+	for (int p = 0; p < 3; p++)
+	{
+		if (!planes->data[p] || planes->row_stride_in_bytes[p] < size_t(g.plane_width[p]) ||
+		    planes->row_stride_in_bytes[p] > 0x7fffffffu)
+			return PYROWAVE_ERROR_INVALID_ARGUMENT;
+		in.data[p] = static_cast<const uint8_t *>(planes->data[p]);
+		in.pitch[p] = int32_t(planes->row_stride_in_bytes[p]);
+		in.xstride[p] = 1;
+	}
+	cudaStream_t s = pick_stream(encoder->device, stream);
+	pyrowave_device_opaque *dev = encoder->device;
+	StageEvents &timing = encoder->timing;
+	timing.collect(dev);
+	timing.prepare(dev);
+	timing.begin(dev, s);
+	static const char *const tags[kLevels] = {"xdwt0", "xdwt1", "xdwt2", "xdwt3", "xdwt4"};
+	const EncodeBuffers b = encoder->buffers();
+	for (int level = 0; level < kLevels; level++)
+	{
+		launch_dwt_forward_level(encoder->lp[level], in, b, &encoder->in_maps[level], false,
+		                         level > 0 && !dev->stage_timing, s);
+		timing.mark(dev, s, tags[level]);
+	}
+	timing.launched(dev);
+	return launches_ok("kernel launch") ? PYROWAVE_SUCCESS : PYROWAVE_ERROR_GENERIC;
 }
 
 pyrowave_result pyrowave_cuda_encoder_read_wavelet(pyrowave_encoder encoder, float *pyramid, pyrowave_cuda_stream stream)

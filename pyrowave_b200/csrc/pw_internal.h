@@ -134,18 +134,32 @@ struct RateControlState
 	uint32_t block_cut;            // ops of blocks >= this in the partial subdivision are not applied
 	uint32_t sequence;
 	uint32_t decode_error;         // kDecodeError* bits of the batched form's decode of this frame
+	uint32_t small_ticket;         // next work item of the small-levels launch
+	uint32_t level_done[kLevels];  // transform tiles finished per level (small-levels launch)
 	// Per resolve slice: words << 32 | non-empty blocks << 1 | 1 once published.
 	unsigned long long slice_total[kMaxResolveSlices];
 };
 
 // Error bits of a decoder's error word.
-constexpr uint32_t kDecodeErrorTileWait = 1u; // an inverse-transform tile load did not complete in time
+constexpr uint32_t kDecodeErrorTileWait = 1u;  // an inverse-transform tile load did not complete in time
+constexpr uint32_t kDecodeErrorLevelWait = 2u; // a small-levels tile gave up waiting for the coarser level
+
+// Per-decode device state of a decoder, cleared by the dequantiser (or by a
+// clear before an inverse-only decode).
+struct DecodeState
+{
+	uint32_t error;               // kDecodeError* bits
+	uint32_t ticket;              // next tile of the small-levels inverse launch
+	uint32_t level_done[kLevels]; // tiles finished per level (small-levels inverse launch)
+	uint32_t pad;
+};
 
 // Error bits of RateControlState::error.
 constexpr uint32_t kErrorStreamCapacity = 1u; // the coded frame does not fit the stream buffer
 constexpr uint32_t kErrorWordCount = 2u;      // a packed block's size differs from the rate-control estimate
 constexpr uint32_t kErrorSliceWait = 4u;      // a resolve slice gave up waiting for a preceding slice's total
 constexpr uint32_t kErrorTileWait = 8u;       // a forward-transform tile load did not complete in time
+constexpr uint32_t kErrorLevelWait = 16u;     // a small-levels work item gave up waiting for the items it depends on
 
 // Buffers the encode kernels read and write.
 struct EncodeBuffers
@@ -207,6 +221,7 @@ struct DecodeInput
 	const uint32_t *block_meta; // alternatively {offset, num_words} pairs; num_words == 0 = missing
 	const unsigned long long *keys; // alternatively packet-assembly keys: word offset in the low 30 bits, ~0 = missing
 	uint32_t *error;            // kDecodeError* bits, or nullptr
+	DecodeState *state;         // the decoder's per-decode state (small-levels inverse launch), or nullptr
 	const uint32_t *payload;    // concatenated block words
 	uint32_t payload_words;
 	const uint32_t *jobs;
@@ -259,6 +274,30 @@ struct BlockParams
 	int32_t nbands, block_count_32x32, subdivision_shift;
 	int32_t width, height, chroma444; // frame size and chroma format (sequence header)
 	BandEntry band[kMaxBands]; // in block index order
+};
+
+// The small levels of a frame in one launch (levels first_level..4): work
+// items are ticket ranges, per level first its transform tiles (all
+// components) and then its quantiser items (four 32x32 blocks each).
+struct SmallLevelParams
+{
+	LevelParams lp[kLevels];          // levels >= first_level are used
+	BlockParams bp;
+	int32_t first_level;
+	int32_t item_first[2 * kLevels + 1]; // item_first[2 * level + kind] .. [+ 1]: kind 0 transform, 1 quantiser
+	int32_t ntiles[kLevels];          // transform items per level
+	int32_t block_first[kLevels];     // first 32x32 block of each level (block index order)
+	int32_t block_count[kLevels];
+};
+
+// The small inverse levels of a decode in one launch (levels last_level down
+// to first_level): ticket ranges of each level's tiles, coarsest level first.
+struct SmallInverseParams
+{
+	LevelParams lp[kLevels];
+	int32_t first_level, last_level;
+	int32_t item_first[kLevels];
+	int32_t ntiles[kLevels];
 };
 
 struct ResolveParams
@@ -321,9 +360,21 @@ constexpr int kMaxBatchFrames = 256;
 // launch across the whole GPU after the last level instead of inside the
 // transform of each level.
 constexpr int kSmallLevelTiles = 256;
+// Fused quantiser modes of a forward level launch: 0 none, 1 fused, and
+// kFusedSplitTail (levels of fewer than kSplitTailTiles tiles, about two waves
+// of 256-thread CTAs): a last quantiser round with idle groups runs on the
+// whole CTA instead.
+constexpr int kFusedSplitTail = 2;
+constexpr int kSplitTailTiles = 2 * 148 * 4;
+int forward_fused_mode(const LevelParams &p, bool fused_quant);
 void launch_dwt_forward_level(const LevelParams &p, const PlaneInput &in, const EncodeBuffers &buf,
                               const LevelTileMap *maps, bool fused_quant,
                               bool programmatic, cudaStream_t stream);
+// Small levels (forward transform + quantiser) of one frame in one launch.
+SmallLevelParams make_small_level_params(const Geometry &g, int first_level);
+int small_level_items(const SmallLevelParams &sp);
+void launch_dwt_small_levels(const SmallLevelParams &sp, const PlaneInput &in, const EncodeBuffers &buf,
+                             bool programmatic, cudaStream_t stream);
 // Quantise and analyse the first nblocks 32x32 blocks (block index order) from storage.
 void launch_quant_pretransformed(const BlockParams &p, const EncodeBuffers &buf, int nblocks, bool programmatic,
                                  cudaStream_t stream);
@@ -337,6 +388,10 @@ void launch_idwt_level(const LevelParams &p, const DecodeInput &in, const PlaneO
                        cudaStream_t stream);
 void launch_pyramid_io(const BlockParams &p, float *canonical, float *coef32, __half *coef16, bool to_canonical,
                        cudaStream_t stream);
+// Small inverse levels (coarsest first) of one decode in one launch; `in.state` must be set.
+SmallInverseParams make_small_inverse_params(const Geometry &g, int first_level);
+void launch_idwt_small_levels(const SmallInverseParams &sp, const DecodeInput &in, const PlaneOutput &out,
+                              bool programmatic, cudaStream_t stream);
 
 // Device-side packet assembly (pw_packets.cu). The first four fields of
 // PacketStatus are the public pyrowave_cuda_packet_status.

@@ -335,3 +335,22 @@ def test_tensor_maps_follow_reused_addresses(device):
             assert err is None, err
         enc.close()
         dec.close()
+
+
+@pytest.mark.parametrize("w,h,c444", [(1920, 1080, False), (640, 360, True)])
+def test_transform_only_matches_oracle(device, w, h, c444):
+    """pyrowave_cuda_encoder_transform (the forward levels without the quantiser)
+    gives the oracle's pyramid bit for bit."""
+    import torch
+
+    planes = synth.synth_frame(w, h, c444, 31)
+    chroma = capi.CHROMA_444 if c444 else capi.CHROMA_420
+    enc = capi.Encoder(device, w, h, chroma)
+    d = _to_dev(planes)
+    enc.transform([p.data_ptr() for p in d], [p.stride(0) for p in d])
+    pyr = torch.zeros(enc.layout().pyramid_size, dtype=torch.float32, device="cuda")
+    enc.read_wavelet(pyr.data_ptr())
+    torch.cuda.synchronize()
+    ref = O.Oracle(w, h, c444).dwt(planes, O.MODE_F32)
+    err = _mismatch("transform-only pyramid", pyr.cpu().numpy().view(np.uint32), ref.view(np.uint32))
+    assert err is None, err
