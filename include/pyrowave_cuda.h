@@ -60,6 +60,15 @@ PYROWAVE_PUBLIC_API pyrowave_result pyrowave_cuda_decoder_set_precision(pyrowave
 PYROWAVE_PUBLIC_API pyrowave_result pyrowave_cuda_encoder_get_layout(pyrowave_encoder encoder, pyrowave_cuda_layout *layout);
 PYROWAVE_PUBLIC_API pyrowave_result pyrowave_cuda_decoder_get_layout(pyrowave_decoder decoder, pyrowave_cuda_layout *layout);
 
+/* 16-bit planes (R16_UNORM samples, little-endian uint16: the reference's
+ * high bit depth input and output, encode.cpp:152 and decode.cpp:215 of the
+ * reference) for pyrowave_encoder_encode_cpu_synchronous and
+ * pyrowave_decoder_decode_cpu_buffer_synchronous: row strides and plane sizes
+ * in bytes, as for the 8-bit formats. These values extend the reference's
+ * pyrowave_cpu_buffer_format, which has no 16-bit planar formats. */
+#define PYROWAVE_CPU_BUFFER_FORMAT_YUV420P16 ((pyrowave_cpu_buffer_format)0x101)
+#define PYROWAVE_CPU_BUFFER_FORMAT_YUV444P16 ((pyrowave_cpu_buffer_format)0x102)
+
 /* Encode device planes on `stream`; returns without waiting. The packetized
  * frame (8-byte start-of-frame header followed by the coded 32x32 blocks in
  * block index order, exactly what pyrowave_encoder_packetize emits with an
@@ -68,6 +77,13 @@ PYROWAVE_PUBLIC_API pyrowave_result pyrowave_cuda_encoder_encode(pyrowave_encode
                                                                  const pyrowave_cuda_planes *planes,
                                                                  const pyrowave_rate_control *rate_control,
                                                                  pyrowave_cuda_stream stream);
+
+/* As pyrowave_cuda_encoder_encode, from 16-bit planes (R16_UNORM samples, each
+ * row_stride_in_bytes a multiple of 2 and at least 2 * width). */
+PYROWAVE_PUBLIC_API pyrowave_result pyrowave_cuda_encoder_encode16(pyrowave_encoder encoder,
+                                                                   const pyrowave_cuda_planes *planes,
+                                                                   const pyrowave_rate_control *rate_control,
+                                                                   pyrowave_cuda_stream stream);
 
 /* Device view of the last encode: stream = packetized frame (words), block_meta
  * = {offset_u32, num_words} per 32x32 block (the reference's BitstreamPacket
@@ -137,6 +153,14 @@ PYROWAVE_PUBLIC_API pyrowave_result pyrowave_cuda_decoder_decode_blocks(pyrowave
                                                                         const uint32_t *words, size_t num_words,
                                                                         const pyrowave_cuda_planes *planes,
                                                                         pyrowave_cuda_stream stream);
+
+/* As pyrowave_cuda_decoder_decode_blocks, into 16-bit planes (R16_UNORM samples,
+ * each row_stride_in_bytes a multiple of 2 and at least 2 * width). */
+PYROWAVE_PUBLIC_API pyrowave_result pyrowave_cuda_decoder_decode_blocks16(pyrowave_decoder decoder,
+                                                                          const uint32_t *block_meta,
+                                                                          const uint32_t *words, size_t num_words,
+                                                                          const pyrowave_cuda_planes *planes,
+                                                                          pyrowave_cuda_stream stream);
 
 /* Assemble a frame from received packets on the GPU and decode it: the
  * device-side counterpart of pyrowave_decoder_clear, then

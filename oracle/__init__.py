@@ -109,6 +109,10 @@ def lib():
         L.oracle_idwt.argtypes = [c_void_p, c_void_p, c_int, c_void_p, c_void_p]
         L.oracle_idwt_f64.restype = c_int
         L.oracle_idwt_f64.argtypes = [c_void_p, c_void_p, c_void_p, c_void_p]
+        L.oracle_dwt16.restype = c_int
+        L.oracle_dwt16.argtypes = [c_void_p, c_void_p, c_void_p, c_int, c_void_p]
+        L.oracle_idwt16.restype = c_int
+        L.oracle_idwt16.argtypes = [c_void_p, c_void_p, c_int, c_void_p, c_void_p]
         L.oracle_float_to_half.restype = c_uint16
         L.oracle_float_to_half.argtypes = [c_float]
         L.oracle_half_to_float.restype = c_float
@@ -176,6 +180,15 @@ class Oracle:
 
     # --- transform ------------------------------------------------------------
     def dwt(self, planes, mode: int = MODE_F32) -> np.ndarray:
+        """Forward transform of 8-bit planes, or of 16-bit (R16_UNORM) planes when they are uint16."""
+        if np.asarray(planes[0]).dtype == np.uint16:
+            arrs = [np.ascontiguousarray(p, np.uint16) for p in planes]
+            ptrs = (c_void_p * 3)(*[a.ctypes.data for a in arrs])
+            strides = (c_int * 3)(*[a.shape[1] for a in arrs])
+            out = np.zeros(self.pyramid_size, np.float32)
+            if self.L.oracle_dwt16(self.h, ptrs, strides, mode, _ptr(out)) != 0:
+                raise RuntimeError("oracle_dwt16 failed")
+            return out
         arrs, ptrs, strides = _plane_args(planes)
         if mode == MODE_F64:
             out = np.zeros(self.pyramid_size, np.float64)
@@ -186,6 +199,16 @@ class Oracle:
         if rc != 0:
             raise RuntimeError("oracle_dwt failed")
         return out
+
+    def idwt16(self, pyramid: np.ndarray, mode: int = MODE_F32):
+        """Inverse transform into 16-bit (R16_UNORM) planes."""
+        outs = [np.zeros(s, np.uint16) for s in self.plane_shapes()]
+        ptrs = (c_void_p * 3)(*[a.ctypes.data for a in outs])
+        strides = (c_int * 3)(*[a.shape[1] for a in outs])
+        p = np.ascontiguousarray(pyramid, np.float32)
+        if self.L.oracle_idwt16(self.h, _ptr(p), mode, ptrs, strides) != 0:
+            raise RuntimeError("oracle_idwt16 failed")
+        return outs
 
     def idwt(self, pyramid: np.ndarray, mode: int = MODE_F32):
         outs = [np.zeros(s, np.uint8) for s in self.plane_shapes()]

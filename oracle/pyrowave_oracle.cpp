@@ -19,6 +19,7 @@
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
+#include <type_traits>
 #include <vector>
 
 namespace
@@ -1187,7 +1188,13 @@ void dequant_block(const oracle_codec &c, const uint32_t *offsets, const uint32_
 	}
 }
 
-template <typename T> void load_plane(Plane<T> &p, const uint8_t *data, int stride, int w, int h, bool round16)
+// UNORM texel of an 8-bit (R8_UNORM) or 16-bit (R16_UNORM, encode.cpp:152) plane.
+template <typename S> constexpr float unorm_max() { return sizeof(S) == 1 ? 255.0f : 65535.0f; }
+
+// The DWT input: UNORM value minus the DC shift of 0.5 (dwt.comp:48,66,75,85).
+// `stride` is in samples.
+template <typename T, typename S>
+void load_plane(Plane<T> &p, const S *data, int stride, int w, int h, bool round16)
 {
 	p.width = w;
 	p.height = h;
@@ -1197,10 +1204,10 @@ template <typename T> void load_plane(Plane<T> &p, const uint8_t *data, int stri
 		{
 			T v;
 			if (std::is_same<T, double>::value)
-				v = T(double(data[size_t(y) * stride + x]) / 255.0 - 0.5);
+				v = T(double(data[size_t(y) * stride + x]) / double(unorm_max<S>()) - 0.5);
 			else
 			{
-				float f = float(data[size_t(y) * stride + x]) / 255.0f;
+				float f = float(data[size_t(y) * stride + x]) / unorm_max<S>();
 				f = f - 0.5f;
 				v = T(f);
 			}
@@ -1217,8 +1224,8 @@ template <typename T> T store_round(const oracle_codec &c, int level, T v, int m
 	return v;
 }
 
-template <typename T>
-int run_dwt(oracle_codec &c, const uint8_t *const planes[3], const int strides[3], int mode, T *out)
+template <typename T, typename S = uint8_t>
+int run_dwt(oracle_codec &c, const S *const planes[3], const int strides[3], int mode, T *out)
 {
 	bool round16 = mode == ORACLE_MODE_REF16;
 	for (int comp = 0; comp < NumComponents; comp++)
@@ -1260,8 +1267,10 @@ int run_dwt(oracle_codec &c, const uint8_t *const planes[3], const int strides[3
 	return 0;
 }
 
-template <typename T>
-int run_idwt(oracle_codec &c, const T *pyramid, int mode, uint8_t *const planes[3], const int strides[3])
+// The final store adds the DC shift back and converts to UNORM with the
+// store's clamp (idwt.comp:208-211); `strides` in samples.
+template <typename T, typename S = uint8_t>
+int run_idwt(oracle_codec &c, const T *pyramid, int mode, S *const planes[3], const int strides[3])
 {
 	bool round16 = mode == ORACLE_MODE_REF16;
 	for (int comp = 0; comp < NumComponents; comp++)
@@ -1298,18 +1307,18 @@ int run_idwt(oracle_codec &c, const T *pyramid, int mode, uint8_t *const planes[
 					for (int x = 0; x < pw; x++)
 					{
 						T v = out[size_t(y) * ow + x];
-						uint8_t u;
+						S u;
 						if (std::is_same<T, double>::value)
 						{
 							double f = double(v) + 0.5;
 							f = std::min(std::max(f, 0.0), 1.0);
-							u = uint8_t(int(f * 255.0 + 0.5));
+							u = S(int(f * double(unorm_max<S>()) + 0.5));
 						}
 						else
 						{
 							float f = float(v) + 0.5f;
 							f = std::min(std::max(f, 0.0f), 1.0f);
-							u = uint8_t(int(f * 255.0f + 0.5f));
+							u = S(int(f * unorm_max<S>() + 0.5f));
 						}
 						planes[comp][size_t(y) * strides[comp] + x] = u;
 					}
@@ -1534,6 +1543,13 @@ int oracle_dwt(oracle_codec *c, const uint8_t *const planes[3], const int stride
 int oracle_dwt_f64(oracle_codec *c, const uint8_t *const planes[3], const int strides[3], double *out)
 {
 	return run_dwt<double>(*c, planes, strides, ORACLE_MODE_F64, out);
+}
+
+int oracle_dwt16(oracle_codec *c, const uint16_t *const planes[3], const int strides[3], int mode, float *out)
+{
+	if (mode != ORACLE_MODE_F32 && mode != ORACLE_MODE_REF16)
+		return -1;
+	return run_dwt<float, uint16_t>(*c, planes, strides, mode, out);
 }
 
 // pyrowave_encoder.cpp:1117-1183 minus the DWT: quant -> analyze -> finalize ->
@@ -1816,6 +1832,13 @@ int oracle_idwt(oracle_codec *c, const float *pyramid, int mode, uint8_t *const 
 int oracle_idwt_f64(oracle_codec *c, const double *pyramid, uint8_t *const planes[3], const int strides[3])
 {
 	return run_idwt<double>(*c, pyramid, ORACLE_MODE_F64, planes, strides);
+}
+
+int oracle_idwt16(oracle_codec *c, const float *pyramid, int mode, uint16_t *const planes[3], const int strides[3])
+{
+	if (mode != ORACLE_MODE_F32 && mode != ORACLE_MODE_REF16)
+		return -1;
+	return run_idwt<float, uint16_t>(*c, pyramid, mode, planes, strides);
 }
 
 uint16_t oracle_float_to_half(float v) { return float_to_half(v); }

@@ -72,6 +72,8 @@ void oracle_quant_tables(const oracle_codec *codec, float *quant_resolution, flo
  * planes/strides: Y, Cb, Cr (4:2:0 chroma planes are width/2 x height/2). */
 int oracle_dwt(oracle_codec *codec, const uint8_t *const planes[3], const int strides[3], int mode, float *out_pyramid);
 int oracle_dwt_f64(oracle_codec *codec, const uint8_t *const planes[3], const int strides[3], double *out_pyramid);
+/* 16-bit (R16_UNORM) planes, strides in samples. */
+int oracle_dwt16(oracle_codec *codec, const uint16_t *const planes[3], const int strides[3], int mode, float *out_pyramid);
 
 /* Encodes a canonical pyramid (the reference's Encoder::encode_pre_transformed when
  * quant_scale >= 0, otherwise the default per-band resolutions). Results are kept
@@ -116,6 +118,7 @@ int oracle_dequant(const oracle_codec *codec, const uint32_t *offsets, const uin
 /* Inverse DWT of a canonical pyramid into 8-bit planes. */
 int oracle_idwt(oracle_codec *codec, const float *pyramid, int mode, uint8_t *const planes[3], const int strides[3]);
 int oracle_idwt_f64(oracle_codec *codec, const double *pyramid, uint8_t *const planes[3], const int strides[3]);
+int oracle_idwt16(oracle_codec *codec, const float *pyramid, int mode, uint16_t *const planes[3], const int strides[3]);
 
 /* PSNR-HVS-M (shaders/psnr_hvs_m.comp, psnr.cpp:25-28,126-224,245-320 of the
  * reference): adds, per height factor 1 + i/8 (i = 0..15), the fixed-point

@@ -38,6 +38,9 @@ REFERENCE_PRECISION = PRECISION_STAGE16 | 0x3
 FORMAT_NV12 = 0
 FORMAT_YUV420P = 1
 FORMAT_YUV444P = 2
+# 16-bit planar extensions (pyrowave_cuda.h): R16_UNORM samples.
+FORMAT_YUV420P16 = 0x101
+FORMAT_YUV444P16 = 0x102
 
 # Every exported symbol of include/pyrowave.h and include/pyrowave_cuda.h.
 API_SYMBOLS = [
@@ -62,6 +65,7 @@ API_SYMBOLS = [
     "pyrowave_cuda_decoder_decode_packets", "pyrowave_cuda_decoder_get_packet_status",
     "pyrowave_cuda_decoder_get_error", "pyrowave_cuda_decode_blocks_static",
     "pyrowave_cuda_psnr_hvs_m", "pyrowave_psnr_hvs_m_pixels", "pyrowave_psnr_hvs_m_from_errors",
+    "pyrowave_cuda_encoder_encode16", "pyrowave_cuda_decoder_decode_blocks16",
     "pyrowave_cuda_batch_create", "pyrowave_cuda_batch_destroy", "pyrowave_cuda_batch_encode",
     "pyrowave_cuda_batch_get_device_bitstream", "pyrowave_cuda_batch_get_sizes", "pyrowave_cuda_batch_autotune",
     "pyrowave_cuda_server_create", "pyrowave_cuda_server_destroy", "pyrowave_cuda_server_open_stream",
@@ -204,6 +208,9 @@ def lib():
                                                        POINTER(CudaPlanes), c_void_p]
     L.pyrowave_cuda_decoder_get_packet_status.argtypes = [c_void_p, POINTER(PacketStatus)]
     L.pyrowave_cuda_decoder_get_error.argtypes = [c_void_p, POINTER(c_uint32)]
+    L.pyrowave_cuda_encoder_encode16.argtypes = [c_void_p, POINTER(CudaPlanes), POINTER(RateControl), c_void_p]
+    L.pyrowave_cuda_decoder_decode_blocks16.argtypes = [c_void_p, c_void_p, c_void_p, c_size_t, POINTER(CudaPlanes),
+                                                        c_void_p]
     L.pyrowave_cuda_psnr_hvs_m.argtypes = [c_int, c_int, c_void_p, c_size_t, c_void_p, c_size_t, c_void_p, c_void_p]
     L.pyrowave_psnr_hvs_m_pixels.argtypes = [c_int, c_int]
     L.pyrowave_psnr_hvs_m_pixels.restype = ctypes.c_uint64
@@ -344,7 +351,11 @@ class Encoder:
 
     def encode_cpu(self, planes, budget: int, fmt: int | None = None) -> int:
         if fmt is None:
-            fmt = FORMAT_YUV444P if self.chroma == CHROMA_444 else FORMAT_YUV420P
+            wide = np.asarray(planes[0]).dtype == np.uint16
+            if self.chroma == CHROMA_444:
+                fmt = FORMAT_YUV444P16 if wide else FORMAT_YUV444P
+            else:
+                fmt = FORMAT_YUV420P16 if wide else FORMAT_YUV420P
         buf, keep = cpu_buffer(planes, self.width, self.height, fmt)
         rc = RateControl(budget)
         return self.L.pyrowave_encoder_encode_cpu_synchronous(self.h, ctypes.byref(buf), ctypes.byref(rc))
@@ -372,6 +383,16 @@ class Encoder:
         rc = RateControl(budget)
         check(self.L.pyrowave_cuda_encoder_encode(self.h, ctypes.byref(cp), ctypes.byref(rc), c_void_p(stream)),
               "pyrowave_cuda_encoder_encode")
+
+    def encode_device16(self, plane_ptrs, strides, budget: int, stream: int = 0):
+        """pyrowave_cuda_encoder_encode16: 16-bit (R16_UNORM) device planes; strides in bytes."""
+        cp = CudaPlanes()
+        for i in range(3):
+            cp.data[i] = plane_ptrs[i]
+            cp.row_stride_in_bytes[i] = strides[i]
+        rc = RateControl(budget)
+        check(self.L.pyrowave_cuda_encoder_encode16(self.h, ctypes.byref(cp), ctypes.byref(rc), c_void_p(stream)),
+              "pyrowave_cuda_encoder_encode16")
 
     def transform(self, plane_ptrs, strides, stream: int = 0):
         """pyrowave_cuda_encoder_transform: the five forward levels alone (no quantiser)."""
@@ -467,11 +488,18 @@ class Decoder:
     def is_ready(self, allow_partial: bool = False) -> bool:
         return bool(self.L.pyrowave_decoder_decode_is_ready(self.h, allow_partial))
 
-    def decode_cpu(self, planes=None, fmt: int | None = None):
+    def decode_cpu(self, planes=None, fmt: int | None = None, wide: bool = False):
+        """Synchronous decode into host planes (uint16 planes, or wide=True: 16-bit output)."""
+        if planes is not None:
+            wide = np.asarray(planes[0]).dtype == np.uint16
         if fmt is None:
-            fmt = FORMAT_YUV444P if self.chroma == CHROMA_444 else FORMAT_YUV420P
+            if self.chroma == CHROMA_444:
+                fmt = FORMAT_YUV444P16 if wide else FORMAT_YUV444P
+            else:
+                fmt = FORMAT_YUV420P16 if wide else FORMAT_YUV420P
         if planes is None:
-            planes = [np.zeros(s, np.uint8) for s in _plane_shapes(self.width, self.height, self.chroma)]
+            planes = [np.zeros(s, np.uint16 if wide else np.uint8)
+                      for s in _plane_shapes(self.width, self.height, self.chroma)]
         buf, keep = cpu_buffer(planes, self.width, self.height, fmt)
         code = self.L.pyrowave_decoder_decode_cpu_buffer_synchronous(self.h, ctypes.byref(buf))
         return code, planes
@@ -490,6 +518,16 @@ class Decoder:
             cp.row_stride_in_bytes[i] = strides[i]
         check(self.L.pyrowave_cuda_decoder_decode_blocks(self.h, c_void_p(meta_ptr), c_void_p(words_ptr), num_words,
                                                          ctypes.byref(cp), c_void_p(stream)), "decode_blocks")
+
+    def decode_blocks16(self, meta_ptr: int, words_ptr: int, num_words: int, plane_ptrs, strides, stream: int = 0):
+        """pyrowave_cuda_decoder_decode_blocks16: into 16-bit device planes; strides in bytes."""
+        cp = CudaPlanes()
+        for i in range(3):
+            cp.data[i] = plane_ptrs[i]
+            cp.row_stride_in_bytes[i] = strides[i]
+        check(self.L.pyrowave_cuda_decoder_decode_blocks16(self.h, c_void_p(meta_ptr), c_void_p(words_ptr),
+                                                           num_words, ctypes.byref(cp), c_void_p(stream)),
+              "decode_blocks16")
 
     def decode_packets(self, data_ptr: int, data_size: int, packets_ptr: int, count: int, plane_ptrs, strides,
                        stream: int = 0) -> int:

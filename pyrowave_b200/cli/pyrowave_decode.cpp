@@ -17,6 +17,7 @@
 #include <vector>
 
 #include "pyrowave.h"
+#include "pyrowave_cuda.h"
 #include "wave_container.hpp"
 #include "y4m.hpp"
 
@@ -60,8 +61,7 @@ int main(int argc, char **argv)
 	std::string error;
 	if (!read_wave_header(s.in, wh, error))
 		return fail(error);
-	if (format_is_16bit(wh.format))
-		return fail("16-bit streams are not supported (this library codes 8-bit planes)");
+	const bool wide = format_is_16bit(wh.format);
 	if (wh.chroma == 0 && ((wh.width | wh.height) & 1))
 		return fail("4:2:0 streams need an even width and height");
 
@@ -80,6 +80,7 @@ int main(int argc, char **argv)
 	info.width = wh.width;
 	info.height = wh.height;
 	info.format = wh.format;
+	info.bit_depth = wide ? 16 : 8;
 	info.full_range = wh.full_range;
 	info.frame_rate_num = wh.frame_rate_num;
 	info.frame_rate_den = wh.frame_rate_den;
@@ -92,7 +93,7 @@ int main(int argc, char **argv)
 	{
 		int w, h;
 		plane_dims(info, p, w, h);
-		planes[p].assign(size_t(w) * size_t(h), 0);
+		planes[p].assign(size_t(w) * size_t(h) * (wide ? 2 : 1), 0);
 	}
 	std::vector<uint8_t> packet;
 	size_t frames = 0, packets = 0;
@@ -118,12 +119,15 @@ int main(int argc, char **argv)
 			int w, h;
 			plane_dims(info, p, w, h);
 			buf.data[p] = planes[p].data();
-			buf.row_stride_in_bytes[p] = size_t(w);
+			buf.row_stride_in_bytes[p] = size_t(w) * (wide ? 2 : 1);
 			buf.plane_size_in_bytes[p] = planes[p].size();
 		}
 		buf.width = wh.width;
 		buf.height = wh.height;
-		buf.format = wh.chroma == 0 ? PYROWAVE_CPU_BUFFER_FORMAT_YUV420P : PYROWAVE_CPU_BUFFER_FORMAT_YUV444P;
+		if (wide)
+			buf.format = wh.chroma == 0 ? PYROWAVE_CPU_BUFFER_FORMAT_YUV420P16 : PYROWAVE_CPU_BUFFER_FORMAT_YUV444P16;
+		else
+			buf.format = wh.chroma == 0 ? PYROWAVE_CPU_BUFFER_FORMAT_YUV420P : PYROWAVE_CPU_BUFFER_FORMAT_YUV444P;
 		if (pyrowave_decoder_decode_cpu_buffer_synchronous(s.decoder, &buf) != PYROWAVE_SUCCESS)
 			return fail("decode failed at frame " + std::to_string(frames));
 		if (!output.write_frame(planes))

@@ -1,8 +1,9 @@
 // pyrowave-encode <input.y4m> <output.pyrowave> <bytes_per_frame>
 //
 // The reference's encoder tool (encode.cpp:128-261) over this library's C API:
-// every frame of an 8-bit 4:2:0 or 4:4:4 YUV4MPEG2 stream is encoded at the
-// given byte budget and written to the .pyrowave container as one packet.
+// every frame of a 4:2:0 or 4:4:4 YUV4MPEG2 stream, 8-bit or 10- to 16-bit
+// (coded from 16-bit planes, encode.cpp:152), is encoded at the given byte
+// budget and written to the .pyrowave container as one packet.
 // Messages go to stderr; the exit status is 0 on success and 1 on any error
 // (the reference prints the error and exits 0).
 #include <stdint.h>
@@ -13,6 +14,7 @@
 #include <vector>
 
 #include "pyrowave.h"
+#include "pyrowave_cuda.h"
 #include "wave_container.hpp"
 #include "y4m.hpp"
 
@@ -58,8 +60,7 @@ int main(int argc, char **argv)
 	if (!input.open(argv[1], error))
 		return fail(error);
 	const Y4mInfo &info = input.info();
-	if (format_is_16bit(info.format))
-		return fail("16-bit YUV4MPEG2 input is not supported (this library codes 8-bit planes)");
+	const bool wide = format_is_16bit(info.format);
 	const bool c420 = format_is_420(info.format);
 	if (c420 && ((info.width | info.height) & 1))
 		return fail("4:2:0 input needs an even width and height");
@@ -81,6 +82,8 @@ int main(int argc, char **argv)
 	WaveHeader wh;
 	wh.width = info.width;
 	wh.height = info.height;
+	// 10- to 14-bit streams were up-converted to 16 bits, so the container
+	// records the 16-bit format of the same chroma (as the reference does).
 	wh.format = info.format;
 	wh.chroma = c420 ? 0 : 1;
 	wh.full_range = info.full_range;
@@ -110,12 +113,15 @@ int main(int argc, char **argv)
 			int w, h;
 			plane_dims(info, p, w, h);
 			buf.data[p] = planes[p].data();
-			buf.row_stride_in_bytes[p] = size_t(w);
+			buf.row_stride_in_bytes[p] = size_t(w) * (wide ? 2 : 1);
 			buf.plane_size_in_bytes[p] = planes[p].size();
 		}
 		buf.width = info.width;
 		buf.height = info.height;
-		buf.format = c420 ? PYROWAVE_CPU_BUFFER_FORMAT_YUV420P : PYROWAVE_CPU_BUFFER_FORMAT_YUV444P;
+		if (wide)
+			buf.format = c420 ? PYROWAVE_CPU_BUFFER_FORMAT_YUV420P16 : PYROWAVE_CPU_BUFFER_FORMAT_YUV444P16;
+		else
+			buf.format = c420 ? PYROWAVE_CPU_BUFFER_FORMAT_YUV420P : PYROWAVE_CPU_BUFFER_FORMAT_YUV444P;
 		if (pyrowave_encoder_encode_cpu_synchronous(s.encoder, &buf, &rc) != PYROWAVE_SUCCESS)
 			return fail("encode failed at frame " + std::to_string(frames));
 		size_t num_packets = 0, got = 0;

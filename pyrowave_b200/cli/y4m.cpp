@@ -120,9 +120,15 @@ bool parse_params(const std::string &params, Y4mInfo &info, std::string &error)
 			else if (val == "444")
 				info.format = Y4mFormat::YUV444P;
 			else if (val == "420p10" || val == "420p12" || val == "420p14" || val == "420p16")
+			{
 				info.format = Y4mFormat::YUV420P16;
+				info.bit_depth = atoi(val.c_str() + 4);
+			}
 			else if (val == "444p10" || val == "444p12" || val == "444p14" || val == "444p16")
+			{
 				info.format = Y4mFormat::YUV444P16;
+				info.bit_depth = atoi(val.c_str() + 4);
+			}
 			else
 			{
 				error = "unsupported chroma format '" + tok + "' (4:2:0 and 4:4:4 only)";
@@ -200,6 +206,19 @@ bool Y4mReader::read_frame(std::vector<uint8_t> (&planes)[3], std::string &error
 		{
 			error = "stream ends inside a frame";
 			return false;
+		}
+		if (bpc == 2 && info_.bit_depth < 16)
+		{
+			// Up-convert to 16 bits (yuv4mpeg.cpp:191-213): min(1, v / max) * 65535, rounded.
+			const float max_code = float((1 << info_.bit_depth) - 1);
+			for (size_t i = 0; i + 1 < planes[p].size(); i += 2)
+			{
+				const uint32_t v = uint32_t(planes[p][i]) | (uint32_t(planes[p][i + 1]) << 8);
+				const float f = float(v) / max_code;
+				const uint32_t u = uint32_t((f < 1.0f ? f : 1.0f) * 65535.0f + 0.5f);
+				planes[p][i] = uint8_t(u);
+				planes[p][i + 1] = uint8_t(u >> 8);
+			}
 		}
 	}
 	return true;

@@ -8,10 +8,14 @@
 // LIMITED sets the range flag (limited by default). A tag of "jpeg" marks
 // centred chroma. Frames: a "FRAME" line (optionally with tags), then Y, Cb, Cr.
 //
-// The reference up-converts 10- to 16-bit streams (C420p10 ... C444p16) to 16-bit
-// planes; this library codes 8-bit planes only, so those streams are reported as
-// unsupported. Other chroma tags (C422, Cmono, C444alpha), which the reference
-// reads as 4:2:0 or 4:4:4 planes of the wrong size, are rejected.
+// 10- to 16-bit streams (C420p10 ... C444p16; little-endian 16-bit samples)
+// are up-converted to full-range 16-bit planes on reading, min(1, v / max) *
+// 65535 rounded, max being the stream's largest code (yuv4mpeg.cpp:101-141,
+// 191-213), and written back at 16 bits (C420p16 / C444p16, as the reference's
+// decoder writes them). The reference up-converts only 4:2:0 streams and reads
+// 4:4:4 ones raw; here both are converted. Other chroma tags (C422, Cmono,
+// C444alpha), which the reference reads as 4:2:0 or 4:4:4 planes of the wrong
+// size, are rejected.
 #pragma once
 
 #include <stdint.h>
@@ -41,12 +45,14 @@ struct Y4mInfo
 	bool center_chroma = false;
 	int frame_rate_num = 60;
 	int frame_rate_den = 1;
+	int bit_depth = 8; // 8, or 10 / 12 / 14 / 16 for the 16-bit formats
 };
 
 bool format_is_16bit(Y4mFormat f);
 bool format_is_420(Y4mFormat f);
 
-// Plane sizes of one 8-bit frame (4:2:0 chroma rounds up, as YUV4MPEG2 does).
+// Plane sizes in samples (4:2:0 chroma rounds up, as YUV4MPEG2 does); 16-bit
+// formats take two bytes per sample.
 void plane_dims(const Y4mInfo &info, int plane, int &w, int &h);
 size_t frame_bytes(const Y4mInfo &info);
 
@@ -60,7 +66,8 @@ public:
 	~Y4mReader();
 	bool open(const char *path, std::string &error);
 	const Y4mInfo &info() const { return info_; }
-	// Reads the next frame into planes[3] (resized as needed). Returns false at
+	// Reads the next frame into planes[3] (resized as needed; 16-bit formats as
+	// little-endian 16-bit samples, up-converted to 16 bits). Returns false at
 	// the end of the stream; `error` is empty there, and holds a message when
 	// the stream is malformed or ends inside a frame.
 	bool read_frame(std::vector<uint8_t> (&planes)[3], std::string &error);

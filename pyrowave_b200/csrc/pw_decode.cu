@@ -523,7 +523,21 @@ __device__ __forceinline__ void idwt_body(IdwtShared &sh, const LevelParams &p, 
 			const int pw = p.plane_width[comp], ph = p.plane_height[comp];
 			uint8_t *const plane = comp == 0 ? out.data[0] : (comp == 1 ? out.data[1] : out.data[2]);
 			const int opitch = comp == 0 ? out.pitch[0] : (comp == 1 ? out.pitch[1] : out.pitch[2]);
-			if (gy < ph)
+			if (gy < ph && out.sample16)
+			{
+				// 16-bit samples (R16_UNORM store: clamp, then round to 1/65535).
+				uint16_t *dst = reinterpret_cast<uint16_t *>(plane + size_t(gy) * opitch);
+#pragma unroll
+				for (int jj = 4; jj < 4 + kOut; jj++)
+				{
+					float f = __fadd_rn(e[jj], 0.5f);
+					f = fminf(fmaxf(f, 0.0f), 1.0f);
+					const int gx = gx0 + jj - 4;
+					if (gx < pw)
+						dst[gx] = uint16_t(int(__fadd_rn(__fmul_rn(f, 65535.0f), 0.5f)));
+				}
+			}
+			else if (gy < ph)
 			{
 				uint8_t *dst = plane + size_t(gy) * opitch;
 				uint32_t packed[kOut / 4];

@@ -405,8 +405,38 @@ __device__ __forceinline__ void dwt_forward_body(DwtShared &sh, const LevelParam
 		const uint8_t *src = comp == 0 ? in.data[0] : (comp == 1 ? in.data[1] : in.data[2]);
 		const int pitch = comp == 0 ? in.pitch[0] : (comp == 1 ? in.pitch[1] : in.pitch[2]);
 		const int xs = comp == 0 ? in.xstride[0] : (comp == 1 ? in.xstride[1] : in.xstride[2]);
-		const bool vec_ok = interior && xs == 1 && ((reinterpret_cast<uintptr_t>(src) | uintptr_t(pitch)) & 3u) == 0;
-		if (vec_ok)
+		const bool vec_ok = interior && xs == 1 && !in.sample16 &&
+		                    ((reinterpret_cast<uintptr_t>(src) | uintptr_t(pitch)) & 3u) == 0;
+		if (in.sample16)
+		{
+			// 16-bit samples (R16_UNORM): u / 65535 - 0.5, gathered through the index tables.
+			for (int base = threadIdx.x; base < kTileIn * kTileIn; base += kThreads * Split::kGen)
+			{
+				uint32_t v[Split::kGen];
+#pragma unroll
+				for (int u = 0; u < Split::kGen; u++)
+				{
+					const int k = base + u * kThreads;
+					const int i = k / kTileIn, j = k - i * kTileIn;
+					v[u] = k < kTileIn * kTileIn
+					           ? uint32_t(*reinterpret_cast<const uint16_t *>(src + size_t(sh.yidx[i]) * pitch +
+					                                                          size_t(sh.xidx[j]) * xs))
+					           : 0u;
+				}
+#pragma unroll
+				for (int u = 0; u < Split::kGen; u++)
+				{
+					const int k = base + u * kThreads;
+					if (k < kTileIn * kTileIn)
+					{
+						const int i = k / kTileIn, j = k - i * kTileIn;
+						const float f = __fsub_rn(__fdiv_rn(float(v[u]), 65535.0f), 0.5f);
+						sh.in[i][j] = L.stage16 ? round_to_half(f) : f;
+					}
+				}
+			}
+		}
+		else if (vec_ok)
 		{
 			uint32_t v[kVecIters];
 #pragma unroll

@@ -884,8 +884,8 @@ struct pyrowave_encoder_opaque
 		bool ok = true;
 		for (int c = 0; c < 3; c++)
 		{
-			// Chroma rows are sized for the interleaved CbCr plane of NV12 as well.
-			in_pitch[c] = align_up(c == 0 ? g.plane_width[c] : 2 * g.plane_width[c], 128);
+			// Rows are sized for 16-bit samples and for the interleaved CbCr plane of NV12.
+			in_pitch[c] = align_up(2 * g.plane_width[c], 128);
 			in_planes[c] = dev_alloc<uint8_t>(size_t(in_pitch[c]) * g.plane_height[c], ok);
 		}
 		return ok ? PYROWAVE_SUCCESS : PYROWAVE_ERROR_OUT_OF_DEVICE_MEMORY;
@@ -1354,7 +1354,7 @@ struct pyrowave_decoder_opaque
 		bool ok = true;
 		for (int c = 0; c < 3; c++)
 		{
-			out_pitch[c] = align_up(g.plane_width[c], 128);
+			out_pitch[c] = align_up(2 * g.plane_width[c], 128); // room for 16-bit samples
 			out_planes[c] = dev_alloc<uint8_t>(size_t(out_pitch[c]) * g.plane_height[c], ok);
 		}
 		return ok ? PYROWAVE_SUCCESS : PYROWAVE_ERROR_OUT_OF_DEVICE_MEMORY;
@@ -1800,22 +1800,32 @@ pyrowave_result pyrowave_encoder_encode_cpu_synchronous(pyrowave_encoder encoder
 	const Geometry &g = encoder->g;
 	const pyrowave_chroma_subsampling chroma =
 	    g.chroma444 ? PYROWAVE_CHROMA_SUBSAMPLING_444 : PYROWAVE_CHROMA_SUBSAMPLING_420;
-	// Validation order and rules of pyrowave_c.cpp:1058-1088.
-	const int num_planes = buffers->format == PYROWAVE_CPU_BUFFER_FORMAT_NV12 ? 2 : 3;
+	// Validation order and rules of pyrowave_c.cpp:1058-1088; the 16-bit planar
+	// formats (an extension) follow the rules of their 8-bit counterparts.
+	const bool wide = buffers->format == PYROWAVE_CPU_BUFFER_FORMAT_YUV420P16 ||
+	                  buffers->format == PYROWAVE_CPU_BUFFER_FORMAT_YUV444P16;
+	const pyrowave_cpu_buffer_format fmt = buffers->format == PYROWAVE_CPU_BUFFER_FORMAT_YUV420P16
+	                                           ? PYROWAVE_CPU_BUFFER_FORMAT_YUV420P
+	                                       : buffers->format == PYROWAVE_CPU_BUFFER_FORMAT_YUV444P16
+	                                           ? PYROWAVE_CPU_BUFFER_FORMAT_YUV444P
+	                                           : buffers->format;
+	const int num_planes = fmt == PYROWAVE_CPU_BUFFER_FORMAT_NV12 ? 2 : 3;
 	if (buffers->width != g.width || buffers->height != g.height)
 		return PYROWAVE_ERROR_INVALID_ARGUMENT;
-	if (chroma == PYROWAVE_CHROMA_SUBSAMPLING_420 && buffers->format == PYROWAVE_CPU_BUFFER_FORMAT_YUV444P)
+	if (chroma == PYROWAVE_CHROMA_SUBSAMPLING_420 && fmt == PYROWAVE_CPU_BUFFER_FORMAT_YUV444P)
 		return PYROWAVE_ERROR_INVALID_ARGUMENT;
-	if (chroma == PYROWAVE_CHROMA_SUBSAMPLING_444 && buffers->format != PYROWAVE_CPU_BUFFER_FORMAT_YUV444P)
+	if (chroma == PYROWAVE_CHROMA_SUBSAMPLING_444 && fmt != PYROWAVE_CPU_BUFFER_FORMAT_YUV444P)
 		return PYROWAVE_ERROR_INVALID_ARGUMENT;
-	if (buffers->format != PYROWAVE_CPU_BUFFER_FORMAT_NV12 && buffers->format != PYROWAVE_CPU_BUFFER_FORMAT_YUV420P &&
-	    buffers->format != PYROWAVE_CPU_BUFFER_FORMAT_YUV444P)
+	if (fmt != PYROWAVE_CPU_BUFFER_FORMAT_NV12 && fmt != PYROWAVE_CPU_BUFFER_FORMAT_YUV420P &&
+	    fmt != PYROWAVE_CPU_BUFFER_FORMAT_YUV444P)
 		return PYROWAVE_ERROR_INVALID_ARGUMENT;
 	for (int p = 0; p < num_planes; p++)
 	{
 		int w, h;
 		plane_dims(chroma, g.width, g.height, p, w, h);
-		const size_t bpp = (num_planes == 2 && p == 1) ? 2 : 1;
+		const size_t bpp = ((num_planes == 2 && p == 1) || wide) ? 2 : 1;
+		if (wide && ((buffers->row_stride_in_bytes[p] & 1u) || (reinterpret_cast<uintptr_t>(buffers->data[p]) & 1u)))
+			return PYROWAVE_ERROR_INVALID_ARGUMENT;
 		if (buffers->row_stride_in_bytes[p] < size_t(w) * bpp)
 			return PYROWAVE_ERROR_INVALID_ARGUMENT;
 		// stride * h > plane size, written so that an absurd stride cannot wrap around
@@ -1857,24 +1867,27 @@ pyrowave_result pyrowave_encoder_encode_cpu_synchronous(pyrowave_encoder encoder
 	}
 	else
 	{
+		const size_t bps = wide ? 2 : 1; // bytes per sample
+		in.sample16 = wide ? 1 : 0;
 		for (int p = 0; p < 3; p++)
 		{
 			int w, h;
 			plane_dims(chroma, g.width, g.height, p, w, h);
 			const size_t stride = buffers->row_stride_in_bytes[p];
+			const size_t row = size_t(w) * bps;
 			in.data[p] = encoder->in_planes[p];
-			in.xstride[p] = 1;
+			in.xstride[p] = int32_t(bps);
 			if (stride <= size_t(encoder->in_pitch[p]))
 			{
 				// One linear copy (row padding included) at the source's own pitch:
 				// a pitched copy of narrow rows runs far below the link's bandwidth.
-				cudaMemcpyAsync(encoder->in_planes[p], buffers->data[p], stride * size_t(h - 1) + size_t(w),
+				cudaMemcpyAsync(encoder->in_planes[p], buffers->data[p], stride * size_t(h - 1) + row,
 				                cudaMemcpyHostToDevice, s);
 				in.pitch[p] = int32_t(stride);
 			}
 			else
 			{
-				cudaMemcpy2DAsync(encoder->in_planes[p], encoder->in_pitch[p], buffers->data[p], stride, size_t(w),
+				cudaMemcpy2DAsync(encoder->in_planes[p], encoder->in_pitch[p], buffers->data[p], stride, row,
 				                  size_t(h), cudaMemcpyHostToDevice, s);
 				in.pitch[p] = encoder->in_pitch[p];
 			}
@@ -2037,22 +2050,33 @@ pyrowave_result pyrowave_decoder_decode_cpu_buffer_synchronous(pyrowave_decoder 
 	const Geometry &g = decoder->g;
 	const pyrowave_chroma_subsampling chroma =
 	    g.chroma444 ? PYROWAVE_CHROMA_SUBSAMPLING_444 : PYROWAVE_CHROMA_SUBSAMPLING_420;
-	// Validation of pyrowave_c.cpp:1345-1373.
+	// Validation of pyrowave_c.cpp:1345-1373; the 16-bit planar formats (an
+	// extension) follow the rules of their 8-bit counterparts.
+	const bool wide = buffers->format == PYROWAVE_CPU_BUFFER_FORMAT_YUV420P16 ||
+	                  buffers->format == PYROWAVE_CPU_BUFFER_FORMAT_YUV444P16;
+	const pyrowave_cpu_buffer_format fmt = buffers->format == PYROWAVE_CPU_BUFFER_FORMAT_YUV420P16
+	                                           ? PYROWAVE_CPU_BUFFER_FORMAT_YUV420P
+	                                       : buffers->format == PYROWAVE_CPU_BUFFER_FORMAT_YUV444P16
+	                                           ? PYROWAVE_CPU_BUFFER_FORMAT_YUV444P
+	                                           : buffers->format;
+	const size_t bps = wide ? 2 : 1;
 	if (buffers->width != g.width || buffers->height != g.height)
 		return PYROWAVE_ERROR_INVALID_ARGUMENT;
-	if (buffers->format == PYROWAVE_CPU_BUFFER_FORMAT_NV12)
+	if (fmt == PYROWAVE_CPU_BUFFER_FORMAT_NV12)
 		return PYROWAVE_ERROR_INVALID_ARGUMENT;
-	if (chroma == PYROWAVE_CHROMA_SUBSAMPLING_420 && buffers->format == PYROWAVE_CPU_BUFFER_FORMAT_YUV444P)
+	if (chroma == PYROWAVE_CHROMA_SUBSAMPLING_420 && fmt == PYROWAVE_CPU_BUFFER_FORMAT_YUV444P)
 		return PYROWAVE_ERROR_INVALID_ARGUMENT;
-	if (chroma == PYROWAVE_CHROMA_SUBSAMPLING_444 && buffers->format != PYROWAVE_CPU_BUFFER_FORMAT_YUV444P)
+	if (chroma == PYROWAVE_CHROMA_SUBSAMPLING_444 && fmt != PYROWAVE_CPU_BUFFER_FORMAT_YUV444P)
 		return PYROWAVE_ERROR_INVALID_ARGUMENT;
-	if (buffers->format != PYROWAVE_CPU_BUFFER_FORMAT_YUV420P && buffers->format != PYROWAVE_CPU_BUFFER_FORMAT_YUV444P)
+	if (fmt != PYROWAVE_CPU_BUFFER_FORMAT_YUV420P && fmt != PYROWAVE_CPU_BUFFER_FORMAT_YUV444P)
 		return PYROWAVE_ERROR_INVALID_ARGUMENT;
 	for (int p = 0; p < 3; p++)
 	{
 		int w, h;
 		plane_dims(chroma, g.width, g.height, p, w, h);
-		if (buffers->row_stride_in_bytes[p] < size_t(w))
+		if (buffers->row_stride_in_bytes[p] < size_t(w) * bps)
+			return PYROWAVE_ERROR_INVALID_ARGUMENT;
+		if (wide && ((buffers->row_stride_in_bytes[p] & 1u) || (reinterpret_cast<uintptr_t>(buffers->data[p]) & 1u)))
 			return PYROWAVE_ERROR_INVALID_ARGUMENT;
 		// stride * h > plane size, written so that an absurd stride cannot wrap around
 		if (h > 0 && buffers->row_stride_in_bytes[p] > buffers->plane_size_in_bytes[p] / size_t(h))
@@ -2068,6 +2092,7 @@ pyrowave_result pyrowave_decoder_decode_cpu_buffer_synchronous(pyrowave_decoder 
 		return r;
 	cudaStream_t s = decoder->device->stream;
 	PlaneOutput out = {};
+	out.sample16 = wide ? 1 : 0;
 	bool linear[3];
 	for (int p = 0; p < 3; p++)
 	{
@@ -2075,9 +2100,9 @@ pyrowave_result pyrowave_decoder_decode_cpu_buffer_synchronous(pyrowave_decoder 
 		plane_dims(chroma, g.width, g.height, p, w, h);
 		// Unpadded host rows: decode at that pitch and copy back in one piece
 		// (a pitched copy of narrow rows runs far below the link's bandwidth).
-		linear[p] = buffers->row_stride_in_bytes[p] == size_t(w);
+		linear[p] = buffers->row_stride_in_bytes[p] == size_t(w) * bps;
 		out.data[p] = decoder->out_planes[p];
-		out.pitch[p] = linear[p] ? int32_t(w) : decoder->out_pitch[p];
+		out.pitch[p] = linear[p] ? int32_t(size_t(w) * bps) : decoder->out_pitch[p];
 	}
 	r = decoder->decode_parsed(out, s, true);
 	if (r != PYROWAVE_SUCCESS)
@@ -2086,11 +2111,12 @@ pyrowave_result pyrowave_decoder_decode_cpu_buffer_synchronous(pyrowave_decoder 
 	{
 		int w, h;
 		plane_dims(chroma, g.width, g.height, p, w, h);
+		const size_t row = size_t(w) * bps;
 		if (linear[p])
-			cudaMemcpyAsync(buffers->data[p], decoder->out_planes[p], size_t(w) * size_t(h), cudaMemcpyDeviceToHost, s);
+			cudaMemcpyAsync(buffers->data[p], decoder->out_planes[p], row * size_t(h), cudaMemcpyDeviceToHost, s);
 		else
 			cudaMemcpy2DAsync(buffers->data[p], buffers->row_stride_in_bytes[p], decoder->out_planes[p],
-			                  decoder->out_pitch[p], size_t(w), size_t(h), cudaMemcpyDeviceToHost, s);
+			                  decoder->out_pitch[p], row, size_t(h), cudaMemcpyDeviceToHost, s);
 	}
 	cudaMemcpyAsync(decoder->h_error, decoder->error_d, sizeof(uint32_t), cudaMemcpyDeviceToHost, s);
 	if (cudaStreamSynchronize(s) != cudaSuccess)
@@ -2144,8 +2170,9 @@ pyrowave_result pyrowave_cuda_decoder_get_layout(pyrowave_decoder decoder, pyrow
 	return fill_layout(decoder->g, decoder->fp16_mask, layout);
 }
 
-pyrowave_result pyrowave_cuda_encoder_encode(pyrowave_encoder encoder, const pyrowave_cuda_planes *planes,
-                                             const pyrowave_rate_control *rate_control, pyrowave_cuda_stream stream)
+static pyrowave_result encode_device_planes(pyrowave_encoder encoder, const pyrowave_cuda_planes *planes,
+                                            const pyrowave_rate_control *rate_control, pyrowave_cuda_stream stream,
+                                            bool wide)
 {
 	if (!encoder || !planes || !rate_control)
 		return PYROWAVE_ERROR_INVALID_ARGUMENT;
@@ -2153,17 +2180,33 @@ pyrowave_result pyrowave_cuda_encoder_encode(pyrowave_encoder encoder, const pyr
 	if (r != PYROWAVE_SUCCESS)
 		return r;
 	const Geometry &g = encoder->g;
+	const size_t bps = wide ? 2 : 1;
 	PlaneInput in = {};
+	in.sample16 = wide ? 1 : 0;
 	for (int p = 0; p < 3; p++)
 	{
-		if (!planes->data[p] || planes->row_stride_in_bytes[p] < size_t(g.plane_width[p]) ||
+		if (!planes->data[p] || planes->row_stride_in_bytes[p] < size_t(g.plane_width[p]) * bps ||
 		    planes->row_stride_in_bytes[p] > 0x7fffffffu)
+			return PYROWAVE_ERROR_INVALID_ARGUMENT;
+		if (wide && ((planes->row_stride_in_bytes[p] & 1u) || (reinterpret_cast<uintptr_t>(planes->data[p]) & 1u)))
 			return PYROWAVE_ERROR_INVALID_ARGUMENT;
 		in.data[p] = static_cast<const uint8_t *>(planes->data[p]);
 		in.pitch[p] = int32_t(planes->row_stride_in_bytes[p]);
-		in.xstride[p] = 1;
+		in.xstride[p] = int32_t(bps);
 	}
 	return encoder->enqueue(in, rate_control, pick_stream(encoder->device, stream));
+}
+
+pyrowave_result pyrowave_cuda_encoder_encode(pyrowave_encoder encoder, const pyrowave_cuda_planes *planes,
+                                             const pyrowave_rate_control *rate_control, pyrowave_cuda_stream stream)
+{
+	return encode_device_planes(encoder, planes, rate_control, stream, false);
+}
+
+pyrowave_result pyrowave_cuda_encoder_encode16(pyrowave_encoder encoder, const pyrowave_cuda_planes *planes,
+                                               const pyrowave_rate_control *rate_control, pyrowave_cuda_stream stream)
+{
+	return encode_device_planes(encoder, planes, rate_control, stream, true);
 }
 
 pyrowave_result pyrowave_cuda_encoder_get_device_bitstream(pyrowave_encoder encoder, const uint32_t **stream,
@@ -2319,20 +2362,44 @@ pyrowave_result pyrowave_cuda_decoder_decode(pyrowave_decoder decoder, const pyr
 	return decoder->decode_parsed(out, pick_stream(decoder->device, stream));
 }
 
+static pyrowave_result decode_device_blocks(pyrowave_decoder decoder, const uint32_t *block_meta,
+                                            const uint32_t *words, size_t num_words,
+                                            const pyrowave_cuda_planes *planes, pyrowave_cuda_stream stream,
+                                            bool wide);
+
 pyrowave_result pyrowave_cuda_decoder_decode_blocks(pyrowave_decoder decoder, const uint32_t *block_meta,
                                                     const uint32_t *words, size_t num_words,
                                                     const pyrowave_cuda_planes *planes, pyrowave_cuda_stream stream)
+{
+	return decode_device_blocks(decoder, block_meta, words, num_words, planes, stream, false);
+}
+
+pyrowave_result pyrowave_cuda_decoder_decode_blocks16(pyrowave_decoder decoder, const uint32_t *block_meta,
+                                                      const uint32_t *words, size_t num_words,
+                                                      const pyrowave_cuda_planes *planes, pyrowave_cuda_stream stream)
+{
+	return decode_device_blocks(decoder, block_meta, words, num_words, planes, stream, true);
+}
+
+static pyrowave_result decode_device_blocks(pyrowave_decoder decoder, const uint32_t *block_meta,
+                                            const uint32_t *words, size_t num_words,
+                                            const pyrowave_cuda_planes *planes, pyrowave_cuda_stream stream,
+                                            bool wide)
 {
 	if (!decoder || !block_meta || !words || !planes || num_words > 0xffffffffu)
 		return PYROWAVE_ERROR_INVALID_ARGUMENT;
 	pyrowave_result r = decoder->allocate();
 	if (r != PYROWAVE_SUCCESS)
 		return r;
+	const size_t bps = wide ? 2 : 1;
 	PlaneOutput out = {};
+	out.sample16 = wide ? 1 : 0;
 	for (int p = 0; p < 3; p++)
 	{
-		if (!planes->data[p] || planes->row_stride_in_bytes[p] < size_t(decoder->g.plane_width[p]) ||
+		if (!planes->data[p] || planes->row_stride_in_bytes[p] < size_t(decoder->g.plane_width[p]) * bps ||
 		    planes->row_stride_in_bytes[p] > 0x7fffffffu)
+			return PYROWAVE_ERROR_INVALID_ARGUMENT;
+		if (wide && ((planes->row_stride_in_bytes[p] & 1u) || (reinterpret_cast<uintptr_t>(planes->data[p]) & 1u)))
 			return PYROWAVE_ERROR_INVALID_ARGUMENT;
 		out.data[p] = static_cast<uint8_t *>(planes->data[p]);
 		out.pitch[p] = int32_t(planes->row_stride_in_bytes[p]);

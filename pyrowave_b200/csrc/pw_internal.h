@@ -206,13 +206,15 @@ struct PlaneInput
 {
 	const uint8_t *data[3];
 	int32_t pitch[3];   // bytes between rows
-	int32_t xstride[3]; // bytes between samples (2 for the interleaved CbCr plane of NV12)
+	int32_t xstride[3]; // bytes between samples (2 for the interleaved CbCr plane of NV12 and for 16-bit planes)
+	int32_t sample16;   // 1: 16-bit little-endian samples (R16_UNORM), else 8-bit (R8_UNORM)
 };
 
 struct PlaneOutput
 {
 	uint8_t *data[3];
-	int32_t pitch[3];
+	int32_t pitch[3];   // bytes between rows
+	int32_t sample16;   // 1: write 16-bit samples (R16_UNORM), else 8-bit
 };
 
 struct DecodeInput

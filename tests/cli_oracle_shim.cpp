@@ -10,6 +10,7 @@
 #include <vector>
 
 #include "pyrowave.h"
+#include "pyrowave_cuda.h"
 #include "pyrowave_oracle.h"
 
 struct pyrowave_device_opaque
@@ -42,17 +43,19 @@ void plane_dims(bool c444, int w, int h, int p, int &pw, int &ph)
 	ph = (p == 0 || c444) ? h : h / 2;
 }
 
-bool planes_ok(const pyrowave_cpu_buffer *b, bool c444, int w, int h)
+// Planar 8-bit or 16-bit buffers only; `wide` is set for the 16-bit formats.
+bool planes_ok(const pyrowave_cpu_buffer *b, bool c444, int w, int h, bool &wide)
 {
 	if (!b || b->width != w || b->height != h)
 		return false;
-	if (b->format != (c444 ? PYROWAVE_CPU_BUFFER_FORMAT_YUV444P : PYROWAVE_CPU_BUFFER_FORMAT_YUV420P))
-		return false; // the shim takes planar input only
+	wide = b->format == (c444 ? PYROWAVE_CPU_BUFFER_FORMAT_YUV444P16 : PYROWAVE_CPU_BUFFER_FORMAT_YUV420P16);
+	if (!wide && b->format != (c444 ? PYROWAVE_CPU_BUFFER_FORMAT_YUV444P : PYROWAVE_CPU_BUFFER_FORMAT_YUV420P))
+		return false;
 	for (int p = 0; p < 3; p++)
 	{
 		int pw, ph;
 		plane_dims(c444, w, h, p, pw, ph);
-		if (!b->data[p] || b->row_stride_in_bytes[p] < size_t(pw) ||
+		if (!b->data[p] || b->row_stride_in_bytes[p] < size_t(pw) * (wide ? 2 : 1) ||
 		    b->row_stride_in_bytes[p] > b->plane_size_in_bytes[p] / size_t(ph))
 			return false;
 	}
@@ -98,20 +101,36 @@ pyrowave_result pyrowave_encoder_create(const pyrowave_encoder_create_info *info
 pyrowave_result pyrowave_encoder_encode_cpu_synchronous(pyrowave_encoder e, const pyrowave_cpu_buffer *buffers,
                                                         const pyrowave_rate_control *rc)
 {
-	if (!e || !planes_ok(buffers, e->c444, e->width, e->height) || !rc)
+	bool wide = false;
+	if (!e || !planes_ok(buffers, e->c444, e->width, e->height, wide) || !rc)
 		return PYROWAVE_ERROR_INVALID_ARGUMENT;
 	const uint64_t target = uint64_t(rc->maximum_bitstream_size) & ~uint64_t(3);
 	if (target == 0 || target > 0xffffffffull)
 		return PYROWAVE_ERROR_INVALID_ARGUMENT;
-	const uint8_t *planes[3];
-	int strides[3];
-	for (int p = 0; p < 3; p++)
-	{
-		planes[p] = static_cast<const uint8_t *>(buffers->data[p]);
-		strides[p] = int(buffers->row_stride_in_bytes[p]);
-	}
 	std::vector<float> pyramid(oracle_pyramid_size(e->codec));
-	if (oracle_dwt(e->codec, planes, strides, ORACLE_MODE_F32, pyramid.data()) != 0)
+	int strides[3];
+	int rc_dwt;
+	if (wide)
+	{
+		const uint16_t *planes[3];
+		for (int p = 0; p < 3; p++)
+		{
+			planes[p] = static_cast<const uint16_t *>(buffers->data[p]);
+			strides[p] = int(buffers->row_stride_in_bytes[p] / 2);
+		}
+		rc_dwt = oracle_dwt16(e->codec, planes, strides, ORACLE_MODE_F32, pyramid.data());
+	}
+	else
+	{
+		const uint8_t *planes[3];
+		for (int p = 0; p < 3; p++)
+		{
+			planes[p] = static_cast<const uint8_t *>(buffers->data[p]);
+			strides[p] = int(buffers->row_stride_in_bytes[p]);
+		}
+		rc_dwt = oracle_dwt(e->codec, planes, strides, ORACLE_MODE_F32, pyramid.data());
+	}
+	if (rc_dwt != 0)
 		return PYROWAVE_ERROR_GENERIC;
 	e->sequence = (e->sequence + 1) & 7u;
 	if (oracle_encode_pyramid(e->codec, pyramid.data(), rc->maximum_bitstream_size, e->sequence, -1.0f) != 0)
@@ -187,7 +206,8 @@ bool pyrowave_decoder_decode_is_ready(pyrowave_decoder d, bool allow_partial_fra
 
 pyrowave_result pyrowave_decoder_decode_cpu_buffer_synchronous(pyrowave_decoder d, const pyrowave_cpu_buffer *buffers)
 {
-	if (!d || !planes_ok(buffers, d->c444, d->width, d->height))
+	bool wide = false;
+	if (!d || !planes_ok(buffers, d->c444, d->width, d->height, wide))
 		return PYROWAVE_ERROR_INVALID_ARGUMENT;
 	std::vector<uint32_t> offsets(size_t(oracle_block_count_32x32(d->codec)));
 	const size_t nwords = oracle_parser_payload_words(d->parser);
@@ -196,14 +216,29 @@ pyrowave_result pyrowave_decoder_decode_cpu_buffer_synchronous(pyrowave_decoder 
 	std::vector<float> pyramid(oracle_pyramid_size(d->codec));
 	if (oracle_dequant(d->codec, offsets.data(), payload.data(), nwords, ORACLE_MODE_F32, pyramid.data()) != 0)
 		return PYROWAVE_ERROR_GENERIC;
-	uint8_t *planes[3];
 	int strides[3];
-	for (int p = 0; p < 3; p++)
+	int rc_idwt;
+	if (wide)
 	{
-		planes[p] = static_cast<uint8_t *>(buffers->data[p]);
-		strides[p] = int(buffers->row_stride_in_bytes[p]);
+		uint16_t *planes[3];
+		for (int p = 0; p < 3; p++)
+		{
+			planes[p] = static_cast<uint16_t *>(buffers->data[p]);
+			strides[p] = int(buffers->row_stride_in_bytes[p] / 2);
+		}
+		rc_idwt = oracle_idwt16(d->codec, pyramid.data(), ORACLE_MODE_F32, planes, strides);
 	}
-	if (oracle_idwt(d->codec, pyramid.data(), ORACLE_MODE_F32, planes, strides) != 0)
+	else
+	{
+		uint8_t *planes[3];
+		for (int p = 0; p < 3; p++)
+		{
+			planes[p] = static_cast<uint8_t *>(buffers->data[p]);
+			strides[p] = int(buffers->row_stride_in_bytes[p]);
+		}
+		rc_idwt = oracle_idwt(d->codec, pyramid.data(), ORACLE_MODE_F32, planes, strides);
+	}
+	if (rc_idwt != 0)
 		return PYROWAVE_ERROR_GENERIC;
 	oracle_parser_mark_decoded(d->parser);
 	return PYROWAVE_SUCCESS;

@@ -28,13 +28,15 @@ def _plane_shapes(w, h, c444):
 
 
 def write_y4m(path, frames, w, h, c444, tags="F30:1 Ip A1:1", chroma_tag=None):
+    """8-bit planes, or uint16 planes written as little-endian 16-bit samples (tag C420p10 etc.)."""
     ctag = chroma_tag if chroma_tag is not None else ("C444" if c444 else "C420jpeg")
     with open(path, "wb") as f:
         f.write(f"YUV4MPEG2 W{w} H{h} {tags} {ctag}\n".encode())
         for planes in frames:
             f.write(b"FRAME\n")
             for p in planes:
-                f.write(np.ascontiguousarray(p, np.uint8).tobytes())
+                dt = "<u2" if np.asarray(p).dtype == np.uint16 else np.uint8
+                f.write(np.ascontiguousarray(p, dt).tobytes())
 
 
 def read_y4m(path, c444):
@@ -43,6 +45,7 @@ def read_y4m(path, c444):
     header = data[:nl].decode()
     tags = {t[0]: t[1:] for t in header.split()[1:]}
     w, h = int(tags["W"]), int(tags["H"])
+    wide = tags["C"].endswith("p16")
     shapes = _plane_shapes(w, h, c444)
     pos, frames = nl + 1, []
     while pos < len(data):
@@ -50,11 +53,18 @@ def read_y4m(path, c444):
         pos += 6
         planes = []
         for s in shapes:
-            n = s[0] * s[1]
-            planes.append(np.frombuffer(data[pos:pos + n], np.uint8).reshape(s))
+            n = s[0] * s[1] * (2 if wide else 1)
+            planes.append(np.frombuffer(data[pos:pos + n], "<u2" if wide else np.uint8).reshape(s).astype(
+                np.uint16 if wide else np.uint8))
             pos += n
         frames.append(planes)
     return header, frames
+
+
+def up_convert16(plane, depth):
+    """yuv4mpeg.cpp:191-213: min(1, v / (2^depth - 1)) * 65535 + 0.5, in float."""
+    f = plane.astype(np.float32) / np.float32((1 << depth) - 1)
+    return (np.minimum(np.float32(1.0), f) * np.float32(65535.0) + np.float32(0.5)).astype(np.uint16)
 
 
 def read_container(path):
@@ -78,7 +88,8 @@ def write_container(path, params, packets):
 
 
 def oracle_expect(frames, w, h, c444, budget):
-    """Packetized frames (one packet each) and their decodes, from the oracle."""
+    """Packetized frames (one packet each) and their decodes, from the oracle
+    (16-bit decodes for uint16 frames)."""
     enc = O.Oracle(w, h, c444)
     dec = O.Oracle(w, h, c444)
     parser = dec.parser()
@@ -92,7 +103,8 @@ def oracle_expect(frames, w, h, c444, budget):
         packets.append(packet)
         assert parser.push(packet) and parser.ready()
         offs, payload = parser.get()
-        decoded.append(dec.idwt(dec.dequant(offs, payload)))
+        pyr = dec.dequant(offs, payload)
+        decoded.append(dec.idwt16(pyr) if planes[0].dtype == np.uint16 else dec.idwt(pyr))
         parser.mark_decoded()
     return packets, decoded
 
@@ -155,6 +167,50 @@ def test_round_trip_444_odd_size(shim_tools, tmp_path):
     assert header == "YUV4MPEG2 W70 H50 F30:1 Ip A1:1 XCOLORRANGE=LIMITED C444"
 
 
+def _frames16(w, h, c444, n, seed, depth):
+    """n frames of depth-bit samples (the synthetic 8-bit frame widened, seeded low bits)."""
+    rng = np.random.default_rng(seed)
+    out = []
+    for i in range(n):
+        planes = synth.synth_frame(w, h, c444, seed + i)
+        out.append([((p.astype(np.uint16) << (depth - 8)) |
+                     rng.integers(0, 1 << (depth - 8), p.shape, dtype=np.uint16)) for p in planes])
+    return out
+
+
+def _round_trip16(tools, tmp_path, w, h, c444, nframes, budget, seed, depth):
+    """A depth-bit stream: read and up-converted to 16 bits (the oracle codes
+    the up-converted planes), written back as a 16-bit stream."""
+    frames = _frames16(w, h, c444, nframes, seed, depth)
+    tag = ("C444p" if c444 else "C420p") + str(depth)
+    y4m, wave, out = tmp_path / "in16.y4m", tmp_path / "out16.pyrowave", tmp_path / "out16.y4m"
+    write_y4m(y4m, frames, w, h, c444, chroma_tag=tag)
+    r = _run(tools["pyrowave-encode"], y4m, wave, budget)
+    assert r.returncode == 0, r.stderr
+    params, packets = read_container(wave)
+    up = [[up_convert16(p, depth) for p in f] for f in frames]
+    exp_packets, exp_decoded = oracle_expect(up, w, h, c444, budget)
+    assert packets == exp_packets
+    r = _run(tools["pyrowave-decode"], wave, out)
+    assert r.returncode == 0, r.stderr
+    header, decoded = read_y4m(out, c444)
+    assert header.endswith("C444p16" if c444 else "C420p16")
+    for i in range(nframes):
+        for p in range(3):
+            assert decoded[i][p].dtype == np.uint16
+            assert np.array_equal(decoded[i][p], exp_decoded[i][p]), f"frame {i} plane {p}"
+    return params
+
+
+def test_round_trip_16_bit(shim_tools, tmp_path):
+    # 10-bit 4:2:0: the container records the 16-bit 4:2:0 format (2) the planes were coded from.
+    params = _round_trip16(shim_tools, tmp_path, 96, 64, False, 2, 8000, 90, 10)
+    assert params[:4] == (96, 64, 2, 0)
+    # 16-bit 4:4:4 at an odd size.
+    params = _round_trip16(shim_tools, tmp_path, 70, 50, True, 2, 12000, 95, 16)
+    assert params[:4] == (70, 50, 3, 1)
+
+
 def test_eight_frames_wrap_the_sequence_number(shim_tools, tmp_path):
     # The 3-bit sequence number wraps after 8 frames; each frame still decodes.
     _round_trip(shim_tools, tmp_path, 64, 64, False, 10, 3000, 40)
@@ -197,7 +253,6 @@ def test_usage_and_input_errors(shim_tools, tmp_path):
     frame = synth.synth_frame(64, 64, False, 1)
     cases = {
         "C422": ("unsupported chroma format", dict(chroma_tag="C422")),
-        "C420p10": ("16-bit", dict(chroma_tag="C420p10")),
     }
     for name, (msg, kw) in cases.items():
         y = tmp_path / f"{name}.y4m"
@@ -235,7 +290,7 @@ def test_container_errors(shim_tools, tmp_path):
     r = _run(dec, bad, tmp_path / "o.y4m")
     assert r.returncode == 1 and "bad magic" in r.stderr
     for params, msg in (((64, 64, 0, 1, 0, 60, 1, 0), "disagree"), ((0, 64, 0, 0, 0, 60, 1, 0), "frame size"),
-                        ((64, 64, 2, 0, 0, 60, 1, 0), "16-bit"), ((64, 64, 7, 0, 0, 60, 1, 0), "format")):
+                        ((64, 64, 2, 1, 0, 60, 1, 0), "disagree"), ((64, 64, 7, 0, 0, 60, 1, 0), "format")):
         write_container(bad, params, [])
         r = _run(dec, bad, tmp_path / "o.y4m")
         assert r.returncode == 1 and msg in r.stderr, (params, r.stderr)
@@ -264,3 +319,5 @@ def test_shipped_tools_round_trip_on_gpu(gpu, tmp_path):
         assert os.access(exe, os.X_OK), f"{exe} is not built (python -m pyrowave_b200.build)"
     _round_trip(tools, tmp_path, 256, 144, False, 3, 16000, 70)
     _round_trip(tools, tmp_path, 200, 128, True, 2, 30000, 80)
+    _round_trip16(tools, tmp_path, 256, 144, False, 2, 20000, 85, 10)
+    _round_trip16(tools, tmp_path, 200, 128, True, 2, 40000, 88, 16)

@@ -354,3 +354,65 @@ def test_transform_only_matches_oracle(device, w, h, c444):
     ref = O.Oracle(w, h, c444).dwt(planes, O.MODE_F32)
     err = _mismatch("transform-only pyramid", pyr.cpu().numpy().view(np.uint32), ref.view(np.uint32))
     assert err is None, err
+
+
+def _frame16(w, h, c444, seed):
+    """A 16-bit frame: the 8-bit synthetic frame widened, with seeded low bits."""
+    rng = np.random.default_rng(seed)
+    return [(p.astype(np.uint16) << 8) | rng.integers(0, 256, p.shape, dtype=np.uint16)
+            for p in synth.synth_frame(w, h, c444, seed)]
+
+
+@pytest.mark.parametrize("w,h,c444,budget", [(640, 360, False, 60000), (333, 197, True, 40000),
+                                              (1920, 1080, False, 400000)])
+def test_sixteen_bit_planes_bit_exact(device, w, h, c444, budget):
+    """16-bit (R16_UNORM) input and output, the reference's high bit depth path
+    (encode.cpp:152, decode.cpp:215): host-buffer and device-plane encodes give
+    the oracle's stream, and both decodes give the oracle's 16-bit planes."""
+    import torch
+
+    chroma = capi.CHROMA_444 if c444 else capi.CHROMA_420
+    planes = _frame16(w, h, c444, 12)
+    o = O.Oracle(w, h, c444)
+    pyr = o.dwt(planes, O.MODE_F32)
+    o.encode_pyramid(pyr, budget, sequence=1)
+    ostream, opackets = o.packetize(1 << 30, budget)
+    total = int(sum(int(sz) for _, sz in opackets))
+    want = o.idwt16(o.dequant(*_parse_all(o, ostream[:total])), O.MODE_F32)
+
+    enc = capi.Encoder(device, w, h, chroma)
+    assert enc.encode_cpu(planes, budget) == capi.PYROWAVE_SUCCESS
+    stream, packets = enc.packetize(1 << 30, budget)
+    assert sum(p[1] for p in packets) == total
+    assert np.array_equal(stream[:total], ostream[:total]), "16-bit host encode differs from the oracle"
+
+    dec = capi.Decoder(device, w, h, chroma)
+    assert dec.push_packet(stream[:total]) == capi.PYROWAVE_SUCCESS
+    code, out = dec.decode_cpu(wide=True)
+    assert code == capi.PYROWAVE_SUCCESS
+    for i in range(3):
+        assert out[i].dtype == np.uint16
+        err = _mismatch(f"16-bit decoded plane {i}", out[i], want[i])
+        assert err is None, err
+
+    # Device planes: encode16 (second frame of the encoder, sequence 2) and decode_blocks16.
+    d = [torch.from_numpy(p.view(np.int16)).cuda() for p in planes]
+    enc.encode_device16([p.data_ptr() for p in d], [p.stride(0) * 2 for p in d], budget)
+    torch.cuda.synchronize()
+    s, m, _ = enc.device_bitstream()
+    n = enc.size()
+    assert n == total
+    outs = [torch.zeros(p.shape, dtype=torch.int16, device="cuda") for p in planes]
+    dec2 = capi.Decoder(device, w, h, chroma)
+    dec2.decode_blocks16(m, s + 8, n // 4 - 2, [t.data_ptr() for t in outs], [t.stride(0) * 2 for t in outs])
+    assert dec2.error() == (capi.PYROWAVE_SUCCESS, 0)
+    torch.cuda.synchronize()
+    for i in range(3):
+        err = _mismatch(f"16-bit device plane {i}", outs[i].cpu().numpy().view(np.uint16), want[i])
+        assert err is None, err
+
+
+def _parse_all(o, data):
+    p = o.parser()
+    assert p.push(data.tobytes())
+    return p.get()
