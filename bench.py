@@ -596,6 +596,14 @@ def run_batched(iters: int, frames_n: int = 64, seed: int = 7):
 
     batch_ms = timed(batched)
     sizes = batch.sizes()
+    chosen = batch.shape()
+    # Both execution modes at their best shape among a few, for the record.
+    modes = {}
+    for name, kw in (("persistent", dict(persistent=True, small_level=chosen["small_level"], ctas_per_sm=0)),
+                     ("per_stage", dict(persistent=False, small_level=chosen["small_level"], large_below=256))):
+        batch.set_shape(**kw, stream=stream.cuda_stream)
+        modes[name] = round(frames_n / (timed(batched) * 1e-3), 1)
+    batch.set_shape(**{k: v for k, v in chosen.items()}, stream=stream.cuda_stream)
 
     encs, decs = [], []
     for w, h, c, _ in slots:
@@ -619,6 +627,8 @@ def run_batched(iters: int, frames_n: int = 64, seed: int = 7):
         "plain_frames_per_s": round(frames_n / (plain_ms * 1e-3), 1),
         "speedup_vs_plain": round(plain_ms / batch_ms, 2),
         "bytes_within_budget": all(s <= b for s, b in zip(sizes, budgets)),
+        "autotuned_shape": chosen,
+        "frames_per_s_by_mode": modes,
     }
     for o in encs + decs:
         o.close()

@@ -328,11 +328,37 @@ PYROWAVE_PUBLIC_API pyrowave_result pyrowave_cuda_batch_get_device_bitstream(pyr
 /* Bytes of every frame's last bitstream (waits for the last call). */
 PYROWAVE_PUBLIC_API pyrowave_result pyrowave_cuda_batch_get_sizes(pyrowave_cuda_batch batch, size_t *bytes);
 
-/* Choose the batch's CTA shapes by timing the candidates on these inputs (the
- * batch's autotuner) and keep the fastest: which coarse levels are transformed
- * first and quantised together afterwards, and below how many tiles a level
- * runs 1024-thread CTAs. The bitstreams do not depend on the choice, and the
- * tuning calls do not advance the frames' sequence numbers. Waits. */
+/* How a batch runs its calls. persistent = 1 (the default): one persistent
+ * kernel per call runs every stage of every frame, taking (frame, stage, item)
+ * work items in order from a counter, each item waiting (bounded) for its
+ * frame's previous stage; ctas_per_sm resident CTAs per SM (0: as many as fit)
+ * and large_first = 1 orders each stage's frames largest first. persistent = 0:
+ * one launch per stage over all frames, levels with fewer than large_below
+ * tiles on 1024-thread CTAs. Both: forward levels >= small_level only
+ * transform, and their blocks are quantised afterwards. The bitstreams do not
+ * depend on the shape. */
+typedef struct pyrowave_cuda_batch_shape
+{
+	uint32_t persistent;
+	int32_t small_level;
+	int32_t large_below;
+	int32_t ctas_per_sm;
+	uint32_t large_first;
+} pyrowave_cuda_batch_shape;
+
+PYROWAVE_PUBLIC_API pyrowave_result pyrowave_cuda_batch_get_shape(pyrowave_cuda_batch batch,
+                                                                  pyrowave_cuda_batch_shape *shape);
+/* Waits for the batch's last call, then switches to `shape`. */
+PYROWAVE_PUBLIC_API pyrowave_result pyrowave_cuda_batch_set_shape(pyrowave_cuda_batch batch,
+                                                                  const pyrowave_cuda_batch_shape *shape,
+                                                                  pyrowave_cuda_stream stream);
+
+/* Choose the batch's shape by timing the candidates on these inputs (the
+ * batch's autotuner) and keep the fastest: persistent launches with 2 to 4
+ * resident CTAs per SM and both frame orders, and per-stage launches with
+ * three thresholds for 1024-thread CTAs, each with the transform-only suffix
+ * starting at levels 5 down to 2. The bitstreams do not depend on the choice,
+ * and the tuning calls do not advance the frames' sequence numbers. Waits. */
 PYROWAVE_PUBLIC_API pyrowave_result pyrowave_cuda_batch_autotune(pyrowave_cuda_batch batch,
                                                                  const pyrowave_cuda_planes *inputs,
                                                                  const size_t *budgets,

@@ -68,6 +68,7 @@ API_SYMBOLS = [
     "pyrowave_cuda_encoder_encode16", "pyrowave_cuda_decoder_decode_blocks16",
     "pyrowave_cuda_batch_create", "pyrowave_cuda_batch_destroy", "pyrowave_cuda_batch_encode",
     "pyrowave_cuda_batch_get_device_bitstream", "pyrowave_cuda_batch_get_sizes", "pyrowave_cuda_batch_autotune",
+    "pyrowave_cuda_batch_get_shape", "pyrowave_cuda_batch_set_shape",
     "pyrowave_cuda_server_create", "pyrowave_cuda_server_destroy", "pyrowave_cuda_server_open_stream",
     "pyrowave_cuda_server_close_stream", "pyrowave_cuda_server_submit", "pyrowave_cuda_server_poll",
     "pyrowave_cuda_server_stats", "pyrowave_cuda_server_get_memory",
@@ -228,6 +229,8 @@ def lib():
     L.pyrowave_cuda_batch_get_sizes.argtypes = [c_void_p, POINTER(c_size_t)]
     L.pyrowave_cuda_batch_autotune.argtypes = [c_void_p, POINTER(CudaPlanes), POINTER(c_size_t), POINTER(CudaPlanes),
                                                c_void_p]
+    L.pyrowave_cuda_batch_get_shape.argtypes = [c_void_p, c_void_p]
+    L.pyrowave_cuda_batch_set_shape.argtypes = [c_void_p, c_void_p, c_void_p]
     L.pyrowave_cuda_server_create.argtypes = [c_void_p, POINTER(ServerInfo), POINTER(c_void_p)]
     L.pyrowave_cuda_server_destroy.argtypes = [c_void_p]
     L.pyrowave_cuda_server_destroy.restype = None
@@ -646,6 +649,21 @@ class Batch:
         out = (c_size_t * self.count)()
         check(self.L.pyrowave_cuda_batch_get_sizes(self.h, out), "batch_get_sizes")
         return list(out)
+
+    def shape(self) -> dict:
+        sh = BatchShape()
+        check(self.L.pyrowave_cuda_batch_get_shape(self.h, ctypes.byref(sh)), "batch_get_shape")
+        return {k: int(getattr(sh, k)) for k, _ in BatchShape._fields_}
+
+    def set_shape(self, persistent=True, small_level=5, large_below=0, ctas_per_sm=0, large_first=False,
+                  stream: int = 0):
+        sh = BatchShape(int(persistent), small_level, large_below, ctas_per_sm, int(large_first))
+        check(self.L.pyrowave_cuda_batch_set_shape(self.h, ctypes.byref(sh), c_void_p(stream)), "batch_set_shape")
+
+
+class BatchShape(Structure):
+    _fields_ = [("persistent", c_uint32), ("small_level", c_int32), ("large_below", c_int32),
+                ("ctas_per_sm", c_int32), ("large_first", c_uint32)]
 
 
 class Server:

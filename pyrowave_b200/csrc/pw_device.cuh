@@ -238,6 +238,11 @@ __device__ __forceinline__ void store_subblock(float *c32, __half *c16, bool fp1
 	}
 }
 
+// Barrier of one 128-thread group of a CTA (hardware barrier `id`, 1 or 2):
+// the block-level bodies (packing, dequantisation) run one 32x32 block per
+// group, so a CTA of 256 threads can hold two independent blocks.
+__device__ __forceinline__ void group_sync(int id) { asm volatile("bar.sync %0, 128;" ::"r"(id) : "memory"); }
+
 // Cooperative copy of a parameter struct from global to shared memory (the
 // caller synchronises before use).
 template <typename T> __device__ __forceinline__ void load_params(T &dst, const T &src)

@@ -9,7 +9,7 @@
 //                      shaders/resolve_rate_control.comp:38-81, pyrowave_encoder.cpp:283-338
 //   block packing      shaders/block_packing.comp:97-379
 //   packetize layout   pyrowave_encoder.cpp:1048-1115
-#include "pw_device.cuh"
+#include "pw_decode_body.cuh"
 
 namespace pw
 {
@@ -21,7 +21,6 @@ constexpr int kTileIn = 72;  // 64 input samples + 4-sample apron on each side
 // interior tile of a level above 0 is one TMA box (72 rows of 76 samples).
 constexpr int kInPitch = 76;
 constexpr uint32_t kInBoxBytes = kTileIn * kInPitch * 4;
-constexpr uint32_t kTmaMaxPolls = 1u << 20; // bounded wait for a tile load
 constexpr int kHPitch = 65;
 constexpr int kBandPitch = 33;
 
@@ -1357,20 +1356,32 @@ __global__ void __launch_bounds__(kResolveBatchThreads) resolve_batch_kernel(con
 // ---------------------------------------------------------------------------
 // Block packing: one 32x32 block per 128-thread CTA, assembled in shared
 // memory and written as whole words at its prefix-scanned offset.
-__device__ __forceinline__ void pack_body(const BlockParams &p, const EncodeBuffers &buf, const int blk)
+struct PackShared
 {
-	__shared__ uint32_t pkt[kMaxBlockWords];
-	__shared__ uint32_t s_ballot[4];
-	__shared__ uint32_t s_bytes[16];
-	__shared__ uint32_t s_sig[4];
-	__shared__ float s_inv_scale[16];
+	uint32_t pkt[kMaxBlockWords];
+	uint32_t s_ballot[4];
+	uint32_t s_bytes[16];
+	uint32_t s_sig[4];
+	float s_inv_scale[16];
+};
+
+// One 32x32 block on a group of 128 threads (threadIdx.x & 127), synchronised
+// with hardware barrier `bar`.
+__device__ __forceinline__ void pack_body(PackShared &sh, const BlockParams &p, const EncodeBuffers &buf, const int blk,
+                                          const int bar)
+{
+	uint32_t *const pkt = sh.pkt;
+	uint32_t *const s_ballot = sh.s_ballot;
+	uint32_t *const s_bytes = sh.s_bytes;
+	uint32_t *const s_sig = sh.s_sig;
+	float *const s_inv_scale = sh.s_inv_scale;
 	pdl_trigger();
 	const int k = find_band(p, blk);
 	const BandEntry &B = p.band[k];
 	const LevelDesc &L = p.level[B.level];
 	const int rel = blk - B.block32_offset;
 	const int by32 = rel / B.block32_stride, bx32 = rel - by32 * B.block32_stride;
-	const int t = threadIdx.x, lane = t & 31;
+	const int t = threadIdx.x & 127, lane = t & 31;
 	const int sub = t & 7, lx = (t >> 3) & 3, ly = t >> 5;
 	const int grp = ly * 4 + lx;
 	const int x8 = bx32 * 4 + lx, y8 = by32 * 4 + ly;
@@ -1396,7 +1407,7 @@ __device__ __forceinline__ void pack_body(const BlockParams &p, const EncodeBuff
 	const uint32_t offset = meta.x;
 	const uint32_t cw = quantize_code_word(cw0, quant);
 	const bool active = (cw & 0xffffu) != 0;
-	__syncthreads(); // s_inv_scale
+	group_sync(bar); // s_inv_scale
 
 	// Re-quantise this sub-block exactly as the quantiser did.
 	const float qs = s_inv_scale[(cw0 >> kQuantScaleOffset) & 0xfu];
@@ -1453,7 +1464,7 @@ __device__ __forceinline__ void pack_body(const BlockParams &p, const EncodeBuff
 	const uint32_t sub_plane_offset = pinc - planes;
 	for (int w = t; w < int(words) && w < kMaxBlockWords; w += 128)
 		pkt[w] = 0u;
-	__syncthreads();
+	group_sync(bar);
 
 	const uint32_t ballot = s_ballot[0] | (s_ballot[1] << 4) | (s_ballot[2] << 8) | (s_ballot[3] << 12);
 	const uint32_t n = uint32_t(__popc(ballot));
@@ -1509,7 +1520,7 @@ __device__ __forceinline__ void pack_body(const BlockParams &p, const EncodeBuff
 				bytes[plane_base + pl] = uint8_t(by);
 		}
 	}
-	__syncthreads();
+	group_sync(bar);
 
 	// Sign bits of significant coefficients, in coefficient order, after the planes.
 	// This thread's sign bits are consecutive in the stream: gather them (sign
@@ -1528,15 +1539,15 @@ __device__ __forceinline__ void pack_body(const BlockParams &p, const EncodeBuff
 				k++;
 			}
 		}
-		const uint32_t w = bitpos >> 5, sh = bitpos & 31u;
+		const uint32_t w = bitpos >> 5, shift = bitpos & 31u;
 		if (bits != 0 && w < uint32_t(kMaxBlockWords))
 		{
-			atomicOr(&pkt[w], bits << sh);
-			if (sh != 0 && (bits >> (32u - sh)) != 0 && w + 1 < uint32_t(kMaxBlockWords))
-				atomicOr(&pkt[w + 1], bits >> (32u - sh));
+			atomicOr(&pkt[w], bits << shift);
+			if (shift != 0 && (bits >> (32u - shift)) != 0 && w + 1 < uint32_t(kMaxBlockWords))
+				atomicOr(&pkt[w + 1], bits >> (32u - shift));
 		}
 	}
-	__syncthreads();
+	group_sync(bar);
 
 	// The word count must match the rate-control estimate the offsets were built from.
 	const uint32_t bits = 8 * (3 * n + total_bytes) + total_sig;
@@ -1553,7 +1564,8 @@ __device__ __forceinline__ void pack_body(const BlockParams &p, const EncodeBuff
 
 __global__ void __launch_bounds__(128, 12) pack_kernel(const BlockParams p, const EncodeBuffers buf)
 {
-	pack_body(p, buf, int(blockIdx.x));
+	__shared__ PackShared sh;
+	pack_body(sh, p, buf, int(blockIdx.x), 1);
 }
 
 // Batched form: one CTA per (frame, block).
@@ -1566,10 +1578,220 @@ __global__ void __launch_bounds__(128, 12) pack_batch_kernel(const BatchFrame *f
 	load_params(s_p, frames[f].bp);
 	load_params(s_buf, frames[f].eb);
 	__syncthreads();
-	pack_body(s_p, s_buf, local);
+	__shared__ PackShared sh;
+	pack_body(sh, s_p, s_buf, local, 1);
+}
+
+// ---------------------------------------------------------------------------
+// The batched form as one persistent launch. Each CTA loops: take the next
+// work item from the ticket counter, wait (bounded) until every item of the
+// frame's gating stage has finished, copy the stage's parameters of that frame
+// into shared memory, run the stage's body on the item, and count the item as
+// finished. Items are taken in ticket order, so a CTA only ever waits for items
+// that running CTAs took before it: the waits end whether or not every CTA of
+// the grid is resident. Every stage body is the one the single-frame kernels
+// run (at 256 threads; the block-level stages run two blocks per item, one per
+// 128-thread group), so each frame's results are those of the single-frame path.
+constexpr uint32_t kBatchWaitSpins = 1u << 22;
+
+struct BatchQuantShared
+{
+	float tile[2][32][kBandPitch];
+	QuantGroupShared q[2];
+};
+
+struct BatchShared
+{
+	union
+	{
+		DwtShared dwt;
+		IdwtShared idwt;
+		PackShared pack[2];
+		DequantShared deq[2];
+		BatchQuantShared quant;
+	} u;
+	union
+	{
+		LevelParams lp;
+		BlockParams bp;
+		ResolveParams rp;
+	} prm;
+	EncodeBuffers eb;
+	DecodeInput di;
+	PlaneInput in;
+	PlaneOutput out;
+	int item;
+};
+static_assert(sizeof(BatchShared) <= 56 * 1024, "the persistent kernel's stage storage fits four CTAs per SM");
+
+// The kernel's shared memory (dynamic: its stages' storage is a union larger
+// than a static allocation may be).
+extern __shared__ __align__(128) unsigned char batch_smem[];
+__device__ __forceinline__ BatchShared &batch_shared() { return *reinterpret_cast<BatchShared *>(batch_smem); }
+
+// Each stage body is its own function (not inlined into the loop), so that
+// register allocation happens per stage, as in the single-frame kernels; each
+// reaches the shared storage through the kernel's own symbol.
+__device__ __noinline__ void batch_forward_item(int level, int small_level, int local)
+{
+	BatchShared &sh = batch_shared();
+	const int per_comp = sh.prm.lp.L.tiles_x * sh.prm.lp.L.tiles_y;
+	dwt_forward_body<kBatchPersistentThreads>(sh.u.dwt, sh.prm.lp, sh.in, sh.eb, nullptr, level < small_level ? 1 : 0,
+	                                          local % per_comp, local / per_comp);
+}
+
+__device__ __noinline__ void batch_quant_item(int small_blocks, int local)
+{
+	BatchShared &sh = batch_shared();
+	quant_blocks_body<1, 2>(sh.prm.bp, sh.eb, 0, small_blocks, local, sh.u.quant.tile, sh.u.quant.q);
+}
+
+__device__ __noinline__ void batch_resolve_item(int slice, int slices)
+{
+	BatchShared &sh = batch_shared();
+	resolve_body(sh.prm.rp, sh.eb, slice, slices);
+}
+
+__device__ __noinline__ void batch_pack_item(int blk, int half)
+{
+	BatchShared &sh = batch_shared();
+	pack_body(sh.u.pack[half], sh.prm.bp, sh.eb, blk, 1 + half);
+}
+
+__device__ __noinline__ void batch_dequant_item(int blk, int half)
+{
+	BatchShared &sh = batch_shared();
+	dequant_body(sh.u.deq[half], sh.prm.bp, sh.di, blk, blk == 0, 1 + half);
+}
+
+__device__ __noinline__ void batch_inverse_item(int local)
+{
+	BatchShared &sh = batch_shared();
+	const int per_comp = sh.prm.lp.L.tiles_x * sh.prm.lp.L.tiles_y;
+	idwt_body<kBatchPersistentThreads>(sh.u.idwt, sh.prm.lp, sh.di, sh.out, nullptr, local % per_comp,
+	                                   local / per_comp);
+}
+
+__global__ void __launch_bounds__(kBatchPersistentThreads, 4) batch_persistent_kernel(const BatchRunParams rp)
+{
+	BatchShared &sh = batch_shared();
+	for (;;)
+	{
+		if (threadIdx.x == 0)
+			sh.item = int(atomicAdd(rp.ticket, 1u));
+		__syncthreads();
+		const int item = sh.item;
+		if (item >= rp.nwork)
+			return;
+		const uint32_t w = __ldg(rp.work + item);
+		const int f = int(w >> 24), stage = int((w >> kBatchLocalBits) & 31u);
+		const int local = int(w & ((1u << kBatchLocalBits) - 1u));
+		const BatchFrame &fr = rp.frames[f];
+		if (threadIdx.x == 0)
+		{
+			const uint32_t gate = __ldg(rp.gates + f * kBatchStages + stage);
+			if (gate != kNoGate)
+			{
+				const uint32_t *count = rp.done + f * kBatchStages + (gate >> 24);
+				const uint32_t target = gate & 0xffffffu;
+				uint32_t spins = 0;
+				while (ld_acquire_u32(count) < target)
+				{
+					if (++spins > kBatchWaitSpins)
+					{
+						atomicOr(&fr.eb.rc->error, kErrorLevelWait);
+						break;
+					}
+					__nanosleep(64);
+				}
+			}
+		}
+		if (stage < kStageQuant)
+		{
+			load_params(sh.prm.lp, fr.lp[stage - kStageDwt0]);
+			load_params(sh.in, rp.io[f].in);
+			load_params(sh.eb, fr.eb);
+		}
+		else if (stage == kStageQuant || stage == kStagePack)
+		{
+			load_params(sh.prm.bp, fr.bp);
+			load_params(sh.eb, fr.eb);
+		}
+		else if (stage == kStageResolve)
+		{
+			load_params(sh.prm.rp, rp.io[f].rp);
+			load_params(sh.eb, fr.eb);
+		}
+		else if (stage == kStageDequant)
+		{
+			load_params(sh.prm.bp, fr.bp);
+			load_params(sh.di, fr.di);
+		}
+		else
+		{
+			load_params(sh.prm.lp, fr.lp[kStageIdwt4 + 4 - stage]);
+			load_params(sh.di, fr.di);
+			load_params(sh.out, rp.io[f].out);
+		}
+		__syncthreads();
+		const int half = int(threadIdx.x) >> 7;
+		if (stage < kStageQuant)
+			batch_forward_item(stage - kStageDwt0, rp.small_level, local);
+		else if (stage == kStageQuant)
+			batch_quant_item(fr.small_blocks, local);
+		else if (stage == kStageResolve)
+			batch_resolve_item(local, fr.slices);
+		else if (stage == kStagePack)
+		{
+			const int blk = local * 2 + half;
+			if (blk < fr.block_count)
+				batch_pack_item(blk, half);
+		}
+		else if (stage == kStageDequant)
+		{
+			const int blk = local * 2 + half;
+			if (blk < fr.block_count)
+				batch_dequant_item(blk, half);
+		}
+		else
+			batch_inverse_item(local);
+		__syncthreads();
+		if (threadIdx.x == 0)
+		{
+			__threadfence();
+			atomicAdd(rp.done + f * kBatchStages + stage, 1u);
+		}
+	}
 }
 
 } // namespace
+
+int batch_persistent_max_ctas_per_sm()
+{
+	static int cached = 0;
+	if (!cached)
+	{
+		cudaFuncSetAttribute(batch_persistent_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+		                     int(sizeof(BatchShared)));
+		int n = 0;
+		if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, batch_persistent_kernel, kBatchPersistentThreads,
+		                                                  sizeof(BatchShared)) != cudaSuccess ||
+		    n < 1)
+		{
+			(void)cudaGetLastError();
+			n = 1;
+		}
+		cached = n;
+	}
+	return cached;
+}
+
+// The kernel's shared-memory attribute is set by batch_persistent_max_ctas_per_sm,
+// which the batch calls before any launch (outside stream capture).
+void launch_batch_persistent(const BatchRunParams &rp, int ctas, cudaStream_t stream)
+{
+	batch_persistent_kernel<<<ctas, kBatchPersistentThreads, sizeof(BatchShared), stream>>>(rp);
+}
 
 LaunchConfig::LaunchConfig(dim3 grid, dim3 block, cudaStream_t stream, bool programmatic)
 {

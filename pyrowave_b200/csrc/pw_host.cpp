@@ -18,6 +18,7 @@
 #include "pyrowave_cuda.h"
 
 #include <algorithm>
+#include <array>
 #include <cmath>
 #include <cstdio>
 #include <cstdlib>
@@ -2508,17 +2509,23 @@ pyrowave_result pyrowave_cuda_decoder_decode_pyramid(pyrowave_decoder decoder, c
 
 // ---------------------------------------------------------------------------
 // Batched form. Every frame of the batch owns the same buffers an encoder
-// owns; the kernels of each stage run once over all frames, mapped CTA by CTA
-// through per-stage tables of batch_cta() words. A call is one CUDA graph
-// launch: upload of the per-call table, rate-control clear, the stages.
+// owns. A call is one CUDA graph launch: upload of the per-call table, the
+// clears of the rate-control states and the work counters, then one
+// persistent kernel that runs every stage of every frame from a list of
+// (frame, stage, item) work words (batch_persistent_kernel). The per-stage
+// kernels (one launch per stage over all frames, CTAs mapped to frames through
+// tables of batch_cta() words) remain as a second execution mode among the
+// autotuner's candidates.
 namespace
 {
-// CTA shape choices of one batch (the autotuner's search space).
+// Execution choices of one batch (the autotuner's search space).
 struct BatchShape
 {
-	int small_level = kLevels; // levels >= this: transform only, quantised after the last level
-	int large_below = 0;       // other levels (forward and inverse) run 1024-thread CTAs when they have fewer tiles
-	bool operator==(const BatchShape &o) const { return small_level == o.small_level && large_below == o.large_below; }
+	bool persistent = true;     // one persistent launch, or one launch per stage
+	int small_level = kLevels;  // levels >= this: transform only, quantised after the last level
+	int large_below = 0;        // per-stage mode: levels with fewer tiles run 1024-thread CTAs
+	int ctas_per_sm = 0;        // persistent mode: resident CTAs per SM (0: as many as fit)
+	bool large_first = false;   // persistent mode: within a stage, frames in decreasing size
 };
 } // namespace
 
@@ -2556,6 +2563,14 @@ struct pyrowave_cuda_batch_opaque
 
 	BatchShape shape;
 	CapturedGraph graphs[2][2]; // [slot][with decode]
+
+	// Persistent mode: work lists (encode only, encode + decode), per-frame
+	// stage gates, and the ticket / finished-item counters cleared per call.
+	uint32_t *work_d[2] = {};
+	int work_n[2] = {};
+	uint32_t *gates_d = nullptr;
+	uint32_t *sync_d = nullptr; // ticket, then count x kBatchStages finished counters
+	int sm_count = 148;
 
 	template <typename T> T *alloc(size_t n, bool &ok)
 	{
@@ -2618,6 +2633,69 @@ struct pyrowave_cuda_batch_opaque
 		block_n = int(maps_h.size()) - block_off;
 	}
 
+	// Items of each stage of frame f (persistent mode).
+	void stage_counts(int f, int (&n)[kBatchStages]) const
+	{
+		const Geometry &g = geo[f];
+		const BatchFrame &fr = frames_h[f];
+		for (int level = 0; level < kLevels; level++)
+		{
+			const int tiles = g.level[level].tiles_x * g.level[level].tiles_y * ((level == 0 && !g.chroma444) ? 1 : 3);
+			n[kStageDwt0 + level] = tiles;
+			n[kStageIdwt4 + 4 - level] = tiles;
+		}
+		n[kStageQuant] = (fr.small_blocks + 1) / 2;
+		n[kStageResolve] = fr.slices;
+		n[kStagePack] = (fr.block_count + 1) / 2;
+		n[kStageDequant] = (fr.block_count + 1) / 2;
+	}
+
+	// Work lists and gates of the persistent mode: stage by stage, every frame's
+	// items (frames in index order, or largest first); an item is gated by the
+	// nearest earlier stage of its frame that has items.
+	void build_work(std::vector<uint32_t> (&work)[2], std::vector<uint32_t> &gates) const
+	{
+		std::vector<int> order(static_cast<size_t>(count));
+		for (int f = 0; f < count; f++)
+			order[size_t(f)] = f;
+		if (shape.large_first)
+			std::stable_sort(order.begin(), order.end(), [&](int a, int b) {
+				return geo[a].storage_elems32 > geo[b].storage_elems32;
+			});
+		std::vector<std::array<int, kBatchStages>> n(static_cast<size_t>(count));
+		gates.assign(size_t(count) * kBatchStages, kNoGate);
+		for (int f = 0; f < count; f++)
+		{
+			int c[kBatchStages];
+			stage_counts(f, c);
+			int prev = -1;
+			for (int st = 0; st < kBatchStages; st++)
+			{
+				n[size_t(f)][size_t(st)] = c[st];
+				if (prev >= 0)
+					gates[size_t(f) * kBatchStages + st] = (uint32_t(prev) << 24) | uint32_t(c[prev]);
+				if (c[st] > 0)
+					prev = st;
+			}
+		}
+		for (int d = 0; d < 2; d++)
+		{
+			work[d].clear();
+			const int last = d ? kBatchStages : kStageDequant;
+			for (int st = 0; st < last; st++)
+				for (int f : order)
+					for (int i = 0; i < n[size_t(f)][size_t(st)]; i++)
+						work[d].push_back(batch_work(f, st, i));
+		}
+	}
+
+	int persistent_ctas() const
+	{
+		const int fit = batch_persistent_max_ctas_per_sm();
+		const int per_sm = shape.ctas_per_sm > 0 ? std::min(shape.ctas_per_sm, fit) : fit;
+		return std::max(1, per_sm) * sm_count;
+	}
+
 	// Per-frame blocks of the levels >= small_level (a prefix in block index order).
 	void apply_shape(const BatchShape &s)
 	{
@@ -2634,11 +2712,38 @@ struct pyrowave_cuda_batch_opaque
 				gr.destroy();
 	}
 
-	// Upload the frame table and the CTA maps (after apply_shape).
+	// Upload the frame table, the CTA maps and the work lists (after apply_shape).
 	bool upload(cudaStream_t s)
 	{
 		build_maps();
+		(void)batch_persistent_max_ctas_per_sm(); // kernel attributes, set outside any capture
 		bool ok = true;
+		std::vector<uint32_t> work[2], gates;
+		build_work(work, gates);
+		for (int d = 0; d < 2; d++)
+		{
+			if (work_d[d])
+			{
+				dev_free(work_d[d]);
+				owned.erase(std::find(owned.begin(), owned.end(), static_cast<void *>(work_d[d])));
+			}
+			work_d[d] = alloc<uint32_t>(std::max<size_t>(work[d].size(), 1), ok);
+			work_n[d] = int(work[d].size());
+		}
+		if (!gates_d)
+			gates_d = alloc<uint32_t>(gates.size(), ok);
+		if (!sync_d)
+			sync_d = alloc<uint32_t>(1 + size_t(count) * kBatchStages, ok);
+		if (!ok)
+			return false;
+		for (int d = 0; d < 2; d++)
+			if (!work[d].empty() &&
+			    !cuda_ok(cudaMemcpyAsync(work_d[d], work[d].data(), work[d].size() * 4, cudaMemcpyHostToDevice, s),
+			             "cudaMemcpyAsync"))
+				return false;
+		if (!cuda_ok(cudaMemcpyAsync(gates_d, gates.data(), gates.size() * 4, cudaMemcpyHostToDevice, s),
+		             "cudaMemcpyAsync"))
+			return false;
 		if (!frames_d)
 			frames_d = alloc<BatchFrame>(size_t(count), ok);
 		if (maps_d)
@@ -2669,6 +2774,26 @@ struct pyrowave_cuda_batch_opaque
 		bool ok = cuda_ok(cudaMemcpyAsync(io_d, io_h[slot_index], sizeof(BatchFrameIO) * size_t(count),
 		                                  cudaMemcpyHostToDevice, s), "cudaMemcpyAsync");
 		ok = ok && cuda_ok(cudaMemsetAsync(rc_d, 0, sizeof(RateControlState) * size_t(count), s), "cudaMemsetAsync");
+		if (shape.persistent)
+		{
+			ok = ok && cuda_ok(cudaMemsetAsync(sync_d, 0, (1 + size_t(count) * kBatchStages) * 4, s),
+			                   "cudaMemsetAsync");
+			BatchRunParams rp = {};
+			rp.frames = frames_d;
+			rp.io = io_d;
+			rp.work = work_d[decode ? 1 : 0];
+			rp.gates = gates_d;
+			rp.ticket = sync_d;
+			rp.done = sync_d + 1;
+			rp.nwork = work_n[decode ? 1 : 0];
+			rp.small_level = shape.small_level;
+			launch_batch_persistent(rp, persistent_ctas(), s);
+			ok = launches_ok("kernel launch") && ok;
+			ok = graph.end(s, 0) && ok;
+			if (!ok)
+				graph.destroy();
+			return ok;
+		}
 		for (int level = 0; level < kLevels; level++)
 			launch_dwt_forward_batch(frames_d, io_d, maps_d + level_off[level], level_n[level], level, &fwd_maps[level],
 			                         level < shape.small_level, large(level), level > 0, s);
@@ -2857,6 +2982,9 @@ pyrowave_result pyrowave_cuda_batch_create(pyrowave_device device, const pyrowav
 	for (int level = kLevels - 1; level >= 0 && tiles[level] < kSmallLevelTiles; level--)
 		shape.small_level = level;
 	shape.large_below = kSmallLevelTiles;
+	int sms = 0;
+	if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device->cuda_device) == cudaSuccess && sms > 0)
+		b->sm_count = sms;
 	b->apply_shape(shape);
 	if (!b->upload(device->stream))
 	{
@@ -2905,6 +3033,37 @@ pyrowave_result pyrowave_cuda_batch_get_sizes(pyrowave_cuda_batch batch, size_t 
 	return PYROWAVE_SUCCESS;
 }
 
+pyrowave_result pyrowave_cuda_batch_get_shape(pyrowave_cuda_batch batch, pyrowave_cuda_batch_shape *shape)
+{
+	if (!batch || !shape)
+		return PYROWAVE_ERROR_INVALID_ARGUMENT;
+	shape->persistent = batch->shape.persistent ? 1u : 0u;
+	shape->small_level = batch->shape.small_level;
+	shape->large_below = batch->shape.large_below;
+	shape->ctas_per_sm = batch->shape.persistent ? batch->persistent_ctas() / batch->sm_count : 0;
+	shape->large_first = batch->shape.large_first ? 1u : 0u;
+	return PYROWAVE_SUCCESS;
+}
+
+pyrowave_result pyrowave_cuda_batch_set_shape(pyrowave_cuda_batch batch, const pyrowave_cuda_batch_shape *shape,
+                                              pyrowave_cuda_stream stream)
+{
+	if (!batch || !shape || shape->small_level < 0 || shape->small_level > kLevels || shape->ctas_per_sm < 0 ||
+	    shape->large_below < 0)
+		return PYROWAVE_ERROR_INVALID_ARGUMENT;
+	BatchShape s;
+	s.persistent = shape->persistent != 0;
+	s.small_level = shape->small_level;
+	s.large_below = shape->large_below;
+	s.ctas_per_sm = shape->ctas_per_sm;
+	s.large_first = shape->large_first != 0;
+	cudaStream_t st = pick_stream(batch->device, stream);
+	if (batch->last_stream && !cuda_ok(cudaStreamSynchronize(batch->last_stream), "cudaStreamSynchronize"))
+		return PYROWAVE_ERROR_GENERIC;
+	batch->apply_shape(s);
+	return batch->upload(st) ? PYROWAVE_SUCCESS : PYROWAVE_ERROR_GENERIC;
+}
+
 pyrowave_result pyrowave_cuda_batch_autotune(pyrowave_cuda_batch batch, const pyrowave_cuda_planes *inputs,
                                              const size_t *budgets, const pyrowave_cuda_planes *outputs,
                                              pyrowave_cuda_stream stream)
@@ -2916,47 +3075,69 @@ pyrowave_result pyrowave_cuda_batch_autotune(pyrowave_cuda_batch batch, const py
 	cudaEvent_t e0 = nullptr, e1 = nullptr;
 	if (!cuda_ok(cudaEventCreate(&e0), "cudaEventCreate") || !cuda_ok(cudaEventCreate(&e1), "cudaEventCreate"))
 		return PYROWAVE_ERROR_GENERIC;
-	// Candidates: where the transform-only suffix of levels starts, and below how
-	// many tiles a level runs 1024-thread CTAs. Each is timed over a few calls.
-	static const int kLargeBelow[] = {0, 148, 256, 512, 1024, 4096};
+	// Candidates. Persistent launch: where the transform-only suffix of levels
+	// starts (its blocks quantised in a stage of their own), resident CTAs per
+	// SM, and the order of frames within a stage. Per-stage launches: the same
+	// suffix, and below how many tiles a level runs 1024-thread CTAs. Each is
+	// timed over a few calls; the fastest is kept.
+	std::vector<BatchShape> cands;
+	for (int small = kLevels; small >= 2; small--)
+	{
+		for (int per_sm = 2; per_sm <= std::max(2, batch_persistent_max_ctas_per_sm()); per_sm++)
+			for (int large_first = 0; large_first < 2; large_first++)
+			{
+				BatchShape c;
+				c.persistent = true;
+				c.small_level = small;
+				c.ctas_per_sm = per_sm;
+				c.large_first = large_first != 0;
+				cands.push_back(c);
+			}
+		for (int lb : {0, 256, 1024})
+		{
+			BatchShape c;
+			c.persistent = false;
+			c.small_level = small;
+			c.large_below = lb;
+			cands.push_back(c);
+		}
+	}
 	BatchShape best = batch->shape;
 	float best_ms = 0.0f;
 	bool have_best = false;
 	pyrowave_result r = PYROWAVE_SUCCESS;
-	for (int small = kLevels; small >= 1 && r == PYROWAVE_SUCCESS; small--)
-		for (int lb : kLargeBelow)
+	for (const BatchShape &cand : cands)
+	{
+		if (r != PYROWAVE_SUCCESS)
+			break;
+		batch->apply_shape(cand);
+		if (!batch->upload(s))
 		{
-			BatchShape cand;
-			cand.small_level = small;
-			cand.large_below = lb;
-			batch->apply_shape(cand);
-			if (!batch->upload(s))
-			{
-				r = PYROWAVE_ERROR_GENERIC;
-				break;
-			}
-			for (int w = 0; w < 2 && r == PYROWAVE_SUCCESS; w++)
-				r = batch->run(inputs, budgets, outputs, s);
-			if (r != PYROWAVE_SUCCESS)
-				break;
-			cudaEventRecord(e0, s);
-			for (int it = 0; it < 4 && r == PYROWAVE_SUCCESS; it++)
-				r = batch->run(inputs, budgets, outputs, s);
-			cudaEventRecord(e1, s);
-			float ms = 0.0f;
-			if (r != PYROWAVE_SUCCESS || !cuda_ok(cudaEventSynchronize(e1), "cudaEventSynchronize") ||
-			    !cuda_ok(cudaEventElapsedTime(&ms, e0, e1), "cudaEventElapsedTime"))
-			{
-				r = r != PYROWAVE_SUCCESS ? r : PYROWAVE_ERROR_GENERIC;
-				break;
-			}
-			if (!have_best || ms < best_ms)
-			{
-				best_ms = ms;
-				best = cand;
-				have_best = true;
-			}
+			r = PYROWAVE_ERROR_GENERIC;
+			break;
 		}
+		for (int w = 0; w < 2 && r == PYROWAVE_SUCCESS; w++)
+			r = batch->run(inputs, budgets, outputs, s);
+		if (r != PYROWAVE_SUCCESS)
+			break;
+		cudaEventRecord(e0, s);
+		for (int it = 0; it < 4 && r == PYROWAVE_SUCCESS; it++)
+			r = batch->run(inputs, budgets, outputs, s);
+		cudaEventRecord(e1, s);
+		float ms = 0.0f;
+		if (r != PYROWAVE_SUCCESS || !cuda_ok(cudaEventSynchronize(e1), "cudaEventSynchronize") ||
+		    !cuda_ok(cudaEventElapsedTime(&ms, e0, e1), "cudaEventElapsedTime"))
+		{
+			r = r != PYROWAVE_SUCCESS ? r : PYROWAVE_ERROR_GENERIC;
+			break;
+		}
+		if (!have_best || ms < best_ms)
+		{
+			best_ms = ms;
+			best = cand;
+			have_best = true;
+		}
+	}
 	cudaEventDestroy(e0);
 	cudaEventDestroy(e1);
 	batch->apply_shape(best);

@@ -353,6 +353,41 @@ struct BatchFrameIO
 __host__ __device__ inline uint32_t batch_cta(int frame, int local) { return (uint32_t(frame) << 24) | uint32_t(local); }
 constexpr int kMaxBatchFrames = 256;
 
+// The batched form's persistent launch: one kernel runs every stage of every
+// frame. Its work items are (frame, stage, item) words in a fixed order; CTAs
+// take them from a ticket counter, and an item first waits until every item
+// of its frame's gating stage (the nearest earlier stage with items) has
+// finished. Stages of a frame in dependency order:
+constexpr int kStageDwt0 = 0;     // forward level L is stage kStageDwt0 + L (levels 0..4)
+constexpr int kStageQuant = 5;    // quantiser of the transform-only levels, two 32x32 blocks per item
+constexpr int kStageResolve = 6;  // rate-control slices
+constexpr int kStagePack = 7;     // two 32x32 blocks per item
+constexpr int kStageDequant = 8;  // two 32x32 blocks per item
+constexpr int kStageIdwt4 = 9;    // inverse level L is stage kStageIdwt4 + 4 - L
+constexpr int kBatchStages = 14;
+constexpr int kBatchLocalBits = 19;
+__host__ __device__ inline uint32_t batch_work(int frame, int stage, int local)
+{
+	return (uint32_t(frame) << 24) | (uint32_t(stage) << kBatchLocalBits) | uint32_t(local);
+}
+constexpr uint32_t kNoGate = 0xffffffffu;
+
+struct BatchRunParams
+{
+	const BatchFrame *frames;
+	const BatchFrameIO *io;
+	const uint32_t *work;  // work items in ticket order
+	const uint32_t *gates; // per frame and stage: gating stage << 24 | its item count, or kNoGate
+	uint32_t *ticket;      // zero at launch
+	uint32_t *done;        // per frame and stage: items finished, zero at launch
+	int32_t nwork;
+	int32_t small_level;   // forward levels >= this only transform; kStageQuant quantises their blocks
+};
+constexpr int kBatchPersistentThreads = 256;
+// Resident CTAs per SM of the persistent kernel (its register and shared-memory limit).
+int batch_persistent_max_ctas_per_sm();
+void launch_batch_persistent(const BatchRunParams &rp, int ctas, cudaStream_t stream);
+
 // Host-side kernel launchers (implemented in the .cu files). Every launch but
 // the first of a sequence may start early (programmatic dependent launch):
 // kernels wait for their predecessor with griddepcontrol before touching

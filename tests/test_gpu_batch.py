@@ -149,9 +149,12 @@ def test_batch_validation(device):
     batch.close()
 
 
-def test_batch_frames_past_tensor_map_table(device):
-    """Frames past the batch's per-frame TMA map table (64 frames) load their
-    tiles with plain loads; both kinds give the oracle's bitstreams and planes."""
+@pytest.mark.parametrize("persistent", [False, True], ids=["per-stage", "persistent"])
+def test_batch_frames_past_tensor_map_table(device, persistent):
+    """Per-stage launches: frames past the batch's per-frame TMA map table (64
+    frames) load their tiles with plain loads, the first 64 through their maps;
+    the persistent launch loads every tile with plain loads. All give the
+    oracle's bitstreams and planes, across 66 frames."""
     import torch
 
     big = (640, 360, True, 60000)
@@ -160,6 +163,7 @@ def test_batch_frames_past_tensor_map_table(device):
     dev_planes = [[torch.from_numpy(p).cuda() for p in pl] for pl in planes]
     infos = [(w, h, capi.CHROMA_444 if c444 else capi.CHROMA_420, b) for w, h, c444, b in shapes]
     batch = capi.Batch(device, infos)
+    batch.set_shape(persistent=persistent, small_level=batch.shape()["small_level"], large_below=256)
     outs = [[torch.zeros_like(p) for p in pl] for pl in dev_planes]
     in_ptrs, in_strides = _ptrs(dev_planes)
     out_ptrs, out_strides = _ptrs(outs)
@@ -175,4 +179,35 @@ def test_batch_frames_past_tensor_map_table(device):
         assert np.array_equal(words_as_bytes(_copy_device_words(bs, sizes[i] // 4)), data), f"frame {i}"
         for p in range(3):
             assert np.array_equal(outs[i][p].cpu().numpy(), decoded[p]), f"frame {i} plane {p}"
+    batch.close()
+
+
+@pytest.mark.parametrize("shape", [
+    dict(persistent=True, small_level=5, ctas_per_sm=2, large_first=True),
+    dict(persistent=True, small_level=3, ctas_per_sm=4, large_first=False),
+    dict(persistent=True, small_level=1, ctas_per_sm=3, large_first=False),
+    dict(persistent=False, small_level=4, large_below=256),
+], ids=["persistent-fused-2cta-large-first", "persistent-small3-4cta", "persistent-small1-3cta", "per-stage"])
+def test_batch_shapes_match_oracle(device, shape):
+    """Every execution shape (one persistent launch with its CTA count, frame
+    order and transform-only suffix, or one launch per stage) gives the oracle's
+    bitstreams and planes."""
+    import torch
+
+    frames = [(1280, 720, False, 150000), (640, 360, True, 60000), (200, 128, True, 30000), (1920, 1080, False, 400000),
+              (34, 30, False, 65536)]
+    planes = [synth.synth_frame(w, h, c444, 80 + i) for i, (w, h, c444, _) in enumerate(frames)]
+    dev_planes = [[torch.from_numpy(p).cuda() for p in pl] for pl in planes]
+    batch = capi.Batch(device, [(w, h, capi.CHROMA_444 if c else capi.CHROMA_420, b) for w, h, c, b in frames])
+    batch.set_shape(**shape)
+    got = batch.shape()
+    assert got["persistent"] == int(shape["persistent"]) and got["small_level"] == shape["small_level"]
+    outs = [[torch.zeros_like(p) for p in pl] for pl in dev_planes]
+    in_ptrs, in_strides = _ptrs(dev_planes)
+    out_ptrs, out_strides = _ptrs(outs)
+    budgets = [b for *_, b in frames]
+    for call in range(2):
+        assert batch.encode(in_ptrs, in_strides, budgets, out_ptrs, out_strides) == capi.PYROWAVE_SUCCESS
+        torch.cuda.synchronize()
+        _check_against_oracle(batch, frames, planes, outs, budgets, call + 1, f"{shape} call {call}")
     batch.close()
