@@ -131,17 +131,35 @@ def psnr_delta(cfg, frames, budget, mask):
     chroma = capi.CHROMA_444 if c444 else capi.CHROMA_420
     dev = capi.Device()
 
+    hvs = {}
+
     def coded(m):
+        """PSNR per frame and plane, and the luma PSNR-HVS-M over all frames (the
+        reference's metric on the GPU, pyrowave_cuda_psnr_hvs_m)."""
         enc = capi.Encoder(dev, w, h, chroma, m)
         dec = capi.Decoder(dev, w, h, chroma, m)
+        errors = torch.zeros(16, dtype=torch.int64, device="cuda")
         res = []
+        hvs_ms = 0.0
         for f in frames:
             d = [torch.from_numpy(p).cuda() for p in f]
             o = [torch.empty_like(p) for p in d]
             enc.encode_device([p.data_ptr() for p in d], [p.stride(0) for p in d], budget)
             s, mt, cap = enc.device_bitstream()
             dec.decode_blocks(mt, s + 8, cap - 2, [p.data_ptr() for p in o], [p.stride(0) for p in o])
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record()
+            capi.check(capi.psnr_hvs_m(w, h, d[0].data_ptr(), d[0].stride(0), o[0].data_ptr(), o[0].stride(0),
+                                       errors.data_ptr()), "psnr_hvs_m")
+            e1.record()
+            e1.synchronize()
+            hvs_ms += e0.elapsed_time(e1)
             res.append([_psnr(a, b.cpu().numpy()) for a, b in zip(f, o)])
+        db = capi.psnr_hvs_m_db(errors.cpu().numpy().view(np.uint64),
+                                capi.lib().pyrowave_psnr_hvs_m_pixels(w, h) * len(frames))
+        hvs[m] = {"height_factor_1": round(float(db[0]), 3), "height_factor_2": round(float(db[8]), 3),
+                  "height_factor_2.875": round(float(db[15]), 3),
+                  "kernel_us_per_frame": round(hvs_ms * 1e3 / len(frames), 2)}
         enc.close()
         dec.close()
         return np.array(res)
@@ -152,7 +170,8 @@ def psnr_delta(cfg, frames, budget, mask):
     return {"mask": hex(mask), "against": "REFERENCE_PRECISION (0x103)", "frames": len(frames),
             "mean_y_cb_cr": [round(float(x), 4) for x in d.mean(axis=0)],
             "worst_frame_y_cb_cr": [round(float(x), 4) for x in worst],
-            "within_0.02_db_mean": bool(np.abs(d.mean(axis=0)).max() <= 0.02)}
+            "within_0.02_db_mean": bool(np.abs(d.mean(axis=0)).max() <= 0.02),
+            "psnr_hvs_m_luma_db": {"this_precision": hvs[mask], "reference_precision": hvs[0x103]}}
 
 
 def _psnr(a, b):
