@@ -536,6 +536,7 @@ def run_packet_decode(cfg, frames, steps: int = 50, boundary: int = 8192):
     ptrs, strides = [t.data_ptr() for t in out], [t.stride(0) for t in out]
     s, m, cap = enc.device_bitstream()
     stream = torch.cuda.Stream()
+    torch.cuda.synchronize()  # inputs complete before the library's stream reads them
 
     def timed(fn):
         for _ in range(5):
@@ -595,6 +596,7 @@ def run_batched(iters: int, frames_n: int = 64, seed: int = 7):
 
     dev = capi.Device()
     stream = torch.cuda.Stream()
+    torch.cuda.synchronize()  # inputs complete before the library's stream reads them
     batch = capi.Batch(dev, [(w, h, capi.CHROMA_444 if c else capi.CHROMA_420, b) for w, h, c, b in slots])
     capi.check(batch.autotune(in_ptrs, in_strides, budgets, out_ptrs, out_strides, stream.cuda_stream), "autotune")
 
@@ -693,6 +695,7 @@ def run_serving(seconds: float, streams_n: int = 32, pool_bytes: int = 16 << 30,
                                                                   [p.stride(0) for p in inp]),
                             out=([p.data_ptr() for p in out], [p.stride(0) for p in out]), keep=out,
                             next=float(rng.exponential(1.0 / fps))))
+    torch.cuda.synchronize()  # inputs complete before the server's streams read them
     # Warm up every stream once (first-use allocation and graph capture).
     for st in streams:
         server.submit(st["sid"], *st["inp"], st["budget"], *st["out"])
@@ -798,6 +801,7 @@ def measure_config(dev, cfg, budget, mask, steps, warmup):
     stream = torch.cuda.Stream()
     sid = stream.cuda_stream
     sizes = []
+    torch.cuda.synchronize()  # inputs complete before the library's stream reads them
 
     def step(i):
         f = frames[i % len(frames)]
@@ -867,6 +871,7 @@ def measure_transform(dev, cfg, steps: int = 30):
               for i in range(n)]
     enc = capi.Encoder(dev, w, h, chroma)
     stream = torch.cuda.Stream()
+    torch.cuda.synchronize()  # inputs complete before the library's stream reads them
     for i in range(3):
         f = frames[i % n]
         enc.transform([p.data_ptr() for p in f], [p.stride(0) for p in f], stream.cuda_stream)

@@ -499,20 +499,30 @@ struct StageEvents
 		created = true;
 	}
 	// Inside stream capture the records become event-record graph nodes
-	// (cudaEventRecordExternal), replayed with every launch of the graph.
-	void begin(pyrowave_device_opaque *dev, cudaStream_t s)
+	// (cudaEventRecordExternal), replayed with every launch of the graph;
+	// outside a capture (captured = false) they are plain records.
+	bool captured = true;
+	void record(cudaStream_t s, cudaEvent_t e)
+	{
+		if (captured)
+			cuda_ok(cudaEventRecordWithFlags(e, s, cudaEventRecordExternal), "cudaEventRecordWithFlags");
+		else
+			cuda_ok(cudaEventRecord(e, s), "cudaEventRecord");
+	}
+	void begin(pyrowave_device_opaque *dev, cudaStream_t s, bool in_capture = true)
 	{
 		if (!dev->stage_timing || !created)
 			return;
 		count = 0;
-		cuda_ok(cudaEventRecordWithFlags(ev[0], s, cudaEventRecordExternal), "cudaEventRecordWithFlags");
+		captured = in_capture;
+		record(s, ev[0]);
 	}
 	void mark(pyrowave_device_opaque *dev, cudaStream_t s, const char *tag)
 	{
 		if (!dev->stage_timing || !created || count >= kMax)
 			return;
 		tags[count++] = tag;
-		cuda_ok(cudaEventRecordWithFlags(ev[count], s, cudaEventRecordExternal), "cudaEventRecordWithFlags");
+		record(s, ev[count]);
 	}
 	// The events of the captured sequence were launched (they are graph nodes).
 	void launched(pyrowave_device_opaque *dev)
@@ -743,6 +753,7 @@ struct pyrowave_encoder_opaque
 	uint32_t h_stream_capacity = 0;
 	uint32_t *h_total = nullptr;
 	cudaEvent_t done = nullptr;
+	cudaEvent_t encoded = nullptr; // recorded after every encode launch (device path included)
 	bool has_frame = false;     // a completed CPU-visible encode exists
 	bool has_device_frame = false;
 	uint32_t sequence_count = 0;
@@ -796,6 +807,9 @@ struct pyrowave_encoder_opaque
 		if (done)
 			cudaEventDestroy(done);
 		done = nullptr;
+		if (encoded)
+			cudaEventDestroy(encoded);
+		encoded = nullptr;
 		timing.destroy();
 		graph.destroy();
 		coef32 = nullptr;
@@ -843,6 +857,8 @@ struct pyrowave_encoder_opaque
 		h_meta = host_alloc<uint32_t>(size_t(g.block_count_32x32) * 2, ok);
 		h_total = host_alloc<uint32_t>(4, ok);
 		if (ok && cudaEventCreateWithFlags(&done, cudaEventDisableTiming) != cudaSuccess)
+			ok = false;
+		if (ok && cudaEventCreateWithFlags(&encoded, cudaEventDisableTiming) != cudaSuccess)
 			ok = false;
 		if (!ok)
 		{
@@ -980,6 +996,7 @@ struct pyrowave_encoder_opaque
 		if (!cuda_ok(cudaGraphLaunch(graph.exec, s), "cudaGraphLaunch"))
 			return PYROWAVE_ERROR_GENERIC;
 		timing.launched(device);
+		cudaEventRecord(encoded, s);
 		has_device_frame = true;
 		return PYROWAVE_SUCCESS;
 	}
@@ -1631,7 +1648,9 @@ pyrowave_result pyrowave_create_default_device(pyrowave_device *device)
 	// first when other work shares the GPU.
 	int least = 0, greatest = 0;
 	cudaDeviceGetStreamPriorityRange(&least, &greatest);
-	if (cudaStreamCreateWithPriority(&dev->stream, cudaStreamNonBlocking, greatest) != cudaSuccess)
+	// A blocking stream: work a caller queues on the legacy default stream (its
+	// uploads, or the buffers it prepares) is ordered with the library's work.
+	if (cudaStreamCreateWithPriority(&dev->stream, cudaStreamDefault, greatest) != cudaSuccess)
 	{
 		delete dev;
 		return PYROWAVE_ERROR_GENERIC;
@@ -2228,8 +2247,11 @@ pyrowave_result pyrowave_cuda_encoder_get_size(pyrowave_encoder encoder, size_t 
 {
 	if (!encoder || !bytes || !encoder->has_device_frame)
 		return PYROWAVE_ERROR_INVALID_ARGUMENT;
+	// The encode ran on the caller's stream, which need not be ordered with the
+	// copy below: wait for it first.
 	uint32_t v[2] = {0, 0};
-	if (cudaMemcpy(v, &encoder->rc->error, 8, cudaMemcpyDeviceToHost) != cudaSuccess)
+	if (!cuda_ok(cudaEventSynchronize(encoder->encoded), "cudaEventSynchronize") ||
+	    cudaMemcpy(v, &encoder->rc->error, 8, cudaMemcpyDeviceToHost) != cudaSuccess)
 		return PYROWAVE_ERROR_GENERIC;
 	if (v[0] != 0)
 		return PYROWAVE_ERROR_GENERIC;
@@ -2265,6 +2287,7 @@ pyrowave_result pyrowave_cuda_encoder_encode_pre_transformed(pyrowave_encoder en
 	launch_pack(bp, b, s);
 	if (!launches_ok("kernel launch"))
 		return PYROWAVE_ERROR_GENERIC;
+	cudaEventRecord(encoder->encoded, s);
 	encoder->has_device_frame = true;
 	return encoder->queue_readback(s);
 }
@@ -2293,7 +2316,7 @@ pyrowave_result pyrowave_cuda_encoder_transform(pyrowave_encoder encoder, const 
 	StageEvents &timing = encoder->timing;
 	timing.collect(dev);
 	timing.prepare(dev);
-	timing.begin(dev, s);
+	timing.begin(dev, s, false);
 	static const char *const tags[kLevels] = {"xdwt0", "xdwt1", "xdwt2", "xdwt3", "xdwt4"};
 	const EncodeBuffers b = encoder->buffers();
 	for (int level = 0; level < kLevels; level++)

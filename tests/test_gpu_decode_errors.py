@@ -7,6 +7,9 @@ the decode as failed. The failure is injected on the host
 completed load is then handled as a timed-out one, so the report path runs
 without stalling or faulting the GPU. Every decode entry point must return an
 error for such a frame, and a decoder built without the injection must not.
+The frame is 1080p: its two finest inverse levels run the 256-thread CTAs
+that load interior tiles this way (the coarser levels load without the
+accelerator, as does the batched form's persistent launch).
 """
 import os
 
@@ -17,7 +20,7 @@ from pyrowave_b200 import capi, synth
 
 pytestmark = pytest.mark.gpu
 
-W, H, BUDGET = 1280, 720, 150000
+W, H, BUDGET = 1920, 1080, 400000
 
 
 @pytest.fixture(scope="module")
@@ -45,6 +48,7 @@ def _encoded(device):
     assert enc.encode_cpu(planes, BUDGET) == capi.PYROWAVE_SUCCESS
     stream, packets = enc.packetize(1 << 30, BUDGET)
     d = [torch.from_numpy(p).cuda() for p in planes]
+    torch.cuda.synchronize()  # the library works on its own stream
     enc.encode_device([p.data_ptr() for p in d], [p.stride(0) for p in d], BUDGET)
     torch.cuda.synchronize()
     return enc, planes, stream, packets
@@ -60,6 +64,7 @@ def _decode_all_ways(dec, enc, planes, stream, packets):
     sync_code, _ = dec.decode_cpu()
 
     outs = [torch.zeros(p.shape, dtype=torch.uint8, device="cuda") for p in planes]
+    torch.cuda.synchronize()
     s, m, _ = enc.device_bitstream()
     n = enc.size()
     dec.decode_blocks(m, s + 8, n // 4 - 2, [t.data_ptr() for t in outs], [t.stride(0) for t in outs])
@@ -68,6 +73,7 @@ def _decode_all_ways(dec, enc, planes, stream, packets):
     total = sum(sz for _, sz in packets)
     d_data = torch.from_numpy(np.ascontiguousarray(stream[:total])).cuda()
     d_desc = torch.from_numpy(np.array(packets, np.int64).reshape(-1)).cuda()
+    torch.cuda.synchronize()
     assert dec.decode_packets(d_data.data_ptr(), total, d_desc.data_ptr(), len(packets),
                               [t.data_ptr() for t in outs], [t.stride(0) for t in outs]) == capi.PYROWAVE_SUCCESS
     st = capi.PacketStatus()
@@ -101,8 +107,11 @@ def test_tile_wait_failure_fails_the_batch(device):
     outs = [torch.zeros_like(p) for p in d]
     args = ([[p.data_ptr() for p in d]], [[p.stride(0) for p in d]], [BUDGET], [[t.data_ptr() for t in outs]],
             [[t.stride(0) for t in outs]])
+    torch.cuda.synchronize()
     with _injected():
         bad = capi.Batch(device, [(W, H, capi.CHROMA_420, BUDGET)])
+    # One launch per stage: its 256-thread inverse levels load tiles with the accelerator.
+    bad.set_shape(persistent=False, small_level=bad.shape()["small_level"], large_below=256)
     assert bad.encode(*args) == capi.PYROWAVE_SUCCESS
     with pytest.raises(capi.PyrowaveError):
         bad.sizes()
@@ -111,6 +120,7 @@ def test_tile_wait_failure_fails_the_batch(device):
     assert bad.sizes()[0] <= BUDGET
     bad.close()
     good = capi.Batch(device, [(W, H, capi.CHROMA_420, BUDGET)])
+    good.set_shape(persistent=False, small_level=good.shape()["small_level"], large_below=256)
     assert good.encode(*args) == capi.PYROWAVE_SUCCESS
     assert good.sizes()[0] <= BUDGET
     good.close()

@@ -61,9 +61,12 @@ def device(gpu):
 
 
 def _to_dev(planes):
+    """Device copies, complete before the library (which works on its own stream) reads them."""
     import torch
 
-    return [torch.from_numpy(np.ascontiguousarray(p)).cuda() for p in planes]
+    out = [torch.from_numpy(np.ascontiguousarray(p)).cuda() for p in planes]
+    torch.cuda.synchronize()
+    return out
 
 
 def _mismatch(name, got, want):

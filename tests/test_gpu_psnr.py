@@ -36,6 +36,7 @@ def _gpu_psnr(device, w, h, c444, mode, frames, budget):
     for planes in frames:
         d = [torch.from_numpy(p).cuda() for p in planes]
         o = [torch.zeros_like(p) for p in d]
+        torch.cuda.synchronize()  # the library works on its own stream
         enc.encode_device([p.data_ptr() for p in d], [p.stride(0) for p in d], budget)
         s, m, _ = enc.device_bitstream()
         n = enc.size()

@@ -49,6 +49,7 @@ def _serve(device, which, interleave):
         ids[si] = sid
         frames[si] = _frames(si)
         outs[si] = [[torch.full_like(p, 0x55) for p in f] for f in frames[si]]
+    torch.cuda.synchronize()  # the server's streams do not order with torch's
     order = [(si, k) for k in range(FRAMES_PER_STREAM) for si in which] if interleave else \
         [(si, k) for si in which for k in range(FRAMES_PER_STREAM)]
     req = {}
@@ -130,6 +131,7 @@ def test_admission_by_memory(device):
     frames = [[synth.synth_frame(w, h, False, 300 + 10 * j + k) for k in range(3)] for j in range(2)]
     dev_frames = [[[torch.from_numpy(p).cuda() for p in f] for f in fr] for fr in frames]
     outs = [[[torch.zeros_like(p) for p in f] for f in fr] for fr in dev_frames]
+    torch.cuda.synchronize()
     req = {}
     for k in range(3):
         for j, sid in enumerate(ids):
