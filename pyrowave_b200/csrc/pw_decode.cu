@@ -68,60 +68,6 @@ __global__ void __launch_bounds__(kThreads, kMinBlocks) idwt_batch_kernel(const 
 	                    local / ntiles);
 }
 
-// The small levels of one decode in one launch, coarsest first: every CTA
-// takes the next tile from the decode's ticket counter, and a level's tiles
-// wait for every tile of the coarser level (bounded; a wait that gives up sets
-// kDecodeErrorLevelWait). Taking tickets in order means a CTA only waits for
-// tiles that running CTAs hold.
-constexpr int kSmallInvThreads = 1024;
-constexpr uint32_t kInvLevelWaitSpins = 1u << 22;
-
-__global__ void __launch_bounds__(kSmallInvThreads, 1)
-    idwt_small_levels_kernel(const __grid_constant__ SmallInverseParams sp, const DecodeInput in, const PlaneOutput out)
-{
-	__shared__ IdwtShared sh;
-	__shared__ int s_item;
-	DecodeState *st = in.state;
-	// The dequantiser clears the decode's counters: take a ticket only after it completed.
-	pdl_wait();
-	if (threadIdx.x == 0)
-		s_item = int(atomicAdd(&st->ticket, 1u));
-	__syncthreads();
-	const int item = s_item;
-	int level = -1, local = 0;
-	for (int l = sp.last_level; l >= sp.first_level; l--)
-		if (item >= sp.item_first[l] && item < sp.item_first[l] + sp.ntiles[l])
-		{
-			level = l;
-			local = item - sp.item_first[l];
-		}
-	if (level < 0)
-		return;
-	if (level < sp.last_level && threadIdx.x == 0)
-	{
-		uint32_t spins = 0;
-		while (ld_acquire_u32(&st->level_done[level + 1]) < uint32_t(sp.ntiles[level + 1]))
-		{
-			if (++spins > kInvLevelWaitSpins)
-			{
-				atomicOr(&st->error, kDecodeErrorLevelWait);
-				break;
-			}
-			__nanosleep(32);
-		}
-	}
-	__syncthreads();
-	const LevelParams &p = sp.lp[level];
-	const int per_comp = p.L.tiles_x * p.L.tiles_y;
-	idwt_body<kSmallInvThreads>(sh, p, in, out, nullptr, local % per_comp, local / per_comp);
-	__syncthreads();
-	if (threadIdx.x == 0)
-	{
-		__threadfence();
-		atomicAdd(&st->level_done[level], 1u);
-	}
-}
-
 // Canonical pyramid (all transmitted bands, band-major, unpadded) <-> padded storage.
 __global__ void pyramid_io_kernel(const BlockParams p, float *canonical, float *coef32, __half *coef16,
                                   int to_canonical)
@@ -180,16 +126,6 @@ void launch_idwt_level(const LevelParams &p, const DecodeInput &in, const PlaneO
 		LaunchConfig lc(grid, dim3(256), stream, programmatic);
 		cudaLaunchKernelEx(&lc.cfg, idwt_kernel<256, 4>, p, in, out, m);
 	}
-}
-
-void launch_idwt_small_levels(const SmallInverseParams &sp, const DecodeInput &in, const PlaneOutput &out,
-                              bool programmatic, cudaStream_t stream)
-{
-	int items = 0;
-	for (int l = sp.first_level; l <= sp.last_level; l++)
-		items += sp.ntiles[l];
-	LaunchConfig lc(dim3(items), dim3(kSmallInvThreads), stream, programmatic);
-	cudaLaunchKernelEx(&lc.cfg, idwt_small_levels_kernel, sp, in, out);
 }
 
 void launch_pyramid_io(const BlockParams &p, float *canonical, float *coef32, __half *coef16, bool to_canonical,

@@ -179,6 +179,39 @@ __device__ __forceinline__ void st_release_u64(unsigned long long *p, unsigned l
 	asm volatile("st.release.gpu.global.u64 [%0], %1;" ::"l"(p), "l"(v) : "memory");
 }
 
+// Thread-block clusters: this CTA's rank, the cluster's CTA count, hardware
+// cluster barriers (every thread of every CTA of the cluster takes part) and
+// 64-bit stores into another CTA's shared memory (distributed shared memory).
+__device__ __forceinline__ uint32_t cluster_rank()
+{
+	uint32_t r;
+	asm volatile("mov.u32 %0, %%cluster_ctarank;" : "=r"(r));
+	return r;
+}
+__device__ __forceinline__ uint32_t cluster_size()
+{
+	uint32_t n;
+	asm volatile("mov.u32 %0, %%cluster_nctarank;" : "=r"(n));
+	return n;
+}
+// Arrive early (relaxed: orders nothing) and wait before the first access to
+// another CTA's shared memory: every CTA of the cluster has started by then.
+__device__ __forceinline__ void cluster_arrive_relaxed() { asm volatile("barrier.cluster.arrive.relaxed.aligned;" ::: "memory"); }
+__device__ __forceinline__ void cluster_wait() { asm volatile("barrier.cluster.wait.acquire.aligned;" ::: "memory"); }
+// Full barrier: shared and global memory writes before it are visible to every
+// thread of the cluster after it.
+__device__ __forceinline__ void cluster_sync()
+{
+	asm volatile("barrier.cluster.arrive.release.aligned;" ::: "memory");
+	asm volatile("barrier.cluster.wait.acquire.aligned;" ::: "memory");
+}
+__device__ __forceinline__ void st_cluster_u64(const void *local_smem, uint32_t rank, unsigned long long v)
+{
+	uint32_t remote;
+	asm volatile("mapa.shared::cluster.u32 %0, %1, %2;" : "=r"(remote) : "r"(smem_addr(local_smem)), "r"(rank));
+	asm volatile("st.shared::cluster.u64 [%0], %1;" ::"r"(remote), "l"(v) : "memory");
+}
+
 // 8x8 bit-matrix transpose: bit j of byte i of the input becomes bit i of byte
 // j of the output (three swap stages of 1, 2 and 4 bit-square blocks).
 __device__ __forceinline__ unsigned long long transpose8x8(unsigned long long x)

@@ -800,92 +800,6 @@ __global__ void __launch_bounds__(256 * S) quant_blocks_batch_kernel(const Batch
 }
 
 // ---------------------------------------------------------------------------
-// The small levels of one frame in one launch: for each level from the first
-// small one to the last, the transform of its tiles (input: the finer level's
-// LL), then the quantiser and RD analysis of its blocks. Every CTA takes the
-// next work item from a per-frame ticket counter, so an item that waits for
-// another (a level's transform for the finer level's; a level's quantiser for
-// its transform) only waits for items that running CTAs hold: the waits end
-// even when not every CTA of the grid is resident. The quantiser of a level
-// runs while the coarser levels transform. Waits are bounded; a wait that
-// gives up sets kErrorLevelWait.
-constexpr int kSmallThreads = 1024;
-constexpr int kSmallQuantGroups = kSmallThreads / 256; // 32x32 blocks per quantiser item (two threads per sub-block)
-constexpr uint32_t kLevelWaitSpins = 1u << 22;
-
-__device__ __forceinline__ void wait_count(const uint32_t *counter, uint32_t target, uint32_t *error)
-{
-	__shared__ int s_failed;
-	if (threadIdx.x == 0)
-	{
-		uint32_t spins = 0;
-		int failed = 0;
-		while (ld_acquire_u32(counter) < target)
-		{
-			if (++spins > kLevelWaitSpins)
-			{
-				atomicOr(error, kErrorLevelWait);
-				failed = 1;
-				break;
-			}
-			__nanosleep(32);
-		}
-		s_failed = failed;
-	}
-	__syncthreads();
-	(void)s_failed;
-}
-
-__global__ void __launch_bounds__(kSmallThreads, 1)
-    dwt_small_levels_kernel(const __grid_constant__ SmallLevelParams sp, const PlaneInput in, const EncodeBuffers buf)
-{
-	__shared__ DwtShared sh;
-	__shared__ int s_item;
-	if (threadIdx.x == 0)
-		s_item = int(atomicAdd(&buf.rc->small_ticket, 1u));
-	__syncthreads();
-	const int item = s_item;
-	int level = -1, kind = 0, local = 0;
-	for (int l = sp.first_level; l < kLevels; l++)
-		for (int k = 0; k < 2; k++)
-		{
-			const int i0 = sp.item_first[2 * l + k], i1 = sp.item_first[2 * l + k + 1];
-			if (item >= i0 && item < i1)
-			{
-				level = l;
-				kind = k;
-				local = item - i0;
-			}
-		}
-	if (level < 0)
-		return;
-	if (kind == 0)
-	{
-		// Transform: after every tile of the finer level (the first small level
-		// follows the previous launch through the dependency wait in the body).
-		if (level > sp.first_level)
-			wait_count(&buf.rc->level_done[level - 1], uint32_t(sp.ntiles[level - 1]), &buf.rc->error);
-		const LevelParams &p = sp.lp[level];
-		const int per_comp = p.L.tiles_x * p.L.tiles_y;
-		dwt_forward_body<kSmallThreads>(sh, p, in, buf, nullptr, 0, local % per_comp, local / per_comp);
-		__syncthreads();
-		if (threadIdx.x == 0)
-		{
-			__threadfence();
-			atomicAdd(&buf.rc->level_done[level], 1u);
-		}
-	}
-	else
-	{
-		// Quantiser: after every tile of its own level, four blocks per item.
-		wait_count(&buf.rc->level_done[level], uint32_t(sp.ntiles[level]), &buf.rc->error);
-		float(*tile)[32][kBandPitch] = reinterpret_cast<float(*)[32][kBandPitch]>(&sh.in[0][0]);
-		quant_blocks_body<2, kSmallQuantGroups>(sp.bp, buf, sp.block_first[level],
-		                                        sp.block_first[level] + sp.block_count[level], local, tile, sh.q);
-	}
-}
-
-// ---------------------------------------------------------------------------
 // Block-wide exclusive scan (blockDim.x a multiple of 32, at most 1024);
 // returns the exclusive prefix and the block total.
 template <typename T> __device__ __forceinline__ T block_exclusive_scan(T v, T *warp_sums, T &total)
@@ -1128,8 +1042,6 @@ __device__ __forceinline__ void resolve_body(const ResolveParams &p, const Encod
 			ex += sv;
 		});
 		__syncthreads();
-		if (t == 0 && s_cut != 0xffffffffu)
-			rc->block_cut = s_cut; // every slice that reaches the cut finds the same block
 	}
 	const uint32_t cut = s_cut;
 
@@ -1325,8 +1237,159 @@ __global__ void __launch_bounds__(kSingleResolveThreads, 1)
 	{
 		const uint32_t total_words = uint32_t(all >> 32);
 		const uint32_t non_zero = uint32_t(all & 0xffffffffull) >> 1;
-		if (cut != 0xffffffffu)
-			rc->block_cut = cut;
+		rc->xstar = xstar;
+		rc->sequence = p.sequence & 7u;
+		rc->total_words = total_words;
+		rc->non_zero_blocks = non_zero;
+		if (2 + uint64_t(total_words) > buf.stream_capacity_words)
+			atomicOr(&rc->error, kErrorStreamCapacity);
+		// Start-of-frame sequence header (bitstream.md:250-265).
+		buf.stream[0] = uint32_t(p.width - 1) | (uint32_t(p.height - 1) << 14) | ((p.sequence & 7u) << 28) | (1u << 31);
+		buf.stream[1] = (non_zero & 0xffffffu) | (uint32_t(p.chroma444 ? 1 : 0) << 26);
+	}
+}
+
+// The same resolve on one thread-block cluster of C CTAs (C a power of two up
+// to 16), for frames of at most C * 1024 * R blocks: thread g = rank * 1024 + t
+// owns the run of at most R consecutive blocks from g * R', R' = ceil(blocks /
+// (C * 1024)), its RD rows loaded once into registers. Every CTA scans the
+// whole histogram itself (8 KB), so all of them find x* and the requirement
+// with no exchange. The cut and the offsets need prefixes across CTAs: each
+// CTA writes its totals into the shared memory of every higher-ranked CTA
+// (distributed shared memory) and a hardware cluster barrier publishes them,
+// twice per frame. An operation at the x* slot is applied when the exclusive
+// prefix of the x* subdivision's savings before its block is below the
+// requirement, which is the same set as the blocks before the cut. Results are
+// those of resolve_body.
+constexpr int kClusterResolveThreads = 1024;
+constexpr int kMaxResolveCluster = 16;
+
+template <int R>
+__global__ void __launch_bounds__(kClusterResolveThreads, 1)
+    resolve_cluster_kernel(const ResolveParams p, const EncodeBuffers buf)
+{
+	__shared__ uint32_t scan[kHistSize];
+	__shared__ uint32_t warp_sums[32];
+	__shared__ unsigned long long warp_sums64[32];
+	__shared__ int s_xstar;
+	__shared__ unsigned long long s_saving_totals[kMaxResolveCluster]; // [r]: savings total of rank r < this rank
+	__shared__ unsigned long long s_word_totals[kMaxResolveCluster];   // [r]: words << 32 | non-empty << 1 of rank r
+	// Peers write into this CTA's shared memory only after every CTA started.
+	cluster_arrive_relaxed();
+	RateControlState *rc = buf.rc;
+	const int t = threadIdx.x;
+	const uint32_t rank = cluster_rank(), ncta = cluster_size();
+	const int n = p.block_count_32x32;
+	const int per = (n + int(ncta) * kClusterResolveThreads - 1) / (int(ncta) * kClusterResolveThreads); // <= R
+	const int b0 = min((int(rank) * kClusterResolveThreads + t) * per, n), b1 = min(b0 + per, n);
+	pdl_wait();
+	pdl_trigger();
+
+	RawRD rows[R];
+#pragma unroll
+	for (int i = 0; i < R; i++)
+		if (b0 + i < b1)
+			rows[i] = load_raw_rd(buf, b0 + i);
+	static_assert(kHistSize == 2 * kClusterResolveThreads, "two histogram slots per thread");
+	const uint32_t h0 = __ldcg(&rc->histogram[2 * t]), h1 = __ldcg(&rc->histogram[2 * t + 1]);
+	const uint32_t consumed = __ldcg(&rc->consumed);
+	if (t == 0)
+		s_xstar = -1;
+	uint32_t total;
+	const uint32_t run = block_exclusive_scan(h0 + h1, warp_sums, total);
+	scan[2 * t] = run + h0;
+	scan[2 * t + 1] = run + h0 + h1;
+	__syncthreads();
+
+	const int64_t need = int64_t(consumed) - int64_t(p.target_words);
+	if (need > 0)
+	{
+		for (int x = 2 * t; x < 2 * t + 2; x++)
+			if (int64_t(scan[x]) >= need && (x == 0 || int64_t(scan[x - 1]) < need))
+				s_xstar = x;
+	}
+	__syncthreads();
+	const int xstar = s_xstar; // the same in every CTA: each scanned the same histogram
+	cluster_wait();
+
+	// Which of this thread's blocks apply their operation at the x* slot.
+	bool apply_x[R];
+#pragma unroll
+	for (int i = 0; i < R; i++)
+		apply_x[i] = false;
+	if (xstar >= 0)
+	{
+		const int start = (xstar & (kSubdivisions - 1)) * p.blocks_per_subdivision;
+		const int end = min(start + p.blocks_per_subdivision, n);
+		const int64_t required = need - (xstar > 0 ? int64_t(scan[xstar - 1]) : 0);
+		const uint32_t bk = uint32_t(xstar >> 4);
+		uint32_t sv[R];
+		uint32_t local = 0;
+#pragma unroll
+		for (int i = 0; i < R; i++)
+		{
+			const int blk = b0 + i;
+			sv[i] = (blk < b1 && blk >= start && blk < end) ? op_saving_at_bucket(rows[i], bk) : 0u;
+			local += sv[i];
+		}
+		uint32_t cta_total;
+		uint32_t ex = block_exclusive_scan(local, warp_sums, cta_total);
+		if (t < int(ncta) && t > int(rank))
+			st_cluster_u64(&s_saving_totals[rank], uint32_t(t), cta_total);
+		cluster_sync();
+		uint64_t base = 0;
+		for (uint32_t r = 0; r < rank; r++)
+			base += s_saving_totals[r];
+#pragma unroll
+		for (int i = 0; i < R; i++)
+		{
+			apply_x[i] = sv[i] != 0 && int64_t(base + ex) < required;
+			ex += sv[i];
+		}
+	}
+
+	// Word counts, the cluster-wide scan of offsets, the per-block decisions.
+	uint32_t w[R];
+	int q[R];
+	unsigned long long local = 0; // words << 32 | non-empty blocks << 1
+#pragma unroll
+	for (int i = 0; i < R; i++)
+	{
+		const int blk = b0 + i;
+		w[i] = 0;
+		q[i] = 0;
+		if (blk < b1)
+		{
+			// Operations before the x* slot, plus the one at it where applied.
+			w[i] = block_words(rows[i], blk, blk >> p.subdivision_shift, xstar, apply_x[i] ? 0xffffffffu : 0u, q[i]);
+			local += (uint64_t(w[i]) << 32) | (uint64_t(w[i] != 0 ? 1 : 0) << 1);
+		}
+	}
+	unsigned long long cta_words;
+	unsigned long long pos = block_exclusive_scan(local, warp_sums64, cta_words);
+	if (t < int(ncta) && t > int(rank))
+		st_cluster_u64(&s_word_totals[rank], uint32_t(t), cta_words);
+	cluster_sync();
+	unsigned long long base = 0;
+	for (uint32_t r = 0; r < rank; r++)
+		base += s_word_totals[r];
+	pos += base;
+#pragma unroll
+	for (int i = 0; i < R; i++)
+	{
+		const int blk = b0 + i;
+		if (blk < b1)
+		{
+			buf.quant[blk] = q[i];
+			*reinterpret_cast<uint2 *>(buf.block_meta + 2 * size_t(blk)) = make_uint2(uint32_t(pos >> 32), w[i]);
+			pos += uint64_t(w[i]) << 32;
+		}
+	}
+	if (t == 0 && rank == ncta - 1)
+	{
+		const unsigned long long all = base + cta_words;
+		const uint32_t total_words = uint32_t(all >> 32);
+		const uint32_t non_zero = uint32_t(all & 0xffffffffull) >> 1;
 		rc->xstar = xstar;
 		rc->sequence = p.sequence & 7u;
 		rc->total_words = total_words;
@@ -1834,15 +1897,6 @@ void launch_dwt_forward_level(const LevelParams &p, const PlaneInput &in, const 
 	}
 }
 
-int small_level_items(const SmallLevelParams &sp) { return sp.item_first[2 * kLevels]; }
-
-void launch_dwt_small_levels(const SmallLevelParams &sp, const PlaneInput &in, const EncodeBuffers &buf,
-                             bool programmatic, cudaStream_t stream)
-{
-	LaunchConfig lc(dim3(small_level_items(sp)), dim3(kSmallThreads), stream, programmatic);
-	cudaLaunchKernelEx(&lc.cfg, dwt_small_levels_kernel, sp, in, buf);
-}
-
 void launch_quant_pretransformed(const BlockParams &p, const EncodeBuffers &buf, int nblocks, bool programmatic,
                                  cudaStream_t stream)
 {
@@ -1850,12 +1904,77 @@ void launch_quant_pretransformed(const BlockParams &p, const EncodeBuffers &buf,
 	cudaLaunchKernelEx(&lc.cfg, quant_pretransformed_kernel<2>, p, buf, nblocks);
 }
 
+int resolve_cluster_max()
+{
+	static int cached = 0;
+	if (cached == 0)
+	{
+		// Clusters of 16 CTAs are opt-in; use them where the device can place one.
+		int n = 0;
+		if (cudaFuncSetAttribute(resolve_cluster_kernel<1>, cudaFuncAttributeNonPortableClusterSizeAllowed, 1) ==
+		        cudaSuccess &&
+		    cudaFuncSetAttribute(resolve_cluster_kernel<2>, cudaFuncAttributeNonPortableClusterSizeAllowed, 1) ==
+		        cudaSuccess &&
+		    cudaFuncSetAttribute(resolve_cluster_kernel<4>, cudaFuncAttributeNonPortableClusterSizeAllowed, 1) ==
+		        cudaSuccess)
+		{
+			cudaLaunchConfig_t cfg = {};
+			cudaLaunchAttribute attr = {};
+			cfg.gridDim = dim3(kMaxResolveCluster);
+			cfg.blockDim = dim3(kClusterResolveThreads);
+			attr.id = cudaLaunchAttributeClusterDimension;
+			attr.val.clusterDim.x = kMaxResolveCluster;
+			attr.val.clusterDim.y = 1;
+			attr.val.clusterDim.z = 1;
+			cfg.attrs = &attr;
+			cfg.numAttrs = 1;
+			if (cudaOccupancyMaxActiveClusters(&n, resolve_cluster_kernel<4>, &cfg) != cudaSuccess)
+				n = 0;
+		}
+		(void)cudaGetLastError();
+		cached = n > 0 ? kMaxResolveCluster : 8;
+	}
+	return cached;
+}
+
+bool resolve_cluster_shape(int blocks, int &ctas, int &rows)
+{
+	const int cmax = resolve_cluster_max();
+	int c = 1;
+	while (c < cmax && c * kClusterResolveThreads < blocks)
+		c *= 2;
+	const int r = (blocks + c * kClusterResolveThreads - 1) / (c * kClusterResolveThreads);
+	if (r > 4)
+		return false;
+	ctas = c;
+	rows = r <= 1 ? 1 : (r <= 2 ? 2 : 4);
+	return true;
+}
+
 void launch_resolve(const ResolveParams &p, const EncodeBuffers &buf, cudaStream_t stream)
 {
-	if (p.block_count_32x32 <= kSingleResolveRows * kSingleResolveThreads)
+	int ctas = 0, rows = 0;
+	if (resolve_cluster_shape(p.block_count_32x32, ctas, rows))
 	{
-		LaunchConfig lc(dim3(1), dim3(kSingleResolveThreads), stream, true);
-		cudaLaunchKernelEx(&lc.cfg, resolve_single_kernel, p, buf);
+		cudaLaunchConfig_t cfg = {};
+		cudaLaunchAttribute attrs[2] = {};
+		cfg.gridDim = dim3(ctas);
+		cfg.blockDim = dim3(kClusterResolveThreads);
+		cfg.stream = stream;
+		attrs[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+		attrs[0].val.programmaticStreamSerializationAllowed = 1;
+		attrs[1].id = cudaLaunchAttributeClusterDimension;
+		attrs[1].val.clusterDim.x = unsigned(ctas);
+		attrs[1].val.clusterDim.y = 1;
+		attrs[1].val.clusterDim.z = 1;
+		cfg.attrs = attrs;
+		cfg.numAttrs = 2;
+		if (rows == 1)
+			cudaLaunchKernelEx(&cfg, resolve_cluster_kernel<1>, p, buf);
+		else if (rows == 2)
+			cudaLaunchKernelEx(&cfg, resolve_cluster_kernel<2>, p, buf);
+		else
+			cudaLaunchKernelEx(&cfg, resolve_cluster_kernel<4>, p, buf);
 		return;
 	}
 	const int slices = resolve_slices(p.block_count_32x32, p.blocks_per_subdivision);

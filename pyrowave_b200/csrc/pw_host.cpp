@@ -382,52 +382,6 @@ BlockParams make_block_params(const Geometry &g)
 	return p;
 }
 
-SmallInverseParams make_small_inverse_params(const Geometry &g, int first_level)
-{
-	SmallInverseParams sp = {};
-	for (int level = 0; level < kLevels; level++)
-		sp.lp[level] = make_level_params(g, level);
-	sp.first_level = first_level;
-	sp.last_level = kLevels - 1;
-	int item = 0;
-	for (int level = kLevels - 1; level >= 0; level--)
-	{
-		const int ncomp = (level == 0 && !g.chroma444) ? 1 : 3;
-		sp.ntiles[level] = g.level[level].tiles_x * g.level[level].tiles_y * ncomp;
-		sp.item_first[level] = item;
-		if (level >= first_level)
-			item += sp.ntiles[level];
-	}
-	return sp;
-}
-
-SmallLevelParams make_small_level_params(const Geometry &g, int first_level)
-{
-	SmallLevelParams sp = {};
-	for (int level = 0; level < kLevels; level++)
-		sp.lp[level] = make_level_params(g, level);
-	sp.bp = make_block_params(g);
-	sp.first_level = first_level;
-	int item = 0;
-	for (int level = 0; level < kLevels; level++)
-	{
-		const int ncomp = (level == 0 && !g.chroma444) ? 1 : 3;
-		const int first = level == kLevels - 1 ? 0 : g.band[0][level][1].block32_offset;
-		const int end = level == 0 ? g.block_count_32x32 : g.band[0][level - 1][1].block32_offset;
-		sp.ntiles[level] = g.level[level].tiles_x * g.level[level].tiles_y * ncomp;
-		sp.block_first[level] = first;
-		sp.block_count[level] = end - first;
-		sp.item_first[2 * level] = item;
-		if (level >= first_level)
-			item += sp.ntiles[level];
-		sp.item_first[2 * level + 1] = item;
-		if (level >= first_level)
-			item += (sp.block_count[level] + 3) / 4;
-	}
-	sp.item_first[2 * kLevels] = item;
-	return sp;
-}
-
 ResolveParams make_resolve_params(const Geometry &g, uint32_t target_words, uint32_t sequence)
 {
 	ResolveParams p = {};
@@ -760,10 +714,8 @@ struct pyrowave_encoder_opaque
 	StageEvents timing;
 	CapturedGraph graph;
 	KernelNode node_dwt[kLevels];
-	int small_level = kLevels; // levels >= this run in one launch: their transforms and quantisers
+	int small_level = kLevels; // levels >= this: transform only, then one quantiser launch over their blocks
 	int small_blocks = 0;      // 32x32 blocks of those levels (a prefix in block index order)
-	SmallLevelParams small = {};
-	KernelNode node_small;
 	KernelNode node_resolve;
 
 	EncodeBuffers buffers() const
@@ -842,7 +794,7 @@ struct pyrowave_encoder_opaque
 			lp[level] = make_level_params(g, level);
 		bp = make_block_params(g);
 		small_level_split(g, small_level, small_blocks);
-		small = make_small_level_params(g, small_level);
+		(void)resolve_cluster_max();
 		bool ok = true;
 		coef32 = dev_alloc<float>(size_t(g.storage_elems32), ok);
 		coef16 = dev_alloc<__half>(size_t(g.storage_elems16), ok);
@@ -948,17 +900,19 @@ struct pyrowave_encoder_opaque
 			cudaMemsetAsync(rc, 0, sizeof(RateControlState), s);
 			static const char *const dwt_tags[kLevels] = {"dwt0", "dwt1", "dwt2", "dwt3", "dwt4"};
 			const bool pdl = !device->stage_timing; // event nodes between kernels break programmatic edges
-			for (int level = 0; level < small_level; level++)
+			// The small levels (few tiles each) transform only, each level one launch;
+			// one launch then quantises all their blocks, so no level's quantiser
+			// waits on the critical path of the transforms.
+			for (int level = 0; level < kLevels; level++)
 			{
-				launch_dwt_forward_level(lp[level], in, b, &in_maps[level], true, pdl && level > 0, s);
+				launch_dwt_forward_level(lp[level], in, b, &in_maps[level], level < small_level, pdl && level > 0, s);
 				ok = ok && last_captured_node(s, node_dwt[level]);
 				timing.mark(device, s, dwt_tags[level]);
 			}
-			if (small_level < kLevels)
+			if (small_blocks > 0)
 			{
-				launch_dwt_small_levels(small, in, b, pdl && small_level > 0, s);
-				ok = ok && last_captured_node(s, node_small);
-				timing.mark(device, s, "dwt_small");
+				launch_quant_pretransformed(bp, b, small_blocks, pdl, s);
+				timing.mark(device, s, "quant");
 			}
 			launch_resolve(make_resolve_params(g, target_words, sequence_count), b, s);
 			ok = ok && last_captured_node(s, node_resolve);
@@ -978,13 +932,11 @@ struct pyrowave_encoder_opaque
 			PlaneInput pin = in;
 			ResolveParams rp = make_resolve_params(g, target_words, sequence_count);
 			bool ok = true;
-			for (int level = 0; level < small_level; level++)
+			for (int level = 0; level < kLevels; level++)
 			{
-				int fused = forward_fused_mode(lp[level], true);
+				int fused = forward_fused_mode(lp[level], level < small_level);
 				ok = ok && set_kernel_args(graph.exec, node_dwt[level], lp[level], pin, b, fused, in_maps[level]);
 			}
-			if (small_level < kLevels)
-				ok = ok && set_kernel_args(graph.exec, node_small, small, pin, b);
 			ok = ok && set_kernel_args(graph.exec, node_resolve, rp, b);
 			if (!ok)
 			{
@@ -1103,11 +1055,7 @@ struct pyrowave_decoder_opaque
 	KernelNode node_idwt_full[kLevels], node_idwt_only[kLevels];
 
 	LevelTileMap band_maps[kLevels] = {}; // TMA maps of the FP32 bands (inverse transform tile loads)
-	int small_level = kLevels;            // levels >= this: one inverse launch (coarsest first)
-	int small_blocks = 0;
-	SmallInverseParams small = {};
-	KernelNode node_small_full, node_small_only;
-	DecodeState *state_d = nullptr;  // per-decode state: error bits and the small-levels launch's counters
+	DecodeState *state_d = nullptr;  // per-decode state: error bits
 	uint32_t *error_d = nullptr;     // &state_d->error: kDecodeError* bits of the last decode (cleared by each decode)
 	uint32_t *h_error = nullptr;     // page-locked copy of error_d
 	cudaEvent_t decode_done = nullptr; // recorded after every decode launch
@@ -1318,8 +1266,6 @@ struct pyrowave_decoder_opaque
 		h_error = host_alloc<uint32_t>(1, ok);
 		if (state_d)
 			cudaMemset(state_d, 0, sizeof(DecodeState));
-		small_level_split(g, small_level, small_blocks);
-		small = make_small_inverse_params(g, small_level);
 		if (ok && cudaEventCreateWithFlags(&decode_done, cudaEventDisableTiming) != cudaSuccess)
 			ok = false;
 		build_tile_maps(g, lp, coef32, nullptr, band_maps);
@@ -1407,17 +1353,10 @@ struct pyrowave_decoder_opaque
 				timing.mark(device, s, "dequant");
 			}
 			// Programmatic launches follow a kernel only (not the clear of an inverse-only decode).
-			if (small_level < kLevels)
-			{
-				launch_idwt_small_levels(small, in, out, pdl && dequant, s);
-				ok = ok && last_captured_node(s, dequant ? node_small_full : node_small_only);
-				timing.mark(device, s, "idwt_small");
-			}
 			static const char *const idwt_tags[kLevels] = {"idwt0", "idwt1", "idwt2", "idwt3", "idwt4"};
-			for (int level = small_level - 1; level >= 0; level--)
+			for (int level = kLevels - 1; level >= 0; level--)
 			{
-				launch_idwt_level(lp[level], in, out, &band_maps[level],
-				                  pdl && (dequant || small_level < kLevels || level < kLevels - 1), s);
+				launch_idwt_level(lp[level], in, out, &band_maps[level], pdl && (dequant || level < kLevels - 1), s);
 				ok = ok && last_captured_node(s, dequant ? node_idwt_full[level] : node_idwt_only[level]);
 				timing.mark(device, s, idwt_tags[level]);
 			}
@@ -1439,9 +1378,7 @@ struct pyrowave_decoder_opaque
 				int first = 0;
 				ok = set_kernel_args(graph.exec, node_dequant, bp, din, first);
 			}
-			if (small_level < kLevels)
-				ok = ok && set_kernel_args(graph.exec, dequant ? node_small_full : node_small_only, small, din, pout);
-			for (int level = 0; level < small_level; level++)
+			for (int level = 0; level < kLevels; level++)
 				ok = ok && set_kernel_args(graph.exec, dequant ? node_idwt_full[level] : node_idwt_only[level], lp[level],
 				                           din, pout, band_maps[level]);
 			if (!ok)

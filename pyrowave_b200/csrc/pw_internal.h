@@ -131,27 +131,21 @@ struct RateControlState
 	uint32_t total_words;          // coded words after rate control (blocks only)
 	uint32_t non_zero_blocks;
 	int32_t xstar;                 // first partially applied bucket*16+subdivision (-1 none)
-	uint32_t block_cut;            // ops of blocks >= this in the partial subdivision are not applied
 	uint32_t sequence;
 	uint32_t decode_error;         // kDecodeError* bits of the batched form's decode of this frame
-	uint32_t small_ticket;         // next work item of the small-levels launch
-	uint32_t level_done[kLevels];  // transform tiles finished per level (small-levels launch)
 	// Per resolve slice: words << 32 | non-empty blocks << 1 | 1 once published.
 	unsigned long long slice_total[kMaxResolveSlices];
 };
 
 // Error bits of a decoder's error word.
 constexpr uint32_t kDecodeErrorTileWait = 1u;  // an inverse-transform tile load did not complete in time
-constexpr uint32_t kDecodeErrorLevelWait = 2u; // a small-levels tile gave up waiting for the coarser level
 
 // Per-decode device state of a decoder, cleared by the dequantiser (or by a
 // clear before an inverse-only decode).
 struct DecodeState
 {
-	uint32_t error;               // kDecodeError* bits
-	uint32_t ticket;              // next tile of the small-levels inverse launch
-	uint32_t level_done[kLevels]; // tiles finished per level (small-levels inverse launch)
-	uint32_t pad;
+	uint32_t error; // kDecodeError* bits
+	uint32_t pad[3];
 };
 
 // Error bits of RateControlState::error.
@@ -159,7 +153,7 @@ constexpr uint32_t kErrorStreamCapacity = 1u; // the coded frame does not fit th
 constexpr uint32_t kErrorWordCount = 2u;      // a packed block's size differs from the rate-control estimate
 constexpr uint32_t kErrorSliceWait = 4u;      // a resolve slice gave up waiting for a preceding slice's total
 constexpr uint32_t kErrorTileWait = 8u;       // a forward-transform tile load did not complete in time
-constexpr uint32_t kErrorLevelWait = 16u;     // a small-levels work item gave up waiting for the items it depends on
+constexpr uint32_t kErrorLevelWait = 16u;     // a work item of the batched launch gave up waiting for the items it depends on
 
 // Buffers the encode kernels read and write.
 struct EncodeBuffers
@@ -278,30 +272,6 @@ struct BlockParams
 	BandEntry band[kMaxBands]; // in block index order
 };
 
-// The small levels of a frame in one launch (levels first_level..4): work
-// items are ticket ranges, per level first its transform tiles (all
-// components) and then its quantiser items (four 32x32 blocks each).
-struct SmallLevelParams
-{
-	LevelParams lp[kLevels];          // levels >= first_level are used
-	BlockParams bp;
-	int32_t first_level;
-	int32_t item_first[2 * kLevels + 1]; // item_first[2 * level + kind] .. [+ 1]: kind 0 transform, 1 quantiser
-	int32_t ntiles[kLevels];          // transform items per level
-	int32_t block_first[kLevels];     // first 32x32 block of each level (block index order)
-	int32_t block_count[kLevels];
-};
-
-// The small inverse levels of a decode in one launch (levels last_level down
-// to first_level): ticket ranges of each level's tiles, coarsest level first.
-struct SmallInverseParams
-{
-	LevelParams lp[kLevels];
-	int32_t first_level, last_level;
-	int32_t item_first[kLevels];
-	int32_t ntiles[kLevels];
-};
-
 struct ResolveParams
 {
 	int32_t block_count_32x32, blocks_per_subdivision, subdivision_shift;
@@ -407,14 +377,12 @@ int forward_fused_mode(const LevelParams &p, bool fused_quant);
 void launch_dwt_forward_level(const LevelParams &p, const PlaneInput &in, const EncodeBuffers &buf,
                               const LevelTileMap *maps, bool fused_quant,
                               bool programmatic, cudaStream_t stream);
-// Small levels (forward transform + quantiser) of one frame in one launch.
-SmallLevelParams make_small_level_params(const Geometry &g, int first_level);
-int small_level_items(const SmallLevelParams &sp);
-void launch_dwt_small_levels(const SmallLevelParams &sp, const PlaneInput &in, const EncodeBuffers &buf,
-                             bool programmatic, cudaStream_t stream);
 // Quantise and analyse the first nblocks 32x32 blocks (block index order) from storage.
 void launch_quant_pretransformed(const BlockParams &p, const EncodeBuffers &buf, int nblocks, bool programmatic,
                                  cudaStream_t stream);
+// Largest thread-block cluster the resolve uses on this device (8 or 16);
+// queried once, outside stream capture, before the first launch_resolve.
+int resolve_cluster_max();
 void launch_resolve(const ResolveParams &p, const EncodeBuffers &buf, cudaStream_t stream);
 void launch_pack(const BlockParams &p, const EncodeBuffers &buf, cudaStream_t stream);
 // Dequantise blocks [first, first + count) (block index order).
@@ -425,10 +393,6 @@ void launch_idwt_level(const LevelParams &p, const DecodeInput &in, const PlaneO
                        cudaStream_t stream);
 void launch_pyramid_io(const BlockParams &p, float *canonical, float *coef32, __half *coef16, bool to_canonical,
                        cudaStream_t stream);
-// Small inverse levels (coarsest first) of one decode in one launch; `in.state` must be set.
-SmallInverseParams make_small_inverse_params(const Geometry &g, int first_level);
-void launch_idwt_small_levels(const SmallInverseParams &sp, const DecodeInput &in, const PlaneOutput &out,
-                              bool programmatic, cudaStream_t stream);
 
 // Device-side packet assembly (pw_packets.cu). The first four fields of
 // PacketStatus are the public pyrowave_cuda_packet_status.

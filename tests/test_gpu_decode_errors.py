@@ -7,9 +7,9 @@ the decode as failed. The failure is injected on the host
 completed load is then handled as a timed-out one, so the report path runs
 without stalling or faulting the GPU. Every decode entry point must return an
 error for such a frame, and a decoder built without the injection must not.
-The frame is 1080p: its two finest inverse levels run the 256-thread CTAs
-that load interior tiles this way (the coarser levels load without the
-accelerator, as does the batched form's persistent launch).
+The frame is 1080p: its inverse levels have interior tiles, loaded this way
+(the batched form's persistent launch loads every tile without the
+accelerator, so its test runs the batch as one launch per stage).
 """
 import os
 
