@@ -367,6 +367,39 @@ __device__ __forceinline__ void dwt_forward_body(DwtShared &sh, const LevelParam
 		res_h = al_h = p.P.height;
 	}
 
+	// Tile load. A tile whose 72x72 window lies inside the source maps every
+	// sample to itself: an FP32 level above 0 with a tensor map is one TMA box
+	// (barrier and map made ready before the dependency wait); otherwise whole
+	// rows are read with vector loads, all in flight at once. Edge tiles go
+	// through the mirrored index tables in batches of independent loads.
+	const int x0 = tx * 64 - 4, y0 = ty * 64 - 4;
+	const bool interior = x0 >= 0 && y0 >= 0 && x0 + kTileIn <= res_w && y0 + kTileIn <= res_h;
+	const bool use_tma = !from_plane && interior && maps && ((maps->valid >> comp) & 1u) && !p.P.fp16;
+	const CUtensorMap *tmap = use_tma ? &maps->map : nullptr;
+	constexpr int kVecPerRow = kTileIn / 4;     // 18 vectors of 4 samples
+	constexpr int kVecs = kVecPerRow * kTileIn; // 1296
+	constexpr int kVecIters = (kVecs + kThreads - 1) / kThreads;
+	const uint8_t *src = comp == 0 ? in.data[0] : (comp == 1 ? in.data[1] : in.data[2]);
+	const int pitch = comp == 0 ? in.pitch[0] : (comp == 1 ? in.pitch[1] : in.pitch[2]);
+	const int xs = comp == 0 ? in.xstride[0] : (comp == 1 ? in.xstride[1] : in.xstride[2]);
+	const bool vec_ok = from_plane && interior && xs == 1 && !in.sample16 &&
+	                    ((reinterpret_cast<uintptr_t>(src) | uintptr_t(pitch)) & 3u) == 0;
+	// An interior tile of an 8-bit input plane is read first, before the index
+	// tables and before the dependency wait: the planes are complete before the
+	// frame's first kernel, so the load latency overlaps the set-up (and, at
+	// level 1, the end of level 0).
+	uint32_t pv[kVecIters];
+	if (vec_ok)
+	{
+#pragma unroll
+		for (int u = 0; u < kVecIters; u++)
+		{
+			const int k = threadIdx.x + u * kThreads;
+			const int i = k / kVecPerRow, j = k - i * kVecPerRow;
+			pv[u] = k < kVecs ? __ldg(reinterpret_cast<const uint32_t *>(src + size_t(y0 + i) * pitch + x0) + j) : 0u;
+		}
+	}
+
 	for (int k = threadIdx.x; k < 2 * kTileIn; k += kThreads)
 	{
 		if (k < kTileIn)
@@ -380,15 +413,6 @@ __device__ __forceinline__ void dwt_forward_body(DwtShared &sh, const LevelParam
 			const float f = unorm8_centered(uint32_t(u));
 			sh.unorm[u] = L.stage16 ? round_to_half(f) : f;
 		}
-	// Tile load. A tile whose 72x72 window lies inside the source maps every
-	// sample to itself: an FP32 level above 0 with a tensor map is one TMA box
-	// (barrier and map made ready before the dependency wait); otherwise whole
-	// rows are read with vector loads, all in flight at once. Edge tiles go
-	// through the mirrored index tables in batches of independent loads.
-	const int x0 = tx * 64 - 4, y0 = ty * 64 - 4;
-	const bool interior = x0 >= 0 && y0 >= 0 && x0 + kTileIn <= res_w && y0 + kTileIn <= res_h;
-	const bool use_tma = !from_plane && interior && maps && ((maps->valid >> comp) & 1u) && !p.P.fp16;
-	const CUtensorMap *tmap = use_tma ? &maps->map : nullptr;
 	if (use_tma && threadIdx.x == 0)
 	{
 		mbarrier_init(&sh.tile_bar, 1);
@@ -396,16 +420,8 @@ __device__ __forceinline__ void dwt_forward_body(DwtShared &sh, const LevelParam
 	}
 	__syncthreads();
 	pdl_wait();
-	constexpr int kVecPerRow = kTileIn / 4;     // 18 vectors of 4 samples
-	constexpr int kVecs = kVecPerRow * kTileIn; // 1296
-	constexpr int kVecIters = (kVecs + kThreads - 1) / kThreads;
 	if (from_plane)
 	{
-		const uint8_t *src = comp == 0 ? in.data[0] : (comp == 1 ? in.data[1] : in.data[2]);
-		const int pitch = comp == 0 ? in.pitch[0] : (comp == 1 ? in.pitch[1] : in.pitch[2]);
-		const int xs = comp == 0 ? in.xstride[0] : (comp == 1 ? in.xstride[1] : in.xstride[2]);
-		const bool vec_ok = interior && xs == 1 && !in.sample16 &&
-		                    ((reinterpret_cast<uintptr_t>(src) | uintptr_t(pitch)) & 3u) == 0;
 		if (in.sample16)
 		{
 			// 16-bit samples (R16_UNORM): u / 65535 - 0.5, gathered through the index tables.
@@ -437,14 +453,6 @@ __device__ __forceinline__ void dwt_forward_body(DwtShared &sh, const LevelParam
 		}
 		else if (vec_ok)
 		{
-			uint32_t v[kVecIters];
-#pragma unroll
-			for (int u = 0; u < kVecIters; u++)
-			{
-				const int k = threadIdx.x + u * kThreads;
-				const int i = k / kVecPerRow, j = k - i * kVecPerRow;
-				v[u] = k < kVecs ? __ldg(reinterpret_cast<const uint32_t *>(src + size_t(y0 + i) * pitch + x0) + j) : 0u;
-			}
 #pragma unroll
 			for (int u = 0; u < kVecIters; u++)
 			{
@@ -454,7 +462,7 @@ __device__ __forceinline__ void dwt_forward_body(DwtShared &sh, const LevelParam
 					const int i = k / kVecPerRow, j = k - i * kVecPerRow;
 #pragma unroll
 					for (int b = 0; b < 4; b++)
-						sh.in[i][4 * j + b] = sh.unorm[(v[u] >> (8 * b)) & 0xffu];
+						sh.in[i][4 * j + b] = sh.unorm[(pv[u] >> (8 * b)) & 0xffu];
 				}
 			}
 		}
@@ -774,13 +782,16 @@ __device__ __forceinline__ void quant_blocks_body(const BlockParams &p, const En
 	quant_analyze_block<S>(&tile[grp][0][0], kBandPitch, active, t, q[grp], L, B, p.subdivision_shift, bx, by, buf);
 }
 
+// One 32x32 block per CTA: the launch follows the last small-level transform
+// on the critical path, and one block per CTA is the shortest CTA lifetime
+// (the blocks of a frame's small levels fit one wave).
 template <int S>
-__global__ void __launch_bounds__(256 * S) quant_pretransformed_kernel(const BlockParams p, const EncodeBuffers buf,
+__global__ void __launch_bounds__(128 * S) quant_pretransformed_kernel(const BlockParams p, const EncodeBuffers buf,
                                                                        const int nblocks)
 {
-	__shared__ float tile[2][32][kBandPitch];
-	__shared__ QuantGroupShared q[2];
-	quant_blocks_body<S, 2>(p, buf, 0, nblocks, int(blockIdx.x), tile, q);
+	__shared__ float tile[1][32][kBandPitch];
+	__shared__ QuantGroupShared q[1];
+	quant_blocks_body<S, 1>(p, buf, 0, nblocks, int(blockIdx.x), tile, q);
 }
 
 // Batched form: one CTA per pair of blocks among each frame's small-level blocks.
@@ -1900,7 +1911,7 @@ void launch_dwt_forward_level(const LevelParams &p, const PlaneInput &in, const 
 void launch_quant_pretransformed(const BlockParams &p, const EncodeBuffers &buf, int nblocks, bool programmatic,
                                  cudaStream_t stream)
 {
-	LaunchConfig lc(dim3((nblocks + 1) / 2), dim3(512), stream, programmatic);
+	LaunchConfig lc(dim3(nblocks), dim3(256), stream, programmatic);
 	cudaLaunchKernelEx(&lc.cfg, quant_pretransformed_kernel<2>, p, buf, nblocks);
 }
 
