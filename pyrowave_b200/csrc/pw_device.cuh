@@ -179,6 +179,52 @@ __device__ __forceinline__ void st_release_u64(unsigned long long *p, unsigned l
 	asm volatile("st.release.gpu.global.u64 [%0], %1;" ::"l"(p), "l"(v) : "memory");
 }
 
+// Packed pairs of FP32 values (sm_100 f32x2 arithmetic): each lane of the pair
+// is rounded exactly as the scalar operation of the same name rounds it, so a
+// computation written on pairs gives the scalar results bit for bit in half
+// the instructions.
+typedef unsigned long long f32x2;
+__device__ __forceinline__ f32x2 f2_pack(float lo, float hi)
+{
+	f32x2 r;
+	asm("mov.b64 %0, {%1, %2};" : "=l"(r) : "f"(lo), "f"(hi));
+	return r;
+}
+__device__ __forceinline__ void f2_unpack(f32x2 v, float &lo, float &hi)
+{
+	asm("mov.b64 {%0, %1}, %2;" : "=f"(lo), "=f"(hi) : "l"(v));
+}
+__device__ __forceinline__ f32x2 f2_add_rz(f32x2 a, f32x2 b)
+{
+	f32x2 r;
+	asm("add.rz.f32x2 %0, %1, %2;" : "=l"(r) : "l"(a), "l"(b));
+	return r;
+}
+__device__ __forceinline__ f32x2 f2_add_rn(f32x2 a, f32x2 b)
+{
+	f32x2 r;
+	asm("add.rn.f32x2 %0, %1, %2;" : "=l"(r) : "l"(a), "l"(b));
+	return r;
+}
+__device__ __forceinline__ f32x2 f2_sub_rn(f32x2 a, f32x2 b)
+{
+	f32x2 r;
+	asm("sub.rn.f32x2 %0, %1, %2;" : "=l"(r) : "l"(a), "l"(b));
+	return r;
+}
+__device__ __forceinline__ f32x2 f2_mul_rn(f32x2 a, f32x2 b)
+{
+	f32x2 r;
+	asm("mul.rn.f32x2 %0, %1, %2;" : "=l"(r) : "l"(a), "l"(b));
+	return r;
+}
+__device__ __forceinline__ f32x2 f2_fma_rn(f32x2 a, f32x2 b, f32x2 c)
+{
+	f32x2 r;
+	asm("fma.rn.f32x2 %0, %1, %2, %3;" : "=l"(r) : "l"(a), "l"(b), "l"(c));
+	return r;
+}
+
 // Thread-block clusters: this CTA's rank, the cluster's CTA count, hardware
 // cluster barriers (every thread of every CTA of the cluster takes part) and
 // 64-bit stores into another CTA's shared memory (distributed shared memory).

@@ -155,6 +155,13 @@ __device__ __forceinline__ void quant_analyze_block(const float *tile, int tile_
 		d_lo = drop;
 
 	const int warp_msb = __reduce_max_sync(0xffffffffu, max(msb, 0));
+	// Magnitudes as pairs (i, i + 4): the two lanes of a pair accumulate the two
+	// halves of the squared error, e0 over i = 0..3 and e1 over i = 4..7, in the
+	// same order as eight scalar steps would.
+	f32x2 avp[4];
+#pragma unroll
+	for (int j = 0; j < 4; j++)
+		avp[j] = f2_pack(av[j], av[j + 4]);
 	for (int q = 1 + r; q <= warp_msb; q += S)
 	{
 		// compute_square_error + compute_quant_stats at q (wavelet_quant.comp:113-165).
@@ -164,24 +171,27 @@ __device__ __forceinline__ void quant_analyze_block(const float *tile, int tile_
 		// again is exact. The reconstruction R + 2^(q-1) is an exact integer, so
 		// err equals the integer formulation above. With sg = min(R, 1) (1 when
 		// significant), err = (|v| - R) - sg * 2^(q-1): the difference and the
-		// fused multiply-add are exact, so they round to themselves.
+		// fused multiply-add are exact, so they round to themselves. The count
+		// of significant values is a sum of zeros and ones, exact in any order.
 		const float hq = __int_as_float((126 + q) << 23);
 		const float mq = __int_as_float((150 + q) << 23);
-		float nsig_f = 0.0f;
-		float e0 = 0.0f, e1 = 0.0f;
+		const f32x2 mq2 = f2_pack(mq, mq), neg_hq2 = f2_pack(-hq, -hq);
+		f32x2 nsig2 = 0ull, e2 = 0ull;
 #pragma unroll
-		for (int i = 0; i < 8; i++)
+		for (int j = 0; j < 4; j++)
 		{
-			const float R = __fsub_rn(__fadd_rz(av[i], mq), mq);
-			const float sg = fminf(R, 1.0f);
-			nsig_f = __fadd_rn(nsig_f, sg);
-			const float err = __fmaf_rn(-sg, hq, __fsub_rn(av[i], R));
-			if (i < 4)
-				e0 = (i == 0) ? __fmul_rn(err, err) : __fmaf_rn(err, err, e0);
-			else
-				e1 = (i == 4) ? __fmul_rn(err, err) : __fmaf_rn(err, err, e1);
+			const f32x2 R = f2_sub_rn(f2_add_rz(avp[j], mq2), mq2);
+			float r_lo, r_hi;
+			f2_unpack(R, r_lo, r_hi);
+			const f32x2 sg = f2_pack(fminf(r_lo, 1.0f), fminf(r_hi, 1.0f));
+			nsig2 = j == 0 ? sg : f2_add_rn(nsig2, sg);
+			const f32x2 err = f2_fma_rn(sg, neg_hq2, f2_sub_rn(avp[j], R));
+			e2 = j == 0 ? f2_mul_rn(err, err) : f2_fma_rn(err, err, e2);
 		}
-		const int nsig = int(nsig_f);
+		float e0, e1, n_lo, n_hi;
+		f2_unpack(e2, e0, e1);
+		f2_unpack(nsig2, n_lo, n_hi);
+		const int nsig = int(n_lo) + int(n_hi);
 		float se = __fmul_rn(__fmul_rn(__fadd_rn(e0, e1), rdo), iqs);
 		se = __fadd_rn(se, __shfl_xor_sync(0xffffffffu, se, 1));
 		se = __fadd_rn(se, __shfl_xor_sync(0xffffffffu, se, 2));
