@@ -47,6 +47,20 @@ __global__ void __launch_bounds__(kThreads, kMinBlocks) idwt_kernel(const LevelP
 	idwt_body<kThreads>(sh, p, in, out, &maps, int(blockIdx.x), int(blockIdx.y));
 }
 
+// Small levels (fewer tiles than SMs): four 256-thread CTAs per tile, one per
+// stripe of 16 output rows (blockIdx.x = tile * 4 + stripe).
+constexpr int kIdwtStripes = 4;
+// Same parameters as idwt_kernel (graph nodes are updated with one argument
+// list); the stripes load with plain vector loads, not tensor maps.
+__global__ void __launch_bounds__(256, 4) idwt_stripes_kernel(const LevelParams p, const DecodeInput in, const PlaneOutput out,
+                                                              const __grid_constant__ LevelTileMap maps)
+{
+	(void)maps;
+	__shared__ IdwtShared sh;
+	idwt_body<256, kIdwtStripes>(sh, p, in, out, nullptr, int(blockIdx.x) / kIdwtStripes, int(blockIdx.y),
+	                             int(blockIdx.x) % kIdwtStripes);
+}
+
 // Batched form: one CTA per (frame, component, tile) of this level.
 template <int kThreads, int kMinBlocks = kIdwtMinBlocks<kThreads>>
 __global__ void __launch_bounds__(kThreads, kMinBlocks) idwt_batch_kernel(const BatchFrame *frames, const BatchFrameIO *io,
@@ -113,8 +127,8 @@ void launch_idwt_level(const LevelParams &p, const DecodeInput &in, const PlaneO
 		m = *maps;
 	if (int(grid.x * grid.y) < kSmallLevelTiles)
 	{
-		LaunchConfig lc(grid, dim3(1024), stream, programmatic);
-		cudaLaunchKernelEx(&lc.cfg, idwt_kernel<1024>, p, in, out, m);
+		LaunchConfig lc(dim3(grid.x * kIdwtStripes, grid.y), dim3(256), stream, programmatic);
+		cudaLaunchKernelEx(&lc.cfg, idwt_stripes_kernel, p, in, out, m);
 	}
 	else if (int(grid.x * grid.y) < kIdwtManyTiles)
 	{

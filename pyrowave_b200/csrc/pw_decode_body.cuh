@@ -312,17 +312,23 @@ struct IdwtShared
 };
 
 // One inverse level for a 64x64 output tile (32x32 band tile) of one component.
-// Large levels run 256-thread CTAs, several per SM; small levels (fewer tiles
-// than SMs) run 1024-thread CTAs whose lifting items cover half as many
-// outputs, shortening every serial phase.
-template <int kThreads>
+// Large levels run 256-thread CTAs, several per SM; the batched form's small
+// levels run 1024-thread CTAs whose lifting items cover half as many outputs.
+// With kStripes = 4 a CTA computes one stripe of 16 output rows of the tile
+// (small levels: four times the CTAs, each with a quarter of the lifting and
+// a third of the loads), with the same arithmetic per output.
+template <int kThreads, int kStripes = 1>
 __device__ __forceinline__ void idwt_body(IdwtShared &sh, const LevelParams &p, const DecodeInput &in,
                                           const PlaneOutput &out, const LevelTileMap *maps, const int tile,
-                                          const int comp_index)
+                                          const int comp_index, const int stripe = 0)
 {
 	constexpr int kOut = kThreads >= 1024 ? 8 : 16; // outputs per lifting item
 	constexpr int kSegs = 64 / kOut;
 	constexpr int kWin = kOut + 8;
+	static_assert(kStripes == 1 || (kStripes == kSegs && kOut == 16), "a stripe is one lifting segment of 16 rows");
+	// Band tile rows this CTA reads: all 36, or the 12 that the stripe's segment spans.
+	constexpr int kRows = kStripes == 1 ? kBandTile : kWin / 2;
+	const int row0 = kStripes == 1 ? 0 : stripe * (kOut / 2);
 	pdl_trigger();
 	const int level = p.level;
 	const int comp = (level == 0 && !p.chroma444) ? 0 : comp_index;
@@ -354,7 +360,8 @@ __device__ __forceinline__ void idwt_body(IdwtShared &sh, const LevelParams &p, 
 	// row, all in flight at once. Edge tiles use the mirrored index tables.
 	const int bx0 = tx * 32 - 2, by0 = ty * 32 - 2;
 	const bool interior = bx0 - 2 >= 0 && by0 >= 0 && bx0 + 38 <= nx && by0 + kBandTile <= ny;
-	const bool use_tma = kThreads == 256 && interior && maps && ((maps->valid >> comp) & 1u) && !f16 && !L.stage16;
+	const bool use_tma = kThreads == 256 && kStripes == 1 && interior && maps && ((maps->valid >> comp) & 1u) && !f16 &&
+	                     !L.stage16;
 	if (use_tma && threadIdx.x == 0)
 	{
 		mbarrier_init(&sh.tile_bar, 1);
@@ -386,16 +393,16 @@ __device__ __forceinline__ void idwt_body(IdwtShared &sh, const LevelParams &p, 
 	else if (interior)
 	{
 		constexpr int kVecPerRow = 10;
-		constexpr int kVecs = 4 * kBandTile * kVecPerRow; // 1440
+		constexpr int kVecs = 4 * kRows * kVecPerRow; // 1440 for a whole tile
 		constexpr int kIters = (kVecs + kThreads - 1) / kThreads;
 		float4 v[kIters];
 #pragma unroll
 		for (int u = 0; u < kIters; u++)
 		{
 			const int k = threadIdx.x + u * kThreads;
-			const int b = k / (kBandTile * kVecPerRow);
-			const int r = k - b * kBandTile * kVecPerRow;
-			const int i = r / kVecPerRow, j = r - i * kVecPerRow;
+			const int b = k / (kRows * kVecPerRow);
+			const int r = k - b * kRows * kVecPerRow;
+			const int i = row0 + r / kVecPerRow, j = r % kVecPerRow;
 			if (k >= kVecs)
 			{
 				v[u] = make_float4(0.f, 0.f, 0.f, 0.f);
@@ -419,9 +426,9 @@ __device__ __forceinline__ void idwt_body(IdwtShared &sh, const LevelParams &p, 
 			const int k = threadIdx.x + u * kThreads;
 			if (k >= kVecs)
 				continue;
-			const int b = k / (kBandTile * kVecPerRow);
-			const int r = k - b * kBandTile * kVecPerRow;
-			const int i = r / kVecPerRow, j = r - i * kVecPerRow;
+			const int b = k / (kRows * kVecPerRow);
+			const int r = k - b * kRows * kVecPerRow;
+			const int i = row0 + r / kVecPerRow, j = r % kVecPerRow;
 			float4 f = v[u];
 			if (L.stage16)
 			{
@@ -435,7 +442,7 @@ __device__ __forceinline__ void idwt_body(IdwtShared &sh, const LevelParams &p, 
 	}
 	else
 	{
-		constexpr int kN = 4 * kBandTile * kBandTile;
+		constexpr int kN = 4 * kRows * kBandTile;
 		constexpr int kIdwtGen = (kN + kThreads - 1) / kThreads; // every load in flight at once
 		for (int base = threadIdx.x; base < kN; base += kThreads * kIdwtGen)
 		{
@@ -444,9 +451,9 @@ __device__ __forceinline__ void idwt_body(IdwtShared &sh, const LevelParams &p, 
 			for (int u = 0; u < kIdwtGen; u++)
 			{
 				const int k = base + u * kThreads;
-				const int b = k / (kBandTile * kBandTile);
-				const int r = k - b * kBandTile * kBandTile;
-				const int i = r / kBandTile, j = r - i * kBandTile;
+				const int b = k / (kRows * kBandTile);
+				const int r = k - b * kRows * kBandTile;
+				const int i = row0 + r / kBandTile, j = r % kBandTile;
 				const int yy = (b >> 1) ? sh.yh[i] : sh.yl[i];
 				const int xx = (b & 1) ? sh.xh[j] : sh.xl[j];
 				const int64_t bo = b == 0 ? o0 : (b == 1 ? o1 : (b == 2 ? o2 : o3));
@@ -460,9 +467,9 @@ __device__ __forceinline__ void idwt_body(IdwtShared &sh, const LevelParams &p, 
 				const int k = base + u * kThreads;
 				if (k < kN)
 				{
-					const int b = k / (kBandTile * kBandTile);
-					const int r = k - b * kBandTile * kBandTile;
-					const int i = r / kBandTile, j = r - i * kBandTile;
+					const int b = k / (kRows * kBandTile);
+					const int r = k - b * kRows * kBandTile;
+					const int i = row0 + r / kBandTile, j = r % kBandTile;
 					sh.band[b][i][j + kBandCol0] = L.stage16 ? round_to_half(v[u]) : v[u];
 				}
 			}
@@ -470,12 +477,14 @@ __device__ __forceinline__ void idwt_body(IdwtShared &sh, const LevelParams &p, 
 	}
 	__syncthreads();
 
-	// Vertical lifting: 36 band columns x {horizontal low: LL/LH, horizontal high: HL/HH} x kSegs segments.
-	for (int item = threadIdx.x; item < kBandTile * 2 * kSegs; item += kThreads)
+	// Vertical lifting: 36 band columns x {horizontal low: LL/LH, horizontal high: HL/HH} x kSegs segments
+	// (the stripe's segment only).
+	constexpr int kVSegs = kStripes == 1 ? kSegs : 1;
+	for (int item = threadIdx.x; item < kBandTile * 2 * kVSegs; item += kThreads)
 	{
 		const int col = item % kBandTile;
 		const int which = (item / kBandTile) & 1;
-		const int seg = item / (2 * kBandTile);
+		const int seg = kStripes == 1 ? item / (2 * kBandTile) : stripe;
 		const int b_low = which ? 1 : 0, b_high = which ? 3 : 2;
 		float e[kWin];
 #pragma unroll
@@ -493,10 +502,11 @@ __device__ __forceinline__ void idwt_body(IdwtShared &sh, const LevelParams &p, 
 	}
 	__syncthreads();
 
-	// Horizontal lifting: 64 output rows x kSegs segments of kOut outputs.
-	for (int item = threadIdx.x; item < 64 * kSegs; item += kThreads)
+	// Horizontal lifting: 64 output rows (the stripe's 16) x kSegs segments of kOut outputs.
+	constexpr int kHRows = kStripes == 1 ? 64 : kOut;
+	for (int item = threadIdx.x; item < kHRows * kSegs; item += kThreads)
 	{
-		const int row = item & 63, seg = item >> 6;
+		const int row = (kStripes == 1 ? 0 : stripe * kOut) + item % kHRows, seg = item / kHRows;
 		float e[kWin];
 #pragma unroll
 		for (int jj = 0; jj < kWin; jj++)

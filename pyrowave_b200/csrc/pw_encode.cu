@@ -339,7 +339,6 @@ template <int kThreads> struct DwtSplit
 	static constexpr int kQSplit = kThreads >= 1024 ? 2 : 1;    // threads per 4x2 sub-block in the quantiser
 	static constexpr int kGroupThreads = 128 * kQSplit;         // threads per quantised 32x32 block
 	static constexpr int kGroups = kThreads / kGroupThreads;    // 32x32 blocks quantised at once
-	static constexpr int kGen = (kTileIn * kTileIn + kThreads - 1) / kThreads; // edge-tile loads per thread
 	static constexpr int kMinBlocks = kThreads >= 1024 ? 1 : (kThreads >= 384 ? 2 : 4); // CTAs per SM to fit
 };
 
@@ -349,13 +348,21 @@ constexpr int kLargeLevelThreads = 256;
 
 // One forward level for one 32x32 band tile of one component (64x64 input
 // samples): `tile` in row-major tile order, `comp_index` the component among
-// those at this level. Run by every thread of a kThreads-thread CTA.
-template <int kThreads>
+// those at this level. Run by every thread of a kThreads-thread CTA. With
+// kStripes > 1 (transform only) the CTA computes one stripe of 32 / kStripes
+// band rows of the tile, one vertical lifting segment: it loads and lifts
+// horizontally only the input rows that segment spans.
+template <int kThreads, int kStripes = 1>
 __device__ __forceinline__ void dwt_forward_body(DwtShared &sh, const LevelParams &p, const PlaneInput &in,
                                                  const EncodeBuffers &buf, const LevelTileMap *maps, const int fused,
-                                                 const int tile, const int comp_index)
+                                                 const int tile, const int comp_index, const int stripe = 0)
 {
 	using Split = DwtSplit<kThreads>;
+	static_assert(kStripes == 1 || kStripes == Split::kSegs, "a stripe is one vertical lifting segment");
+	// Input rows this CTA loads and lifts horizontally: all 72, or the window of its stripe.
+	constexpr int kRowsIn = kStripes == 1 ? kTileIn : Split::kWin;
+	const int r0 = kStripes == 1 ? 0 : stripe * 2 * Split::kSegPairs;
+	constexpr int kGen = (kRowsIn * kTileIn + kThreads - 1) / kThreads; // gathered loads per thread
 	pdl_trigger();
 	const int level = p.level;
 	const int comp = (level == 0 && !p.chroma444) ? 0 : comp_index;
@@ -384,10 +391,10 @@ __device__ __forceinline__ void dwt_forward_body(DwtShared &sh, const LevelParam
 	// through the mirrored index tables in batches of independent loads.
 	const int x0 = tx * 64 - 4, y0 = ty * 64 - 4;
 	const bool interior = x0 >= 0 && y0 >= 0 && x0 + kTileIn <= res_w && y0 + kTileIn <= res_h;
-	const bool use_tma = !from_plane && interior && maps && ((maps->valid >> comp) & 1u) && !p.P.fp16;
+	const bool use_tma = kStripes == 1 && !from_plane && interior && maps && ((maps->valid >> comp) & 1u) && !p.P.fp16;
 	const CUtensorMap *tmap = use_tma ? &maps->map : nullptr;
 	constexpr int kVecPerRow = kTileIn / 4;     // 18 vectors of 4 samples
-	constexpr int kVecs = kVecPerRow * kTileIn; // 1296
+	constexpr int kVecs = kVecPerRow * kRowsIn; // 1296 for a whole tile
 	constexpr int kVecIters = (kVecs + kThreads - 1) / kThreads;
 	const uint8_t *src = comp == 0 ? in.data[0] : (comp == 1 ? in.data[1] : in.data[2]);
 	const int pitch = comp == 0 ? in.pitch[0] : (comp == 1 ? in.pitch[1] : in.pitch[2]);
@@ -405,7 +412,7 @@ __device__ __forceinline__ void dwt_forward_body(DwtShared &sh, const LevelParam
 		for (int u = 0; u < kVecIters; u++)
 		{
 			const int k = threadIdx.x + u * kThreads;
-			const int i = k / kVecPerRow, j = k - i * kVecPerRow;
+			const int ii = k / kVecPerRow, i = r0 + ii, j = k - ii * kVecPerRow;
 			pv[u] = k < kVecs ? __ldg(reinterpret_cast<const uint32_t *>(src + size_t(y0 + i) * pitch + x0) + j) : 0u;
 		}
 	}
@@ -435,26 +442,26 @@ __device__ __forceinline__ void dwt_forward_body(DwtShared &sh, const LevelParam
 		if (in.sample16)
 		{
 			// 16-bit samples (R16_UNORM): u / 65535 - 0.5, gathered through the index tables.
-			for (int base = threadIdx.x; base < kTileIn * kTileIn; base += kThreads * Split::kGen)
+			for (int base = threadIdx.x; base < kRowsIn * kTileIn; base += kThreads * kGen)
 			{
-				uint32_t v[Split::kGen];
+				uint32_t v[kGen];
 #pragma unroll
-				for (int u = 0; u < Split::kGen; u++)
+				for (int u = 0; u < kGen; u++)
 				{
 					const int k = base + u * kThreads;
-					const int i = k / kTileIn, j = k - i * kTileIn;
-					v[u] = k < kTileIn * kTileIn
+					const int ii = k / kTileIn, i = r0 + ii, j = k - ii * kTileIn;
+					v[u] = k < kRowsIn * kTileIn
 					           ? uint32_t(*reinterpret_cast<const uint16_t *>(src + size_t(sh.yidx[i]) * pitch +
 					                                                          size_t(sh.xidx[j]) * xs))
 					           : 0u;
 				}
 #pragma unroll
-				for (int u = 0; u < Split::kGen; u++)
+				for (int u = 0; u < kGen; u++)
 				{
 					const int k = base + u * kThreads;
-					if (k < kTileIn * kTileIn)
+					if (k < kRowsIn * kTileIn)
 					{
-						const int i = k / kTileIn, j = k - i * kTileIn;
+						const int ii = k / kTileIn, i = r0 + ii, j = k - ii * kTileIn;
 						const float f = __fsub_rn(__fdiv_rn(float(v[u]), 65535.0f), 0.5f);
 						sh.in[i][j] = L.stage16 ? round_to_half(f) : f;
 					}
@@ -469,7 +476,7 @@ __device__ __forceinline__ void dwt_forward_body(DwtShared &sh, const LevelParam
 				const int k = threadIdx.x + u * kThreads;
 				if (k < kVecs)
 				{
-					const int i = k / kVecPerRow, j = k - i * kVecPerRow;
+					const int ii = k / kVecPerRow, i = r0 + ii, j = k - ii * kVecPerRow;
 #pragma unroll
 					for (int b = 0; b < 4; b++)
 						sh.in[i][4 * j + b] = sh.unorm[(pv[u] >> (8 * b)) & 0xffu];
@@ -478,23 +485,23 @@ __device__ __forceinline__ void dwt_forward_body(DwtShared &sh, const LevelParam
 		}
 		else
 		{
-			for (int base = threadIdx.x; base < kTileIn * kTileIn; base += kThreads * Split::kGen)
+			for (int base = threadIdx.x; base < kRowsIn * kTileIn; base += kThreads * kGen)
 			{
-				uint32_t v[Split::kGen];
+				uint32_t v[kGen];
 #pragma unroll
-				for (int u = 0; u < Split::kGen; u++)
+				for (int u = 0; u < kGen; u++)
 				{
 					const int k = base + u * kThreads;
-					const int i = k / kTileIn, j = k - i * kTileIn;
-					v[u] = k < kTileIn * kTileIn ? src[size_t(sh.yidx[i]) * pitch + size_t(sh.xidx[j]) * xs] : 0u;
+					const int ii = k / kTileIn, i = r0 + ii, j = k - ii * kTileIn;
+					v[u] = k < kRowsIn * kTileIn ? src[size_t(sh.yidx[i]) * pitch + size_t(sh.xidx[j]) * xs] : 0u;
 				}
 #pragma unroll
-				for (int u = 0; u < Split::kGen; u++)
+				for (int u = 0; u < kGen; u++)
 				{
 					const int k = base + u * kThreads;
-					if (k < kTileIn * kTileIn)
+					if (k < kRowsIn * kTileIn)
 					{
-						const int i = k / kTileIn, j = k - i * kTileIn;
+						const int ii = k / kTileIn, i = r0 + ii, j = k - ii * kTileIn;
 						sh.in[i][j] = sh.unorm[v[u] & 0xffu];
 					}
 				}
@@ -531,7 +538,7 @@ __device__ __forceinline__ void dwt_forward_body(DwtShared &sh, const LevelParam
 			for (int u = 0; u < kVecIters; u++)
 			{
 				const int k = threadIdx.x + u * kThreads;
-				const int i = k / kVecPerRow, j = k - i * kVecPerRow;
+				const int ii = k / kVecPerRow, i = r0 + ii, j = k - ii * kVecPerRow;
 				const int64_t idx = ll + int64_t(y0 + i) * P.pitch + x0 + 4 * j;
 				if (k >= kVecs)
 					v[u] = make_float4(0.f, 0.f, 0.f, 0.f);
@@ -551,32 +558,32 @@ __device__ __forceinline__ void dwt_forward_body(DwtShared &sh, const LevelParam
 				const int k = threadIdx.x + u * kThreads;
 				if (k < kVecs)
 				{
-					const int i = k / kVecPerRow, j = k - i * kVecPerRow;
+					const int ii = k / kVecPerRow, i = r0 + ii, j = k - ii * kVecPerRow;
 					*reinterpret_cast<float4 *>(&sh.in[i][4 * j]) = v[u];
 				}
 			}
 		}
 		else
 		{
-			for (int base = threadIdx.x; base < kTileIn * kTileIn; base += kThreads * Split::kGen)
+			for (int base = threadIdx.x; base < kRowsIn * kTileIn; base += kThreads * kGen)
 			{
-				float v[Split::kGen];
+				float v[kGen];
 #pragma unroll
-				for (int u = 0; u < Split::kGen; u++)
+				for (int u = 0; u < kGen; u++)
 				{
 					const int k = base + u * kThreads;
-					const int i = k / kTileIn, j = k - i * kTileIn;
-					v[u] = k < kTileIn * kTileIn
+					const int ii = k / kTileIn, i = r0 + ii, j = k - ii * kTileIn;
+					v[u] = k < kRowsIn * kTileIn
 					           ? load_coef(buf.coef32, buf.coef16, f16, ll + int64_t(sh.yidx[i]) * P.pitch + sh.xidx[j])
 					           : 0.0f;
 				}
 #pragma unroll
-				for (int u = 0; u < Split::kGen; u++)
+				for (int u = 0; u < kGen; u++)
 				{
 					const int k = base + u * kThreads;
-					if (k < kTileIn * kTileIn)
+					if (k < kRowsIn * kTileIn)
 					{
-						const int i = k / kTileIn, j = k - i * kTileIn;
+						const int ii = k / kTileIn, i = r0 + ii, j = k - ii * kTileIn;
 						sh.in[i][j] = v[u];
 					}
 				}
@@ -585,11 +592,11 @@ __device__ __forceinline__ void dwt_forward_body(DwtShared &sh, const LevelParam
 	}
 	__syncthreads();
 
-	// Horizontal lifting: 72 rows x kSegs segments of kSegPairs output pairs.
+	// Horizontal lifting: 72 rows (the stripe's 24) x kSegs segments of kSegPairs output pairs.
 	constexpr int kSegPairs = Split::kSegPairs, kWin = Split::kWin;
-	for (int item = threadIdx.x; item < kTileIn * Split::kSegs; item += kThreads)
+	for (int item = threadIdx.x; item < kRowsIn * Split::kSegs; item += kThreads)
 	{
-		const int row = item % kTileIn, seg = item / kTileIn;
+		const int row = r0 + item % kRowsIn, seg = item / kRowsIn;
 		float e[kWin];
 #pragma unroll
 		for (int j = 0; j < kWin; j += 4)
@@ -619,9 +626,10 @@ __device__ __forceinline__ void dwt_forward_body(DwtShared &sh, const LevelParam
 	// Vertical lifting: 64 columns x kSegs segments. Columns 0..31 hold the
 	// horizontal low band (-> LL, LH), 32..63 the high band (-> HL, HH).
 	float(*bands)[32][kBandPitch] = reinterpret_cast<float(*)[32][kBandPitch]>(&sh.in[0][0]);
-	for (int item = threadIdx.x; item < 64 * Split::kSegs; item += kThreads)
+	constexpr int kVSegs = kStripes == 1 ? Split::kSegs : 1;
+	for (int item = threadIdx.x; item < 64 * kVSegs; item += kThreads)
 	{
-		const int col = item & 63, seg = item >> 6;
+		const int col = item & 63, seg = kStripes == 1 ? item >> 6 : stripe;
 		float e[kWin];
 #pragma unroll
 		for (int j = 0; j < kWin; j++)
@@ -650,10 +658,11 @@ __device__ __forceinline__ void dwt_forward_body(DwtShared &sh, const LevelParam
 	}
 	__syncthreads();
 
-	// Store all four bands (LL feeds the next level): 4 x 32 rows x 8 vectors.
-	for (int item = threadIdx.x; item < 4 * 256; item += kThreads)
+	// Store all four bands (LL feeds the next level): 4 x 32 rows (the stripe's rows) x 8 vectors.
+	constexpr int kBandRows = 32 / kStripes;
+	for (int item = threadIdx.x; item < 4 * kBandRows * 8; item += kThreads)
 	{
-		const int b = item >> 8, r = (item >> 3) & 31, c4 = (item & 7) * 4;
+		const int b = item / (kBandRows * 8), r = stripe * kBandRows + (item >> 3) % kBandRows, c4 = (item & 7) * 4;
 		const int64_t idx = p.band[comp][b].offset + int64_t(ty * 32 + r) * L.pitch + tx * 32 + c4;
 		if (L.fp16)
 		{
@@ -671,7 +680,7 @@ __device__ __forceinline__ void dwt_forward_body(DwtShared &sh, const LevelParam
 		}
 	}
 
-	if (!fused)
+	if (kStripes > 1 || !fused)
 		return;
 
 	// Quantise the transmitted bands of this tile: HL, LH, HH (+ LL at the last
@@ -712,6 +721,22 @@ __global__ void __launch_bounds__(kThreads, DwtSplit<kThreads>::kMinBlocks)
 {
 	__shared__ DwtShared sh;
 	dwt_forward_body<kThreads>(sh, p, in, buf, &maps, fused, int(blockIdx.x), int(blockIdx.y));
+}
+
+// Small transform-only levels (fewer tiles than SMs): four 256-thread CTAs per
+// tile, one per stripe of 8 band rows (blockIdx.x = tile * 4 + stripe). Same
+// parameters as dwt_forward_kernel (graph nodes are updated with one argument
+// list); the stripes load with plain vector loads, not tensor maps.
+constexpr int kDwtStripes = DwtSplit<kLargeLevelThreads>::kSegs;
+__global__ void __launch_bounds__(kLargeLevelThreads, 4)
+    dwt_stripes_kernel(const LevelParams p, const PlaneInput in, const EncodeBuffers buf, const int fused,
+                       const __grid_constant__ LevelTileMap maps)
+{
+	(void)fused;
+	(void)maps;
+	__shared__ DwtShared sh;
+	dwt_forward_body<kLargeLevelThreads, kDwtStripes>(sh, p, in, buf, nullptr, 0, int(blockIdx.x) / kDwtStripes,
+	                                                  int(blockIdx.y), int(blockIdx.x) % kDwtStripes);
 }
 
 // Batched form: one CTA per (frame, component, tile) of this level.
@@ -1133,141 +1158,6 @@ template <int kThreads>
 __global__ void __launch_bounds__(kThreads) resolve_kernel(const ResolveParams p, const EncodeBuffers buf)
 {
 	resolve_body(p, buf, int(blockIdx.x), int(gridDim.x));
-}
-
-// The same resolve in one 1024-thread CTA, for frames of at most
-// kSingleResolveRows * 1024 blocks: every thread loads the RD rows of its run
-// of consecutive blocks once, into registers, together with two histogram
-// slots; the histogram scan, x*, the cut and the block offsets are then four
-// block-wide scans with no global round trip between them and no wait on
-// other CTAs. Results are those of resolve_body.
-constexpr int kSingleResolveRows = 4;
-constexpr int kSingleResolveThreads = 1024;
-
-__global__ void __launch_bounds__(kSingleResolveThreads, 1)
-    resolve_single_kernel(const ResolveParams p, const EncodeBuffers buf)
-{
-	__shared__ uint32_t scan[kHistSize];
-	__shared__ uint32_t warp_sums[32];
-	__shared__ unsigned long long warp_sums64[32];
-	__shared__ int s_xstar;
-	__shared__ uint32_t s_cut;
-	RateControlState *rc = buf.rc;
-	const int t = threadIdx.x;
-	const int n = p.block_count_32x32;
-	const int per = (n + kSingleResolveThreads - 1) / kSingleResolveThreads; // at most kSingleResolveRows
-	const int b0 = min(t * per, n), b1 = min(b0 + per, n);
-	// Every quantiser has finished once the wait returns; the packer is released only then.
-	pdl_wait();
-	pdl_trigger();
-
-	RawRD rows[kSingleResolveRows];
-#pragma unroll
-	for (int i = 0; i < kSingleResolveRows; i++)
-		if (b0 + i < b1)
-			rows[i] = load_raw_rd(buf, b0 + i);
-	static_assert(kHistSize == 2 * kSingleResolveThreads, "two histogram slots per thread");
-	const uint32_t h0 = __ldcg(&rc->histogram[2 * t]), h1 = __ldcg(&rc->histogram[2 * t + 1]);
-	const uint32_t consumed = __ldcg(&rc->consumed);
-	if (t == 0)
-	{
-		s_xstar = -1;
-		s_cut = 0xffffffffu;
-	}
-	uint32_t total;
-	const uint32_t run = block_exclusive_scan(h0 + h1, warp_sums, total);
-	scan[2 * t] = run + h0;
-	scan[2 * t + 1] = run + h0 + h1;
-	__syncthreads();
-
-	const int64_t need = int64_t(consumed) - int64_t(p.target_words);
-	if (need > 0)
-	{
-		for (int x = 2 * t; x < 2 * t + 2; x++)
-			if (int64_t(scan[x]) >= need && (x == 0 || int64_t(scan[x - 1]) < need))
-				s_xstar = x;
-	}
-	__syncthreads();
-	const int xstar = s_xstar;
-
-	if (xstar >= 0)
-	{
-		// The cut: exclusive prefix of the savings at bucket b* over the x*
-		// subdivision's blocks, in block order; the first operation whose
-		// prefix reaches the requirement is not applied, nor any after it.
-		const int start = (xstar & (kSubdivisions - 1)) * p.blocks_per_subdivision;
-		const int end = min(start + p.blocks_per_subdivision, n);
-		const int64_t required = need - (xstar > 0 ? int64_t(scan[xstar - 1]) : 0);
-		const uint32_t bk = uint32_t(xstar >> 4);
-		uint32_t sv[kSingleResolveRows];
-		uint32_t local = 0;
-#pragma unroll
-		for (int i = 0; i < kSingleResolveRows; i++)
-		{
-			const int blk = b0 + i;
-			sv[i] = (blk < b1 && blk >= start && blk < end) ? op_saving_at_bucket(rows[i], bk) : 0u;
-			local += sv[i];
-		}
-		uint32_t tot;
-		uint32_t ex = block_exclusive_scan(local, warp_sums, tot);
-		bool found = false;
-#pragma unroll
-		for (int i = 0; i < kSingleResolveRows; i++)
-		{
-			if (!found && sv[i] != 0 && int64_t(ex) >= required)
-			{
-				atomicMin(&s_cut, uint32_t(b0 + i));
-				found = true;
-			}
-			ex += sv[i];
-		}
-		__syncthreads();
-	}
-	const uint32_t cut = s_cut;
-
-	// Word counts, the block scan of offsets, the per-block decisions.
-	uint32_t w[kSingleResolveRows];
-	int q[kSingleResolveRows];
-	unsigned long long local = 0; // words << 32 | non-empty blocks << 1
-#pragma unroll
-	for (int i = 0; i < kSingleResolveRows; i++)
-	{
-		const int blk = b0 + i;
-		w[i] = 0;
-		q[i] = 0;
-		if (blk < b1)
-		{
-			w[i] = block_words(rows[i], blk, blk >> p.subdivision_shift, xstar, cut, q[i]);
-			local += (uint64_t(w[i]) << 32) | (uint64_t(w[i] != 0 ? 1 : 0) << 1);
-		}
-	}
-	unsigned long long all;
-	unsigned long long pos = block_exclusive_scan(local, warp_sums64, all);
-#pragma unroll
-	for (int i = 0; i < kSingleResolveRows; i++)
-	{
-		const int blk = b0 + i;
-		if (blk < b1)
-		{
-			buf.quant[blk] = q[i];
-			*reinterpret_cast<uint2 *>(buf.block_meta + 2 * size_t(blk)) = make_uint2(uint32_t(pos >> 32), w[i]);
-			pos += uint64_t(w[i]) << 32;
-		}
-	}
-	if (t == 0)
-	{
-		const uint32_t total_words = uint32_t(all >> 32);
-		const uint32_t non_zero = uint32_t(all & 0xffffffffull) >> 1;
-		rc->xstar = xstar;
-		rc->sequence = p.sequence & 7u;
-		rc->total_words = total_words;
-		rc->non_zero_blocks = non_zero;
-		if (2 + uint64_t(total_words) > buf.stream_capacity_words)
-			atomicOr(&rc->error, kErrorStreamCapacity);
-		// Start-of-frame sequence header (bitstream.md:250-265).
-		buf.stream[0] = uint32_t(p.width - 1) | (uint32_t(p.height - 1) << 14) | ((p.sequence & 7u) << 28) | (1u << 31);
-		buf.stream[1] = (non_zero & 0xffffffu) | (uint32_t(p.chroma444 ? 1 : 0) << 26);
-	}
 }
 
 // The same resolve on one thread-block cluster of C CTAs (C a power of two up
@@ -1906,7 +1796,12 @@ void launch_dwt_forward_level(const LevelParams &p, const PlaneInput &in, const 
 	LevelTileMap m = {};
 	if (maps)
 		m = *maps;
-	if (int(grid.x * grid.y) < kSmallLevelTiles)
+	if (int(grid.x * grid.y) < kSmallLevelTiles && f == 0)
+	{
+		LaunchConfig lc(dim3(grid.x * kDwtStripes, grid.y), dim3(kLargeLevelThreads), stream, programmatic);
+		cudaLaunchKernelEx(&lc.cfg, dwt_stripes_kernel, p, in, buf, f, m);
+	}
+	else if (int(grid.x * grid.y) < kSmallLevelTiles)
 	{
 		LaunchConfig lc(grid, dim3(1024), stream, programmatic);
 		cudaLaunchKernelEx(&lc.cfg, dwt_forward_kernel<1024>, p, in, buf, f, m);
