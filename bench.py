@@ -441,6 +441,9 @@ def run_ours(args, cfg, ws, rank, local):
         roofline = {"bound": "hbm", "kernel": dom, "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
                     "frac": round(achieved / peak, 4), "traffic": _ncu_traffic(dom, cfg), "peak_source": peak_kind,
                     "algorithmic_bytes": alg[dom], "avg_launch_us": round(ms * 1e3, 2)}
+        limit = _ncu_limit(dom, cfg)
+        if limit:
+            roofline.update(limit)
     dwt_ms = sum(v for k, v in stages.items() if k.startswith("dwt"))
     dwt_stage = {"us": round(dwt_ms * 1e3, 2), "algorithmic_bytes": alg["dwt_stage"],
                  "achieved_gbs": round(alg["dwt_stage"] / (dwt_ms * 1e-3) / 1e9, 1) if dwt_ms else None}
@@ -458,7 +461,7 @@ def run_ours(args, cfg, ws, rank, local):
         cpu = cpu_baseline(cfg, frames, args.cpu_seconds)
     batched = None
     if rank == 0 and ws == 1 and not args.no_batch:
-        batched = run_batched(iters=10)
+        batched = run_batched(iters=10, frames_n=args.batch_frames)
     packet_decode = None
     if rank == 0 and ws == 1 and not args.no_configs:
         packet_decode = run_packet_decode(cfg, frames)
@@ -918,16 +921,36 @@ def run_secondary(steps, warmup):
     return out
 
 
-def _ncu_traffic(kernel, cfg):
-    """DRAM bytes per launch of `kernel` from the committed ncu summary, if present."""
+def _ncu_entry(kernel, cfg):
+    """The committed ncu figures of `kernel` at this workload (profiles/ncu_traffic.json):
+    DRAM bytes per launch and, where captured, the share of issue slots busy and of
+    DRAM throughput."""
     p = os.path.join(ROOT, "profiles", "ncu_traffic.json")
     try:
         with open(p) as f:
             d = json.load(f)
         key = f"{cfg['width']}x{cfg['height']}{'_444' if cfg['chroma444'] else ''}:{kernel}"
-        return d.get(key)
+        e = d.get(key)
+        return e if isinstance(e, dict) else ({"traffic": e} if e is not None else None)
     except Exception:
         return None
+
+
+def _ncu_traffic(kernel, cfg):
+    """DRAM bytes per launch of `kernel` from the committed ncu summary, if present."""
+    e = _ncu_entry(kernel, cfg)
+    return e.get("traffic") if e else None
+
+
+def _ncu_limit(kernel, cfg):
+    """What bounds `kernel` by its committed ncu figures: instruction issue when the
+    issue slots are far busier than DRAM."""
+    e = _ncu_entry(kernel, cfg)
+    if not e or "issue_active_pct" not in e or "dram_pct" not in e:
+        return None
+    kind = "instruction issue" if e["issue_active_pct"] > 2 * e["dram_pct"] else "hbm"
+    return {"limit": kind, "issue_slots_busy_pct": e["issue_active_pct"], "dram_throughput_pct": e["dram_pct"],
+            "source": e.get("source", "profiles/ncu_traffic.json")}
 
 
 def run_e2e(args, cfg, frames, dev):
@@ -1157,6 +1180,8 @@ def main():
     ap.add_argument("--cpu-seconds", type=float, default=10.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-batch", action="store_true", help="skip the batched-form measurement")
+    ap.add_argument("--batch-frames", type=int, default=64,
+                    help="frames in the batched-form measurement (64: the batched benchmark's set)")
     ap.add_argument("--no-configs", action="store_true",
                     help="skip the other configurations (720p, FP16 storage, reference precision, 4K, 4K 4:4:4 sweep)")
     ap.add_argument("--serve-seconds", type=float, default=60.0,

@@ -1649,14 +1649,23 @@ __device__ __noinline__ void batch_inverse_item(int local)
 __global__ void __launch_bounds__(kBatchPersistentThreads, 4) batch_persistent_kernel(const BatchRunParams rp)
 {
 	BatchShared &sh = batch_shared();
+	// Thread 0 holds the CTA's next ticket, taken while the current item runs,
+	// so the ticket's round trip overlaps the work. Tickets are still processed
+	// in increasing order by every CTA, and an item only waits for items with
+	// smaller tickets, so every wait still ends.
+	int next = 0;
+	if (threadIdx.x == 0)
+		next = int(atomicAdd(rp.ticket, 1u));
 	for (;;)
 	{
 		if (threadIdx.x == 0)
-			sh.item = int(atomicAdd(rp.ticket, 1u));
+			sh.item = next;
 		__syncthreads();
 		const int item = sh.item;
 		if (item >= rp.nwork)
 			return;
+		if (threadIdx.x == 0)
+			next = int(atomicAdd(rp.ticket, 1u));
 		const uint32_t w = __ldg(rp.work + item);
 		const int f = int(w >> 24), stage = int((w >> kBatchLocalBits) & 31u);
 		const int local = int(w & ((1u << kBatchLocalBits) - 1u));
