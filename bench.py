@@ -953,6 +953,9 @@ def _ncu_limit(kernel, cfg):
             "source": e.get("source", "profiles/ncu_traffic.json")}
 
 
+E2E_PAIRS = 3  # encoder/decoder pairs (streams, host threads) in flight in the end-to-end measurement
+
+
 def run_e2e(args, cfg, frames, dev):
     """Encode + decode through the reference-facing C API with host (pinned)
     buffers: pyrowave_encoder_encode_cpu_synchronous (input planes uploaded
@@ -962,26 +965,29 @@ def run_e2e(args, cfg, frames, dev):
     pyrowave_decoder_decode_cpu_buffer_synchronous (payload uploaded, planes
     read back).
 
-    The timed run keeps two encoder/decoder pairs on two devices (two CUDA
-    streams): the encode of frame i+1, which returns without waiting
-    (pyrowave.h:445-447), is issued before frame i is packetized and decoded,
-    so one frame's copies and kernels overlap the other's. A sequential pass
-    with one pair gives the per-call breakdown."""
+    The timed run keeps E2E_PAIRS encoder/decoder pairs, each on its own device
+    object (its own CUDA stream) and host thread: a thread encodes its frame
+    (which returns without waiting, pyrowave.h:445-447), packetizes, pushes and
+    decodes it, then takes its next frame, so the frames of different threads
+    overlap their copies and kernels (the C API calls release the interpreter
+    lock). A sequential pass with one pair gives the per-call breakdown."""
+    import concurrent.futures
+
     import torch
 
     from pyrowave_b200 import capi
 
     w, h, c444, budget = cfg["width"], cfg["height"], cfg["chroma444"], cfg["budget"]
     chroma = capi.CHROMA_444 if c444 else capi.CHROMA_420
-    devs = [dev, capi.Device()]
+    devs = [dev] + [capi.Device() for _ in range(E2E_PAIRS - 1)]
     pairs = [(capi.Encoder(d, w, h, chroma, args.fp16_mask), capi.Decoder(d, w, h, chroma, args.fp16_mask))
              for d in devs]
     pinned = [[torch.from_numpy(p).pin_memory().numpy() for p in f] for f in frames]
     outs = [[torch.empty(p.shape, dtype=torch.uint8).pin_memory().numpy() for p in frames[0]] for _ in pairs]
     bitstreams = [torch.empty(budget, dtype=torch.uint8).pin_memory().numpy() for _ in pairs]
     boundary = 8192
-    packets = (capi.Packet * 4096)()
-    got = capi.c_size_t()
+    packets = [(capi.Packet * 4096)() for _ in pairs]
+    got = [capi.c_size_t() for _ in pairs]
 
     def encode(k, i):
         capi.check(pairs[k][0].encode_cpu(pinned[i % len(pinned)], budget), "encode_cpu_synchronous")
@@ -990,10 +996,10 @@ def run_e2e(args, cfg, frames, dev):
         enc, dec = pairs[k]
         bs = bitstreams[k]
         n = enc.compute_num_packets(boundary)
-        assert n <= len(packets)
-        capi.check(enc.L.pyrowave_encoder_packetize(enc.h, packets, boundary, capi.ctypes.byref(got),
+        assert n <= len(packets[k])
+        capi.check(enc.L.pyrowave_encoder_packetize(enc.h, packets[k], boundary, capi.ctypes.byref(got[k]),
                                                     capi.ctypes.c_void_p(bs.ctypes.data), budget), "packetize")
-        total = packets[got.value - 1].offset + packets[got.value - 1].size
+        total = packets[k][got[k].value - 1].offset + packets[k][got[k].value - 1].size
         t_pk = time.perf_counter()
         capi.check(dec.push_packet_ptr(bs.ctypes.data, total), "push_packet")
         t_push = time.perf_counter()
@@ -1025,31 +1031,37 @@ def run_e2e(args, cfg, frames, dev):
                           "reads the frame back, cuts packets; push_packet: host parse of the whole frame; "
                           "decode: payload upload, dequantise + inverse DWT, planes read back")
 
-    # Timed run: two pairs alternating, frame i+1 encoding while frame i finishes.
-    for i in range(4):
-        encode(i & 1, i)
-        finish(i & 1)
+    # Timed run: one host thread per pair, frames dealt round robin.
+    for i in range(2 * E2E_PAIRS):
+        encode(i % E2E_PAIRS, i)
+        finish(i % E2E_PAIRS)
     n = max(args.steps, 10)
-    total_bytes = 0
+
+    def worker(k):
+        done = 0
+        for i in range(k, n, E2E_PAIRS):
+            encode(k, i)
+            done += finish(k)[0]
+        return done
+
     t0 = time.perf_counter()
-    encode(0, 0)
-    for i in range(n):
-        if i + 1 < n:
-            encode((i + 1) & 1, i + 1)
-        total_bytes += finish(i & 1)[0]
+    with concurrent.futures.ThreadPoolExecutor(E2E_PAIRS) as ex:
+        total_bytes = sum(ex.map(worker, range(E2E_PAIRS)))
     t1 = time.perf_counter()
     blocks32 = pairs[0][0].layout().block_count_32x32
     for enc, dec in pairs:
         enc.close()
         dec.close()
-    devs[1].close()
+    for d in devs[1:]:
+        d.close()
     planes_bytes = sum(p.nbytes for p in frames[0])
     avg_stream = total_bytes // n
     return {"total_s": t1 - t0, "frames": n,
             "h2d": planes_bytes + avg_stream + 4 * blocks32,
             "d2h": planes_bytes + budget + 8 * blocks32 + 8,
-            "method": "two encoder/decoder pairs on two CUDA streams, frame i+1's encode issued before frame i "
-                      "is packetized and decoded; one push_packet per frame",
+            "method": f"{E2E_PAIRS} encoder/decoder pairs on {E2E_PAIRS} CUDA streams and host threads, frames "
+                      "dealt round robin; per frame: encode (upload + launch), packetize, one push_packet of the "
+                      "whole frame, decode (payload upload, kernels, planes read back)",
             "breakdown_us": breakdown}
 
 

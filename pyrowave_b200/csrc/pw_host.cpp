@@ -2486,7 +2486,9 @@ struct BatchShape
 	int large_below = 0;        // per-stage mode: levels with fewer tiles run 1024-thread CTAs
 	int ctas_per_sm = 0;        // persistent mode: resident CTAs per SM (0: as many as fit)
 	bool large_first = false;   // persistent mode: within a stage, frames in decreasing size
+	int branches = 1;           // per-stage mode: groups of frames, each its own chain of launches
 };
+constexpr int kMaxBatchBranches = 8;
 } // namespace
 
 struct pyrowave_cuda_batch_opaque
@@ -2511,12 +2513,20 @@ struct pyrowave_cuda_batch_opaque
 	cudaStream_t last_stream = nullptr;
 	bool has_result = false;
 
-	// CTA maps, one device array, per-stage ranges.
+	// CTA maps, one device array; per branch (group of frames), per-stage ranges.
 	uint32_t *maps_d = nullptr;
 	std::vector<uint32_t> maps_h;
-	int level_off[kLevels] = {}, level_n[kLevels] = {};
-	int quant_off = 0, quant_n = 0, resolve_off = 0, resolve_n = 0, block_off = 0, block_n = 0;
+	struct StageRanges
+	{
+		int level_off[kLevels] = {}, level_n[kLevels] = {};
+		int quant_off = 0, quant_n = 0, resolve_off = 0, resolve_n = 0, block_off = 0, block_n = 0;
+	};
+	std::vector<StageRanges> ranges;
 	int level_tiles[kLevels] = {}; // all frames' tiles per level
+	// Per-stage mode with branches: one stream per branch joins the capture
+	// through fork / join events (the branches become parallel graph paths).
+	cudaStream_t branch_stream[kMaxBatchBranches] = {};
+	cudaEvent_t fork_event = nullptr, join_event[kMaxBatchBranches] = {};
 	// Per-level TMA maps of the first kBatchTileMapFrames frames (kernel parameters).
 	std::vector<BatchTileMaps> fwd_maps = std::vector<BatchTileMaps>(kLevels);
 	std::vector<BatchTileMaps> inv_maps = std::vector<BatchTileMaps>(kLevels);
@@ -2558,6 +2568,38 @@ struct pyrowave_cuda_batch_opaque
 				cudaEventDestroy(io_free[i]);
 		}
 		host_free(h_totals);
+		for (int i = 0; i < kMaxBatchBranches; i++)
+		{
+			if (branch_stream[i])
+				cudaStreamDestroy(branch_stream[i]);
+			if (join_event[i])
+				cudaEventDestroy(join_event[i]);
+		}
+		if (fork_event)
+			cudaEventDestroy(fork_event);
+	}
+
+	// Frames of each branch: largest first, each to the branch with the least
+	// work so far (samples coded), so the branches end close together.
+	std::vector<std::vector<int>> branch_frames() const
+	{
+		const int nb = std::max(1, std::min(shape.persistent ? 1 : shape.branches, count));
+		std::vector<std::vector<int>> out(static_cast<size_t>(nb));
+		std::vector<int> order(static_cast<size_t>(count));
+		std::vector<double> load(size_t(nb), 0.0);
+		for (int f = 0; f < count; f++)
+			order[size_t(f)] = f;
+		auto work = [&](int f) { return double(geo[f].width) * geo[f].height * (geo[f].chroma444 ? 3.0 : 1.5); };
+		std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return work(a) > work(b); });
+		for (int f : order)
+		{
+			const size_t g = size_t(std::min_element(load.begin(), load.end()) - load.begin());
+			out[g].push_back(f);
+			load[g] += work(f);
+		}
+		for (auto &v : out)
+			std::sort(v.begin(), v.end());
+		return out;
 	}
 
 	void build_maps()
@@ -2565,32 +2607,72 @@ struct pyrowave_cuda_batch_opaque
 		maps_h.clear();
 		for (int level = 0; level < kLevels; level++)
 		{
-			level_off[level] = int(maps_h.size());
+			level_tiles[level] = 0;
 			for (int f = 0; f < count; f++)
-			{
-				const LevelDesc &L = geo[f].level[level];
-				const int ncomp = (level == 0 && !geo[f].chroma444) ? 1 : 3;
-				for (int i = 0; i < L.tiles_x * L.tiles_y * ncomp; i++)
-					maps_h.push_back(batch_cta(f, i));
-			}
-			level_n[level] = int(maps_h.size()) - level_off[level];
-			level_tiles[level] = level_n[level];
+				level_tiles[level] += geo[f].level[level].tiles_x * geo[f].level[level].tiles_y *
+				                      ((level == 0 && !geo[f].chroma444) ? 1 : 3);
 		}
-		quant_off = int(maps_h.size());
-		for (int f = 0; f < count; f++)
-			for (int i = 0; i < (frames_h[f].small_blocks + 1) / 2; i++)
-				maps_h.push_back(batch_cta(f, i));
-		quant_n = int(maps_h.size()) - quant_off;
-		resolve_off = int(maps_h.size());
-		for (int f = 0; f < count; f++)
-			for (int i = 0; i < frames_h[f].slices; i++)
-				maps_h.push_back(batch_cta(f, i));
-		resolve_n = int(maps_h.size()) - resolve_off;
-		block_off = int(maps_h.size());
-		for (int f = 0; f < count; f++)
-			for (int i = 0; i < frames_h[f].block_count; i++)
-				maps_h.push_back(batch_cta(f, i));
-		block_n = int(maps_h.size()) - block_off;
+		const std::vector<std::vector<int>> groups = branch_frames();
+		ranges.assign(groups.size(), StageRanges{});
+		for (size_t g = 0; g < groups.size(); g++)
+		{
+			StageRanges &r = ranges[g];
+			const std::vector<int> &fs = groups[g];
+			for (int level = 0; level < kLevels; level++)
+			{
+				r.level_off[level] = int(maps_h.size());
+				for (int f : fs)
+				{
+					const LevelDesc &L = geo[f].level[level];
+					const int ncomp = (level == 0 && !geo[f].chroma444) ? 1 : 3;
+					for (int i = 0; i < L.tiles_x * L.tiles_y * ncomp; i++)
+						maps_h.push_back(batch_cta(f, i));
+				}
+				r.level_n[level] = int(maps_h.size()) - r.level_off[level];
+			}
+			r.quant_off = int(maps_h.size());
+			for (int f : fs)
+				for (int i = 0; i < (frames_h[f].small_blocks + 1) / 2; i++)
+					maps_h.push_back(batch_cta(f, i));
+			r.quant_n = int(maps_h.size()) - r.quant_off;
+			r.resolve_off = int(maps_h.size());
+			for (int f : fs)
+				for (int i = 0; i < frames_h[f].slices; i++)
+					maps_h.push_back(batch_cta(f, i));
+			r.resolve_n = int(maps_h.size()) - r.resolve_off;
+			r.block_off = int(maps_h.size());
+			for (int f : fs)
+				for (int i = 0; i < frames_h[f].block_count; i++)
+					maps_h.push_back(batch_cta(f, i));
+			r.block_n = int(maps_h.size()) - r.block_off;
+		}
+	}
+
+	// One branch's stage launches (per-stage mode) on stream s; the first launch
+	// follows the fork without a programmatic edge.
+	void launch_stages(const StageRanges &r, bool decode, bool first_programmatic, cudaStream_t s)
+	{
+		bool pdl = first_programmatic;
+		for (int level = 0; level < kLevels; level++)
+		{
+			if (r.level_n[level] == 0)
+				continue;
+			launch_dwt_forward_batch(frames_d, io_d, maps_d + r.level_off[level], r.level_n[level], level,
+			                         &fwd_maps[level], level < shape.small_level, large(level), pdl, s);
+			pdl = true;
+		}
+		if (r.quant_n > 0)
+			launch_quant_blocks_batch(frames_d, maps_d + r.quant_off, r.quant_n, pdl, s);
+		launch_resolve_batch(frames_d, io_d, maps_d + r.resolve_off, r.resolve_n, s);
+		launch_pack_batch(frames_d, maps_d + r.block_off, r.block_n, s);
+		if (decode)
+		{
+			launch_dequant_batch(frames_d, maps_d + r.block_off, r.block_n, true, s);
+			for (int level = kLevels - 1; level >= 0; level--)
+				if (r.level_n[level] > 0)
+					launch_idwt_batch(frames_d, io_d, maps_d + r.level_off[level], r.level_n[level], level,
+					                  &inv_maps[level], large(level), true, s);
+		}
 	}
 
 	// Items of each stage of frame f (persistent mode).
@@ -2676,6 +2758,17 @@ struct pyrowave_cuda_batch_opaque
 	bool upload(cudaStream_t s)
 	{
 		build_maps();
+		for (size_t g = 0; g < ranges.size() && ranges.size() > 1; g++)
+		{
+			if (!branch_stream[g] &&
+			    !cuda_ok(cudaStreamCreateWithFlags(&branch_stream[g], cudaStreamNonBlocking), "cudaStreamCreate"))
+				return false;
+			if (!join_event[g] &&
+			    !cuda_ok(cudaEventCreateWithFlags(&join_event[g], cudaEventDisableTiming), "cudaEventCreate"))
+				return false;
+		}
+		if (!fork_event && !cuda_ok(cudaEventCreateWithFlags(&fork_event, cudaEventDisableTiming), "cudaEventCreate"))
+			return false;
 		(void)batch_persistent_max_ctas_per_sm(); // kernel attributes, set outside any capture
 		bool ok = true;
 		std::vector<uint32_t> work[2], gates;
@@ -2754,19 +2847,20 @@ struct pyrowave_cuda_batch_opaque
 				graph.destroy();
 			return ok;
 		}
-		for (int level = 0; level < kLevels; level++)
-			launch_dwt_forward_batch(frames_d, io_d, maps_d + level_off[level], level_n[level], level, &fwd_maps[level],
-			                         level < shape.small_level, large(level), level > 0, s);
-		if (quant_n > 0)
-			launch_quant_blocks_batch(frames_d, maps_d + quant_off, quant_n, true, s);
-		launch_resolve_batch(frames_d, io_d, maps_d + resolve_off, resolve_n, s);
-		launch_pack_batch(frames_d, maps_d + block_off, block_n, s);
-		if (decode)
+		if (ranges.size() <= 1)
+			launch_stages(ranges[0], decode, false, s);
+		else
 		{
-			launch_dequant_batch(frames_d, maps_d + block_off, block_n, true, s);
-			for (int level = kLevels - 1; level >= 0; level--)
-				launch_idwt_batch(frames_d, io_d, maps_d + level_off[level], level_n[level], level, &inv_maps[level],
-				                  large(level), true, s);
+			// Fork: every branch stream waits for the clears above; join: the
+			// capturing stream waits for every branch.
+			ok = ok && cuda_ok(cudaEventRecord(fork_event, s), "cudaEventRecord");
+			for (size_t g = 0; g < ranges.size() && ok; g++)
+			{
+				ok = cuda_ok(cudaStreamWaitEvent(branch_stream[g], fork_event, 0), "cudaStreamWaitEvent");
+				launch_stages(ranges[g], decode, false, branch_stream[g]);
+				ok = ok && cuda_ok(cudaEventRecord(join_event[g], branch_stream[g]), "cudaEventRecord") &&
+				     cuda_ok(cudaStreamWaitEvent(s, join_event[g], 0), "cudaStreamWaitEvent");
+			}
 		}
 		ok = launches_ok("kernel launch") && ok;
 		ok = graph.end(s, 0) && ok;
@@ -3002,6 +3096,7 @@ pyrowave_result pyrowave_cuda_batch_get_shape(pyrowave_cuda_batch batch, pyrowav
 	shape->large_below = batch->shape.large_below;
 	shape->ctas_per_sm = batch->shape.persistent ? batch->persistent_ctas() / batch->sm_count : 0;
 	shape->large_first = batch->shape.large_first ? 1u : 0u;
+	shape->branches = batch->shape.persistent ? 1u : uint32_t(batch->ranges.size());
 	return PYROWAVE_SUCCESS;
 }
 
@@ -3009,7 +3104,7 @@ pyrowave_result pyrowave_cuda_batch_set_shape(pyrowave_cuda_batch batch, const p
                                               pyrowave_cuda_stream stream)
 {
 	if (!batch || !shape || shape->small_level < 0 || shape->small_level > kLevels || shape->ctas_per_sm < 0 ||
-	    shape->large_below < 0)
+	    shape->large_below < 0 || shape->branches > uint32_t(kMaxBatchBranches))
 		return PYROWAVE_ERROR_INVALID_ARGUMENT;
 	BatchShape s;
 	s.persistent = shape->persistent != 0;
@@ -3017,6 +3112,7 @@ pyrowave_result pyrowave_cuda_batch_set_shape(pyrowave_cuda_batch batch, const p
 	s.large_below = shape->large_below;
 	s.ctas_per_sm = shape->ctas_per_sm;
 	s.large_first = shape->large_first != 0;
+	s.branches = std::max(1, int(shape->branches));
 	cudaStream_t st = pick_stream(batch->device, stream);
 	if (batch->last_stream && !cuda_ok(cudaStreamSynchronize(batch->last_stream), "cudaStreamSynchronize"))
 		return PYROWAVE_ERROR_GENERIC;
@@ -3038,8 +3134,9 @@ pyrowave_result pyrowave_cuda_batch_autotune(pyrowave_cuda_batch batch, const py
 	// Candidates. Persistent launch: where the transform-only suffix of levels
 	// starts (its blocks quantised in a stage of their own), resident CTAs per
 	// SM, and the order of frames within a stage. Per-stage launches: the same
-	// suffix, and below how many tiles a level runs 1024-thread CTAs. Each is
-	// timed over a few calls; the fastest is kept.
+	// suffix, below how many tiles a level runs 1024-thread CTAs, and how many
+	// concurrent groups of frames. Each is timed over a few calls; the fastest
+	// is kept.
 	std::vector<BatchShape> cands;
 	for (int small = kLevels; small >= 2; small--)
 	{
@@ -3054,13 +3151,17 @@ pyrowave_result pyrowave_cuda_batch_autotune(pyrowave_cuda_batch batch, const py
 				cands.push_back(c);
 			}
 		for (int lb : {0, 256, 1024})
-		{
-			BatchShape c;
-			c.persistent = false;
-			c.small_level = small;
-			c.large_below = lb;
-			cands.push_back(c);
-		}
+			for (int br : {1, 2, 4, 8})
+			{
+				if (br > batch->count || (br > 1 && lb == 1024))
+					continue;
+				BatchShape c;
+				c.persistent = false;
+				c.small_level = small;
+				c.large_below = lb;
+				c.branches = br;
+				cands.push_back(c);
+			}
 	}
 	BatchShape best = batch->shape;
 	float best_ms = 0.0f;
