@@ -344,10 +344,16 @@ typedef struct pyrowave_cuda_batch_shape
 	int32_t large_below;
 	int32_t ctas_per_sm;
 	uint32_t large_first;
-	/* Per-stage launches only: the frames split into this many groups (1 to 8),
+	/* Per-stage launches: the frames split into this many groups (1 to 8),
 	 * each group its own chain of stage launches, the chains running
-	 * concurrently (parallel paths of the call's graph). */
+	 * concurrently (parallel paths of the call's graph). Frame graphs: the
+	 * number of streams the frames are spread over. */
 	uint32_t branches;
+	/* Nonzero (with persistent = 0): every frame through its own single-frame
+	 * encode and decode graphs (as pyrowave_cuda_encoder_encode and
+	 * pyrowave_cuda_decoder_decode_blocks), the frames dealt round robin over
+	 * `branches` streams that fork from and join into the call's stream. */
+	uint32_t frame_graphs;
 } pyrowave_cuda_batch_shape;
 
 PYROWAVE_PUBLIC_API pyrowave_result pyrowave_cuda_batch_get_shape(pyrowave_cuda_batch batch,
@@ -359,9 +365,10 @@ PYROWAVE_PUBLIC_API pyrowave_result pyrowave_cuda_batch_set_shape(pyrowave_cuda_
 
 /* Choose the batch's shape by timing the candidates on these inputs (the
  * batch's autotuner) and keep the fastest: persistent launches with 2 to 4
- * resident CTAs per SM and both frame orders, and per-stage launches with
+ * resident CTAs per SM and both frame orders, per-stage launches with
  * three thresholds for 1024-thread CTAs and 1, 2, 4 or 8 concurrent groups of
- * frames, each with the transform-only suffix starting at levels 5 down to 2. The bitstreams do not depend on the choice,
+ * frames, each with the transform-only suffix starting at levels 5 down to 2,
+ * and frame graphs over 4 or 8 streams. The bitstreams do not depend on the choice,
  * and the tuning calls do not advance the frames' sequence numbers. Waits. */
 PYROWAVE_PUBLIC_API pyrowave_result pyrowave_cuda_batch_autotune(pyrowave_cuda_batch batch,
                                                                  const pyrowave_cuda_planes *inputs,

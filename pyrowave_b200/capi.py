@@ -656,14 +656,16 @@ class Batch:
         return {k: int(getattr(sh, k)) for k, _ in BatchShape._fields_}
 
     def set_shape(self, persistent=True, small_level=5, large_below=0, ctas_per_sm=0, large_first=False,
-                  branches=1, stream: int = 0):
-        sh = BatchShape(int(persistent), small_level, large_below, ctas_per_sm, int(large_first), branches)
+                  branches=1, frame_graphs=False, stream: int = 0):
+        sh = BatchShape(int(persistent), small_level, large_below, ctas_per_sm, int(large_first), branches,
+                        int(frame_graphs))
         check(self.L.pyrowave_cuda_batch_set_shape(self.h, ctypes.byref(sh), c_void_p(stream)), "batch_set_shape")
 
 
 class BatchShape(Structure):
     _fields_ = [("persistent", c_uint32), ("small_level", c_int32), ("large_below", c_int32),
-                ("ctas_per_sm", c_int32), ("large_first", c_uint32), ("branches", c_uint32)]
+                ("ctas_per_sm", c_int32), ("large_first", c_uint32), ("branches", c_uint32),
+                ("frame_graphs", c_uint32)]
 
 
 class Server:

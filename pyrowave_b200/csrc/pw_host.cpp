@@ -2486,7 +2486,9 @@ struct BatchShape
 	int large_below = 0;        // per-stage mode: levels with fewer tiles run 1024-thread CTAs
 	int ctas_per_sm = 0;        // persistent mode: resident CTAs per SM (0: as many as fit)
 	bool large_first = false;   // persistent mode: within a stage, frames in decreasing size
-	int branches = 1;           // per-stage mode: groups of frames, each its own chain of launches
+	int branches = 1;           // per-stage mode: groups of frames, each its own chain of launches;
+	                            // frame-graph mode: streams the frames are spread over
+	bool frame_graphs = false;  // each frame through its own single-frame encode and decode graphs
 };
 constexpr int kMaxBatchBranches = 8;
 } // namespace
@@ -2527,6 +2529,11 @@ struct pyrowave_cuda_batch_opaque
 	// through fork / join events (the branches become parallel graph paths).
 	cudaStream_t branch_stream[kMaxBatchBranches] = {};
 	cudaEvent_t fork_event = nullptr, join_event[kMaxBatchBranches] = {};
+	// Frame-graph mode: one single-frame encoder and decoder per frame (created
+	// on first use, stream buffers sized for the frame's largest budget).
+	std::vector<pyrowave_encoder> frame_enc;
+	std::vector<pyrowave_decoder> frame_dec;
+	bool result_frame_graphs = false; // the last call ran in frame-graph mode
 	// Per-level TMA maps of the first kBatchTileMapFrames frames (kernel parameters).
 	std::vector<BatchTileMaps> fwd_maps = std::vector<BatchTileMaps>(kLevels);
 	std::vector<BatchTileMaps> inv_maps = std::vector<BatchTileMaps>(kLevels);
@@ -2568,6 +2575,10 @@ struct pyrowave_cuda_batch_opaque
 				cudaEventDestroy(io_free[i]);
 		}
 		host_free(h_totals);
+		for (pyrowave_encoder e : frame_enc)
+			pyrowave_encoder_destroy(e);
+		for (pyrowave_decoder d : frame_dec)
+			pyrowave_decoder_destroy(d);
 		for (int i = 0; i < kMaxBatchBranches; i++)
 		{
 			if (branch_stream[i])
@@ -2583,7 +2594,7 @@ struct pyrowave_cuda_batch_opaque
 	// work so far (samples coded), so the branches end close together.
 	std::vector<std::vector<int>> branch_frames() const
 	{
-		const int nb = std::max(1, std::min(shape.persistent ? 1 : shape.branches, count));
+		const int nb = std::max(1, std::min(shape.persistent || shape.frame_graphs ? 1 : shape.branches, count));
 		std::vector<std::vector<int>> out(static_cast<size_t>(nb));
 		std::vector<int> order(static_cast<size_t>(count));
 		std::vector<double> load(size_t(nb), 0.0);
@@ -2758,7 +2769,8 @@ struct pyrowave_cuda_batch_opaque
 	bool upload(cudaStream_t s)
 	{
 		build_maps();
-		for (size_t g = 0; g < ranges.size() && ranges.size() > 1; g++)
+		const size_t nstreams = shape.frame_graphs ? size_t(std::max(1, std::min(shape.branches, count))) : ranges.size();
+		for (size_t g = 0; g < nstreams && nstreams > 1; g++)
 		{
 			if (!branch_stream[g] &&
 			    !cuda_ok(cudaStreamCreateWithFlags(&branch_stream[g], cudaStreamNonBlocking), "cudaStreamCreate"))
@@ -2869,6 +2881,92 @@ struct pyrowave_cuda_batch_opaque
 		return ok;
 	}
 
+	bool ensure_frame_coders()
+	{
+		if (!frame_enc.empty())
+			return true;
+		for (int f = 0; f < count; f++)
+		{
+			const Geometry &g = geo[f];
+			pyrowave_encoder_create_info ei = {device, g.width, g.height,
+			                                   g.chroma444 ? PYROWAVE_CHROMA_SUBSAMPLING_444
+			                                               : PYROWAVE_CHROMA_SUBSAMPLING_420};
+			pyrowave_decoder_create_info di = {};
+			di.device = device;
+			di.width = g.width;
+			di.height = g.height;
+			di.chroma = ei.chroma;
+			pyrowave_encoder e = nullptr;
+			pyrowave_decoder d = nullptr;
+			if (pyrowave_encoder_create(&ei, &e) != PYROWAVE_SUCCESS)
+				return false;
+			frame_enc.push_back(e);
+			if (pyrowave_decoder_create(&di, &d) != PYROWAVE_SUCCESS)
+				return false;
+			frame_dec.push_back(d);
+			// Buffers now, sized for the largest budget the batch accepts, so no
+			// call reallocates while other frames' work is in flight.
+			if (e->allocate() != PYROWAVE_SUCCESS || e->ensure_stream_capacity(capacity_words[f]) != PYROWAVE_SUCCESS ||
+			    d->allocate() != PYROWAVE_SUCCESS)
+				return false;
+		}
+		return true;
+	}
+
+	// Frame-graph mode: every frame's encode (and decode) through its own
+	// single-frame graphs, the frames dealt round robin over the branch
+	// streams, which fork from and join into s. Each frame's totals and decode
+	// error word are read back on its stream.
+	pyrowave_result run_frame_graphs(const pyrowave_cuda_planes *inputs, const size_t *budgets,
+	                                 const pyrowave_cuda_planes *outputs, cudaStream_t s)
+	{
+		if (!ensure_frame_coders())
+			return PYROWAVE_ERROR_OUT_OF_DEVICE_MEMORY;
+		const int nb = std::max(1, std::min(shape.branches, count));
+		if (!cuda_ok(cudaEventRecord(fork_event, s), "cudaEventRecord"))
+			return PYROWAVE_ERROR_GENERIC;
+		for (int k = 0; k < nb; k++)
+			if (!cuda_ok(cudaStreamWaitEvent(branch_stream[k], fork_event, 0), "cudaStreamWaitEvent"))
+				return PYROWAVE_ERROR_GENERIC;
+		pyrowave_result r = PYROWAVE_SUCCESS;
+		for (int f = 0; f < count && r == PYROWAVE_SUCCESS; f++)
+		{
+			cudaStream_t bs = branch_stream[f % nb];
+			const pyrowave_cuda_stream ps = reinterpret_cast<pyrowave_cuda_stream>(bs);
+			encoder_set_frames(frame_enc[size_t(f)], (sequence[f] + 7u) & 7u); // the encode advances it to sequence[f]
+			const pyrowave_rate_control rc = {budgets[f]};
+			r = pyrowave_cuda_encoder_encode(frame_enc[size_t(f)], &inputs[f], &rc, ps);
+			uint32_t *tot = h_totals + size_t(f) * kTotalsWords;
+			if (r == PYROWAVE_SUCCESS &&
+			    !cuda_ok(cudaMemcpyAsync(tot, &frame_enc[size_t(f)]->rc->error, kTotalsWords * 4, cudaMemcpyDeviceToHost,
+			                             bs),
+			             "cudaMemcpyAsync"))
+				r = PYROWAVE_ERROR_GENERIC;
+			if (r == PYROWAVE_SUCCESS && outputs)
+			{
+				const uint32_t *words = nullptr, *meta = nullptr;
+				size_t cap = 0;
+				r = pyrowave_cuda_encoder_get_device_bitstream(frame_enc[size_t(f)], &words, &meta, &cap);
+				if (r == PYROWAVE_SUCCESS)
+					r = pyrowave_cuda_decoder_decode_blocks(frame_dec[size_t(f)], meta, words + 2, cap - 2, &outputs[f], ps);
+				if (r == PYROWAVE_SUCCESS &&
+				    !cuda_ok(cudaMemcpyAsync(tot + kTotalsWords - 1, frame_dec[size_t(f)]->error_d, 4,
+				                             cudaMemcpyDeviceToHost, bs),
+				             "cudaMemcpyAsync"))
+					r = PYROWAVE_ERROR_GENERIC;
+			}
+		}
+		// Join every branch, also after a failed frame, so the stream state stays whole.
+		for (int k = 0; k < nb; k++)
+			if (!cuda_ok(cudaEventRecord(join_event[k], branch_stream[k]), "cudaEventRecord") ||
+			    !cuda_ok(cudaStreamWaitEvent(s, join_event[k], 0), "cudaStreamWaitEvent"))
+				r = PYROWAVE_ERROR_GENERIC;
+		last_stream = s;
+		has_result = r == PYROWAVE_SUCCESS;
+		result_frame_graphs = true;
+		return r;
+	}
+
 	pyrowave_result run(const pyrowave_cuda_planes *inputs, const size_t *budgets, const pyrowave_cuda_planes *outputs,
 	                    cudaStream_t s)
 	{
@@ -2914,6 +3012,9 @@ struct pyrowave_cuda_batch_opaque
 			sequence[f] = (sequence[f] + 1) & 7u;
 			io.rp = make_resolve_params(geo[f], uint32_t((target >= 8 ? target - 8 : target) / 4), sequence[f]);
 		}
+		if (shape.frame_graphs)
+			return run_frame_graphs(inputs, budgets, outputs, s);
+		result_frame_graphs = false;
 		if (!capture(k, outputs != nullptr, s))
 			return PYROWAVE_ERROR_GENERIC;
 		if (!cuda_ok(cudaGraphLaunch(graphs[k][outputs ? 1 : 0].exec, s), "cudaGraphLaunch") ||
@@ -3065,6 +3166,11 @@ pyrowave_result pyrowave_cuda_batch_get_device_bitstream(pyrowave_cuda_batch bat
 {
 	if (!batch || index >= uint32_t(batch->count) || !stream || !block_meta)
 		return PYROWAVE_ERROR_INVALID_ARGUMENT;
+	if (batch->result_frame_graphs)
+	{
+		size_t cap = 0;
+		return pyrowave_cuda_encoder_get_device_bitstream(batch->frame_enc[index], stream, block_meta, &cap);
+	}
 	*stream = batch->frames_h[index].eb.stream;
 	*block_meta = batch->frames_h[index].eb.block_meta;
 	return PYROWAVE_SUCCESS;
@@ -3096,7 +3202,10 @@ pyrowave_result pyrowave_cuda_batch_get_shape(pyrowave_cuda_batch batch, pyrowav
 	shape->large_below = batch->shape.large_below;
 	shape->ctas_per_sm = batch->shape.persistent ? batch->persistent_ctas() / batch->sm_count : 0;
 	shape->large_first = batch->shape.large_first ? 1u : 0u;
-	shape->branches = batch->shape.persistent ? 1u : uint32_t(batch->ranges.size());
+	shape->branches = batch->shape.persistent ? 1u
+	                  : batch->shape.frame_graphs ? uint32_t(std::max(1, std::min(batch->shape.branches, batch->count)))
+	                                              : uint32_t(batch->ranges.size());
+	shape->frame_graphs = batch->shape.frame_graphs ? 1u : 0u;
 	return PYROWAVE_SUCCESS;
 }
 
@@ -3113,6 +3222,7 @@ pyrowave_result pyrowave_cuda_batch_set_shape(pyrowave_cuda_batch batch, const p
 	s.ctas_per_sm = shape->ctas_per_sm;
 	s.large_first = shape->large_first != 0;
 	s.branches = std::max(1, int(shape->branches));
+	s.frame_graphs = shape->frame_graphs != 0 && !s.persistent;
 	cudaStream_t st = pick_stream(batch->device, stream);
 	if (batch->last_stream && !cuda_ok(cudaStreamSynchronize(batch->last_stream), "cudaStreamSynchronize"))
 		return PYROWAVE_ERROR_GENERIC;
@@ -3148,6 +3258,18 @@ pyrowave_result pyrowave_cuda_batch_autotune(pyrowave_cuda_batch batch, const py
 				c.small_level = small;
 				c.ctas_per_sm = per_sm;
 				c.large_first = large_first != 0;
+				cands.push_back(c);
+			}
+		if (small == kLevels)
+			for (int br : {4, 8})
+			{
+				// Frame graphs do not depend on the suffix or the CTA threshold.
+				if (br > batch->count)
+					continue;
+				BatchShape c;
+				c.persistent = false;
+				c.frame_graphs = true;
+				c.branches = br;
 				cands.push_back(c);
 			}
 		for (int lb : {0, 256, 1024})

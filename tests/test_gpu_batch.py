@@ -189,12 +189,14 @@ def test_batch_frames_past_tensor_map_table(device, persistent):
     dict(persistent=False, small_level=4, large_below=256),
     dict(persistent=False, small_level=5, large_below=0, branches=3),
     dict(persistent=False, small_level=2, large_below=256, branches=8),
+    dict(persistent=False, small_level=5, large_below=0, branches=3, frame_graphs=True),
 ], ids=["persistent-fused-2cta-large-first", "persistent-small3-4cta", "persistent-small1-3cta", "per-stage",
-        "per-stage-3-branches", "per-stage-branches-past-frames"])
+        "per-stage-3-branches", "per-stage-branches-past-frames", "frame-graphs-3-streams"])
 def test_batch_shapes_match_oracle(device, shape):
     """Every execution shape (one persistent launch with its CTA count, frame
-    order and transform-only suffix, or one launch per stage, in one or more
-    concurrent groups of frames) gives the oracle's bitstreams and planes."""
+    order and transform-only suffix; one launch per stage, in one or more
+    concurrent groups of frames; or each frame's own encode and decode graphs
+    over several streams) gives the oracle's bitstreams and planes."""
     import torch
 
     frames = [(1280, 720, False, 150000), (640, 360, True, 60000), (200, 128, True, 30000), (1920, 1080, False, 400000),
@@ -207,6 +209,7 @@ def test_batch_shapes_match_oracle(device, shape):
     assert got["persistent"] == int(shape["persistent"]) and got["small_level"] == shape["small_level"]
     # At most one group of frames per frame.
     assert got["branches"] == (1 if shape["persistent"] else min(shape.get("branches", 1), len(frames)))
+    assert got["frame_graphs"] == int(shape.get("frame_graphs", False))
     outs = [[torch.zeros_like(p) for p in pl] for pl in dev_planes]
     in_ptrs, in_strides = _ptrs(dev_planes)
     out_ptrs, out_strides = _ptrs(outs)
