@@ -16,7 +16,8 @@ namespace
 __global__ void __launch_bounds__(128) dequant_kernel(const BlockParams p, const DecodeInput in, const int first)
 {
 	__shared__ DequantShared sh;
-	dequant_body(sh, p, in, first + int(blockIdx.x), blockIdx.x == 0, 1);
+	// Only the launch that starts at block 0 clears the decode's error word.
+	dequant_body(sh, p, in, first + int(blockIdx.x), blockIdx.x == 0 && first == 0, 1);
 }
 
 // Batched form: one CTA per (frame, block), decoding the frame's own bitstream.
@@ -118,6 +119,27 @@ void launch_dequant(const BlockParams &p, const DecodeInput &in, int first, int 
 	cudaLaunchKernelEx(&lc.cfg, dequant_kernel, p, in, first);
 }
 
+// SMs of the current device (queried once).
+int device_sm_count()
+{
+	static int cached = 0;
+	if (cached == 0)
+	{
+		int dev = 0, n = 0;
+		if (cudaGetDevice(&dev) != cudaSuccess || cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess ||
+		    n <= 0)
+		{
+			(void)cudaGetLastError();
+			n = 148;
+		}
+		cached = n;
+	}
+	return cached;
+}
+
+// Levels that fit one wave at three CTAs per SM run the 80-register CTAs (the
+// faster per tile); larger levels run four 64-register CTAs per SM, so a level
+// just above one wave at three (1080p level 0: 510 tiles) still runs in one.
 void launch_idwt_level(const LevelParams &p, const DecodeInput &in, const PlaneOutput &out, const LevelTileMap *maps,
                        bool programmatic, cudaStream_t stream)
 {
@@ -130,7 +152,7 @@ void launch_idwt_level(const LevelParams &p, const DecodeInput &in, const PlaneO
 		LaunchConfig lc(dim3(grid.x * kIdwtStripes, grid.y), dim3(256), stream, programmatic);
 		cudaLaunchKernelEx(&lc.cfg, idwt_stripes_kernel, p, in, out, m);
 	}
-	else if (int(grid.x * grid.y) < kIdwtManyTiles)
+	else if (int(grid.x * grid.y) <= 3 * device_sm_count())
 	{
 		LaunchConfig lc(grid, dim3(256), stream, programmatic);
 		cudaLaunchKernelEx(&lc.cfg, idwt_kernel<256>, p, in, out, m);
