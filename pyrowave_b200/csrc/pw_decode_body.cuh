@@ -45,28 +45,39 @@ struct StagedReader
 
 constexpr uint32_t kSpeculativeWords = 128; // staged with the header when the block size is not yet known
 
-// s[i] = payload word off + i for i in [begin, end), by 128 threads with up to
-// eight loads per thread in flight together.
+// s[i] = payload word off + i for i in [begin, end), by kThreads threads with
+// up to eight loads per thread in flight together.
+template <int kThreads = 128>
 __device__ __forceinline__ void stage_words(uint32_t *s, const PayloadReader &g, uint32_t off, uint32_t begin,
                                             uint32_t end, int t)
 {
-	for (uint32_t base = begin + uint32_t(t); base < end; base += 128 * 8)
+	for (uint32_t base = begin + uint32_t(t); base < end; base += kThreads * 8)
 	{
 		uint32_t v[8];
 #pragma unroll
 		for (int u = 0; u < 8; u++)
 		{
-			const uint32_t i = base + 128u * u;
+			const uint32_t i = base + uint32_t(kThreads) * u;
 			v[u] = i < end ? g.w32(off + i) : 0u;
 		}
 #pragma unroll
 		for (int u = 0; u < 8; u++)
 		{
-			const uint32_t i = base + 128u * u;
+			const uint32_t i = base + uint32_t(kThreads) * u;
 			if (i < end)
 				s[i] = v[u];
 		}
 	}
+}
+
+// The barrier of a block's thread group: hardware barrier `bar` of 128
+// threads, or the whole CTA when a CTA holds one smaller group.
+template <int kSubs> __device__ __forceinline__ void block_sync(int bar)
+{
+	if constexpr (kSubs == 1)
+		group_sync(bar);
+	else
+		__syncthreads();
 }
 
 __device__ __forceinline__ void store_coef(float *c32, __half *c16, bool fp16, int64_t idx, float v)
@@ -77,10 +88,11 @@ __device__ __forceinline__ void store_coef(float *c32, __half *c16, bool fp16, i
 		c32[idx] = v;
 }
 
-// One 32x32 block per 128-thread CTA; thread = one 4x2 sub-block (the
-// reference's mapping, wavelet_dequant.comp:222-238). The CTA with
-// `clear_error` set clears the decode's error word: every inverse level runs
-// after the dequantiser has completed, so the clear precedes any error report.
+// One 32x32 block per thread group; thread = one 4x2 sub-block (the
+// reference's mapping, wavelet_dequant.comp:222-238), or kSubs sub-blocks two
+// 8x8 rows apart. The group with `clear_error` set clears the decode's error
+// word: every inverse level runs after the dequantiser has completed, so the
+// clear precedes any error report.
 struct DequantShared
 {
 	uint32_t s_words[kMaxBlockWords];
@@ -89,11 +101,17 @@ struct DequantShared
 	uint32_t s_sig[4];
 };
 
-// One 32x32 block on a group of 128 threads (threadIdx.x & 127), synchronised
-// with hardware barrier `bar`.
+// One 32x32 block on a group of 128 / kSubs threads: with kSubs = 1 the group
+// is threadIdx.x & 127, synchronised with hardware barrier `bar`; with kSubs =
+// 2 the whole 64-thread CTA, each thread decoding the sub-blocks of 8x8 rows
+// ly and ly + 2.
+template <int kSubs = 1>
 __device__ __forceinline__ void dequant_body(DequantShared &sh, const BlockParams &p, const DecodeInput &in,
                                              const int blk, const bool clear_error, const int bar)
 {
+	static_assert(kSubs == 1 || kSubs == 2, "one or two sub-blocks per thread");
+	constexpr int kGroup = 128 / kSubs;
+	constexpr int kRowStep = 4 / kSubs;
 	uint32_t *const s_words = sh.s_words;
 	uint32_t *const s_plane_off = sh.s_plane_off;
 	uint32_t &s_sign_base = sh.s_sign_base;
@@ -105,10 +123,9 @@ __device__ __forceinline__ void dequant_body(DequantShared &sh, const BlockParam
 	const int rel = blk - B.block32_offset;
 	const int by32 = rel / B.block32_stride, bx32 = rel - by32 * B.block32_stride;
 	const bool f16 = L.fp16 != 0;
-	const int t = threadIdx.x & 127, lane = t & 31;
-	const int sub = t & 7, lx = (t >> 3) & 3, ly = t >> 5;
-	const int grp = ly * 4 + lx;
-	const int ox = bx32 * 32 + lx * 8 + sub_x(sub), oy = by32 * 32 + ly * 8 + sub_y(sub);
+	const int t = threadIdx.x & (kGroup - 1), lane = t & 31;
+	const int sub = t & 7, lx = (t >> 3) & 3, ly0 = t >> 5;
+	const int ox = bx32 * 32 + lx * 8 + sub_x(sub);
 	pdl_wait();
 	if (clear_error && t == 0 && in.error)
 		*in.error = 0u;
@@ -135,7 +152,12 @@ __device__ __forceinline__ void dequant_body(DequantShared &sh, const BlockParam
 	{
 		// Missing block: all coefficients are zero (wavelet_dequant.comp:242-248).
 		const float zero[8] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
-		store_subblock(in.coef32, in.coef16, f16, B.offset + int64_t(oy) * L.pitch + ox, L.pitch, zero);
+#pragma unroll
+		for (int h = 0; h < kSubs; h++)
+		{
+			const int oy = by32 * 32 + (ly0 + h * kRowStep) * 8 + sub_y(sub);
+			store_subblock(in.coef32, in.coef16, f16, B.offset + int64_t(oy) * L.pitch + ox, L.pitch, zero);
+		}
 		return;
 	}
 
@@ -147,18 +169,18 @@ __device__ __forceinline__ void dequant_body(DequantShared &sh, const BlockParam
 	uint32_t staged;
 	if (sized_by_header)
 	{
-		stage_words(s_words, grd, off, 0, kSpeculativeWords, t);
-		group_sync(bar);
+		stage_words<kGroup>(s_words, grd, off, 0, kSpeculativeWords, t);
+		block_sync<kSubs>(bar);
 		words = (s_words[0] >> 16) & 0xfffu;
 		staged = min(max(words, kSpeculativeWords), uint32_t(kMaxBlockWords));
-		stage_words(s_words, grd, off, kSpeculativeWords, staged, t);
+		stage_words<kGroup>(s_words, grd, off, kSpeculativeWords, staged, t);
 	}
 	else
 	{
 		staged = min(words, uint32_t(kMaxBlockWords));
-		stage_words(s_words, grd, off, 0, staged, t);
+		stage_words<kGroup>(s_words, grd, off, 0, staged, t);
 	}
-	group_sync(bar);
+	block_sync<kSubs>(bar);
 	const StagedReader rd{s_words, off, staged, grd};
 	const uint32_t ballot = rd.w32(off) & 0xffffu;
 	const uint32_t q_code = rd.w32(off + 1) & 0xffu;
@@ -190,107 +212,124 @@ __device__ __forceinline__ void dequant_body(DequantShared &sh, const BlockParam
 		if (t == 15)
 			s_sign_base = 8u * (base + inc);
 	}
-	group_sync(bar);
+	block_sync<kSubs>(bar);
 
-	float v[8];
+	float v[kSubs][8];
 #pragma unroll
-	for (int i = 0; i < 8; i++)
-		v[i] = 0.0f;
-	if ((ballot >> grp) & 1u)
+	for (int h = 0; h < kSubs; h++)
 	{
-		const uint32_t local = uint32_t(__popc(ballot & ((1u << grp) - 1u)));
-		const uint32_t cw = rd.u16(off * 2 + 4 + local);
-		const uint32_t cw2 = rd.u8(off * 4 + 8 + n * 2 + local);
-		const uint32_t qb = cw2 & 0xfu;
-		if (cw != 0)
-		{
-			const uint32_t mask = (1u << (2 * sub)) - 1u;
-			const uint32_t lsbs = cw & 0x5555u;
-			uint32_t msbs = cw & 0xaaaau;
-			msbs |= msbs >> 1;
-			uint32_t byte_offset =
-			    uint32_t(__popc(lsbs & mask) + __popc(msbs & mask)) + qb * uint32_t(sub) + s_plane_off[grp];
-			const int planes = int(qb + ((cw >> (2 * sub)) & 3u));
-			uint32_t dec[8] = {0, 0, 0, 0, 0, 0, 0, 0};
-			if (planes <= 16)
-			{
-				// Plane bytes (most significant first) as the rows of two 8x8 bit
-				// matrices; transposed, byte i holds coefficient i's magnitude bits.
-				unsigned long long lo = 0, hi = 0;
-				for (int pl = planes - 1; pl >= 0; pl--)
-				{
-					const unsigned long long bits = rd.u8(byte_offset++);
-					if (pl < 8)
-						lo |= bits << (8 * pl);
-					else
-						hi |= bits << (8 * (pl - 8));
-				}
-				lo = transpose8x8(lo);
-				hi = transpose8x8(hi);
-#pragma unroll
-				for (int i = 0; i < 8; i++)
-					dec[i] = uint32_t((lo >> (8 * i)) & 0xffu) | (uint32_t((hi >> (8 * i)) & 0xffu) << 8);
-			}
-			else
-			{
-				// Only a malformed header gives more than 16 planes.
-				for (int pl = planes - 1; pl >= 0; pl--)
-				{
-					const uint32_t bits = rd.u8(byte_offset++);
-#pragma unroll
-					for (int i = 0; i < 8; i++)
-						dec[i] |= ((bits >> i) & 1u) << pl;
-				}
-			}
-#pragma unroll
-			for (int i = 0; i < 8; i++)
-			{
-				float f = float(dec[i]);
-				if (f != 0.0f)
-					f = __fadd_rn(f, 0.5f);
-				v[i] = f;
-			}
-		}
-		const float inv_scale = __fmul_rn(decode_quant(q_code), decode_quant_scale((cw2 >> 4) & 0xfu));
+		const int grp = (ly0 + h * kRowStep) * 4 + lx;
 #pragma unroll
 		for (int i = 0; i < 8; i++)
-			v[i] = __fmul_rn(v[i], inv_scale);
-	}
-
-	// Sign bits: position = number of significant coefficients before this one.
-	uint32_t nsig = 0;
-#pragma unroll
-	for (int i = 0; i < 8; i++)
-		nsig += v[i] != 0.0f ? 1u : 0u;
-	uint32_t inc = nsig;
-#pragma unroll
-	for (int o = 1; o < 32; o *= 2)
-	{
-		const uint32_t y = __shfl_up_sync(0xffffffffu, inc, o);
-		if (lane >= o)
-			inc += y;
-	}
-	if (lane == 31)
-		s_sig[ly] = inc;
-	group_sync(bar);
-	uint32_t bitpos = s_sign_base + inc - nsig;
-	for (int w = 0; w < ly; w++)
-		bitpos += s_sig[w];
-	// This thread's (at most 8) sign bits are consecutive: one 64-bit window.
-	const uint32_t sw = bitpos >> 5, shift = bitpos & 31u;
-	const uint64_t window = (uint64_t(rd.w32(sw + 1)) << 32 | rd.w32(sw)) >> shift;
-	int nth = 0;
-#pragma unroll
-	for (int i = 0; i < 8; i++)
-	{
-		if (v[i] != 0.0f)
+			v[h][i] = 0.0f;
+		if ((ballot >> grp) & 1u)
 		{
-			if ((window >> nth) & 1u)
-				v[i] = -v[i];
-			nth++;
+			const uint32_t local = uint32_t(__popc(ballot & ((1u << grp) - 1u)));
+			const uint32_t cw = rd.u16(off * 2 + 4 + local);
+			const uint32_t cw2 = rd.u8(off * 4 + 8 + n * 2 + local);
+			const uint32_t qb = cw2 & 0xfu;
+			if (cw != 0)
+			{
+				const uint32_t mask = (1u << (2 * sub)) - 1u;
+				const uint32_t lsbs = cw & 0x5555u;
+				uint32_t msbs = cw & 0xaaaau;
+				msbs |= msbs >> 1;
+				uint32_t byte_offset =
+				    uint32_t(__popc(lsbs & mask) + __popc(msbs & mask)) + qb * uint32_t(sub) + s_plane_off[grp];
+				const int planes = int(qb + ((cw >> (2 * sub)) & 3u));
+				uint32_t dec[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+				if (planes <= 16)
+				{
+					// Plane bytes (most significant first) as the rows of two 8x8 bit
+					// matrices; transposed, byte i holds coefficient i's magnitude bits.
+					unsigned long long lo = 0, hi = 0;
+					for (int pl = planes - 1; pl >= 0; pl--)
+					{
+						const unsigned long long bits = rd.u8(byte_offset++);
+						if (pl < 8)
+							lo |= bits << (8 * pl);
+						else
+							hi |= bits << (8 * (pl - 8));
+					}
+					lo = transpose8x8(lo);
+					hi = transpose8x8(hi);
+#pragma unroll
+					for (int i = 0; i < 8; i++)
+						dec[i] = uint32_t((lo >> (8 * i)) & 0xffu) | (uint32_t((hi >> (8 * i)) & 0xffu) << 8);
+				}
+				else
+				{
+					// Only a malformed header gives more than 16 planes.
+					for (int pl = planes - 1; pl >= 0; pl--)
+					{
+						const uint32_t bits = rd.u8(byte_offset++);
+#pragma unroll
+						for (int i = 0; i < 8; i++)
+							dec[i] |= ((bits >> i) & 1u) << pl;
+					}
+				}
+#pragma unroll
+				for (int i = 0; i < 8; i++)
+				{
+					float f = float(dec[i]);
+					if (f != 0.0f)
+						f = __fadd_rn(f, 0.5f);
+					v[h][i] = f;
+				}
+			}
+			const float inv_scale = __fmul_rn(decode_quant(q_code), decode_quant_scale((cw2 >> 4) & 0xfu));
+#pragma unroll
+			for (int i = 0; i < 8; i++)
+				v[h][i] = __fmul_rn(v[h][i], inv_scale);
 		}
 	}
-	store_subblock(in.coef32, in.coef16, f16, B.offset + int64_t(oy) * L.pitch + ox, L.pitch, v);
+
+	// Sign bits: position = number of significant coefficients before this one
+	// (in sub-block order: 8x8 rows, then the 32 sub-blocks of a row).
+	uint32_t nsig[kSubs], inc[kSubs];
+#pragma unroll
+	for (int h = 0; h < kSubs; h++)
+	{
+		nsig[h] = 0;
+#pragma unroll
+		for (int i = 0; i < 8; i++)
+			nsig[h] += v[h][i] != 0.0f ? 1u : 0u;
+		inc[h] = nsig[h];
+#pragma unroll
+		for (int o = 1; o < 32; o *= 2)
+		{
+			const uint32_t y = __shfl_up_sync(0xffffffffu, inc[h], o);
+			if (lane >= o)
+				inc[h] += y;
+		}
+		if (lane == 31)
+			s_sig[ly0 + h * kRowStep] = inc[h];
+	}
+	block_sync<kSubs>(bar);
+#pragma unroll
+	for (int h = 0; h < kSubs; h++)
+	{
+		const int ly = ly0 + h * kRowStep;
+		uint32_t bitpos = s_sign_base + inc[h] - nsig[h];
+		for (int w = 0; w < ly; w++)
+			bitpos += s_sig[w];
+		// This thread's (at most 8) sign bits are consecutive: one 64-bit window.
+		const uint32_t sw = bitpos >> 5, shift = bitpos & 31u;
+		const uint64_t window = (uint64_t(rd.w32(sw + 1)) << 32 | rd.w32(sw)) >> shift;
+		int nth = 0;
+#pragma unroll
+		for (int i = 0; i < 8; i++)
+		{
+			if (v[h][i] != 0.0f)
+			{
+				if ((window >> nth) & 1u)
+					v[h][i] = -v[h][i];
+				nth++;
+			}
+		}
+		const int oy = by32 * 32 + ly * 8 + sub_y(sub);
+		store_subblock(in.coef32, in.coef16, f16, B.offset + int64_t(oy) * L.pitch + ox, L.pitch, v[h]);
+	}
 }
 
 constexpr int kBandTile = 36; // 32 band samples + 2 on each side

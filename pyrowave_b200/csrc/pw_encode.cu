@@ -1339,11 +1339,17 @@ struct PackShared
 	float s_inv_scale[16];
 };
 
-// One 32x32 block on a group of 128 threads (threadIdx.x & 127), synchronised
-// with hardware barrier `bar`.
+// One 32x32 block on a group of 128 / kSubs threads: with kSubs = 1 the group
+// is threadIdx.x & 127, synchronised with hardware barrier `bar`; with kSubs =
+// 2 the whole 64-thread CTA, each thread packing the sub-blocks of 8x8 rows ly
+// and ly + 2.
+template <int kSubs = 1>
 __device__ __forceinline__ void pack_body(PackShared &sh, const BlockParams &p, const EncodeBuffers &buf, const int blk,
                                           const int bar)
 {
+	static_assert(kSubs == 1 || kSubs == 2, "one or two sub-blocks per thread");
+	constexpr int kGroup = 128 / kSubs;
+	constexpr int kRowStep = 4 / kSubs;
 	uint32_t *const pkt = sh.pkt;
 	uint32_t *const s_ballot = sh.s_ballot;
 	uint32_t *const s_bytes = sh.s_bytes;
@@ -1355,12 +1361,10 @@ __device__ __forceinline__ void pack_body(PackShared &sh, const BlockParams &p, 
 	const LevelDesc &L = p.level[B.level];
 	const int rel = blk - B.block32_offset;
 	const int by32 = rel / B.block32_stride, bx32 = rel - by32 * B.block32_stride;
-	const int t = threadIdx.x & 127, lane = t & 31;
-	const int sub = t & 7, lx = (t >> 3) & 3, ly = t >> 5;
-	const int grp = ly * 4 + lx;
-	const int x8 = bx32 * 4 + lx, y8 = by32 * 4 + ly;
-	const bool in_range = x8 < L.blocks8_x && y8 < L.blocks8_y;
-	const int ox = bx32 * 32 + lx * 8 + sub_x(sub), oy = by32 * 32 + ly * 8 + sub_y(sub);
+	const int t = threadIdx.x & (kGroup - 1), lane = t & 31;
+	const int sub = t & 7, lx = (t >> 3) & 3, ly0 = t >> 5;
+	const int x8 = bx32 * 4 + lx;
+	const int ox = bx32 * 32 + lx * 8 + sub_x(sub);
 	// 1 / (code / 8 + 0.25) for every 4-bit scale code, as the quantiser computed it.
 	if (t < 16)
 		s_inv_scale[t] = __fdiv_rn(1.0f, decode_quant_scale(uint32_t(t)));
@@ -1368,9 +1372,17 @@ __device__ __forceinline__ void pack_body(PackShared &sh, const BlockParams &p, 
 	// The resolve kernel releases this grid only after every quantiser has
 	// finished, so coefficients and code words can be fetched before the wait;
 	// only the rate-control decisions come from the resolve kernel itself.
-	const uint32_t cw0 = in_range ? __ldcg(&buf.code_words[B.block8_offset + y8 * B.block8_stride + x8]) : 0u;
-	float coef[8];
-	load_subblock(buf.coef32, buf.coef16, L.fp16 != 0, B.offset + int64_t(oy) * L.pitch + ox, L.pitch, coef);
+	uint32_t cw0[kSubs];
+	float coef[kSubs][8];
+#pragma unroll
+	for (int h = 0; h < kSubs; h++)
+	{
+		const int ly = ly0 + h * kRowStep, y8 = by32 * 4 + ly;
+		const bool in_range = x8 < L.blocks8_x && y8 < L.blocks8_y;
+		const int oy = by32 * 32 + ly * 8 + sub_y(sub);
+		cw0[h] = in_range ? __ldcg(&buf.code_words[B.block8_offset + y8 * B.block8_stride + x8]) : 0u;
+		load_subblock(buf.coef32, buf.coef16, L.fp16 != 0, B.offset + int64_t(oy) * L.pitch + ox, L.pitch, coef[h]);
+	}
 	pdl_wait();
 
 	const uint2 meta = __ldcg(reinterpret_cast<const uint2 *>(buf.block_meta) + blk);
@@ -1379,70 +1391,80 @@ __device__ __forceinline__ void pack_body(PackShared &sh, const BlockParams &p, 
 	if (words == 0)
 		return;
 	const uint32_t offset = meta.x;
-	const uint32_t cw = quantize_code_word(cw0, quant);
-	const bool active = (cw & 0xffffu) != 0;
-	group_sync(bar); // s_inv_scale
+	block_sync<kSubs>(bar); // s_inv_scale
 
-	// Re-quantise this sub-block exactly as the quantiser did.
-	const float qs = s_inv_scale[(cw0 >> kQuantScaleOffset) & 0xfu];
-	uint32_t mag[8];
-	uint32_t neg = 0;
+	// Re-quantise the thread's sub-blocks exactly as the quantiser did.
+	uint32_t cw[kSubs], mag[kSubs][8], neg[kSubs], planes[kSubs], sig[kSubs];
+	bool active[kSubs];
 #pragma unroll
-	for (int i = 0; i < 8; i++)
+	for (int h = 0; h < kSubs; h++)
 	{
-		const float c = coef[i];
-		float v = __fmul_rn(__fmul_rn(c, B.quant_resolution), qs);
-		v = fminf(fmaxf(v, -kMaxScaledMagnitude), kMaxScaledMagnitude);
-		mag[i] = uint32_t(abs(int(v)));
-		if (v < 0.0f)
-			neg |= 1u << i;
-	}
-	const uint32_t out_q = (cw >> kQPlanesOffset) & 0xfu;
-	const uint32_t planes = active ? ((cw >> (2 * sub)) & 3u) + out_q : 0u;
-	uint32_t sig = 0;
-	if (planes != 0)
-	{
+		cw[h] = quantize_code_word(cw0[h], quant);
+		active[h] = (cw[h] & 0xffffu) != 0;
+		const float qs = s_inv_scale[(cw0[h] >> kQuantScaleOffset) & 0xfu];
+		neg[h] = 0;
 #pragma unroll
 		for (int i = 0; i < 8; i++)
-			if ((mag[i] >> quant) != 0)
-				sig |= 1u << i;
+		{
+			float v = __fmul_rn(__fmul_rn(coef[h][i], B.quant_resolution), qs);
+			v = fminf(fmaxf(v, -kMaxScaledMagnitude), kMaxScaledMagnitude);
+			mag[h][i] = uint32_t(abs(int(v)));
+			if (v < 0.0f)
+				neg[h] |= 1u << i;
+		}
+		const uint32_t out_q = (cw[h] >> kQPlanesOffset) & 0xfu;
+		planes[h] = active[h] ? ((cw[h] >> (2 * sub)) & 3u) + out_q : 0u;
+		sig[h] = 0;
+		if (planes[h] != 0)
+		{
+#pragma unroll
+			for (int i = 0; i < 8; i++)
+				if ((mag[h][i] >> quant) != 0)
+					sig[h] |= 1u << i;
+		}
 	}
 
-	const uint32_t wb = __ballot_sync(0xffffffffu, active && sub == 0);
-	if (lane == 0)
-		s_ballot[ly] = ((wb >> 0) & 1u) | ((wb >> 7) & 2u) | ((wb >> 14) & 4u) | ((wb >> 21) & 8u);
-	if (sub == 0)
-		s_bytes[grp] = required_8x8_bytes(cw);
-
-	// Exclusive prefix of significant coefficients over threads 0..127.
-	const uint32_t nsig = uint32_t(__popc(sig));
-	uint32_t inc = nsig;
+	// Per 8x8 row (one warp per row): the ballot of coded 8x8s, their plane
+	// bytes, and the inclusive prefix of significant coefficients.
+	uint32_t nsig[kSubs], inc[kSubs], sub_plane_offset[kSubs];
 #pragma unroll
-	for (int off = 1; off < 32; off *= 2)
+	for (int h = 0; h < kSubs; h++)
 	{
-		const uint32_t y = __shfl_up_sync(0xffffffffu, inc, off);
-		if (lane >= off)
-			inc += y;
-	}
-	if (lane == 31)
-		s_sig[ly] = inc;
-	// Exclusive prefix of plane bytes over the 8 sub-blocks of this 8x8.
-	uint32_t pinc = planes;
+		const int ly = ly0 + h * kRowStep, grp = ly * 4 + lx;
+		const uint32_t wb = __ballot_sync(0xffffffffu, active[h] && sub == 0);
+		if (lane == 0)
+			s_ballot[ly] = ((wb >> 0) & 1u) | ((wb >> 7) & 2u) | ((wb >> 14) & 4u) | ((wb >> 21) & 8u);
+		if (sub == 0)
+			s_bytes[grp] = required_8x8_bytes(cw[h]);
+		nsig[h] = uint32_t(__popc(sig[h]));
+		inc[h] = nsig[h];
 #pragma unroll
-	for (int off = 1; off < 8; off *= 2)
-	{
-		const uint32_t y = __shfl_up_sync(0xffffffffu, pinc, off);
-		if (sub >= off)
-			pinc += y;
+		for (int off = 1; off < 32; off *= 2)
+		{
+			const uint32_t y = __shfl_up_sync(0xffffffffu, inc[h], off);
+			if (lane >= off)
+				inc[h] += y;
+		}
+		if (lane == 31)
+			s_sig[ly] = inc[h];
+		// Exclusive prefix of plane bytes over the 8 sub-blocks of this 8x8.
+		uint32_t pinc = planes[h];
+#pragma unroll
+		for (int off = 1; off < 8; off *= 2)
+		{
+			const uint32_t y = __shfl_up_sync(0xffffffffu, pinc, off);
+			if (sub >= off)
+				pinc += y;
+		}
+		sub_plane_offset[h] = pinc - planes[h];
 	}
-	const uint32_t sub_plane_offset = pinc - planes;
-	for (int w = t; w < int(words) && w < kMaxBlockWords; w += 128)
+	for (int w = t; w < int(words) && w < kMaxBlockWords; w += kGroup)
 		pkt[w] = 0u;
-	group_sync(bar);
+	block_sync<kSubs>(bar);
 
 	const uint32_t ballot = s_ballot[0] | (s_ballot[1] << 4) | (s_ballot[2] << 8) | (s_ballot[3] << 12);
 	const uint32_t n = uint32_t(__popc(ballot));
-	// Plane bytes before this 8x8 and in total: a 16-lane inclusive scan in every warp.
+	// Plane bytes before each 8x8 and in total: a 16-lane inclusive scan in every warp.
 	uint32_t scan_bytes = s_bytes[lane & 15];
 #pragma unroll
 	for (int off = 1; off < 16; off *= 2)
@@ -1452,12 +1474,7 @@ __device__ __forceinline__ void pack_body(PackShared &sh, const BlockParams &p, 
 			scan_bytes += y;
 	}
 	const uint32_t total_bytes = __shfl_sync(0xffffffffu, scan_bytes, 15);
-	const uint32_t excl_bytes = __shfl_sync(0xffffffffu, scan_bytes, grp) - s_bytes[grp];
-	uint32_t sig_base = 0;
-	for (int w = 0; w < ly; w++)
-		sig_base += s_sig[w];
 	const uint32_t total_sig = s_sig[0] + s_sig[1] + s_sig[2] + s_sig[3];
-	const uint32_t sig_excl = sig_base + inc - nsig;
 
 	uint8_t *bytes = reinterpret_cast<uint8_t *>(pkt);
 	if (t == 0)
@@ -1465,52 +1482,65 @@ __device__ __forceinline__ void pack_body(PackShared &sh, const BlockParams &p, 
 		pkt[0] = (ballot & 0xffffu) | (words << 16) | ((__ldcg(&buf.rc->sequence) & 7u) << 28);
 		pkt[1] = modify_quant_code(B.quant_code, quant) | (uint32_t(blk) << 8);
 	}
-	if (active && sub == 0)
-	{
-		const uint32_t compact = uint32_t(__popc(ballot & ((1u << grp) - 1u)));
-		bytes[8 + 2 * compact + 0] = uint8_t(cw);
-		bytes[8 + 2 * compact + 1] = uint8_t(cw >> 8);
-		bytes[8 + 2 * n + compact] = uint8_t(cw >> 16);
-	}
-	const uint32_t plane_base = 8 + 3 * n + excl_bytes + sub_plane_offset;
-	if (planes != 0)
-	{
-		// Bit plane k of the 8 magnitudes is byte k of the transposed bit matrix
-		// whose byte i holds the magnitude of coefficient i (low and high 8 bits).
-		unsigned long long lo = 0, hi = 0;
+	uint32_t sig_excl[kSubs];
 #pragma unroll
-		for (int i = 0; i < 8; i++)
+	for (int h = 0; h < kSubs; h++)
+	{
+		const int ly = ly0 + h * kRowStep, grp = ly * 4 + lx;
+		const uint32_t excl_bytes = __shfl_sync(0xffffffffu, scan_bytes, grp) - s_bytes[grp];
+		uint32_t sig_base = 0;
+		for (int w = 0; w < ly; w++)
+			sig_base += s_sig[w];
+		sig_excl[h] = sig_base + inc[h] - nsig[h];
+		if (active[h] && sub == 0)
 		{
-			lo |= (unsigned long long)(mag[i] & 0xffu) << (8 * i);
-			hi |= (unsigned long long)((mag[i] >> 8) & 0xffu) << (8 * i);
+			const uint32_t compact = uint32_t(__popc(ballot & ((1u << grp) - 1u)));
+			bytes[8 + 2 * compact + 0] = uint8_t(cw[h]);
+			bytes[8 + 2 * compact + 1] = uint8_t(cw[h] >> 8);
+			bytes[8 + 2 * n + compact] = uint8_t(cw[h] >> 16);
 		}
-		lo = transpose8x8(lo);
-		hi = transpose8x8(hi);
-		for (uint32_t pl = 0; pl < planes; pl++)
+		const uint32_t plane_base = 8 + 3 * n + excl_bytes + sub_plane_offset[h];
+		if (planes[h] != 0)
 		{
-			const uint32_t bit = uint32_t(quant) + planes - 1u - pl; // most significant plane first
-			const uint32_t by = bit < 8 ? uint32_t(lo >> (8 * bit)) : (bit < 16 ? uint32_t(hi >> (8 * (bit - 8))) : 0u);
-			if (plane_base + pl < uint32_t(kMaxBlockWords) * 4)
-				bytes[plane_base + pl] = uint8_t(by);
+			// Bit plane k of the 8 magnitudes is byte k of the transposed bit matrix
+			// whose byte i holds the magnitude of coefficient i (low and high 8 bits).
+			unsigned long long lo = 0, hi = 0;
+#pragma unroll
+			for (int i = 0; i < 8; i++)
+			{
+				lo |= (unsigned long long)(mag[h][i] & 0xffu) << (8 * i);
+				hi |= (unsigned long long)((mag[h][i] >> 8) & 0xffu) << (8 * i);
+			}
+			lo = transpose8x8(lo);
+			hi = transpose8x8(hi);
+			for (uint32_t pl = 0; pl < planes[h]; pl++)
+			{
+				const uint32_t bit = uint32_t(quant) + planes[h] - 1u - pl; // most significant plane first
+				const uint32_t by = bit < 8 ? uint32_t(lo >> (8 * bit)) : (bit < 16 ? uint32_t(hi >> (8 * (bit - 8))) : 0u);
+				if (plane_base + pl < uint32_t(kMaxBlockWords) * 4)
+					bytes[plane_base + pl] = uint8_t(by);
+			}
 		}
 	}
-	group_sync(bar);
+	block_sync<kSubs>(bar);
 
 	// Sign bits of significant coefficients, in coefficient order, after the planes.
-	// This thread's sign bits are consecutive in the stream: gather them (sign
+	// A sub-block's sign bits are consecutive in the stream: gather them (sign
 	// of each significant coefficient, in order) and OR them in with at most two
 	// word updates.
+#pragma unroll
+	for (int h = 0; h < kSubs; h++)
 	{
-		const uint32_t bitpos = (8 + 3 * n + total_bytes) * 8 + sig_excl;
+		const uint32_t bitpos = (8 + 3 * n + total_bytes) * 8 + sig_excl[h];
 		uint32_t bits = 0;
-		int k = 0;
+		int kk = 0;
 #pragma unroll
 		for (int i = 0; i < 8; i++)
 		{
-			if ((sig >> i) & 1u)
+			if ((sig[h] >> i) & 1u)
 			{
-				bits |= ((neg >> i) & 1u) << k;
-				k++;
+				bits |= ((neg[h] >> i) & 1u) << kk;
+				kk++;
 			}
 		}
 		const uint32_t w = bitpos >> 5, shift = bitpos & 31u;
@@ -1521,7 +1551,7 @@ __device__ __forceinline__ void pack_body(PackShared &sh, const BlockParams &p, 
 				atomicOr(&pkt[w + 1], bits >> (32u - shift));
 		}
 	}
-	group_sync(bar);
+	block_sync<kSubs>(bar);
 
 	// The word count must match the rate-control estimate the offsets were built from.
 	const uint32_t bits = 8 * (3 * n + total_bytes) + total_sig;
@@ -1532,14 +1562,18 @@ __device__ __forceinline__ void pack_body(PackShared &sh, const BlockParams &p, 
 	if (!fits)
 		return;
 	uint32_t *dst = buf.stream + 2 + offset;
-	for (int w = t; w < int(words); w += 128)
+	for (int w = t; w < int(words); w += kGroup)
 		dst[w] = pkt[w];
 }
 
-__global__ void __launch_bounds__(128, 12) pack_kernel(const BlockParams p, const EncodeBuffers buf)
+// One 32x32 block per 64-thread CTA, two sub-blocks per thread, registers
+// bounded for 23 CTAs per SM: about twice the blocks resident per SM of
+// 128-thread CTAs (a 1080p frame's 3261 blocks in one wave).
+constexpr int kPackThreads = 64;
+__global__ void __launch_bounds__(kPackThreads, 23) pack_kernel(const BlockParams p, const EncodeBuffers buf)
 {
 	__shared__ PackShared sh;
-	pack_body(sh, p, buf, int(blockIdx.x), 1);
+	pack_body<128 / kPackThreads>(sh, p, buf, int(blockIdx.x), 1);
 }
 
 // Batched form: one CTA per (frame, block).
@@ -1923,7 +1957,7 @@ void launch_resolve(const ResolveParams &p, const EncodeBuffers &buf, cudaStream
 
 void launch_pack(const BlockParams &p, const EncodeBuffers &buf, cudaStream_t stream)
 {
-	LaunchConfig lc(dim3(p.block_count_32x32), dim3(128), stream, true);
+	LaunchConfig lc(dim3(p.block_count_32x32), dim3(kPackThreads), stream, true);
 	cudaLaunchKernelEx(&lc.cfg, pack_kernel, p, buf);
 }
 
