@@ -953,7 +953,7 @@ def _ncu_limit(kernel, cfg):
             "source": e.get("source", "profiles/ncu_traffic.json")}
 
 
-E2E_PAIRS = 3  # encoder/decoder pairs (streams, host threads) in flight in the end-to-end measurement
+E2E_PAIRS = 6  # encoder/decoder pairs (streams, host threads) in flight in the end-to-end measurement
 
 
 def run_e2e(args, cfg, frames, dev):

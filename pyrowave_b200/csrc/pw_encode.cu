@@ -1167,8 +1167,9 @@ __global__ void __launch_bounds__(kThreads) resolve_kernel(const ResolveParams p
 // whole histogram itself (8 KB), so all of them find x* and the requirement
 // with no exchange. The cut and the offsets need prefixes across CTAs: each
 // CTA writes its totals into the shared memory of every higher-ranked CTA
-// (distributed shared memory) and a hardware cluster barrier publishes them,
-// twice per frame. An operation at the x* slot is applied when the exclusive
+// (distributed shared memory) and a hardware cluster barrier publishes them:
+// once for the offsets, and once for the cut unless the x* subdivision lies
+// inside one CTA. An operation at the x* slot is applied when the exclusive
 // prefix of the x* subdivision's savings before its block is below the
 // requirement, which is the same set as the blocks before the cut. Results are
 // those of resolve_body.
@@ -1245,12 +1246,19 @@ __global__ void __launch_bounds__(kClusterResolveThreads, 1)
 		}
 		uint32_t cta_total;
 		uint32_t ex = block_exclusive_scan(local, warp_sums, cta_total);
-		if (t < int(ncta) && t > int(rank))
-			st_cluster_u64(&s_saving_totals[rank], uint32_t(t), cta_total);
-		cluster_sync();
+		// When the x* subdivision lies inside one CTA's blocks (every CTA sees
+		// the same x*, so all take the same branch), the other CTAs hold none of
+		// its savings and the prefix needs no exchange.
+		const int cta_blocks = per * kClusterResolveThreads;
 		uint64_t base = 0;
-		for (uint32_t r = 0; r < rank; r++)
-			base += s_saving_totals[r];
+		if (start / cta_blocks != (end - 1) / cta_blocks)
+		{
+			if (t < int(ncta) && t > int(rank))
+				st_cluster_u64(&s_saving_totals[rank], uint32_t(t), cta_total);
+			cluster_sync();
+			for (uint32_t r = 0; r < rank; r++)
+				base += s_saving_totals[r];
+		}
 #pragma unroll
 		for (int i = 0; i < R; i++)
 		{
