@@ -167,6 +167,37 @@ __device__ __forceinline__ uint32_t ld_acquire_u32(const uint32_t *p)
 	return v;
 }
 
+// Orders this thread's generic-proxy view of global memory (data other CTAs
+// stored, observed through an acquire) before its later async-proxy (TMA) reads.
+__device__ __forceinline__ void fence_proxy_async_global() { asm volatile("fence.proxy.async.global;" ::: "memory"); }
+
+// Bounded wait until a counter reaches `target` (one thread). Returns false
+// when it gave up after kDataflowWaitSpins polls.
+__device__ __forceinline__ bool wait_counter(const uint32_t *c, uint32_t target)
+{
+	uint32_t spins = 0;
+	while (ld_acquire_u32(c) < target)
+	{
+		if (++spins > kDataflowWaitSpins)
+			return false;
+		__nanosleep(64);
+	}
+	return true;
+}
+
+// Adds one to a counter once every thread of the CTA has stored its part
+// (called by every thread; the barrier orders the CTA's stores before the
+// fence of thread 0).
+__device__ __forceinline__ void cta_count_done(uint32_t *c)
+{
+	__syncthreads();
+	if (threadIdx.x == 0)
+	{
+		__threadfence();
+		atomicAdd(c, 1u);
+	}
+}
+
 // GPU-scope acquire load / release store of a 64-bit word (flags between CTAs).
 __device__ __forceinline__ unsigned long long ld_acquire_u64(const unsigned long long *p)
 {

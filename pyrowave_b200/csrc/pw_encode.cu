@@ -85,6 +85,22 @@ __device__ __forceinline__ void quant_analyze_block(const float *tile, int tile_
 	max_sub = fminf(__fmul_rn(max_sub, qs), kMaxScaledMagnitude);
 	max_wave = fminf(__fmul_rn(max_wave, qs), kMaxScaledMagnitude);
 
+	// The packer's input: the scaled values as sign-magnitude (|int(v)| <= 32767),
+	// one 16-byte store per sub-block, written by the first thread of each.
+	if (active && r == 0 && buf.mag16)
+	{
+		uint32_t w[4];
+#pragma unroll
+		for (int j = 0; j < 4; j++)
+		{
+			const uint32_t a = uint32_t(int(fabsf(v[2 * j]))) | (v[2 * j] < 0.0f ? 0x8000u : 0u);
+			const uint32_t b = uint32_t(int(fabsf(v[2 * j + 1]))) | (v[2 * j + 1] < 0.0f ? 0x8000u : 0u);
+			w[j] = a | (b << 16);
+		}
+		const int blk = B.block32_offset + by32 * B.block32_stride + bx32;
+		*reinterpret_cast<uint4 *>(buf.mag16 + int64_t(blk) * 1024 + 8 * (t & 127)) = make_uint4(w[0], w[1], w[2], w[3]);
+	}
+
 	const float overall = __fmul_rn(qres, qs);
 	const float inv_quant = __fdiv_rn(1.0f, overall);
 	const float iqs = __fmul_rn(inv_quant, inv_quant);
@@ -346,6 +362,42 @@ template <int kThreads> struct DwtSplit
 // quantise the three high bands of a tile in one round, measured no faster.
 constexpr int kLargeLevelThreads = 256;
 
+// Tile dataflow: waits (bounded) until every tile of the finer level whose LL
+// samples this CTA reads has been stored. The rows and columns read are those
+// of the index tables (mirrored at the edges), so the tiles are the ranges
+// their minimum and maximum fall in: at most 4 x 4 for a whole tile. Called by
+// every thread after the index tables are built; ends with a CTA barrier.
+template <int kRowsIn>
+__device__ __forceinline__ void wait_finer_tiles(const DwtShared &sh, const LevelParams &p, const EncodeBuffers &buf,
+                                                 const int comp, const int r0)
+{
+	if (threadIdx.x < 32)
+	{
+		const int lane = threadIdx.x;
+		int ylo = 0x7fffffff, yhi = 0, xlo = 0x7fffffff, xhi = 0;
+		for (int i = lane; i < kRowsIn; i += 32)
+		{
+			ylo = min(ylo, sh.yidx[r0 + i]);
+			yhi = max(yhi, sh.yidx[r0 + i]);
+		}
+		for (int i = lane; i < kTileIn; i += 32)
+		{
+			xlo = min(xlo, sh.xidx[i]);
+			xhi = max(xhi, sh.xidx[i]);
+		}
+		const int ty0 = __reduce_min_sync(0xffffffffu, ylo) >> 5, ty1 = __reduce_max_sync(0xffffffffu, yhi) >> 5;
+		const int tx0 = __reduce_min_sync(0xffffffffu, xlo) >> 5, tx1 = __reduce_max_sync(0xffffffffu, xhi) >> 5;
+		const int w = tx1 - tx0 + 1, n = w * (ty1 - ty0 + 1);
+		const uint32_t *base = buf.tile_done + p.prev_done_offset + comp * p.P.tiles_x * p.P.tiles_y;
+		bool ok = true;
+		for (int k = lane; k < n && ok; k += 32)
+			ok = wait_counter(base + (ty0 + k / w) * p.P.tiles_x + tx0 + k % w, uint32_t(p.prev_parts));
+		if (!__all_sync(0xffffffffu, ok) && lane == 0)
+			atomicOr(&buf.rc->error, kErrorLevelWait);
+	}
+	__syncthreads();
+}
+
 // One forward level for one 32x32 band tile of one component (64x64 input
 // samples): `tile` in row-major tile order, `comp_index` the component among
 // those at this level. Run by every thread of a kThreads-thread CTA. With
@@ -436,7 +488,15 @@ __device__ __forceinline__ void dwt_forward_body(DwtShared &sh, const LevelParam
 		prefetch_tensor_map(tmap);
 	}
 	__syncthreads();
-	pdl_wait();
+	if (buf.tile_done)
+	{
+		// Tile dataflow: the input planes are complete before the frame's first
+		// kernel; the finer level's LL is read once the tiles it comes from are.
+		if (!from_plane)
+			wait_finer_tiles<kRowsIn>(sh, p, buf, comp, r0);
+	}
+	else
+		pdl_wait();
 	if (from_plane)
 	{
 		if (in.sample16)
@@ -512,6 +572,8 @@ __device__ __forceinline__ void dwt_forward_body(DwtShared &sh, const LevelParam
 	{
 		if (threadIdx.x == 0)
 		{
+			if (buf.tile_done)
+				fence_proxy_async_global(); // LL stored by other CTAs, observed through the counters
 			mbarrier_expect_tx(&sh.tile_bar, kInBoxBytes);
 			tma_load_2d(&sh.in[0][0], tmap, x0, maps->row[comp][0] + y0, &sh.tile_bar);
 		}
@@ -680,6 +742,8 @@ __device__ __forceinline__ void dwt_forward_body(DwtShared &sh, const LevelParam
 		}
 	}
 
+	if (buf.tile_done)
+		cta_count_done(buf.tile_done + p.done_offset + comp * L.tiles_x * L.tiles_y + tile);
 	if (kStripes > 1 || !fused)
 		return;
 
@@ -711,6 +775,13 @@ __device__ __forceinline__ void dwt_forward_body(DwtShared &sh, const LevelParam
 			quant_analyze_block<2 * Split::kQSplit>(&bands[band][0][0], kBandPitch, true, int(threadIdx.x), sh.q[0],
 			                                        L, p.band[comp][band], p.subdivision_shift, tx, ty, buf);
 		}
+	}
+	// Tile dataflow: the resolve waits for every fused quantiser (the last
+	// round ended with a CTA barrier after its statistics were stored).
+	if (buf.tile_done && threadIdx.x == 0)
+	{
+		__threadfence();
+		atomicAdd(&buf.rc->fused_done, 1u);
 	}
 }
 
@@ -780,7 +851,15 @@ __device__ __forceinline__ void quant_blocks_body(const BlockParams &p, const En
 	const LevelDesc &L = p.level[E.level];
 	const int rel = b - E.block32_offset;
 	const int by = rel / E.block32_stride, bx = rel - by * E.block32_stride;
-	pdl_wait();
+	if (buf.tile_done)
+	{
+		// Tile dataflow: the block's transform tile is stored once its counter is complete.
+		if (active && t == 0 && !wait_counter(buf.tile_done + E.done_index + rel, uint32_t(E.done_parts)))
+			atomicOr(&buf.rc->error, kErrorLevelWait);
+		__syncthreads();
+	}
+	else
+		pdl_wait();
 	if (active)
 	{
 		// The block's 32 rows as 8 vectors of 4 each, every load in flight at once.
@@ -997,6 +1076,18 @@ __device__ __forceinline__ void load_rows(const EncodeBuffers &buf, int b0, int 
 			r[i] = load_raw_rd(buf, b0 + i);
 }
 
+// Tile dataflow: the forward levels with a fused quantiser may still run when
+// the resolve starts (its wait covers only the launch before it); wait, bounded,
+// until each has counted its quantiser finished. Called by every thread.
+__device__ __forceinline__ void wait_fused_quantisers(const ResolveParams &p, RateControlState *rc)
+{
+	if (p.fused_ctas == 0)
+		return;
+	if (threadIdx.x == 0 && !wait_counter(&rc->fused_done, p.fused_ctas))
+		atomicOr(&rc->error, kErrorLevelWait);
+	__syncthreads();
+}
+
 __device__ __forceinline__ void resolve_body(const ResolveParams &p, const EncodeBuffers &buf, const int slice,
                                              const int nslices)
 {
@@ -1015,9 +1106,11 @@ __device__ __forceinline__ void resolve_body(const ResolveParams &p, const Encod
 	const int s0 = min(slice * slice_blocks, nblocks), s1 = min(s0 + slice_blocks, nblocks);
 	const int per = (s1 - s0 + nthreads - 1) / nthreads;
 	const int b0 = min(s0 + t * per, s1), b1 = min(b0 + per, s1);
-	// Every quantiser has finished once the wait returns. The packer is released
-	// only then, because it reads their output before its own wait.
+	// Every quantiser has finished once the wait returns (with the tile dataflow,
+	// the fused ones once their count is complete). The packer is released only
+	// then, because it reads their output before its own wait.
 	pdl_wait();
+	wait_fused_quantisers(p, rc);
 	pdl_trigger();
 
 	RawRD own[kOwnBatch];
@@ -1195,6 +1288,7 @@ __global__ void __launch_bounds__(kClusterResolveThreads, 1)
 	const int per = (n + int(ncta) * kClusterResolveThreads - 1) / (int(ncta) * kClusterResolveThreads); // <= R
 	const int b0 = min((int(rank) * kClusterResolveThreads + t) * per, n), b1 = min(b0 + per, n);
 	pdl_wait();
+	wait_fused_quantisers(p, rc);
 	pdl_trigger();
 
 	RawRD rows[R];
@@ -1344,7 +1438,6 @@ struct PackShared
 	uint32_t s_ballot[4];
 	uint32_t s_bytes[16];
 	uint32_t s_sig[4];
-	float s_inv_scale[16];
 };
 
 // One 32x32 block on a group of 128 / kSubs threads: with kSubs = 1 the group
@@ -1362,7 +1455,6 @@ __device__ __forceinline__ void pack_body(PackShared &sh, const BlockParams &p, 
 	uint32_t *const s_ballot = sh.s_ballot;
 	uint32_t *const s_bytes = sh.s_bytes;
 	uint32_t *const s_sig = sh.s_sig;
-	float *const s_inv_scale = sh.s_inv_scale;
 	pdl_trigger();
 	const int k = find_band(p, blk);
 	const BandEntry &B = p.band[k];
@@ -1372,24 +1464,19 @@ __device__ __forceinline__ void pack_body(PackShared &sh, const BlockParams &p, 
 	const int t = threadIdx.x & (kGroup - 1), lane = t & 31;
 	const int sub = t & 7, lx = (t >> 3) & 3, ly0 = t >> 5;
 	const int x8 = bx32 * 4 + lx;
-	const int ox = bx32 * 32 + lx * 8 + sub_x(sub);
-	// 1 / (code / 8 + 0.25) for every 4-bit scale code, as the quantiser computed it.
-	if (t < 16)
-		s_inv_scale[t] = __fdiv_rn(1.0f, decode_quant_scale(uint32_t(t)));
 
 	// The resolve kernel releases this grid only after every quantiser has
-	// finished, so coefficients and code words can be fetched before the wait;
-	// only the rate-control decisions come from the resolve kernel itself.
+	// finished, so the quantised magnitudes and code words can be fetched before
+	// the wait; only the rate-control decisions come from the resolve kernel itself.
 	uint32_t cw0[kSubs];
-	float coef[kSubs][8];
+	uint4 sm[kSubs];
 #pragma unroll
 	for (int h = 0; h < kSubs; h++)
 	{
 		const int ly = ly0 + h * kRowStep, y8 = by32 * 4 + ly;
 		const bool in_range = x8 < L.blocks8_x && y8 < L.blocks8_y;
-		const int oy = by32 * 32 + ly * 8 + sub_y(sub);
 		cw0[h] = in_range ? __ldcg(&buf.code_words[B.block8_offset + y8 * B.block8_stride + x8]) : 0u;
-		load_subblock(buf.coef32, buf.coef16, L.fp16 != 0, B.offset + int64_t(oy) * L.pitch + ox, L.pitch, coef[h]);
+		sm[h] = __ldcg(reinterpret_cast<const uint4 *>(buf.mag16 + int64_t(blk) * 1024 + 8 * (sub + 8 * lx + 32 * ly)));
 	}
 	pdl_wait();
 
@@ -1399,9 +1486,8 @@ __device__ __forceinline__ void pack_body(PackShared &sh, const BlockParams &p, 
 	if (words == 0)
 		return;
 	const uint32_t offset = meta.x;
-	block_sync<kSubs>(bar); // s_inv_scale
 
-	// Re-quantise the thread's sub-blocks exactly as the quantiser did.
+	// The thread's sub-blocks as the quantiser scaled them (sign-magnitude).
 	uint32_t cw[kSubs], mag[kSubs][8], neg[kSubs], planes[kSubs], sig[kSubs];
 	bool active[kSubs];
 #pragma unroll
@@ -1409,16 +1495,14 @@ __device__ __forceinline__ void pack_body(PackShared &sh, const BlockParams &p, 
 	{
 		cw[h] = quantize_code_word(cw0[h], quant);
 		active[h] = (cw[h] & 0xffffu) != 0;
-		const float qs = s_inv_scale[(cw0[h] >> kQuantScaleOffset) & 0xfu];
+		const uint32_t w[4] = {sm[h].x, sm[h].y, sm[h].z, sm[h].w};
 		neg[h] = 0;
 #pragma unroll
 		for (int i = 0; i < 8; i++)
 		{
-			float v = __fmul_rn(__fmul_rn(coef[h][i], B.quant_resolution), qs);
-			v = fminf(fmaxf(v, -kMaxScaledMagnitude), kMaxScaledMagnitude);
-			mag[h][i] = uint32_t(abs(int(v)));
-			if (v < 0.0f)
-				neg[h] |= 1u << i;
+			const uint32_t x = (w[i >> 1] >> (16 * (i & 1))) & 0xffffu;
+			mag[h][i] = x & 0x7fffu;
+			neg[h] |= (x >> 15) << i;
 		}
 		const uint32_t out_q = (cw[h] >> kQPlanesOffset) & 0xfu;
 		planes[h] = active[h] ? ((cw[h] >> (2 * sub)) & 3u) + out_q : 0u;

@@ -378,8 +378,49 @@ BlockParams make_block_params(const Geometry &g)
 				e.quant_code = B.quant_code;
 				e.rdo_scale = B.rdo_scale;
 				e.level = level;
+				e.comp = comp;
 			}
 	return p;
+}
+
+// Tile dataflow of the single-frame encode: one counter per (level, component,
+// transform tile), components and tiles in order within a level. Fills in the
+// counters' offsets and the count at which each level's tiles are complete
+// (the CTAs storing one tile: row stripes for the small transform-only levels,
+// as launch_dwt_forward_level launches them), and the number of forward-level
+// CTAs with a fused quantiser. Returns the number of counters.
+int setup_tile_dataflow(const Geometry &g, int small_level, LevelParams (&lp)[kLevels], BlockParams &bp,
+                        uint32_t &fused_ctas)
+{
+	int32_t offset[kLevels] = {}, parts[kLevels] = {};
+	int total = 0;
+	fused_ctas = 0;
+	for (int level = 0; level < kLevels; level++)
+	{
+		const int comps = (level == 0 && !g.chroma444) ? 1 : kComponents;
+		const int tiles = comps * g.level[level].tiles_x * g.level[level].tiles_y;
+		offset[level] = total;
+		total += tiles;
+		const bool transform_only = level >= small_level;
+		parts[level] = (transform_only && tiles < kSmallLevelTiles) ? kDwtStripeCtas : 1;
+		if (!transform_only)
+			fused_ctas += uint32_t(tiles);
+	}
+	for (int level = 0; level < kLevels; level++)
+	{
+		lp[level].done_offset = offset[level];
+		lp[level].prev_done_offset = level > 0 ? offset[level - 1] : 0;
+		lp[level].prev_parts = level > 0 ? parts[level - 1] : 0;
+	}
+	for (int i = 0; i < bp.nbands; i++)
+	{
+		BandEntry &e = bp.band[i];
+		const LevelDesc &L = g.level[e.level];
+		const int comp = (e.level == 0 && !g.chroma444) ? 0 : e.comp;
+		e.done_index = offset[e.level] + comp * L.tiles_x * L.tiles_y;
+		e.done_parts = parts[e.level];
+	}
+	return total;
 }
 
 ResolveParams make_resolve_params(const Geometry &g, uint32_t target_words, uint32_t sequence)
@@ -688,6 +729,7 @@ struct pyrowave_encoder_opaque
 	BlockParams bp = {};
 	float *coef32 = nullptr;
 	__half *coef16 = nullptr;
+	uint16_t *mag16 = nullptr;
 	uint32_t *code_words = nullptr;
 	uint16_t *rd_cost = nullptr;
 	uint8_t *rd_bucket = nullptr;
@@ -717,12 +759,19 @@ struct pyrowave_encoder_opaque
 	int small_level = kLevels; // levels >= this: transform only, then one quantiser launch over their blocks
 	int small_blocks = 0;      // 32x32 blocks of those levels (a prefix in block index order)
 	KernelNode node_resolve;
+	// Tile dataflow of the captured encode: counters right after the rate-control
+	// state in the same allocation (one clear covers both).
+	int tile_counters = 0;
+	uint32_t fused_ctas = 0;
+	uint32_t *tile_done() const { return reinterpret_cast<uint32_t *>(rc + 1); }
+	size_t rc_bytes() const { return sizeof(RateControlState) + size_t(tile_counters) * 4; }
 
 	EncodeBuffers buffers() const
 	{
 		EncodeBuffers b;
 		b.coef32 = coef32;
 		b.coef16 = coef16;
+		b.mag16 = mag16;
 		b.code_words = code_words;
 		b.rd_cost = rd_cost;
 		b.rd_bucket = rd_bucket;
@@ -733,6 +782,7 @@ struct pyrowave_encoder_opaque
 		b.stream = stream_buf;
 		b.stream_capacity_words = stream_capacity;
 		b.jobs = jobs_d;
+		b.tile_done = nullptr; // set only for the captured single-frame encode
 		return b;
 	}
 
@@ -742,6 +792,7 @@ struct pyrowave_encoder_opaque
 			cudaStreamSynchronize(device->stream);
 		dev_free(coef32);
 		dev_free(coef16);
+		dev_free(mag16);
 		dev_free(code_words);
 		dev_free(rd_cost);
 		dev_free(rd_bucket);
@@ -766,6 +817,7 @@ struct pyrowave_encoder_opaque
 		graph.destroy();
 		coef32 = nullptr;
 		coef16 = nullptr;
+		mag16 = nullptr;
 		code_words = nullptr;
 		rd_cost = nullptr;
 		rd_bucket = nullptr;
@@ -794,15 +846,17 @@ struct pyrowave_encoder_opaque
 			lp[level] = make_level_params(g, level);
 		bp = make_block_params(g);
 		small_level_split(g, small_level, small_blocks);
+		tile_counters = setup_tile_dataflow(g, small_level, lp, bp, fused_ctas);
 		(void)resolve_cluster_max();
 		bool ok = true;
 		coef32 = dev_alloc<float>(size_t(g.storage_elems32), ok);
 		coef16 = dev_alloc<__half>(size_t(g.storage_elems16), ok);
+		mag16 = dev_alloc<uint16_t>(size_t(g.block_count_32x32) * 1024, ok);
 		code_words = dev_alloc<uint32_t>(size_t(g.block_count_8x8), ok);
 		rd_cost = dev_alloc<uint16_t>(size_t(g.block_count_32x32) * 16, ok);
 		rd_bucket = dev_alloc<uint8_t>(size_t(g.block_count_32x32) * 16, ok);
 		rd_dist = dev_alloc<float>(size_t(g.block_count_32x32) * 16, ok);
-		rc = dev_alloc<RateControlState>(1, ok);
+		rc = reinterpret_cast<RateControlState *>(dev_alloc<uint8_t>(rc_bytes(), ok));
 		quant = dev_alloc<int32_t>(size_t(g.block_count_32x32), ok);
 		block_meta = dev_alloc<uint32_t>(size_t(g.block_count_32x32) * 2, ok);
 		jobs_d = dev_alloc<uint32_t>(jobs.size(), ok);
@@ -875,6 +929,13 @@ struct pyrowave_encoder_opaque
 		return true;
 	}
 
+	ResolveParams dataflow_resolve_params(uint32_t target_words) const
+	{
+		ResolveParams rp = make_resolve_params(g, target_words, sequence_count);
+		rp.fused_ctas = fused_ctas;
+		return rp;
+	}
+
 	// Queue the encode of resident input planes (pyrowave_encoder.cpp:1153-1183).
 	pyrowave_result enqueue(const PlaneInput &in, const pyrowave_rate_control *rc_in, cudaStream_t s)
 	{
@@ -886,6 +947,7 @@ struct pyrowave_encoder_opaque
 			return r;
 		sequence_count = (sequence_count + 1) & 7u;
 		EncodeBuffers b = buffers();
+		b.tile_done = tile_done();
 		timing.collect(device);
 		timing.prepare(device);
 		const uint64_t key = uint64_t(stream_capacity) | (device->stage_timing ? (1ull << 40) : 0ull);
@@ -897,7 +959,7 @@ struct pyrowave_encoder_opaque
 				return PYROWAVE_ERROR_GENERIC;
 			bool ok = true;
 			timing.begin(device, s);
-			cudaMemsetAsync(rc, 0, sizeof(RateControlState), s);
+			cudaMemsetAsync(rc, 0, rc_bytes(), s);
 			static const char *const dwt_tags[kLevels] = {"dwt0", "dwt1", "dwt2", "dwt3", "dwt4"};
 			const bool pdl = !device->stage_timing; // event nodes between kernels break programmatic edges
 			// The small levels (few tiles each) transform only, each level one launch;
@@ -914,7 +976,7 @@ struct pyrowave_encoder_opaque
 				launch_quant_pretransformed(bp, b, small_blocks, pdl, s);
 				timing.mark(device, s, "quant");
 			}
-			launch_resolve(make_resolve_params(g, target_words, sequence_count), b, s);
+			launch_resolve(dataflow_resolve_params(target_words), b, s);
 			ok = ok && last_captured_node(s, node_resolve);
 			timing.mark(device, s, "resolve");
 			launch_pack(bp, b, s);
@@ -930,7 +992,7 @@ struct pyrowave_encoder_opaque
 		else
 		{
 			PlaneInput pin = in;
-			ResolveParams rp = make_resolve_params(g, target_words, sequence_count);
+			ResolveParams rp = dataflow_resolve_params(target_words);
 			bool ok = true;
 			for (int level = 0; level < kLevels; level++)
 			{
@@ -3082,6 +3144,7 @@ pyrowave_result pyrowave_cuda_batch_create(pyrowave_device device, const pyrowav
 		EncodeBuffers &eb = fr.eb;
 		eb.coef32 = b->alloc<float>(size_t(g.storage_elems32), ok);
 		eb.coef16 = nullptr;
+		eb.mag16 = b->alloc<uint16_t>(n32 * 1024, ok);
 		eb.code_words = b->alloc<uint32_t>(n8, ok);
 		eb.rd_cost = b->alloc<uint16_t>(n32 * 16, ok);
 		eb.rd_bucket = b->alloc<uint8_t>(n32 * 16, ok);

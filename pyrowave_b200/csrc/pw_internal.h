@@ -133,6 +133,7 @@ struct RateControlState
 	int32_t xstar;                 // first partially applied bucket*16+subdivision (-1 none)
 	uint32_t sequence;
 	uint32_t decode_error;         // kDecodeError* bits of the batched form's decode of this frame
+	uint32_t fused_done;           // tile dataflow: fused forward-level CTAs whose quantiser finished
 	// Per resolve slice: words << 32 | non-empty blocks << 1 | 1 once published.
 	unsigned long long slice_total[kMaxResolveSlices];
 };
@@ -153,13 +154,18 @@ constexpr uint32_t kErrorStreamCapacity = 1u; // the coded frame does not fit th
 constexpr uint32_t kErrorWordCount = 2u;      // a packed block's size differs from the rate-control estimate
 constexpr uint32_t kErrorSliceWait = 4u;      // a resolve slice gave up waiting for a preceding slice's total
 constexpr uint32_t kErrorTileWait = 8u;       // a forward-transform tile load did not complete in time
-constexpr uint32_t kErrorLevelWait = 16u;     // a work item of the batched launch gave up waiting for the items it depends on
+constexpr uint32_t kErrorLevelWait = 16u;     // a work item gave up waiting for the tiles or items it depends on
 
 // Buffers the encode kernels read and write.
 struct EncodeBuffers
 {
 	float *coef32;
 	__half *coef16;
+	// Per 32x32 block, 1024 values: the quantiser's scaled coefficients as
+	// sign-magnitude (|int(v)| in bits 0-14, v < 0 in bit 15), eight per 4x2
+	// sub-block at [block * 1024 + 8 * (sub + 8 * col8 + 32 * row8) + i], so the
+	// packer reads a sub-block as one 16-byte vector instead of re-quantising.
+	uint16_t *mag16;
 	uint32_t *code_words;   // per 8x8: q=0 code word (plane codes | Q planes << 16 | scale << 20)
 	uint16_t *rd_cost;      // per 32x32 x 16: words when quantised by q
 	uint8_t *rd_bucket;     // per 32x32 x 16: bucket index of the step to q
@@ -170,6 +176,13 @@ struct EncodeBuffers
 	uint32_t *stream;       // packetized output: 2-word sequence header, then blocks
 	uint32_t stream_capacity_words;
 	const uint32_t *jobs;   // per 32x32: pack_job(...)
+	// Tile dataflow of the single-frame encode (null: every kernel waits for the
+	// whole previous grid). One counter per (level, component, transform tile),
+	// cleared with the rate-control state before the frame: each CTA that stores
+	// part of a tile adds one after its stores, and a consumer reads a tile only
+	// once its counter is complete, so a level starts on the tiles whose inputs
+	// exist while the finer level's quantisers still run.
+	uint32_t *tile_done;
 };
 
 // TMA map of one transform level: the frame's FP32 coefficient storage viewed
@@ -248,6 +261,11 @@ struct LevelParams
 	int32_t plane_width[3], plane_height[3];
 	int64_t prev_ll[3];     // offset of LL at level - 1 per component
 	BandParam band[3][4];   // this level's four bands per component
+	// Tile dataflow of the single-frame encode (used when EncodeBuffers::tile_done
+	// is set): this level's tile counters start at done_offset (component-major,
+	// tiles in row-major order), the finer level's at prev_done_offset, and each
+	// finer tile is complete once prev_parts CTAs have counted it.
+	int32_t done_offset, prev_done_offset, prev_parts, pad_done;
 };
 
 // One transmitted band, for kernels that walk the 32x32 blocks of all bands.
@@ -260,7 +278,11 @@ struct BandEntry
 	float quant_resolution;
 	uint32_t quant_code;
 	float rdo_scale;
-	int32_t level;
+	int32_t level, comp;
+	// Tile dataflow: the counter of the transform tile holding block rel of this
+	// band is done_index + rel (tiles and blocks share their row-major order);
+	// it is complete at done_parts.
+	int32_t done_index, done_parts;
 };
 
 constexpr int kMaxBands = 48;
@@ -277,6 +299,7 @@ struct ResolveParams
 	int32_t block_count_32x32, blocks_per_subdivision, subdivision_shift;
 	int32_t width, height, chroma444;
 	uint32_t target_words, sequence;
+	uint32_t fused_ctas; // tile dataflow: forward-level CTAs with a fused quantiser to wait for (0: none)
 };
 
 // cudaLaunchKernelEx configuration, optionally marked as a programmatic
@@ -373,6 +396,12 @@ constexpr int kSmallLevelTiles = 256;
 // whole CTA instead.
 constexpr int kFusedSplitTail = 2;
 constexpr int kSplitTailTiles = 2 * 148 * 4;
+// CTAs per tile of a small transform-only level (row stripes of the tile).
+constexpr int kDwtStripeCtas = 4;
+// Bounded waits of the tile dataflow (each poll sleeps about 64 ns or more):
+// about a second at most, after which the waiting CTA records kErrorLevelWait
+// and carries on.
+constexpr uint32_t kDataflowWaitSpins = 1u << 20;
 int forward_fused_mode(const LevelParams &p, bool fused_quant);
 void launch_dwt_forward_level(const LevelParams &p, const PlaneInput &in, const EncodeBuffers &buf,
                               const LevelTileMap *maps, bool fused_quant,

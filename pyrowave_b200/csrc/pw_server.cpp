@@ -42,7 +42,7 @@ size_t stream_state_bytes(const Geometry &g, size_t capacity_words)
 {
 	const size_t n8 = size_t(g.block_count_8x8), n32 = size_t(g.block_count_32x32);
 	const size_t coef = size_t(g.storage_elems32) * 4 + size_t(g.storage_elems16) * 2;
-	const size_t enc = coef + n8 * 4 + n32 * (16 * 2 + 16 + 16 * 4 + 4 + 8 + 4) + sizeof(RateControlState) +
+	const size_t enc = coef + n8 * 4 + n32 * (1024 * 2 + 16 * 2 + 16 + 16 * 4 + 4 + 8 + 4 + 4) + sizeof(RateControlState) +
 	                   capacity_words * 4;
 	const size_t dec = coef + n32 * 8;
 	return enc + dec;
