@@ -450,8 +450,8 @@ def run_ours(args, cfg, ws, rank, local):
     if dwt_ms:
         dwt_stage["frac_of_peak"] = round(dwt_stage["achieved_gbs"] / peak, 4)
 
-    e2e = run_e2e(args, cfg, frames, dev) if rank == 0 or ws > 1 else None
-    if ws > 1:
+    e2e = run_e2e(args, cfg, frames, dev) if (rank == 0 or ws > 1) and not getattr(args, "no_e2e", False) else None
+    if ws > 1 and e2e is not None:
         e2e["total_s"] = max_over_ranks([e2e["total_s"]], ws, "cuda")[0]
     psnr = None
     if rank == 0 and not args.no_configs:
@@ -489,9 +489,10 @@ def run_ours(args, cfg, ws, rank, local):
             "config": workload_config(cfg, frames, ws),
             "l2": l2_note,
             "wall_us_per_frame": round(plain_wall_ms * 1e3 / args.steps, 3),
-            "e2e": {"value": round(e2e["total_s"] * 1e6 / (e2e["frames"] * ws), 2), "unit": "us/frame",
-                    "h2d_bytes_per_step": e2e["h2d"], "d2h_bytes_per_step": e2e["d2h"],
-                    "method": e2e["method"], "breakdown_us": e2e["breakdown_us"]},
+            "e2e": None if e2e is None else {
+                "value": round(e2e["total_s"] * 1e6 / (e2e["frames"] * ws), 2), "unit": "us/frame",
+                "h2d_bytes_per_step": e2e["h2d"], "d2h_bytes_per_step": e2e["d2h"],
+                "method": e2e["method"], "breakdown_us": e2e["breakdown_us"]},
             "parity": PARITY,
             "psnr_delta_db": psnr,
             "gpu_launches": len(stages) * args.steps,  # one stage-timing tag per kernel launch
@@ -1192,6 +1193,8 @@ def main():
     ap.add_argument("--cpu-seconds", type=float, default=10.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-batch", action="store_true", help="skip the batched-form measurement")
+    ap.add_argument("--no-e2e", action="store_true",
+                    help="skip the end-to-end measurement through host buffers (profiling runs)")
     ap.add_argument("--batch-frames", type=int, default=64,
                     help="frames in the batched-form measurement (64: the batched benchmark's set)")
     ap.add_argument("--no-configs", action="store_true",
