@@ -471,6 +471,9 @@ def run_ours(args, cfg, ws, rank, local):
     secondary = None
     if rank == 0 and ws == 1 and not args.no_configs:
         secondary = run_secondary(steps=30, warmup=5)
+    packing = None
+    if rank == 0 and ws == 1 and not args.no_configs:
+        packing = run_packing_analysis(cfg, frames)
 
     if rank == 0:
         line = {
@@ -495,6 +498,7 @@ def run_ours(args, cfg, ws, rank, local):
                 "method": e2e["method"], "breakdown_us": e2e["breakdown_us"]},
             "parity": PARITY,
             "psnr_delta_db": psnr,
+            "packing_analysis": packing,
             "gpu_launches": len(stages) * args.steps,  # one stage-timing tag per kernel launch
             "roofline": roofline,
             "dwt_stage": dwt_stage,
@@ -516,6 +520,36 @@ def run_ours(args, cfg, ws, rank, local):
 
 
 BATCH_SIZES = [(1280, 720), (1366, 768), (1920, 1080), (2560, 1080), (2560, 1440), (3840, 2160)]
+
+
+PACKING_LAYOUTS = ["32x32/2x2", "32x32/4x2", "32x32/2x4", "64x32/4x4", "64x64/8x4"]
+
+
+def run_packing_analysis(cfg, frames):
+    """Packing statistics of the workload's first frame, computed on the device
+    (pyrowave_cuda_encoder_analyze_packing: the reference's disabled
+    report_stats / analyze_alternative_packing pass, pyrowave_encoder.cpp:625-958):
+    estimated bytes of five packet / sub-block shapes beside the coded bytes, and
+    the byte entropy of each magnitude plane position."""
+    from pyrowave_b200 import capi
+
+    w, h, c444, budget = cfg["width"], cfg["height"], cfg["chroma444"], cfg["budget"]
+    dev = capi.Device()
+    enc = capi.Encoder(dev, w, h, capi.CHROMA_444 if c444 else capi.CHROMA_420)
+    try:
+        assert enc.encode_cpu(frames[0], budget) == capi.PYROWAVE_SUCCESS
+        a = enc.analyze_packing()
+    finally:
+        enc.close()
+        dev.close()
+    coded = a["coded_bytes"]
+    planes = int(np.count_nonzero(a["plane_bytes"]))
+    return {"coded_bytes": coded, "significant": a["significant"],
+            "layout_bytes": {n: int(b) for n, b in zip(PACKING_LAYOUTS, a["layout_bytes"])},
+            "layout_vs_coded": {n: round(int(b) / coded, 4) if coded else None
+                                for n, b in zip(PACKING_LAYOUTS, a["layout_bytes"])},
+            "plane_bytes": [int(v) for v in a["plane_bytes"][:planes]],
+            "plane_entropy": [round(float(v), 4) for v in a["plane_entropy"][:planes]]}
 
 
 def run_packet_decode(cfg, frames, steps: int = 50, boundary: int = 8192):

@@ -139,6 +139,35 @@ typedef struct pyrowave_cuda_encoder_debug
 PYROWAVE_PUBLIC_API pyrowave_result pyrowave_cuda_encoder_read_debug(pyrowave_encoder encoder,
                                                                      const pyrowave_cuda_encoder_debug *debug);
 
+/* Packing statistics of the last encode, computed on the device (waits for the
+ * encode, then for its own kernel). The reference keeps this analysis as
+ * disabled code (pyrowave_encoder.cpp:625-958, Encoder::Impl::report_stats and
+ * analyze_alternative_packing); here it covers the current block format:
+ *   layout_bytes: estimated bytes of the frame's coded bands packed as 32x32
+ *     packets with 2x2, 4x2 (the current shape) and 2x4 sub-blocks, 64x32
+ *     packets with 4x4 and 64x64 packets with 8x4 sub-blocks (the reference's
+ *     analyze_cost over 64x64 regions of the quantised integers);
+ *   band_bytes: coded bytes (block words x 4) per component, level and band;
+ *     coded_bytes their sum (the frame minus its 8-byte sequence header);
+ *   significant: nonzero coefficients (one sign bit each);
+ *   plane_histogram[j]: the plane bytes at position j of their sub-block's run
+ *     of magnitude planes (0: most significant); plane_bytes[j] their count and
+ *     plane_entropy[j] their byte entropy in bits / 8 (1.0: incompressible).
+ * The first call on an encoder allocates its region table and accumulators. */
+typedef struct pyrowave_cuda_packing_analysis
+{
+	uint64_t layout_bytes[5];
+	uint64_t band_bytes[3][5][4];
+	uint64_t coded_bytes;
+	uint64_t significant;
+	uint64_t plane_bytes[16];
+	double plane_entropy[16];
+	uint32_t plane_histogram[16][256];
+} pyrowave_cuda_packing_analysis;
+
+PYROWAVE_PUBLIC_API pyrowave_result pyrowave_cuda_encoder_analyze_packing(pyrowave_encoder encoder,
+                                                                          pyrowave_cuda_packing_analysis *analysis);
+
 /* Decode the packets pushed so far into device planes on `stream` (uploads the
  * parsed payload, then dequantises and inverse transforms). */
 PYROWAVE_PUBLIC_API pyrowave_result pyrowave_cuda_decoder_decode(pyrowave_decoder decoder,

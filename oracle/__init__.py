@@ -113,6 +113,9 @@ def lib():
         L.oracle_dwt16.argtypes = [c_void_p, c_void_p, c_void_p, c_int, c_void_p]
         L.oracle_idwt16.restype = c_int
         L.oracle_idwt16.argtypes = [c_void_p, c_void_p, c_int, c_void_p, c_void_p]
+        L.oracle_analyze_packing.restype = c_int
+        L.oracle_analyze_packing.argtypes = [c_void_p, c_void_p, c_void_p, c_size_t, c_void_p, c_void_p, c_void_p,
+                                             c_void_p]
         L.oracle_float_to_half.restype = c_uint16
         L.oracle_float_to_half.argtypes = [c_float]
         L.oracle_half_to_float.restype = c_float
@@ -311,6 +314,23 @@ class Oracle:
             nwords = pay.size
         self.L.oracle_dequant(self.h, _ptr(off), _ptr(pay), nwords, mode, _ptr(out))
         return out
+
+    def analyze_packing(self, offsets: np.ndarray, payload: np.ndarray) -> dict:
+        """Packing statistics of a parsed frame (pyrowave_encoder.cpp:625-958): the
+        estimated bytes of the five alternative layouts, coded bytes per band,
+        the nonzero count and the plane-byte histograms."""
+        off = np.ascontiguousarray(offsets, np.uint32)
+        pay = np.ascontiguousarray(payload, np.uint32)
+        nwords = pay.size
+        if pay.size == 0:
+            pay = np.zeros(1, np.uint32)
+        layouts = np.zeros(5, np.uint64)
+        bands = np.zeros((3, 5, 4), np.uint64)
+        sig = np.zeros(1, np.uint64)
+        hist = np.zeros((16, 256), np.uint32)
+        self.L.oracle_analyze_packing(self.h, _ptr(off), _ptr(pay), nwords, _ptr(layouts), _ptr(bands), _ptr(sig),
+                                      _ptr(hist))
+        return {"layout_bytes": layouts, "band_bytes": bands, "significant": int(sig[0]), "plane_histogram": hist}
 
     def parser(self):
         return Parser(self)

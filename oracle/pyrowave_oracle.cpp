@@ -2095,3 +2095,174 @@ void oracle_hvs_dct8(const float *in, float *out)
 	hvs_dct8(out, s);
 }
 }
+
+// ---------------------------------------------------------------------------
+// Packing analysis: the reference's disabled statistics pass
+// (pyrowave_encoder.cpp:625-958, Encoder::Impl::report_stats and
+// analyze_alternative_packing) restated for the current block format. It reads
+// a decoded frame's integer coefficients back out of the bitstream and
+// estimates what other packet / block / sub-block shapes would cost.
+namespace
+{
+constexpr int kLayouts = 5;
+
+int magnitude_bits(uint32_t v) { return v ? 32 - __builtin_clz(v) : 0; }
+
+// analyze_cost<PacketW, PacketH, SubW, SubH> of pyrowave_encoder.cpp:650-713 on
+// one 64x64 region of quantised magnitudes: 8 bytes per packet holding any
+// significant value; per block (a packet's 4x4 grid) with one, 2 bits of plane
+// code per sub-block plus a byte of Q bits and scale, then the planes (each
+// sub-block at max(its magnitude bits, Q bits), Q bits = magnitude bits of the
+// block minus 3) and a sign bit per significant value, rounded up to bytes.
+template <int PW, int PH, int SW, int SH>
+uint64_t analyze_cost(const uint16_t (&v)[64][64])
+{
+	constexpr int BW = PW / 4, BH = PH / 4, NS = (BW / SW) * (BH / SH);
+	uint64_t cost = 0;
+	for (int py = 0; py < 64; py += PH)
+		for (int px = 0; px < 64; px += PW)
+		{
+			bool any = false;
+			for (int y = 0; y < PH; y++)
+				for (int x = 0; x < PW; x++)
+					any |= v[py + y][px + x] != 0;
+			if (any)
+				cost += 8;
+		}
+	for (int by = 0; by < 64; by += BH)
+		for (int bx = 0; bx < 64; bx += BW)
+		{
+			uint32_t mag = 0;
+			int nnz = 0;
+			for (int y = 0; y < BH; y++)
+				for (int x = 0; x < BW; x++)
+				{
+					mag = std::max<uint32_t>(mag, v[by + y][bx + x]);
+					nnz += v[by + y][bx + x] != 0;
+				}
+			if (mag == 0)
+				continue;
+			cost += 2 * NS / 8 + 1;
+			const int q_bits = std::max(magnitude_bits(mag) - 3, 0);
+			int weight_bits = 0;
+			for (int sy = 0; sy < BH; sy += SH)
+				for (int sx = 0; sx < BW; sx += SW)
+				{
+					uint32_t smag = 0;
+					for (int y = 0; y < SH; y++)
+						for (int x = 0; x < SW; x++)
+							smag = std::max<uint32_t>(smag, v[by + sy + y][bx + sx + x]);
+					weight_bits += SW * SH * std::max(magnitude_bits(smag), q_bits);
+				}
+			cost += uint64_t((weight_bits + nnz + 7) / 8);
+		}
+	return cost;
+}
+
+// The integer magnitudes of one coded 32x32 block, read from the stream the way
+// the dequantiser reads it (dequant_block above), into out (zeros when absent),
+// with each plane byte counted in hist by its position in the sub-block's run of
+// planes (0: most significant). Returns the block's word count (0 when absent).
+uint32_t decode_block_magnitudes(const uint32_t *offsets, const uint32_t *payload, size_t payload_words,
+                                 uint32_t block_index, uint16_t (&out)[32][32], uint32_t *hist, uint64_t &significant)
+{
+	memset(out, 0, sizeof(out));
+	const uint32_t offset_u32 = offsets[block_index];
+	if (offset_u32 == ~0u)
+		return 0;
+	const uint8_t *p8 = reinterpret_cast<const uint8_t *>(payload);
+	const size_t payload_bytes = payload_words * 4;
+	auto rd8 = [&](size_t i) -> uint32_t { return i < payload_bytes ? p8[i] : 0u; };
+	auto rd16 = [&](size_t i) -> uint32_t { return rd8(2 * i) | (rd8(2 * i + 1) << 8); };
+	auto rd32 = [&](size_t i) -> uint32_t { return i < payload_words ? payload[i] : 0u; };
+
+	const uint32_t header = rd32(offset_u32);
+	const uint32_t ballot = header & 0xffffu, words = (header >> 16) & 0xfffu;
+	const uint32_t nballot = uint32_t(popcount(ballot));
+	uint32_t byte_pos = offset_u32 * 4 + 8 + 3 * nballot;
+	for (int l = 0; l < 16; l++)
+	{
+		if (!((ballot >> l) & 1u))
+			continue;
+		const uint32_t local = uint32_t(popcount(ballot & ((1u << l) - 1u)));
+		const uint32_t cw = rd16(size_t(offset_u32) * 2 + 4 + local);
+		const uint32_t q_bits = rd8(size_t(offset_u32) * 4 + 8 + nballot * 2 + local) & 0xfu;
+		const int lx = l & 3, ly = l >> 2;
+		for (int s = 0; s < 8; s++)
+		{
+			const int planes = int(q_bits + ((cw >> (2 * s)) & 3u));
+			uint32_t dec[8] = {};
+			for (int j = 0; j < planes; j++)
+			{
+				const uint32_t pl = rd8(byte_pos++);
+				if (j < 16)
+					hist[j * 256 + pl]++;
+				for (int b = 0; b < 8; b++)
+					dec[b] |= ((pl >> b) & 1u) << (planes - 1 - j);
+			}
+			int sx, sy;
+			subblock_origin(s, sx, sy);
+			for (int b = 0; b < 8; b++)
+			{
+				int dx, dy;
+				pixel_offset(b, dx, dy);
+				out[ly * 8 + sy + dy][lx * 8 + sx + dx] = uint16_t(dec[b]);
+				significant += dec[b] != 0;
+			}
+		}
+	}
+	return words;
+}
+} // namespace
+
+extern "C" {
+// Packing statistics of one decoded frame (offsets and payload as the parser
+// returns them). layout_bytes[5]: analyze_cost over every 64x64 region of every
+// coded band (pyrowave_encoder.cpp:717-829) for 32x32 packets with 2x2, 4x2 and
+// 2x4 sub-blocks, 64x32 with 4x4 and 64x64 with 8x4; band_bytes[(c * 5 + level)
+// * 4 + band]: coded bytes (block words x 4, pyrowave_encoder.cpp:869-912);
+// hist[16 * 256]: plane bytes by position (pyrowave_encoder.cpp:884-895).
+int oracle_analyze_packing(const oracle_codec *c, const uint32_t *offsets, const uint32_t *payload,
+                           size_t payload_words, uint64_t *layout_bytes, uint64_t *band_bytes, uint64_t *significant,
+                           uint32_t *hist)
+{
+	memset(layout_bytes, 0, kLayouts * sizeof(uint64_t));
+	memset(band_bytes, 0, NumComponents * DecompositionLevels * 4 * sizeof(uint64_t));
+	memset(hist, 0, 16 * 256 * sizeof(uint32_t));
+	*significant = 0;
+	uint16_t region[64][64];
+	uint16_t block[32][32];
+	for (int comp = 0; comp < NumComponents; comp++)
+		for (int level = 0; level < DecompositionLevels; level++)
+			for (int band = 0; band < 4; band++)
+			{
+				if (!c->has_band(comp, level, band))
+					continue;
+				const BandInfo &info = c->bands[comp][level][band];
+				const int bw = (c->level_width(level) + 31) / 32, bh = (c->level_height(level) + 31) / 32;
+				for (int ry = 0; ry < (bh + 1) / 2; ry++)
+					for (int rx = 0; rx < (bw + 1) / 2; rx++)
+					{
+						memset(region, 0, sizeof(region));
+						for (int q = 0; q < 4; q++)
+						{
+							const int bx = 2 * rx + (q & 1), by = 2 * ry + (q >> 1);
+							if (bx >= bw || by >= bh)
+								continue;
+							const uint32_t bi = uint32_t(info.block_offset_32x32 + by * info.block_stride_32x32 + bx);
+							const uint32_t words =
+							    decode_block_magnitudes(offsets, payload, payload_words, bi, block, hist, *significant);
+							band_bytes[(comp * DecompositionLevels + level) * 4 + band] += uint64_t(words) * 4;
+							for (int y = 0; y < 32; y++)
+								memcpy(&region[(q >> 1) * 32 + y][(q & 1) * 32], block[y], sizeof(block[y]));
+						}
+						layout_bytes[0] += analyze_cost<32, 32, 2, 2>(region);
+						layout_bytes[1] += analyze_cost<32, 32, 4, 2>(region);
+						layout_bytes[2] += analyze_cost<32, 32, 2, 4>(region);
+						layout_bytes[3] += analyze_cost<64, 32, 4, 4>(region);
+						layout_bytes[4] += analyze_cost<64, 64, 8, 4>(region);
+					}
+			}
+	return 0;
+}
+}

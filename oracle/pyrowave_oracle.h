@@ -130,6 +130,17 @@ void oracle_psnr_hvs_m_tables(int height, float *out);
 uint64_t oracle_psnr_hvs_m_pixels(int width, int height);
 void oracle_hvs_dct8(const float *in, float *out);
 
+/* Packing analysis of a decoded frame (the reference's disabled statistics pass,
+ * pyrowave_encoder.cpp:625-958, for the current block format), from the
+ * parser's offsets and payload: layout_bytes[5] = estimated bytes of 32x32
+ * packets with 2x2, 4x2 and 2x4 sub-blocks, 64x32 with 4x4 and 64x64 with 8x4;
+ * band_bytes[(c * 5 + level) * 4 + band] = coded bytes; significant = nonzero
+ * coefficients; hist[16 * 256] = plane bytes by position in their sub-block's
+ * run of planes (0: most significant). */
+int oracle_analyze_packing(const oracle_codec *codec, const uint32_t *offsets, const uint32_t *payload,
+                           size_t payload_words, uint64_t *layout_bytes, uint64_t *band_bytes, uint64_t *significant,
+                           uint32_t *hist);
+
 /* Helpers exposed for unit tests. */
 uint16_t oracle_float_to_half(float v);
 float oracle_half_to_float(uint16_t h);

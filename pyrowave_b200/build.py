@@ -25,7 +25,7 @@ SONAME = "libpyrowave-shared.so.0"
 LIB = os.path.join(HERE, SONAME)
 LINK = os.path.join(HERE, "libpyrowave-shared.so")
 
-SOURCES = ["pw_encode.cu", "pw_decode.cu", "pw_packets.cu", "pw_quality.cu", "pw_host.cpp", "pw_server.cpp"]
+SOURCES = ["pw_encode.cu", "pw_decode.cu", "pw_packets.cu", "pw_quality.cu", "pw_analysis.cu", "pw_host.cpp", "pw_server.cpp"]
 HEADERS = ["pw_internal.h", "pw_device.cuh", "pw_decode_body.cuh"]
 PUBLIC_HEADERS = ["pyrowave.h", "pyrowave_cuda.h", "pyrowave_vk_types.h"]
 

@@ -60,7 +60,7 @@ API_SYMBOLS = [
     "pyrowave_cuda_device_set_stage_timing", "pyrowave_cuda_encoder_set_precision", "pyrowave_cuda_decoder_set_precision", "pyrowave_cuda_encoder_get_layout",
     "pyrowave_cuda_decoder_get_layout", "pyrowave_cuda_encoder_encode", "pyrowave_cuda_encoder_get_device_bitstream",
     "pyrowave_cuda_encoder_get_size", "pyrowave_cuda_encoder_encode_pre_transformed",
-    "pyrowave_cuda_encoder_read_wavelet", "pyrowave_cuda_encoder_read_debug", "pyrowave_cuda_encoder_transform", "pyrowave_cuda_decoder_decode",
+    "pyrowave_cuda_encoder_read_wavelet", "pyrowave_cuda_encoder_read_debug", "pyrowave_cuda_encoder_analyze_packing", "pyrowave_cuda_encoder_transform", "pyrowave_cuda_decoder_decode",
     "pyrowave_cuda_decoder_decode_blocks", "pyrowave_cuda_decoder_read_wavelet", "pyrowave_cuda_decoder_decode_pyramid",
     "pyrowave_cuda_decoder_decode_packets", "pyrowave_cuda_decoder_get_packet_status",
     "pyrowave_cuda_decoder_get_error", "pyrowave_cuda_decode_blocks_static",
@@ -124,6 +124,13 @@ class CudaEncoderDebug(Structure):
     _fields_ = [("code_words", c_void_p), ("rd_cost", c_void_p), ("rd_bucket", c_void_p), ("rd_dist", c_void_p),
                 ("histogram", c_void_p), ("consumed", c_void_p), ("quant", c_void_p), ("block_meta", c_void_p),
                 ("error_flags", c_void_p)]
+
+
+class PackingAnalysis(Structure):
+    _fields_ = [("layout_bytes", ctypes.c_uint64 * 5), ("band_bytes", ctypes.c_uint64 * 60),
+                ("coded_bytes", ctypes.c_uint64), ("significant", ctypes.c_uint64),
+                ("plane_bytes", ctypes.c_uint64 * 16), ("plane_entropy", ctypes.c_double * 16),
+                ("plane_histogram", c_uint32 * 4096)]
 
 
 class BatchFrameInfo(Structure):
@@ -201,6 +208,7 @@ def lib():
     L.pyrowave_cuda_encoder_read_wavelet.argtypes = [c_void_p, c_void_p, c_void_p]
     L.pyrowave_cuda_encoder_transform.argtypes = [c_void_p, POINTER(CudaPlanes), c_void_p]
     L.pyrowave_cuda_encoder_read_debug.argtypes = [c_void_p, POINTER(CudaEncoderDebug)]
+    L.pyrowave_cuda_encoder_analyze_packing.argtypes = [c_void_p, POINTER(PackingAnalysis)]
     L.pyrowave_cuda_decoder_decode.argtypes = [c_void_p, POINTER(CudaPlanes), c_void_p]
     L.pyrowave_cuda_decoder_decode_blocks.argtypes = [c_void_p, c_void_p, c_void_p, c_size_t, POINTER(CudaPlanes),
                                                       c_void_p]
@@ -445,6 +453,20 @@ class Encoder:
                                                             "consumed", "quant", "block_meta", "error_flags")])
         check(self.L.pyrowave_cuda_encoder_read_debug(self.h, ctypes.byref(dbg)), "read_debug")
         return d
+
+    def analyze_packing(self) -> dict:
+        """Packing statistics of the last encode (pyrowave_cuda_encoder_analyze_packing)."""
+        a = PackingAnalysis()
+        check(self.L.pyrowave_cuda_encoder_analyze_packing(self.h, ctypes.byref(a)), "analyze_packing")
+        return {
+            "layout_bytes": np.ctypeslib.as_array(a.layout_bytes).copy(),
+            "band_bytes": np.ctypeslib.as_array(a.band_bytes).reshape(3, 5, 4).copy(),
+            "coded_bytes": int(a.coded_bytes),
+            "significant": int(a.significant),
+            "plane_bytes": np.ctypeslib.as_array(a.plane_bytes).copy(),
+            "plane_entropy": np.ctypeslib.as_array(a.plane_entropy).copy(),
+            "plane_histogram": np.ctypeslib.as_array(a.plane_histogram).reshape(16, 256).copy(),
+        }
 
 
 class Decoder:

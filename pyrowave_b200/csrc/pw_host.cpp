@@ -763,6 +763,11 @@ struct pyrowave_encoder_opaque
 	// state in the same allocation (one clear covers both).
 	int tile_counters = 0;
 	uint32_t fused_ctas = 0;
+	// Packing analysis (allocated by its first call): the 64x64 region table and
+	// the device accumulators.
+	int32_t *analysis_regions = nullptr;
+	int analysis_region_count = 0;
+	PackingAnalysisAccum *analysis_acc = nullptr;
 	uint32_t *tile_done() const { return reinterpret_cast<uint32_t *>(rc + 1); }
 	size_t rc_bytes() const { return sizeof(RateControlState) + size_t(tile_counters) * 4; }
 
@@ -802,6 +807,11 @@ struct pyrowave_encoder_opaque
 		dev_free(block_meta);
 		dev_free(stream_buf);
 		dev_free(jobs_d);
+		dev_free(analysis_regions);
+		dev_free(analysis_acc);
+		analysis_regions = nullptr;
+		analysis_acc = nullptr;
+		analysis_region_count = 0;
 		for (auto &p : in_planes)
 			dev_free(p);
 		host_free(h_meta);
@@ -2363,6 +2373,96 @@ pyrowave_result pyrowave_cuda_encoder_read_debug(pyrowave_encoder encoder, const
 	if (d->error_flags)
 		cudaMemcpy(d->error_flags, &encoder->rc->error, 4, cudaMemcpyDeviceToHost);
 	return cudaGetLastError() == cudaSuccess ? PYROWAVE_SUCCESS : PYROWAVE_ERROR_GENERIC;
+}
+
+// The reference's disabled statistics pass (pyrowave_encoder.cpp:625-958) on the
+// device: every 64x64 region of every coded band, in the reference's band order
+// (component, level, band), as four 32x32 block indices.
+pyrowave_result pyrowave_cuda_encoder_analyze_packing(pyrowave_encoder encoder, pyrowave_cuda_packing_analysis *a)
+{
+	if (!encoder || !a || !encoder->allocated || !encoder->has_device_frame)
+		return PYROWAVE_ERROR_INVALID_ARGUMENT;
+	if (cudaEventSynchronize(encoder->encoded) != cudaSuccess)
+		return PYROWAVE_ERROR_GENERIC;
+	const Geometry &g = encoder->g;
+	if (!encoder->analysis_acc)
+	{
+		std::vector<int32_t> regions;
+		for (int comp = 0; comp < kComponents; comp++)
+			for (int level = 0; level < kLevels; level++)
+				for (int band = 0; band < 4; band++)
+				{
+					const BandDesc &B = g.band[comp][level][band];
+					if (!B.present)
+						continue;
+					const int bw = g.level[level].tiles_x, bh = g.level[level].tiles_y;
+					for (int ry = 0; ry < (bh + 1) / 2; ry++)
+						for (int rx = 0; rx < (bw + 1) / 2; rx++)
+						{
+							for (int q = 0; q < 4; q++)
+							{
+								const int bx = 2 * rx + (q & 1), by = 2 * ry + (q >> 1);
+								regions.push_back(bx < bw && by < bh ? B.block32_offset + by * B.block32_stride + bx : -1);
+							}
+							regions.push_back((comp * kLevels + level) * 4 + band);
+						}
+				}
+		bool ok = true;
+		int32_t *table = dev_alloc<int32_t>(regions.size(), ok);
+		PackingAnalysisAccum *acc = dev_alloc<PackingAnalysisAccum>(1, ok);
+		if (!ok || cudaMemcpy(table, regions.data(), regions.size() * 4, cudaMemcpyHostToDevice) != cudaSuccess)
+		{
+			dev_free(table);
+			dev_free(acc);
+			(void)cudaGetLastError();
+			return PYROWAVE_ERROR_OUT_OF_DEVICE_MEMORY;
+		}
+		encoder->analysis_regions = table;
+		encoder->analysis_acc = acc;
+		encoder->analysis_region_count = int(regions.size() / 5);
+	}
+	cudaStream_t stream = encoder->device->stream;
+	PackingAnalysisAccum host = {};
+	if (launch_packing_analysis(encoder->bp, encoder->buffers(), encoder->analysis_regions,
+	                            encoder->analysis_region_count, encoder->analysis_acc, stream) != cudaSuccess ||
+	    cudaMemcpyAsync(&host, encoder->analysis_acc, sizeof(host), cudaMemcpyDeviceToHost, stream) != cudaSuccess ||
+	    cudaStreamSynchronize(stream) != cudaSuccess)
+	{
+		(void)cudaGetLastError();
+		return PYROWAVE_ERROR_GENERIC;
+	}
+	memset(a, 0, sizeof(*a));
+	for (int i = 0; i < kPackingLayouts; i++)
+		a->layout_bytes[i] = host.layout_bytes[i];
+	for (int i = 0; i < kComponents * kLevels * 4; i++)
+	{
+		(&a->band_bytes[0][0][0])[i] = host.band_bytes[i];
+		a->coded_bytes += host.band_bytes[i];
+	}
+	a->significant = host.significant;
+	for (int j = 0; j < 16; j++)
+	{
+		uint64_t total = 0;
+		for (int b = 0; b < 256; b++)
+		{
+			a->plane_histogram[j][b] = host.plane_histogram[j * 256 + b];
+			total += host.plane_histogram[j * 256 + b];
+		}
+		a->plane_bytes[j] = total;
+		// Byte entropy of the plane, as a fraction of 8 bits (pyrowave_encoder.cpp:932-950).
+		double h = 0.0;
+		for (int b = 0; b < 256 && total; b++)
+		{
+			const uint32_t n = host.plane_histogram[j * 256 + b];
+			if (n)
+			{
+				const double pr = double(n) / double(total);
+				h -= pr * std::log2(pr);
+			}
+		}
+		a->plane_entropy[j] = h / 8.0;
+	}
+	return PYROWAVE_SUCCESS;
 }
 
 pyrowave_result pyrowave_cuda_decoder_decode(pyrowave_decoder decoder, const pyrowave_cuda_planes *planes,

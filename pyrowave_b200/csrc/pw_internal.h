@@ -312,6 +312,22 @@ struct LaunchConfig
 	LaunchConfig(const LaunchConfig &) = delete;
 };
 
+// Packing analysis (statistics of a coded frame beside the hot path): device
+// accumulators of packing_analysis_kernel, cleared by the launcher. Layouts:
+// 32x32 packets with 2x2, 4x2 and 2x4 sub-blocks, 64x32 with 4x4, 64x64 with 8x4.
+constexpr int kPackingLayouts = 5;
+struct PackingAnalysisAccum
+{
+	unsigned long long layout_bytes[kPackingLayouts];
+	unsigned long long band_bytes[kComponents * kLevels * 4]; // (component * 5 + level) * 4 + band
+	unsigned long long significant;
+	uint32_t plane_histogram[16 * 256];
+};
+// regions: 5 ints per 64x64 region of a coded band (four 32x32 block indices,
+// -1 beyond the band, then the band's slot).
+cudaError_t launch_packing_analysis(const BlockParams &p, const EncodeBuffers &buf, const int32_t *regions,
+                                    int num_regions, PackingAnalysisAccum *acc, cudaStream_t stream);
+
 // Frame layout without the job table; allocates nothing.
 bool make_geometry(Geometry &g, int width, int height, bool chroma444, uint32_t fp16_mask);
 LevelParams make_level_params(const Geometry &g, int level);
