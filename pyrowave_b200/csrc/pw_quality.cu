@@ -4,10 +4,14 @@
 // and its reference, without allocating anything.
 //
 // Work split: a half-warp per 8x8 window (windows at a stride of 4 samples).
-// Its 16 lanes stage the two windows in shared memory, eight of them run the
-// row and then the column DCTs of both windows (one 8-point DCT each), and
-// then lane f evaluates height factor f: the masking of both windows and the
-// CSF-weighted error of the window pair. The per-factor fixed-point (2^-24)
+// Its 16 lanes stage the two windows in shared memory (UNORM values from a
+// per-CTA table of x / 255), eight of them sum the four quadrants of both
+// windows for the masking's variances, all 16 run the row and then the column
+// DCTs (one 8-point DCT each), then each lane stores four coefficients' squares
+// and absolute differences for the window, and lane f evaluates height factor
+// f: the masking of both windows and the CSF-weighted error of the window
+// pair, reading the coefficient terms and its factor's tables four at a time.
+// The per-factor fixed-point (2^-24)
 // error sums are integers, so their accumulation (per lane, per CTA in shared
 // memory, then one global atomic per factor and CTA) is exact in any order.
 // Every floating-point operation is one rounded IEEE operation in the order
@@ -25,8 +29,9 @@ namespace pw
 namespace
 {
 constexpr int kHvsFactors = 16;
-constexpr int kHvsThreads = 128;
+constexpr int kHvsThreads = 256;
 constexpr int kHvsSlots = kHvsThreads / 16; // windows per CTA and round
+constexpr int kHvsPitch = 68;               // floats per factor row of the shared tables (16-byte rows, no bank conflicts)
 
 // The tables of all factors, factor-minor: entry [y * 8 + x][f], so the 16
 // lanes of a window read 16 consecutive words.
@@ -88,34 +93,41 @@ __device__ __forceinline__ float vari(float e, float e2, int count) // psnr_hvs_
 	return __fdiv_rn(fmaxf(__fsub_rn(__fmul_rn(e2, float(count)), __fmul_rn(e, e)), 0.0f), float(count - 1));
 }
 
-// The factor-independent part of maskeff (psnr_hvs_m.comp:109-153).
-__device__ float window_pop(const float (&sig)[8][9])
+// Sum and sum of squares of quadrant (y, x) = (q >> 1, q & 1) of a window, in
+// the row-major order of psnr_hvs_m.comp:115-126.
+__device__ __forceinline__ void quadrant_sums(const float (&sig)[8][9], int q, float &e, float &e2)
 {
-	float sum_e2[2][2], sum_e[2][2];
-	float sum_e2_total = 0.0f, sum_e_total = 0.0f;
-	for (int y = 0; y < 2; y++)
-		for (int x = 0; x < 2; x++)
+	const int y0 = (q >> 1) * 4, x0 = (q & 1) * 4;
+	e = 0.0f;
+	e2 = 0.0f;
+	for (int suby = 0; suby < 4; suby++)
+		for (int subx = 0; subx < 4; subx++)
 		{
-			float e = 0.0f, e2 = 0.0f;
-			for (int suby = 0; suby < 4; suby++)
-				for (int subx = 0; subx < 4; subx++)
-				{
-					const float v = sig[y * 4 + suby][x * 4 + subx];
-					e = __fadd_rn(e, v);
-					e2 = __fadd_rn(e2, __fmul_rn(v, v));
-				}
-			sum_e[y][x] = e;
-			sum_e2[y][x] = e2;
-			sum_e_total = __fadd_rn(sum_e_total, e);
-			sum_e2_total = __fadd_rn(sum_e2_total, e2);
+			const float v = sig[y0 + suby][x0 + subx];
+			e = __fadd_rn(e, v);
+			e2 = __fadd_rn(e2, __fmul_rn(v, v));
 		}
+}
+
+// The factor-independent part of maskeff (psnr_hvs_m.comp:109-153) from the
+// quadrant sums {e, e2} in quadrant order (0,0), (0,1), (1,0), (1,1): the
+// totals add them in that order, the variance ratio in the shader's order
+// (0,0), (1,0), (0,1), (1,1).
+__device__ float window_pop(const float (&quad)[4][2])
+{
+	float sum_e_total = 0.0f, sum_e2_total = 0.0f;
+	for (int q = 0; q < 4; q++)
+	{
+		sum_e_total = __fadd_rn(sum_e_total, quad[q][0]);
+		sum_e2_total = __fadd_rn(sum_e2_total, quad[q][1]);
+	}
 	float pop = vari(sum_e_total, sum_e2_total, 64);
 	if (pop != 0.0f)
 	{
-		float q = __fadd_rn(vari(sum_e[0][0], sum_e2[0][0], 16), vari(sum_e[1][0], sum_e2[1][0], 16));
-		q = __fadd_rn(q, vari(sum_e[0][1], sum_e2[0][1], 16));
-		q = __fadd_rn(q, vari(sum_e[1][1], sum_e2[1][1], 16));
-		pop = __fdiv_rn(q, pop);
+		float v = __fadd_rn(vari(quad[0][0], quad[0][1], 16), vari(quad[2][0], quad[2][1], 16));
+		v = __fadd_rn(v, vari(quad[1][0], quad[1][1], 16));
+		v = __fadd_rn(v, vari(quad[3][0], quad[3][1], 16));
+		pop = __fdiv_rn(v, pop);
 	}
 	return pop;
 }
@@ -125,16 +137,26 @@ __global__ void __launch_bounds__(kHvsThreads) psnr_hvs_m_kernel(const __grid_co
                                                                  const uint8_t *dist, const int dist_pitch,
                                                                  unsigned long long *errors)
 {
-	__shared__ float s_csf[64][kHvsFactors], s_mask[64][kHvsFactors], s_inv[64][kHvsFactors];
+	// Tables factor-major ([f][k], rows of kHvsPitch): lane f reads four
+	// consecutive coefficients of its own row as one 16-byte load.
+	__shared__ __align__(16) float s_csf[kHvsFactors][kHvsPitch], s_mask[kHvsFactors][kHvsPitch],
+	    s_inv[kHvsFactors][kHvsPitch];
+	__shared__ float s_unorm[256];
 	__shared__ float s_sig[kHvsSlots][2][8][9]; // [window][image][y][x], then the 2D DCT in place
+	// Per window and coefficient: a^2, b^2 and |a - b| of the two DCTs.
+	__shared__ __align__(16) float s_a2[kHvsSlots][64], s_b2[kHvsSlots][64], s_diff[kHvsSlots][64];
+	__shared__ float s_quad[kHvsSlots][2][4][2];
 	__shared__ float s_pop[kHvsSlots][2];
 	__shared__ unsigned long long s_err[kHvsFactors];
 	for (int i = threadIdx.x; i < 64 * kHvsFactors; i += kHvsThreads)
 	{
-		(&s_csf[0][0])[i] = (&hp.csf[0][0])[i];
-		(&s_mask[0][0])[i] = (&hp.mask[0][0])[i];
-		(&s_inv[0][0])[i] = (&hp.inv_mask[0][0])[i];
+		const int k = i / kHvsFactors, f = i % kHvsFactors;
+		s_csf[f][k] = (&hp.csf[0][0])[i];
+		s_mask[f][k] = (&hp.mask[0][0])[i];
+		s_inv[f][k] = (&hp.inv_mask[0][0])[i];
 	}
+	for (int i = threadIdx.x; i < 256; i += kHvsThreads)
+		s_unorm[i] = __fdiv_rn(float(i), 255.0f);
 	if (threadIdx.x < kHvsFactors)
 		s_err[threadIdx.x] = 0ull;
 	__syncthreads();
@@ -157,16 +179,15 @@ __global__ void __launch_bounds__(kHvsThreads) psnr_hvs_m_kernel(const __grid_co
 			const int px = wx + x, py = wy + y;
 			float v = 0.0f;
 			if (valid && px < hp.width && py < hp.height)
-			{
-				const uint8_t u = img == 0 ? ref[size_t(py) * ref_pitch + px] : dist[size_t(py) * dist_pitch + px];
-				v = __fdiv_rn(float(u), 255.0f);
-			}
+				v = s_unorm[img == 0 ? ref[size_t(py) * ref_pitch + px] : dist[size_t(py) * dist_pitch + px]];
 			sig[img][y][x] = v;
 		}
 		__syncwarp(half_mask);
-		if (l < 2)
-			s_pop[slot][l] = window_pop(sig[l]);
+		if (l < 8)
+			quadrant_sums(sig[l >> 2], l & 3, s_quad[slot][l >> 2][l & 3][0], s_quad[slot][l >> 2][l & 3][1]);
 		__syncwarp(half_mask);
+		if (l < 2)
+			s_pop[slot][l] = window_pop(s_quad[slot][l]);
 		// Row DCTs (lanes 0-7 the reference window, 8-15 the distorted one), then column DCTs.
 		{
 			const int img = l >> 3, r = l & 7;
@@ -184,25 +205,57 @@ __global__ void __launch_bounds__(kHvsThreads) psnr_hvs_m_kernel(const __grid_co
 				sig[img][i][r] = d[i];
 		}
 		__syncwarp(half_mask);
+		{
+			float a2[4], b2[4], df[4];
+#pragma unroll
+			for (int j = 0; j < 4; j++)
+			{
+				const int k = 4 * l + j;
+				const float a = sig[0][k >> 3][k & 7], b = sig[1][k >> 3][k & 7];
+				a2[j] = __fmul_rn(a, a);
+				b2[j] = __fmul_rn(b, b);
+				df[j] = fabsf(__fsub_rn(a, b));
+			}
+			*reinterpret_cast<float4 *>(&s_a2[slot][4 * l]) = make_float4(a2[0], a2[1], a2[2], a2[3]);
+			*reinterpret_cast<float4 *>(&s_b2[slot][4 * l]) = make_float4(b2[0], b2[1], b2[2], b2[3]);
+			*reinterpret_cast<float4 *>(&s_diff[slot][4 * l]) = make_float4(df[0], df[1], df[2], df[3]);
+		}
+		__syncwarp(half_mask);
 		// Height factor l: masking of both windows (maskeff), then the weighted error (dct_error).
 		{
 			float ma = 0.0f, mb = 0.0f;
-			for (int k = 0; k < 64; k++)
+#pragma unroll 4
+			for (int k = 0; k < 64; k += 4)
 			{
-				const float a = sig[0][k >> 3][k & 7], b = sig[1][k >> 3][k & 7];
-				ma = __fadd_rn(ma, __fmul_rn(__fmul_rn(a, a), s_mask[k][l]));
-				mb = __fadd_rn(mb, __fmul_rn(__fmul_rn(b, b), s_mask[k][l]));
+				const float4 A = *reinterpret_cast<const float4 *>(&s_a2[slot][k]);
+				const float4 B = *reinterpret_cast<const float4 *>(&s_b2[slot][k]);
+				const float4 M = *reinterpret_cast<const float4 *>(&s_mask[l][k]);
+				ma = __fadd_rn(ma, __fmul_rn(A.x, M.x));
+				mb = __fadd_rn(mb, __fmul_rn(B.x, M.x));
+				ma = __fadd_rn(ma, __fmul_rn(A.y, M.y));
+				mb = __fadd_rn(mb, __fmul_rn(B.y, M.y));
+				ma = __fadd_rn(ma, __fmul_rn(A.z, M.z));
+				mb = __fadd_rn(mb, __fmul_rn(B.z, M.z));
+				ma = __fadd_rn(ma, __fmul_rn(A.w, M.w));
+				mb = __fadd_rn(mb, __fmul_rn(B.w, M.w));
 			}
 			const float mask_a = __fdiv_rn(__fsqrt_rn(__fmul_rn(ma, s_pop[slot][0])), 32.0f);
 			const float mask_b = __fdiv_rn(__fsqrt_rn(__fmul_rn(mb, s_pop[slot][1])), 32.0f);
 			const float mask = fmaxf(mask_a, mask_b);
 			float total = 0.0f;
-			for (int k = 0; k < 64; k++)
+#pragma unroll 4
+			for (int k = 0; k < 64; k += 4)
 			{
-				const float e = fabsf(__fsub_rn(sig[0][k >> 3][k & 7], sig[1][k >> 3][k & 7]));
-				const float m = __fmul_rn(mask, s_inv[k][l]);
-				const float w = __fmul_rn(fmaxf(__fsub_rn(e, m), 0.0f), s_csf[k][l]);
-				total = __fadd_rn(total, __fmul_rn(w, w));
+				const float4 E = *reinterpret_cast<const float4 *>(&s_diff[slot][k]);
+				const float4 I = *reinterpret_cast<const float4 *>(&s_inv[l][k]);
+				const float4 C = *reinterpret_cast<const float4 *>(&s_csf[l][k]);
+				const float e[4] = {E.x, E.y, E.z, E.w}, inv[4] = {I.x, I.y, I.z, I.w}, csf[4] = {C.x, C.y, C.z, C.w};
+#pragma unroll
+				for (int j = 0; j < 4; j++)
+				{
+					const float w = __fmul_rn(fmaxf(__fsub_rn(e[j], __fmul_rn(mask, inv[j])), 0.0f), csf[j]);
+					total = __fadd_rn(total, __fmul_rn(w, w));
+				}
 			}
 			if (valid)
 				acc += __float2ull_rz(__fmul_rn(total, 16777216.0f)); // ldexp(total, 24), truncated
@@ -290,14 +343,27 @@ pyrowave_result pyrowave_cuda_psnr_hvs_m(int width, int height, const uint8_t *r
 	if (reference_stride < size_t(width) || distorted_stride < size_t(width) || reference_stride > 0x7fffffffu ||
 	    distorted_stride > 0x7fffffffu || (reinterpret_cast<uintptr_t>(errors) & 7u) != 0)
 		return PYROWAVE_ERROR_INVALID_ARGUMENT;
-	HvsParams hp;
-	hvs_tables(height, hp);
+	// The tables depend only on the plane height; each calling thread keeps the
+	// last height's (about 1000 exp/pow evaluations otherwise per call).
+	thread_local int table_height = -1;
+	thread_local HvsParams hp;
+	if (table_height != height)
+	{
+		hvs_tables(height, hp);
+		table_height = height;
+	}
 	hp.width = width;
 	hp.height = height;
 	hp.nbx = (width - 1) / 4 + 1;
 	hp.nby = (height - 1) / 4 + 1;
 	const int nwin = hp.nbx * hp.nby;
-	const int grid = std::max(1, std::min((nwin + kHvsSlots - 1) / kHvsSlots, 148 * 16));
+	// A few CTAs per SM, each looping over windows: every CTA copies the tables
+	// into shared memory once.
+	int device = 0, sms = 148;
+	if (cudaGetDevice(&device) != cudaSuccess ||
+	    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device) != cudaSuccess)
+		return PYROWAVE_ERROR_GENERIC;
+	const int grid = std::max(1, std::min((nwin + kHvsSlots - 1) / kHvsSlots, sms * 4));
 	psnr_hvs_m_kernel<<<grid, kHvsThreads, 0, reinterpret_cast<cudaStream_t>(stream)>>>(
 	    hp, reference, int(reference_stride), distorted, int(distorted_stride),
 	    reinterpret_cast<unsigned long long *>(errors));
