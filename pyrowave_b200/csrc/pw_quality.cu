@@ -9,9 +9,8 @@
 // windows for the masking's variances, all 16 run the row and then the column
 // DCTs (one 8-point DCT each), then each lane stores four coefficients' squares
 // and absolute differences for the window, and lane f evaluates height factor
-// f: the masking of both windows (the two sums as one f32x2 pair) and the
-// CSF-weighted error of the window pair (two coefficients per f32x2 operation),
-// reading the coefficient terms and its factor's tables 16 bytes at a time.
+// f: the masking of both windows and the CSF-weighted error of the window
+// pair, reading the coefficient terms and its factor's tables four at a time.
 // The per-factor fixed-point (2^-24)
 // error sums are integers, so their accumulation (per lane, per CTA in shared
 // memory, then one global atomic per factor and CTA) is exact in any order.
@@ -140,12 +139,12 @@ __global__ void __launch_bounds__(kHvsThreads) psnr_hvs_m_kernel(const __grid_co
 {
 	// Tables factor-major ([f][k], rows of kHvsPitch): lane f reads four
 	// consecutive coefficients of its own row as one 16-byte load.
-	__shared__ __align__(16) float s_csf[kHvsFactors][kHvsPitch], s_inv[kHvsFactors][kHvsPitch];
-	__shared__ __align__(16) float s_mask2[kHvsFactors][2 * kHvsPitch + 4]; // each entry twice: {m, m} pairs
+	__shared__ __align__(16) float s_csf[kHvsFactors][kHvsPitch], s_mask[kHvsFactors][kHvsPitch],
+	    s_inv[kHvsFactors][kHvsPitch];
 	__shared__ float s_unorm[256];
 	__shared__ float s_sig[kHvsSlots][2][8][9]; // [window][image][y][x], then the 2D DCT in place
-	// Per window and coefficient: {a^2, b^2} pairs and |a - b| of the two DCTs.
-	__shared__ __align__(16) float s_ab2[kHvsSlots][128], s_diff[kHvsSlots][64];
+	// Per window and coefficient: a^2, b^2 and |a - b| of the two DCTs.
+	__shared__ __align__(16) float s_a2[kHvsSlots][64], s_b2[kHvsSlots][64], s_diff[kHvsSlots][64];
 	__shared__ float s_quad[kHvsSlots][2][4][2];
 	__shared__ float s_pop[kHvsSlots][2];
 	__shared__ unsigned long long s_err[kHvsFactors];
@@ -153,7 +152,7 @@ __global__ void __launch_bounds__(kHvsThreads) psnr_hvs_m_kernel(const __grid_co
 	{
 		const int k = i / kHvsFactors, f = i % kHvsFactors;
 		s_csf[f][k] = (&hp.csf[0][0])[i];
-		s_mask2[f][2 * k] = s_mask2[f][2 * k + 1] = (&hp.mask[0][0])[i];
+		s_mask[f][k] = (&hp.mask[0][0])[i];
 		s_inv[f][k] = (&hp.inv_mask[0][0])[i];
 	}
 	for (int i = threadIdx.x; i < 256; i += kHvsThreads)
@@ -217,48 +216,45 @@ __global__ void __launch_bounds__(kHvsThreads) psnr_hvs_m_kernel(const __grid_co
 				b2[j] = __fmul_rn(b, b);
 				df[j] = fabsf(__fsub_rn(a, b));
 			}
-			*reinterpret_cast<float4 *>(&s_ab2[slot][8 * l]) = make_float4(a2[0], b2[0], a2[1], b2[1]);
-			*reinterpret_cast<float4 *>(&s_ab2[slot][8 * l + 4]) = make_float4(a2[2], b2[2], a2[3], b2[3]);
+			*reinterpret_cast<float4 *>(&s_a2[slot][4 * l]) = make_float4(a2[0], a2[1], a2[2], a2[3]);
+			*reinterpret_cast<float4 *>(&s_b2[slot][4 * l]) = make_float4(b2[0], b2[1], b2[2], b2[3]);
 			*reinterpret_cast<float4 *>(&s_diff[slot][4 * l]) = make_float4(df[0], df[1], df[2], df[3]);
 		}
 		__syncwarp(half_mask);
 		// Height factor l: masking of both windows (maskeff), then the weighted error (dct_error).
 		{
-			// Both windows' masking sums as one pair {ma, mb}, k in order.
-			f32x2 mab = f2_pack(0.0f, 0.0f);
+			float ma = 0.0f, mb = 0.0f;
 #pragma unroll 4
-			for (int k = 0; k < 64; k += 2)
+			for (int k = 0; k < 64; k += 4)
 			{
-				const ulonglong2 ab = *reinterpret_cast<const ulonglong2 *>(&s_ab2[slot][2 * k]);
-				const ulonglong2 m = *reinterpret_cast<const ulonglong2 *>(&s_mask2[l][2 * k]);
-				mab = f2_add_rn(mab, f2_mul_rn(ab.x, m.x));
-				mab = f2_add_rn(mab, f2_mul_rn(ab.y, m.y));
+				const float4 A = *reinterpret_cast<const float4 *>(&s_a2[slot][k]);
+				const float4 B = *reinterpret_cast<const float4 *>(&s_b2[slot][k]);
+				const float4 M = *reinterpret_cast<const float4 *>(&s_mask[l][k]);
+				ma = __fadd_rn(ma, __fmul_rn(A.x, M.x));
+				mb = __fadd_rn(mb, __fmul_rn(B.x, M.x));
+				ma = __fadd_rn(ma, __fmul_rn(A.y, M.y));
+				mb = __fadd_rn(mb, __fmul_rn(B.y, M.y));
+				ma = __fadd_rn(ma, __fmul_rn(A.z, M.z));
+				mb = __fadd_rn(mb, __fmul_rn(B.z, M.z));
+				ma = __fadd_rn(ma, __fmul_rn(A.w, M.w));
+				mb = __fadd_rn(mb, __fmul_rn(B.w, M.w));
 			}
-			float ma, mb;
-			f2_unpack(mab, ma, mb);
 			const float mask_a = __fdiv_rn(__fsqrt_rn(__fmul_rn(ma, s_pop[slot][0])), 32.0f);
 			const float mask_b = __fdiv_rn(__fsqrt_rn(__fmul_rn(mb, s_pop[slot][1])), 32.0f);
 			const float mask = fmaxf(mask_a, mask_b);
-			const f32x2 mask2 = f2_pack(mask, mask);
-			// The weighted error two coefficients at a time, added in order.
 			float total = 0.0f;
 #pragma unroll 4
 			for (int k = 0; k < 64; k += 4)
 			{
-				const ulonglong2 E = *reinterpret_cast<const ulonglong2 *>(&s_diff[slot][k]);
-				const ulonglong2 I = *reinterpret_cast<const ulonglong2 *>(&s_inv[l][k]);
-				const ulonglong2 C = *reinterpret_cast<const ulonglong2 *>(&s_csf[l][k]);
-				const f32x2 e2[2] = {E.x, E.y}, i2[2] = {I.x, I.y}, c2[2] = {C.x, C.y};
+				const float4 E = *reinterpret_cast<const float4 *>(&s_diff[slot][k]);
+				const float4 I = *reinterpret_cast<const float4 *>(&s_inv[l][k]);
+				const float4 C = *reinterpret_cast<const float4 *>(&s_csf[l][k]);
+				const float e[4] = {E.x, E.y, E.z, E.w}, inv[4] = {I.x, I.y, I.z, I.w}, csf[4] = {C.x, C.y, C.z, C.w};
 #pragma unroll
-				for (int j = 0; j < 2; j++)
+				for (int j = 0; j < 4; j++)
 				{
-					float d0, d1;
-					f2_unpack(f2_sub_rn(e2[j], f2_mul_rn(mask2, i2[j])), d0, d1);
-					const f32x2 w = f2_mul_rn(f2_pack(fmaxf(d0, 0.0f), fmaxf(d1, 0.0f)), c2[j]);
-					float w0, w1;
-					f2_unpack(f2_mul_rn(w, w), w0, w1);
-					total = __fadd_rn(total, w0);
-					total = __fadd_rn(total, w1);
+					const float w = __fmul_rn(fmaxf(__fsub_rn(e[j], __fmul_rn(mask, inv[j])), 0.0f), csf[j]);
+					total = __fadd_rn(total, __fmul_rn(w, w));
 				}
 			}
 			if (valid)
